@@ -1,0 +1,191 @@
+/*
+ * labinius_gpu.h — the C ABI of the B200 prover path for labinius.
+ *
+ * Every entry point replaces one call of the reference's scheme API (osdnk/labinius,
+ * crates/pcs/src/scheme/) for the commit / evaluate / fold hot path. The Rust `scheme` bodies call
+ * these through a thin `extern "C"` crate; the public Rust signatures stay.
+ *
+ * Conventions (after the only FFI the reference has, crates/pcs/src/labrador/ffi.rs:1-30):
+ *  - opaque, caller-owned handles with explicit free;
+ *  - plain pointers and sizes, host buffers caller-owned, little-endian;
+ *  - every call returns LBG_OK (0) or a negative status, with a message in lbg_last_error();
+ *    shape misuse the reference answers with a panic (assert!) is LBG_ERR_INVALID here; nothing
+ *    panics across the boundary.
+ *  - One handle is used from one host thread at a time (the reference's Prover is &mut).
+ *
+ * Layouts:
+ *  - F162: 3 x uint64 limbs, bits 128..161 in limb 2 (crates/pcs/src/fields/scalar.rs:10).
+ *  - Commitment matrix: int16 [columns][4 rows][limbs][162], centered, slot s of R_162 in the
+ *    reference's POW3_SLOT_EXP order — VerticallyAlignedMatrix column-major
+ *    (crates/pcs/src/ring/element.rs:72-117) with each PowerOfThreeRingElementWithLimbs flattened.
+ *  - Key (A): int16 [limbs][len_ring][648], row j of A_i in the reference's tree order, centered
+ *    (CommitmentKey::row, crates/pcs/src/key.rs:135-141, de-interleaved from Batch32).
+ *  - Folded witness: int16 [len_ring][648], centered coefficients (FoldedWitness,
+ *    crates/pcs/src/scheme/commitment.rs:249-279).
+ *  - Folded commitment: int16 [4 rows][limbs][162] (FoldedCommitment, :281-296).
+ *  - Dropped commitment: top uint16 [columns*648], digits uint16 [limbs-1][columns*648]
+ *    (crates/pcs/src/bd/mod.rs:7-56).
+ */
+#ifndef LABINIUS_GPU_H
+#define LABINIUS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBG_OK 0
+#define LBG_ERR_INVALID (-1)     /* shape or argument misuse (reference: assert! panics) */
+#define LBG_ERR_PARAMS (-2)      /* ParamError (crates/pcs/src/scheme/params.rs:20-50) */
+#define LBG_ERR_CUDA (-3)        /* a CUDA call failed */
+#define LBG_ERR_OOM (-4)         /* device allocation failed */
+#define LBG_ERR_UNSUPPORTED (-5) /* e.g. Opening::Recursive: LaBRADOR stays on the host */
+#define LBG_ERR_WITNESS (-6)     /* WitnessError::WrongLength (crates/pcs/src/scheme/witness.rs:10-23) */
+
+#define LBG_OPENING_CLEAR 0
+#define LBG_OPENING_BIT_DROPPED 1
+#define LBG_OPENING_RECURSIVE 2
+
+/* Params (crates/pcs/src/scheme/params.rs:62-68): the base modulus first, then the extra ones. */
+typedef struct lbg_params {
+  uint32_t witness_log_len;
+  uint32_t column_log_len;
+  uint32_t n_moduli;      /* 1 + extra_moduli.len() */
+  uint32_t moduli[7];     /* primes, base first: any of 2917, 3889, 4861, 9721, 12637, 17497, 19441 */
+  uint32_t opening;       /* LBG_OPENING_* */
+  uint32_t dropped_bits;  /* Opening::BitDropped { bits } */
+} lbg_params;
+
+/* ShortChallenge (crates/pcs/src/challenge.rs:227-235): 40 bytes. */
+typedef struct lbg_challenge {
+  uint8_t positions[32];
+  uint32_t signs;
+  uint32_t weight;
+} lbg_challenge;
+
+typedef struct lbg_pp lbg_pp;                 /* PublicParameters: params + device key */
+typedef struct lbg_prover lbg_prover;         /* Prover: stream + device workspace */
+typedef struct lbg_witness lbg_witness;       /* Witness: device-resident F162 (refcounted) */
+typedef struct lbg_opening lbg_opening;       /* CommitmentOpening: device handle */
+typedef struct lbg_transcript lbg_transcript; /* Transcript (host) */
+
+const char* lbg_last_error(void);
+int lbg_version(void);
+
+/* Params::with_base validation (crates/pcs/src/scheme/params.rs:172-203). */
+int lbg_params_check(const lbg_params* p);
+
+/* PublicParameters::from_seed (crates/pcs/src/scheme/params.rs:320-338): blake3 of the seed on
+ * the host, A expanded on the device (xorshift64*, crates/pcs/src/key.rs:48-88) and kept
+ * resident with its R_162 component form. */
+int lbg_public_parameters_from_seed(const lbg_params* p, const uint8_t matrix_seed[32], lbg_pp** out);
+void lbg_public_parameters_free(lbg_pp* pp);
+/* CommitmentKey::row (crates/pcs/src/key.rs:135-141) for every limb, into int16 [limbs][len_ring][648]. */
+int lbg_key_download(const lbg_pp* pp, int16_t* out);
+
+/* Prover::new (crates/pcs/src/scheme/prover.rs:31-53): device workspace + warm-up round. */
+int lbg_prover_new(const lbg_pp* pp, lbg_prover** out);
+void lbg_prover_free(lbg_prover* pr);
+
+/* Witness::from_elements (crates/pcs/src/scheme/witness.rs:54-62): upload n F162. */
+int lbg_witness_from_host(const lbg_pp* pp, const uint64_t* f162, size_t n, lbg_witness** out);
+/* Witness::random (crates/pcs/src/scheme/witness.rs:66-87), generated on the device. */
+int lbg_witness_random(const lbg_pp* pp, const uint8_t seed[32], lbg_witness** out);
+/* Witness::lifted (crates/pcs/src/scheme/witness.rs:45-52): B128 traces (2 x uint64) lifted. */
+int lbg_witness_lifted(const lbg_pp* pp, const uint64_t* b128, size_t n, lbg_witness** out);
+int lbg_witness_download(const lbg_witness* w, uint64_t* out, size_t n);
+void lbg_witness_free(lbg_witness* w);
+
+/* Prover::commit (crates/pcs/src/scheme/prover.rs:55-91, crates/pcs/src/key.rs:192-234,
+ * crates/pcs/src/bd/digits.rs:141-181). Clear mode fills matrix_out; bit-dropped mode fills
+ * top_out / digits_out. Any output pointer may be NULL (the value stays on the device, readable
+ * from the opening). The opening keeps a reference to the witness. */
+int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16_t* top_out,
+               uint16_t* digits_out, lbg_opening** opening_out);
+int lbg_opening_matrix(const lbg_opening* op, int16_t* matrix_out);
+int lbg_opening_dropped(const lbg_opening* op, uint16_t* top_out, uint16_t* digits_out);
+/* Prover::recycle (crates/pcs/src/scheme/prover.rs:116-118): drop an unfolded opening. */
+void lbg_opening_free(lbg_opening* op);
+
+/* Witness::row_evaluate (crates/pcs/src/scheme/witness.rs:100-106, crates/pcs/src/eval.rs:171-182):
+ * u_out = columns F162. */
+int lbg_row_evaluate(const lbg_pp* pp, const lbg_witness* w, const uint64_t* p0, size_t p0_len,
+                     uint64_t* u_out);
+/* Witness::mle_evaluate (crates/pcs/src/scheme/witness.rs:94-98, crates/pcs/src/eval.rs:185-193). */
+int lbg_mle_evaluate(const lbg_pp* pp, const lbg_witness* w, const uint64_t* p0, size_t p0_len,
+                     const uint64_t* p1, size_t p1_len, uint64_t out[3]);
+
+/* Prover::fold (crates/pcs/src/scheme/prover.rs:120-133, crates/pcs/src/fold.rs:659-677): consumes
+ * the opening (freed on return, also on error). v_out may be NULL (kept on the device). */
+int lbg_fold(lbg_prover* pr, lbg_opening* consumed, const lbg_challenge* challenges, size_t r,
+             int16_t* v_out);
+/* The last fold's result, int16 [len_ring][648]. */
+int lbg_prover_folded(const lbg_prover* pr, int16_t* v_out);
+
+/* Verifier::fold_commitment (crates/pcs/src/scheme/verifier.rs:114-146). */
+int lbg_fold_commitment(const lbg_pp* pp, const int16_t* matrix, size_t columns,
+                        const lbg_challenge* challenges, size_t r, int16_t* out);
+
+/* Transcript (crates/pcs/src/challenge.rs:66-161), host side. */
+lbg_transcript* lbg_transcript_new(const uint8_t* domain, size_t len);
+lbg_transcript* lbg_transcript_clone(const lbg_transcript* t);
+void lbg_transcript_free(lbg_transcript* t);
+void lbg_transcript_absorb_bytes(lbg_transcript* t, const uint8_t* b, size_t len);
+void lbg_transcript_absorb_u64(lbg_transcript* t, uint64_t x);
+void lbg_transcript_fill(lbg_transcript* t, const char* label, uint8_t* out, size_t n);
+/* sample_short_challenge (crates/pcs/src/challenge.rs:517-533). */
+int lbg_sample_short_challenge(lbg_transcript* t, uint32_t weight, double bound, lbg_challenge* out,
+                               uint64_t* attempts);
+/* Verifier::derive_evaluation_point (crates/pcs/src/scheme/verifier.rs:61-100): matrix (Clear) or
+ * top/digits (bit-dropped) as produced by lbg_commit. */
+int lbg_derive_evaluation_point(const lbg_pp* pp, lbg_transcript* t, const int16_t* matrix,
+                                const uint16_t* top, const uint16_t* digits, uint64_t* p0_out,
+                                uint64_t* p1_out);
+/* FoldingChallenges::derive (crates/pcs/src/scheme/commitment.rs:217-229). */
+int lbg_derive_folding_challenges(const lbg_pp* pp, lbg_transcript* t, const uint64_t* u,
+                                  lbg_challenge* out);
+/* wire::pack_dropped (crates/pcs/src/wire/mod.rs:386-397): returns the byte count; writes when
+ * out has room (cap). */
+size_t lbg_pack_dropped(const lbg_pp* pp, const uint16_t* top, const uint16_t* digits, uint8_t* out,
+                        size_t cap);
+
+/* The same three host steps from the parameters alone (no device handle): what a verifier that
+ * holds only Params and the seed runs. */
+int lbg_params_derive_evaluation_point(const lbg_params* p, const uint8_t matrix_seed[32], lbg_transcript* t,
+                                       const int16_t* matrix, const uint16_t* top, const uint16_t* digits,
+                                       uint64_t* p0_out, uint64_t* p1_out);
+int lbg_params_derive_folding_challenges(const lbg_params* p, lbg_transcript* t, const uint64_t* u,
+                                         lbg_challenge* out);
+size_t lbg_params_pack_dropped(const lbg_params* p, const uint16_t* top, const uint16_t* digits, uint8_t* out,
+                               size_t cap);
+
+/* Shape queries. */
+size_t lbg_pp_columns(const lbg_pp* pp);
+size_t lbg_pp_len_ring(const lbg_pp* pp);
+size_t lbg_pp_witness_len(const lbg_pp* pp);
+uint32_t lbg_pp_limbs(const lbg_pp* pp);
+
+/* Device synchronisation and timing support for benchmarks: the prover's CUDA stream. */
+void* lbg_prover_stream(const lbg_prover* pr);
+int lbg_prover_sync(lbg_prover* pr);
+/* Kernel accounting of a prover: with profiling on, every launch of the prover is bracketed by
+ * CUDA events on its stream; lbg_prover_kernel_stats reads (and keeps) the per-kernel totals of
+ * the launches since profiling was last switched on. Kernel names: "commit", "commit_finish",
+ * "challenge_slots", "fold", "column_residues", "garner". The launch counter counts every kernel
+ * launch of the prover, profiled or not. */
+int lbg_prover_profile(lbg_prover* pr, int enable);
+int lbg_prover_kernel_stats(lbg_prover* pr, const char* kernel, uint64_t* launches, double* total_ms);
+uint64_t lbg_prover_launch_count(const lbg_prover* pr);
+
+#ifdef __cplusplus
+}
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#endif /* LABINIUS_GPU_H */

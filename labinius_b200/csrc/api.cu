@@ -1,0 +1,844 @@
+// The C ABI of include/labinius_gpu.h: handles, device buffers, streams, and the per-call
+// drivers that chain the kernels of kernels.cu.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/labinius_gpu.h"
+#include "prime_structs.h"
+#include "launch.h"
+#include "ring_tables.h"
+#include "transcript.h"
+
+using namespace lbg;
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+}  // namespace
+
+#define LBG_CU(x)                                                                       \
+  do {                                                                                  \
+    cudaError_t e_ = (x);                                                               \
+    if (e_ != cudaSuccess) return fail(LBG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define LBG_ALLOC(ptr, bytes)                                                           \
+  do {                                                                                  \
+    cudaError_t e_ = cudaMalloc((void**)&(ptr), (bytes) ? (bytes) : 16);                \
+    if (e_ != cudaSuccess) {                                                            \
+      cudaGetLastError();                                                               \
+      return fail(LBG_ERR_OOM, std::string("cudaMalloc ") + std::to_string(bytes) + ": " + cudaGetErrorString(e_)); \
+    }                                                                                   \
+  } while (0)
+
+struct lbg_pp {
+  lbg_params params;
+  int limbs = 0;
+  uint32_t primes[7];
+  int pidx[7];
+  size_t cols = 0, wdim = 0, len_ring = 0, n = 0;
+  uint8_t seed[32];
+  uint64_t key_seed = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int16_t* d_A = nullptr;     // [limbs][len_ring][648]
+  int4* d_Ahat = nullptr;     // [limbs][len_ring][162][2]
+  DevPrime* d_prime[7] = {nullptr};
+  uint64_t* d_jumps = nullptr;
+  std::mutex mu;              // guards the scratch below (Witness::row_evaluate takes &self)
+  uint64_t* d_eq = nullptr;   // [wdim][3]
+  uint64_t* d_p = nullptr;    // point coordinates
+  uint64_t* d_u = nullptr;    // [cols][3]
+  uint64_t* d_out = nullptr;  // [3]
+  int16_t* d_C = nullptr;     // fold_commitment input [cols][4][limbs][162]
+  lbg_challenge_d* d_ch = nullptr;
+  uint32_t* d_chat = nullptr;  // [cols][162]
+  int16_t* d_fc = nullptr;     // [4][limbs][162]
+};
+
+struct lbg_witness {
+  std::atomic<int> refs{1};
+  uint64_t* d = nullptr;
+  size_t n = 0;
+  int device = 0;
+};
+
+struct lbg_prover {
+  const lbg_pp* pp = nullptr;
+  cudaStream_t stream = nullptr;
+  int chunk = 0, nchunks = 0;
+  int32_t* d_partial = nullptr;
+  lbg_challenge_d* d_ch = nullptr;
+  uint32_t* d_chat = nullptr;
+  int16_t* d_v = nullptr;     // [len_ring][648]
+  uint16_t* d_res = nullptr;  // [limbs][cols*648]
+  std::mutex mu;
+  std::vector<struct OpeningBufs*> spare;
+  // kernel accounting
+  uint64_t launches = 0;
+  bool profiling = false;
+  struct Mark {
+    const char* name;
+    cudaEvent_t a, b;
+  };
+  std::vector<Mark> marks;
+  std::vector<cudaEvent_t> event_pool;
+};
+
+// Brackets one launch of the prover with events when profiling is on, and counts it.
+struct KernelScope {
+  lbg_prover* pr;
+  const char* name;
+  cudaEvent_t a = nullptr, b = nullptr;
+  static cudaEvent_t take(lbg_prover* pr) {
+    if (!pr->event_pool.empty()) {
+      cudaEvent_t e = pr->event_pool.back();
+      pr->event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  KernelScope(lbg_prover* p, const char* n) : pr(p), name(n) {
+    pr->launches++;
+    if (pr->profiling) {
+      a = take(pr);
+      b = take(pr);
+      cudaEventRecord(a, pr->stream);
+    }
+  }
+  ~KernelScope() {
+    if (a) {
+      cudaEventRecord(b, pr->stream);
+      pr->marks.push_back({name, a, b});
+    }
+  }
+};
+
+struct OpeningBufs {
+  int16_t* d_C = nullptr;       // [cols][4][limbs][162]
+  uint16_t* d_top = nullptr;    // [cols*648]
+  uint16_t* d_digits = nullptr; // [limbs-1][cols*648]
+};
+
+struct lbg_opening {
+  lbg_prover* pr = nullptr;
+  lbg_witness* w = nullptr;
+  OpeningBufs* bufs = nullptr;
+};
+
+struct lbg_transcript {
+  Transcript t;
+  explicit lbg_transcript(const uint8_t* d, size_t n) : t(d, n) {}
+};
+
+static void witness_release(lbg_witness* w) {
+  if (w && w->refs.fetch_sub(1) == 1) {
+    cudaSetDevice(w->device);
+    cudaFree(w->d);
+    delete w;
+  }
+}
+
+extern "C" {
+
+const char* lbg_last_error(void) { return g_err.c_str(); }
+int lbg_version(void) { return 1; }
+
+// crates/pcs/src/scheme/params.rs:172-203, plus what this path supports.
+int lbg_params_check(const lbg_params* p) {
+  if (!p) return fail(LBG_ERR_INVALID, "null params");
+  if (p->column_log_len > p->witness_log_len) return fail(LBG_ERR_PARAMS, "column_log_len exceeds witness_log_len");
+  if (p->column_log_len < 1) return fail(LBG_ERR_PARAMS, "column_log_len must be at least 1");
+  if (p->witness_log_len - p->column_log_len < 7) return fail(LBG_ERR_PARAMS, "a column must hold at least 2^7 F162 elements");
+  if (p->n_moduli < 1 || p->n_moduli > 7) return fail(LBG_ERR_PARAMS, "between 1 and 7 moduli");
+  for (uint32_t i = 0; i < p->n_moduli; i++) {
+    if (prime_index(p->moduli[i]) < 0) return fail(LBG_ERR_PARAMS, "unsupported modulus " + std::to_string(p->moduli[i]));
+    for (uint32_t j = 0; j < i; j++)
+      if (p->moduli[j] == p->moduli[i])
+        return fail(LBG_ERR_PARAMS, j == 0 ? "the base modulus is listed again as an extra one" : "a modulus is listed twice");
+  }
+  if (p->opening == LBG_OPENING_RECURSIVE) return fail(LBG_ERR_UNSUPPORTED, "Opening::Recursive runs LaBRADOR on the host; not on this path");
+  if (p->opening == LBG_OPENING_BIT_DROPPED && (p->dropped_bits < 1 || p->dropped_bits > 14))
+    return fail(LBG_ERR_PARAMS, "dropped bits out of range");
+  if (p->opening > LBG_OPENING_RECURSIVE) return fail(LBG_ERR_PARAMS, "unknown opening mode");
+  if (p->witness_log_len > 30) return fail(LBG_ERR_PARAMS, "witness too large");
+  return LBG_OK;
+}
+
+static int upload_prime(lbg_pp* pp, int k) {
+  const PrimeTables& T = prime_tables(pp->primes[k]);
+  HotPrime h;
+  std::memcpy(h.tw, T.tw, sizeof(h.tw));
+  h.omega = T.omega;
+  h.omega_s = T.omega_s;
+  LBG_CU(upload_hot(pp->pidx[k], h));
+  DevPrime* D = new DevPrime();
+  std::memcpy(D->lut, T.lut, sizeof(D->lut));
+  std::memcpy(D->pow3_to_leaf, T.pow3_to_leaf, sizeof(D->pow3_to_leaf));
+  std::memcpy(D->leaf_to_pow3, T.leaf_to_pow3, sizeof(D->leaf_to_pow3));
+  std::memcpy(D->theta_leaf, T.theta_leaf, sizeof(D->theta_leaf));
+  std::memcpy(D->key_rows, T.key_rows, sizeof(D->key_rows));
+  std::memcpy(D->key_D, T.key_D, sizeof(D->key_D));
+  uint64_t q = T.q;
+  for (int L = 1; L <= 4; L++) {
+    int cnt = 2;
+    for (int l = 1; l < L; l++) cnt *= 3;
+    for (int kk = 0; kk < cnt; kk++) {
+      uint64_t zi = inv_mod(T.z_level[L][kk], q);
+      D->zinv3[L][kk] = (uint32_t)(zi * T.inv3 % q);
+      D->zinv3sq[L][kk] = (uint32_t)(zi * zi % q * T.inv3 % q);
+    }
+  }
+  D->omega = T.omega;
+  D->inv3 = T.inv3;
+  D->zeta6 = T.zeta6;
+  D->det0 = T.det0;
+  std::memcpy(D->chal, T.chal_table.data(), sizeof(D->chal));
+  cudaError_t e = cudaMalloc((void**)&pp->d_prime[k], sizeof(DevPrime));
+  if (e == cudaSuccess) e = cudaMemcpy(pp->d_prime[k], D, sizeof(DevPrime), cudaMemcpyHostToDevice);
+  delete D;
+  if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("prime tables: ") + cudaGetErrorString(e));
+  return LBG_OK;
+}
+
+void lbg_public_parameters_free(lbg_pp* pp) {
+  if (!pp) return;
+  cudaSetDevice(pp->device);
+  if (pp->stream) cudaStreamSynchronize(pp->stream);
+  cudaFree(pp->d_A);
+  cudaFree(pp->d_Ahat);
+  for (int k = 0; k < 7; k++) cudaFree(pp->d_prime[k]);
+  cudaFree(pp->d_jumps);
+  cudaFree(pp->d_eq);
+  cudaFree(pp->d_p);
+  cudaFree(pp->d_u);
+  cudaFree(pp->d_out);
+  cudaFree(pp->d_C);
+  cudaFree(pp->d_ch);
+  cudaFree(pp->d_chat);
+  cudaFree(pp->d_fc);
+  if (pp->stream) cudaStreamDestroy(pp->stream);
+  delete pp;
+}
+
+int lbg_public_parameters_from_seed(const lbg_params* p, const uint8_t matrix_seed[32], lbg_pp** out) {
+  if (!out || !matrix_seed) return fail(LBG_ERR_INVALID, "null argument");
+  *out = nullptr;
+  int rc = lbg_params_check(p);
+  if (rc) return rc;
+  lbg_pp* pp = new lbg_pp();
+  pp->params = *p;
+  pp->limbs = (int)p->n_moduli;
+  for (int k = 0; k < pp->limbs; k++) {
+    pp->primes[k] = p->moduli[k];
+    pp->pidx[k] = prime_index(p->moduli[k]);
+  }
+  pp->cols = (size_t)1 << p->column_log_len;
+  pp->wdim = (size_t)1 << (p->witness_log_len - p->column_log_len);
+  pp->len_ring = pp->wdim / 4;
+  pp->n = (size_t)1 << p->witness_log_len;
+  std::memcpy(pp->seed, matrix_seed, 32);
+  // crates/pcs/src/scheme/params.rs:321-322
+  Blake3 h;
+  h.update(matrix_seed, 32);
+  uint8_t d[8];
+  h.finalize(0, d, 8);
+  uint64_t s = 0;
+  for (int i = 7; i >= 0; i--) s = (s << 8) | d[i];
+  pp->key_seed = s;
+
+  auto bail = [&](int code) {
+    lbg_public_parameters_free(pp);
+    return code;
+  };
+  if (cudaGetDevice(&pp->device) != cudaSuccess) return bail(fail(LBG_ERR_CUDA, "no CUDA device"));
+  if (cudaStreamCreateWithFlags(&pp->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(LBG_ERR_CUDA, "stream"));
+  for (int k = 0; k < pp->limbs; k++)
+    if ((rc = upload_prime(pp, k))) return bail(rc);
+  const std::vector<uint64_t>& J = xorshift_jumps();
+  size_t a_elems = (size_t)pp->limbs * pp->len_ring * N648;
+  size_t ahat_elems = (size_t)pp->limbs * pp->len_ring * N162 * 2;
+  if (cudaMalloc((void**)&pp->d_jumps, J.size() * 8) != cudaSuccess ||
+      cudaMalloc((void**)&pp->d_A, a_elems * 2) != cudaSuccess ||
+      cudaMalloc((void**)&pp->d_Ahat, ahat_elems * sizeof(int4)) != cudaSuccess ||
+      cudaMalloc((void**)&pp->d_eq, pp->wdim * 24) != cudaSuccess ||
+      cudaMalloc((void**)&pp->d_p, 64 * 24) != cudaSuccess ||
+      cudaMalloc((void**)&pp->d_u, pp->cols * 24) != cudaSuccess ||
+      cudaMalloc((void**)&pp->d_out, 64) != cudaSuccess ||
+      cudaMalloc((void**)&pp->d_C, pp->cols * 4 * pp->limbs * N162 * 2) != cudaSuccess ||
+      cudaMalloc((void**)&pp->d_ch, pp->cols * sizeof(lbg_challenge_d)) != cudaSuccess ||
+      cudaMalloc((void**)&pp->d_chat, pp->cols * N162 * 4) != cudaSuccess ||
+      cudaMalloc((void**)&pp->d_fc, 4 * pp->limbs * N162 * 2) != cudaSuccess) {
+    cudaGetLastError();
+    return bail(fail(LBG_ERR_OOM, "public parameters: device allocation failed"));
+  }
+  if (cudaMemcpyAsync(pp->d_jumps, J.data(), J.size() * 8, cudaMemcpyHostToDevice, pp->stream) != cudaSuccess)
+    return bail(fail(LBG_ERR_CUDA, "jump tables"));
+  for (int k = 0; k < pp->limbs; k++) {
+    // crates/pcs/src/key.rs:68 and crates/pcs/src/rng.rs:6-8
+    uint64_t seed_k = pp->key_seed ^ (0x9E3779B9ull * (uint64_t)(k + 1));
+    uint64_t state0 = (seed_k * 0x9E3779B97F4A7C15ull) | 1;
+    int16_t* Ak = pp->d_A + (size_t)k * pp->len_ring * N648;
+    if (launch_key_expand(pp->d_jumps, state0, pp->primes[k], (int)(pp->len_ring / 32), Ak, pp->stream) != cudaSuccess ||
+        launch_key_components(pp->pidx[k], Ak, pp->d_prime[k], (int)pp->len_ring,
+                              pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2, pp->stream) != cudaSuccess)
+      return bail(fail(LBG_ERR_CUDA, std::string("key expansion: ") + cudaGetErrorString(cudaGetLastError())));
+  }
+  cudaError_t e = cudaStreamSynchronize(pp->stream);
+  if (e != cudaSuccess) return bail(fail(LBG_ERR_CUDA, std::string("key expansion: ") + cudaGetErrorString(e)));
+  *out = pp;
+  return LBG_OK;
+}
+
+int lbg_key_download(const lbg_pp* pp, int16_t* out) {
+  if (!pp || !out) return fail(LBG_ERR_INVALID, "null argument");
+  LBG_CU(cudaSetDevice(pp->device));
+  LBG_CU(cudaMemcpy(out, pp->d_A, (size_t)pp->limbs * pp->len_ring * N648 * 2, cudaMemcpyDeviceToHost));
+  return LBG_OK;
+}
+
+size_t lbg_pp_columns(const lbg_pp* pp) { return pp ? pp->cols : 0; }
+size_t lbg_pp_len_ring(const lbg_pp* pp) { return pp ? pp->len_ring : 0; }
+size_t lbg_pp_witness_len(const lbg_pp* pp) { return pp ? pp->n : 0; }
+uint32_t lbg_pp_limbs(const lbg_pp* pp) { return pp ? (uint32_t)pp->limbs : 0; }
+
+// ---------------------------------------------------------------------------------------------
+// witnesses
+// ---------------------------------------------------------------------------------------------
+static int witness_alloc(const lbg_pp* pp, size_t n, lbg_witness** out) {
+  lbg_witness* w = new lbg_witness();
+  w->n = n;
+  w->device = pp->device;
+  if (cudaMalloc((void**)&w->d, n * 24) != cudaSuccess) {
+    cudaGetLastError();
+    delete w;
+    return fail(LBG_ERR_OOM, "witness: device allocation failed");
+  }
+  *out = w;
+  return LBG_OK;
+}
+
+int lbg_witness_from_host(const lbg_pp* pp, const uint64_t* f162, size_t n, lbg_witness** out) {
+  if (!pp || !f162 || !out) return fail(LBG_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (n != pp->n) return fail(LBG_ERR_WITNESS, "the witness is not witness_len() elements");
+  LBG_CU(cudaSetDevice(pp->device));
+  lbg_witness* w;
+  int rc = witness_alloc(pp, n, &w);
+  if (rc) return rc;
+  if (cudaMemcpy(w->d, f162, n * 24, cudaMemcpyHostToDevice) != cudaSuccess) {
+    witness_release(w);
+    return fail(LBG_ERR_CUDA, "witness upload");
+  }
+  *out = w;
+  return LBG_OK;
+}
+
+int lbg_witness_lifted(const lbg_pp* pp, const uint64_t* b128, size_t n, lbg_witness** out) {
+  if (!pp || !b128 || !out) return fail(LBG_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (n != pp->n) return fail(LBG_ERR_WITNESS, "the witness is not witness_len() elements");
+  LBG_CU(cudaSetDevice(pp->device));
+  lbg_witness* w;
+  int rc = witness_alloc(pp, n, &w);
+  if (rc) return rc;
+  uint64_t* tmp = nullptr;
+  cudaError_t e = cudaMalloc((void**)&tmp, n * 16);
+  if (e == cudaSuccess) e = cudaMemcpy(tmp, b128, n * 16, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_lift_b128(tmp, n, w->d, pp->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(pp->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) {
+    witness_release(w);
+    return fail(LBG_ERR_CUDA, std::string("lifted witness: ") + cudaGetErrorString(e));
+  }
+  *out = w;
+  return LBG_OK;
+}
+
+int lbg_witness_random(const lbg_pp* pp, const uint8_t seed[32], lbg_witness** out) {
+  if (!pp || !seed || !out) return fail(LBG_ERR_INVALID, "null argument");
+  *out = nullptr;
+  LBG_CU(cudaSetDevice(pp->device));
+  lbg_witness* w;
+  int rc = witness_alloc(pp, pp->n, &w);
+  if (rc) return rc;
+  // keyed BLAKE3 of "labinius/witness": one chunk, one block, so the XOF is the root node's
+  // output blocks.
+  XofRoot root;
+  for (int i = 0; i < 8; i++)
+    root.cv[i] = (uint32_t)seed[4 * i] | ((uint32_t)seed[4 * i + 1] << 8) | ((uint32_t)seed[4 * i + 2] << 16) |
+                 ((uint32_t)seed[4 * i + 3] << 24);
+  uint8_t msg[64] = {0};
+  std::memcpy(msg, "labinius/witness", 16);
+  for (int i = 0; i < 16; i++)
+    root.m[i] = (uint32_t)msg[4 * i] | ((uint32_t)msg[4 * i + 1] << 8) | ((uint32_t)msg[4 * i + 2] << 16) |
+                ((uint32_t)msg[4 * i + 3] << 24);
+  root.block_len = 16;
+  root.flags = 16 | 1 | 2 | 8;  // keyed hash, chunk start, chunk end, root
+  cudaError_t e = launch_xof(root, pp->n * 24, (uint8_t*)w->d, pp->stream);
+  if (e == cudaSuccess) e = launch_mask_f162(w->d, pp->n, pp->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(pp->stream);
+  if (e != cudaSuccess) {
+    witness_release(w);
+    return fail(LBG_ERR_CUDA, std::string("random witness: ") + cudaGetErrorString(e));
+  }
+  *out = w;
+  return LBG_OK;
+}
+
+int lbg_witness_download(const lbg_witness* w, uint64_t* out, size_t n) {
+  if (!w || !out) return fail(LBG_ERR_INVALID, "null argument");
+  if (n != w->n) return fail(LBG_ERR_INVALID, "length mismatch");
+  LBG_CU(cudaSetDevice(w->device));
+  LBG_CU(cudaMemcpy(out, w->d, n * 24, cudaMemcpyDeviceToHost));
+  return LBG_OK;
+}
+
+void lbg_witness_free(lbg_witness* w) { witness_release(w); }
+
+// ---------------------------------------------------------------------------------------------
+// prover
+// ---------------------------------------------------------------------------------------------
+static void free_bufs(OpeningBufs* b) {
+  if (!b) return;
+  cudaFree(b->d_C);
+  cudaFree(b->d_top);
+  cudaFree(b->d_digits);
+  delete b;
+}
+
+void lbg_prover_free(lbg_prover* pr) {
+  if (!pr) return;
+  cudaSetDevice(pr->pp->device);
+  if (pr->stream) cudaStreamSynchronize(pr->stream);
+  cudaFree(pr->d_partial);
+  cudaFree(pr->d_ch);
+  cudaFree(pr->d_chat);
+  cudaFree(pr->d_v);
+  cudaFree(pr->d_res);
+  for (auto* b : pr->spare) free_bufs(b);
+  for (auto& m : pr->marks) {
+    cudaEventDestroy(m.a);
+    cudaEventDestroy(m.b);
+  }
+  for (auto e : pr->event_pool) cudaEventDestroy(e);
+  if (pr->stream) cudaStreamDestroy(pr->stream);
+  delete pr;
+}
+
+static int get_bufs(lbg_prover* pr, OpeningBufs** out) {
+  {
+    std::lock_guard<std::mutex> g(pr->mu);
+    if (!pr->spare.empty()) {
+      *out = pr->spare.back();
+      pr->spare.pop_back();
+      return LBG_OK;
+    }
+  }
+  const lbg_pp* pp = pr->pp;
+  OpeningBufs* b = new OpeningBufs();
+  size_t count = pp->cols * N648;
+  if (cudaMalloc((void**)&b->d_C, pp->cols * 4 * pp->limbs * N162 * 2) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_top, count * 2) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_digits, (pp->limbs > 1 ? pp->limbs - 1 : 1) * count * 2) != cudaSuccess) {
+    cudaGetLastError();
+    free_bufs(b);
+    return fail(LBG_ERR_OOM, "opening: device allocation failed");
+  }
+  *out = b;
+  return LBG_OK;
+}
+
+int lbg_prover_new(const lbg_pp* pp, lbg_prover** out) {
+  if (!pp || !out) return fail(LBG_ERR_INVALID, "null argument");
+  *out = nullptr;
+  LBG_CU(cudaSetDevice(pp->device));
+  lbg_prover* pr = new lbg_prover();
+  pr->pp = pp;
+  auto bail = [&](int code) {
+    lbg_prover_free(pr);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&pr->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(LBG_ERR_CUDA, "stream"));
+  // Grid: ceil(cols / 32) column tiles x nchunks ring-element chunks, aiming at >= 2 waves of 148.
+  int col_tiles = (int)((pp->cols + commit_cols_per_cta() - 1) / commit_cols_per_cta());
+  int want = (296 + col_tiles - 1) / col_tiles;
+  int max_chunks = (int)(pp->len_ring / 16);
+  if (max_chunks < 1) max_chunks = 1;
+  pr->nchunks = want < max_chunks ? want : max_chunks;
+  int step = commit_ring_per_step();
+  pr->chunk = (int)((pp->len_ring + pr->nchunks - 1) / pr->nchunks);
+  pr->chunk = (pr->chunk + step - 1) / step * step;
+  pr->nchunks = (int)((pp->len_ring + pr->chunk - 1) / pr->chunk);
+  size_t count = pp->cols * N648;
+  if (cudaMalloc((void**)&pr->d_partial, (size_t)pr->nchunks * pp->cols * N162 * 16) != cudaSuccess ||
+      cudaMalloc((void**)&pr->d_ch, pp->cols * sizeof(lbg_challenge_d)) != cudaSuccess ||
+      cudaMalloc((void**)&pr->d_chat, pp->cols * N162 * 4) != cudaSuccess ||
+      cudaMalloc((void**)&pr->d_v, pp->len_ring * N648 * 2) != cudaSuccess ||
+      cudaMalloc((void**)&pr->d_res, (size_t)pp->limbs * count * 2) != cudaSuccess) {
+    cudaGetLastError();
+    return bail(fail(LBG_ERR_OOM, "prover workspace: device allocation failed"));
+  }
+  // warm-up: one commitment and one fold of a zero witness (crates/pcs/src/scheme/prover.rs:31-53)
+  lbg_witness* zw = nullptr;
+  int rc = witness_alloc(pp, pp->n, &zw);
+  if (rc) return bail(rc);
+  if (cudaMemsetAsync(zw->d, 0, pp->n * 24, pr->stream) != cudaSuccess) {
+    witness_release(zw);
+    return bail(fail(LBG_ERR_CUDA, "warm-up"));
+  }
+  lbg_opening* op = nullptr;
+  rc = lbg_commit(pr, zw, nullptr, nullptr, nullptr, &op);
+  witness_release(zw);
+  if (rc) return bail(rc);
+  std::vector<lbg_challenge> zero(pp->cols);
+  std::memset(zero.data(), 0, zero.size() * sizeof(lbg_challenge));
+  rc = lbg_fold(pr, op, zero.data(), pp->cols, nullptr);
+  if (rc) return bail(rc);
+  if (cudaStreamSynchronize(pr->stream) != cudaSuccess) return bail(fail(LBG_ERR_CUDA, "warm-up sync"));
+  *out = pr;
+  return LBG_OK;
+}
+
+void* lbg_prover_stream(const lbg_prover* pr) { return pr ? (void*)pr->stream : nullptr; }
+
+int lbg_prover_profile(lbg_prover* pr, int enable) {
+  if (!pr) return fail(LBG_ERR_INVALID, "null prover");
+  LBG_CU(cudaSetDevice(pr->pp->device));
+  LBG_CU(cudaStreamSynchronize(pr->stream));
+  for (auto& m : pr->marks) {
+    pr->event_pool.push_back(m.a);
+    pr->event_pool.push_back(m.b);
+  }
+  pr->marks.clear();
+  pr->profiling = enable != 0;
+  return LBG_OK;
+}
+
+int lbg_prover_kernel_stats(lbg_prover* pr, const char* kernel, uint64_t* launches, double* total_ms) {
+  if (!pr || !kernel) return fail(LBG_ERR_INVALID, "null argument");
+  LBG_CU(cudaSetDevice(pr->pp->device));
+  LBG_CU(cudaStreamSynchronize(pr->stream));
+  uint64_t n = 0;
+  double ms = 0;
+  for (auto& m : pr->marks) {
+    if (std::strcmp(m.name, kernel) != 0) continue;
+    float t = 0;
+    LBG_CU(cudaEventElapsedTime(&t, m.a, m.b));
+    n++;
+    ms += t;
+  }
+  if (launches) *launches = n;
+  if (total_ms) *total_ms = ms;
+  return LBG_OK;
+}
+
+uint64_t lbg_prover_launch_count(const lbg_prover* pr) { return pr ? pr->launches : 0; }
+int lbg_prover_sync(lbg_prover* pr) {
+  if (!pr) return fail(LBG_ERR_INVALID, "null prover");
+  LBG_CU(cudaStreamSynchronize(pr->stream));
+  return LBG_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// commit
+// ---------------------------------------------------------------------------------------------
+int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16_t* top_out,
+               uint16_t* digits_out, lbg_opening** opening_out) {
+  if (!pr || !w) return fail(LBG_ERR_INVALID, "null argument");
+  const lbg_pp* pp = pr->pp;
+  if (w->n != pp->n) return fail(LBG_ERR_INVALID, "the witness was built for other parameters");
+  LBG_CU(cudaSetDevice(pp->device));
+  OpeningBufs* b = nullptr;
+  int rc = get_bufs(pr, &b);
+  if (rc) return rc;
+  cudaStream_t st = pr->stream;
+  int cols = (int)pp->cols, L = pp->limbs;
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < L && e == cudaSuccess; k++) {
+    {
+      KernelScope ks(pr, "commit");
+      e = launch_commit(pp->pidx[k], w->d, pp->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2,
+                        pp->d_prime[k], cols, (int)pp->len_ring, pr->chunk, pr->nchunks, pr->d_partial, st);
+    }
+    if (e == cudaSuccess) {
+      KernelScope ks(pr, "commit_finish");
+      e = launch_commit_finish(pp->pidx[k], pr->d_partial, pr->nchunks, cols, pp->d_prime[k], k, L, b->d_C, st);
+    }
+  }
+  bool bd = pp->params.opening == LBG_OPENING_BIT_DROPPED;
+  size_t count = pp->cols * N648;
+  if (bd && e == cudaSuccess) {
+    for (int k = 0; k < L && e == cudaSuccess; k++) {
+      KernelScope ks(pr, "column_residues");
+      e = launch_column_residues(pp->pidx[k], b->d_C, cols, k, L, pp->d_prime[k], pr->d_res + (size_t)k * count, st);
+    }
+    if (e == cudaSuccess) {
+      GarnerConsts g;
+      std::memset(&g, 0, sizeof(g));
+      for (int k = 0; k < L; k++) {
+        g.q[k] = pp->primes[k];
+        for (int m = 0; m < k; m++) g.inv[k][m] = (uint32_t)inv_mod(pp->primes[m], pp->primes[k]);
+      }
+      g.dropped_bits = pp->params.dropped_bits;
+      KernelScope ks(pr, "garner");
+      e = launch_garner(pr->d_res, count, L, g, b->d_top, b->d_digits, st);
+    }
+  }
+  if (e == cudaSuccess && matrix_out && !bd)
+    e = cudaMemcpyAsync(matrix_out, b->d_C, pp->cols * 4 * L * N162 * 2, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && bd && top_out) e = cudaMemcpyAsync(top_out, b->d_top, count * 2, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && bd && digits_out && L > 1)
+    e = cudaMemcpyAsync(digits_out, b->d_digits, (size_t)(L - 1) * count * 2, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && (matrix_out || top_out || digits_out)) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    std::lock_guard<std::mutex> g(pr->mu);
+    pr->spare.push_back(b);
+    return fail(LBG_ERR_CUDA, std::string("commit: ") + cudaGetErrorString(e));
+  }
+  lbg_opening* op = new lbg_opening();
+  op->pr = pr;
+  op->w = const_cast<lbg_witness*>(w);
+  op->w->refs.fetch_add(1);
+  op->bufs = b;
+  if (opening_out)
+    *opening_out = op;
+  else
+    lbg_opening_free(op);
+  return LBG_OK;
+}
+
+int lbg_opening_matrix(const lbg_opening* op, int16_t* matrix_out) {
+  if (!op || !matrix_out) return fail(LBG_ERR_INVALID, "null argument");
+  const lbg_pp* pp = op->pr->pp;
+  LBG_CU(cudaSetDevice(pp->device));
+  LBG_CU(cudaMemcpyAsync(matrix_out, op->bufs->d_C, pp->cols * 4 * pp->limbs * N162 * 2, cudaMemcpyDeviceToHost,
+                         op->pr->stream));
+  LBG_CU(cudaStreamSynchronize(op->pr->stream));
+  return LBG_OK;
+}
+
+int lbg_opening_dropped(const lbg_opening* op, uint16_t* top_out, uint16_t* digits_out) {
+  if (!op) return fail(LBG_ERR_INVALID, "null argument");
+  const lbg_pp* pp = op->pr->pp;
+  if (pp->params.opening != LBG_OPENING_BIT_DROPPED) return fail(LBG_ERR_INVALID, "this commitment is not bit-dropped");
+  size_t count = pp->cols * N648;
+  LBG_CU(cudaSetDevice(pp->device));
+  if (top_out) LBG_CU(cudaMemcpyAsync(top_out, op->bufs->d_top, count * 2, cudaMemcpyDeviceToHost, op->pr->stream));
+  if (digits_out && pp->limbs > 1)
+    LBG_CU(cudaMemcpyAsync(digits_out, op->bufs->d_digits, (size_t)(pp->limbs - 1) * count * 2,
+                           cudaMemcpyDeviceToHost, op->pr->stream));
+  LBG_CU(cudaStreamSynchronize(op->pr->stream));
+  return LBG_OK;
+}
+
+void lbg_opening_free(lbg_opening* op) {
+  if (!op) return;
+  {
+    std::lock_guard<std::mutex> g(op->pr->mu);
+    op->pr->spare.push_back(op->bufs);
+  }
+  // the last reference frees the witness with cudaFree, which waits for the device first
+  cudaSetDevice(op->pr->pp->device);
+  witness_release(op->w);
+  delete op;
+}
+
+// ---------------------------------------------------------------------------------------------
+// evaluation
+// ---------------------------------------------------------------------------------------------
+int lbg_row_evaluate(const lbg_pp* pp_c, const lbg_witness* w, const uint64_t* p0, size_t p0_len, uint64_t* u_out) {
+  if (!pp_c || !w || !p0 || !u_out) return fail(LBG_ERR_INVALID, "null argument");
+  lbg_pp* pp = const_cast<lbg_pp*>(pp_c);
+  if (p0_len != (size_t)(pp->params.witness_log_len - pp->params.column_log_len) || w->n != pp->n)
+    return fail(LBG_ERR_INVALID, "the evaluation point does not match the witness");
+  std::lock_guard<std::mutex> g(pp->mu);
+  LBG_CU(cudaSetDevice(pp->device));
+  LBG_CU(cudaMemcpyAsync(pp->d_p, p0, p0_len * 24, cudaMemcpyHostToDevice, pp->stream));
+  LBG_CU(launch_eq_table(pp->d_p, (int)p0_len, pp->wdim, pp->d_eq, pp->stream));
+  LBG_CU(launch_row_eval(w->d, pp->wdim, (int)pp->cols, pp->d_eq, pp->d_u, pp->stream));
+  LBG_CU(cudaMemcpyAsync(u_out, pp->d_u, pp->cols * 24, cudaMemcpyDeviceToHost, pp->stream));
+  LBG_CU(cudaStreamSynchronize(pp->stream));
+  return LBG_OK;
+}
+
+int lbg_mle_evaluate(const lbg_pp* pp_c, const lbg_witness* w, const uint64_t* p0, size_t p0_len, const uint64_t* p1,
+                     size_t p1_len, uint64_t out[3]) {
+  if (!pp_c || !w || !p0 || !p1 || !out) return fail(LBG_ERR_INVALID, "null argument");
+  lbg_pp* pp = const_cast<lbg_pp*>(pp_c);
+  if (p0_len != (size_t)(pp->params.witness_log_len - pp->params.column_log_len) ||
+      p1_len != (size_t)pp->params.column_log_len || w->n != pp->n)
+    return fail(LBG_ERR_INVALID, "the evaluation point does not match the witness");
+  std::lock_guard<std::mutex> g(pp->mu);
+  LBG_CU(cudaSetDevice(pp->device));
+  LBG_CU(cudaMemcpyAsync(pp->d_p, p0, p0_len * 24, cudaMemcpyHostToDevice, pp->stream));
+  LBG_CU(cudaMemcpyAsync(pp->d_p + 3 * 32, p1, p1_len * 24, cudaMemcpyHostToDevice, pp->stream));
+  LBG_CU(launch_eq_table(pp->d_p, (int)p0_len, pp->wdim, pp->d_eq, pp->stream));
+  LBG_CU(launch_row_eval(w->d, pp->wdim, (int)pp->cols, pp->d_eq, pp->d_u, pp->stream));
+  LBG_CU(launch_claim(pp->d_u, (int)pp->cols, pp->d_p + 3 * 32, (int)p1_len, pp->d_out, pp->stream));
+  LBG_CU(cudaMemcpyAsync(out, pp->d_out, 24, cudaMemcpyDeviceToHost, pp->stream));
+  LBG_CU(cudaStreamSynchronize(pp->stream));
+  return LBG_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// fold
+// ---------------------------------------------------------------------------------------------
+int lbg_fold(lbg_prover* pr, lbg_opening* op, const lbg_challenge* challenges, size_t r, int16_t* v_out) {
+  if (!pr || !op) return fail(LBG_ERR_INVALID, "null argument");
+  const lbg_pp* pp = pr->pp;
+  int rc = LBG_OK;
+  if (op->pr != pr) rc = fail(LBG_ERR_INVALID, "the opening belongs to another prover");
+  else if (!challenges || r != pp->cols) rc = fail(LBG_ERR_INVALID, "one challenge per column");
+  if (rc) {
+    lbg_opening_free(op);
+    return rc;
+  }
+  cudaSetDevice(pp->device);
+  cudaStream_t st = pr->stream;
+  cudaError_t e = cudaMemcpyAsync(pr->d_ch, challenges, r * sizeof(lbg_challenge), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    KernelScope ks(pr, "challenge_slots");
+    e = launch_challenge_slots(pp->pidx[0], pr->d_ch, (int)r, pp->d_prime[0], pr->d_chat, st);
+  }
+  if (e == cudaSuccess) {
+    KernelScope ks(pr, "fold");
+    e = launch_fold(pp->pidx[0], op->w->d, pp->wdim, (int)pp->cols, pr->d_chat, pp->d_prime[0], pr->d_v, st);
+  }
+  if (e == cudaSuccess && v_out) e = cudaMemcpyAsync(v_out, pr->d_v, pp->len_ring * N648 * 2, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && v_out) e = cudaStreamSynchronize(st);
+  lbg_opening_free(op);
+  if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("fold: ") + cudaGetErrorString(e));
+  return LBG_OK;
+}
+
+int lbg_prover_folded(const lbg_prover* pr, int16_t* v_out) {
+  if (!pr || !v_out) return fail(LBG_ERR_INVALID, "null argument");
+  LBG_CU(cudaSetDevice(pr->pp->device));
+  LBG_CU(cudaMemcpyAsync(v_out, pr->d_v, pr->pp->len_ring * N648 * 2, cudaMemcpyDeviceToHost, pr->stream));
+  LBG_CU(cudaStreamSynchronize(pr->stream));
+  return LBG_OK;
+}
+
+int lbg_fold_commitment(const lbg_pp* pp_c, const int16_t* matrix, size_t columns, const lbg_challenge* challenges,
+                        size_t r, int16_t* out) {
+  if (!pp_c || !matrix || !challenges || !out) return fail(LBG_ERR_INVALID, "null argument");
+  lbg_pp* pp = const_cast<lbg_pp*>(pp_c);
+  if (columns != pp->cols || r != columns) return fail(LBG_ERR_INVALID, "one challenge per column");
+  std::lock_guard<std::mutex> g(pp->mu);
+  LBG_CU(cudaSetDevice(pp->device));
+  int L = pp->limbs;
+  LBG_CU(cudaMemcpyAsync(pp->d_C, matrix, pp->cols * 4 * L * N162 * 2, cudaMemcpyHostToDevice, pp->stream));
+  LBG_CU(cudaMemcpyAsync(pp->d_ch, challenges, r * sizeof(lbg_challenge), cudaMemcpyHostToDevice, pp->stream));
+  for (int k = 0; k < L; k++) {
+    LBG_CU(launch_challenge_slots(pp->pidx[k], pp->d_ch, (int)r, pp->d_prime[k], pp->d_chat, pp->stream));
+    LBG_CU(launch_fold_commitment(pp->pidx[k], pp->d_C, (int)pp->cols, k, L, pp->d_chat, pp->d_prime[k], pp->d_fc,
+                                  pp->stream));
+  }
+  LBG_CU(cudaMemcpyAsync(out, pp->d_fc, 4 * L * N162 * 2, cudaMemcpyDeviceToHost, pp->stream));
+  LBG_CU(cudaStreamSynchronize(pp->stream));
+  return LBG_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// transcript (host)
+// ---------------------------------------------------------------------------------------------
+lbg_transcript* lbg_transcript_new(const uint8_t* domain, size_t len) { return new lbg_transcript(domain, len); }
+lbg_transcript* lbg_transcript_clone(const lbg_transcript* t) { return t ? new lbg_transcript(*t) : nullptr; }
+void lbg_transcript_free(lbg_transcript* t) { delete t; }
+void lbg_transcript_absorb_bytes(lbg_transcript* t, const uint8_t* b, size_t len) { t->t.absorb_bytes(b, len); }
+void lbg_transcript_absorb_u64(lbg_transcript* t, uint64_t x) { t->t.absorb_u64(x); }
+void lbg_transcript_fill(lbg_transcript* t, const char* label, uint8_t* out, size_t n) { t->t.fill(label, out, n); }
+
+int lbg_sample_short_challenge(lbg_transcript* t, uint32_t weight, double bound, lbg_challenge* out, uint64_t* attempts) {
+  if (!t || !out) return fail(LBG_ERR_INVALID, "null argument");
+  if (weight > 32 || weight > 162) return fail(LBG_ERR_INVALID, "weight exceeds MAX_WEIGHT = 32");
+  Challenge c = sample_short_challenge(t->t, weight, bound, attempts);
+  std::memcpy(out, &c, sizeof(c));
+  return LBG_OK;
+}
+
+static RoundShape shape_of_params(const lbg_params* p, const uint8_t* seed) {
+  RoundShape s;
+  s.witness_log_len = p->witness_log_len;
+  s.column_log_len = p->column_log_len;
+  s.limbs = p->n_moduli;
+  s.dropped_bits = p->opening == LBG_OPENING_BIT_DROPPED ? p->dropped_bits : 0;
+  for (int k = 0; k < 8; k++) s.primes[k] = k < (int)p->n_moduli ? p->moduli[k] : 0;
+  if (seed)
+    std::memcpy(s.matrix_seed, seed, 32);
+  else
+    std::memset(s.matrix_seed, 0, 32);
+  return s;
+}
+static RoundShape shape_of(const lbg_pp* pp) { return shape_of_params(&pp->params, pp->seed); }
+
+static int derive_point(const RoundShape& s, lbg_transcript* t, const int16_t* matrix, const uint16_t* top,
+                        const uint16_t* digits, uint64_t* p0_out, uint64_t* p1_out) {
+  if (s.dropped_bits == 0 && !matrix) return fail(LBG_ERR_INVALID, "a Clear commitment needs its matrix");
+  if (s.dropped_bits > 0 && (!top || (!digits && s.limbs > 1)))
+    return fail(LBG_ERR_INVALID, "a bit-dropped commitment needs its digits");
+  derive_evaluation_point(s, t->t, matrix, top, digits, p0_out, p1_out);
+  return LBG_OK;
+}
+
+int lbg_params_derive_evaluation_point(const lbg_params* p, const uint8_t matrix_seed[32], lbg_transcript* t,
+                                       const int16_t* matrix, const uint16_t* top, const uint16_t* digits,
+                                       uint64_t* p0_out, uint64_t* p1_out) {
+  if (!p || !matrix_seed || !t || !p0_out || !p1_out) return fail(LBG_ERR_INVALID, "null argument");
+  int rc = lbg_params_check(p);
+  if (rc) return rc;
+  return derive_point(shape_of_params(p, matrix_seed), t, matrix, top, digits, p0_out, p1_out);
+}
+
+int lbg_params_derive_folding_challenges(const lbg_params* p, lbg_transcript* t, const uint64_t* u,
+                                         lbg_challenge* out) {
+  if (!p || !t || !u || !out) return fail(LBG_ERR_INVALID, "null argument");
+  int rc = lbg_params_check(p);
+  if (rc) return rc;
+  derive_folding_challenges(shape_of_params(p, nullptr), t->t, u, (Challenge*)out);
+  return LBG_OK;
+}
+
+size_t lbg_params_pack_dropped(const lbg_params* p, const uint16_t* top, const uint16_t* digits, uint8_t* out,
+                               size_t cap) {
+  if (!p || !top || lbg_params_check(p) != LBG_OK || p->opening != LBG_OPENING_BIT_DROPPED) return 0;
+  std::vector<uint8_t> b = pack_dropped(shape_of_params(p, nullptr), top, digits);
+  if (out && cap >= b.size()) std::memcpy(out, b.data(), b.size());
+  return b.size();
+}
+
+int lbg_derive_evaluation_point(const lbg_pp* pp, lbg_transcript* t, const int16_t* matrix, const uint16_t* top,
+                                const uint16_t* digits, uint64_t* p0_out, uint64_t* p1_out) {
+  if (!pp || !t || !p0_out || !p1_out) return fail(LBG_ERR_INVALID, "null argument");
+  return derive_point(shape_of(pp), t, matrix, top, digits, p0_out, p1_out);
+}
+
+int lbg_derive_folding_challenges(const lbg_pp* pp, lbg_transcript* t, const uint64_t* u, lbg_challenge* out) {
+  if (!pp || !t || !u || !out) return fail(LBG_ERR_INVALID, "null argument");
+  derive_folding_challenges(shape_of(pp), t->t, u, (Challenge*)out);
+  return LBG_OK;
+}
+
+size_t lbg_pack_dropped(const lbg_pp* pp, const uint16_t* top, const uint16_t* digits, uint8_t* out, size_t cap) {
+  if (!pp || !top) return 0;
+  std::vector<uint8_t> b = pack_dropped(shape_of(pp), top, digits);
+  if (out && cap >= b.size()) std::memcpy(out, b.data(), b.size());
+  return b.size();
+}
+
+}  // extern "C"

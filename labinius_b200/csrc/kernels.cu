@@ -1,0 +1,693 @@
+// Kernels of the B200 prover path. Launch wrappers at the bottom dispatch on the prime index.
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+#include "launch.h"
+
+namespace lbg {
+
+// =============================================================================================
+// Key expansion: A from xorshift64* (crates/pcs/src/rng.rs:6-19, crates/pcs/src/key.rs:63-80)
+// =============================================================================================
+// Draw d of limb k's stream is the state after d + 1 steps; thread (b, j) produces the 32 draws
+// (b * 648 + j) * 32 + p, p < 32, i.e. row j of ring elements 32 b + p. The start state is reached
+// with the GF(2) jump matrices T^(2^t) (64 columns each).
+__global__ void k_key_expand(const uint64_t* __restrict__ jumps, uint64_t state0, uint32_t q,
+                             int nb, int16_t* __restrict__ A /* [len_ring][648] */) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nb * N648) return;
+  int b = gid / N648, j = gid % N648;
+  uint64_t d0 = ((uint64_t)b * N648 + j) * 32;
+  uint64_t s = state0;
+  for (int t = 0; t < 40; t++) {
+    if (!((d0 >> t) & 1)) continue;
+    const uint64_t* M = jumps + t * 64;
+    uint64_t r = 0;
+    for (int c = 0; c < 64; c++) r ^= M[c] & (0 - ((s >> c) & 1));
+    s = r;
+  }
+  int16_t half = (int16_t)((q - 1) / 2);
+  for (int p = 0; p < 32; p++) {
+    s ^= s >> 12;
+    s ^= s << 25;
+    s ^= s >> 27;
+    uint64_t out = s * 0x2545F4914F6CDD1Dull;
+    uint32_t below = (uint32_t)(((out >> 32) * (uint64_t)q) >> 32);
+    A[(size_t)(32 * b + p) * N648 + j] = (int16_t)((int16_t)below - half);
+  }
+}
+
+// The key in component form: for ring element i and leaf j of the 162-point tree,
+// Ahat[i][j] = (a_0, a_1, a_2, a_3, theta^v a_1, theta^v a_2, theta^v a_3, 0), the R_162 slot
+// values of A_i's four components (the decomposition of crates/pcs/src/ring/mod.rs:217-426
+// applied to the key), centered.
+template <int PI>
+__global__ void k_key_components(const int16_t* __restrict__ A, const DevPrime* __restrict__ D,
+                                 int len_ring, int4* __restrict__ Ahat /* [len_ring][162][2] */) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= len_ring * N162) return;
+  constexpr int32_t q = Pr<PI>::q;
+  int i = gid / N162, s = gid % N162;
+  const int16_t* a = A + (size_t)i * N648;
+  uint32_t e[4];
+  for (int t = 0; t < 4; t++) {
+    int32_t x = a[D->key_rows[s][t]];
+    e[t] = (uint32_t)(x < 0 ? x + q : x);
+  }
+  uint32_t y[4];
+  for (int k = 0; k < 4; k++) {
+    uint64_t acc = 0;
+    for (int t = 0; t < 4; t++) acc += (uint64_t)D->key_D[s][k][t] * e[t];
+    y[k] = (uint32_t)(acc % q);
+  }
+  int leaf = D->pow3_to_leaf[s];
+  uint32_t th = D->theta_leaf[leaf];
+  int4 lo, hi;
+  lo.x = center<PI>(y[0]);
+  lo.y = center<PI>(y[1]);
+  lo.z = center<PI>(y[2]);
+  lo.w = center<PI>(y[3]);
+  hi.x = center<PI>(mulmod<PI>(th, y[1]));
+  hi.y = center<PI>(mulmod<PI>(th, y[2]));
+  hi.z = center<PI>(mulmod<PI>(th, y[3]));
+  hi.w = 0;
+  Ahat[((size_t)i * N162 + leaf) * 2] = lo;
+  Ahat[((size_t)i * N162 + leaf) * 2 + 1] = hi;
+}
+
+// =============================================================================================
+// Commit: Y_j(v) = sum_i Ahat_i(v) (x) What_{j,i}(v) per column j and leaf v
+// =============================================================================================
+// CTA: 32 columns x a chunk of ring elements, two ring elements per step.
+//  phase A: warp w transforms F162 number (w & 3) of ring element (w >> 2) for its lane's column
+//           into smem What[ii][v][lane][k] (u16, fully reduced);
+//  phase B: warp w owns the leaves v = w + 8 u; each lane accumulates its column's four components
+//           Y_0..Y_3 for those leaves: 16 multiply-adds per (ring element, leaf).
+constexpr int CT = 32;            // columns per CTA
+constexpr int RT = 2;             // ring elements per step
+constexpr int VPW = 21;           // leaves per warp (8 warps, 162 leaves)
+
+template <int PI>
+__device__ __forceinline__ void commit_phase_a_store(uint16_t* __restrict__ wt, int ii, int k, int lane,
+                                                     const uint32_t idx[7], const uint32_t* lut) {
+  uint32_t v[27];
+#define LBG_BLOCK(TAU)                                                                 \
+  ntt_block<PI, TAU>(idx, lut, v);                                                     \
+  _Pragma("unroll") for (int x = 0; x < 27; x++) wt[(((ii * N162) + TAU * 27 + x) * CT + lane) * 4 + k] = (uint16_t)v[x];
+  LBG_BLOCK(0)
+  LBG_BLOCK(1)
+  LBG_BLOCK(2)
+  LBG_BLOCK(3)
+  LBG_BLOCK(4)
+  LBG_BLOCK(5)
+#undef LBG_BLOCK
+}
+
+// Steps between two fold-backs of the signed accumulators: each step adds at most
+// RT * 4 * (q-1)/2 * (q-1) per lane, and a fold-back leaves |acc| < 2q.
+template <int PI>
+struct CommitRed {
+  static constexpr int raw =
+      (int)((2147483647ull - 2ull * Pr<PI>::q) / ((uint64_t)RT * 4 * ((Pr<PI>::q - 1) / 2) * (Pr<PI>::q - 1)));
+  static constexpr int value = raw < 1 ? 1 : raw;
+};
+
+template <int PI>
+__global__ void __launch_bounds__(256, 1)
+    k_commit(const uint64_t* __restrict__ W, size_t wdim, const int4* __restrict__ Ahat,
+             const DevPrime* __restrict__ D, int cols, int len_ring, int chunk,
+             int32_t* __restrict__ partial /* [nchunks][cols][162][4] */) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* lut = (uint32_t*)smem;                                  // 6 * 64 u32
+  uint64_t* wtile = (uint64_t*)(smem + 6 * 64 * 4);                 // CT * RT * 4 * 3 u64
+  uint16_t* wt = (uint16_t*)(smem + 6 * 64 * 4 + CT * RT * 4 * 24);  // RT * 162 * CT * 4 u16
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int j0 = blockIdx.x * CT;
+  const int i_begin = blockIdx.y * chunk;
+  const int i_end = min(len_ring, i_begin + chunk);
+  for (int x = tid; x < 6 * 64; x += 256) lut[x] = D->lut[x / 64][x % 64];
+
+  int32_t acc[VPW][4];
+#pragma unroll
+  for (int u = 0; u < VPW; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
+  constexpr int RED = CommitRed<PI>::value;
+  int since = 0;
+
+  for (int i0 = i_begin; i0 < i_end; i0 += RT) {
+    __syncthreads();
+    // stage the witness tile: column jj, ring elements i0, i0+1 -> 8 F162 = 24 u64, contiguous
+    for (int x = tid; x < CT * RT * 12; x += 256) {
+      int jj = x / (RT * 12), wd = x % (RT * 12);
+      int j = j0 + jj;
+      uint64_t val = 0;
+      size_t f = (size_t)4 * i0 + wd / 3;  // F162 index inside the column
+      if (j < cols && f < (size_t)4 * i_end) val = W[((size_t)j * wdim + f) * 3 + wd % 3];
+      wtile[x] = val;
+    }
+    __syncthreads();
+    {
+      int ii = warp >> 2, k = warp & 3;
+      const uint64_t* e = wtile + lane * (RT * 12) + (ii * 4 + k) * 3;
+      uint32_t idx[7];
+      f162_windows(e[0], e[1], e[2], idx);
+      commit_phase_a_store<PI>(wt, ii, k, lane, idx, lut);
+    }
+    __syncthreads();
+    const int nsteps = min(RT, i_end - i0);
+    for (int ii = 0; ii < nsteps; ii++) {
+      const int4* ah = Ahat + (size_t)(i0 + ii) * N162 * 2;
+#pragma unroll
+      for (int u = 0; u < VPW; u++) {
+        int v = warp + 8 * u;
+        if (v < N162) {
+          uint2 wv = *(const uint2*)(wt + (((ii * N162) + v) * CT + lane) * 4);
+          int32_t w0 = wv.x & 0xFFFF, w1 = wv.x >> 16, w2 = wv.y & 0xFFFF, w3 = wv.y >> 16;
+          int4 lo = __ldg(ah + 2 * v), hi = __ldg(ah + 2 * v + 1);
+          acc[u][0] += lo.x * w0 + hi.x * w3 + hi.y * w2 + hi.z * w1;
+          acc[u][1] += lo.y * w0 + lo.x * w1 + hi.y * w3 + hi.z * w2;
+          acc[u][2] += lo.z * w0 + lo.y * w1 + lo.x * w2 + hi.z * w3;
+          acc[u][3] += lo.w * w0 + lo.z * w1 + lo.y * w2 + lo.x * w3;
+        }
+      }
+    }
+    if (++since >= RED) {
+      since = 0;
+#pragma unroll
+      for (int u = 0; u < VPW; u++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[u][c] = red_signed<PI>(acc[u][c]);
+    }
+  }
+  const int j = j0 + lane;
+  if (j < cols) {
+#pragma unroll
+    for (int u = 0; u < VPW; u++) {
+      int v = warp + 8 * u;
+      if (v < N162) {
+        int4 o;
+        o.x = (int)red_signed_full<PI>(acc[u][0]);
+        o.y = (int)red_signed_full<PI>(acc[u][1]);
+        o.z = (int)red_signed_full<PI>(acc[u][2]);
+        o.w = (int)red_signed_full<PI>(acc[u][3]);
+        ((int4*)partial)[((size_t)blockIdx.y * cols + j) * N162 + v] = o;
+      }
+    }
+  }
+}
+
+// Sum the chunk partials, center, and write the reference layout C[col][row][limb][s].
+template <int PI>
+__global__ void k_commit_finish(const int32_t* __restrict__ partial, int nchunks, int cols,
+                                const DevPrime* __restrict__ D, int limb, int limbs,
+                                int16_t* __restrict__ C) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= cols * N162) return;
+  int j = gid / N162, s = gid % N162;
+  int v = D->pow3_to_leaf[s];
+  uint64_t acc[4] = {0, 0, 0, 0};
+  for (int c = 0; c < nchunks; c++) {
+    int4 p = ((const int4*)partial)[((size_t)c * cols + j) * N162 + v];
+    acc[0] += (uint32_t)p.x;
+    acc[1] += (uint32_t)p.y;
+    acc[2] += (uint32_t)p.z;
+    acc[3] += (uint32_t)p.w;
+  }
+  for (int row = 0; row < 4; row++)
+    C[(((size_t)j * 4 + row) * limbs + limb) * N162 + s] = center<PI>((uint32_t)(acc[row] % Pr<PI>::q));
+}
+
+// =============================================================================================
+// Fold: v_p = sum_j c_j(-Y) w_{j,p}(Y) in Z_q[Y]/(Y^162 - Y^81 + 1), one F162 position p at a time
+// =============================================================================================
+// Challenge slot values: chat[j][leaf] = c_j(-theta^{E[leaf]}) (crates/pcs/src/fold.rs:287-335).
+template <int PI>
+__global__ void k_challenge_slots(const lbg_challenge_d* __restrict__ ch, int r,
+                                  const DevPrime* __restrict__ D, uint32_t* __restrict__ chat) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= r * N162) return;
+  int j = gid / N162, leaf = gid % N162;
+  constexpr uint32_t q = Pr<PI>::q;
+  const lbg_challenge_d& c = ch[j];
+  uint32_t acc = 0;
+  uint32_t w = c.weight > 32 ? 32 : c.weight;
+  for (uint32_t t = 0; t < w; t++) {
+    uint32_t p = c.positions[t];
+    if (p >= N162) continue;
+    uint32_t x = D->chal[p * N162 + leaf];
+    acc += ((c.signs >> t) & 1) ? (q - x) : x;
+  }
+  chat[(size_t)j * N162 + leaf] = acc % q;
+}
+
+constexpr int FP = 32;  // positions per CTA
+constexpr int FJ = 8;   // columns per step
+
+template <int PI>
+struct FoldRed {
+  static constexpr int raw = (int)((4294967295ull - 2ull * Pr<PI>::q) / ((uint64_t)FJ * Pr<PI>::q * Pr<PI>::q));
+  static constexpr int value = raw < 1 ? 1 : raw;
+};
+
+template <int PI>
+__device__ __forceinline__ void fold_phase_a_store(uint16_t* __restrict__ wt, int jj, int lane,
+                                                   const uint32_t idx[7], const uint32_t* lut) {
+  uint32_t v[27];
+#define LBG_BLOCK(TAU)                  \
+  ntt_block<PI, TAU>(idx, lut, v);      \
+  _Pragma("unroll") for (int x = 0; x < 27; x++) wt[((jj * N162) + TAU * 27 + x) * FP + lane] = (uint16_t)v[x];
+  LBG_BLOCK(0)
+  LBG_BLOCK(1)
+  LBG_BLOCK(2)
+  LBG_BLOCK(3)
+  LBG_BLOCK(4)
+  LBG_BLOCK(5)
+#undef LBG_BLOCK
+}
+
+template <int PI>
+__global__ void __launch_bounds__(256, 1)
+    k_fold(const uint64_t* __restrict__ W, size_t wdim, int cols, const uint32_t* __restrict__ chat,
+           const DevPrime* __restrict__ D, int16_t* __restrict__ v_out /* [len_ring][648] */) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* lut = (uint32_t*)smem;
+  uint16_t* wt = (uint16_t*)(smem + 6 * 64 * 4);  // FJ * 162 * FP u16 (also reused for v-hat)
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const size_t p0 = (size_t)blockIdx.x * FP;
+  for (int x = tid; x < 6 * 64; x += 256) lut[x] = D->lut[x / 64][x % 64];
+  uint32_t acc[VPW];
+#pragma unroll
+  for (int u = 0; u < VPW; u++) acc[u] = 0;
+  constexpr int RED = FoldRed<PI>::value;
+  int since = 0;
+  for (int j0 = 0; j0 < cols; j0 += FJ) {
+    __syncthreads();
+    {
+      int j = j0 + warp;
+      size_t p = p0 + lane;
+      uint64_t e0 = 0, e1 = 0, e2 = 0;
+      if (j < cols && p < wdim) {
+        const uint64_t* e = W + ((size_t)j * wdim + p) * 3;
+        e0 = e[0];
+        e1 = e[1];
+        e2 = e[2];
+      }
+      uint32_t idx[7];
+      f162_windows(e0, e1, e2, idx);
+      fold_phase_a_store<PI>(wt, warp, lane, idx, lut);
+    }
+    __syncthreads();
+    const int nj = min(FJ, cols - j0);
+    for (int jj = 0; jj < nj; jj++) {
+      const uint32_t* ch = chat + (size_t)(j0 + jj) * N162;
+#pragma unroll
+      for (int u = 0; u < VPW; u++) {
+        int v = warp + 8 * u;
+        if (v < N162) acc[u] += __ldg(ch + v) * (uint32_t)wt[((jj * N162) + v) * FP + lane];
+      }
+    }
+    if (++since >= RED) {
+      since = 0;
+#pragma unroll
+      for (int u = 0; u < VPW; u++) acc[u] = red_full<PI>(acc[u]);
+    }
+  }
+  __syncthreads();
+  // v-hat of the 32 positions into smem, [pos][162] u32
+  uint32_t* vh = (uint32_t*)wt;
+#pragma unroll
+  for (int u = 0; u < VPW; u++) {
+    int v = warp + 8 * u;
+    if (v < N162) vh[lane * N162 + v] = red_full<PI>(acc[u]);
+  }
+  __syncthreads();
+  if (tid < FP) {
+    size_t p = p0 + tid;
+    if (p < wdim) {
+      uint32_t* x = vh + tid * N162;
+      intt162_serial<PI>(x, *D);
+      size_t i = p / 4;
+      int k = (int)(p % 4);
+      for (int m = 0; m < N162; m++) v_out[i * N648 + 4 * m + k] = center<PI>(x[m]);
+    }
+  }
+}
+
+// Verifier::fold_commitment: out[row][limb][s] = sum_j chat_j(s) C_j[row][limb][s]
+// (crates/pcs/src/scheme/verifier.rs:114-146).
+template <int PI>
+__global__ void k_fold_commitment(const int16_t* __restrict__ C, int cols, int limb, int limbs,
+                                  const uint32_t* __restrict__ chat, const DevPrime* __restrict__ D,
+                                  int16_t* __restrict__ out) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 4 * N162) return;
+  int row = gid / N162, s = gid % N162;
+  int leaf = D->pow3_to_leaf[s];
+  constexpr int32_t q = Pr<PI>::q;
+  uint64_t acc = 0;
+  for (int j = 0; j < cols; j++) {
+    int32_t c = C[(((size_t)j * 4 + row) * limbs + limb) * N162 + s];
+    uint32_t cm = (uint32_t)(c < 0 ? c + q : c);
+    acc += (uint64_t)chat[(size_t)j * N162 + leaf] * cm;
+  }
+  out[(row * limbs + limb) * N162 + s] = center<PI>((uint32_t)(acc % q));
+}
+
+// =============================================================================================
+// Bit-drop (crates/pcs/src/bd/digits.rs:121-181): per limb, the coefficients of each column's
+// commitment (component d's coefficients are coefficients 4m + d), then Garner digits.
+// =============================================================================================
+template <int PI>
+__global__ void k_column_residues(const int16_t* __restrict__ C, int cols, int limb, int limbs,
+                                  const DevPrime* __restrict__ D, uint16_t* __restrict__ res /* [cols*648] */) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= cols * 4) return;
+  int j = gid / 4, d = gid % 4;
+  constexpr int32_t q = Pr<PI>::q;
+  uint32_t x[N162];
+  for (int s = 0; s < N162; s++) {
+    int32_t c = C[(((size_t)j * 4 + d) * limbs + limb) * N162 + s];
+    x[D->pow3_to_leaf[s]] = (uint32_t)(c < 0 ? c + q : c);
+  }
+  intt162_serial<PI>(x, *D);
+  for (int m = 0; m < N162; m++) res[(size_t)j * N648 + 4 * m + d] = (uint16_t)x[m];
+}
+
+__global__ void k_garner(const uint16_t* __restrict__ res, size_t count, int limbs, GarnerConsts g,
+                         uint16_t* __restrict__ top, uint16_t* __restrict__ digits) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint32_t base = res[i];
+  top[i] = (uint16_t)((base + (1u << (g.dropped_bits - 1))) >> g.dropped_bits);
+  uint32_t mixed[7];
+  mixed[0] = base;
+  for (int k = 1; k < limbs; k++) {
+    uint32_t q = g.q[k];
+    uint32_t x = res[(size_t)k * count + i];
+    for (int m = 0; m < k; m++)
+      x = (uint32_t)((uint64_t)((x + q - mixed[m] % q) % q) * g.inv[k][m] % q);
+    mixed[k] = x;
+    digits[(size_t)(k - 1) * count + i] = (uint16_t)x;
+  }
+}
+
+// =============================================================================================
+// Row evaluation over F162 (crates/pcs/src/eval.rs:51-63, 171-193)
+// =============================================================================================
+// eq(p, i) = prod_k (p_k if bit k of i else 1 + p_k).
+__global__ void k_eq_table(const uint64_t* __restrict__ p, int n, size_t count, uint64_t* __restrict__ eq) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  F162d x{{1, 0, 0}};
+  for (int k = 0; k < n; k++) {
+    F162d pk{{p[3 * k], p[3 * k + 1], p[3 * k + 2]}};
+    if (!((i >> k) & 1)) pk.w[0] ^= 1;
+    x = f_mul(x, pk);
+  }
+  eq[3 * i] = x.w[0];
+  eq[3 * i + 1] = x.w[1];
+  eq[3 * i + 2] = x.w[2];
+}
+
+// One CTA per column: thread b < 162 accumulates S_b = sum over rows i with bit b of W[i] set of
+// eq[i]; then u = sum_b x^b S_b reduced modulo x^162 + x^81 + 1.
+__global__ void __launch_bounds__(192) k_row_eval(const uint64_t* __restrict__ W, size_t wdim,
+                                                  const uint64_t* __restrict__ eq, uint64_t* __restrict__ u) {
+  __shared__ uint64_t S[N162][3];
+  const int b = threadIdx.x;
+  const int j = blockIdx.x;
+  const uint64_t* col = W + (size_t)j * wdim * 3;
+  uint64_t a0 = 0, a1 = 0, a2 = 0;
+  if (b < N162) {
+    const int limb = b >> 6, sh = b & 63;
+    for (size_t i = 0; i < wdim; i++) {
+      uint64_t m = 0 - ((__ldg(col + 3 * i + limb) >> sh) & 1);
+      a0 ^= __ldg(eq + 3 * i) & m;
+      a1 ^= __ldg(eq + 3 * i + 1) & m;
+      a2 ^= __ldg(eq + 3 * i + 2) & m;
+    }
+    S[b][0] = a0;
+    S[b][1] = a1;
+    S[b][2] = a2;
+  }
+  __syncthreads();
+  if (b == 0) {
+    uint64_t P[6] = {0, 0, 0, 0, 0, 0};
+    for (int bb = 0; bb < N162; bb++) {
+      int ws = bb >> 6, bs = bb & 63;
+      for (int t = 0; t < 3; t++) {
+        uint64_t x = S[bb][t];
+        P[t + ws] ^= x << bs;
+        if (bs) P[t + ws + 1] ^= x >> (64 - bs);
+      }
+    }
+    // reduce bits 322..162 by x^162 = x^81 + 1
+    for (int bit = 322; bit >= 162; bit--) {
+      if ((P[bit >> 6] >> (bit & 63)) & 1) {
+        P[bit >> 6] ^= 1ull << (bit & 63);
+        int a = bit - 162, c = bit - 81;
+        P[a >> 6] ^= 1ull << (a & 63);
+        P[c >> 6] ^= 1ull << (c & 63);
+      }
+    }
+    u[3 * j] = P[0];
+    u[3 * j + 1] = P[1];
+    u[3 * j + 2] = P[2];
+  }
+}
+
+// claim(u, p1) = sum_j eq(p1, j) u_j: one thread per column, XOR-reduced per warp, then one
+// atomic XOR per warp into out (zeroed by the caller).
+__global__ void k_claim(const uint64_t* __restrict__ u, int cols, const uint64_t* __restrict__ p1, int n,
+                        unsigned long long* __restrict__ out) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t a0 = 0, a1 = 0, a2 = 0;
+  if (j < cols) {
+    F162d x{{1, 0, 0}};
+    for (int k = 0; k < n; k++) {
+      F162d pk{{p1[3 * k], p1[3 * k + 1], p1[3 * k + 2]}};
+      if (!((j >> k) & 1)) pk.w[0] ^= 1;
+      x = f_mul(x, pk);
+    }
+    F162d y = f_mul(x, F162d{{u[3 * j], u[3 * j + 1], u[3 * j + 2]}});
+    a0 = y.w[0];
+    a1 = y.w[1];
+    a2 = y.w[2];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 ^= __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 ^= __shfl_xor_sync(0xffffffffu, a1, o);
+    a2 ^= __shfl_xor_sync(0xffffffffu, a2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicXor(out, (unsigned long long)a0);
+    atomicXor(out + 1, (unsigned long long)a1);
+    atomicXor(out + 2, (unsigned long long)a2);
+  }
+}
+
+// =============================================================================================
+// Witness generation: keyed BLAKE3 XOF of "labinius/witness" (crates/pcs/src/scheme/witness.rs:66-87)
+// =============================================================================================
+__device__ __forceinline__ uint32_t rotr32(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
+__device__ __forceinline__ void g_mix(uint32_t* s, int a, int b, int c, int d, uint32_t x, uint32_t y) {
+  s[a] += s[b] + x;
+  s[d] = rotr32(s[d] ^ s[a], 16);
+  s[c] += s[d];
+  s[b] = rotr32(s[b] ^ s[c], 12);
+  s[a] += s[b] + y;
+  s[d] = rotr32(s[d] ^ s[a], 8);
+  s[c] += s[d];
+  s[b] = rotr32(s[b] ^ s[c], 7);
+}
+__constant__ uint8_t c_b3_sched[7][16] = {
+    {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15},
+    {2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8},
+    {3, 4, 10, 12, 13, 2, 7, 14, 6, 5, 9, 0, 11, 15, 8, 1},
+    {10, 7, 12, 9, 14, 3, 13, 15, 4, 0, 11, 2, 5, 8, 1, 6},
+    {12, 13, 9, 11, 15, 10, 14, 8, 7, 2, 5, 3, 0, 1, 6, 4},
+    {9, 14, 11, 5, 8, 12, 15, 1, 13, 3, 0, 10, 2, 6, 4, 7},
+    {11, 15, 5, 0, 1, 9, 8, 6, 14, 10, 2, 12, 3, 4, 7, 13},
+};
+
+// Output block t of a single-block root node (key words, message words, length, flags).
+__global__ void k_xof_blocks(XofRoot root, size_t nbytes, uint8_t* __restrict__ out) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t * 64 >= nbytes) return;
+  const uint32_t IV[4] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au};
+  uint32_t s[16];
+  for (int i = 0; i < 8; i++) s[i] = root.cv[i];
+  for (int i = 0; i < 4; i++) s[8 + i] = IV[i];
+  s[12] = (uint32_t)t;
+  s[13] = (uint32_t)((uint64_t)t >> 32);
+  s[14] = root.block_len;
+  s[15] = root.flags;
+  for (int r = 0; r < 7; r++) {
+    const uint8_t* w = c_b3_sched[r];
+    g_mix(s, 0, 4, 8, 12, root.m[w[0]], root.m[w[1]]);
+    g_mix(s, 1, 5, 9, 13, root.m[w[2]], root.m[w[3]]);
+    g_mix(s, 2, 6, 10, 14, root.m[w[4]], root.m[w[5]]);
+    g_mix(s, 3, 7, 11, 15, root.m[w[6]], root.m[w[7]]);
+    g_mix(s, 0, 5, 10, 15, root.m[w[8]], root.m[w[9]]);
+    g_mix(s, 1, 6, 11, 12, root.m[w[10]], root.m[w[11]]);
+    g_mix(s, 2, 7, 8, 13, root.m[w[12]], root.m[w[13]]);
+    g_mix(s, 3, 4, 9, 14, root.m[w[14]], root.m[w[15]]);
+  }
+  uint32_t o[16];
+  for (int i = 0; i < 8; i++) {
+    o[i] = s[i] ^ s[i + 8];
+    o[i + 8] = s[i + 8] ^ root.cv[i];
+  }
+  size_t base = t * 64;
+  for (int i = 0; i < 64; i++)
+    if (base + i < nbytes) out[base + i] = (uint8_t)(o[i >> 2] >> (8 * (i & 3)));
+}
+
+__global__ void k_mask_f162(uint64_t* __restrict__ W, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) W[3 * i + 2] &= (1ull << 34) - 1;
+}
+
+// Witness::lifted: F162 = [lo, hi, 0] (crates/pcs/src/fields/scalar.rs:72-74).
+__global__ void k_lift_b128(const uint64_t* __restrict__ b, size_t n, uint64_t* __restrict__ W) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    W[3 * i] = b[2 * i];
+    W[3 * i + 1] = b[2 * i + 1];
+    W[3 * i + 2] = 0;
+  }
+}
+
+// =============================================================================================
+// launch wrappers
+// =============================================================================================
+#define LBG_DISPATCH(pi, CALL)                 \
+  switch (pi) {                                \
+    case 0: { constexpr int P = 0; CALL; } break; \
+    case 1: { constexpr int P = 1; CALL; } break; \
+    case 2: { constexpr int P = 2; CALL; } break; \
+    case 3: { constexpr int P = 3; CALL; } break; \
+    case 4: { constexpr int P = 4; CALL; } break; \
+    case 5: { constexpr int P = 5; CALL; } break; \
+    case 6: { constexpr int P = 6; CALL; } break; \
+    default: return cudaErrorInvalidValue;     \
+  }
+
+static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+cudaError_t upload_hot(int pi, const HotPrime& h) {
+  return cudaMemcpyToSymbol(c_hot, &h, sizeof(HotPrime), sizeof(HotPrime) * pi, cudaMemcpyHostToDevice);
+}
+
+cudaError_t launch_key_expand(const uint64_t* jumps, uint64_t state0, uint32_t q, int nb, int16_t* A,
+                              cudaStream_t st) {
+  size_t n = (size_t)nb * N648;
+  k_key_expand<<<blocks_for(n, 128), 128, 0, st>>>(jumps, state0, q, nb, A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_key_components(int pi, const int16_t* A, const DevPrime* D, int len_ring, int4* Ahat,
+                                  cudaStream_t st) {
+  size_t n = (size_t)len_ring * N162;
+  LBG_DISPATCH(pi, (k_key_components<P><<<blocks_for(n, 128), 128, 0, st>>>(A, D, len_ring, Ahat)));
+  return cudaGetLastError();
+}
+
+size_t commit_smem_bytes() { return 6 * 64 * 4 + CT * RT * 4 * 24 + RT * N162 * CT * 4 * 2; }
+int commit_cols_per_cta() { return CT; }
+int commit_ring_per_step() { return RT; }
+
+cudaError_t launch_commit(int pi, const uint64_t* W, size_t wdim, const int4* Ahat, const DevPrime* D, int cols,
+                          int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st) {
+  dim3 grid((cols + CT - 1) / CT, nchunks);
+  size_t smem = commit_smem_bytes();
+  LBG_DISPATCH(pi, ({
+                 cudaFuncSetAttribute(k_commit<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                 k_commit<P><<<grid, 256, smem, st>>>(W, wdim, Ahat, D, cols, len_ring, chunk, partial);
+               }));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_commit_finish(int pi, const int32_t* partial, int nchunks, int cols, const DevPrime* D,
+                                 int limb, int limbs, int16_t* C, cudaStream_t st) {
+  size_t n = (size_t)cols * N162;
+  LBG_DISPATCH(pi, (k_commit_finish<P><<<blocks_for(n, 128), 128, 0, st>>>(partial, nchunks, cols, D, limb, limbs, C)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_challenge_slots(int pi, const lbg_challenge_d* ch, int r, const DevPrime* D, uint32_t* chat,
+                                   cudaStream_t st) {
+  size_t n = (size_t)r * N162;
+  LBG_DISPATCH(pi, (k_challenge_slots<P><<<blocks_for(n, 128), 128, 0, st>>>(ch, r, D, chat)));
+  return cudaGetLastError();
+}
+
+size_t fold_smem_bytes() {
+  size_t a = (size_t)FJ * N162 * FP * 2, b = (size_t)FP * N162 * 4;
+  return 6 * 64 * 4 + (a > b ? a : b);
+}
+
+cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, const uint32_t* chat, const DevPrime* D,
+                        int16_t* v, cudaStream_t st) {
+  unsigned grid = blocks_for(wdim, FP);
+  size_t smem = fold_smem_bytes();
+  LBG_DISPATCH(pi, ({
+                 cudaFuncSetAttribute(k_fold<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                 k_fold<P><<<grid, 256, smem, st>>>(W, wdim, cols, chat, D, v);
+               }));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fold_commitment(int pi, const int16_t* C, int cols, int limb, int limbs, const uint32_t* chat,
+                                   const DevPrime* D, int16_t* out, cudaStream_t st) {
+  LBG_DISPATCH(pi, (k_fold_commitment<P><<<blocks_for(4 * N162, 128), 128, 0, st>>>(C, cols, limb, limbs, chat, D, out)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_column_residues(int pi, const int16_t* C, int cols, int limb, int limbs, const DevPrime* D,
+                                   uint16_t* res, cudaStream_t st) {
+  size_t n = (size_t)cols * 4;
+  LBG_DISPATCH(pi, (k_column_residues<P><<<blocks_for(n, 64), 64, 0, st>>>(C, cols, limb, limbs, D, res)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_garner(const uint16_t* res, size_t count, int limbs, const GarnerConsts& g, uint16_t* top,
+                          uint16_t* digits, cudaStream_t st) {
+  k_garner<<<blocks_for(count, 256), 256, 0, st>>>(res, count, limbs, g, top, digits);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq, cudaStream_t st) {
+  k_eq_table<<<blocks_for(count, 128), 128, 0, st>>>(p, n, count, eq);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_row_eval(const uint64_t* W, size_t wdim, int cols, const uint64_t* eq, uint64_t* u,
+                            cudaStream_t st) {
+  k_row_eval<<<cols, 192, 0, st>>>(W, wdim, eq, u);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_claim(const uint64_t* u, int cols, const uint64_t* p1, int n, uint64_t* out, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(out, 0, 24, st);
+  if (e != cudaSuccess) return e;
+  k_claim<<<blocks_for(cols, 64), 64, 0, st>>>(u, cols, p1, n, (unsigned long long*)out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_xof(const XofRoot& root, size_t nbytes, uint8_t* out, cudaStream_t st) {
+  size_t blocks = (nbytes + 63) / 64;
+  k_xof_blocks<<<blocks_for(blocks, 128), 128, 0, st>>>(root, nbytes, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mask_f162(uint64_t* W, size_t n, cudaStream_t st) {
+  k_mask_f162<<<blocks_for(n, 256), 256, 0, st>>>(W, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lift_b128(const uint64_t* b, size_t n, uint64_t* W, cudaStream_t st) {
+  k_lift_b128<<<blocks_for(n, 256), 256, 0, st>>>(b, n, W);
+  return cudaGetLastError();
+}
+
+}  // namespace lbg

@@ -1,0 +1,201 @@
+// Device kernels of the labinius prover path for B200 (sm_100a).
+//
+// Arithmetic: exact modular integer arithmetic mod q < 2^15 on 32-bit lanes (Shoup products with
+// precomputed companions, lazily reduced between levels) and GF(2) XOR arithmetic for F162.
+// Nothing here is floating point; every output is canonical, so results are bit-identical to the
+// reference's whatever the internal representatives.
+#pragma once
+#include <cstdint>
+
+#include "prime_structs.h"
+#include "ring_tables.h"
+
+namespace lbg {
+
+// Compile-time primes, indexed like PRIMES.
+template <int PI>
+struct Pr;
+#define LBG_PRIME(I, QV)                                     \
+  template <>                                                \
+  struct Pr<I> {                                             \
+    static constexpr uint32_t q = QV;                        \
+    static constexpr uint32_t qs = (uint32_t)((1ull << 32) / QV); \
+  };
+LBG_PRIME(0, 2917)
+LBG_PRIME(1, 3889)
+LBG_PRIME(2, 4861)
+LBG_PRIME(3, 9721)
+LBG_PRIME(4, 12637)
+LBG_PRIME(5, 17497)
+LBG_PRIME(6, 19441)
+#undef LBG_PRIME
+
+// Hot per-prime constants in constant memory. This header is included by kernels.cu only (the
+// one translation unit that launches kernels), so the definition lives here.
+__constant__ HotPrime c_hot[7];
+
+// ---------------------------------------------------------------------------------------------
+// modular helpers
+// ---------------------------------------------------------------------------------------------
+// a * w mod q in [0, 2q) for any a < 2^32 (ws = floor(w 2^32 / q)).
+__device__ __forceinline__ uint32_t mul_shoup(uint32_t a, uint32_t w, uint32_t ws, uint32_t q) {
+  uint32_t t = __umulhi(a, ws);
+  return a * w - t * q;
+}
+// x mod q, fully reduced, for x < 2^32.
+template <int PI>
+__device__ __forceinline__ uint32_t red_full(uint32_t x) {
+  constexpr uint32_t q = Pr<PI>::q;
+  uint32_t r = x - __umulhi(x, Pr<PI>::qs) * q;
+  return r >= q ? r - q : r;
+}
+// a * b mod q for a, b < q (rare paths).
+template <int PI>
+__device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b) {
+  return (uint32_t)(((uint64_t)a * b) % Pr<PI>::q);
+}
+// a signed accumulator brought back to |r| < 2q (exact modulo q).
+template <int PI>
+__device__ __forceinline__ int32_t red_signed(int32_t x) {
+  return x - __mulhi(x, (int32_t)Pr<PI>::qs) * (int32_t)Pr<PI>::q;
+}
+template <int PI>
+__device__ __forceinline__ uint32_t red_signed_full(int32_t x) {
+  constexpr int32_t q = Pr<PI>::q;
+  int32_t r = x % q;
+  return (uint32_t)(r < 0 ? r + q : r);
+}
+template <int PI>
+__device__ __forceinline__ int16_t center(uint32_t x) {
+  constexpr uint32_t q = Pr<PI>::q;
+  return (int16_t)(x > (q - 1) / 2 ? (int32_t)x - (int32_t)q : (int32_t)x);
+}
+
+// Lazy radix-3 butterfly of the 162-point tree: sub-ring Y^n - z^3 -> children Y^{n/3} - z w^s.
+// Inputs any u32 below 2^32 - 4q; outputs grow by at most 4q.
+template <int PI>
+__device__ __forceinline__ void bfly3(uint32_t& a0, uint32_t& a1, uint32_t& a2, const Twiddle& t,
+                                      uint32_t om, uint32_t oms) {
+  constexpr uint32_t q = Pr<PI>::q;
+  uint32_t t1 = mul_shoup(a1, t.z, t.zs, q);
+  uint32_t t2 = mul_shoup(a2, t.z2, t.z2s, q);
+  uint32_t m = mul_shoup(t1 + 2 * q - t2, om, oms, q);
+  uint32_t y0 = a0 + t1 + t2;
+  uint32_t y1 = a0 + 2 * q - t2 + m;
+  uint32_t y2 = a0 + 4 * q - t1 - m;
+  a0 = y0;
+  a1 = y1;
+  a2 = y2;
+}
+
+// The 27 six-bit LUT indices of one F162 (4 per word, one per byte): index m collects bits
+// m + 27 t, t = 0..5, of the element, the coefficients levels 0 and 1 of the tree combine.
+__device__ __forceinline__ void f162_windows(uint64_t w0, uint64_t w1, uint64_t w2, uint32_t idx[7]) {
+  const uint32_t M27 = 0x7FFFFFFu;
+  uint32_t c[6];
+  c[0] = (uint32_t)w0 & M27;
+  c[1] = (uint32_t)(w0 >> 27) & M27;
+  c[2] = (uint32_t)((w0 >> 54) | (w1 << 10)) & M27;
+  c[3] = (uint32_t)(w1 >> 17) & M27;
+  c[4] = (uint32_t)((w1 >> 44) | (w2 << 20)) & M27;
+  c[5] = (uint32_t)(w2 >> 7) & M27;
+#pragma unroll
+  for (int g = 0; g < 7; g++) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int t = 0; t < 6; t++) {
+      uint32_t nib = (c[t] >> (4 * g)) & 15u;
+      acc += ((nib * 0x00204081u) & 0x01010101u) << t;
+    }
+    idx[g] = acc;
+  }
+}
+
+// Forward transform of one level-2 block (27 leaves) of one F162, fully reduced to [0, q):
+// v[x] = w(theta^{E[27 tau + x]}).
+template <int PI, int TAU>
+__device__ __forceinline__ void ntt_block(const uint32_t idx[7], const uint32_t* __restrict__ lut,
+                                          uint32_t v[27]) {
+  const HotPrime& H = c_hot[PI];
+  const uint32_t om = H.omega, oms = H.omega_s;
+#pragma unroll
+  for (int m = 0; m < 27; m++) v[m] = lut[TAU * 64 + ((idx[m >> 2] >> (8 * (m & 3))) & 63u)];
+#pragma unroll
+  for (int i = 0; i < 9; i++) bfly3<PI>(v[i], v[9 + i], v[18 + i], H.tw[TAU][0], om, oms);
+#pragma unroll
+  for (int s = 0; s < 3; s++)
+#pragma unroll
+    for (int i = 0; i < 3; i++) bfly3<PI>(v[9 * s + i], v[9 * s + 3 + i], v[9 * s + 6 + i], H.tw[TAU][1 + s], om, oms);
+#pragma unroll
+  for (int s = 0; s < 9; s++) bfly3<PI>(v[3 * s], v[3 * s + 1], v[3 * s + 2], H.tw[TAU][4 + s], om, oms);
+#pragma unroll
+  for (int m = 0; m < 27; m++) v[m] = red_full<PI>(v[m]);
+}
+
+// Exact inverse of the 162-point transform, in place on x[0..161] (values in [0, q)), one
+// thread. Used for the folded witness and the bit-dropped residues, a few thousand per round.
+template <int PI>
+__device__ void intt162_serial(uint32_t* x, const DevPrime& D) {
+  constexpr uint32_t q = Pr<PI>::q;
+  const uint32_t w = D.omega, w2 = mulmod<PI>(D.omega, D.omega);
+  // inverse radix-3 levels 4, 3, 2, 1: sub-ring k of level L spans n = 81 / 3^{L-1}
+  for (int L = 4; L >= 1; L--) {
+    int n = 81;
+    for (int l = 1; l < L; l++) n /= 3;
+    int m = n / 3;
+    int subrings = 162 / n;
+    for (int k = 0; k < subrings; k++) {
+      uint32_t zi = D.zinv3[L][k], zi2 = D.zinv3sq[L][k];
+      int base = k * n;
+      for (int i = 0; i < m; i++) {
+        uint32_t y0 = x[base + i], y1 = x[base + m + i], y2 = x[base + 2 * m + i];
+        uint32_t s0 = (y0 + y1 + y2) % q;
+        uint32_t s1 = (y0 + mulmod<PI>(w2, y1) + mulmod<PI>(w, y2)) % q;
+        uint32_t s2 = (y0 + mulmod<PI>(w, y1) + mulmod<PI>(w2, y2)) % q;
+        x[base + i] = mulmod<PI>(s0, D.inv3);
+        x[base + m + i] = mulmod<PI>(s1, zi);
+        x[base + 2 * m + i] = mulmod<PI>(s2, zi2);
+      }
+    }
+  }
+  // level 0: y0 = a + zeta6 b, y1 = a + zeta6^-1 b  =>  b = (y0 - y1) / (2 zeta6 - 1), a = y0 - zeta6 b
+  for (int i = 0; i < 81; i++) {
+    uint32_t y0 = x[i], y1 = x[i + 81];
+    uint32_t b = mulmod<PI>((y0 + q - y1) % q, D.det0);
+    uint32_t a = (y0 + q - mulmod<PI>(D.zeta6, b)) % q;
+    x[i] = a;
+    x[i + 81] = b;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// F162 arithmetic: GF(2)[x]/(x^162 + x^81 + 1) (crates/pcs/src/fields/scalar.rs:65-116)
+// ---------------------------------------------------------------------------------------------
+struct F162d {
+  uint64_t w[3];
+};
+__device__ __forceinline__ F162d f_add(F162d a, F162d b) {
+  return F162d{{a.w[0] ^ b.w[0], a.w[1] ^ b.w[1], a.w[2] ^ b.w[2]}};
+}
+// Shift-and-add product with the reduction folded into the shift (x^162 = x^81 + 1).
+__device__ inline F162d f_mul(F162d a, F162d b) {
+  F162d r{{0, 0, 0}};
+  const uint64_t M34 = (1ull << 34) - 1;
+  for (int i = 161; i >= 0; i--) {
+    // r <- r * x
+    uint64_t top = (r.w[2] >> 33) & 1;
+    r.w[2] = ((r.w[2] << 1) | (r.w[1] >> 63)) & M34;
+    r.w[1] = (r.w[1] << 1) | (r.w[0] >> 63);
+    r.w[0] <<= 1;
+    uint64_t tm = 0 - top;
+    r.w[0] ^= tm & 1;
+    r.w[1] ^= tm & (1ull << 17);
+    uint64_t bm = 0 - ((b.w[i >> 6] >> (i & 63)) & 1);
+    r.w[0] ^= a.w[0] & bm;
+    r.w[1] ^= a.w[1] & bm;
+    r.w[2] ^= a.w[2] & bm;
+  }
+  return r;
+}
+
+}  // namespace lbg

@@ -1,0 +1,64 @@
+// Host-callable launch wrappers of the device kernels (kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace lbg {
+
+struct HotPrime;
+struct DevPrime;
+
+// lbg_challenge as the device sees it (40 bytes).
+struct lbg_challenge_d {
+  uint8_t positions[32];
+  uint32_t signs;
+  uint32_t weight;
+};
+
+struct GarnerConsts {
+  uint32_t q[7];
+  uint32_t inv[7][7];  // inv[k][m] = q_m^-1 mod q_k
+  uint32_t dropped_bits;
+};
+
+// A single-block BLAKE3 root node (key words, message words, block length, flags without ROOT|).
+struct XofRoot {
+  uint32_t cv[8];
+  uint32_t m[16];
+  uint32_t block_len;
+  uint32_t flags;
+};
+
+cudaError_t upload_hot(int pi, const HotPrime& h);
+cudaError_t launch_key_expand(const uint64_t* jumps, uint64_t state0, uint32_t q, int nb, int16_t* A,
+                              cudaStream_t st);
+cudaError_t launch_key_components(int pi, const int16_t* A, const DevPrime* D, int len_ring, int4* Ahat,
+                                  cudaStream_t st);
+size_t commit_smem_bytes();
+int commit_cols_per_cta();
+int commit_ring_per_step();
+cudaError_t launch_commit(int pi, const uint64_t* W, size_t wdim, const int4* Ahat, const DevPrime* D, int cols,
+                          int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st);
+cudaError_t launch_commit_finish(int pi, const int32_t* partial, int nchunks, int cols, const DevPrime* D,
+                                 int limb, int limbs, int16_t* C, cudaStream_t st);
+cudaError_t launch_challenge_slots(int pi, const lbg_challenge_d* ch, int r, const DevPrime* D, uint32_t* chat,
+                                   cudaStream_t st);
+size_t fold_smem_bytes();
+cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, const uint32_t* chat, const DevPrime* D,
+                        int16_t* v, cudaStream_t st);
+cudaError_t launch_fold_commitment(int pi, const int16_t* C, int cols, int limb, int limbs, const uint32_t* chat,
+                                   const DevPrime* D, int16_t* out, cudaStream_t st);
+cudaError_t launch_column_residues(int pi, const int16_t* C, int cols, int limb, int limbs, const DevPrime* D,
+                                   uint16_t* res, cudaStream_t st);
+cudaError_t launch_garner(const uint16_t* res, size_t count, int limbs, const GarnerConsts& g, uint16_t* top,
+                          uint16_t* digits, cudaStream_t st);
+cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq, cudaStream_t st);
+cudaError_t launch_row_eval(const uint64_t* W, size_t wdim, int cols, const uint64_t* eq, uint64_t* u,
+                            cudaStream_t st);
+cudaError_t launch_claim(const uint64_t* u, int cols, const uint64_t* p1, int n, uint64_t* out, cudaStream_t st);
+cudaError_t launch_xof(const XofRoot& root, size_t nbytes, uint8_t* out, cudaStream_t st);
+cudaError_t launch_mask_f162(uint64_t* W, size_t n, cudaStream_t st);
+cudaError_t launch_lift_b128(const uint64_t* b, size_t n, uint64_t* W, cudaStream_t st);
+
+}  // namespace lbg

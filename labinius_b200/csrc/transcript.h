@@ -1,0 +1,57 @@
+// Host side of the round: the Fiat-Shamir transcript, the short-challenge sampler and the
+// absorb/derive steps of the verifier. These stay on the host (they are sequential BLAKE3 work
+// and must reproduce the reference's transcript bytes); the GPU path consumes their outputs.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "blake3_host.h"
+
+namespace lbg {
+
+// crates/pcs/src/challenge.rs:227-235 (positions sorted, signs bit i = -1 at positions[i]).
+struct Challenge {
+  uint8_t positions[32];
+  uint32_t signs;
+  uint32_t weight;
+};
+static_assert(sizeof(Challenge) == 40, "lbg_challenge layout");
+
+// crates/pcs/src/challenge.rs:66-161
+class Transcript {
+ public:
+  explicit Transcript(const uint8_t* domain, size_t len);
+  void absorb_bytes(const uint8_t* b, size_t len);
+  void absorb_u64(uint64_t x);
+  void absorb_raw(const uint8_t* b, size_t len) { state_.update(b, len); }
+  void fill(const char* label, uint8_t* out, size_t n);
+  Blake3 derive(const char* label);
+
+ private:
+  Blake3 state_;
+  uint64_t counter_ = 0;
+};
+
+// crates/pcs/src/challenge.rs:517-533
+Challenge sample_short_challenge(Transcript& t, uint32_t weight, double bound, uint64_t* attempts);
+
+// The round shape the host steps need (crates/pcs/src/scheme/params.rs:62-68).
+struct RoundShape {
+  uint32_t witness_log_len, column_log_len, limbs, dropped_bits;
+  uint32_t primes[8];
+  uint8_t matrix_seed[32];
+  size_t columns() const { return (size_t)1 << column_log_len; }
+  uint32_t row_log_len() const { return witness_log_len - column_log_len; }
+};
+
+// crates/pcs/src/scheme/verifier.rs:41-100
+void derive_evaluation_point(const RoundShape& s, Transcript& t, const int16_t* matrix,
+                             const uint16_t* top, const uint16_t* digits, uint64_t* p0, uint64_t* p1);
+// crates/pcs/src/scheme/commitment.rs:217-229, 320-331
+void derive_folding_challenges(const RoundShape& s, Transcript& t, const uint64_t* u, Challenge* out);
+// crates/pcs/src/wire/mod.rs:386-397
+std::vector<uint8_t> pack_dropped(const RoundShape& s, const uint16_t* top, const uint16_t* digits);
+uint32_t top_bits(uint32_t q, uint32_t dropped_bits);
+uint32_t residue_bits(uint32_t q);
+
+}  // namespace lbg

@@ -1,0 +1,407 @@
+"""TEST INFRASTRUCTURE: Python bindings of the CPU oracle (``oracle/oracle.cpp``).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg import this
+module, and only as the checker or the timed CPU baseline. The product (``labinius_b200``) never
+imports it.
+
+Parity unpinned: the reference (osdnk/labinius) ships no golden vectors for this path and cannot be
+built here; the oracle is a restatement of its scalar definitions, cross-checked against the
+reference's relational tests and, for BLAKE3, against the Python ``blake3`` package.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_lib = None
+
+CHALLENGE_DTYPE = np.dtype([("positions", np.uint8, 32), ("signs", np.uint32), ("weight", np.uint32)])
+N = 648
+N162 = 162
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = _build.LIB
+        if not os.path.exists(path):
+            _build.build()
+        _lib = ctypes.CDLL(path)
+        _setup(_lib)
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _setup(L):
+    vp, sz, u32, u64, i32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+    sig = {
+        "orc_blake3": (None, [i32, vp, sz, vp, sz, u64, vp, sz]),
+        "orc_prime_info": (None, [u32, vp]),
+        "orc_slot_tables": (None, [vp, vp, vp, vp, vp]),
+        "orc_ntt": (None, [u32, vp, vp]),
+        "orc_intt": (None, [u32, vp, vp]),
+        "orc_eval_at": (u32, [u32, vp, u32]),
+        "orc_eval_quad_at": (None, [u32, vp, u32, vp]),
+        "orc_components": (None, [u32, vp, vp]),
+        "orc_recombine": (None, [u32, vp, vp]),
+        "orc_f162_mul": (None, [vp, vp, vp]),
+        "orc_f162_mul_serial": (None, [vp, vp, vp]),
+        "orc_eq_table": (None, [vp, i32, vp]),
+        "orc_key_seed": (u64, [vp]),
+        "orc_key_expand": (None, [vp, i32, sz, u64, vp]),
+        "orc_witness_random": (None, [sz, vp, vp]),
+        "orc_commit": (None, [vp, vp, vp, sz, sz, vp, vp, i32]),
+        "orc_row_evaluate": (None, [vp, sz, vp, i32, vp]),
+        "orc_claim": (None, [vp, vp, i32, vp]),
+        "orc_fold": (None, [vp, vp, vp, sz, sz, vp, i32, i32]),
+        "orc_fold_commitment": (None, [vp, vp, vp, vp]),
+        "orc_slot_table": (None, [u32, vp]),
+        "orc_drop_bits": (None, [vp, vp, vp, vp]),
+        "orc_pack_dropped": (sz, [vp, vp, vp, vp, sz]),
+        "orc_transcript_new": (vp, [vp, sz]),
+        "orc_transcript_free": (None, [vp]),
+        "orc_transcript_clone": (vp, [vp]),
+        "orc_transcript_absorb_bytes": (None, [vp, vp, sz]),
+        "orc_transcript_absorb_u64": (None, [vp, u64]),
+        "orc_transcript_fill": (None, [vp, ctypes.c_char_p, vp, sz]),
+        "orc_sample_short_challenge": (None, [vp, u32, ctypes.c_double, vp, vp]),
+        "orc_within": (i32, [vp, ctypes.c_double]),
+        "orc_derive_evaluation_point": (None, [vp, vp, vp, vp, vp, vp, vp]),
+        "orc_derive_folding_challenges": (None, [vp, vp, vp, vp]),
+        "orc_verify_folded_opening": (i32, [vp, vp, vp, vp, vp, vp]),
+        "orc_fold_binary": (None, [vp, vp, sz, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+
+# ------------------------------------------------------------------------------------------------
+# parameters
+# ------------------------------------------------------------------------------------------------
+class Params:
+    """The round shape of crates/pcs/src/scheme/params.rs:62-68: moduli with the base first."""
+
+    def __init__(self, witness_log_len, column_log_len, primes, dropped_bits=0):
+        self.witness_log_len = witness_log_len
+        self.column_log_len = column_log_len
+        self.primes = list(primes)
+        self.dropped_bits = dropped_bits
+
+    @property
+    def limbs(self):
+        return len(self.primes)
+
+    @property
+    def columns(self):
+        return 1 << self.column_log_len
+
+    @property
+    def row_log_len(self):
+        return self.witness_log_len - self.column_log_len
+
+    @property
+    def column_len(self):
+        return 1 << self.row_log_len
+
+    @property
+    def len_ring(self):
+        return self.column_len // 4
+
+    @property
+    def witness_len(self):
+        return 1 << self.witness_log_len
+
+    def arr(self):
+        return np.array([self.witness_log_len, self.column_log_len, self.limbs, self.dropped_bits, *self.primes],
+                        dtype=np.uint32)
+
+
+# ------------------------------------------------------------------------------------------------
+# primitives
+# ------------------------------------------------------------------------------------------------
+def blake3(data: bytes, n: int = 32, seek: int = 0, key: bytes = None, context: bytes = None) -> bytes:
+    mode, k = 0, b""
+    if key is not None:
+        mode, k = 1, key
+    elif context is not None:
+        mode, k = 2, context
+    kb = np.frombuffer(k, dtype=np.uint8).copy() if k else np.zeros(1, np.uint8)
+    db = np.frombuffer(data, dtype=np.uint8).copy() if data else np.zeros(1, np.uint8)
+    out = np.zeros(max(n, 1), dtype=np.uint8)
+    lib().orc_blake3(mode, _p(kb), len(k), _p(db), len(data), seek, _p(out), n)
+    return out[:n].tobytes()
+
+
+def prime_info(q):
+    out = np.zeros(5, dtype=np.uint64)
+    lib().orc_prime_info(q, _p(out))
+    return dict(quad=bool(out[0]), psi=int(out[1]), omega=int(out[2]), zeta6=int(out[3]), theta=int(out[4]))
+
+
+def slot_tables():
+    se = np.zeros(N, np.uint32)
+    qse = np.zeros(324, np.uint32)
+    pow3 = np.zeros(N162, np.uint32)
+    s648 = np.zeros((4, N162), np.uint32)
+    qcs = np.zeros((2, N162), np.uint32)
+    lib().orc_slot_tables(_p(se), _p(qse), _p(pow3), _p(s648), _p(qcs))
+    return dict(slot_exp=se, quad_slot_exp=qse, pow3_slot_exp=pow3, slot_648=s648, quad_class_slot=qcs)
+
+
+def ntt(q, a):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    out = np.zeros(N, np.uint32)
+    lib().orc_ntt(q, _p(a), _p(out))
+    return out
+
+
+def intt(q, a):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    out = np.zeros(N, np.uint32)
+    lib().orc_intt(q, _p(a), _p(out))
+    return out
+
+
+def eval_at(q, a, u):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    return int(lib().orc_eval_at(q, _p(a), u))
+
+
+def eval_quad_at(q, a, u):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    r = np.zeros(2, np.uint32)
+    lib().orc_eval_quad_at(q, _p(a), u, _p(r))
+    return int(r[0]), int(r[1])
+
+
+def components(q, y):
+    y = np.ascontiguousarray(y, dtype=np.uint32)
+    out = np.zeros((4, N162), np.int16)
+    lib().orc_components(q, _p(y), _p(out))
+    return out
+
+
+def recombine(q, comp):
+    comp = np.ascontiguousarray(comp, dtype=np.int16)
+    y = np.zeros(N, np.uint32)
+    lib().orc_recombine(q, _p(comp), _p(y))
+    return y
+
+
+def f162_mul(a, b, serial=False):
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    b = np.ascontiguousarray(b, dtype=np.uint64)
+    out = np.zeros(3, np.uint64)
+    (lib().orc_f162_mul_serial if serial else lib().orc_f162_mul)(_p(a), _p(b), _p(out))
+    return out
+
+
+def eq_table(ps):
+    ps = np.ascontiguousarray(ps, dtype=np.uint64).reshape(-1, 3)
+    out = np.zeros((1 << len(ps), 3), np.uint64)
+    lib().orc_eq_table(_p(ps), len(ps), _p(out))
+    return out
+
+
+def key_seed(seed: bytes) -> int:
+    s = np.frombuffer(seed, dtype=np.uint8).copy()
+    return int(lib().orc_key_seed(_p(s)))
+
+
+def key_expand(params: Params, seed64: int):
+    primes = np.array(params.primes, dtype=np.uint32)
+    A = np.zeros((params.limbs, params.len_ring, N), np.int16)
+    lib().orc_key_expand(_p(primes), params.limbs, params.len_ring, seed64, _p(A))
+    return A
+
+
+def witness_random(n: int, seed: bytes):
+    s = np.frombuffer(seed, dtype=np.uint8).copy()
+    out = np.zeros((n, 3), np.uint64)
+    lib().orc_witness_random(n, _p(s), _p(out))
+    return out
+
+
+def commit(params: Params, A, witness, c0=0, c1=None, threads=1, raw=False):
+    c1 = params.columns if c1 is None else c1
+    w = np.ascontiguousarray(witness, dtype=np.uint64)
+    A = np.ascontiguousarray(A, dtype=np.int16)
+    C = np.zeros((params.columns, 4, params.limbs, N162), np.int16)
+    R = np.zeros((params.columns, params.limbs, N), np.uint32) if raw else None
+    pa = params.arr()
+    lib().orc_commit(_p(pa), _p(A), _p(w), c0, c1, _p(C), _p(R) if raw else None, threads)
+    return (C, R) if raw else C
+
+
+def row_evaluate(witness, p0):
+    w = np.ascontiguousarray(witness, dtype=np.uint64)
+    p0 = np.ascontiguousarray(p0, dtype=np.uint64).reshape(-1, 3)
+    n = len(w)
+    u = np.zeros((n >> len(p0), 3), np.uint64)
+    lib().orc_row_evaluate(_p(w), n, _p(p0), len(p0), _p(u))
+    return u
+
+
+def claim(u, p1):
+    u = np.ascontiguousarray(u, dtype=np.uint64)
+    p1 = np.ascontiguousarray(p1, dtype=np.uint64).reshape(-1, 3)
+    out = np.zeros(3, np.uint64)
+    lib().orc_claim(_p(u), _p(p1), len(p1), _p(out))
+    return out
+
+
+def fold(params: Params, witness, challenges, i0=0, i1=None, threads=1, use_ntt=False):
+    i1 = params.len_ring if i1 is None else i1
+    w = np.ascontiguousarray(witness, dtype=np.uint64)
+    ch = np.ascontiguousarray(challenges, dtype=CHALLENGE_DTYPE)
+    v = np.zeros((params.len_ring, N), np.int16)
+    pa = params.arr()
+    lib().orc_fold(_p(pa), _p(w), _p(ch), i0, i1, _p(v), threads, int(use_ntt))
+    return v
+
+
+def fold_commitment(params: Params, C, challenges):
+    C = np.ascontiguousarray(C, dtype=np.int16)
+    ch = np.ascontiguousarray(challenges, dtype=CHALLENGE_DTYPE)
+    out = np.zeros((4, params.limbs, N162), np.int16)
+    pa = params.arr()
+    lib().orc_fold_commitment(_p(pa), _p(C), _p(ch), _p(out))
+    return out
+
+
+def slot_table(q):
+    out = np.zeros((N162, N162), np.int16)
+    lib().orc_slot_table(q, _p(out))
+    return out
+
+
+def drop_bits(params: Params, C):
+    C = np.ascontiguousarray(C, dtype=np.int16)
+    count = params.columns * N
+    top = np.zeros(count, np.uint16)
+    digits = np.zeros((max(params.limbs - 1, 1), count), np.uint16)
+    pa = params.arr()
+    lib().orc_drop_bits(_p(pa), _p(C), _p(top), _p(digits))
+    return top, digits[: params.limbs - 1]
+
+
+def pack_dropped(params: Params, top, digits):
+    pa = params.arr()
+    top = np.ascontiguousarray(top, dtype=np.uint16)
+    digits = np.ascontiguousarray(digits, dtype=np.uint16) if params.limbs > 1 else np.zeros(1, np.uint16)
+    n = lib().orc_pack_dropped(_p(pa), _p(top), _p(digits), None, 0)
+    out = np.zeros(n, np.uint8)
+    lib().orc_pack_dropped(_p(pa), _p(top), _p(digits), _p(out), n)
+    return out.tobytes()
+
+
+class Transcript:
+    """crates/pcs/src/challenge.rs:66-161"""
+
+    def __init__(self, domain: bytes = None, _handle=None):
+        if _handle is not None:
+            self.h = _handle
+        else:
+            d = np.frombuffer(domain, dtype=np.uint8).copy()
+            self.h = lib().orc_transcript_new(_p(d), len(domain))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.orc_transcript_free(self.h)
+            self.h = None
+
+    def clone(self):
+        return Transcript(_handle=lib().orc_transcript_clone(self.h))
+
+    def absorb_bytes(self, b: bytes):
+        a = np.frombuffer(b, dtype=np.uint8).copy() if b else np.zeros(1, np.uint8)
+        lib().orc_transcript_absorb_bytes(self.h, _p(a), len(b))
+
+    def absorb_u64(self, x: int):
+        lib().orc_transcript_absorb_u64(self.h, x)
+
+    def fill(self, label: bytes, n: int) -> bytes:
+        out = np.zeros(max(n, 1), np.uint8)
+        lib().orc_transcript_fill(self.h, label, _p(out), n)
+        return out[:n].tobytes()
+
+
+def sample_short_challenge(t: Transcript, weight=28, bound=12.0):
+    out = np.zeros(1, CHALLENGE_DTYPE)
+    att = np.zeros(1, np.uint64)
+    lib().orc_sample_short_challenge(t.h, weight, bound, _p(out), _p(att))
+    return out[0], int(att[0])
+
+
+def derive_evaluation_point(params: Params, matrix_seed: bytes, t: Transcript, C=None, top=None, digits=None):
+    pa = params.arr()
+    seed = np.frombuffer(matrix_seed, dtype=np.uint8).copy()
+    n = params.row_log_len + params.column_log_len
+    p = np.zeros((n, 3), np.uint64)
+    Cc = np.ascontiguousarray(C, dtype=np.int16) if C is not None else None
+    tp = np.ascontiguousarray(top, dtype=np.uint16) if top is not None else None
+    dg = (np.ascontiguousarray(digits, dtype=np.uint16) if (digits is not None and params.limbs > 1)
+          else np.zeros(1, np.uint16))
+    lib().orc_derive_evaluation_point(_p(pa), _p(seed), t.h, _p(Cc) if Cc is not None else None,
+                                      _p(tp) if tp is not None else None, _p(dg), _p(p))
+    return p[: params.row_log_len], p[params.row_log_len:]
+
+
+def derive_folding_challenges(params: Params, t: Transcript, u):
+    pa = params.arr()
+    u = np.ascontiguousarray(u, dtype=np.uint64)
+    out = np.zeros(params.columns, CHALLENGE_DTYPE)
+    lib().orc_derive_folding_challenges(_p(pa), t.h, _p(u), _p(out))
+    return out
+
+
+def verify_folded_opening(params: Params, A, folded_commitment, v, p0, folded_row_value):
+    pa = params.arr()
+    A = np.ascontiguousarray(A, dtype=np.int16)
+    fc = np.ascontiguousarray(folded_commitment, dtype=np.int16)
+    v = np.ascontiguousarray(v, dtype=np.int16)
+    p0 = np.ascontiguousarray(p0, dtype=np.uint64)
+    fr = np.ascontiguousarray(folded_row_value, dtype=np.uint64)
+    return bool(lib().orc_verify_folded_opening(_p(pa), _p(A), _p(fc), _p(v), _p(p0), _p(fr)))
+
+
+def fold_binary(u, challenges):
+    u = np.ascontiguousarray(u, dtype=np.uint64)
+    ch = np.ascontiguousarray(challenges, dtype=CHALLENGE_DTYPE)
+    out = np.zeros(3, np.uint64)
+    lib().orc_fold_binary(_p(u), _p(ch), len(ch), _p(out))
+    return out
+
+
+def round_trip(params: Params, matrix_seed: bytes, witness_seed: bytes = None, witness=None,
+               domain: bytes = b"labinius/reference", threads=1):
+    """One reference round (crates/bench/src/bin/labinius.rs:104-130): commit, evaluation point,
+    mle and row evaluation, folding challenges, fold, and (Clear mode) the folded commitment."""
+    if witness is None:
+        witness = witness_random(params.witness_len, witness_seed)
+    A = key_expand(params, key_seed(matrix_seed))
+    C = commit(params, A, witness, threads=threads)
+    out = dict(A=A, witness=witness, C=C)
+    t = Transcript(domain)
+    if params.dropped_bits:
+        top, digits = drop_bits(params, C)
+        out.update(top=top, digits=digits, packed=pack_dropped(params, top, digits))
+        p0, p1 = derive_evaluation_point(params, matrix_seed, t, top=top, digits=digits)
+    else:
+        p0, p1 = derive_evaluation_point(params, matrix_seed, t, C=C)
+    u = row_evaluate(witness, p0)
+    mle = claim(u, p1)
+    ch = derive_folding_challenges(params, t, u)
+    v = fold(params, witness, ch, threads=threads)
+    out.update(p0=p0, p1=p1, u=u, mle=mle, challenges=ch, v=v)
+    if not params.dropped_bits:
+        out["folded_commitment"] = fold_commitment(params, C, ch)
+    out["transcript_tail"] = t.fill(b"labinius/test-tail", 32)
+    return out
