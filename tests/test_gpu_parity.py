@@ -62,7 +62,7 @@ def oracle_params(oracle, shape):
     return oracle.Params(wl, cl, primes, d)
 
 
-@pytest.mark.parametrize("shape", [(10, 2, ALL, 0), (12, 6, [3889, 9721], 0), (13, 1, [19441, 2917], 0)],
+@pytest.mark.parametrize("shape", [(10, 2, ALL, 0), (13, 6, [3889, 9721], 0), (13, 1, [19441, 2917], 0)],
                          ids=["allprimes", "64cols", "2cols"])
 def test_key_matches_oracle(oracle, shape):
     L, params, pp, _ = setup(shape)
@@ -90,7 +90,7 @@ def test_commit_every_prime_adversarial(oracle, base):
     prover.recycle(op)
 
 
-@pytest.mark.parametrize("shape", [(12, 6, [3889, 2917, 4861], 0), (13, 3, [9721], 0), (11, 1, [4861, 12637], 0),
+@pytest.mark.parametrize("shape", [(13, 6, [3889, 2917, 4861], 0), (13, 3, [9721], 0), (11, 1, [4861, 12637], 0),
                                    (14, 4, [3889, 2917, 9721], 0)],
                          ids=["64cols", "8cols", "2cols", "xl-limbs"])
 def test_commit_shapes(oracle, shape):
@@ -167,7 +167,7 @@ def edge_challenges(r):
             c[j]["signs"] = 0b101010
         else:
             c[j]["weight"] = 28
-            c[j]["positions"][:28] = np.arange(0, 162, 6)[:28]
+            c[j]["positions"][:28] = np.arange(0, 162, 5)[:28]
             c[j]["signs"] = 0x0F0F0F0
     return c
 
