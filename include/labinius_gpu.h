@@ -164,6 +164,19 @@ int lbg_params_derive_folding_challenges(const lbg_params* p, lbg_transcript* t,
 size_t lbg_params_pack_dropped(const lbg_params* p, const uint16_t* top, const uint16_t* digits, uint8_t* out,
                                size_t cap);
 
+/* Prover::fold for callers that may not allocate device memory. No counterpart in the reference:
+ * an embedding runtime that owns all device memory, or replays its steps where allocator calls
+ * are not allowed, folds through this entry point, which allocates nothing. Witness (F162,
+ * column-major as lbg_witness holds it), challenges and output v (int16 [len_ring][648]) are device
+ * pointers the caller owns; the scratch and tables live in static device arrays (about 1.4 MB per
+ * GPU, held until exit). At most LBG_FOLD_STATIC_MAX_COLUMNS columns; larger shapes are rejected.
+ * The first call on a device sets it up and synchronises (make it before any stream capture);
+ * calls share the scratch, so calls that overlap on the GPU race. Asynchronous on `stream`. */
+#define LBG_FOLD_STATIC_MAX_COLUMNS 1024
+int lbg_fold_static(uint32_t base_prime, uint32_t witness_log_len, uint32_t column_log_len,
+                    const uint64_t* d_witness, const lbg_challenge* d_challenges, size_t r, int16_t* d_v_out,
+                    void* stream);
+
 /* Shape queries. */
 size_t lbg_pp_columns(const lbg_pp* pp);
 size_t lbg_pp_len_ring(const lbg_pp* pp);

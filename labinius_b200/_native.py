@@ -78,6 +78,7 @@ SIGNATURES = {
     "lbg_params_derive_evaluation_point": (_int, [_P, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "lbg_params_derive_folding_challenges": (_int, [_P, _vp, _vp, _vp]),
     "lbg_params_pack_dropped": (_sz, [_P, _vp, _vp, _vp, _sz]),
+    "lbg_fold_static": (_int, [_u32, _u32, _u32, _vp, _vp, _sz, _vp, _vp]),
 }
 
 _lib = None

@@ -10,6 +10,7 @@
 
 #include "../../include/labinius_gpu.h"
 #include "prime_structs.h"
+#include "error.h"
 #include "launch.h"
 #include "ring_tables.h"
 #include "transcript.h"
@@ -24,6 +25,10 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 }  // namespace
+
+namespace lbg {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace lbg
 
 #define LBG_CU(x)                                                                       \
   do {                                                                                  \

@@ -1,0 +1,50 @@
+"""lbg_fold_static: the fold for callers that may not allocate device memory when they fold (an
+embedding runtime that owns all device memory through its own arena, or one that replays its
+steps where allocator calls are not allowed). Its scratch is a static device array, so it is
+checked here against the allocating entry point lbg_fold, twice in a row on the same scratch.
+
+This file is collected last (test_zz_*) and passes both alone in a fresh process and after the
+rest of the suite: the entry point sets its device up on first use either way."""
+import numpy as np
+import pytest
+
+from rounds import MATRIX_SEED, WITNESS_SEED, product_params
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("shape", [(12, 4, [3889, 2917, 4861], 0), (13, 5, [2917, 9721], 0)], ids=["3889", "2917"])
+def test_fold_static_matches_fold(shape):
+    import torch
+
+    import labinius_b200 as L
+    from labinius_b200._native import LBG_ERR_INVALID, LBG_OK, lib
+
+    params = product_params(shape)
+    pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+    w = L.Witness.random(pp, WITNESS_SEED)
+    prover = L.Prover(pp)
+    verifier = L.Verifier(pp)
+    c, op = prover.commit(w)
+    t = L.Transcript(b"labinius/reference")
+    point = verifier.derive_evaluation_point(t, c)
+    ch = verifier.derive_folding_challenges(t, w.row_evaluate(point))
+    want = prover.fold(op, ch).elements
+
+    # device memory the caller owns
+    d_w = torch.from_numpy(w.elements().view(np.int64)).cuda()
+    d_ch = torch.from_numpy(np.ascontiguousarray(ch.challenges).view(np.uint8).copy()).cuda()
+    d_v = torch.empty((params.len_ring(), 648), dtype=torch.int16, device="cuda")
+    base, wl, cl, r = params.primes()[0], params.witness_log_len, params.column_log_len, params.columns()
+    for _ in range(2):
+        d_v.fill_(0x5A5A)
+        torch.cuda.synchronize()
+        rc = lib().lbg_fold_static(base, wl, cl, d_w.data_ptr(), d_ch.data_ptr(), r, d_v.data_ptr(), None)
+        assert rc == LBG_OK, lib().lbg_last_error()
+        torch.cuda.synchronize()
+        assert np.array_equal(d_v.cpu().numpy(), want)
+
+    # beyond the static maximum: rejected with a clear message, nothing launched
+    rc = lib().lbg_fold_static(base, 20, 11, d_w.data_ptr(), d_ch.data_ptr(), 2048, d_v.data_ptr(), None)
+    assert rc == LBG_ERR_INVALID
+    assert b"at most 1024 columns" in lib().lbg_last_error()
