@@ -293,7 +293,7 @@ def run_ours(args):
 
     # roofline of the dominant kernel (commit, one launch per limb): algorithmic bytes per launch =
     # the witness (24 B per F162) + the key's component form (32 B per ring element and leaf) + the
-    # per-chunk partial sums it writes
+    # limb's commitment (16 B per column and leaf)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -304,7 +304,7 @@ def run_ours(args):
     cnt, tot = stats["commit"]
     per_launch_ms = tot / max(cnt, 1)
     len_ring = params.len_ring()
-    algo_bytes = 24 * n + len_ring * 162 * 32 + r * 162 * 16 * 8
+    algo_bytes = 24 * n + len_ring * 162 * 32 + r * 162 * 16
     achieved = algo_bytes / (per_launch_ms / 1000.0) / 1e9
     traffic = None
     try:

@@ -81,7 +81,9 @@ struct lbg_prover {
   const lbg_pp* pp = nullptr;
   cudaStream_t stream = nullptr;
   int chunk = 0, nchunks = 0;
+  int fold_cols_per_split = 0;
   int32_t* d_partial = nullptr;
+  uint32_t* d_vhat = nullptr;  // [wdim][162]
   lbg_challenge_d* d_ch = nullptr;
   uint32_t* d_chat = nullptr;
   int16_t* d_v = nullptr;     // [len_ring][648]
@@ -114,8 +116,8 @@ struct KernelScope {
     cudaEventCreate(&e);
     return e;
   }
-  KernelScope(lbg_prover* p, const char* n) : pr(p), name(n) {
-    pr->launches++;
+  KernelScope(lbg_prover* p, const char* n, int kernels = 1) : pr(p), name(n) {
+    pr->launches += kernels;
     if (pr->profiling) {
       a = take(pr);
       b = take(pr);
@@ -430,6 +432,7 @@ void lbg_prover_free(lbg_prover* pr) {
   cudaSetDevice(pr->pp->device);
   if (pr->stream) cudaStreamSynchronize(pr->stream);
   cudaFree(pr->d_partial);
+  cudaFree(pr->d_vhat);
   cudaFree(pr->d_ch);
   cudaFree(pr->d_chat);
   cudaFree(pr->d_v);
@@ -479,18 +482,51 @@ int lbg_prover_new(const lbg_pp* pp, lbg_prover** out) {
   };
   if (cudaStreamCreateWithFlags(&pr->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(LBG_ERR_CUDA, "stream"));
-  // Grid: ceil(cols / 32) column tiles x nchunks ring-element chunks, aiming at >= 2 waves of 148.
+  // Grid: column tiles x ring-element chunks. A wave of the commit kernel is (SMs x resident CTAs)
+  // CTAs and its length is proportional to the chunk, so pick the chunk count that minimises
+  // waves x chunk (ties: fewer chunks, fewer partial sums).
   int col_tiles = (int)((pp->cols + commit_cols_per_cta() - 1) / commit_cols_per_cta());
-  int want = (296 + col_tiles - 1) / col_tiles;
-  int max_chunks = (int)(pp->len_ring / 16);
-  if (max_chunks < 1) max_chunks = 1;
-  pr->nchunks = want < max_chunks ? want : max_chunks;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pp->device);
+  int slots = sms * commit_blocks_per_sm(pp->pidx[0]);
   int step = commit_ring_per_step();
-  pr->chunk = (int)((pp->len_ring + pr->nchunks - 1) / pr->nchunks);
-  pr->chunk = (pr->chunk + step - 1) / step * step;
-  pr->nchunks = (int)((pp->len_ring + pr->chunk - 1) / pr->chunk);
+  long best_cost = -1;
+  int max_chunks = (int)((pp->len_ring + step - 1) / step);
+  for (int nch = 1; nch <= max_chunks; nch++) {
+    int chunk = (int)((pp->len_ring + nch - 1) / nch);
+    chunk = (chunk + step - 1) / step * step;
+    int nact = (int)((pp->len_ring + chunk - 1) / chunk);
+    long total = (long)col_tiles * nact;
+    long waves = (total + slots - 1) / slots;
+    long cost = waves * chunk;
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      pr->chunk = chunk;
+      pr->nchunks = nact;
+    }
+  }
+  // the fold: position tiles x column splits, chosen the same way
+  {
+    int tiles = (int)((pp->wdim + fold_positions_per_cta() - 1) / fold_positions_per_cta());
+    int fslots = sms * fold_blocks_per_sm(pp->pidx[0]);
+    int fstep = fold_cols_per_step();
+    long best = -1;
+    int max_splits = (int)((pp->cols + fstep - 1) / fstep);
+    for (int ns = 1; ns <= max_splits; ns++) {
+      int per = (int)((pp->cols + ns - 1) / ns);
+      per = (per + fstep - 1) / fstep * fstep;
+      int nact = (int)((pp->cols + per - 1) / per);
+      long total = (long)tiles * nact;
+      long cost = ((total + fslots - 1) / fslots) * per;
+      if (best < 0 || cost < best) {
+        best = cost;
+        pr->fold_cols_per_split = per;
+      }
+    }
+  }
   size_t count = pp->cols * N648;
   if (cudaMalloc((void**)&pr->d_partial, (size_t)pr->nchunks * pp->cols * N162 * 16) != cudaSuccess ||
+      cudaMalloc((void**)&pr->d_vhat, pp->wdim * N162 * 4) != cudaSuccess ||
       cudaMalloc((void**)&pr->d_ch, pp->cols * sizeof(lbg_challenge_d)) != cudaSuccess ||
       cudaMalloc((void**)&pr->d_chat, pp->cols * N162 * 4) != cudaSuccess ||
       cudaMalloc((void**)&pr->d_v, pp->len_ring * N648 * 2) != cudaSuccess ||
@@ -721,8 +757,9 @@ int lbg_fold(lbg_prover* pr, lbg_opening* op, const lbg_challenge* challenges, s
     e = launch_challenge_slots(pp->pidx[0], pr->d_ch, (int)r, pp->d_prime[0], pr->d_chat, st);
   }
   if (e == cudaSuccess) {
-    KernelScope ks(pr, "fold");
-    e = launch_fold(pp->pidx[0], op->w->d, pp->wdim, (int)pp->cols, pr->d_chat, pp->d_prime[0], pr->d_v, st);
+    KernelScope ks(pr, "fold", 2);  // k_fold + k_fold_finish
+    e = launch_fold(pp->pidx[0], op->w->d, pp->wdim, (int)pp->cols, pr->fold_cols_per_split, pr->d_chat,
+                    pp->d_prime[0], pr->d_vhat, pr->d_v, st);
   }
   if (e == cudaSuccess && v_out) e = cudaMemcpyAsync(v_out, pr->d_v, pp->len_ring * N648 * 2, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess && v_out) e = cudaStreamSynchronize(st);

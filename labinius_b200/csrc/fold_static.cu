@@ -137,7 +137,8 @@ int lbg_fold_static(uint32_t base_prime, uint32_t witness_log_len, uint32_t colu
   uint32_t* d_chat = (uint32_t*)S->scratch;
   // every slot value of the r challenges is rewritten by the first launch, so nothing needs clearing
   e = launch_challenge_slots(pi, (const lbg_challenge_d*)d_challenges, (int)r, S->tables + pi, d_chat, st);
-  if (e == cudaSuccess) e = launch_fold(pi, d_witness, wdim, (int)cols, d_chat, S->tables + pi, d_v_out, st);
+  if (e == cudaSuccess)
+    e = launch_fold(pi, d_witness, wdim, (int)cols, (int)cols, d_chat, S->tables + pi, nullptr, d_v_out, st);
   if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("lbg_fold_static: ") + cudaGetErrorString(e));
   return LBG_OK;
 }

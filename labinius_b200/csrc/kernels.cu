@@ -78,22 +78,24 @@ __global__ void k_key_components(const int16_t* __restrict__ A, const DevPrime* 
 // =============================================================================================
 // Commit: Y_j(v) = sum_i Ahat_i(v) (x) What_{j,i}(v) per column j and leaf v
 // =============================================================================================
-// CTA: 32 columns x a chunk of ring elements, two ring elements per step.
-//  phase A: warp w transforms F162 number (w & 3) of ring element (w >> 2) for its lane's column
-//           into smem What[ii][v][lane][k] (u16, fully reduced);
-//  phase B: warp w owns the leaves v = w + 8 u; each lane accumulates its column's four components
-//           Y_0..Y_3 for those leaves: 16 multiply-adds per (ring element, leaf).
-constexpr int CT = 32;            // columns per CTA
-constexpr int RT = 2;             // ring elements per step
-constexpr int VPW = 21;           // leaves per warp (8 warps, 162 leaves)
+// CTA: 16 columns x a chunk of ring elements, four ring elements per step, 256 threads.
+//  phase A: thread t transforms F162 number t of the step's tile (column t / 16, F162 t % 16 of
+//           the column's 16) into smem What[ii][v][jj][k] (u16, in [0, 2q));
+//  phase B: lane l of warp w serves column l % 16 and the leaves v = 2 (w + 8 u) + l / 16; it
+//           accumulates Y_0..Y_3 of those leaves: 16 multiply-adds per (ring element, leaf).
+constexpr int CT = 16;   // columns per CTA
+constexpr int RT = 4;    // ring elements per step
+constexpr int VPT = 11;  // leaves per thread (8 warps x 2 halves x 11 >= 162)
+constexpr int WROW = RT * 12 + 1;          // staged witness words per column, padded
+constexpr int LUT_BYTES = 6 * 64 * 2;      // the six u16 tables
 
 template <int PI>
-__device__ __forceinline__ void commit_phase_a_store(uint16_t* __restrict__ wt, int ii, int k, int lane,
-                                                     const uint32_t idx[7], const uint32_t* lut) {
+__device__ __forceinline__ void commit_phase_a_store(uint16_t* __restrict__ wt, int ii, int k, int jj,
+                                                     const uint32_t idx[7], const uint8_t* lut) {
   uint32_t v[27];
 #define LBG_BLOCK(TAU)                                                                 \
   ntt_block<PI, TAU>(idx, lut, v);                                                     \
-  _Pragma("unroll") for (int x = 0; x < 27; x++) wt[(((ii * N162) + TAU * 27 + x) * CT + lane) * 4 + k] = (uint16_t)v[x];
+  _Pragma("unroll") for (int x = 0; x < 27; x++) wt[(((ii * N162) + TAU * 27 + x) * CT + jj) * 4 + k] = (uint16_t)v[x];
   LBG_BLOCK(0)
   LBG_BLOCK(1)
   LBG_BLOCK(2)
@@ -103,64 +105,66 @@ __device__ __forceinline__ void commit_phase_a_store(uint16_t* __restrict__ wt, 
 #undef LBG_BLOCK
 }
 
-// Steps between two fold-backs of the signed accumulators: each step adds at most
-// RT * 4 * (q-1)/2 * (q-1) per lane, and a fold-back leaves |acc| < 2q.
+// Ring elements between two fold-backs of the signed accumulators: one ring element adds at most
+// 4 products |Ahat| |What| < (q-1)/2 * 2q per lane, and a fold-back leaves |acc| < 2q.
 template <int PI>
 struct CommitRed {
-  static constexpr int raw =
-      (int)((2147483647ull - 2ull * Pr<PI>::q) / ((uint64_t)RT * 4 * ((Pr<PI>::q - 1) / 2) * (Pr<PI>::q - 1)));
+  static constexpr int raw = (int)((2147483647ull - 2ull * Pr<PI>::q) /
+                                   ((uint64_t)4 * ((Pr<PI>::q - 1) / 2) * (2 * Pr<PI>::q)));
   static constexpr int value = raw < 1 ? 1 : raw;
 };
 
 template <int PI>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, 2)
     k_commit(const uint64_t* __restrict__ W, size_t wdim, const int4* __restrict__ Ahat,
              const DevPrime* __restrict__ D, int cols, int len_ring, int chunk,
              int32_t* __restrict__ partial /* [nchunks][cols][162][4] */) {
   extern __shared__ __align__(16) uint8_t smem[];
-  uint32_t* lut = (uint32_t*)smem;                                  // 6 * 64 u32
-  uint64_t* wtile = (uint64_t*)(smem + 6 * 64 * 4);                 // CT * RT * 4 * 3 u64
-  uint16_t* wt = (uint16_t*)(smem + 6 * 64 * 4 + CT * RT * 4 * 24);  // RT * 162 * CT * 4 u16
+  uint16_t* lut = (uint16_t*)smem;                        // 6 * 64 u16
+  uint64_t* wtile = (uint64_t*)(smem + LUT_BYTES);        // CT rows of WROW u64 (one pad word)
+  uint16_t* wt = (uint16_t*)(smem + LUT_BYTES + CT * WROW * 8);  // RT * 162 * CT * 4 u16
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int j0 = blockIdx.x * CT;
   const int i_begin = blockIdx.y * chunk;
   const int i_end = min(len_ring, i_begin + chunk);
-  for (int x = tid; x < 6 * 64; x += 256) lut[x] = D->lut[x / 64][x % 64];
+  for (int x = tid; x < 6 * 64; x += 256) lut[x] = (uint16_t)D->lut[x / 64][x % 64];
+  const int jj_b = lane & 15, half = lane >> 4;
 
-  int32_t acc[VPW][4];
+  int32_t acc[VPT][4];
 #pragma unroll
-  for (int u = 0; u < VPW; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
+  for (int u = 0; u < VPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
   constexpr int RED = CommitRed<PI>::value;
   int since = 0;
 
   for (int i0 = i_begin; i0 < i_end; i0 += RT) {
     __syncthreads();
-    // stage the witness tile: column jj, ring elements i0, i0+1 -> 8 F162 = 24 u64, contiguous
+    // stage the witness tile: column jj, ring elements i0 .. i0+3 -> 16 F162 = 48 u64, contiguous
     for (int x = tid; x < CT * RT * 12; x += 256) {
       int jj = x / (RT * 12), wd = x % (RT * 12);
       int j = j0 + jj;
       uint64_t val = 0;
       size_t f = (size_t)4 * i0 + wd / 3;  // F162 index inside the column
       if (j < cols && f < (size_t)4 * i_end) val = W[((size_t)j * wdim + f) * 3 + wd % 3];
-      wtile[x] = val;
+      wtile[jj * WROW + wd] = val;
     }
     __syncthreads();
     {
-      int ii = warp >> 2, k = warp & 3;
-      const uint64_t* e = wtile + lane * (RT * 12) + (ii * 4 + k) * 3;
+      // lanes run over columns, so a warp's What stores hit 16 distinct banks
+      int jj = tid & 15, g = tid >> 4;  // column, F162 within the column's tile
+      const uint64_t* e = wtile + jj * WROW + g * 3;
       uint32_t idx[7];
       f162_windows(e[0], e[1], e[2], idx);
-      commit_phase_a_store<PI>(wt, ii, k, lane, idx, lut);
+      commit_phase_a_store<PI>(wt, g >> 2, g & 3, jj, idx, (const uint8_t*)lut);
     }
     __syncthreads();
     const int nsteps = min(RT, i_end - i0);
     for (int ii = 0; ii < nsteps; ii++) {
       const int4* ah = Ahat + (size_t)(i0 + ii) * N162 * 2;
 #pragma unroll
-      for (int u = 0; u < VPW; u++) {
-        int v = warp + 8 * u;
+      for (int u = 0; u < VPT; u++) {
+        int v = 2 * (warp + 8 * u) + half;
         if (v < N162) {
-          uint2 wv = *(const uint2*)(wt + (((ii * N162) + v) * CT + lane) * 4);
+          uint2 wv = *(const uint2*)(wt + (((ii * N162) + v) * CT + jj_b) * 4);
           int32_t w0 = wv.x & 0xFFFF, w1 = wv.x >> 16, w2 = wv.y & 0xFFFF, w3 = wv.y >> 16;
           int4 lo = __ldg(ah + 2 * v), hi = __ldg(ah + 2 * v + 1);
           acc[u][0] += lo.x * w0 + hi.x * w3 + hi.y * w2 + hi.z * w1;
@@ -169,20 +173,20 @@ __global__ void __launch_bounds__(256, 1)
           acc[u][3] += lo.w * w0 + lo.z * w1 + lo.y * w2 + lo.x * w3;
         }
       }
-    }
-    if (++since >= RED) {
-      since = 0;
+      if (++since >= RED) {
+        since = 0;
 #pragma unroll
-      for (int u = 0; u < VPW; u++)
+        for (int u = 0; u < VPT; u++)
 #pragma unroll
-        for (int c = 0; c < 4; c++) acc[u][c] = red_signed<PI>(acc[u][c]);
+          for (int c = 0; c < 4; c++) acc[u][c] = red_signed<PI>(acc[u][c]);
+      }
     }
   }
-  const int j = j0 + lane;
+  const int j = j0 + jj_b;
   if (j < cols) {
 #pragma unroll
-    for (int u = 0; u < VPW; u++) {
-      int v = warp + 8 * u;
+    for (int u = 0; u < VPT; u++) {
+      int v = 2 * (warp + 8 * u) + half;
       if (v < N162) {
         int4 o;
         o.x = (int)red_signed_full<PI>(acc[u][0]);
@@ -241,16 +245,19 @@ __global__ void k_challenge_slots(const lbg_challenge_d* __restrict__ ch, int r,
 
 constexpr int FP = 32;  // positions per CTA
 constexpr int FJ = 8;   // columns per step
+constexpr int VPW = 21; // leaves per warp (8 warps, 162 leaves)
 
+// Columns between two fold-backs of the unsigned accumulators: a column adds one product
+// chat * What < q * 2q per lane, and a fold-back leaves acc < 2q.
 template <int PI>
 struct FoldRed {
-  static constexpr int raw = (int)((4294967295ull - 2ull * Pr<PI>::q) / ((uint64_t)FJ * Pr<PI>::q * Pr<PI>::q));
+  static constexpr int raw = (int)((4294967295ull - 2ull * Pr<PI>::q) / (2ull * Pr<PI>::q * Pr<PI>::q));
   static constexpr int value = raw < 1 ? 1 : raw;
 };
 
 template <int PI>
 __device__ __forceinline__ void fold_phase_a_store(uint16_t* __restrict__ wt, int jj, int lane,
-                                                   const uint32_t idx[7], const uint32_t* lut) {
+                                                   const uint32_t idx[7], const uint8_t* lut) {
   uint32_t v[27];
 #define LBG_BLOCK(TAU)                  \
   ntt_block<PI, TAU>(idx, lut, v);      \
@@ -264,28 +271,37 @@ __device__ __forceinline__ void fold_phase_a_store(uint16_t* __restrict__ wt, in
 #undef LBG_BLOCK
 }
 
-template <int PI>
-__global__ void __launch_bounds__(256, 1)
-    k_fold(const uint64_t* __restrict__ W, size_t wdim, int cols, const uint32_t* __restrict__ chat,
-           const DevPrime* __restrict__ D, int16_t* __restrict__ v_out /* [len_ring][648] */) {
+// One CTA: 32 F162 positions x the columns [c_begin, c_end), eight columns per step.
+//  phase A: warp w transforms the F162 of column c + w at its lane's position into smem;
+//  phase B: warp w owns the leaves v = w + 8 u; lane = position; one multiply-add per (column, leaf).
+// Split mode: the CTA's sums, reduced to [0, q), are added into vhat[p][v] (u32, zeroed by the
+// caller; with at most 2^16 column splits the total stays below 2^32) and k_fold_finish inverts.
+// Direct mode (one split): the CTA inverts its 32 positions itself and writes v, no vhat.
+template <int PI, bool DIRECT>
+__global__ void __launch_bounds__(256, 2)
+    k_fold(const uint64_t* __restrict__ W, size_t wdim, int cols, int cols_per_split,
+           const uint32_t* __restrict__ chat, const DevPrime* __restrict__ D, uint32_t* __restrict__ vhat,
+           int16_t* __restrict__ v_out) {
   extern __shared__ __align__(16) uint8_t smem[];
-  uint32_t* lut = (uint32_t*)smem;
-  uint16_t* wt = (uint16_t*)(smem + 6 * 64 * 4);  // FJ * 162 * FP u16 (also reused for v-hat)
+  uint16_t* lut = (uint16_t*)smem;
+  uint16_t* wt = (uint16_t*)(smem + LUT_BYTES);  // FJ * 162 * FP u16
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const size_t p0 = (size_t)blockIdx.x * FP;
-  for (int x = tid; x < 6 * 64; x += 256) lut[x] = D->lut[x / 64][x % 64];
+  const int c_begin = blockIdx.y * cols_per_split;
+  const int c_end = min(cols, c_begin + cols_per_split);
+  for (int x = tid; x < 6 * 64; x += 256) lut[x] = (uint16_t)D->lut[x / 64][x % 64];
   uint32_t acc[VPW];
 #pragma unroll
   for (int u = 0; u < VPW; u++) acc[u] = 0;
   constexpr int RED = FoldRed<PI>::value;
   int since = 0;
-  for (int j0 = 0; j0 < cols; j0 += FJ) {
+  for (int j0 = c_begin; j0 < c_end; j0 += FJ) {
     __syncthreads();
     {
       int j = j0 + warp;
       size_t p = p0 + lane;
       uint64_t e0 = 0, e1 = 0, e2 = 0;
-      if (j < cols && p < wdim) {
+      if (j < c_end && p < wdim) {
         const uint64_t* e = W + ((size_t)j * wdim + p) * 3;
         e0 = e[0];
         e1 = e[1];
@@ -293,10 +309,10 @@ __global__ void __launch_bounds__(256, 1)
       }
       uint32_t idx[7];
       f162_windows(e0, e1, e2, idx);
-      fold_phase_a_store<PI>(wt, warp, lane, idx, lut);
+      fold_phase_a_store<PI>(wt, warp, lane, idx, (const uint8_t*)lut);
     }
     __syncthreads();
-    const int nj = min(FJ, cols - j0);
+    const int nj = min(FJ, c_end - j0);
     for (int jj = 0; jj < nj; jj++) {
       const uint32_t* ch = chat + (size_t)(j0 + jj) * N162;
 #pragma unroll
@@ -304,16 +320,26 @@ __global__ void __launch_bounds__(256, 1)
         int v = warp + 8 * u;
         if (v < N162) acc[u] += __ldg(ch + v) * (uint32_t)wt[((jj * N162) + v) * FP + lane];
       }
-    }
-    if (++since >= RED) {
-      since = 0;
+      if (++since >= RED) {
+        since = 0;
 #pragma unroll
-      for (int u = 0; u < VPW; u++) acc[u] = red_full<PI>(acc[u]);
+        for (int u = 0; u < VPW; u++) acc[u] = red_half<PI>(acc[u]);
+      }
     }
   }
+  if (!DIRECT) {
+    const size_t p = p0 + lane;
+    if (p < wdim) {
+#pragma unroll
+      for (int u = 0; u < VPW; u++) {
+        int v = warp + 8 * u;
+        if (v < N162) atomicAdd(vhat + p * N162 + v, red_full<PI>(acc[u]));
+      }
+    }
+    return;
+  }
   __syncthreads();
-  // v-hat of the 32 positions into smem, [pos][162] u32
-  uint32_t* vh = (uint32_t*)wt;
+  uint32_t* vh = (uint32_t*)wt;  // [FP][162] u32, 20.7 KB of the 83 KB stage
 #pragma unroll
   for (int u = 0; u < VPW; u++) {
     int v = warp + 8 * u;
@@ -330,6 +356,21 @@ __global__ void __launch_bounds__(256, 1)
       for (int m = 0; m < N162; m++) v_out[i * N648 + 4 * m + k] = center<PI>(x[m]);
     }
   }
+}
+
+// The inverse transform of each position's sums, centred, into the folded witness: position
+// p = 4 i + k gives coefficients 4 m + k of ring element i (crates/pcs/src/fold.rs:620-677).
+template <int PI>
+__global__ void k_fold_finish(const uint32_t* __restrict__ vhat, size_t wdim, const DevPrime* __restrict__ D,
+                              int16_t* __restrict__ v_out /* [len_ring][648] */) {
+  size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= wdim) return;
+  uint32_t x[N162];
+  for (int v = 0; v < N162; v++) x[v] = vhat[p * N162 + v] % Pr<PI>::q;
+  intt162_serial<PI>(x, *D);
+  size_t i = p / 4;
+  int k = (int)(p % 4);
+  for (int m = 0; m < N162; m++) v_out[i * N648 + 4 * m + k] = center<PI>(x[m]);
 }
 
 // Verifier::fold_commitment: out[row][limb][s] = sum_j chat_j(s) C_j[row][limb][s]
@@ -592,7 +633,23 @@ cudaError_t launch_key_components(int pi, const int16_t* A, const DevPrime* D, i
   return cudaGetLastError();
 }
 
-size_t commit_smem_bytes() { return 6 * 64 * 4 + CT * RT * 4 * 24 + RT * N162 * CT * 4 * 2; }
+size_t commit_smem_bytes() { return LUT_BYTES + CT * WROW * 8 + RT * N162 * CT * 4 * 2; }
+
+int commit_blocks_per_sm(int pi) {
+  int n = 0;
+  size_t smem = commit_smem_bytes();
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (pi) {
+#define LBG_OCC(I)                                                                                      \
+  case I:                                                                                               \
+    cudaFuncSetAttribute(k_commit<I>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);          \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_commit<I>, 256, smem);                      \
+    break;
+    LBG_OCC(0) LBG_OCC(1) LBG_OCC(2) LBG_OCC(3) LBG_OCC(4) LBG_OCC(5) LBG_OCC(6)
+#undef LBG_OCC
+  }
+  return (e == cudaSuccess && n > 0) ? n : 1;
+}
 int commit_cols_per_cta() { return CT; }
 int commit_ring_per_step() { return RT; }
 
@@ -621,18 +678,46 @@ cudaError_t launch_challenge_slots(int pi, const lbg_challenge_d* ch, int r, con
   return cudaGetLastError();
 }
 
-size_t fold_smem_bytes() {
-  size_t a = (size_t)FJ * N162 * FP * 2, b = (size_t)FP * N162 * 4;
-  return 6 * 64 * 4 + (a > b ? a : b);
+size_t fold_smem_bytes() { return LUT_BYTES + (size_t)FJ * N162 * FP * 2; }
+int fold_positions_per_cta() { return FP; }
+int fold_cols_per_step() { return FJ; }
+
+int fold_blocks_per_sm(int pi) {
+  int n = 0;
+  size_t smem = fold_smem_bytes();
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (pi) {
+#define LBG_OCC(I)                                                                                      \
+  case I:                                                                                               \
+    cudaFuncSetAttribute(k_fold<I, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fold<I, false>, 256, smem);                 \
+    break;
+    LBG_OCC(0) LBG_OCC(1) LBG_OCC(2) LBG_OCC(3) LBG_OCC(4) LBG_OCC(5) LBG_OCC(6)
+#undef LBG_OCC
+  }
+  return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
-cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, const uint32_t* chat, const DevPrime* D,
-                        int16_t* v, cudaStream_t st) {
-  unsigned grid = blocks_for(wdim, FP);
+cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
+                        const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st) {
   size_t smem = fold_smem_bytes();
+  if (!vhat) {  // direct mode: one split, no scratch beyond chat
+    dim3 grid(blocks_for(wdim, FP), 1);
+    LBG_DISPATCH(pi, ({
+                   cudaFuncSetAttribute(k_fold<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                   k_fold<P, true><<<grid, 256, smem, st>>>(W, wdim, cols, cols, chat, D, nullptr, v);
+                 }));
+    return cudaGetLastError();
+  }
+  int splits = (cols + cols_per_split - 1) / cols_per_split;
+  if (splits < 1 || splits > 65535) return cudaErrorInvalidValue;
+  dim3 grid(blocks_for(wdim, FP), splits);
+  cudaError_t e = cudaMemsetAsync(vhat, 0, wdim * N162 * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
   LBG_DISPATCH(pi, ({
-                 cudaFuncSetAttribute(k_fold<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                 k_fold<P><<<grid, 256, smem, st>>>(W, wdim, cols, chat, D, v);
+                 cudaFuncSetAttribute(k_fold<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                 k_fold<P, false><<<grid, 256, smem, st>>>(W, wdim, cols, cols_per_split, chat, D, vhat, nullptr);
+                 k_fold_finish<P><<<blocks_for(wdim, 64), 64, 0, st>>>(vhat, wdim, D, v);
                }));
   return cudaGetLastError();
 }

@@ -49,6 +49,11 @@ __device__ __forceinline__ uint32_t red_full(uint32_t x) {
   uint32_t r = x - __umulhi(x, Pr<PI>::qs) * q;
   return r >= q ? r - q : r;
 }
+// x mod q up to one extra q: [0, 2q), for x < 2^32.
+template <int PI>
+__device__ __forceinline__ uint32_t red_half(uint32_t x) {
+  return x - __umulhi(x, Pr<PI>::qs) * Pr<PI>::q;
+}
 // a * b mod q for a, b < q (rare paths).
 template <int PI>
 __device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b) {
@@ -71,25 +76,27 @@ __device__ __forceinline__ int16_t center(uint32_t x) {
   return (int16_t)(x > (q - 1) / 2 ? (int32_t)x - (int32_t)q : (int32_t)x);
 }
 
-// Lazy radix-3 butterfly of the 162-point tree: sub-ring Y^n - z^3 -> children Y^{n/3} - z w^s.
-// Inputs any u32 below 2^32 - 4q; outputs grow by at most 4q.
+// Lazy radix-3 butterfly of the 162-point tree: sub-ring Y^n - z^3 -> children Y^{n/3} - z w^s,
+// y_s = a0 + (z w^s) a1 + (z w^s)^2 a2, with w^2 = -1 - w:
+//   t1 = z a1, t2 = z^2 a2, m = w (t1 - t2);  y0 = a0 + t1 + t2,  y1 = a0 - t2 + m,  y2 = a0 - t1 - m.
+// Products are Shoup's, in [0, 2q); the constant 4q keeps every difference non-negative, so an
+// output exceeds its inputs' bound by at most 6q.
 template <int PI>
 __device__ __forceinline__ void bfly3(uint32_t& a0, uint32_t& a1, uint32_t& a2, const Twiddle& t,
                                       uint32_t om, uint32_t oms) {
   constexpr uint32_t q = Pr<PI>::q;
   uint32_t t1 = mul_shoup(a1, t.z, t.zs, q);
   uint32_t t2 = mul_shoup(a2, t.z2, t.z2s, q);
-  uint32_t m = mul_shoup(t1 + 2 * q - t2, om, oms, q);
-  uint32_t y0 = a0 + t1 + t2;
-  uint32_t y1 = a0 + 2 * q - t2 + m;
-  uint32_t y2 = a0 + 4 * q - t1 - m;
-  a0 = y0;
-  a1 = y1;
-  a2 = y2;
+  uint32_t m = mul_shoup(t1 - t2 + 2 * q, om, oms, q);
+  uint32_t b = a0 + 4 * q;
+  a0 = a0 + t1 + t2;
+  a1 = b - t2 + m;
+  a2 = b - t1 - m;
 }
 
-// The 27 six-bit LUT indices of one F162 (4 per word, one per byte): index m collects bits
-// m + 27 t, t = 0..5, of the element, the coefficients levels 0 and 1 of the tree combine.
+// The 27 six-bit LUT indices of one F162, as byte offsets into a u16 table (2 x index, one per
+// byte, four per word): index m collects bits m + 27 t, t = 0..5, of the element, the
+// coefficients that levels 0 and 1 of the tree combine.
 __device__ __forceinline__ void f162_windows(uint64_t w0, uint64_t w1, uint64_t w2, uint32_t idx[7]) {
   const uint32_t M27 = 0x7FFFFFFu;
   uint32_t c[6];
@@ -105,21 +112,23 @@ __device__ __forceinline__ void f162_windows(uint64_t w0, uint64_t w1, uint64_t 
 #pragma unroll
     for (int t = 0; t < 6; t++) {
       uint32_t nib = (c[t] >> (4 * g)) & 15u;
-      acc += ((nib * 0x00204081u) & 0x01010101u) << t;
+      acc += ((nib * 0x00204081u) & 0x01010101u) << (t + 1);
     }
     idx[g] = acc;
   }
 }
 
-// Forward transform of one level-2 block (27 leaves) of one F162, fully reduced to [0, q):
-// v[x] = w(theta^{E[27 tau + x]}).
+// Forward transform of one level-2 block (27 leaves) of one F162: v[x] = w(theta^{E[27 tau + x]}),
+// reduced to [0, 2q). `lut` holds the six blocks' 64-entry u16 tables in shared memory: 128 bytes
+// a block, one row of the 32 banks, so the 32 lanes' lookups never conflict.
 template <int PI, int TAU>
-__device__ __forceinline__ void ntt_block(const uint32_t idx[7], const uint32_t* __restrict__ lut,
+__device__ __forceinline__ void ntt_block(const uint32_t idx[7], const uint8_t* __restrict__ lut,
                                           uint32_t v[27]) {
   const HotPrime& H = c_hot[PI];
   const uint32_t om = H.omega, oms = H.omega_s;
 #pragma unroll
-  for (int m = 0; m < 27; m++) v[m] = lut[TAU * 64 + ((idx[m >> 2] >> (8 * (m & 3))) & 63u)];
+  for (int m = 0; m < 27; m++)
+    v[m] = *(const uint16_t*)(lut + TAU * 128 + __byte_perm(idx[m >> 2], 0, 0x4440 | (m & 3)));
 #pragma unroll
   for (int i = 0; i < 9; i++) bfly3<PI>(v[i], v[9 + i], v[18 + i], H.tw[TAU][0], om, oms);
 #pragma unroll
@@ -129,7 +138,7 @@ __device__ __forceinline__ void ntt_block(const uint32_t idx[7], const uint32_t*
 #pragma unroll
   for (int s = 0; s < 9; s++) bfly3<PI>(v[3 * s], v[3 * s + 1], v[3 * s + 2], H.tw[TAU][4 + s], om, oms);
 #pragma unroll
-  for (int m = 0; m < 27; m++) v[m] = red_full<PI>(v[m]);
+  for (int m = 0; m < 27; m++) v[m] = red_half<PI>(v[m]);
 }
 
 // Exact inverse of the 162-point transform, in place on x[0..161] (values in [0, q)), one

@@ -36,6 +36,7 @@ cudaError_t launch_key_expand(const uint64_t* jumps, uint64_t state0, uint32_t q
 cudaError_t launch_key_components(int pi, const int16_t* A, const DevPrime* D, int len_ring, int4* Ahat,
                                   cudaStream_t st);
 size_t commit_smem_bytes();
+int commit_blocks_per_sm(int pi);
 int commit_cols_per_cta();
 int commit_ring_per_step();
 cudaError_t launch_commit(int pi, const uint64_t* W, size_t wdim, const int4* Ahat, const DevPrime* D, int cols,
@@ -45,8 +46,14 @@ cudaError_t launch_commit_finish(int pi, const int32_t* partial, int nchunks, in
 cudaError_t launch_challenge_slots(int pi, const lbg_challenge_d* ch, int r, const DevPrime* D, uint32_t* chat,
                                    cudaStream_t st);
 size_t fold_smem_bytes();
-cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, const uint32_t* chat, const DevPrime* D,
-                        int16_t* v, cudaStream_t st);
+int fold_positions_per_cta();
+int fold_cols_per_step();
+int fold_blocks_per_sm(int pi);
+// The fold over all columns: k_fold accumulates column splits of cols_per_split columns into vhat
+// (u32 [wdim][162], zeroed here), then k_fold_finish inverts and centres into v. With vhat null
+// the fold runs in one pass over all columns, each CTA inverting its own positions.
+cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
+                        const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st);
 cudaError_t launch_fold_commitment(int pi, const int16_t* C, int cols, int limb, int limbs, const uint32_t* chat,
                                    const DevPrime* D, int16_t* out, cudaStream_t st);
 cudaError_t launch_column_residues(int pi, const int16_t* C, int cols, int limb, int limbs, const DevPrime* D,
