@@ -177,6 +177,30 @@ int lbg_fold_static(uint32_t base_prime, uint32_t witness_log_len, uint32_t colu
                     const uint64_t* d_witness, const lbg_challenge* d_challenges, size_t r, int16_t* d_v_out,
                     void* stream);
 
+/* Batched rounds: many independent witnesses under one key (all share the public parameters'
+ * column length, moduli and opening; instance i has 2^column_log_lens[i] columns). Every stage is
+ * one launch over all instances; the device stages can be replayed as CUDA graphs, and
+ * lbg_batch_autotune times candidate grid schedules on the batch's own shape. No single reference
+ * call corresponds; each instance's outputs are exactly those of Prover::commit, row_evaluate,
+ * mle_evaluate and fold run on it alone (crates/pcs/src/scheme/prover.rs:55-133). Layouts:
+ * instances one after another (columns, commitments, row values, folded witnesses). */
+typedef struct lbg_batch lbg_batch;
+int lbg_batch_new(const lbg_pp* pp, const uint32_t* column_log_lens, size_t count, lbg_batch** out);
+void lbg_batch_free(lbg_batch* b);
+size_t lbg_batch_columns(const lbg_batch* b);
+int lbg_batch_witness_random(lbg_batch* b, const uint8_t* seeds /* count x 32 bytes */);
+int lbg_batch_witness_upload(lbg_batch* b, size_t instance, const uint64_t* f162, size_t n);
+int lbg_batch_witness_download(const lbg_batch* b, size_t instance, uint64_t* out, size_t n);
+int lbg_batch_use_graphs(lbg_batch* b, int enable);
+int lbg_batch_autotune(lbg_batch* b, uint32_t* chunks_out, uint32_t* fold_cols_out);
+int lbg_batch_commit(lbg_batch* b, int16_t* matrix_out, uint16_t* top_out, uint16_t* digits_out);
+int lbg_batch_row_evaluate(lbg_batch* b, const uint64_t* p0 /* [count][row_log][3] */, uint64_t* u_out);
+int lbg_batch_mle_evaluate(lbg_batch* b, const uint64_t* p0, const uint64_t* p1 /* concatenated */,
+                           uint64_t* out /* [count][3] */);
+int lbg_batch_fold(lbg_batch* b, const lbg_challenge* challenges, size_t r, int16_t* v_out);
+void* lbg_batch_stream(const lbg_batch* b);
+uint64_t lbg_batch_launch_count(const lbg_batch* b);
+
 /* Shape queries. */
 size_t lbg_pp_columns(const lbg_pp* pp);
 size_t lbg_pp_len_ring(const lbg_pp* pp);

@@ -79,6 +79,20 @@ SIGNATURES = {
     "lbg_params_derive_folding_challenges": (_int, [_P, _vp, _vp, _vp]),
     "lbg_params_pack_dropped": (_sz, [_P, _vp, _vp, _vp, _sz]),
     "lbg_fold_static": (_int, [_u32, _u32, _u32, _vp, _vp, _sz, _vp, _vp]),
+    "lbg_batch_new": (_int, [_vp, _vp, _sz, ctypes.POINTER(_vp)]),
+    "lbg_batch_free": (None, [_vp]),
+    "lbg_batch_columns": (_sz, [_vp]),
+    "lbg_batch_witness_random": (_int, [_vp, _vp]),
+    "lbg_batch_witness_upload": (_int, [_vp, _sz, _vp, _sz]),
+    "lbg_batch_witness_download": (_int, [_vp, _sz, _vp, _sz]),
+    "lbg_batch_use_graphs": (_int, [_vp, _int]),
+    "lbg_batch_autotune": (_int, [_vp, _vp, _vp]),
+    "lbg_batch_commit": (_int, [_vp, _vp, _vp, _vp]),
+    "lbg_batch_row_evaluate": (_int, [_vp, _vp, _vp]),
+    "lbg_batch_mle_evaluate": (_int, [_vp, _vp, _vp, _vp]),
+    "lbg_batch_fold": (_int, [_vp, _vp, _sz, _vp]),
+    "lbg_batch_stream": (_vp, [_vp]),
+    "lbg_batch_launch_count": (_u64, [_vp]),
 }
 
 _lib = None

@@ -1,0 +1,163 @@
+"""Batched rounds over the C ABI's lbg_batch: many independent witnesses under one key.
+
+Every instance shares the public parameters' column length, moduli and opening mode; instance i
+has 2^column_log_lens[i] columns, i.e. it is a round of
+``Params(row_log_len + column_log_lens[i], column_log_lens[i], same moduli)``. Each device stage
+(commit, row evaluation, fold) is one launch over all instances; the host steps of the round
+(evaluation point, folding challenges) run per instance in the library's host code.
+"""
+import ctypes
+from dataclasses import dataclass
+from typing import List
+
+import numpy as np
+
+from . import _native as nat
+from ._native import check, lib, ptr
+from .scheme import CHALLENGE_DTYPE, N, N162, Params, PublicParameters
+
+_CH = CHALLENGE_DTYPE
+
+
+@dataclass
+class InstanceRound:
+    matrix: np.ndarray = None  # int16 [cols][4][limbs][162] (Clear)
+    top: np.ndarray = None     # uint16 [cols*648] (bit-dropped)
+    digits: np.ndarray = None  # uint16 [limbs-1][cols*648]
+    p0: np.ndarray = None
+    p1: np.ndarray = None
+    u: np.ndarray = None
+    mle: np.ndarray = None
+    challenges: np.ndarray = None
+    v: np.ndarray = None
+
+
+class Batch:
+    def __init__(self, pp: PublicParameters, column_log_lens):
+        self.pp = pp
+        self.column_log_lens = [int(c) for c in column_log_lens]
+        self.count = len(self.column_log_lens)
+        self.row_log = pp.params.row_log_len()
+        self.wdim = 1 << self.row_log
+        self.len_ring = self.wdim // 4
+        self.limbs = len(pp.params.primes())
+        self.dropped = pp.params.dropped_bits()
+        self.cols = [1 << c for c in self.column_log_lens]
+        self.col_off = np.concatenate([[0], np.cumsum(self.cols)]).astype(np.int64)
+        arr = np.array(self.column_log_lens, np.uint32)
+        h = ctypes.c_void_p()
+        check(lib().lbg_batch_new(pp._h, ptr(arr), self.count, ctypes.byref(h)))
+        self._h = h
+        self.total_cols = int(lib().lbg_batch_columns(h))
+
+    def params_of(self, i) -> Params:
+        p = self.pp.params
+        return Params(self.row_log + self.column_log_lens[i], self.column_log_lens[i], p.base, list(p.extra_moduli),
+                      p.opening)
+
+    def witness_random(self, seeds: List[bytes]):
+        s = np.frombuffer(b"".join(bytes(x) for x in seeds), dtype=np.uint8).copy()
+        assert len(s) == 32 * self.count
+        check(lib().lbg_batch_witness_random(self._h, ptr(s)))
+
+    def witness_upload(self, i, elements):
+        e = np.ascontiguousarray(elements, dtype=np.uint64).reshape(-1, 3)
+        check(lib().lbg_batch_witness_upload(self._h, i, ptr(e), len(e)))
+
+    def elements(self, i) -> np.ndarray:
+        out = np.zeros((self.cols[i] * self.wdim, 3), np.uint64)
+        check(lib().lbg_batch_witness_download(self._h, i, ptr(out), len(out)))
+        return out
+
+    def use_graphs(self, enable=True):
+        check(lib().lbg_batch_use_graphs(self._h, int(enable)))
+
+    def autotune(self):
+        c, f = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().lbg_batch_autotune(self._h, ctypes.byref(c), ctypes.byref(f)))
+        return {"commit_chunks": c.value, "fold_columns_per_split": f.value}
+
+    def commit(self) -> List[InstanceRound]:
+        C, L = self.total_cols, self.limbs
+        out = [InstanceRound() for _ in range(self.count)]
+        if self.dropped:
+            top = np.zeros(C * N, np.uint16)
+            dig = np.zeros((max(L - 1, 1), C * N), np.uint16)
+            check(lib().lbg_batch_commit(self._h, None, ptr(top), ptr(dig)))
+            for i in range(self.count):
+                a, b = self.col_off[i] * N, self.col_off[i + 1] * N
+                out[i].top, out[i].digits = top[a:b].copy(), dig[: L - 1, a:b].copy()
+        else:
+            m = np.zeros((C, 4, L, N162), np.int16)
+            check(lib().lbg_batch_commit(self._h, ptr(m), None, None))
+            for i in range(self.count):
+                out[i].matrix = m[self.col_off[i]:self.col_off[i + 1]].copy()
+        return out
+
+    def commit_device(self):
+        """The commit stage with the results left on the device (for timing)."""
+        check(lib().lbg_batch_commit(self._h, None, None, None))
+
+    def row_evaluate(self, p0s) -> List[np.ndarray]:
+        p0 = np.ascontiguousarray(np.stack([np.asarray(p, np.uint64) for p in p0s]))
+        u = np.zeros((self.total_cols, 3), np.uint64)
+        check(lib().lbg_batch_row_evaluate(self._h, ptr(p0), ptr(u)))
+        return [u[self.col_off[i]:self.col_off[i + 1]].copy() for i in range(self.count)]
+
+    def mle_evaluate(self, p0s, p1s) -> List[np.ndarray]:
+        p0 = np.ascontiguousarray(np.stack([np.asarray(p, np.uint64) for p in p0s]))
+        p1 = np.ascontiguousarray(np.concatenate([np.asarray(p, np.uint64).reshape(-1, 3) for p in p1s]))
+        out = np.zeros((self.count, 3), np.uint64)
+        check(lib().lbg_batch_mle_evaluate(self._h, ptr(p0), ptr(p1), ptr(out)))
+        return [out[i].copy() for i in range(self.count)]
+
+    def fold(self, challenges, read_back=True):
+        ch = np.ascontiguousarray(np.concatenate([np.asarray(c, _CH) for c in challenges]), dtype=_CH)
+        v = np.zeros((self.count, self.len_ring, N), np.int16) if read_back else None
+        check(lib().lbg_batch_fold(self._h, ptr(ch), len(ch), ptr(v)))
+        return [v[i] for i in range(self.count)] if read_back else None
+
+    def round(self, domain=b"labinius/reference") -> List[InstanceRound]:
+        """commit -> per instance: evaluation point -> row and mle evaluation -> per instance: folding
+        challenges -> fold; the host steps in the library's host code, instance by instance."""
+        rounds = self.commit()
+        seed = np.frombuffer(self.pp.matrix_seed, np.uint8).copy()
+        d = np.frombuffer(domain, np.uint8).copy()
+        ts = []
+        for i, r in enumerate(rounds):
+            pn = self.params_of(i).native()
+            t = lib().lbg_transcript_new(ptr(d), len(domain))
+            ts.append(t)
+            r.p0 = np.zeros((self.row_log, 3), np.uint64)
+            r.p1 = np.zeros((self.column_log_lens[i], 3), np.uint64)
+            if self.dropped:
+                dig = r.digits if self.limbs > 1 else np.zeros(1, np.uint16)
+                check(lib().lbg_params_derive_evaluation_point(ctypes.byref(pn), ptr(seed), t, None, ptr(r.top),
+                                                               ptr(np.ascontiguousarray(dig)), ptr(r.p0), ptr(r.p1)))
+            else:
+                check(lib().lbg_params_derive_evaluation_point(ctypes.byref(pn), ptr(seed), t, ptr(r.matrix), None,
+                                                               None, ptr(r.p0), ptr(r.p1)))
+        mles = self.mle_evaluate([r.p0 for r in rounds], [r.p1 for r in rounds])
+        us = self.row_evaluate([r.p0 for r in rounds])
+        for i, r in enumerate(rounds):
+            r.mle, r.u = mles[i], us[i]
+            pn = self.params_of(i).native()
+            r.challenges = np.zeros(self.cols[i], _CH)
+            check(lib().lbg_params_derive_folding_challenges(ctypes.byref(pn), ts[i], ptr(r.u), ptr(r.challenges)))
+            lib().lbg_transcript_free(ts[i])
+        vs = self.fold([r.challenges for r in rounds])
+        for i, r in enumerate(rounds):
+            r.v = vs[i]
+        return rounds
+
+    def launch_count(self) -> int:
+        return int(lib().lbg_batch_launch_count(self._h))
+
+    def stream(self):
+        return lib().lbg_batch_stream(self._h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and nat._lib is not None:
+            nat._lib.lbg_batch_free(h)
+            self._h = None

@@ -11,6 +11,7 @@
 #include "../../include/labinius_gpu.h"
 #include "prime_structs.h"
 #include "error.h"
+#include "handles.h"
 #include "launch.h"
 #include "ring_tables.h"
 #include "transcript.h"
@@ -45,110 +46,6 @@ void set_last_error(const std::string& msg) { g_err = msg; }
     }                                                                                   \
   } while (0)
 
-struct lbg_pp {
-  lbg_params params;
-  int limbs = 0;
-  uint32_t primes[7];
-  int pidx[7];
-  size_t cols = 0, wdim = 0, len_ring = 0, n = 0;
-  uint8_t seed[32];
-  uint64_t key_seed = 0;
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int16_t* d_A = nullptr;     // [limbs][len_ring][648]
-  int4* d_Ahat = nullptr;     // [limbs][len_ring][162][2]
-  DevPrime* d_prime[7] = {nullptr};
-  uint64_t* d_jumps = nullptr;
-  std::mutex mu;              // guards the scratch below (Witness::row_evaluate takes &self)
-  uint64_t* d_eq = nullptr;   // [wdim][3]
-  uint64_t* d_p = nullptr;    // point coordinates
-  uint64_t* d_u = nullptr;    // [cols][3]
-  uint64_t* d_out = nullptr;  // [3]
-  int16_t* d_C = nullptr;     // fold_commitment input [cols][4][limbs][162]
-  lbg_challenge_d* d_ch = nullptr;
-  uint32_t* d_chat = nullptr;  // [cols][162]
-  int16_t* d_fc = nullptr;     // [4][limbs][162]
-};
-
-struct lbg_witness {
-  std::atomic<int> refs{1};
-  uint64_t* d = nullptr;
-  size_t n = 0;
-  int device = 0;
-};
-
-struct lbg_prover {
-  const lbg_pp* pp = nullptr;
-  cudaStream_t stream = nullptr;
-  int chunk = 0, nchunks = 0;
-  int fold_cols_per_split = 0;
-  int32_t* d_partial = nullptr;
-  uint32_t* d_vhat = nullptr;  // [wdim][162]
-  lbg_challenge_d* d_ch = nullptr;
-  uint32_t* d_chat = nullptr;
-  int16_t* d_v = nullptr;     // [len_ring][648]
-  uint16_t* d_res = nullptr;  // [limbs][cols*648]
-  std::mutex mu;
-  std::vector<struct OpeningBufs*> spare;
-  // kernel accounting
-  uint64_t launches = 0;
-  bool profiling = false;
-  struct Mark {
-    const char* name;
-    cudaEvent_t a, b;
-  };
-  std::vector<Mark> marks;
-  std::vector<cudaEvent_t> event_pool;
-};
-
-// Brackets one launch of the prover with events when profiling is on, and counts it.
-struct KernelScope {
-  lbg_prover* pr;
-  const char* name;
-  cudaEvent_t a = nullptr, b = nullptr;
-  static cudaEvent_t take(lbg_prover* pr) {
-    if (!pr->event_pool.empty()) {
-      cudaEvent_t e = pr->event_pool.back();
-      pr->event_pool.pop_back();
-      return e;
-    }
-    cudaEvent_t e = nullptr;
-    cudaEventCreate(&e);
-    return e;
-  }
-  KernelScope(lbg_prover* p, const char* n, int kernels = 1) : pr(p), name(n) {
-    pr->launches += kernels;
-    if (pr->profiling) {
-      a = take(pr);
-      b = take(pr);
-      cudaEventRecord(a, pr->stream);
-    }
-  }
-  ~KernelScope() {
-    if (a) {
-      cudaEventRecord(b, pr->stream);
-      pr->marks.push_back({name, a, b});
-    }
-  }
-};
-
-struct OpeningBufs {
-  int16_t* d_C = nullptr;       // [cols][4][limbs][162]
-  uint16_t* d_top = nullptr;    // [cols*648]
-  uint16_t* d_digits = nullptr; // [limbs-1][cols*648]
-};
-
-struct lbg_opening {
-  lbg_prover* pr = nullptr;
-  lbg_witness* w = nullptr;
-  OpeningBufs* bufs = nullptr;
-};
-
-struct lbg_transcript {
-  Transcript t;
-  explicit lbg_transcript(const uint8_t* d, size_t n) : t(d, n) {}
-};
-
 static void witness_release(lbg_witness* w) {
   if (w && w->refs.fetch_sub(1) == 1) {
     cudaSetDevice(w->device);
@@ -156,6 +53,7 @@ static void witness_release(lbg_witness* w) {
     delete w;
   }
 }
+void lbg_witness_release_internal(lbg_witness* w) { witness_release(w); }
 
 extern "C" {
 

@@ -1,0 +1,447 @@
+// Batched rounds: many independent witnesses under one key, every stage one launch over all of
+// them, stages replayed as CUDA graphs, grid schedule autotuned per batch shape.
+//
+// All instances share the public parameters' key, so they share its column length (wdim F162)
+// and moduli; they differ in their column counts (2^column_log_len_i). Instance i's columns follow
+// instance i-1's in one device witness buffer, which makes the batched commit the single-instance
+// commit kernel over the concatenated columns (a column's commitment depends on that column and
+// the key only, crates/pcs/src/key.rs:174-191), and the batched fold the single-instance fold with
+// every column split mapped to its instance.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/labinius_gpu.h"
+#include "error.h"
+#include "handles.h"
+#include "launch.h"
+#include "ring_tables.h"
+
+using namespace lbg;
+
+namespace {
+int fail(int code, const std::string& m) {
+  set_last_error(m);
+  return code;
+}
+}  // namespace
+
+#define LBG_BCU(x)                                                                      \
+  do {                                                                                  \
+    cudaError_t e_ = (x);                                                               \
+    if (e_ != cudaSuccess) return fail(LBG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct lbg_batch {
+  const lbg_pp* pp = nullptr;
+  int count = 0;
+  std::vector<uint32_t> col_log;
+  std::vector<size_t> col_off;  // first column of each instance, plus the total at the end
+  size_t total_cols = 0;
+  size_t wdim = 0, len_ring = 0;
+  int min_col_log = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t* d_w = nullptr;        // [total_cols * wdim][3]
+  int* d_col_inst = nullptr;      // [total_cols]
+  int* d_split_inst = nullptr;    // [total_cols] (at most one split per column)
+  int chunk = 0, nchunks = 0, fold_per = 0;
+  int32_t* d_partial = nullptr;   // [max_chunks][total_cols][162][4]
+  int max_chunks = 0;
+  int16_t* d_C = nullptr;         // [total_cols][4][limbs][162]
+  uint16_t* d_res = nullptr;      // [limbs][total_cols*648]
+  uint16_t* d_top = nullptr;
+  uint16_t* d_digits = nullptr;
+  uint64_t* d_p0 = nullptr;       // [count][row_log][3]
+  uint64_t* d_p1 = nullptr;       // [count][32][3]
+  uint64_t* d_eq = nullptr;       // [count][wdim][3]
+  uint64_t* d_u = nullptr;        // [total_cols][3]
+  uint64_t* d_claim = nullptr;    // [count][3]
+  lbg_challenge_d* d_ch = nullptr;
+  uint32_t* d_chat = nullptr;     // [total_cols][162]
+  uint32_t* d_vhat = nullptr;     // [count][wdim][162]
+  int16_t* d_v = nullptr;         // [count][len_ring][648]
+  bool graphs = false;
+  cudaGraphExec_t g_commit = nullptr, g_fold = nullptr;
+  uint64_t launches = 0;
+};
+
+static void free_graphs(lbg_batch* b) {
+  if (b->g_commit) cudaGraphExecDestroy(b->g_commit);
+  if (b->g_fold) cudaGraphExecDestroy(b->g_fold);
+  b->g_commit = b->g_fold = nullptr;
+}
+
+// The device work of each stage, enqueued on the batch's stream (also what the graphs capture).
+static cudaError_t enqueue_commit(lbg_batch* b) {
+  const lbg_pp* pp = b->pp;
+  int L = pp->limbs, cols = (int)b->total_cols;
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < L && e == cudaSuccess; k++) {
+    e = launch_commit(pp->pidx[k], b->d_w, b->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2, pp->d_prime[k],
+                      cols, (int)b->len_ring, b->chunk, b->nchunks, b->d_partial, b->stream);
+    if (e == cudaSuccess)
+      e = launch_commit_finish(pp->pidx[k], b->d_partial, b->nchunks, cols, pp->d_prime[k], k, L, b->d_C, b->stream);
+  }
+  b->launches += 2 * L;
+  if (e == cudaSuccess && pp->params.opening == LBG_OPENING_BIT_DROPPED) {
+    size_t count = b->total_cols * N648;
+    for (int k = 0; k < L && e == cudaSuccess; k++)
+      e = launch_column_residues(pp->pidx[k], b->d_C, cols, k, L, pp->d_prime[k], b->d_res + (size_t)k * count,
+                                 b->stream);
+    GarnerConsts g;
+    std::memset(&g, 0, sizeof(g));
+    for (int k = 0; k < L; k++) {
+      g.q[k] = pp->primes[k];
+      for (int m = 0; m < k; m++) g.inv[k][m] = (uint32_t)inv_mod(pp->primes[m], pp->primes[k]);
+    }
+    g.dropped_bits = pp->params.dropped_bits;
+    if (e == cudaSuccess) e = launch_garner(b->d_res, count, L, g, b->d_top, b->d_digits, b->stream);
+    b->launches += L + 1;
+  }
+  return e;
+}
+
+static cudaError_t enqueue_fold(lbg_batch* b) {
+  const lbg_pp* pp = b->pp;
+  cudaError_t e = launch_challenge_slots(pp->pidx[0], b->d_ch, (int)b->total_cols, pp->d_prime[0], b->d_chat, b->stream);
+  if (e == cudaSuccess)
+    e = launch_fold(pp->pidx[0], b->d_w, b->wdim, (int)b->total_cols, b->fold_per, b->d_chat, pp->d_prime[0],
+                    b->d_vhat, b->d_v, b->stream, b->count, b->d_split_inst);
+  b->launches += 3;
+  return e;
+}
+
+// The split -> instance map for fold splits of `per` columns (per divides every column count).
+static int upload_splits(lbg_batch* b, int per) {
+  std::vector<int> inst(b->total_cols / per);
+  for (int i = 0; i < b->count; i++)
+    for (size_t c = b->col_off[i]; c < b->col_off[i + 1]; c += per) inst[c / per] = i;
+  LBG_BCU(cudaMemcpy(b->d_split_inst, inst.data(), inst.size() * sizeof(int), cudaMemcpyHostToDevice));
+  b->fold_per = per;
+  return LBG_OK;
+}
+
+static void set_chunks(lbg_batch* b, int nch) {
+  int step = commit_ring_per_step();
+  int chunk = (int)((b->len_ring + nch - 1) / nch);
+  chunk = (chunk + step - 1) / step * step;
+  b->chunk = chunk;
+  b->nchunks = (int)((b->len_ring + chunk - 1) / chunk);
+}
+
+// Time one enqueue (median of three) on the batch's stream.
+template <class F>
+static float time_stage(lbg_batch* b, F enqueue) {
+  cudaEvent_t a, c;
+  cudaEventCreate(&a);
+  cudaEventCreate(&c);
+  std::vector<float> ts;
+  enqueue(b);  // warm
+  for (int r = 0; r < 3; r++) {
+    cudaEventRecord(a, b->stream);
+    enqueue(b);
+    cudaEventRecord(c, b->stream);
+    cudaEventSynchronize(c);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, c);
+    ts.push_back(ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(c);
+  std::sort(ts.begin(), ts.end());
+  return ts[1];
+}
+
+extern "C" {
+
+void lbg_batch_free(lbg_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->pp->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  free_graphs(b);
+  void* ptrs[] = {b->d_w, b->d_col_inst, b->d_split_inst, b->d_partial, b->d_C, b->d_res, b->d_top, b->d_digits,
+                  b->d_p0, b->d_p1, b->d_eq, b->d_u, b->d_claim, b->d_ch, b->d_chat, b->d_vhat, b->d_v};
+  for (void* p : ptrs) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int lbg_batch_new(const lbg_pp* pp, const uint32_t* column_log_lens, size_t count, lbg_batch** out) {
+  if (!pp || !column_log_lens || !out || count == 0) return fail(LBG_ERR_INVALID, "null argument or empty batch");
+  *out = nullptr;
+  if (count > 65536) return fail(LBG_ERR_INVALID, "at most 65536 instances");
+  uint32_t row_log = pp->params.witness_log_len - pp->params.column_log_len;
+  lbg_batch* b = new lbg_batch();
+  b->pp = pp;
+  b->count = (int)count;
+  b->wdim = pp->wdim;
+  b->len_ring = pp->len_ring;
+  b->col_off.push_back(0);
+  b->min_col_log = 31;
+  for (size_t i = 0; i < count; i++) {
+    uint32_t cl = column_log_lens[i];
+    if (cl < 1 || cl + row_log > 30) {
+      delete b;
+      return fail(LBG_ERR_PARAMS, "instance " + std::to_string(i) + ": column_log_len out of range");
+    }
+    b->col_log.push_back(cl);
+    b->min_col_log = std::min(b->min_col_log, (int)cl);
+    b->col_off.push_back(b->col_off.back() + ((size_t)1 << cl));
+  }
+  b->total_cols = b->col_off.back();
+  if (b->total_cols > (1u << 30) / b->wdim) {
+    delete b;
+    return fail(LBG_ERR_PARAMS, "batch too large");
+  }
+  auto bail = [&](int code) {
+    lbg_batch_free(b);
+    return code;
+  };
+  if (cudaSetDevice(pp->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(LBG_ERR_CUDA, "stream"));
+  int L = pp->limbs;
+  size_t C = b->total_cols, n = C * b->wdim, count648 = C * N648;
+  b->max_chunks = (int)((b->len_ring + commit_ring_per_step() - 1) / commit_ring_per_step());
+  if (b->max_chunks > 64) b->max_chunks = 64;
+  bool ok = cudaMalloc((void**)&b->d_w, n * 24) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_col_inst, C * sizeof(int)) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_split_inst, C * sizeof(int)) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_partial, (size_t)b->max_chunks * C * N162 * 16) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_C, C * 4 * L * N162 * 2) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_res, (size_t)L * count648 * 2) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_top, count648 * 2) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_digits, (size_t)(L > 1 ? L - 1 : 1) * count648 * 2) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_p0, count * 32 * 24) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_p1, count * 32 * 24) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_eq, count * b->wdim * 24) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_u, C * 24) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_claim, count * 24) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_ch, C * sizeof(lbg_challenge_d)) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_chat, C * N162 * 4) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_vhat, count * b->wdim * N162 * 4) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_v, count * b->len_ring * N648 * 2) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    return bail(fail(LBG_ERR_OOM, "batch: device allocation failed"));
+  }
+  std::vector<int> ci(C);
+  for (int i = 0; i < b->count; i++)
+    for (size_t c = b->col_off[i]; c < b->col_off[i + 1]; c++) ci[c] = i;
+  if (cudaMemcpy(b->d_col_inst, ci.data(), C * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(fail(LBG_ERR_CUDA, "batch maps"));
+  if (cudaMemsetAsync(b->d_w, 0, n * 24, b->stream) != cudaSuccess ||
+      cudaMemsetAsync(b->d_ch, 0, C * sizeof(lbg_challenge_d), b->stream) != cudaSuccess)
+    return bail(fail(LBG_ERR_CUDA, "batch init"));
+  // model schedule (the autotuner refines it): chunks for about two waves, fold splits of 16
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pp->device);
+  long tiles = (long)((C + commit_cols_per_cta() - 1) / commit_cols_per_cta());
+  int want = (int)std::max<long>(1, (2L * sms * commit_blocks_per_sm(pp->pidx[0]) + tiles - 1) / tiles);
+  set_chunks(b, std::min(want, b->max_chunks));
+  int rc = upload_splits(b, std::min(16, 1 << b->min_col_log));
+  if (rc) return bail(rc);
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bail(fail(LBG_ERR_CUDA, "batch init"));
+  *out = b;
+  return LBG_OK;
+}
+
+size_t lbg_batch_columns(const lbg_batch* b) { return b ? b->total_cols : 0; }
+
+int lbg_batch_witness_random(lbg_batch* b, const uint8_t* seeds) {
+  if (!b || !seeds) return fail(LBG_ERR_INVALID, "null argument");
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  for (int i = 0; i < b->count; i++) {
+    XofRoot root;
+    const uint8_t* s = seeds + 32 * i;
+    for (int w = 0; w < 8; w++)
+      root.cv[w] = (uint32_t)s[4 * w] | ((uint32_t)s[4 * w + 1] << 8) | ((uint32_t)s[4 * w + 2] << 16) |
+                   ((uint32_t)s[4 * w + 3] << 24);
+    uint8_t msg[64] = {0};
+    std::memcpy(msg, "labinius/witness", 16);
+    for (int w = 0; w < 16; w++)
+      root.m[w] = (uint32_t)msg[4 * w] | ((uint32_t)msg[4 * w + 1] << 8) | ((uint32_t)msg[4 * w + 2] << 16) |
+                  ((uint32_t)msg[4 * w + 3] << 24);
+    root.block_len = 16;
+    root.flags = 16 | 1 | 2 | 8;
+    size_t n = (b->col_off[i + 1] - b->col_off[i]) * b->wdim;
+    uint64_t* dst = b->d_w + b->col_off[i] * b->wdim * 3;
+    LBG_BCU(launch_xof(root, n * 24, (uint8_t*)dst, b->stream));
+    LBG_BCU(launch_mask_f162(dst, n, b->stream));
+  }
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  return LBG_OK;
+}
+
+int lbg_batch_witness_upload(lbg_batch* b, size_t instance, const uint64_t* f162, size_t n) {
+  if (!b || !f162) return fail(LBG_ERR_INVALID, "null argument");
+  if (instance >= (size_t)b->count) return fail(LBG_ERR_INVALID, "instance out of range");
+  if (n != (b->col_off[instance + 1] - b->col_off[instance]) * b->wdim)
+    return fail(LBG_ERR_WITNESS, "the witness is not witness_len() elements");
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  LBG_BCU(cudaMemcpyAsync(b->d_w + b->col_off[instance] * b->wdim * 3, f162, n * 24, cudaMemcpyHostToDevice,
+                          b->stream));
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  return LBG_OK;
+}
+
+int lbg_batch_witness_download(const lbg_batch* b, size_t instance, uint64_t* out, size_t n) {
+  if (!b || !out) return fail(LBG_ERR_INVALID, "null argument");
+  if (instance >= (size_t)b->count) return fail(LBG_ERR_INVALID, "instance out of range");
+  if (n != (b->col_off[instance + 1] - b->col_off[instance]) * b->wdim) return fail(LBG_ERR_INVALID, "length mismatch");
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  LBG_BCU(cudaMemcpy(out, b->d_w + b->col_off[instance] * b->wdim * 3, n * 24, cudaMemcpyDeviceToHost));
+  return LBG_OK;
+}
+
+// CUDA graphs of the two device stages; rebuilt after the autotuner changes the schedule.
+int lbg_batch_use_graphs(lbg_batch* b, int enable) {
+  if (!b) return fail(LBG_ERR_INVALID, "null batch");
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  free_graphs(b);
+  b->graphs = false;
+  if (!enable) return LBG_OK;
+  cudaGraph_t g = nullptr;
+  uint64_t before = b->launches;
+  LBG_BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = enqueue_commit(b);
+  cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) return fail(LBG_ERR_CUDA, "graph capture (commit)");
+  e = cudaGraphInstantiate(&b->g_commit, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(LBG_ERR_CUDA, "graph instantiate (commit)");
+  LBG_BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  e = enqueue_fold(b);
+  e2 = cudaStreamEndCapture(b->stream, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) return fail(LBG_ERR_CUDA, "graph capture (fold)");
+  e = cudaGraphInstantiate(&b->g_fold, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(LBG_ERR_CUDA, "graph instantiate (fold)");
+  b->launches = before;  // capture launched nothing
+  b->graphs = true;
+  return LBG_OK;
+}
+
+// The autotuner: time candidate schedules of both stages on this batch's shape and keep the
+// fastest (commit: ring-element chunks per column tile; fold: columns per split).
+int lbg_batch_autotune(lbg_batch* b, uint32_t* chunks_out, uint32_t* fold_cols_out) {
+  if (!b) return fail(LBG_ERR_INVALID, "null batch");
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  bool had = b->graphs;
+  if (had) lbg_batch_use_graphs(b, 0);
+  uint64_t launches = b->launches;
+  std::vector<int> cand;
+  for (int c = 1; c <= b->max_chunks; c *= 2) cand.push_back(c);
+  for (int c = 3; c <= b->max_chunks; c *= 2) cand.push_back(c);
+  float best = -1;
+  int best_c = b->nchunks;
+  for (int c : cand) {
+    set_chunks(b, c);
+    float t = time_stage(b, enqueue_commit);
+    if (best < 0 || t < best) {
+      best = t;
+      best_c = c;
+    }
+  }
+  set_chunks(b, best_c);
+  best = -1;
+  int best_p = b->fold_per;
+  for (int per = 8; per <= std::min(256, 1 << b->min_col_log); per *= 2) {
+    if (upload_splits(b, per)) return LBG_ERR_CUDA;
+    float t = time_stage(b, enqueue_fold);
+    if (best < 0 || t < best) {
+      best = t;
+      best_p = per;
+    }
+  }
+  if (1 << b->min_col_log < 8) best_p = 1 << b->min_col_log;
+  int rc = upload_splits(b, best_p);
+  if (rc) return rc;
+  b->launches = launches;
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  if (chunks_out) *chunks_out = (uint32_t)b->nchunks;
+  if (fold_cols_out) *fold_cols_out = (uint32_t)b->fold_per;
+  if (had) return lbg_batch_use_graphs(b, 1);
+  return LBG_OK;
+}
+
+int lbg_batch_commit(lbg_batch* b, int16_t* matrix_out, uint16_t* top_out, uint16_t* digits_out) {
+  if (!b) return fail(LBG_ERR_INVALID, "null batch");
+  const lbg_pp* pp = b->pp;
+  LBG_BCU(cudaSetDevice(pp->device));
+  if (b->graphs) {
+    LBG_BCU(cudaGraphLaunch(b->g_commit, b->stream));
+    b->launches += 2 * pp->limbs + (pp->params.opening == LBG_OPENING_BIT_DROPPED ? pp->limbs + 1 : 0);
+  } else {
+    LBG_BCU(enqueue_commit(b));
+  }
+  size_t C = b->total_cols, count = C * N648;
+  int L = pp->limbs;
+  if (matrix_out) LBG_BCU(cudaMemcpyAsync(matrix_out, b->d_C, C * 4 * L * N162 * 2, cudaMemcpyDeviceToHost, b->stream));
+  if (top_out) LBG_BCU(cudaMemcpyAsync(top_out, b->d_top, count * 2, cudaMemcpyDeviceToHost, b->stream));
+  if (digits_out && L > 1)
+    LBG_BCU(cudaMemcpyAsync(digits_out, b->d_digits, (size_t)(L - 1) * count * 2, cudaMemcpyDeviceToHost, b->stream));
+  if (matrix_out || top_out || digits_out) LBG_BCU(cudaStreamSynchronize(b->stream));
+  return LBG_OK;
+}
+
+int lbg_batch_row_evaluate(lbg_batch* b, const uint64_t* p0, uint64_t* u_out) {
+  if (!b || !p0 || !u_out) return fail(LBG_ERR_INVALID, "null argument");
+  int row_log = (int)(b->pp->params.witness_log_len - b->pp->params.column_log_len);
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  LBG_BCU(cudaMemcpyAsync(b->d_p0, p0, (size_t)b->count * row_log * 24, cudaMemcpyHostToDevice, b->stream));
+  LBG_BCU(launch_eq_table(b->d_p0, row_log, b->wdim, b->d_eq, b->stream, b->count));
+  LBG_BCU(launch_row_eval(b->d_w, b->wdim, (int)b->total_cols, b->d_eq, b->d_u, b->stream, b->d_col_inst));
+  b->launches += 2;
+  LBG_BCU(cudaMemcpyAsync(u_out, b->d_u, b->total_cols * 24, cudaMemcpyDeviceToHost, b->stream));
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  return LBG_OK;
+}
+
+// claims: p1 of instance i is column_log_len_i F162 at p1 + 3 * sum_{l<i} column_log_len_l.
+int lbg_batch_mle_evaluate(lbg_batch* b, const uint64_t* p0, const uint64_t* p1, uint64_t* out) {
+  if (!b || !p0 || !p1 || !out) return fail(LBG_ERR_INVALID, "null argument");
+  int row_log = (int)(b->pp->params.witness_log_len - b->pp->params.column_log_len);
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  LBG_BCU(cudaMemcpyAsync(b->d_p0, p0, (size_t)b->count * row_log * 24, cudaMemcpyHostToDevice, b->stream));
+  LBG_BCU(launch_eq_table(b->d_p0, row_log, b->wdim, b->d_eq, b->stream, b->count));
+  LBG_BCU(launch_row_eval(b->d_w, b->wdim, (int)b->total_cols, b->d_eq, b->d_u, b->stream, b->d_col_inst));
+  size_t off = 0;
+  for (int i = 0; i < b->count; i++) {
+    int cl = (int)b->col_log[i];
+    LBG_BCU(cudaMemcpyAsync(b->d_p1 + 3 * 32 * i, p1 + 3 * off, cl * 24, cudaMemcpyHostToDevice, b->stream));
+    LBG_BCU(launch_claim(b->d_u + 3 * b->col_off[i], 1 << cl, b->d_p1 + 3 * 32 * i, cl, b->d_claim + 3 * i, b->stream));
+    off += cl;
+  }
+  b->launches += 2 + b->count;
+  LBG_BCU(cudaMemcpyAsync(out, b->d_claim, (size_t)b->count * 24, cudaMemcpyDeviceToHost, b->stream));
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  return LBG_OK;
+}
+
+int lbg_batch_fold(lbg_batch* b, const lbg_challenge* challenges, size_t r, int16_t* v_out) {
+  if (!b || !challenges) return fail(LBG_ERR_INVALID, "null argument");
+  if (r != b->total_cols) return fail(LBG_ERR_INVALID, "one challenge per column");
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  LBG_BCU(cudaMemcpyAsync(b->d_ch, challenges, r * sizeof(lbg_challenge), cudaMemcpyHostToDevice, b->stream));
+  if (b->graphs) {
+    LBG_BCU(cudaGraphLaunch(b->g_fold, b->stream));
+    b->launches += 3;
+  } else {
+    LBG_BCU(enqueue_fold(b));
+  }
+  if (v_out) {
+    LBG_BCU(cudaMemcpyAsync(v_out, b->d_v, (size_t)b->count * b->len_ring * N648 * 2, cudaMemcpyDeviceToHost,
+                            b->stream));
+    LBG_BCU(cudaStreamSynchronize(b->stream));
+  }
+  return LBG_OK;
+}
+
+void* lbg_batch_stream(const lbg_batch* b) { return b ? (void*)b->stream : nullptr; }
+uint64_t lbg_batch_launch_count(const lbg_batch* b) { return b ? b->launches : 0; }
+
+}  // extern "C"

@@ -281,7 +281,7 @@ template <int PI, bool DIRECT>
 __global__ void __launch_bounds__(256, 2)
     k_fold(const uint64_t* __restrict__ W, size_t wdim, int cols, int cols_per_split,
            const uint32_t* __restrict__ chat, const DevPrime* __restrict__ D, uint32_t* __restrict__ vhat,
-           int16_t* __restrict__ v_out) {
+           int16_t* __restrict__ v_out, const int* __restrict__ split_inst) {
   extern __shared__ __align__(16) uint8_t smem[];
   uint16_t* lut = (uint16_t*)smem;
   uint16_t* wt = (uint16_t*)(smem + LUT_BYTES);  // FJ * 162 * FP u16
@@ -329,6 +329,8 @@ __global__ void __launch_bounds__(256, 2)
   }
   if (!DIRECT) {
     const size_t p = p0 + lane;
+    // many instances: split s belongs to instance split_inst[s], whose sums start at inst * wdim
+    if (split_inst) vhat += (size_t)split_inst[blockIdx.y] * wdim * N162;
     if (p < wdim) {
 #pragma unroll
       for (int u = 0; u < VPW; u++) {
@@ -435,9 +437,14 @@ __global__ void k_garner(const uint16_t* __restrict__ res, size_t count, int lim
 // Row evaluation over F162 (crates/pcs/src/eval.rs:51-63, 171-193)
 // =============================================================================================
 // eq(p, i) = prod_k (p_k if bit k of i else 1 + p_k).
-__global__ void k_eq_table(const uint64_t* __restrict__ p, int n, size_t count, uint64_t* __restrict__ eq) {
-  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
+__global__ void k_eq_table(const uint64_t* __restrict__ p, int n, size_t count, int instances,
+                           uint64_t* __restrict__ eq) {
+  size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= count * (size_t)instances) return;
+  // instances one after another: instance g / count's table from its own point
+  size_t inst = g / count, i = g % count;
+  p += inst * (size_t)n * 3;
+  eq += inst * count * 3;
   F162d x{{1, 0, 0}};
   for (int k = 0; k < n; k++) {
     F162d pk{{p[3 * k], p[3 * k + 1], p[3 * k + 2]}};
@@ -452,10 +459,12 @@ __global__ void k_eq_table(const uint64_t* __restrict__ p, int n, size_t count, 
 // One CTA per column: thread b < 162 accumulates S_b = sum over rows i with bit b of W[i] set of
 // eq[i]; then u = sum_b x^b S_b reduced modulo x^162 + x^81 + 1.
 __global__ void __launch_bounds__(192) k_row_eval(const uint64_t* __restrict__ W, size_t wdim,
-                                                  const uint64_t* __restrict__ eq, uint64_t* __restrict__ u) {
+                                                  const uint64_t* __restrict__ eq, uint64_t* __restrict__ u,
+                                                  const int* __restrict__ col_inst) {
   __shared__ uint64_t S[N162][3];
   const int b = threadIdx.x;
   const int j = blockIdx.x;
+  if (col_inst) eq += (size_t)col_inst[j] * wdim * 3;  // many instances: each column its own eq table
   const uint64_t* col = W + (size_t)j * wdim * 3;
   uint64_t a0 = 0, a1 = 0, a2 = 0;
   if (b < N162) {
@@ -699,25 +708,28 @@ int fold_blocks_per_sm(int pi) {
 }
 
 cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
-                        const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st) {
+                        const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st, int instances,
+                        const int* split_inst) {
   size_t smem = fold_smem_bytes();
   if (!vhat) {  // direct mode: one split, no scratch beyond chat
     dim3 grid(blocks_for(wdim, FP), 1);
     LBG_DISPATCH(pi, ({
                    cudaFuncSetAttribute(k_fold<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                   k_fold<P, true><<<grid, 256, smem, st>>>(W, wdim, cols, cols, chat, D, nullptr, v);
+                   k_fold<P, true><<<grid, 256, smem, st>>>(W, wdim, cols, cols, chat, D, nullptr, v, nullptr);
                  }));
     return cudaGetLastError();
   }
   int splits = (cols + cols_per_split - 1) / cols_per_split;
   if (splits < 1 || splits > 65535) return cudaErrorInvalidValue;
   dim3 grid(blocks_for(wdim, FP), splits);
-  cudaError_t e = cudaMemsetAsync(vhat, 0, wdim * N162 * sizeof(uint32_t), st);
+  size_t positions = wdim * (size_t)instances;  // instances laid out one after another
+  cudaError_t e = cudaMemsetAsync(vhat, 0, positions * N162 * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   LBG_DISPATCH(pi, ({
                  cudaFuncSetAttribute(k_fold<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                 k_fold<P, false><<<grid, 256, smem, st>>>(W, wdim, cols, cols_per_split, chat, D, vhat, nullptr);
-                 k_fold_finish<P><<<blocks_for(wdim, 64), 64, 0, st>>>(vhat, wdim, D, v);
+                 k_fold<P, false><<<grid, 256, smem, st>>>(W, wdim, cols, cols_per_split, chat, D, vhat, nullptr,
+                                                          split_inst);
+                 k_fold_finish<P><<<blocks_for(positions, 64), 64, 0, st>>>(vhat, positions, D, v);
                }));
   return cudaGetLastError();
 }
@@ -741,14 +753,14 @@ cudaError_t launch_garner(const uint16_t* res, size_t count, int limbs, const Ga
   return cudaGetLastError();
 }
 
-cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq, cudaStream_t st) {
-  k_eq_table<<<blocks_for(count, 128), 128, 0, st>>>(p, n, count, eq);
+cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq, cudaStream_t st, int instances) {
+  k_eq_table<<<blocks_for(count * instances, 128), 128, 0, st>>>(p, n, count, instances, eq);
   return cudaGetLastError();
 }
 
 cudaError_t launch_row_eval(const uint64_t* W, size_t wdim, int cols, const uint64_t* eq, uint64_t* u,
-                            cudaStream_t st) {
-  k_row_eval<<<cols, 192, 0, st>>>(W, wdim, eq, u);
+                            cudaStream_t st, const int* col_inst) {
+  k_row_eval<<<cols, 192, 0, st>>>(W, wdim, eq, u, col_inst);
   return cudaGetLastError();
 }
 

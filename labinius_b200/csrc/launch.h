@@ -52,17 +52,21 @@ int fold_blocks_per_sm(int pi);
 // The fold over all columns: k_fold accumulates column splits of cols_per_split columns into vhat
 // (u32 [wdim][162], zeroed here), then k_fold_finish inverts and centres into v. With vhat null
 // the fold runs in one pass over all columns, each CTA inverting its own positions.
+// Many instances of the same column length (instances > 1): their columns one after another, each
+// split within one instance (split_inst[s] its instance), vhat and v one instance after another.
 cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
-                        const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st);
+                        const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st, int instances = 1,
+                        const int* split_inst = nullptr);
 cudaError_t launch_fold_commitment(int pi, const int16_t* C, int cols, int limb, int limbs, const uint32_t* chat,
                                    const DevPrime* D, int16_t* out, cudaStream_t st);
 cudaError_t launch_column_residues(int pi, const int16_t* C, int cols, int limb, int limbs, const DevPrime* D,
                                    uint16_t* res, cudaStream_t st);
 cudaError_t launch_garner(const uint16_t* res, size_t count, int limbs, const GarnerConsts& g, uint16_t* top,
                           uint16_t* digits, cudaStream_t st);
-cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq, cudaStream_t st);
+cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq, cudaStream_t st,
+                            int instances = 1);
 cudaError_t launch_row_eval(const uint64_t* W, size_t wdim, int cols, const uint64_t* eq, uint64_t* u,
-                            cudaStream_t st);
+                            cudaStream_t st, const int* col_inst = nullptr);
 cudaError_t launch_claim(const uint64_t* u, int cols, const uint64_t* p1, int n, uint64_t* out, cudaStream_t st);
 cudaError_t launch_xof(const XofRoot& root, size_t nbytes, uint8_t* out, cudaStream_t st);
 cudaError_t launch_mask_f162(uint64_t* W, size_t n, cudaStream_t st);
