@@ -46,10 +46,68 @@ void set_last_error(const std::string& msg) { g_err = msg; }
     }                                                                                   \
   } while (0)
 
+// Released witness buffers are kept (a few per process) and handed to the next witness of the
+// same size, so a prover that commits new witnesses repeatedly does not pay cudaMalloc/cudaFree of
+// the whole witness every round (tens of ms for 100 MB), the device-side counterpart of the
+// reference's recycled workspace (crates/pcs/src/scheme/prover.rs:12-20).
+namespace {
+struct CachedBuf {
+  int device;
+  size_t bytes;
+  uint64_t* p;
+};
+std::mutex g_cache_mu;
+std::vector<CachedBuf> g_cache;
+constexpr size_t CACHE_ENTRIES = 4;
+}  // namespace
+
+static uint64_t* witness_buf_get(int device, size_t bytes) {
+  {
+    std::lock_guard<std::mutex> g(g_cache_mu);
+    for (size_t i = 0; i < g_cache.size(); i++)
+      if (g_cache[i].device == device && g_cache[i].bytes == bytes) {
+        uint64_t* p = g_cache[i].p;
+        g_cache.erase(g_cache.begin() + i);
+        return p;
+      }
+  }
+  uint64_t* p = nullptr;
+  if (cudaMalloc((void**)&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    // the cache may hold the memory this allocation needs: release it and retry once
+    std::vector<CachedBuf> drop;
+    {
+      std::lock_guard<std::mutex> g(g_cache_mu);
+      drop.swap(g_cache);
+    }
+    for (auto& c : drop) {
+      cudaSetDevice(c.device);
+      cudaFree(c.p);
+    }
+    cudaSetDevice(device);
+    if (cudaMalloc((void**)&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+  }
+  return p;
+}
+
+static void witness_buf_put(int device, size_t bytes, uint64_t* p) {
+  // no kernel of any stream may still read the buffer when it is handed out again
+  cudaSetDevice(device);
+  cudaDeviceSynchronize();
+  std::lock_guard<std::mutex> g(g_cache_mu);
+  if (g_cache.size() < CACHE_ENTRIES) {
+    g_cache.push_back({device, bytes, p});
+    return;
+  }
+  cudaFree(p);
+}
+
 static void witness_release(lbg_witness* w) {
   if (w && w->refs.fetch_sub(1) == 1) {
-    cudaSetDevice(w->device);
-    cudaFree(w->d);
+    witness_buf_put(w->device, w->n * 24, w->d);
     delete w;
   }
 }
@@ -226,8 +284,8 @@ static int witness_alloc(const lbg_pp* pp, size_t n, lbg_witness** out) {
   lbg_witness* w = new lbg_witness();
   w->n = n;
   w->device = pp->device;
-  if (cudaMalloc((void**)&w->d, n * 24) != cudaSuccess) {
-    cudaGetLastError();
+  w->d = witness_buf_get(pp->device, n * 24);
+  if (!w->d) {
     delete w;
     return fail(LBG_ERR_OOM, "witness: device allocation failed");
   }
