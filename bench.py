@@ -40,6 +40,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-instances", type=int, default=64)
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--served-requests", type=int, default=10000)
+    ap.add_argument("--served-plain-sample", type=int, default=200)
     return ap.parse_args()
 
 
@@ -208,6 +213,206 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------------------------------------
+# batched: 64 uneven witnesses under one key, against 64 sequential single-instance calls
+# ------------------------------------------------------------------------------------------------
+def run_batched(instances, steps, flush_bytes=256 << 20):
+    """Sizes log2 n ~ U[16, 22] (seeded, rounded), each instance Params(log n, max(1, log n - 11),
+    [3889, 9721]): column length 2048 F162 for all, so one key serves every instance. A step is the
+    batched commit + fold of all instances (graphs on, schedule autotuned), timed with CUDA events on
+    the batch's stream; the comparison is the same work as one single-instance commit + fold per
+    instance (device time summed over the calls, and wall clock around the loop)."""
+    import ctypes
+
+    import torch
+
+    import labinius_b200 as L
+    from labinius_b200._native import check, lib, ptr
+    from labinius_b200.batch import Batch
+
+    rng = np.random.default_rng(2026)
+    logs = np.rint(rng.uniform(16, 22, instances)).astype(int)
+    col_logs = [max(1, int(l) - 11) for l in logs]
+    seeds = [bytes([(0x21 + 7 * i) & 0xFF, i & 0xFF]) * 16 for i in range(instances)]
+    total = int(sum(1 << (11 + c) for c in col_logs))
+    pp = L.PublicParameters.from_seed(L.Params.new(11 + col_logs[0], col_logs[0], [L.Modulus.Q9721_FS_S]), MATRIX_SEED)
+    b = Batch(pp, col_logs)
+    b.witness_random(seeds)
+    tuned = b.autotune()
+    b.use_graphs(True)
+    rounds = b.round(DOMAIN)
+    chs = [r.challenges for r in rounds]
+    stream = torch.cuda.ExternalStream(b.stream())
+    flush = torch.empty(flush_bytes // 4, dtype=torch.int32, device="cuda")
+    for _ in range(2):
+        b.commit_device()
+        b.fold(chs, read_back=False)
+    torch.cuda.synchronize()
+    l0 = b.launch_count()
+    ms = 0.0
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.commit_device()
+        b.fold(chs, read_back=False)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms /= steps
+    launches = (b.launch_count() - l0) // steps
+
+    # the same instances one by one through the single-instance path
+    pps, provers, wits = {}, {}, []
+    for i, c in enumerate(col_logs):
+        if c not in pps:
+            pps[c] = L.PublicParameters.from_seed(L.Params.new(11 + c, c, [L.Modulus.Q9721_FS_S]), MATRIX_SEED)
+            provers[c] = L.Prover(pps[c])
+        wits.append(L.Witness.random(pps[c], seeds[i]))
+    N = lib()
+    chal = [np.ascontiguousarray(ch) for ch in chs]
+
+    def one(i):
+        c = col_logs[i]
+        op = ctypes.c_void_p()
+        check(N.lbg_commit(provers[c]._h, wits[i]._h, None, None, None, ctypes.byref(op)))
+        check(N.lbg_fold(provers[c]._h, op, ptr(chal[i]), len(chal[i]), None))
+
+    for i in range(instances):
+        one(i)
+    torch.cuda.synchronize()
+    seq_dev, seq_wall = 0.0, 0.0
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(instances):
+            c = col_logs[i]
+            st = torch.cuda.ExternalStream(N.lbg_prover_stream(provers[c]._h))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            one(i)
+            e1.record(st)
+            e1.synchronize()
+            seq_dev += e0.elapsed_time(e1)
+        seq_wall += (time.perf_counter() - t0) * 1000
+    seq_dev /= steps
+    seq_wall /= steps
+    return {"value": total / (ms / 1000), "unit": "elems/s", "ms_per_step": ms, "instances": instances,
+            "elements": total, "log2_sizes": [int(x) for x in logs],
+            "sequential_device_ms": seq_dev, "sequential_wall_ms": seq_wall,
+            "speedup_vs_sequential_device": seq_dev / ms, "speedup_vs_sequential_wall": seq_wall / ms,
+            "schedule": tuned, "gpu_launches_per_step": launches, "graphs": True,
+            "workload": "commit (2 limbs: 3889, 9721) + fold of every instance, column length 2048"}
+
+
+def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
+    """Served: commit+open requests with log2 n ~ U{18..22} (column length 2048, moduli [3889, 9721]),
+    80% Witness::random and 20% lifted B128 traces, each from its own seed, through the serving loop
+    (continuous batching over two device arenas, host steps on every host core). First the saturated
+    throughput (every request queued at once, a sample of the stream); then the Poisson stream of
+    `requests` arrivals at `load` x that throughput, with p50/p99 latency from arrival to result.
+    The comparison is the plain per-request path, one request after another (commit, evaluation
+    point, row and mle evaluation, folding challenges, fold), on a sample of the same requests,
+    its witnesses made before the clock starts."""
+    import labinius_b200 as L
+    from labinius_b200.batch import Batch
+    from labinius_b200.serve import Request, Server
+
+    rng = np.random.default_rng(seed)
+    logs = rng.integers(18, 23, requests)
+    kinds = (rng.random(requests) < 0.2).astype(int)
+    seeds = [rng.bytes(32) for _ in range(requests)]
+    gaps = rng.exponential(1.0, requests)
+    col_logs = [int(x) - 11 for x in logs]
+
+    def params(c):
+        return L.Params.new(11 + c, c, [L.Modulus.Q9721_FS_S])
+
+    pp = L.PublicParameters.from_seed(params(7), MATRIX_SEED)
+    srv = Server(pp, capacity_columns=8192, max_requests=64, slots=slots, host_threads=os.cpu_count() or 1,
+                 keep_results=False)
+
+    def run(idx, rate):
+        reqs, t0 = [], time.perf_counter()
+        due = 0.0
+        for k, i in enumerate(idx):
+            if rate:
+                due += gaps[k] / rate
+                d = t0 + due - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+            reqs.append(srv.submit(Request(col_logs[i], seeds[i], int(kinds[i]))))
+        for r in reqs:
+            r.wait()
+        errs = [r.error for r in reqs if r.error]
+        if errs:
+            raise RuntimeError(errs[0])
+        first = min(r.arrival for r in reqs)
+        last = max(r.done for r in reqs)
+        elems = sum(1 << int(logs[i]) for i in idx)
+        lat = np.array([r.latency for r in reqs]) * 1000
+        return elems / (last - first), len(idx) / (last - first), lat
+
+    run(range(min(64, requests)), None)  # warm-up: arenas, graphs of the host pool
+    sat_n = min(requests, 2000)
+    sat_elems, sat_reqs, _ = run(range(sat_n), None)
+    rate = load * sat_reqs
+    b0 = srv.batches
+    st_elems, st_reqs, lat = run(range(requests), rate)
+    batches = srv.batches - b0
+    srv.close()
+
+    # the plain per-request path on a sample of the same requests
+    pps = {}
+    sample = list(range(min(plain_sample, requests)))
+    wits = []
+    for i in sample:
+        c = col_logs[i]
+        if c not in pps:
+            pps[c] = (L.PublicParameters.from_seed(params(c), MATRIX_SEED),)
+            pps[c] += (L.Prover(pps[c][0]), L.Verifier(pps[c][0]))
+        p = pps[c][0]
+        if kinds[i]:
+            # the trace a B128 front end would hold on the host (made by the device generator)
+            g = Batch(p, [c])
+            g.witness_random([seeds[i]], [1])
+            wits.append(L.Witness.lifted(p, np.ascontiguousarray(g.elements(0)[:, :2])))
+            del g
+        else:
+            wits.append(L.Witness.random(p, seeds[i]))
+    lat_plain = []
+    t0 = time.perf_counter()
+    for k, i in enumerate(sample):
+        s0 = time.perf_counter()
+        p, prover, verifier = pps[col_logs[i]]
+        w = wits[k]
+        c, op = prover.commit(w)
+        t = L.Transcript(DOMAIN)
+        point = verifier.derive_evaluation_point(t, c)
+        w.mle_evaluate(point)
+        row = w.row_evaluate(point)
+        ch = verifier.derive_folding_challenges(t, row)
+        prover.fold(op, ch)
+        lat_plain.append((time.perf_counter() - s0) * 1000)
+    plain_s = time.perf_counter() - t0
+    plain_elems = sum(1 << int(logs[i]) for i in sample) / plain_s
+    return {"requests": requests, "rate_req_s": rate, "load": load, "batches": batches,
+            "throughput_elems_s": st_elems, "throughput_req_s": st_reqs,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()),
+            "saturated_elems_s": sat_elems, "saturated_req_s": sat_reqs, "saturated_sample": sat_n,
+            "plain_elems_s": plain_elems, "plain_sample": len(sample),
+            "plain_p50_ms": float(np.percentile(lat_plain, 50)), "plain_p99_ms": float(np.percentile(lat_plain, 99)),
+            "speedup_saturated_vs_plain": sat_elems / plain_elems,
+            "workload": "commit+open (commit, evaluation point, mle and row evaluation, folding challenges, fold) "
+                        "per request; log2 n ~ U{18..22}, column length 2048, moduli [3889, 9721]; 80% "
+                        "Witness::random, 20% lifted B128 traces; Poisson arrivals at load x saturated rate",
+            "slots": slots, "slot_columns": 8192, "host_threads": os.cpu_count() or 1}
+
+
+# ------------------------------------------------------------------------------------------------
 # our arm
 # ------------------------------------------------------------------------------------------------
 def run_ours(args):
@@ -347,6 +552,13 @@ def run_ours(args):
                "h2d_bytes_per_step": 24 * n + chal.nbytes, "d2h_bytes_per_step": mat.nbytes + vout.nbytes,
                "timing": "host wall clock around synchronous API calls, max over ranks"}
 
+    batched = None
+    if not args.no_batched:
+        batched = run_batched(args.batch_instances, max(3, min(args.steps, 5)))
+    served = None
+    if not args.no_served and rank == 0 and world == 1:
+        served = run_served(args.served_requests, args.served_plain_sample)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline((params.witness_log_len, params.column_log_len, params.primes()), args.cpu_seconds,
@@ -373,6 +585,8 @@ def run_ours(args):
         "clocks": clk,
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "batched": batched,
+        "served": served,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -186,9 +186,16 @@ int lbg_fold_static(uint32_t base_prime, uint32_t witness_log_len, uint32_t colu
  * instances one after another (columns, commitments, row values, folded witnesses). */
 typedef struct lbg_batch lbg_batch;
 int lbg_batch_new(const lbg_pp* pp, const uint32_t* column_log_lens, size_t count, lbg_batch** out);
+/* An arena sized once for max_cols columns and max_instances instances; lbg_batch_assign lays a
+ * new set of instances out in it without allocating (what a serving loop reuses). */
+int lbg_batch_new_capacity(const lbg_pp* pp, size_t max_cols, size_t max_instances, lbg_batch** out);
+int lbg_batch_assign(lbg_batch* b, const uint32_t* column_log_lens, size_t count);
 void lbg_batch_free(lbg_batch* b);
 size_t lbg_batch_columns(const lbg_batch* b);
 int lbg_batch_witness_random(lbg_batch* b, const uint8_t* seeds /* count x 32 bytes */);
+/* kinds[i] = 0: Witness::random(seed_i); 1: a B128 trace (keyed BLAKE3 XOF of "labinius/b128-trace")
+ * lifted (Witness::lifted). kinds may be null (all 0). */
+int lbg_batch_witness_generate(lbg_batch* b, const uint8_t* seeds, const uint8_t* kinds);
 int lbg_batch_witness_upload(lbg_batch* b, size_t instance, const uint64_t* f162, size_t n);
 int lbg_batch_witness_download(const lbg_batch* b, size_t instance, uint64_t* out, size_t n);
 int lbg_batch_use_graphs(lbg_batch* b, int enable);

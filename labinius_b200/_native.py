@@ -80,6 +80,9 @@ SIGNATURES = {
     "lbg_params_pack_dropped": (_sz, [_P, _vp, _vp, _vp, _sz]),
     "lbg_fold_static": (_int, [_u32, _u32, _u32, _vp, _vp, _sz, _vp, _vp]),
     "lbg_batch_new": (_int, [_vp, _vp, _sz, ctypes.POINTER(_vp)]),
+    "lbg_batch_new_capacity": (_int, [_vp, _sz, _sz, ctypes.POINTER(_vp)]),
+    "lbg_batch_assign": (_int, [_vp, _vp, _sz]),
+    "lbg_batch_witness_generate": (_int, [_vp, _vp, _vp]),
     "lbg_batch_free": (None, [_vp]),
     "lbg_batch_columns": (_sz, [_vp]),
     "lbg_batch_witness_random": (_int, [_vp, _vp]),

@@ -33,32 +33,53 @@ class InstanceRound:
 
 
 class Batch:
-    def __init__(self, pp: PublicParameters, column_log_lens):
+    def __init__(self, pp: PublicParameters, column_log_lens=None, capacity=None):
+        """A batch of the given instances, or (capacity=(max_columns, max_instances)) an empty arena
+        that `assign` lays instances out in."""
         self.pp = pp
-        self.column_log_lens = [int(c) for c in column_log_lens]
-        self.count = len(self.column_log_lens)
         self.row_log = pp.params.row_log_len()
         self.wdim = 1 << self.row_log
         self.len_ring = self.wdim // 4
         self.limbs = len(pp.params.primes())
         self.dropped = pp.params.dropped_bits()
+        h = ctypes.c_void_p()
+        if capacity is not None:
+            check(lib().lbg_batch_new_capacity(pp._h, int(capacity[0]), int(capacity[1]), ctypes.byref(h)))
+            self._h = h
+            self.capacity = (int(capacity[0]), int(capacity[1]))
+            self._layout([])
+            if column_log_lens is not None:
+                self.assign(column_log_lens)
+            return
+        arr = np.array([int(c) for c in column_log_lens], np.uint32)
+        check(lib().lbg_batch_new(pp._h, ptr(arr), len(arr), ctypes.byref(h)))
+        self._h = h
+        self.capacity = (sum(1 << int(c) for c in column_log_lens), len(arr))
+        self._layout(column_log_lens)
+
+    def _layout(self, column_log_lens):
+        self.column_log_lens = [int(c) for c in column_log_lens]
+        self.count = len(self.column_log_lens)
         self.cols = [1 << c for c in self.column_log_lens]
         self.col_off = np.concatenate([[0], np.cumsum(self.cols)]).astype(np.int64)
-        arr = np.array(self.column_log_lens, np.uint32)
-        h = ctypes.c_void_p()
-        check(lib().lbg_batch_new(pp._h, ptr(arr), self.count, ctypes.byref(h)))
-        self._h = h
-        self.total_cols = int(lib().lbg_batch_columns(h))
+        self.total_cols = int(self.col_off[-1])
+
+    def assign(self, column_log_lens):
+        arr = np.array([int(c) for c in column_log_lens], np.uint32)
+        check(lib().lbg_batch_assign(self._h, ptr(arr), len(arr)))
+        self._layout(column_log_lens)
 
     def params_of(self, i) -> Params:
         p = self.pp.params
         return Params(self.row_log + self.column_log_lens[i], self.column_log_lens[i], p.base, list(p.extra_moduli),
                       p.opening)
 
-    def witness_random(self, seeds: List[bytes]):
+    def witness_random(self, seeds: List[bytes], kinds=None):
+        """kinds[i] = 0: Witness::random(seeds[i]); 1: a B128 trace from seeds[i], lifted."""
         s = np.frombuffer(b"".join(bytes(x) for x in seeds), dtype=np.uint8).copy()
         assert len(s) == 32 * self.count
-        check(lib().lbg_batch_witness_random(self._h, ptr(s)))
+        k = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.uint8)
+        check(lib().lbg_batch_witness_generate(self._h, ptr(s), ptr(k)))
 
     def witness_upload(self, i, elements):
         e = np.ascontiguousarray(elements, dtype=np.uint64).reshape(-1, 3)
@@ -117,34 +138,42 @@ class Batch:
         check(lib().lbg_batch_fold(self._h, ptr(ch), len(ch), ptr(v)))
         return [v[i] for i in range(self.count)] if read_back else None
 
-    def round(self, domain=b"labinius/reference") -> List[InstanceRound]:
-        """commit -> per instance: evaluation point -> row and mle evaluation -> per instance: folding
-        challenges -> fold; the host steps in the library's host code, instance by instance."""
-        rounds = self.commit()
+    def _point(self, i, r, domain):
+        """Host: a fresh transcript for instance i, the commitment absorbed, the evaluation point."""
         seed = np.frombuffer(self.pp.matrix_seed, np.uint8).copy()
         d = np.frombuffer(domain, np.uint8).copy()
-        ts = []
-        for i, r in enumerate(rounds):
-            pn = self.params_of(i).native()
-            t = lib().lbg_transcript_new(ptr(d), len(domain))
-            ts.append(t)
-            r.p0 = np.zeros((self.row_log, 3), np.uint64)
-            r.p1 = np.zeros((self.column_log_lens[i], 3), np.uint64)
-            if self.dropped:
-                dig = r.digits if self.limbs > 1 else np.zeros(1, np.uint16)
-                check(lib().lbg_params_derive_evaluation_point(ctypes.byref(pn), ptr(seed), t, None, ptr(r.top),
-                                                               ptr(np.ascontiguousarray(dig)), ptr(r.p0), ptr(r.p1)))
-            else:
-                check(lib().lbg_params_derive_evaluation_point(ctypes.byref(pn), ptr(seed), t, ptr(r.matrix), None,
-                                                               None, ptr(r.p0), ptr(r.p1)))
+        pn = self.params_of(i).native()
+        t = lib().lbg_transcript_new(ptr(d), len(domain))
+        r.p0 = np.zeros((self.row_log, 3), np.uint64)
+        r.p1 = np.zeros((self.column_log_lens[i], 3), np.uint64)
+        if self.dropped:
+            dig = r.digits if self.limbs > 1 else np.zeros(1, np.uint16)
+            check(lib().lbg_params_derive_evaluation_point(ctypes.byref(pn), ptr(seed), t, None, ptr(r.top),
+                                                           ptr(np.ascontiguousarray(dig)), ptr(r.p0), ptr(r.p1)))
+        else:
+            check(lib().lbg_params_derive_evaluation_point(ctypes.byref(pn), ptr(seed), t, ptr(r.matrix), None,
+                                                           None, ptr(r.p0), ptr(r.p1)))
+        return t
+
+    def _challenges(self, i, r, t):
+        """Host: absorb instance i's row values and sample its folding challenges."""
+        pn = self.params_of(i).native()
+        r.challenges = np.zeros(self.cols[i], _CH)
+        check(lib().lbg_params_derive_folding_challenges(ctypes.byref(pn), t, ptr(r.u), ptr(r.challenges)))
+        lib().lbg_transcript_free(t)
+
+    def round(self, domain=b"labinius/reference", pool=None) -> List[InstanceRound]:
+        """commit -> per instance: evaluation point -> row and mle evaluation -> per instance: folding
+        challenges -> fold. The host steps run in the library's host code, on `pool` (a
+        concurrent.futures executor; the calls release the GIL) or instance by instance."""
+        rounds = self.commit()
+        run = (lambda f, xs: list(pool.map(f, xs))) if pool is not None else (lambda f, xs: [f(x) for x in xs])
+        ts = run(lambda i: self._point(i, rounds[i], domain), range(self.count))
         mles = self.mle_evaluate([r.p0 for r in rounds], [r.p1 for r in rounds])
         us = self.row_evaluate([r.p0 for r in rounds])
         for i, r in enumerate(rounds):
             r.mle, r.u = mles[i], us[i]
-            pn = self.params_of(i).native()
-            r.challenges = np.zeros(self.cols[i], _CH)
-            check(lib().lbg_params_derive_folding_challenges(ctypes.byref(pn), ts[i], ptr(r.u), ptr(r.challenges)))
-            lib().lbg_transcript_free(ts[i])
+        run(lambda i: self._challenges(i, rounds[i], ts[i]), range(self.count))
         vs = self.fold([r.challenges for r in rounds])
         for i, r in enumerate(rounds):
             r.v = vs[i]

@@ -43,6 +43,7 @@ struct lbg_batch {
   size_t total_cols = 0;
   size_t wdim = 0, len_ring = 0;
   int min_col_log = 0;
+  size_t cap_cols = 0, cap_instances = 0;
   cudaStream_t stream = nullptr;
   uint64_t* d_w = nullptr;        // [total_cols * wdim][3]
   int* d_col_inst = nullptr;      // [total_cols]
@@ -169,33 +170,19 @@ void lbg_batch_free(lbg_batch* b) {
   delete b;
 }
 
-int lbg_batch_new(const lbg_pp* pp, const uint32_t* column_log_lens, size_t count, lbg_batch** out) {
-  if (!pp || !column_log_lens || !out || count == 0) return fail(LBG_ERR_INVALID, "null argument or empty batch");
+// An arena of `max_cols` columns and `max_instances` instances: the device buffers are sized once;
+// lbg_batch_assign lays out a set of instances inside it without allocating.
+int lbg_batch_new_capacity(const lbg_pp* pp, size_t max_cols, size_t max_instances, lbg_batch** out) {
+  if (!pp || !out || max_cols == 0 || max_instances == 0) return fail(LBG_ERR_INVALID, "null argument or empty batch");
   *out = nullptr;
-  if (count > 65536) return fail(LBG_ERR_INVALID, "at most 65536 instances");
-  uint32_t row_log = pp->params.witness_log_len - pp->params.column_log_len;
+  if (max_instances > 65536) return fail(LBG_ERR_INVALID, "at most 65536 instances");
+  if (max_cols > ((size_t)1 << 30) / pp->wdim) return fail(LBG_ERR_PARAMS, "batch too large");
   lbg_batch* b = new lbg_batch();
   b->pp = pp;
-  b->count = (int)count;
   b->wdim = pp->wdim;
   b->len_ring = pp->len_ring;
-  b->col_off.push_back(0);
-  b->min_col_log = 31;
-  for (size_t i = 0; i < count; i++) {
-    uint32_t cl = column_log_lens[i];
-    if (cl < 1 || cl + row_log > 30) {
-      delete b;
-      return fail(LBG_ERR_PARAMS, "instance " + std::to_string(i) + ": column_log_len out of range");
-    }
-    b->col_log.push_back(cl);
-    b->min_col_log = std::min(b->min_col_log, (int)cl);
-    b->col_off.push_back(b->col_off.back() + ((size_t)1 << cl));
-  }
-  b->total_cols = b->col_off.back();
-  if (b->total_cols > (1u << 30) / b->wdim) {
-    delete b;
-    return fail(LBG_ERR_PARAMS, "batch too large");
-  }
+  b->cap_cols = max_cols;
+  b->cap_instances = max_instances;
   auto bail = [&](int code) {
     lbg_batch_free(b);
     return code;
@@ -203,7 +190,7 @@ int lbg_batch_new(const lbg_pp* pp, const uint32_t* column_log_lens, size_t coun
   if (cudaSetDevice(pp->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(LBG_ERR_CUDA, "stream"));
   int L = pp->limbs;
-  size_t C = b->total_cols, n = C * b->wdim, count648 = C * N648;
+  size_t C = max_cols, I = max_instances, n = C * b->wdim, count648 = C * N648;
   b->max_chunks = (int)((b->len_ring + commit_ring_per_step() - 1) / commit_ring_per_step());
   if (b->max_chunks > 64) b->max_chunks = 64;
   bool ok = cudaMalloc((void**)&b->d_w, n * 24) == cudaSuccess &&
@@ -214,66 +201,130 @@ int lbg_batch_new(const lbg_pp* pp, const uint32_t* column_log_lens, size_t coun
             cudaMalloc((void**)&b->d_res, (size_t)L * count648 * 2) == cudaSuccess &&
             cudaMalloc((void**)&b->d_top, count648 * 2) == cudaSuccess &&
             cudaMalloc((void**)&b->d_digits, (size_t)(L > 1 ? L - 1 : 1) * count648 * 2) == cudaSuccess &&
-            cudaMalloc((void**)&b->d_p0, count * 32 * 24) == cudaSuccess &&
-            cudaMalloc((void**)&b->d_p1, count * 32 * 24) == cudaSuccess &&
-            cudaMalloc((void**)&b->d_eq, count * b->wdim * 24) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_p0, I * 32 * 24) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_p1, I * 32 * 24) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_eq, I * b->wdim * 24) == cudaSuccess &&
             cudaMalloc((void**)&b->d_u, C * 24) == cudaSuccess &&
-            cudaMalloc((void**)&b->d_claim, count * 24) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_claim, I * 24) == cudaSuccess &&
             cudaMalloc((void**)&b->d_ch, C * sizeof(lbg_challenge_d)) == cudaSuccess &&
             cudaMalloc((void**)&b->d_chat, C * N162 * 4) == cudaSuccess &&
-            cudaMalloc((void**)&b->d_vhat, count * b->wdim * N162 * 4) == cudaSuccess &&
-            cudaMalloc((void**)&b->d_v, count * b->len_ring * N648 * 2) == cudaSuccess;
+            cudaMalloc((void**)&b->d_vhat, I * b->wdim * N162 * 4) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_v, I * b->len_ring * N648 * 2) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     return bail(fail(LBG_ERR_OOM, "batch: device allocation failed"));
   }
-  std::vector<int> ci(C);
-  for (int i = 0; i < b->count; i++)
-    for (size_t c = b->col_off[i]; c < b->col_off[i + 1]; c++) ci[c] = i;
-  if (cudaMemcpy(b->d_col_inst, ci.data(), C * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
-    return bail(fail(LBG_ERR_CUDA, "batch maps"));
   if (cudaMemsetAsync(b->d_w, 0, n * 24, b->stream) != cudaSuccess ||
-      cudaMemsetAsync(b->d_ch, 0, C * sizeof(lbg_challenge_d), b->stream) != cudaSuccess)
+      cudaMemsetAsync(b->d_ch, 0, C * sizeof(lbg_challenge_d), b->stream) != cudaSuccess ||
+      cudaStreamSynchronize(b->stream) != cudaSuccess)
     return bail(fail(LBG_ERR_CUDA, "batch init"));
-  // model schedule (the autotuner refines it): chunks for about two waves, fold splits of 16
+  *out = b;
+  return LBG_OK;
+}
+
+// Lay out `count` instances (instance i: 2^column_log_lens[i] columns) in the arena; the model
+// schedule is set, the CUDA graphs (if any) dropped.
+int lbg_batch_assign(lbg_batch* b, const uint32_t* column_log_lens, size_t count) {
+  if (!b || !column_log_lens || count == 0) return fail(LBG_ERR_INVALID, "null argument or empty batch");
+  if (count > b->cap_instances) return fail(LBG_ERR_INVALID, "more instances than the batch holds");
+  const lbg_pp* pp = b->pp;
+  uint32_t row_log = pp->params.witness_log_len - pp->params.column_log_len;
+  std::vector<uint32_t> cl(column_log_lens, column_log_lens + count);
+  std::vector<size_t> off{0};
+  int minc = 31;
+  for (size_t i = 0; i < count; i++) {
+    if (cl[i] < 1 || cl[i] + row_log > 30)
+      return fail(LBG_ERR_PARAMS, "instance " + std::to_string(i) + ": column_log_len out of range");
+    minc = std::min(minc, (int)cl[i]);
+    off.push_back(off.back() + ((size_t)1 << cl[i]));
+  }
+  if (off.back() > b->cap_cols) return fail(LBG_ERR_INVALID, "more columns than the batch holds");
+  LBG_BCU(cudaSetDevice(pp->device));
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  if (b->graphs) {
+    free_graphs(b);
+    b->graphs = false;
+  }
+  b->count = (int)count;
+  b->col_log = cl;
+  b->col_off = off;
+  b->total_cols = off.back();
+  b->min_col_log = minc;
+  std::vector<int> ci(b->total_cols);
+  for (int i = 0; i < b->count; i++)
+    for (size_t c = off[i]; c < off[i + 1]; c++) ci[c] = i;
+  LBG_BCU(cudaMemcpy(b->d_col_inst, ci.data(), ci.size() * sizeof(int), cudaMemcpyHostToDevice));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pp->device);
-  long tiles = (long)((C + commit_cols_per_cta() - 1) / commit_cols_per_cta());
+  long tiles = (long)((b->total_cols + commit_cols_per_cta() - 1) / commit_cols_per_cta());
   int want = (int)std::max<long>(1, (2L * sms * commit_blocks_per_sm(pp->pidx[0]) + tiles - 1) / tiles);
   set_chunks(b, std::min(want, b->max_chunks));
-  int rc = upload_splits(b, std::min(16, 1 << b->min_col_log));
-  if (rc) return bail(rc);
-  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bail(fail(LBG_ERR_CUDA, "batch init"));
+  return upload_splits(b, std::min(16, 1 << b->min_col_log));
+}
+
+int lbg_batch_new(const lbg_pp* pp, const uint32_t* column_log_lens, size_t count, lbg_batch** out) {
+  if (!pp || !column_log_lens || !out || count == 0) return fail(LBG_ERR_INVALID, "null argument or empty batch");
+  *out = nullptr;
+  uint32_t row_log = pp->params.witness_log_len - pp->params.column_log_len;
+  size_t cols = 0;
+  for (size_t i = 0; i < count; i++) {
+    if (column_log_lens[i] < 1 || column_log_lens[i] + row_log > 30)
+      return fail(LBG_ERR_PARAMS, "instance " + std::to_string(i) + ": column_log_len out of range");
+    cols += (size_t)1 << column_log_lens[i];
+  }
+  lbg_batch* b = nullptr;
+  int rc = lbg_batch_new_capacity(pp, cols, count, &b);
+  if (rc) return rc;
+  rc = lbg_batch_assign(b, column_log_lens, count);
+  if (rc) {
+    lbg_batch_free(b);
+    return rc;
+  }
   *out = b;
   return LBG_OK;
 }
 
 size_t lbg_batch_columns(const lbg_batch* b) { return b ? b->total_cols : 0; }
 
-int lbg_batch_witness_random(lbg_batch* b, const uint8_t* seeds) {
+// The keyed BLAKE3 root of a one-block message (the XOF kernels compute its output blocks).
+static XofRoot keyed_root(const uint8_t* key, const char* label) {
+  XofRoot root;
+  for (int w = 0; w < 8; w++)
+    root.cv[w] = (uint32_t)key[4 * w] | ((uint32_t)key[4 * w + 1] << 8) | ((uint32_t)key[4 * w + 2] << 16) |
+                 ((uint32_t)key[4 * w + 3] << 24);
+  uint8_t msg[64] = {0};
+  size_t len = std::strlen(label);
+  std::memcpy(msg, label, len);
+  for (int w = 0; w < 16; w++)
+    root.m[w] = (uint32_t)msg[4 * w] | ((uint32_t)msg[4 * w + 1] << 8) | ((uint32_t)msg[4 * w + 2] << 16) |
+                ((uint32_t)msg[4 * w + 3] << 24);
+  root.block_len = (uint32_t)len;
+  root.flags = 16 | 1 | 2 | 8;  // keyed hash, chunk start, chunk end, root
+  return root;
+}
+
+// Witnesses of every instance from 32-byte seeds: kind 0 is Witness::random (keyed BLAKE3 XOF of
+// "labinius/witness", crates/pcs/src/scheme/witness.rs:66-87); kind 1 is a B128 trace (keyed XOF
+// of "labinius/b128-trace", 16 bytes per element) lifted bit for bit (Witness::lifted,
+// crates/pcs/src/scheme/witness.rs:45-52). `kinds` may be null (all kind 0).
+int lbg_batch_witness_generate(lbg_batch* b, const uint8_t* seeds, const uint8_t* kinds) {
   if (!b || !seeds) return fail(LBG_ERR_INVALID, "null argument");
   LBG_BCU(cudaSetDevice(b->pp->device));
   for (int i = 0; i < b->count; i++) {
-    XofRoot root;
-    const uint8_t* s = seeds + 32 * i;
-    for (int w = 0; w < 8; w++)
-      root.cv[w] = (uint32_t)s[4 * w] | ((uint32_t)s[4 * w + 1] << 8) | ((uint32_t)s[4 * w + 2] << 16) |
-                   ((uint32_t)s[4 * w + 3] << 24);
-    uint8_t msg[64] = {0};
-    std::memcpy(msg, "labinius/witness", 16);
-    for (int w = 0; w < 16; w++)
-      root.m[w] = (uint32_t)msg[4 * w] | ((uint32_t)msg[4 * w + 1] << 8) | ((uint32_t)msg[4 * w + 2] << 16) |
-                  ((uint32_t)msg[4 * w + 3] << 24);
-    root.block_len = 16;
-    root.flags = 16 | 1 | 2 | 8;
     size_t n = (b->col_off[i + 1] - b->col_off[i]) * b->wdim;
     uint64_t* dst = b->d_w + b->col_off[i] * b->wdim * 3;
-    LBG_BCU(launch_xof(root, n * 24, (uint8_t*)dst, b->stream));
-    LBG_BCU(launch_mask_f162(dst, n, b->stream));
+    if (kinds && kinds[i] == 1) {
+      LBG_BCU(launch_xof_lifted(keyed_root(seeds + 32 * i, "labinius/b128-trace"), n, dst, b->stream));
+    } else {
+      LBG_BCU(launch_xof(keyed_root(seeds + 32 * i, "labinius/witness"), n * 24, (uint8_t*)dst, b->stream));
+      LBG_BCU(launch_mask_f162(dst, n, b->stream));
+    }
   }
   LBG_BCU(cudaStreamSynchronize(b->stream));
   return LBG_OK;
 }
+
+int lbg_batch_witness_random(lbg_batch* b, const uint8_t* seeds) { return lbg_batch_witness_generate(b, seeds, nullptr); }
 
 int lbg_batch_witness_upload(lbg_batch* b, size_t instance, const uint64_t* f162, size_t n) {
   if (!b || !f162) return fail(LBG_ERR_INVALID, "null argument");

@@ -560,9 +560,7 @@ __constant__ uint8_t c_b3_sched[7][16] = {
 };
 
 // Output block t of a single-block root node (key words, message words, length, flags).
-__global__ void k_xof_blocks(XofRoot root, size_t nbytes, uint8_t* __restrict__ out) {
-  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t * 64 >= nbytes) return;
+__device__ __forceinline__ void xof_block(const XofRoot& root, size_t t, uint32_t o[16]) {
   const uint32_t IV[4] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au};
   uint32_t s[16];
   for (int i = 0; i < 8; i++) s[i] = root.cv[i];
@@ -582,14 +580,36 @@ __global__ void k_xof_blocks(XofRoot root, size_t nbytes, uint8_t* __restrict__ 
     g_mix(s, 2, 7, 8, 13, root.m[w[12]], root.m[w[13]]);
     g_mix(s, 3, 4, 9, 14, root.m[w[14]], root.m[w[15]]);
   }
-  uint32_t o[16];
   for (int i = 0; i < 8; i++) {
     o[i] = s[i] ^ s[i + 8];
     o[i + 8] = s[i + 8] ^ root.cv[i];
   }
+}
+
+__global__ void k_xof_blocks(XofRoot root, size_t nbytes, uint8_t* __restrict__ out) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t * 64 >= nbytes) return;
+  uint32_t o[16];
+  xof_block(root, t, o);
   size_t base = t * 64;
   for (int i = 0; i < 64; i++)
     if (base + i < nbytes) out[base + i] = (uint8_t)(o[i >> 2] >> (8 * (i & 3)));
+}
+
+// A B128 trace from the XOF (16 bytes per element, little-endian), lifted as it is produced:
+// block t holds elements 4t .. 4t+3, written as F162 [lo, hi, 0] (crates/pcs/src/fields/scalar.rs:72-74).
+__global__ void k_xof_lifted(XofRoot root, size_t n, uint64_t* __restrict__ W) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t * 4 >= n) return;
+  uint32_t o[16];
+  xof_block(root, t, o);
+  for (int k = 0; k < 4; k++) {
+    size_t e = 4 * t + k;
+    if (e >= n) break;
+    W[3 * e] = (uint64_t)o[4 * k] | ((uint64_t)o[4 * k + 1] << 32);
+    W[3 * e + 1] = (uint64_t)o[4 * k + 2] | ((uint64_t)o[4 * k + 3] << 32);
+    W[3 * e + 2] = 0;
+  }
 }
 
 __global__ void k_mask_f162(uint64_t* __restrict__ W, size_t n) {
@@ -774,6 +794,12 @@ cudaError_t launch_claim(const uint64_t* u, int cols, const uint64_t* p1, int n,
 cudaError_t launch_xof(const XofRoot& root, size_t nbytes, uint8_t* out, cudaStream_t st) {
   size_t blocks = (nbytes + 63) / 64;
   k_xof_blocks<<<blocks_for(blocks, 128), 128, 0, st>>>(root, nbytes, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_xof_lifted(const XofRoot& root, size_t n, uint64_t* W, cudaStream_t st) {
+  size_t blocks = (n + 3) / 4;
+  k_xof_lifted<<<blocks_for(blocks, 128), 128, 0, st>>>(root, n, W);
   return cudaGetLastError();
 }
 

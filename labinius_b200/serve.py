@@ -1,0 +1,129 @@
+"""Serving: a request loop with continuous batching over device arenas.
+
+A request is one commit + open round (commit, evaluation point, mle and row evaluation, folding
+challenges, fold) of its own witness under the server's key: any column count 2^c with the key's
+column length, a witness drawn from the request's seed (kind 0: Witness::random; kind 1: a B128
+trace lifted, crates/pcs/src/scheme/witness.rs:45-87).
+
+Continuous batching: the server owns `slots` device arenas (lbg_batch, sized once; admission is by
+arena room, i.e. by the HBM each slot reserved). Whenever a slot is free it admits, in arrival
+order, every queued request that fits, lays them out in the arena and runs their rounds together:
+each device stage is one launch over all of them, their host steps (transcripts, challenge
+sampling) run in parallel on a thread pool, and while one slot is in its host steps the other
+slot's device stages run on its own stream, so requests that arrive while others are on the GPU
+are admitted as soon as a slot and its memory free up and their work overlaps on the device.
+The parameters, the key and each slot's state stay resident on the device.
+"""
+import collections
+import concurrent.futures
+import threading
+import time
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+from .batch import Batch, InstanceRound
+from .scheme import PublicParameters
+
+
+@dataclass
+class Request:
+    column_log_len: int
+    seed: bytes
+    kind: int = 0               # 0: Witness::random(seed); 1: lifted B128 trace from seed
+    arrival: float = 0.0        # seconds on the server's clock
+    admitted: float = 0.0
+    done: float = 0.0
+    result: Optional[InstanceRound] = None
+    error: Optional[str] = None
+    _event: threading.Event = field(default_factory=threading.Event, repr=False)
+
+    def wait(self, timeout=None):
+        return self._event.wait(timeout)
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+class Server:
+    def __init__(self, pp: PublicParameters, capacity_columns: int, max_requests: int = 256, slots: int = 2,
+                 host_threads: int = 16, domain: bytes = b"labinius/reference", keep_results: bool = True):
+        self.pp = pp
+        self.capacity = capacity_columns
+        self.max_requests = max_requests
+        self.domain = domain
+        self.keep_results = keep_results
+        self.slots = [Batch(pp, capacity=(capacity_columns, max_requests)) for _ in range(slots)]
+        self.pool = concurrent.futures.ThreadPoolExecutor(host_threads)
+        self.queue = collections.deque()
+        self.cv = threading.Condition()
+        self.stop = False
+        self.t0 = time.perf_counter()
+        self.batches = 0
+        self.workers = [threading.Thread(target=self._work, args=(b,), daemon=True) for b in self.slots]
+        for w in self.workers:
+            w.start()
+
+    def clock(self):
+        return time.perf_counter() - self.t0
+
+    def submit(self, req: Request) -> Request:
+        if (1 << req.column_log_len) > self.capacity:
+            req.error = "request larger than a slot"
+            req.done = self.clock()
+            req._event.set()
+            return req
+        with self.cv:
+            if not req.arrival:
+                req.arrival = self.clock()
+            self.queue.append(req)
+            self.cv.notify()
+        return req
+
+    def _admit(self) -> List[Request]:
+        """Arrival order, as many as fit the arena (columns) and its request table."""
+        taken, cols = [], 0
+        while self.queue and len(taken) < self.max_requests:
+            c = 1 << self.queue[0].column_log_len
+            if cols + c > self.capacity:
+                break
+            cols += c
+            taken.append(self.queue.popleft())
+        return taken
+
+    def _work(self, b: Batch):
+        while True:
+            with self.cv:
+                while not self.queue and not self.stop:
+                    self.cv.wait()
+                if self.stop and not self.queue:
+                    return
+                reqs = self._admit()
+            if not reqs:
+                continue
+            now = self.clock()
+            for r in reqs:
+                r.admitted = now
+            try:
+                b.assign([r.column_log_len for r in reqs])
+                b.witness_random([r.seed for r in reqs], [r.kind for r in reqs])
+                rounds = b.round(self.domain, pool=self.pool)
+                self.batches += 1
+                err = None
+            except Exception as e:  # noqa: BLE001 - reported on every request of the batch
+                rounds, err = None, str(e)
+            end = self.clock()
+            for i, r in enumerate(reqs):
+                r.done = end
+                r.error = err
+                if rounds is not None and self.keep_results:
+                    r.result = rounds[i]
+                r._event.set()
+
+    def close(self):
+        with self.cv:
+            self.stop = True
+            self.cv.notify_all()
+        for w in self.workers:
+            w.join()
+        self.pool.shutdown()

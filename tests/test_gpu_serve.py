@@ -1,0 +1,65 @@
+"""Serving with continuous batching: each request's result in the mix equals the same request run
+alone through the single-instance path (native witnesses and lifted B128 traces, mixed sizes,
+arrivals while other requests are on the GPU); admission respects the arena size."""
+import time
+
+import numpy as np
+import pytest
+
+from rounds import DOMAIN, MATRIX_SEED, product_params
+
+pytestmark = pytest.mark.gpu
+
+
+def alone(oracle, row_log, primes, req):
+    """The request's round on its own: Witness::random or Witness::lifted, then the plain path."""
+    import labinius_b200 as L
+
+    cl = req.column_log_len
+    params = product_params((row_log + cl, cl, primes, 0))
+    pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+    if req.kind == 1:
+        n = params.witness_len()
+        raw = oracle.blake3(b"labinius/b128-trace", 16 * n, key=req.seed)
+        w = L.Witness.lifted(pp, np.frombuffer(raw, dtype=np.uint64).reshape(-1, 2))
+    else:
+        w = L.Witness.random(pp, req.seed)
+    prover, verifier = L.Prover(pp), L.Verifier(pp)
+    c, op = prover.commit(w)
+    t = L.Transcript(DOMAIN)
+    point = verifier.derive_evaluation_point(t, c)
+    mle, row = w.mle_evaluate(point), w.row_evaluate(point)
+    ch = verifier.derive_folding_challenges(t, row)
+    v = prover.fold(op, ch)
+    return c.matrix, point, mle, row.values, ch.challenges, v.elements
+
+
+def test_results_in_the_mix_equal_results_alone(oracle):
+    import labinius_b200 as L
+    from labinius_b200.serve import Request, Server
+
+    row_log, primes = 8, [3889, 9721]
+    pp = L.PublicParameters.from_seed(product_params((row_log + 3, 3, primes, 0)), MATRIX_SEED)
+    srv = Server(pp, capacity_columns=48, max_requests=8, slots=2, host_threads=4)
+    rng = np.random.default_rng(4)
+    reqs = []
+    for i in range(14):
+        cl = int(rng.integers(1, 6))
+        reqs.append(srv.submit(Request(cl, bytes([0x40 + i]) * 32, kind=int(i % 5 == 4))))
+        if i % 4 == 3:
+            time.sleep(0.01)  # later arrivals join while earlier batches run
+    too_big = srv.submit(Request(6, bytes(32)))  # 64 columns > 48
+    for r in reqs:
+        assert r.wait(120)
+    srv.close()
+    assert too_big.error is not None
+    assert srv.batches >= 2
+    for r in reqs:
+        assert r.error is None, r.error
+        m, point, mle, u, ch, v = alone(oracle, row_log, primes, r)
+        res = r.result
+        assert np.array_equal(res.matrix, m)
+        assert np.array_equal(res.p0, point.p0) and np.array_equal(res.p1, point.p1)
+        assert np.array_equal(res.mle, mle) and np.array_equal(res.u, u)
+        assert np.array_equal(res.challenges, ch)
+        assert np.array_equal(res.v, v)
