@@ -205,6 +205,24 @@ int lbg_batch_row_evaluate(lbg_batch* b, const uint64_t* p0 /* [count][row_log][
 int lbg_batch_mle_evaluate(lbg_batch* b, const uint64_t* p0, const uint64_t* p1 /* concatenated */,
                            uint64_t* out /* [count][3] */);
 int lbg_batch_fold(lbg_batch* b, const lbg_challenge* challenges, size_t r, int16_t* v_out);
+/* A whole commit + open round of every instance on the device, transcript included: per instance
+ * a fresh Transcript::new(domain), then the steps of crates/bench/src/bin/labinius.rs:104-130
+ * (Prover::commit, derive_evaluation_point, mle_evaluate, row_evaluate, FoldingChallenges::derive,
+ * Prover::fold) with the absorbs, the evaluation point and the challenge sampler run by device
+ * kernels in stream order (no host step between commit and fold). The outputs equal those of the
+ * host transcript path bit for bit. Every output pointer may be null (not copied back). */
+typedef struct lbg_batch_outputs {
+  int16_t* matrix;            /* [total_cols][4][limbs][162] (Opening::Clear) */
+  uint16_t* top;              /* [total_cols * 648] (bit-dropped) */
+  uint16_t* digits;           /* [limbs - 1][total_cols * 648] (bit-dropped) */
+  uint64_t* p0;               /* [count][row_log][3] */
+  uint64_t* p1;               /* instance i's column_log_len_i coordinates, one instance after another */
+  uint64_t* mle;              /* [count][3] */
+  uint64_t* u;                /* [total_cols][3] */
+  lbg_challenge* challenges;  /* [total_cols] */
+  int16_t* v;                 /* [count][len_ring][648] */
+} lbg_batch_outputs;
+int lbg_batch_round(lbg_batch* b, const uint8_t* domain, size_t domain_len, const lbg_batch_outputs* out);
 void* lbg_batch_stream(const lbg_batch* b);
 uint64_t lbg_batch_launch_count(const lbg_batch* b);
 

@@ -94,11 +94,17 @@ SIGNATURES = {
     "lbg_batch_row_evaluate": (_int, [_vp, _vp, _vp]),
     "lbg_batch_mle_evaluate": (_int, [_vp, _vp, _vp, _vp]),
     "lbg_batch_fold": (_int, [_vp, _vp, _sz, _vp]),
+    "lbg_batch_round": (_int, [_vp, _vp, _sz, _vp]),
     "lbg_batch_stream": (_vp, [_vp]),
     "lbg_batch_launch_count": (_u64, [_vp]),
 }
 
 _lib = None
+
+
+class lbg_batch_outputs(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in
+                ("matrix", "top", "digits", "p0", "p1", "mle", "u", "challenges", "v")]
 
 
 class NativeError(RuntimeError):

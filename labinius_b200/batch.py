@@ -162,10 +162,16 @@ class Batch:
         check(lib().lbg_params_derive_folding_challenges(ctypes.byref(pn), t, ptr(r.u), ptr(r.challenges)))
         lib().lbg_transcript_free(t)
 
-    def round(self, domain=b"labinius/reference", pool=None) -> List[InstanceRound]:
+    def round(self, domain=b"labinius/reference", pool=None, transcript="device") -> List[InstanceRound]:
         """commit -> per instance: evaluation point -> row and mle evaluation -> per instance: folding
-        challenges -> fold. The host steps run in the library's host code, on `pool` (a
+        challenges -> fold, each instance with a fresh Transcript(domain).
+
+        transcript="device": the whole round in one pass on the device (the absorbs, the point and
+        the challenge sampler are device kernels; lbg_batch_round). transcript="host": the
+        transcript steps run in the library's host code between the device stages, on `pool` (a
         concurrent.futures executor; the calls release the GIL) or instance by instance."""
+        if transcript == "device":
+            return self._round_device(domain)
         rounds = self.commit()
         run = (lambda f, xs: list(pool.map(f, xs))) if pool is not None else (lambda f, xs: [f(x) for x in xs])
         ts = run(lambda i: self._point(i, rounds[i], domain), range(self.count))
@@ -177,6 +183,43 @@ class Batch:
         vs = self.fold([r.challenges for r in rounds])
         for i, r in enumerate(rounds):
             r.v = vs[i]
+        return rounds
+
+    def _round_device(self, domain) -> List[InstanceRound]:
+        C, L, I = self.total_cols, self.limbs, self.count
+        out = nat.lbg_batch_outputs()
+        m = top = dig = None
+        if self.dropped:
+            top = np.zeros(C * N, np.uint16)
+            dig = np.zeros((max(L - 1, 1), C * N), np.uint16)
+            out.top, out.digits = ptr(top).value, ptr(dig).value
+        else:
+            m = np.zeros((C, 4, L, N162), np.int16)
+            out.matrix = ptr(m).value
+        p0 = np.zeros((I, self.row_log, 3), np.uint64)
+        p1 = np.zeros((sum(self.column_log_lens), 3), np.uint64)
+        mle = np.zeros((I, 3), np.uint64)
+        u = np.zeros((C, 3), np.uint64)
+        ch = np.zeros(C, _CH)
+        v = np.zeros((I, self.len_ring, N), np.int16)
+        for name, a in (("p0", p0), ("p1", p1), ("mle", mle), ("u", u), ("challenges", ch), ("v", v)):
+            setattr(out, name, ptr(a).value)
+        d = np.frombuffer(bytes(domain), np.uint8).copy()
+        check(lib().lbg_batch_round(self._h, ptr(d), len(d), ctypes.byref(out)))
+        rounds = []
+        po = 0
+        for i in range(I):
+            a, b = int(self.col_off[i]), int(self.col_off[i + 1])
+            r = InstanceRound()
+            if self.dropped:
+                r.top, r.digits = top[a * N:b * N].copy(), dig[: L - 1, a * N:b * N].copy()
+            else:
+                r.matrix = m[a:b].copy()
+            cl = self.column_log_lens[i]
+            r.p0, r.p1 = p0[i].copy(), p1[po:po + cl].copy()
+            po += cl
+            r.mle, r.u, r.challenges, r.v = mle[i].copy(), u[a:b].copy(), ch[a:b].copy(), v[i]
+            rounds.append(r)
         return rounds
 
     def launch_count(self) -> int:

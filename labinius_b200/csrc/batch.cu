@@ -19,6 +19,8 @@
 #include "handles.h"
 #include "launch.h"
 #include "ring_tables.h"
+#include "transcript.h"
+#include "transcript_dev.h"
 
 using namespace lbg;
 
@@ -65,14 +67,32 @@ struct lbg_batch {
   uint32_t* d_vhat = nullptr;     // [count][wdim][162]
   int16_t* d_v = nullptr;         // [count][len_ring][648]
   bool graphs = false;
-  cudaGraphExec_t g_commit = nullptr, g_fold = nullptr;
+  cudaGraphExec_t g_commit = nullptr, g_fold = nullptr, g_round = nullptr;
   uint64_t launches = 0;
+  // the round on the device: per-instance transcripts, planned once per layout and domain
+  bool plan_ok = false;
+  std::string plan_domain;
+  AbsorbPlan ab_commit, ab_u;
+  SamplerTables sampler;
+  HasherState* d_prefix = nullptr;  // [cap_instances]: each transcript up to the commitment's bytes
+  HasherState* d_states = nullptr;  // [cap_instances]: the transcripts during the round
+  RoundInst* d_inst = nullptr;      // [cap_instances]
+  uint32_t* d_oldcv = nullptr;      // [cap_instances][8]
+  uint8_t* d_stage = nullptr;
+  size_t stage_cap = 0;
+  uint32_t* d_cvs = nullptr;
+  size_t cvs_cap = 0;
+  uint8_t* d_packed = nullptr;      // bit-dropped commitments as absorbed
+  size_t packed_cap = 0;
+  std::vector<uint64_t> packed_off, packed_len;
+  PackDropped pack{};
 };
 
 static void free_graphs(lbg_batch* b) {
   if (b->g_commit) cudaGraphExecDestroy(b->g_commit);
   if (b->g_fold) cudaGraphExecDestroy(b->g_fold);
-  b->g_commit = b->g_fold = nullptr;
+  if (b->g_round) cudaGraphExecDestroy(b->g_round);
+  b->g_commit = b->g_fold = b->g_round = nullptr;
 }
 
 // The device work of each stage, enqueued on the batch's stream (also what the graphs capture).
@@ -156,6 +176,154 @@ static float time_stage(lbg_batch* b, F enqueue) {
   return ts[1];
 }
 
+// ---------------------------------------------------------------------------------------------
+// the whole round on the device
+// ---------------------------------------------------------------------------------------------
+static cudaError_t grow(void** p, size_t* cap, size_t bytes) {
+  if (bytes <= *cap) return cudaSuccess;
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess) *cap = bytes;
+  return e;
+}
+
+static void le64(uint64_t x, uint8_t* b) {
+  for (int i = 0; i < 8; i++) b[i] = (uint8_t)(x >> (8 * i));
+}
+
+// Each instance's transcript up to the commitment's own bytes (host, once per layout and domain),
+// the byte layout of the two device absorbs (the commitment; the row values with their framing)
+// and the derivation counters. The transcript steps are those of derive_evaluation_point and
+// FoldingChallenges::derive (crates/pcs/src/scheme/verifier.rs:41-100,
+// crates/pcs/src/scheme/commitment.rs:217-229).
+static int plan_round(lbg_batch* b, const uint8_t* domain, size_t domain_len) {
+  const lbg_pp* pp = b->pp;
+  int L = pp->limbs;
+  bool dropped = pp->params.opening == LBG_OPENING_BIT_DROPPED;
+  uint32_t row_log = pp->params.witness_log_len - pp->params.column_log_len;
+  RoundShape base;
+  base.limbs = (uint32_t)L;
+  base.dropped_bits = dropped ? pp->params.dropped_bits : 0;
+  for (int k = 0; k < 8; k++) base.primes[k] = k < L ? pp->primes[k] : 0;
+  std::memcpy(base.matrix_seed, pp->seed, 32);
+  // bit-dropped commitments as the transcript reads them (crates/pcs/src/wire/mod.rs:386-397)
+  b->packed_off.assign(1, 0);
+  b->packed_len.clear();
+  if (dropped) {
+    PackDropped pk{};
+    pk.limbs = (uint32_t)L;
+    pk.top_bits = top_bits(pp->primes[0], pp->params.dropped_bits);
+    pk.bits_per = pk.top_bits;
+    for (int k = 1; k < L; k++) {
+      pk.residue_bits[k] = residue_bits(pp->primes[k]);
+      pk.bits_per += pk.residue_bits[k];
+    }
+    b->pack = pk;
+    for (int i = 0; i < b->count; i++) {
+      uint64_t count = (uint64_t)(b->col_off[i + 1] - b->col_off[i]) * N648;
+      uint64_t bytes = (count * pk.bits_per + 7) / 8;
+      b->packed_len.push_back(bytes);
+      b->packed_off.push_back(b->packed_off.back() + (bytes + 15) / 16 * 16);
+    }
+    LBG_BCU(grow((void**)&b->d_packed, &b->packed_cap, b->packed_off.back()));
+  }
+  b->ab_commit.clear();
+  b->ab_u.clear();
+  std::vector<HasherState> pre(b->count);
+  std::vector<RoundInst> ri(b->count);
+  for (int i = 0; i < b->count; i++) {
+    RoundShape s = base;
+    s.column_log_len = b->col_log[i];
+    s.witness_log_len = row_log + b->col_log[i];
+    Transcript t(domain, domain_len);
+    absorb_commitment_header(s, t);
+    t.state().save(pre[i]);
+    uint64_t len0 = absorbed_len(pre[i]);
+    uint64_t cols = b->col_off[i + 1] - b->col_off[i];
+    AbsorbSource sc;
+    std::memset(&sc, 0, sizeof(sc));
+    if (!dropped) {
+      // absorb_elements per column: le64(4), then the column's 4 x limbs x 162 i16, little-endian
+      le64(4, sc.hdr);
+      sc.hdr_len = 8;
+      sc.rows = (uint32_t)cols;
+      sc.row_bytes = (uint32_t)(4 * L * N162 * 2);
+      sc.row_stride = sc.row_bytes;
+      sc.data = (const uint8_t*)(b->d_C + b->col_off[i] * 4 * L * N162);
+    } else {
+      le64(b->packed_len[i], sc.prefix);
+      sc.prefix_len = 8;
+      sc.rows = 1;
+      sc.row_bytes = (uint32_t)b->packed_len[i];
+      sc.row_stride = 0;
+      sc.data = b->d_packed + b->packed_off[i];
+    }
+    plan_absorb(b->ab_commit, b->d_states + i, len0, sc);
+    // absorb_bytes("labinius/row-evaluation"), absorb_bytes(u as 24-byte F162)
+    AbsorbSource su;
+    std::memset(&su, 0, sizeof(su));
+    le64(23, su.prefix);
+    std::memcpy(su.prefix + 8, "labinius/row-evaluation", 23);
+    le64(24 * cols, su.prefix + 31);
+    su.prefix_len = 39;
+    su.rows = 1;
+    su.row_bytes = (uint32_t)(24 * cols);
+    su.data = (const uint8_t*)(b->d_u + 3 * b->col_off[i]);
+    plan_absorb(b->ab_u, b->d_states + i, len0 + sc.length(), su);
+    ri[i].st = b->d_states + i;
+    ri[i].point_counter = t.counter();
+    ri[i].chal_counter = t.counter() + 1;
+    ri[i].row_log = row_log;
+    ri[i].col_log = b->col_log[i];
+    ri[i].col_off = (uint32_t)b->col_off[i];
+    ri[i].pad_ = 0;
+  }
+  LBG_BCU(cudaMemcpy(b->d_prefix, pre.data(), pre.size() * sizeof(HasherState), cudaMemcpyHostToDevice));
+  LBG_BCU(cudaMemcpy(b->d_inst, ri.data(), ri.size() * sizeof(RoundInst), cudaMemcpyHostToDevice));
+  LBG_BCU(upload_absorb(b->ab_commit));
+  LBG_BCU(upload_absorb(b->ab_u));
+  LBG_BCU(grow((void**)&b->d_stage, &b->stage_cap, std::max(b->ab_commit.stage_bytes, b->ab_u.stage_bytes)));
+  LBG_BCU(grow((void**)&b->d_cvs, &b->cvs_cap, 32 * std::max(b->ab_commit.cv_slots, b->ab_u.cv_slots)));
+  LBG_BCU(sampler_tables(pp->device, b->sampler));
+  b->plan_domain.assign((const char*)domain, domain_len);
+  b->plan_ok = true;
+  if (b->g_round) {
+    cudaGraphExecDestroy(b->g_round);
+    b->g_round = nullptr;
+  }
+  return LBG_OK;
+}
+
+static cudaError_t enqueue_round(lbg_batch* b) {
+  const lbg_pp* pp = b->pp;
+  int row_log = (int)(pp->params.witness_log_len - pp->params.column_log_len);
+  int cols = (int)b->total_cols;
+  cudaError_t e = cudaMemcpyAsync(b->d_states, b->d_prefix, (size_t)b->count * sizeof(HasherState),
+                                  cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = enqueue_commit(b);
+  if (e == cudaSuccess && pp->params.opening == LBG_OPENING_BIT_DROPPED) {
+    uint64_t stride = (uint64_t)b->total_cols * N648;
+    for (int i = 0; i < b->count && e == cudaSuccess; i++) {
+      uint64_t o = (uint64_t)b->col_off[i] * N648;
+      e = launch_pack_dropped(b->d_top + o, b->d_digits + o, (uint64_t)(b->col_off[i + 1] - b->col_off[i]) * N648,
+                              stride, b->pack, b->d_packed + b->packed_off[i], b->packed_len[i], b->stream);
+    }
+    b->launches += b->count;
+  }
+  if (e == cudaSuccess) e = launch_absorb(b->ab_commit, b->d_stage, b->d_cvs, b->d_oldcv, b->stream);
+  if (e == cudaSuccess) e = launch_point(b->d_inst, b->count, (uint32_t)row_log, b->d_p0, b->d_p1, b->stream);
+  if (e == cudaSuccess) e = launch_eq_table(b->d_p0, row_log, b->wdim, b->d_eq, b->stream, b->count);
+  if (e == cudaSuccess) e = launch_row_eval(b->d_w, b->wdim, cols, b->d_eq, b->d_u, b->stream, b->d_col_inst);
+  if (e == cudaSuccess) e = launch_claims(b->d_inst, b->d_col_inst, b->d_u, cols, b->d_p1, b->count, b->d_claim, b->stream);
+  if (e == cudaSuccess) e = launch_absorb(b->ab_u, b->d_stage, b->d_cvs, b->d_oldcv, b->stream);
+  if (e == cudaSuccess) e = launch_challenges(b->d_inst, b->d_col_inst, cols, b->sampler, b->d_ch, b->stream);
+  if (e == cudaSuccess) e = enqueue_fold(b);
+  b->launches += 11;
+  return e;
+}
+
 extern "C" {
 
 void lbg_batch_free(lbg_batch* b) {
@@ -164,8 +332,11 @@ void lbg_batch_free(lbg_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   free_graphs(b);
   void* ptrs[] = {b->d_w, b->d_col_inst, b->d_split_inst, b->d_partial, b->d_C, b->d_res, b->d_top, b->d_digits,
-                  b->d_p0, b->d_p1, b->d_eq, b->d_u, b->d_claim, b->d_ch, b->d_chat, b->d_vhat, b->d_v};
+                  b->d_p0, b->d_p1, b->d_eq, b->d_u, b->d_claim, b->d_ch, b->d_chat, b->d_vhat, b->d_v,
+                  b->d_prefix, b->d_states, b->d_inst, b->d_oldcv, b->d_stage, b->d_cvs, b->d_packed};
   for (void* p : ptrs) cudaFree(p);
+  b->ab_commit.release();
+  b->ab_u.release();
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -209,7 +380,11 @@ int lbg_batch_new_capacity(const lbg_pp* pp, size_t max_cols, size_t max_instanc
             cudaMalloc((void**)&b->d_ch, C * sizeof(lbg_challenge_d)) == cudaSuccess &&
             cudaMalloc((void**)&b->d_chat, C * N162 * 4) == cudaSuccess &&
             cudaMalloc((void**)&b->d_vhat, I * b->wdim * N162 * 4) == cudaSuccess &&
-            cudaMalloc((void**)&b->d_v, I * b->len_ring * N648 * 2) == cudaSuccess;
+            cudaMalloc((void**)&b->d_v, I * b->len_ring * N648 * 2) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_prefix, I * sizeof(HasherState)) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_states, I * sizeof(HasherState)) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_inst, I * sizeof(RoundInst)) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_oldcv, I * 32) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     return bail(fail(LBG_ERR_OOM, "batch: device allocation failed"));
@@ -245,6 +420,7 @@ int lbg_batch_assign(lbg_batch* b, const uint32_t* column_log_lens, size_t count
     free_graphs(b);
     b->graphs = false;
   }
+  b->plan_ok = false;
   b->count = (int)count;
   b->col_log = cl;
   b->col_off = off;
@@ -488,6 +664,71 @@ int lbg_batch_fold(lbg_batch* b, const lbg_challenge* challenges, size_t r, int1
     LBG_BCU(cudaMemcpyAsync(v_out, b->d_v, (size_t)b->count * b->len_ring * N648 * 2, cudaMemcpyDeviceToHost,
                             b->stream));
     LBG_BCU(cudaStreamSynchronize(b->stream));
+  }
+  return LBG_OK;
+}
+
+int lbg_batch_round(lbg_batch* b, const uint8_t* domain, size_t domain_len, const lbg_batch_outputs* out) {
+  if (!b || (!domain && domain_len)) return fail(LBG_ERR_INVALID, "null argument");
+  if (b->count == 0) return fail(LBG_ERR_INVALID, "no instances assigned");
+  const lbg_pp* pp = b->pp;
+  LBG_BCU(cudaSetDevice(pp->device));
+  std::string dom((const char*)domain, domain_len);
+  if (!b->plan_ok || b->plan_domain != dom) {
+    LBG_BCU(cudaStreamSynchronize(b->stream));
+    int rc = plan_round(b, domain, domain_len);
+    if (rc) return rc;
+  }
+  uint64_t per_round = 11 + 2 * pp->limbs + 3 +
+                       (pp->params.opening == LBG_OPENING_BIT_DROPPED ? pp->limbs + 1 + b->count : 0);
+  if (b->graphs) {
+    if (!b->g_round) {
+      cudaGraph_t g = nullptr;
+      uint64_t before = b->launches;
+      LBG_BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      cudaError_t e = enqueue_round(b);
+      cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+      b->launches = before;
+      if (e != cudaSuccess || e2 != cudaSuccess) return fail(LBG_ERR_CUDA, "graph capture (round)");
+      e = cudaGraphInstantiate(&b->g_round, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(LBG_ERR_CUDA, "graph instantiate (round)");
+    }
+    LBG_BCU(cudaGraphLaunch(b->g_round, b->stream));
+    b->launches += per_round;
+  } else {
+    LBG_BCU(enqueue_round(b));
+  }
+  size_t C = b->total_cols, count = C * N648;
+  int L = pp->limbs;
+  int row_log = (int)(pp->params.witness_log_len - pp->params.column_log_len);
+  std::vector<lbg_challenge> ch(C);
+  std::vector<uint64_t> p1(out && out->p1 ? (size_t)b->count * 32 * 3 : 0);
+  cudaStream_t st = b->stream;
+  LBG_BCU(cudaMemcpyAsync(ch.data(), b->d_ch, C * sizeof(lbg_challenge), cudaMemcpyDeviceToHost, st));
+  if (out) {
+    if (out->matrix) LBG_BCU(cudaMemcpyAsync(out->matrix, b->d_C, C * 4 * L * N162 * 2, cudaMemcpyDeviceToHost, st));
+    if (out->top) LBG_BCU(cudaMemcpyAsync(out->top, b->d_top, count * 2, cudaMemcpyDeviceToHost, st));
+    if (out->digits && L > 1)
+      LBG_BCU(cudaMemcpyAsync(out->digits, b->d_digits, (size_t)(L - 1) * count * 2, cudaMemcpyDeviceToHost, st));
+    if (out->p0)
+      LBG_BCU(cudaMemcpyAsync(out->p0, b->d_p0, (size_t)b->count * row_log * 24, cudaMemcpyDeviceToHost, st));
+    if (out->p1) LBG_BCU(cudaMemcpyAsync(p1.data(), b->d_p1, p1.size() * 8, cudaMemcpyDeviceToHost, st));
+    if (out->mle) LBG_BCU(cudaMemcpyAsync(out->mle, b->d_claim, (size_t)b->count * 24, cudaMemcpyDeviceToHost, st));
+    if (out->u) LBG_BCU(cudaMemcpyAsync(out->u, b->d_u, C * 24, cudaMemcpyDeviceToHost, st));
+    if (out->v)
+      LBG_BCU(cudaMemcpyAsync(out->v, b->d_v, (size_t)b->count * b->len_ring * N648 * 2, cudaMemcpyDeviceToHost, st));
+  }
+  LBG_BCU(cudaStreamSynchronize(st));
+  for (size_t j = 0; j < C; j++)
+    if (ch[j].weight == 0) return fail(LBG_ERR_CUDA, "the device sampler found no challenge for column " + std::to_string(j));
+  if (out && out->challenges) std::memcpy(out->challenges, ch.data(), C * sizeof(lbg_challenge));
+  if (out && out->p1) {
+    size_t o = 0;
+    for (int i = 0; i < b->count; i++) {
+      std::memcpy(out->p1 + o, p1.data() + (size_t)i * 32 * 3, b->col_log[i] * 24);
+      o += 3 * b->col_log[i];
+    }
   }
   return LBG_OK;
 }

@@ -5,8 +5,7 @@
 namespace lbg {
 
 namespace {
-constexpr uint32_t CHUNK_START = 1, CHUNK_END = 2, PARENT = 4, ROOT = 8, KEYED_HASH = 16,
-                   DERIVE_KEY_CONTEXT = 32, DERIVE_KEY_MATERIAL = 64;
+using namespace b3;
 constexpr uint32_t IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
                             0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
 // message word schedule of the seven rounds (the spec's permutation applied r times)
@@ -184,6 +183,31 @@ void Blake3::finalize(uint64_t seek, uint8_t* out, size_t len) const {
     skip = 0;
     b++;
   }
+}
+
+void Blake3::save(HasherState& s) const {
+  std::memset(&s, 0, sizeof(s));
+  std::memcpy(s.key, key_, sizeof(key_));
+  s.flags = flags_;
+  std::memcpy(s.cv, cv_, sizeof(cv_));
+  std::memcpy(s.buf, buf_, sizeof(buf_));
+  s.buf_len = buf_len_;
+  s.blocks = blocks_;
+  s.chunk_counter = chunk_counter_;
+  std::memcpy(s.stack, stack_, sizeof(uint32_t) * 8 * stack_len_);
+  s.stack_len = stack_len_;
+}
+
+void Blake3::load(const HasherState& s) {
+  std::memcpy(key_, s.key, sizeof(key_));
+  flags_ = s.flags;
+  std::memcpy(cv_, s.cv, sizeof(cv_));
+  std::memcpy(buf_, s.buf, sizeof(buf_));
+  buf_len_ = s.buf_len;
+  blocks_ = s.blocks;
+  chunk_counter_ = s.chunk_counter;
+  stack_len_ = s.stack_len;
+  std::memcpy(stack_, s.stack, sizeof(uint32_t) * 8 * stack_len_);
 }
 
 uint8_t Blake3Reader::byte() {

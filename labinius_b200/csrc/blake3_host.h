@@ -7,6 +7,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "hasher_state.h"
+
 namespace lbg {
 
 class Blake3 {
@@ -17,6 +19,12 @@ class Blake3 {
   void update(const void* data, size_t len);
   // Extendable output of everything absorbed so far, bytes [seek, seek + len).
   void finalize(uint64_t seek, uint8_t* out, size_t len) const;
+  // The state as plain data (canonical form, hasher_state.h) and back.
+  void save(HasherState& s) const;
+  void load(const HasherState& s);
+  // The key words and mode flags (the context key of a derive-key hasher).
+  const uint32_t* key_words() const { return key_; }
+  uint32_t mode_flags() const { return flags_; }
 
  private:
   uint32_t key_[8];

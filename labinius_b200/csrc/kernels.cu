@@ -3,6 +3,7 @@
 
 #include "kernels.cuh"
 #include "launch.h"
+#include "transcript_dev.h"
 
 namespace lbg {
 
@@ -535,6 +536,49 @@ __global__ void k_claim(const uint64_t* __restrict__ u, int cols, const uint64_t
   }
 }
 
+// The claims of all instances of a batch at once: one thread per column; a warp whose columns
+// belong to one instance XOR-reduces and adds once, a warp over several instances adds per thread.
+__global__ void k_claims(const RoundInst* __restrict__ inst, const int* __restrict__ col_inst,
+                         const uint64_t* __restrict__ u, int total_cols, const uint64_t* __restrict__ p1,
+                         unsigned long long* __restrict__ out) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int ii = j < total_cols ? col_inst[j] : -1;
+  uint64_t a0 = 0, a1 = 0, a2 = 0;
+  if (ii >= 0) {
+    const RoundInst& I = inst[ii];
+    int jj = j - (int)I.col_off;
+    const uint64_t* p = p1 + 3 * 32 * ii;
+    F162d x{{1, 0, 0}};
+    for (int k = 0; k < (int)I.col_log; k++) {
+      F162d pk{{p[3 * k], p[3 * k + 1], p[3 * k + 2]}};
+      if (!((jj >> k) & 1)) pk.w[0] ^= 1;
+      x = f_mul(x, pk);
+    }
+    F162d y = f_mul(x, F162d{{u[3 * j], u[3 * j + 1], u[3 * j + 2]}});
+    a0 = y.w[0];
+    a1 = y.w[1];
+    a2 = y.w[2];
+  }
+  int i0 = __shfl_sync(0xffffffffu, ii, 0);
+  bool uniform = __all_sync(0xffffffffu, ii == i0 || ii < 0);
+  if (uniform) {
+    for (int o = 16; o > 0; o >>= 1) {
+      a0 ^= __shfl_xor_sync(0xffffffffu, a0, o);
+      a1 ^= __shfl_xor_sync(0xffffffffu, a1, o);
+      a2 ^= __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if ((threadIdx.x & 31) == 0 && i0 >= 0) {
+      atomicXor(out + 3 * i0, (unsigned long long)a0);
+      atomicXor(out + 3 * i0 + 1, (unsigned long long)a1);
+      atomicXor(out + 3 * i0 + 2, (unsigned long long)a2);
+    }
+  } else if (ii >= 0) {
+    atomicXor(out + 3 * ii, (unsigned long long)a0);
+    atomicXor(out + 3 * ii + 1, (unsigned long long)a1);
+    atomicXor(out + 3 * ii + 2, (unsigned long long)a2);
+  }
+}
+
 // =============================================================================================
 // Witness generation: keyed BLAKE3 XOF of "labinius/witness" (crates/pcs/src/scheme/witness.rs:66-87)
 // =============================================================================================
@@ -788,6 +832,15 @@ cudaError_t launch_claim(const uint64_t* u, int cols, const uint64_t* p1, int n,
   cudaError_t e = cudaMemsetAsync(out, 0, 24, st);
   if (e != cudaSuccess) return e;
   k_claim<<<blocks_for(cols, 64), 64, 0, st>>>(u, cols, p1, n, (unsigned long long*)out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_claims(const RoundInst* d_inst, const int* col_inst, const uint64_t* u, int total_cols,
+                          const uint64_t* p1, int count, uint64_t* out, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(out, 0, (size_t)count * 24, st);
+  if (e != cudaSuccess) return e;
+  k_claims<<<blocks_for(total_cols, 128), 128, 0, st>>>(d_inst, col_inst, u, total_cols, p1,
+                                                         (unsigned long long*)out);
   return cudaGetLastError();
 }
 

@@ -101,10 +101,14 @@ bool within(const Challenge& c, double bound_sq) {
   return true;
 }
 
+const Blake3& signs_hasher() {
+  static const Blake3 key = Blake3::derive_key("labinius 2026 challenge signs v1");
+  return key;
+}
+
 // keyed-by-context hash of the position set (crates/pcs/src/challenge.rs:237-269)
 uint32_t signs_of(const Challenge& c) {
-  static const Blake3 key = Blake3::derive_key("labinius 2026 challenge signs v1");
-  Blake3 h = key;
+  Blake3 h = signs_hasher();
   uint8_t b[8];
   le64(c.weight, b);
   h.update(b, 8);
@@ -128,6 +132,10 @@ uint16_t below(Blake3Reader& x, uint16_t n) {
 }
 
 }  // namespace
+
+const double* sampler_phase_re() { return &phase().re[0][0]; }
+const double* sampler_phase_im() { return &phase().im[0][0]; }
+const uint32_t* sampler_signs_key() { return signs_hasher().key_words(); }
 
 Challenge sample_short_challenge(Transcript& t, uint32_t weight, double bound, uint64_t* attempts) {
   volatile double b2 = bound * bound;
@@ -192,8 +200,7 @@ std::vector<uint8_t> pack_dropped(const RoundShape& s, const uint16_t* top, cons
   return out;
 }
 
-void derive_evaluation_point(const RoundShape& s, Transcript& t, const int16_t* matrix,
-                             const uint16_t* top, const uint16_t* digits, uint64_t* p0, uint64_t* p1) {
+void absorb_commitment_header(const RoundShape& s, Transcript& t) {
   t.absorb_bytes((const uint8_t*)"labinius/parameters", 19);
   t.absorb_u64(s.witness_log_len);
   t.absorb_u64(s.column_log_len);
@@ -206,18 +213,10 @@ void derive_evaluation_point(const RoundShape& s, Transcript& t, const int16_t* 
   t.absorb_bytes(s.matrix_seed, 32);
   t.absorb_bytes((const uint8_t*)"labinius/commitment", 19);
   t.absorb_u64(s.columns());
-  if (s.dropped_bits == 0) {
-    // absorb_elements per column: the element count (4), then each element's limbs as LE i16
-    size_t per_col = 4 * (size_t)s.limbs * 162;
-    for (size_t j = 0; j < s.columns(); j++) {
-      t.absorb_u64(4);
-      t.absorb_raw((const uint8_t*)(matrix + j * per_col), per_col * 2);  // little-endian host
-    }
-  } else {
-    t.absorb_bytes((const uint8_t*)"labinius/dropped-commitment", 27);
-    std::vector<uint8_t> b = pack_dropped(s, top, digits);
-    t.absorb_bytes(b.data(), b.size());
-  }
+  if (s.dropped_bits > 0) t.absorb_bytes((const uint8_t*)"labinius/dropped-commitment", 27);
+}
+
+void evaluation_point_from(const RoundShape& s, Transcript& t, uint64_t* p0, uint64_t* p1) {
   size_t rows = s.row_log_len(), cols = s.column_log_len;
   std::vector<uint8_t> bytes(24 * (rows + cols));
   t.fill("labinius/evaluation-point", bytes.data(), bytes.size());
@@ -228,6 +227,23 @@ void derive_evaluation_point(const RoundShape& s, Transcript& t, const int16_t* 
     uint64_t* dst = i < rows ? p0 + 3 * i : p1 + 3 * (i - rows);
     std::memcpy(dst, limb, 24);
   }
+}
+
+void derive_evaluation_point(const RoundShape& s, Transcript& t, const int16_t* matrix,
+                             const uint16_t* top, const uint16_t* digits, uint64_t* p0, uint64_t* p1) {
+  absorb_commitment_header(s, t);
+  if (s.dropped_bits == 0) {
+    // absorb_elements per column: the element count (4), then each element's limbs as LE i16
+    size_t per_col = 4 * (size_t)s.limbs * 162;
+    for (size_t j = 0; j < s.columns(); j++) {
+      t.absorb_u64(4);
+      t.absorb_raw((const uint8_t*)(matrix + j * per_col), per_col * 2);  // little-endian host
+    }
+  } else {
+    std::vector<uint8_t> b = pack_dropped(s, top, digits);
+    t.absorb_bytes(b.data(), b.size());
+  }
+  evaluation_point_from(s, t, p0, p1);
 }
 
 void derive_folding_challenges(const RoundShape& s, Transcript& t, const uint64_t* u, Challenge* out) {

@@ -26,11 +26,22 @@ class Transcript {
   void absorb_raw(const uint8_t* b, size_t len) { state_.update(b, len); }
   void fill(const char* label, uint8_t* out, size_t n);
   Blake3 derive(const char* label);
+  // The absorbing state and the derivation counter, for moving the transcript to the device.
+  const Blake3& state() const { return state_; }
+  Blake3& state() { return state_; }
+  uint64_t counter() const { return counter_; }
+  void set_counter(uint64_t c) { counter_ = c; }
 
  private:
   Blake3 state_;
   uint64_t counter_ = 0;
 };
+
+// The sampler's tables for the device copy of it: exp(2 pi i p u_k / 243) as re/im [162][81]
+// doubles, and the context key (8 words) of the sign hash.
+const double* sampler_phase_re();
+const double* sampler_phase_im();
+const uint32_t* sampler_signs_key();
 
 // crates/pcs/src/challenge.rs:517-533
 Challenge sample_short_challenge(Transcript& t, uint32_t weight, double bound, uint64_t* attempts);
@@ -44,6 +55,11 @@ struct RoundShape {
   uint32_t row_log_len() const { return witness_log_len - column_log_len; }
 };
 
+// The steps of derive_evaluation_point (crates/pcs/src/scheme/verifier.rs:41-100):
+// the parameters and the commitment's framing (everything up to the commitment's own bytes) ...
+void absorb_commitment_header(const RoundShape& s, Transcript& t);
+// ... and, once the commitment's bytes are absorbed, the point itself.
+void evaluation_point_from(const RoundShape& s, Transcript& t, uint64_t* p0, uint64_t* p1);
 // crates/pcs/src/scheme/verifier.rs:41-100
 void derive_evaluation_point(const RoundShape& s, Transcript& t, const int16_t* matrix,
                              const uint16_t* top, const uint16_t* digits, uint64_t* p0, uint64_t* p1);
