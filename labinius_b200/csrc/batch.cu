@@ -49,6 +49,8 @@ struct lbg_batch {
   cudaStream_t stream = nullptr;
   uint64_t* d_w = nullptr;        // [total_cols * wdim][3]
   int* d_col_inst = nullptr;      // [total_cols]
+  int4* d_row_tiles = nullptr;    // row-evaluation tiles: (first column, columns, instance)
+  int n_row_tiles = 0;
   int* d_split_inst = nullptr;    // [total_cols] (at most one split per column)
   int chunk = 0, nchunks = 0, fold_per = 0;
   int32_t* d_partial = nullptr;   // [max_chunks][total_cols][162][4]
@@ -315,7 +317,7 @@ static cudaError_t enqueue_round(lbg_batch* b) {
   if (e == cudaSuccess) e = launch_absorb(b->ab_commit, b->d_stage, b->d_cvs, b->d_oldcv, b->stream);
   if (e == cudaSuccess) e = launch_point(b->d_inst, b->count, (uint32_t)row_log, b->d_p0, b->d_p1, b->stream);
   if (e == cudaSuccess) e = launch_eq_table(b->d_p0, row_log, b->wdim, b->d_eq, b->stream, b->count);
-  if (e == cudaSuccess) e = launch_row_eval(b->d_w, b->wdim, cols, b->d_eq, b->d_u, b->stream, b->d_col_inst);
+  if (e == cudaSuccess) e = launch_row_eval(b->d_w, b->wdim, cols, b->d_eq, b->d_u, b->stream, b->d_row_tiles, b->n_row_tiles);
   if (e == cudaSuccess) e = launch_claims(b->d_inst, b->d_col_inst, b->d_u, cols, b->d_p1, b->count, b->d_claim, b->stream);
   if (e == cudaSuccess) e = launch_absorb(b->ab_u, b->d_stage, b->d_cvs, b->d_oldcv, b->stream);
   if (e == cudaSuccess) e = launch_challenges(b->d_inst, b->d_col_inst, cols, b->sampler, b->d_ch, b->stream);
@@ -331,7 +333,7 @@ void lbg_batch_free(lbg_batch* b) {
   cudaSetDevice(b->pp->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   free_graphs(b);
-  void* ptrs[] = {b->d_w, b->d_col_inst, b->d_split_inst, b->d_partial, b->d_C, b->d_res, b->d_top, b->d_digits,
+  void* ptrs[] = {b->d_w, b->d_col_inst, b->d_row_tiles, b->d_split_inst, b->d_partial, b->d_C, b->d_res, b->d_top, b->d_digits,
                   b->d_p0, b->d_p1, b->d_eq, b->d_u, b->d_claim, b->d_ch, b->d_chat, b->d_vhat, b->d_v,
                   b->d_prefix, b->d_states, b->d_inst, b->d_oldcv, b->d_stage, b->d_cvs, b->d_packed};
   for (void* p : ptrs) cudaFree(p);
@@ -366,6 +368,7 @@ int lbg_batch_new_capacity(const lbg_pp* pp, size_t max_cols, size_t max_instanc
   if (b->max_chunks > 64) b->max_chunks = 64;
   bool ok = cudaMalloc((void**)&b->d_w, n * 24) == cudaSuccess &&
             cudaMalloc((void**)&b->d_col_inst, C * sizeof(int)) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_row_tiles, C * sizeof(int4)) == cudaSuccess &&
             cudaMalloc((void**)&b->d_split_inst, C * sizeof(int)) == cudaSuccess &&
             cudaMalloc((void**)&b->d_partial, (size_t)b->max_chunks * C * N162 * 16) == cudaSuccess &&
             cudaMalloc((void**)&b->d_C, C * 4 * L * N162 * 2) == cudaSuccess &&
@@ -430,6 +433,13 @@ int lbg_batch_assign(lbg_batch* b, const uint32_t* column_log_lens, size_t count
   for (int i = 0; i < b->count; i++)
     for (size_t c = off[i]; c < off[i + 1]; c++) ci[c] = i;
   LBG_BCU(cudaMemcpy(b->d_col_inst, ci.data(), ci.size() * sizeof(int), cudaMemcpyHostToDevice));
+  std::vector<int4> rtiles;
+  int tc = row_eval_tile_cols();
+  for (int i = 0; i < b->count; i++)
+    for (size_t c = off[i]; c < off[i + 1]; c += tc)
+      rtiles.push_back(make_int4((int)c, (int)std::min<size_t>(tc, off[i + 1] - c), i, 0));
+  LBG_BCU(cudaMemcpy(b->d_row_tiles, rtiles.data(), rtiles.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  b->n_row_tiles = (int)rtiles.size();
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pp->device);
   long tiles = (long)((b->total_cols + commit_cols_per_cta() - 1) / commit_cols_per_cta());
@@ -621,7 +631,7 @@ int lbg_batch_row_evaluate(lbg_batch* b, const uint64_t* p0, uint64_t* u_out) {
   LBG_BCU(cudaSetDevice(b->pp->device));
   LBG_BCU(cudaMemcpyAsync(b->d_p0, p0, (size_t)b->count * row_log * 24, cudaMemcpyHostToDevice, b->stream));
   LBG_BCU(launch_eq_table(b->d_p0, row_log, b->wdim, b->d_eq, b->stream, b->count));
-  LBG_BCU(launch_row_eval(b->d_w, b->wdim, (int)b->total_cols, b->d_eq, b->d_u, b->stream, b->d_col_inst));
+  LBG_BCU(launch_row_eval(b->d_w, b->wdim, (int)b->total_cols, b->d_eq, b->d_u, b->stream, b->d_row_tiles, b->n_row_tiles));
   b->launches += 2;
   LBG_BCU(cudaMemcpyAsync(u_out, b->d_u, b->total_cols * 24, cudaMemcpyDeviceToHost, b->stream));
   LBG_BCU(cudaStreamSynchronize(b->stream));
@@ -635,7 +645,7 @@ int lbg_batch_mle_evaluate(lbg_batch* b, const uint64_t* p0, const uint64_t* p1,
   LBG_BCU(cudaSetDevice(b->pp->device));
   LBG_BCU(cudaMemcpyAsync(b->d_p0, p0, (size_t)b->count * row_log * 24, cudaMemcpyHostToDevice, b->stream));
   LBG_BCU(launch_eq_table(b->d_p0, row_log, b->wdim, b->d_eq, b->stream, b->count));
-  LBG_BCU(launch_row_eval(b->d_w, b->wdim, (int)b->total_cols, b->d_eq, b->d_u, b->stream, b->d_col_inst));
+  LBG_BCU(launch_row_eval(b->d_w, b->wdim, (int)b->total_cols, b->d_eq, b->d_u, b->stream, b->d_row_tiles, b->n_row_tiles));
   size_t off = 0;
   for (int i = 0; i < b->count; i++) {
     int cl = (int)b->col_log[i];

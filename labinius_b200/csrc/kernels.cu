@@ -1,6 +1,8 @@
 // Kernels of the B200 prover path. Launch wrappers at the bottom dispatch on the prime index.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "kernels.cuh"
 #include "launch.h"
 #include "transcript_dev.h"
@@ -457,52 +459,120 @@ __global__ void k_eq_table(const uint64_t* __restrict__ p, int n, size_t count, 
   eq[3 * i + 2] = x.w[2];
 }
 
-// One CTA per column: thread b < 162 accumulates S_b = sum over rows i with bit b of W[i] set of
-// eq[i]; then u = sum_b x^b S_b reduced modulo x^162 + x^81 + 1.
-__global__ void __launch_bounds__(192) k_row_eval(const uint64_t* __restrict__ W, size_t wdim,
-                                                  const uint64_t* __restrict__ eq, uint64_t* __restrict__ u,
-                                                  const int* __restrict__ col_inst) {
-  __shared__ uint64_t S[N162][3];
-  const int b = threadIdx.x;
-  const int j = blockIdx.x;
-  if (col_inst) eq += (size_t)col_inst[j] * wdim * 3;  // many instances: each column its own eq table
-  const uint64_t* col = W + (size_t)j * wdim * 3;
-  uint64_t a0 = 0, a1 = 0, a2 = 0;
-  if (b < N162) {
-    const int limb = b >> 6, sh = b & 63;
-    for (size_t i = 0; i < wdim; i++) {
-      uint64_t m = 0 - ((__ldg(col + 3 * i + limb) >> sh) & 1);
-      a0 ^= __ldg(eq + 3 * i) & m;
-      a1 ^= __ldg(eq + 3 * i + 1) & m;
-      a2 ^= __ldg(eq + 3 * i + 2) & m;
+// Row evaluation by the method of four Russians over 8-row groups (crates/pcs/src/eval.rs:136-193
+// computes the same sums one row at a time): u_j = sum_b x^b S_{j,b} mod x^162 + x^81 + 1 with
+// S_{j,b} = XOR of eq[i] over the rows i whose W[i][j] has bit b set. For a group of 8 rows the
+// 256 XOR-combinations of their eq values form a table T (built once per CTA and group, shared by
+// the CTA's columns); bit b of the 8 rows of column j, read as an 8-bit index, selects T's entry
+// to add to S_{j,b}. A thread owns one byte position m of one column (bits 8m .. 8m+7): it loads
+// the 8 rows' words, transposes the 8x8 bit block, and makes 8 lookups. CTAs split the rows;
+// partial results are combined with atomic XORs into u (zeroed first).
+constexpr int RE_COLS = 12;      // columns per CTA (12 x 21 byte positions = 252 threads)
+constexpr int RE_THREADS = 256;
+
+__device__ __forceinline__ uint64_t transpose8x8(uint64_t x) {
+  // byte k bit r -> byte r bit k
+  uint64_t t;
+  t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+  x = x ^ t ^ (t << 7);
+  t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+  x = x ^ t ^ (t << 14);
+  t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+  x = x ^ t ^ (t << 28);
+  return x;
+}
+
+__global__ void __launch_bounds__(RE_THREADS) k_row_eval(const uint64_t* __restrict__ W, int wdim, int cols,
+                                                         const uint64_t* __restrict__ eq_all,
+                                                         const int4* __restrict__ tiles, int groups_per_split,
+                                                         unsigned long long* __restrict__ u) {
+  __shared__ uint64_t T[256][3];
+  __shared__ uint64_t L4[2][16][3];
+  __shared__ uint64_t Q[RE_COLS][21][4];
+  int4 tile;
+  if (tiles) tile = tiles[blockIdx.x];
+  else tile = make_int4(RE_COLS * blockIdx.x, min(RE_COLS, cols - RE_COLS * (int)blockIdx.x), 0, 0);
+  const uint64_t* eq = eq_all + (size_t)tile.z * wdim * 3;
+  const int t = threadIdx.x;
+  const int c = t / 21, m = t - 21 * (t / 21);
+  const bool active = c < tile.y;
+  const int limb = m >> 3, sh = 8 * (m & 7);
+  const uint64_t* col = W + ((size_t)(tile.x + (active ? c : 0)) * wdim) * 3 + limb;
+  const int G = wdim >> 3;
+  const int g0 = blockIdx.y * groups_per_split, g1 = min(G, g0 + groups_per_split);
+  uint64_t S[8][3];
+#pragma unroll
+  for (int r = 0; r < 8; r++) S[r][0] = S[r][1] = S[r][2] = 0;
+  for (int g = g0; g < g1; g++) {
+    __syncthreads();  // the previous group's lookups are done with T
+    if (t < 32) {
+      // 16 combinations of rows 0..3 (t < 16) or 4..7 of the group
+      const uint64_t* e = eq + (size_t)(8 * g + 4 * (t >> 4)) * 3;
+      uint64_t a0 = 0, a1 = 0, a2 = 0;
+      for (int k = 0; k < 4; k++)
+        if ((t >> k) & 1) {
+          a0 ^= __ldg(e + 3 * k);
+          a1 ^= __ldg(e + 3 * k + 1);
+          a2 ^= __ldg(e + 3 * k + 2);
+        }
+      L4[t >> 4][t & 15][0] = a0;
+      L4[t >> 4][t & 15][1] = a1;
+      L4[t >> 4][t & 15][2] = a2;
     }
-    S[b][0] = a0;
-    S[b][1] = a1;
-    S[b][2] = a2;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 3; q++) T[t][q] = L4[0][t & 15][q] ^ L4[1][t >> 4][q];
+    __syncthreads();
+    if (active) {
+      uint64_t x = 0;
+#pragma unroll
+      for (int k = 0; k < 8; k++) x |= ((__ldg(col + (size_t)(8 * g + k) * 3) >> sh) & 0xFF) << (8 * k);
+      x = transpose8x8(x);
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        const uint64_t* e = T[(x >> (8 * r)) & 0xFF];
+        S[r][0] ^= e[0];
+        S[r][1] ^= e[1];
+        S[r][2] ^= e[2];
+      }
+    }
+  }
+  // this thread's share of sum_b x^b S_b: bits 8m + r, placed from word `limb` on
+  if (active) {
+    uint64_t q4[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      if (8 * m + r >= 162) break;
+      int bs = sh + r;
+#pragma unroll
+      for (int w = 0; w < 3; w++) {
+        q4[w] ^= S[r][w] << bs;
+        if (bs) q4[w + 1] ^= S[r][w] >> (64 - bs);
+      }
+    }
+#pragma unroll
+    for (int w = 0; w < 4; w++) Q[c][m][w] = q4[w];
   }
   __syncthreads();
-  if (b == 0) {
-    uint64_t P[6] = {0, 0, 0, 0, 0, 0};
-    for (int bb = 0; bb < N162; bb++) {
-      int ws = bb >> 6, bs = bb & 63;
-      for (int t = 0; t < 3; t++) {
-        uint64_t x = S[bb][t];
-        P[t + ws] ^= x << bs;
-        if (bs) P[t + ws + 1] ^= x >> (64 - bs);
-      }
+  if (active && m == 0) {
+    uint64_t P[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int mm = 0; mm < 21; mm++) {
+      int ws = mm >> 3;
+      for (int w = 0; w < 4; w++) P[ws + w] ^= Q[c][mm][w];
     }
     // reduce bits 322..162 by x^162 = x^81 + 1
     for (int bit = 322; bit >= 162; bit--) {
       if ((P[bit >> 6] >> (bit & 63)) & 1) {
         P[bit >> 6] ^= 1ull << (bit & 63);
-        int a = bit - 162, c = bit - 81;
+        int a = bit - 162, b = bit - 81;
         P[a >> 6] ^= 1ull << (a & 63);
-        P[c >> 6] ^= 1ull << (c & 63);
+        P[b >> 6] ^= 1ull << (b & 63);
       }
     }
-    u[3 * j] = P[0];
-    u[3 * j + 1] = P[1];
-    u[3 * j + 2] = P[2];
+    unsigned long long* dst = u + 3 * (size_t)(tile.x + c);
+    atomicXor(dst, (unsigned long long)P[0]);
+    atomicXor(dst + 1, (unsigned long long)P[1]);
+    atomicXor(dst + 2, (unsigned long long)P[2]);
   }
 }
 
@@ -822,9 +892,23 @@ cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq
   return cudaGetLastError();
 }
 
+int row_eval_tile_cols() { return RE_COLS; }
+
 cudaError_t launch_row_eval(const uint64_t* W, size_t wdim, int cols, const uint64_t* eq, uint64_t* u,
-                            cudaStream_t st, const int* col_inst) {
-  k_row_eval<<<cols, 192, 0, st>>>(W, wdim, eq, u, col_inst);
+                            cudaStream_t st, const int4* tiles, int ntiles) {
+  cudaError_t e = cudaMemsetAsync(u, 0, (size_t)cols * 24, st);
+  if (e != cudaSuccess) return e;
+  if (!tiles) ntiles = (cols + RE_COLS - 1) / RE_COLS;
+  int G = (int)(wdim >> 3);
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // enough CTAs for about four per SM, each with at least 8 groups of rows
+  int splits = std::max(1, std::min(G / 8, (4 * sms + ntiles - 1) / ntiles));
+  int gps = (G + splits - 1) / splits;
+  splits = (G + gps - 1) / gps;
+  k_row_eval<<<dim3(ntiles, splits), RE_THREADS, 0, st>>>(W, (int)wdim, cols, eq, tiles, gps,
+                                                           (unsigned long long*)u);
   return cudaGetLastError();
 }
 

@@ -65,8 +65,12 @@ cudaError_t launch_garner(const uint16_t* res, size_t count, int limbs, const Ga
                           uint16_t* digits, cudaStream_t st);
 cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq, cudaStream_t st,
                             int instances = 1);
+// u (cols F162, zeroed here) = the row evaluations of W's columns against eq. `tiles` (device,
+// x = first column, y = columns (<= row_eval_tile_cols()), z = instance whose eq table
+// eq + z * wdim * 3 applies) covers a batch of instances; null means one instance.
 cudaError_t launch_row_eval(const uint64_t* W, size_t wdim, int cols, const uint64_t* eq, uint64_t* u,
-                            cudaStream_t st, const int* col_inst = nullptr);
+                            cudaStream_t st, const int4* tiles = nullptr, int ntiles = 0);
+int row_eval_tile_cols();
 cudaError_t launch_claim(const uint64_t* u, int cols, const uint64_t* p1, int n, uint64_t* out, cudaStream_t st);
 cudaError_t launch_xof(const XofRoot& root, size_t nbytes, uint8_t* out, cudaStream_t st);
 cudaError_t launch_mask_f162(uint64_t* W, size_t n, cudaStream_t st);

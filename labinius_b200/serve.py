@@ -8,11 +8,13 @@ trace lifted, crates/pcs/src/scheme/witness.rs:45-87).
 Continuous batching: the server owns `slots` device arenas (lbg_batch, sized once; admission is by
 arena room, i.e. by the HBM each slot reserved). Whenever a slot is free it admits, in arrival
 order, every queued request that fits, lays them out in the arena and runs their rounds together:
-each device stage is one launch over all of them, their host steps (transcripts, challenge
-sampling) run in parallel on a thread pool, and while one slot is in its host steps the other
-slot's device stages run on its own stream, so requests that arrive while others are on the GPU
-are admitted as soon as a slot and its memory free up and their work overlaps on the device.
-The parameters, the key and each slot's state stay resident on the device.
+each device stage is one launch over all of them, and the transcripts (absorbs, evaluation point,
+challenge sampling) run on the device too (lbg_batch_round), so a batch is one pass on the
+slot's stream from witness generation to the folded witnesses. While one slot reads its results
+back and lays out its next batch, the other slot's round runs on its own stream: requests that
+arrive while others are on the GPU are admitted as soon as a slot and its memory free up, and
+their work overlaps on the device. The parameters, the key and each slot's state stay resident.
+With transcript="host" the transcript steps run in the library's host code on a thread pool.
 """
 import collections
 import concurrent.futures
@@ -47,12 +49,14 @@ class Request:
 
 class Server:
     def __init__(self, pp: PublicParameters, capacity_columns: int, max_requests: int = 256, slots: int = 2,
-                 host_threads: int = 16, domain: bytes = b"labinius/reference", keep_results: bool = True):
+                 host_threads: int = 16, domain: bytes = b"labinius/reference", keep_results: bool = True,
+                 transcript: str = "device"):
         self.pp = pp
         self.capacity = capacity_columns
         self.max_requests = max_requests
         self.domain = domain
         self.keep_results = keep_results
+        self.transcript = transcript
         self.slots = [Batch(pp, capacity=(capacity_columns, max_requests)) for _ in range(slots)]
         self.pool = concurrent.futures.ThreadPoolExecutor(host_threads)
         self.queue = collections.deque()
@@ -107,7 +111,7 @@ class Server:
             try:
                 b.assign([r.column_log_len for r in reqs])
                 b.witness_random([r.seed for r in reqs], [r.kind for r in reqs])
-                rounds = b.round(self.domain, pool=self.pool)
+                rounds = b.round(self.domain, pool=self.pool, transcript=self.transcript)
                 self.batches += 1
                 err = None
             except Exception as e:  # noqa: BLE001 - reported on every request of the batch

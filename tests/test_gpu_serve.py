@@ -34,13 +34,14 @@ def alone(oracle, row_log, primes, req):
     return c.matrix, point, mle, row.values, ch.challenges, v.elements
 
 
-def test_results_in_the_mix_equal_results_alone(oracle):
+@pytest.mark.parametrize("transcript", ["device", "host"])
+def test_results_in_the_mix_equal_results_alone(oracle, transcript):
     import labinius_b200 as L
     from labinius_b200.serve import Request, Server
 
     row_log, primes = 8, [3889, 9721]
     pp = L.PublicParameters.from_seed(product_params((row_log + 3, 3, primes, 0)), MATRIX_SEED)
-    srv = Server(pp, capacity_columns=48, max_requests=8, slots=2, host_threads=4)
+    srv = Server(pp, capacity_columns=48, max_requests=8, slots=2, host_threads=4, transcript=transcript)
     rng = np.random.default_rng(4)
     reqs = []
     for i in range(14):
