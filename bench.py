@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-ntt", action="store_true")
+    ap.add_argument("--ntt-count", type=int, default=1 << 20, help="ring elements of the NTT microbenchmark")
     ap.add_argument("--served-requests", type=int, default=10000)
     ap.add_argument("--served-plain-sample", type=int, default=200)
     return ap.parse_args()
@@ -299,12 +301,79 @@ def run_batched(instances, steps, flush_bytes=256 << 20):
         seq_wall += (time.perf_counter() - t0) * 1000
     seq_dev /= steps
     seq_wall /= steps
+
+    # the whole round (commit, evaluation point, mle and row evaluation, folding challenges, fold):
+    # the batch's device round (one graph, transcripts on the device, results read back) against one
+    # plain API round per instance, both by the host clock around the calls
+    b.round(DOMAIN, copy=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        b.round(DOMAIN, copy=False)  # results read back into the batch's page-locked buffers
+    round_ms = (time.perf_counter() - t0) * 1000 / steps
+    verifiers = {c: L.Verifier(pps[c]) for c in pps}
+
+    def plain_round(i):
+        c = col_logs[i]
+        cm, op = provers[c].commit(wits[i])
+        t = L.Transcript(DOMAIN)
+        point = verifiers[c].derive_evaluation_point(t, cm)
+        wits[i].mle_evaluate(point)
+        row = wits[i].row_evaluate(point)
+        ch = verifiers[c].derive_folding_challenges(t, row)
+        provers[c].fold(op, ch)
+
+    plain_round(0)
+    t0 = time.perf_counter()
+    for i in range(instances):
+        plain_round(i)
+    plain_round_ms = (time.perf_counter() - t0) * 1000
     return {"value": total / (ms / 1000), "unit": "elems/s", "ms_per_step": ms, "instances": instances,
             "elements": total, "log2_sizes": [int(x) for x in logs],
             "sequential_device_ms": seq_dev, "sequential_wall_ms": seq_wall,
             "speedup_vs_sequential_device": seq_dev / ms, "speedup_vs_sequential_wall": seq_wall / ms,
             "schedule": tuned, "gpu_launches_per_step": launches, "graphs": True,
-            "workload": "commit (2 limbs: 3889, 9721) + fold of every instance, column length 2048"}
+            "workload": "commit (2 limbs: 3889, 9721) + fold of every instance, column length 2048",
+            "round": {"batched_ms": round_ms, "sequential_plain_ms": plain_round_ms,
+                      "batched_elems_s": total / (round_ms / 1000), "sequential_plain_elems_s": total / (plain_round_ms / 1000),
+                      "speedup": plain_round_ms / round_ms,
+                      "workload": "commit + open of every instance: the batch's device round (graph, device "
+                                  "transcripts, outputs read back) vs one plain API round per instance"}}
+
+
+def run_ntt_micro(steps, count=1 << 20, q=3889):
+    """The 648-point forward transform and its inverse over all ring elements of a 2^22 witness
+    (2^20 ring elements, q = 3889, coefficients uniform in [0, q) from a seeded generator), each
+    timed alone with CUDA events (inputs 1.36 GB, far above L2). GB/s counts 1296 B read + 1296 B
+    written per ring element and direction."""
+    import torch
+
+    from labinius_b200 import ntt
+
+    g = torch.Generator(device="cuda").manual_seed(2026)
+    a = torch.randint(0, q, (count, 648), dtype=torch.int16, device="cuda", generator=g)
+    y = torch.empty_like(a)
+    z = torch.empty_like(a)
+    for _ in range(2):
+        ntt.forward(q, a, y)
+        ntt.inverse(q, y, z)
+    torch.cuda.synchronize()
+    if not torch.equal(z, a):
+        raise RuntimeError("ntt648 round trip failed")
+    res = {}
+    for name, fn, src, dst in (("forward", ntt.forward, a, y), ("inverse", ntt.inverse, y, z)):
+        ts = []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn(q, src, dst)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = float(np.median(ts))
+        res[name] = {"ms": ms, "gbs": 2 * 1296 * count / (ms / 1000) / 1e9}
+    return {"ring_elements": count, "q": q, **res,
+            "bytes_per_ring_element": 2592, "workload": "all ring elements of a 2^22 witness, d = 648, q = 3889"}
 
 
 def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
@@ -555,6 +624,11 @@ def run_ours(args):
     batched = None
     if not args.no_batched:
         batched = run_batched(args.batch_instances, max(3, min(args.steps, 5)))
+    ntt_micro = None
+    if not args.no_ntt:
+        ntt_micro = run_ntt_micro(max(3, min(args.steps, 10)), count=args.ntt_count)
+        for k in ("forward", "inverse"):
+            ntt_micro[k]["frac_of_hbm"] = ntt_micro[k]["gbs"] / hbm
     served = None
     if not args.no_served and rank == 0 and world == 1:
         served = run_served(args.served_requests, args.served_plain_sample)
@@ -587,6 +661,7 @@ def run_ours(args):
         "e2e": e2e,
         "batched": batched,
         "served": served,
+        "ntt_microbench": ntt_micro,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -3,7 +3,7 @@
  *
  * Every entry point replaces one call of the reference's scheme API (osdnk/labinius,
  * crates/pcs/src/scheme/) for the commit / evaluate / fold hot path. The Rust `scheme` bodies call
- * these through a thin `extern "C"` crate (INTEGRATION.md); the public Rust signatures stay.
+ * these through a thin `extern "C"` crate; the public Rust signatures stay.
  *
  * Conventions (after the only FFI the reference has, crates/pcs/src/labrador/ffi.rs:1-30):
  *  - opaque, caller-owned handles with explicit free;
@@ -124,6 +124,11 @@ int lbg_mle_evaluate(const lbg_pp* pp, const lbg_witness* w, const uint64_t* p0,
  * the opening (freed on return, also on error). v_out may be NULL (kept on the device). */
 int lbg_fold(lbg_prover* pr, lbg_opening* consumed, const lbg_challenge* challenges, size_t r,
              int16_t* v_out);
+/* Whether the commit keeps the base limb's transform of the witness for the fold (the reference's
+ * AuxData, crates/pcs/src/key.rs:275-326; 324 bytes of device memory per F162 and opening) or the
+ * fold transforms the witness again (the default). An opening whose kept buffer cannot be
+ * allocated folds by transforming again. Results are identical either way. */
+int lbg_prover_set_kept_transform(lbg_prover* pr, int enable);
 /* The last fold's result, int16 [len_ring][648]. */
 int lbg_prover_folded(const lbg_prover* pr, int16_t* v_out);
 
@@ -177,6 +182,16 @@ int lbg_fold_static(uint32_t base_prime, uint32_t witness_log_len, uint32_t colu
                     const uint64_t* d_witness, const lbg_challenge* d_challenges, size_t r, int16_t* d_v_out,
                     void* stream);
 
+/* The reference's 648-point transform of ring elements of Z_q[X]/(X^648 - X^324 + 1)
+ * (crates/pcs/src/scalar.rs:35-84 forward, :123-177 inverse), the kernels of the NTT
+ * microbenchmark: `count` ring elements, u16 coefficients (forward) or slots in the reference's
+ * slot order (inverse), all in [0, q), [count][648], device pointers, asynchronous on `stream`
+ * (the current device's). Splitting primes (3889, 9721, 17497, 19441); quadratic-leaf primes
+ * return LBG_ERR_UNSUPPORTED. No Rust API entry point corresponds (the reference calls its
+ * transforms internally). */
+int lbg_ntt648_forward(uint32_t q, const uint16_t* d_in, uint16_t* d_out, size_t count, void* stream);
+int lbg_ntt648_inverse(uint32_t q, const uint16_t* d_in, uint16_t* d_out, size_t count, void* stream);
+
 /* Batched rounds: many independent witnesses under one key (all share the public parameters'
  * column length, moduli and opening; instance i has 2^column_log_lens[i] columns). Every stage is
  * one launch over all instances; the device stages can be replayed as CUDA graphs, and
@@ -199,7 +214,11 @@ int lbg_batch_witness_generate(lbg_batch* b, const uint8_t* seeds, const uint8_t
 int lbg_batch_witness_upload(lbg_batch* b, size_t instance, const uint64_t* f162, size_t n);
 int lbg_batch_witness_download(const lbg_batch* b, size_t instance, uint64_t* out, size_t n);
 int lbg_batch_use_graphs(lbg_batch* b, int enable);
+/* The autotuner times candidate commit chunkings and fold splits on the batch's own shape, and
+ * whether the fold reads the commit's kept transform, and keeps the fastest. */
 int lbg_batch_autotune(lbg_batch* b, uint32_t* chunks_out, uint32_t* fold_cols_out);
+/* The kept transform on or off by hand (off by default; see lbg_prover_set_kept_transform). */
+int lbg_batch_set_kept_transform(lbg_batch* b, int enable);
 int lbg_batch_commit(lbg_batch* b, int16_t* matrix_out, uint16_t* top_out, uint16_t* digits_out);
 int lbg_batch_row_evaluate(lbg_batch* b, const uint64_t* p0 /* [count][row_log][3] */, uint64_t* u_out);
 int lbg_batch_mle_evaluate(lbg_batch* b, const uint64_t* p0, const uint64_t* p1 /* concatenated */,

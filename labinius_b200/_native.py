@@ -95,6 +95,10 @@ SIGNATURES = {
     "lbg_batch_mle_evaluate": (_int, [_vp, _vp, _vp, _vp]),
     "lbg_batch_fold": (_int, [_vp, _vp, _sz, _vp]),
     "lbg_batch_round": (_int, [_vp, _vp, _sz, _vp]),
+    "lbg_prover_set_kept_transform": (_int, [_vp, _int]),
+    "lbg_batch_set_kept_transform": (_int, [_vp, _int]),
+    "lbg_ntt648_forward": (_int, [ctypes.c_uint32, _vp, _vp, _sz, _vp]),
+    "lbg_ntt648_inverse": (_int, [ctypes.c_uint32, _vp, _vp, _sz, _vp]),
     "lbg_batch_stream": (_vp, [_vp]),
     "lbg_batch_launch_count": (_u64, [_vp]),
 }

@@ -19,6 +19,21 @@ from .scheme import CHALLENGE_DTYPE, N, N162, Params, PublicParameters
 _CH = CHALLENGE_DTYPE
 
 
+def _pinned(shape, dtype):
+    """A page-locked host array (torch's caching host allocator keeps the blocks for reuse), so the
+    device-to-host copies of a round run at full link speed; falls back to pageable memory when
+    no CUDA device is visible."""
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+            return torch.empty(n, dtype=torch.uint8, pin_memory=True).numpy().view(dtype).reshape(shape)
+    except ImportError:
+        pass
+    return np.zeros(shape, dtype)
+
+
 @dataclass
 class InstanceRound:
     matrix: np.ndarray = None  # int16 [cols][4][limbs][162] (Clear)
@@ -93,6 +108,10 @@ class Batch:
     def use_graphs(self, enable=True):
         check(lib().lbg_batch_use_graphs(self._h, int(enable)))
 
+    def keep_transform(self, enable=True):
+        """The fold reads the commit's kept transform (on) or transforms the witness again (off)."""
+        check(lib().lbg_batch_set_kept_transform(self._h, int(enable)))
+
     def autotune(self):
         c, f = ctypes.c_uint32(), ctypes.c_uint32()
         check(lib().lbg_batch_autotune(self._h, ctypes.byref(c), ctypes.byref(f)))
@@ -162,16 +181,18 @@ class Batch:
         check(lib().lbg_params_derive_folding_challenges(ctypes.byref(pn), t, ptr(r.u), ptr(r.challenges)))
         lib().lbg_transcript_free(t)
 
-    def round(self, domain=b"labinius/reference", pool=None, transcript="device") -> List[InstanceRound]:
+    def round(self, domain=b"labinius/reference", pool=None, transcript="device", copy=True) -> List[InstanceRound]:
         """commit -> per instance: evaluation point -> row and mle evaluation -> per instance: folding
         challenges -> fold, each instance with a fresh Transcript(domain).
 
         transcript="device": the whole round in one pass on the device (the absorbs, the point and
         the challenge sampler are device kernels; lbg_batch_round). transcript="host": the
         transcript steps run in the library's host code between the device stages, on `pool` (a
-        concurrent.futures executor; the calls release the GIL) or instance by instance."""
+        concurrent.futures executor; the calls release the GIL) or instance by instance.
+        copy=False (device transcript) returns views into the batch's page-locked output buffers,
+        valid until its next round."""
         if transcript == "device":
-            return self._round_device(domain)
+            return self._round_device(domain, copy)
         rounds = self.commit()
         run = (lambda f, xs: list(pool.map(f, xs))) if pool is not None else (lambda f, xs: [f(x) for x in xs])
         ts = run(lambda i: self._point(i, rounds[i], domain), range(self.count))
@@ -185,23 +206,39 @@ class Batch:
             r.v = vs[i]
         return rounds
 
-    def _round_device(self, domain) -> List[InstanceRound]:
+    def _outputs(self):
+        """Page-locked output buffers sized for the arena, allocated once per batch."""
+        if getattr(self, "_out", None) is None:
+            Cm, Im, L = self.capacity[0], self.capacity[1], self.limbs
+            o = {"p0": _pinned((Im * self.row_log * 3,), np.uint64), "p1": _pinned((Im * 32 * 3,), np.uint64),
+                 "mle": _pinned((Im * 3,), np.uint64), "u": _pinned((Cm * 3,), np.uint64),
+                 "ch": _pinned((Cm * _CH.itemsize,), np.uint8), "v": _pinned((Im * self.len_ring * N,), np.int16)}
+            if self.dropped:
+                o["top"] = _pinned((Cm * N,), np.uint16)
+                o["dig"] = _pinned((max(L - 1, 1) * Cm * N,), np.uint16)
+            else:
+                o["m"] = _pinned((Cm * 4 * L * N162,), np.int16)
+            self._out = o
+        return self._out
+
+    def _round_device(self, domain, copy=True) -> List[InstanceRound]:
         C, L, I = self.total_cols, self.limbs, self.count
+        o = self._outputs()
         out = nat.lbg_batch_outputs()
         m = top = dig = None
         if self.dropped:
-            top = np.zeros(C * N, np.uint16)
-            dig = np.zeros((max(L - 1, 1), C * N), np.uint16)
+            top = o["top"][: C * N]
+            dig = o["dig"][: max(L - 1, 1) * C * N].reshape(max(L - 1, 1), C * N)
             out.top, out.digits = ptr(top).value, ptr(dig).value
         else:
-            m = np.zeros((C, 4, L, N162), np.int16)
+            m = o["m"][: C * 4 * L * N162].reshape(C, 4, L, N162)
             out.matrix = ptr(m).value
-        p0 = np.zeros((I, self.row_log, 3), np.uint64)
-        p1 = np.zeros((sum(self.column_log_lens), 3), np.uint64)
-        mle = np.zeros((I, 3), np.uint64)
-        u = np.zeros((C, 3), np.uint64)
-        ch = np.zeros(C, _CH)
-        v = np.zeros((I, self.len_ring, N), np.int16)
+        p0 = o["p0"][: I * self.row_log * 3].reshape(I, self.row_log, 3)
+        p1 = o["p1"][: sum(self.column_log_lens) * 3].reshape(-1, 3)
+        mle = o["mle"][: I * 3].reshape(I, 3)
+        u = o["u"][: C * 3].reshape(C, 3)
+        ch = o["ch"][: C * _CH.itemsize].view(_CH)
+        v = o["v"][: I * self.len_ring * N].reshape(I, self.len_ring, N)
         for name, a in (("p0", p0), ("p1", p1), ("mle", mle), ("u", u), ("challenges", ch), ("v", v)):
             setattr(out, name, ptr(a).value)
         d = np.frombuffer(bytes(domain), np.uint8).copy()
@@ -212,13 +249,17 @@ class Batch:
             a, b = int(self.col_off[i]), int(self.col_off[i + 1])
             r = InstanceRound()
             if self.dropped:
-                r.top, r.digits = top[a * N:b * N].copy(), dig[: L - 1, a * N:b * N].copy()
+                r.top, r.digits = top[a * N:b * N], dig[: L - 1, a * N:b * N]
             else:
-                r.matrix = m[a:b].copy()
+                r.matrix = m[a:b]
             cl = self.column_log_lens[i]
-            r.p0, r.p1 = p0[i].copy(), p1[po:po + cl].copy()
+            r.p0, r.p1 = p0[i], p1[po:po + cl]
             po += cl
-            r.mle, r.u, r.challenges, r.v = mle[i].copy(), u[a:b].copy(), ch[a:b].copy(), v[i]
+            r.mle, r.u, r.challenges, r.v = mle[i], u[a:b], ch[a:b], v[i]
+            if copy:
+                for k, val in vars(r).items():
+                    if val is not None:
+                        setattr(r, k, np.array(val))
             rounds.append(r)
         return rounds
 
@@ -230,6 +271,6 @@ class Batch:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and nat._lib is not None:
+        if h and nat is not None and getattr(nat, "_lib", None) is not None:
             nat._lib.lbg_batch_free(h)
             self._h = None

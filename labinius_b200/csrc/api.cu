@@ -380,6 +380,7 @@ static void free_bufs(OpeningBufs* b) {
   cudaFree(b->d_C);
   cudaFree(b->d_top);
   cudaFree(b->d_digits);
+  cudaFree(b->d_keep);
   delete b;
 }
 
@@ -403,12 +404,25 @@ void lbg_prover_free(lbg_prover* pr) {
   delete pr;
 }
 
+// The kept transform of an opening, when the prover keeps it and the device has the room
+// (otherwise the fold transforms the witness again).
+static void attach_keep(const lbg_prover* pr, OpeningBufs* b) {
+  if (!pr->keep) {
+    cudaFree(b->d_keep);
+    b->d_keep = nullptr;
+  } else if (!b->d_keep && cudaMalloc((void**)&b->d_keep, pr->pp->n * N162 * 2) != cudaSuccess) {
+    cudaGetLastError();
+    b->d_keep = nullptr;
+  }
+}
+
 static int get_bufs(lbg_prover* pr, OpeningBufs** out) {
   {
     std::lock_guard<std::mutex> g(pr->mu);
     if (!pr->spare.empty()) {
       *out = pr->spare.back();
       pr->spare.pop_back();
+      attach_keep(pr, *out);
       return LBG_OK;
     }
   }
@@ -422,7 +436,18 @@ static int get_bufs(lbg_prover* pr, OpeningBufs** out) {
     free_bufs(b);
     return fail(LBG_ERR_OOM, "opening: device allocation failed");
   }
+  attach_keep(pr, b);
   *out = b;
+  return LBG_OK;
+}
+
+int lbg_prover_set_kept_transform(lbg_prover* pr, int enable) {
+  if (!pr) return fail(LBG_ERR_INVALID, "null prover");
+  LBG_CU(cudaSetDevice(pr->pp->device));
+  LBG_CU(cudaStreamSynchronize(pr->stream));
+  std::lock_guard<std::mutex> g(pr->mu);
+  pr->keep = enable != 0;
+  for (OpeningBufs* b : pr->spare) attach_keep(pr, b);
   return LBG_OK;
 }
 
@@ -570,7 +595,8 @@ int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16
     {
       KernelScope ks(pr, "commit");
       e = launch_commit(pp->pidx[k], w->d, pp->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2,
-                        pp->d_prime[k], cols, (int)pp->len_ring, pr->chunk, pr->nchunks, pr->d_partial, st);
+                        pp->d_prime[k], cols, (int)pp->len_ring, pr->chunk, pr->nchunks, pr->d_partial, st,
+                        k == 0 ? b->d_keep : nullptr);
     }
     if (e == cudaSuccess) {
       KernelScope ks(pr, "commit_finish");
@@ -713,9 +739,13 @@ int lbg_fold(lbg_prover* pr, lbg_opening* op, const lbg_challenge* challenges, s
     e = launch_challenge_slots(pp->pidx[0], pr->d_ch, (int)r, pp->d_prime[0], pr->d_chat, st);
   }
   if (e == cudaSuccess) {
-    KernelScope ks(pr, "fold", 2);  // k_fold + k_fold_finish
-    e = launch_fold(pp->pidx[0], op->w->d, pp->wdim, (int)pp->cols, pr->fold_cols_per_split, pr->d_chat,
-                    pp->d_prime[0], pr->d_vhat, pr->d_v, st);
+    KernelScope ks(pr, "fold", 2);  // k_fold (or k_fold_kept) + k_fold_finish
+    if (op->bufs->d_keep)
+      e = launch_fold_kept(pp->pidx[0], op->bufs->d_keep, pp->wdim, (int)pp->cols, pr->fold_cols_per_split,
+                           pr->d_chat, pp->d_prime[0], pr->d_vhat, pr->d_v, st);
+    else
+      e = launch_fold(pp->pidx[0], op->w->d, pp->wdim, (int)pp->cols, pr->fold_cols_per_split, pr->d_chat,
+                      pp->d_prime[0], pr->d_vhat, pr->d_v, st);
   }
   if (e == cudaSuccess && v_out) e = cudaMemcpyAsync(v_out, pr->d_v, pp->len_ring * N648 * 2, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess && v_out) e = cudaStreamSynchronize(st);

@@ -56,6 +56,8 @@ struct lbg_batch {
   int32_t* d_partial = nullptr;   // [max_chunks][total_cols][162][4]
   int max_chunks = 0;
   int16_t* d_C = nullptr;         // [total_cols][4][limbs][162]
+  uint16_t* d_keep = nullptr;     // the base limb's kept transform [cap_cols][162][wdim] (allocated on demand)
+  bool keep = false;              // the commit keeps it and the fold reads it
   uint16_t* d_res = nullptr;      // [limbs][total_cols*648]
   uint16_t* d_top = nullptr;
   uint16_t* d_digits = nullptr;
@@ -104,7 +106,8 @@ static cudaError_t enqueue_commit(lbg_batch* b) {
   cudaError_t e = cudaSuccess;
   for (int k = 0; k < L && e == cudaSuccess; k++) {
     e = launch_commit(pp->pidx[k], b->d_w, b->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2, pp->d_prime[k],
-                      cols, (int)b->len_ring, b->chunk, b->nchunks, b->d_partial, b->stream);
+                      cols, (int)b->len_ring, b->chunk, b->nchunks, b->d_partial, b->stream,
+                      k == 0 && b->keep ? b->d_keep : nullptr);
     if (e == cudaSuccess)
       e = launch_commit_finish(pp->pidx[k], b->d_partial, b->nchunks, cols, pp->d_prime[k], k, L, b->d_C, b->stream);
   }
@@ -130,7 +133,10 @@ static cudaError_t enqueue_commit(lbg_batch* b) {
 static cudaError_t enqueue_fold(lbg_batch* b) {
   const lbg_pp* pp = b->pp;
   cudaError_t e = launch_challenge_slots(pp->pidx[0], b->d_ch, (int)b->total_cols, pp->d_prime[0], b->d_chat, b->stream);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && b->keep)
+    e = launch_fold_kept(pp->pidx[0], b->d_keep, b->wdim, (int)b->total_cols, b->fold_per, b->d_chat,
+                         pp->d_prime[0], b->d_vhat, b->d_v, b->stream, b->count, b->d_split_inst);
+  else if (e == cudaSuccess)
     e = launch_fold(pp->pidx[0], b->d_w, b->wdim, (int)b->total_cols, b->fold_per, b->d_chat, pp->d_prime[0],
                     b->d_vhat, b->d_v, b->stream, b->count, b->d_split_inst);
   b->launches += 3;
@@ -335,7 +341,7 @@ void lbg_batch_free(lbg_batch* b) {
   free_graphs(b);
   void* ptrs[] = {b->d_w, b->d_col_inst, b->d_row_tiles, b->d_split_inst, b->d_partial, b->d_C, b->d_res, b->d_top, b->d_digits,
                   b->d_p0, b->d_p1, b->d_eq, b->d_u, b->d_claim, b->d_ch, b->d_chat, b->d_vhat, b->d_v,
-                  b->d_prefix, b->d_states, b->d_inst, b->d_oldcv, b->d_stage, b->d_cvs, b->d_packed};
+                  b->d_prefix, b->d_states, b->d_inst, b->d_oldcv, b->d_stage, b->d_cvs, b->d_packed, b->d_keep};
   for (void* p : ptrs) cudaFree(p);
   b->ab_commit.release();
   b->ab_u.release();
@@ -562,8 +568,34 @@ int lbg_batch_use_graphs(lbg_batch* b, int enable) {
   return LBG_OK;
 }
 
+// The kept transform on or off (allocated on first use: 324 B per F162 of the arena); the
+// captured graphs are rebuilt.
+static int set_keep(lbg_batch* b, bool on) {
+  if (on && !b->d_keep) {
+    if (cudaMalloc((void**)&b->d_keep, b->cap_cols * b->wdim * N162 * 2) != cudaSuccess) {
+      cudaGetLastError();
+      b->d_keep = nullptr;
+      return fail(LBG_ERR_OOM, "kept transform: device allocation failed");
+    }
+  }
+  if (b->keep == on) return LBG_OK;
+  bool had = b->graphs;
+  if (had) lbg_batch_use_graphs(b, 0);
+  b->keep = on;
+  if (had) return lbg_batch_use_graphs(b, 1);
+  return LBG_OK;
+}
+
+int lbg_batch_set_kept_transform(lbg_batch* b, int enable) {
+  if (!b) return fail(LBG_ERR_INVALID, "null batch");
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  return set_keep(b, enable != 0);
+}
+
 // The autotuner: time candidate schedules of both stages on this batch's shape and keep the
-// fastest (commit: ring-element chunks per column tile; fold: columns per split).
+// fastest (commit: ring-element chunks per column tile; fold: columns per split; whether the
+// fold reads the commit's kept transform).
 int lbg_batch_autotune(lbg_batch* b, uint32_t* chunks_out, uint32_t* fold_cols_out) {
   if (!b) return fail(LBG_ERR_INVALID, "null batch");
   LBG_BCU(cudaSetDevice(b->pp->device));
@@ -597,6 +629,23 @@ int lbg_batch_autotune(lbg_batch* b, uint32_t* chunks_out, uint32_t* fold_cols_o
   if (1 << b->min_col_log < 8) best_p = 1 << b->min_col_log;
   int rc = upload_splits(b, best_p);
   if (rc) return rc;
+  {
+    auto both = [](lbg_batch* x) {
+      cudaError_t e = enqueue_commit(x);
+      return e == cudaSuccess ? enqueue_fold(x) : e;
+    };
+    b->keep = false;
+    float t_off = time_stage(b, both);
+    float t_on = -1;
+    if (b->d_keep || cudaMalloc((void**)&b->d_keep, b->cap_cols * b->wdim * N162 * 2) == cudaSuccess) {
+      b->keep = true;
+      t_on = time_stage(b, both);
+    } else {
+      cudaGetLastError();
+      b->d_keep = nullptr;
+    }
+    b->keep = t_on >= 0 && t_on < t_off;
+  }
   b->launches = launches;
   LBG_BCU(cudaStreamSynchronize(b->stream));
   if (chunks_out) *chunks_out = (uint32_t)b->nchunks;

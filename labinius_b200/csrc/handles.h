@@ -63,6 +63,10 @@ struct lbg_prover {
   uint16_t* d_res = nullptr;  // [limbs][cols*648]
   std::mutex mu;
   std::vector<struct OpeningBufs*> spare;
+  // the fold reads the commit's kept transform (the reference's AuxData, crates/pcs/src/key.rs:275-326)
+  // instead of transforming the witness again; 324 B of device memory per F162 and opening. Off by
+  // default: at 2^22 the commit's extra 1.36 GB of stores cost more than the fold saves.
+  bool keep = false;
   // kernel accounting
   uint64_t launches = 0;
   bool profiling = false;
@@ -109,6 +113,7 @@ struct OpeningBufs {
   int16_t* d_C = nullptr;       // [cols][4][limbs][162]
   uint16_t* d_top = nullptr;    // [cols*648]
   uint16_t* d_digits = nullptr; // [limbs-1][cols*648]
+  uint16_t* d_keep = nullptr;   // the base limb's transform [cols][162][wdim] (kept-transform mode)
 };
 
 struct lbg_opening {

@@ -117,11 +117,12 @@ struct CommitRed {
   static constexpr int value = raw < 1 ? 1 : raw;
 };
 
-template <int PI>
+template <int PI, bool KEEP>
 __global__ void __launch_bounds__(256, 2)
     k_commit(const uint64_t* __restrict__ W, size_t wdim, const int4* __restrict__ Ahat,
              const DevPrime* __restrict__ D, int cols, int len_ring, int chunk,
-             int32_t* __restrict__ partial /* [nchunks][cols][162][4] */) {
+             int32_t* __restrict__ partial /* [nchunks][cols][162][4] */,
+             uint16_t* __restrict__ keep /* null, or the kept transform [cols][162][wdim] */) {
   extern __shared__ __align__(16) uint8_t smem[];
   uint16_t* lut = (uint16_t*)smem;                        // 6 * 64 u16
   uint64_t* wtile = (uint64_t*)(smem + LUT_BYTES);        // CT rows of WROW u64 (one pad word)
@@ -161,6 +162,24 @@ __global__ void __launch_bounds__(256, 2)
     }
     __syncthreads();
     const int nsteps = min(RT, i_end - i0);
+    if constexpr (KEEP) {
+      // the kept transform (the fold's input) in blocks of 16 positions: keep[j][p / 16][v][p % 16],
+      // p = 4 i + k, so this tile of a column is one contiguous 5184-byte block; a lane pair writes
+      // one leaf's 16 positions (32 bytes)
+      for (int x = tid; x < CT * N162 * 2; x += 256) {
+        int h = x & 1, jj = (x >> 1) & (CT - 1), v = x >> 5;
+        int j = j0 + jj;
+        if (j >= cols || 2 * h >= nsteps) continue;
+        uint2 a = *(const uint2*)(wt + ((((2 * h) * N162) + v) * CT + jj) * 4);
+        uint16_t* dst = keep + ((size_t)j * (wdim / 16) + i0 / 4) * (N162 * 16) + v * 16 + 8 * h;
+        if (2 * h + 1 < nsteps) {
+          uint2 b = *(const uint2*)(wt + ((((2 * h + 1) * N162) + v) * CT + jj) * 4);
+          *(uint4*)dst = make_uint4(a.x, a.y, b.x, b.y);
+        } else {
+          *(uint2*)dst = a;
+        }
+      }
+    }
     for (int ii = 0; ii < nsteps; ii++) {
       const int4* ah = Ahat + (size_t)(i0 + ii) * N162 * 2;
 #pragma unroll
@@ -359,6 +378,88 @@ __global__ void __launch_bounds__(256, 2)
       size_t i = p / 4;
       int k = (int)(p % 4);
       for (int m = 0; m < N162; m++) v_out[i * N648 + 4 * m + k] = center<PI>(x[m]);
+    }
+  }
+}
+
+// The fold from the kept transform (keep[j][p / 16][v][p % 16], written by the commit at the base
+// limb): the same sums as k_fold without transforming each F162 again. Per step the CTA streams
+// the two 5184-byte blocks of its 32 positions for FJ columns into shared memory (16-byte loads);
+// then warp w owns the leaves v = w + 8 u and lane = position, as in k_fold.
+template <int PI, bool DIRECT>
+__global__ void __launch_bounds__(256, 2)
+    k_fold_kept(const uint16_t* __restrict__ keep, size_t wdim, int cols, int cols_per_split,
+                const uint32_t* __restrict__ chat, const DevPrime* __restrict__ D, uint32_t* __restrict__ vhat,
+                int16_t* __restrict__ v_out, const int* __restrict__ split_inst) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint16_t* st = (uint16_t*)smem;  // [FJ][2 blocks][162][16] u16
+  constexpr int BLK = N162 * 16;   // u16 per block
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const size_t p0 = (size_t)blockIdx.x * FP;
+  const size_t p = p0 + lane;
+  const bool inside = p < wdim;
+  const int c_begin = blockIdx.y * cols_per_split;
+  const int c_end = min(cols, c_begin + cols_per_split);
+  const size_t nblk = wdim / 16, b0 = p0 / 16;
+  const int blocks = (int)min((size_t)2, nblk - b0);
+  uint32_t acc[VPW];
+#pragma unroll
+  for (int u = 0; u < VPW; u++) acc[u] = 0;
+  constexpr int RED = FoldRed<PI>::value;
+  int since = 0;
+  for (int j0 = c_begin; j0 < c_end; j0 += FJ) {
+    const int nj = min(FJ, c_end - j0);
+    __syncthreads();
+    const int per_col = blocks * BLK / 8;  // uint4 per column
+    for (int x = tid; x < nj * per_col; x += 256) {
+      int jj = x / per_col, o = x - jj * per_col;
+      const uint4* src = (const uint4*)(keep + ((size_t)(j0 + jj) * nblk + b0) * BLK);
+      ((uint4*)(st + (size_t)jj * 2 * BLK))[o] = __ldg(src + o);
+    }
+    __syncthreads();
+    const int off = (lane >> 4) * BLK + (lane & 15);
+    for (int jj = 0; jj < nj; jj++) {
+      const uint32_t* ch = chat + (size_t)(j0 + jj) * N162;
+      const uint16_t* sj = st + (size_t)jj * 2 * BLK + off;
+#pragma unroll
+      for (int u = 0; u < VPW; u++) {
+        int v = warp + 8 * u;
+        if (v < N162) acc[u] += __ldg(ch + v) * (uint32_t)sj[v * 16];
+      }
+      if (++since >= RED) {
+        since = 0;
+#pragma unroll
+        for (int u = 0; u < VPW; u++) acc[u] = red_half<PI>(acc[u]);
+      }
+    }
+  }
+  if constexpr (!DIRECT) {
+    if (split_inst) vhat += (size_t)split_inst[blockIdx.y] * wdim * N162;
+    if (inside) {
+#pragma unroll
+      for (int u = 0; u < VPW; u++) {
+        int v = warp + 8 * u;
+        if (v < N162) atomicAdd(vhat + p * N162 + v, red_full<PI>(acc[u]));
+      }
+    }
+  } else {
+    __syncthreads();
+    uint32_t* vh = (uint32_t*)smem;  // [FP][162] u32, 20.7 KB of the stage
+#pragma unroll
+    for (int u = 0; u < VPW; u++) {
+      int v = warp + 8 * u;
+      if (v < N162) vh[lane * N162 + v] = red_full<PI>(acc[u]);
+    }
+    __syncthreads();
+    if (tid < FP) {
+      size_t pp = p0 + tid;
+      if (pp < wdim) {
+        uint32_t* x = vh + tid * N162;
+        intt162_serial<PI>(x, *D);
+        size_t i = pp / 4;
+        int k = (int)(pp % 4);
+        for (int m = 0; m < N162; m++) v_out[i * N648 + 4 * m + k] = center<PI>(x[m]);
+      }
     }
   }
 }
@@ -650,6 +751,216 @@ __global__ void k_claims(const RoundInst* __restrict__ inst, const int* __restri
 }
 
 // =============================================================================================
+// The reference's 648-point transform (crates/pcs/src/scalar.rs:35-84) and its inverse (:123-177)
+// for splitting primes, on general coefficients in [0, q): the NTT microbenchmark. 81 threads per
+// ring element, E elements per CTA, three register stages joined through shared memory:
+//   A: thread r holds indices r + 81k (k < 8): level 0 (the Phi split, stride 324) and the
+//      radix-2 levels 1, 2 (strides 162, 81); afterwards x[k] sits in level-3 sub-ring k.
+//   B: thread (k, t < 9) of sub-ring k holds 81k + t + 9a + 27b: radix-3 levels 3 (stride 27,
+//      twiddle k) and 4 (stride 9, twiddle 3k + b).
+//   C: thread g < 72 (a 9-block) holds 9g + c + 3d: levels 5 (stride 3, twiddle g) and 6
+//      (stride 1, twiddle 3g + d).
+// Forward values stay unreduced (Shoup products in [0, 2q), every level adds at most 6q, under
+// 32q < 2^20 at the end) and are reduced once; the inverse's butterflies end in Shoup products,
+// so its values stay in [0, 2q).
+// =============================================================================================
+constexpr int NTT_E = 4;  // ring elements per CTA
+
+template <int PI>
+__device__ __forceinline__ void bfly3_inv(uint32_t& y0, uint32_t& y1, uint32_t& y2, const Twiddle& t,
+                                          const Ntt648Tables& T) {
+  // a0 = (y0 + y1 + y2) / 3, a1 = (y0 + w^2 y1 + w y2) z^-1 / 3, a2 = (y0 + w y1 + w^2 y2) z^-2 / 3
+  constexpr uint32_t q = Pr<PI>::q;
+  uint32_t d = mul_shoup(y2 + 2 * q - y1, T.omega, T.omega_s, q);  // w (y2 - y1)
+  uint32_t s1 = y0 + 2 * q - y1 + d;                              // y0 - y1 + w (y2 - y1)
+  uint32_t s2 = y0 + 4 * q - y2 - d;                              // y0 - y2 - w (y2 - y1)
+  uint32_t a0 = mul_shoup(y0 + y1 + y2, T.inv3, T.inv3s, q);
+  y1 = mul_shoup(s1, t.z, t.zs, q);
+  y2 = mul_shoup(s2, t.z2, t.z2s, q);
+  y0 = a0;
+}
+
+template <int PI>
+__global__ void __launch_bounds__(81 * NTT_E) k_ntt648_fwd(const uint16_t* __restrict__ in, uint16_t* __restrict__ out,
+                                                           size_t count, const Ntt648Tables* __restrict__ Tg) {
+  constexpr uint32_t q = Pr<PI>::q;
+  __shared__ uint32_t s[NTT_E][N648];
+  const Ntt648Tables& T = *Tg;
+  const uint32_t om = T.omega, oms = T.omega_s;
+  const int tid = threadIdx.x;
+  size_t e0 = (size_t)blockIdx.x * NTT_E;
+  {
+    int e = tid / 81, r = tid - 81 * (tid / 81);
+    size_t el = e0 + e;
+    if (el < count) {
+      const uint16_t* a = in + el * N648;
+      uint32_t x[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) x[k] = a[r + 81 * k];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {  // level 0: (a0 + z6 a1, a0 + a1 - z6 a1)
+        uint32_t t = mul_shoup(x[k + 4], T.z6, T.z6s, q);
+        uint32_t a0 = x[k];
+        x[k] = a0 + t;
+        x[k + 4] = a0 + x[k + 4] + 2 * q - t;
+      }
+#pragma unroll
+      for (int sr = 0; sr < 2; sr++)  // level 1, sub-ring sr: pairs (4sr + k, 4sr + k + 2)
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          uint32_t t = mul_shoup(x[4 * sr + k + 2], T.f1[sr][0], T.f1[sr][1], q);
+          uint32_t a0 = x[4 * sr + k];
+          x[4 * sr + k] = a0 + t;
+          x[4 * sr + k + 2] = a0 + 2 * q - t;
+        }
+#pragma unroll
+      for (int sr = 0; sr < 4; sr++) {  // level 2, sub-ring sr: pair (2sr, 2sr + 1)
+        uint32_t t = mul_shoup(x[2 * sr + 1], T.f2[sr][0], T.f2[sr][1], q);
+        uint32_t a0 = x[2 * sr];
+        x[2 * sr] = a0 + t;
+        x[2 * sr + 1] = a0 + 2 * q - t;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; k++) s[e][r + 81 * k] = x[k];
+    }
+  }
+  __syncthreads();
+  if (tid < 72 * NTT_E) {
+    int e = tid / 72, j = tid - 72 * (tid / 72), k = j / 9, t = j - 9 * (j / 9);
+    if (e0 + e < count) {
+      uint32_t y[3][3];
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) y[a][b] = s[e][81 * k + t + 9 * a + 27 * b];
+      Twiddle t3 = T.f3[k];
+#pragma unroll
+      for (int a = 0; a < 3; a++) bfly3<PI>(y[a][0], y[a][1], y[a][2], t3, om, oms);
+#pragma unroll
+      for (int b = 0; b < 3; b++) bfly3<PI>(y[0][b], y[1][b], y[2][b], T.f4[3 * k + b], om, oms);
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) s[e][81 * k + t + 9 * a + 27 * b] = y[a][b];
+    }
+  }
+  __syncthreads();
+  if (tid < 72 * NTT_E) {
+    int e = tid / 72, g = tid - 72 * (tid / 72);
+    if (e0 + e < count) {
+      uint32_t z[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) z[c][d] = s[e][9 * g + c + 3 * d];
+      Twiddle t5 = T.f5[g];
+#pragma unroll
+      for (int c = 0; c < 3; c++) bfly3<PI>(z[c][0], z[c][1], z[c][2], t5, om, oms);
+#pragma unroll
+      for (int d = 0; d < 3; d++) bfly3<PI>(z[0][d], z[1][d], z[2][d], T.f6[3 * g + d], om, oms);
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) s[e][9 * g + 3 * d + c] = red_full<PI>(z[c][d]);
+    }
+  }
+  __syncthreads();
+  // coalesced write-back, two values per 32-bit word
+  uint32_t* o32 = reinterpret_cast<uint32_t*>(out + e0 * N648);
+  size_t words = (size_t)min((size_t)NTT_E, count - e0) * (N648 / 2);
+  for (size_t w = tid; w < words; w += blockDim.x) {
+    int e = (int)(w / (N648 / 2)), p = (int)(w - (size_t)e * (N648 / 2));
+    o32[w] = s[e][2 * p] | (s[e][2 * p + 1] << 16);
+  }
+}
+
+template <int PI>
+__global__ void __launch_bounds__(81 * NTT_E) k_ntt648_inv(const uint16_t* __restrict__ in, uint16_t* __restrict__ out,
+                                                           size_t count, const Ntt648Tables* __restrict__ Tg) {
+  constexpr uint32_t q = Pr<PI>::q;
+  __shared__ uint32_t s[NTT_E][N648];
+  const Ntt648Tables& T = *Tg;
+  const int tid = threadIdx.x;
+  size_t e0 = (size_t)blockIdx.x * NTT_E;
+  if (tid < 72 * NTT_E) {  // levels 6, 5
+    int e = tid / 72, g = tid - 72 * (tid / 72);
+    size_t el = e0 + e;
+    if (el < count) {
+      const uint16_t* v = in + el * N648 + 9 * g;
+      uint32_t z[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) z[c][d] = v[c + 3 * d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) bfly3_inv<PI>(z[0][d], z[1][d], z[2][d], T.i6[3 * g + d], T);
+      Twiddle t5 = T.i5[g];
+#pragma unroll
+      for (int c = 0; c < 3; c++) bfly3_inv<PI>(z[c][0], z[c][1], z[c][2], t5, T);
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) s[e][9 * g + c + 3 * d] = z[c][d];
+    }
+  }
+  __syncthreads();
+  if (tid < 72 * NTT_E) {  // levels 4, 3
+    int e = tid / 72, j = tid - 72 * (tid / 72), k = j / 9, t = j - 9 * (j / 9);
+    if (e0 + e < count) {
+      uint32_t y[3][3];
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) y[a][b] = s[e][81 * k + t + 9 * a + 27 * b];
+#pragma unroll
+      for (int b = 0; b < 3; b++) bfly3_inv<PI>(y[0][b], y[1][b], y[2][b], T.i4[3 * k + b], T);
+      Twiddle t3 = T.i3[k];
+#pragma unroll
+      for (int a = 0; a < 3; a++) bfly3_inv<PI>(y[a][0], y[a][1], y[a][2], t3, T);
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) s[e][81 * k + t + 9 * a + 27 * b] = y[a][b];
+    }
+  }
+  __syncthreads();
+  {  // levels 2, 1, 0
+    int e = tid / 81, r = tid - 81 * (tid / 81);
+    size_t el = e0 + e;
+    if (el < count) {
+      uint32_t x[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) x[k] = s[e][r + 81 * k];
+#pragma unroll
+      for (int sr = 0; sr < 4; sr++) {  // (y0 + y1) / 2, (y0 - y1) z^-1 / 2
+        uint32_t y0 = x[2 * sr], y1 = x[2 * sr + 1];
+        x[2 * sr] = mul_shoup(y0 + y1, T.inv2, T.inv2s, q);
+        x[2 * sr + 1] = mul_shoup(y0 + 2 * q - y1, T.i2[sr][0], T.i2[sr][1], q);
+      }
+#pragma unroll
+      for (int sr = 0; sr < 2; sr++)
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          uint32_t y0 = x[4 * sr + k], y1 = x[4 * sr + k + 2];
+          x[4 * sr + k] = mul_shoup(y0 + y1, T.inv2, T.inv2s, q);
+          x[4 * sr + k + 2] = mul_shoup(y0 + 2 * q - y1, T.i1[sr][0], T.i1[sr][1], q);
+        }
+#pragma unroll
+      for (int k = 0; k < 4; k++) {  // a1 = (y0 - y1) det, a0 = y0 - z6 a1
+        uint32_t y0 = x[k], y1 = x[k + 4];
+        uint32_t a1 = mul_shoup(y0 + 2 * q - y1, T.det, T.dets, q);
+        uint32_t a0 = y0 + 2 * q - mul_shoup(a1, T.z6, T.z6s, q);
+        x[k] = red_full<PI>(a0);
+        x[k + 4] = red_full<PI>(a1);
+      }
+      uint16_t* a = out + el * N648;
+#pragma unroll
+      for (int k = 0; k < 8; k++) a[r + 81 * k] = (uint16_t)x[k];
+    }
+  }
+}
+
+// =============================================================================================
 // Witness generation: keyed BLAKE3 XOF of "labinius/witness" (crates/pcs/src/scheme/witness.rs:66-87)
 // =============================================================================================
 __device__ __forceinline__ uint32_t rotr32(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
@@ -785,8 +1096,8 @@ int commit_blocks_per_sm(int pi) {
   switch (pi) {
 #define LBG_OCC(I)                                                                                      \
   case I:                                                                                               \
-    cudaFuncSetAttribute(k_commit<I>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);          \
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_commit<I>, 256, smem);                      \
+    cudaFuncSetAttribute(k_commit<I, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_commit<I, false>, 256, smem);               \
     break;
     LBG_OCC(0) LBG_OCC(1) LBG_OCC(2) LBG_OCC(3) LBG_OCC(4) LBG_OCC(5) LBG_OCC(6)
 #undef LBG_OCC
@@ -797,13 +1108,21 @@ int commit_cols_per_cta() { return CT; }
 int commit_ring_per_step() { return RT; }
 
 cudaError_t launch_commit(int pi, const uint64_t* W, size_t wdim, const int4* Ahat, const DevPrime* D, int cols,
-                          int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st) {
+                          int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st, uint16_t* keep) {
   dim3 grid((cols + CT - 1) / CT, nchunks);
   size_t smem = commit_smem_bytes();
-  LBG_DISPATCH(pi, ({
-                 cudaFuncSetAttribute(k_commit<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                 k_commit<P><<<grid, 256, smem, st>>>(W, wdim, Ahat, D, cols, len_ring, chunk, partial);
-               }));
+  if (keep) {
+    LBG_DISPATCH(pi, ({
+                   cudaFuncSetAttribute(k_commit<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                   k_commit<P, true><<<grid, 256, smem, st>>>(W, wdim, Ahat, D, cols, len_ring, chunk, partial, keep);
+                 }));
+  } else {
+    LBG_DISPATCH(pi, ({
+                   cudaFuncSetAttribute(k_commit<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                   k_commit<P, false><<<grid, 256, smem, st>>>(W, wdim, Ahat, D, cols, len_ring, chunk, partial,
+                                                               nullptr);
+                 }));
+  }
   return cudaGetLastError();
 }
 
@@ -868,6 +1187,33 @@ cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int co
   return cudaGetLastError();
 }
 
+cudaError_t launch_fold_kept(int pi, const uint16_t* keep, size_t wdim, int cols, int cols_per_split,
+                             const uint32_t* chat, const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st,
+                             int instances, const int* split_inst) {
+  size_t smem = (size_t)FJ * 2 * N162 * 16 * 2;
+  if (!vhat) {
+    dim3 grid(blocks_for(wdim, FP), 1);
+    LBG_DISPATCH(pi, ({
+                   cudaFuncSetAttribute(k_fold_kept<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                   k_fold_kept<P, true><<<grid, 256, smem, st>>>(keep, wdim, cols, cols, chat, D, nullptr, v, nullptr);
+                 }));
+    return cudaGetLastError();
+  }
+  int splits = (cols + cols_per_split - 1) / cols_per_split;
+  if (splits < 1 || splits > 65535) return cudaErrorInvalidValue;
+  dim3 grid(blocks_for(wdim, FP), splits);
+  cudaError_t e = cudaMemsetAsync(vhat, 0, wdim * (size_t)instances * N162 * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
+  LBG_DISPATCH(pi, ({
+                 cudaFuncSetAttribute(k_fold_kept<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                 k_fold_kept<P, false><<<grid, 256, smem, st>>>(keep, wdim, cols, cols_per_split, chat, D, vhat,
+                                                                nullptr, split_inst);
+               }));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  LBG_DISPATCH(pi, (k_fold_finish<P><<<blocks_for(wdim * instances, 64), 64, 0, st>>>(vhat, wdim * instances, D, v)));
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fold_commitment(int pi, const int16_t* C, int cols, int limb, int limbs, const uint32_t* chat,
                                    const DevPrime* D, int16_t* out, cudaStream_t st) {
   LBG_DISPATCH(pi, (k_fold_commitment<P><<<blocks_for(4 * N162, 128), 128, 0, st>>>(C, cols, limb, limbs, chat, D, out)));
@@ -925,6 +1271,27 @@ cudaError_t launch_claims(const RoundInst* d_inst, const int* col_inst, const ui
   if (e != cudaSuccess) return e;
   k_claims<<<blocks_for(total_cols, 128), 128, 0, st>>>(d_inst, col_inst, u, total_cols, p1,
                                                          (unsigned long long*)out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ntt648(int pi, bool inverse, const uint16_t* in, uint16_t* out, size_t count,
+                          const Ntt648Tables* T, cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  unsigned grid = (unsigned)((count + NTT_E - 1) / NTT_E);
+  switch (pi) {
+#define LBG_NTT648(P)                                                                      \
+  case P:                                                                                  \
+    if (inverse) k_ntt648_inv<P><<<grid, 81 * NTT_E, 0, st>>>(in, out, count, T);          \
+    else k_ntt648_fwd<P><<<grid, 81 * NTT_E, 0, st>>>(in, out, count, T);                  \
+    break;
+    LBG_NTT648(1)
+    LBG_NTT648(3)
+    LBG_NTT648(5)
+    LBG_NTT648(6)
+#undef LBG_NTT648
+    default:
+      return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 

@@ -8,6 +8,7 @@ namespace lbg {
 
 struct HotPrime;
 struct DevPrime;
+struct Ntt648Tables;
 
 // lbg_challenge as the device sees it (40 bytes).
 struct lbg_challenge_d {
@@ -39,8 +40,10 @@ size_t commit_smem_bytes();
 int commit_blocks_per_sm(int pi);
 int commit_cols_per_cta();
 int commit_ring_per_step();
+// keep (optional): the base limb's transform of every F162, u16 [cols][162][wdim], for the fold.
 cudaError_t launch_commit(int pi, const uint64_t* W, size_t wdim, const int4* Ahat, const DevPrime* D, int cols,
-                          int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st);
+                          int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st,
+                          uint16_t* keep = nullptr);
 cudaError_t launch_commit_finish(int pi, const int32_t* partial, int nchunks, int cols, const DevPrime* D,
                                  int limb, int limbs, int16_t* C, cudaStream_t st);
 cudaError_t launch_challenge_slots(int pi, const lbg_challenge_d* ch, int r, const DevPrime* D, uint32_t* chat,
@@ -57,6 +60,10 @@ int fold_blocks_per_sm(int pi);
 cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
                         const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st, int instances = 1,
                         const int* split_inst = nullptr);
+// The fold from the commit's kept transform instead of the witness (same splits and outputs).
+cudaError_t launch_fold_kept(int pi, const uint16_t* keep, size_t wdim, int cols, int cols_per_split,
+                             const uint32_t* chat, const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st,
+                             int instances = 1, const int* split_inst = nullptr);
 cudaError_t launch_fold_commitment(int pi, const int16_t* C, int cols, int limb, int limbs, const uint32_t* chat,
                                    const DevPrime* D, int16_t* out, cudaStream_t st);
 cudaError_t launch_column_residues(int pi, const int16_t* C, int cols, int limb, int limbs, const DevPrime* D,
@@ -71,6 +78,10 @@ cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq
 cudaError_t launch_row_eval(const uint64_t* W, size_t wdim, int cols, const uint64_t* eq, uint64_t* u,
                             cudaStream_t st, const int4* tiles = nullptr, int ntiles = 0);
 int row_eval_tile_cols();
+// The reference's 648-point forward transform or its inverse of `count` ring elements (u16 in
+// [0, q), [count][648]) for the splitting prime with index pi; T: device copy of its tables.
+cudaError_t launch_ntt648(int pi, bool inverse, const uint16_t* in, uint16_t* out, size_t count,
+                          const Ntt648Tables* T, cudaStream_t st);
 cudaError_t launch_claim(const uint64_t* u, int cols, const uint64_t* p1, int n, uint64_t* out, cudaStream_t st);
 cudaError_t launch_xof(const XofRoot& root, size_t nbytes, uint8_t* out, cudaStream_t st);
 cudaError_t launch_mask_f162(uint64_t* W, size_t n, cudaStream_t st);

@@ -1,5 +1,7 @@
 #include "ring_tables.h"
 
+#include "prime_structs.h"
+
 #include <mutex>
 #include <stdexcept>
 
@@ -42,6 +44,80 @@ static uint32_t subring_exp_quad648(int level, int k) {
   if (level == 1) return k == 0 ? 162 : 810;
   uint32_t p = RADIXQ[level - 1];
   return (subring_exp_quad648(level - 1, k / p) + 972u * (k % p)) / p;
+}
+
+static uint32_t shoup32(uint32_t w, uint32_t q) { return (uint32_t)(((uint64_t)w << 32) / q); }
+
+// Twiddles of the 648-point tree: zeta_{L,k} = psi^{subring_exp(L,k) / RADIX[L]}
+// (crates/pcs/src/params.rs:64-76, 115-166), psi the reference's primitive 1944-th root.
+static Ntt648Tables* build_ntt648(uint32_t q) {
+  Ntt648Tables* T = new Ntt648Tables();
+  uint64_t psi = 0;
+  for (uint64_t x = 2;; x++)
+    if (pow_mod(x, 1944, q) == 1 && pow_mod(x, 972, q) != 1 && pow_mod(x, 648, q) != 1) {
+      psi = x;
+      break;
+    }
+  auto zeta = [&](int level, int k) { return (uint32_t)pow_mod(psi, subring_exp648(level, k) / RADIX648[level], q); };
+  auto tw = [&](uint32_t z) {
+    Twiddle w;
+    w.z = z;
+    w.zs = shoup32(z, q);
+    w.z2 = (uint32_t)((uint64_t)z * z % q);
+    w.z2s = shoup32(w.z2, q);
+    return w;
+  };
+  uint64_t inv2 = inv_mod(2, q), inv3 = inv_mod(3, q);
+  auto itw = [&](uint32_t z) {  // (z^-1 / 3, z^-2 / 3)
+    uint64_t zi = inv_mod(z, q);
+    Twiddle w;
+    w.z = (uint32_t)(zi * inv3 % q);
+    w.zs = shoup32(w.z, q);
+    w.z2 = (uint32_t)(zi * zi % q * inv3 % q);
+    w.z2s = shoup32(w.z2, q);
+    return w;
+  };
+  T->z6 = (uint32_t)pow_mod(psi, 324, q);
+  T->z6s = shoup32(T->z6, q);
+  T->omega = (uint32_t)pow_mod(psi, 648, q);
+  T->omega_s = shoup32(T->omega, q);
+  for (int k = 0; k < 2; k++) {
+    uint32_t z = zeta(1, k);
+    T->f1[k][0] = z;
+    T->f1[k][1] = shoup32(z, q);
+    uint32_t zi = (uint32_t)(inv_mod(z, q) * inv2 % q);
+    T->i1[k][0] = zi;
+    T->i1[k][1] = shoup32(zi, q);
+  }
+  for (int k = 0; k < 4; k++) {
+    uint32_t z = zeta(2, k);
+    T->f2[k][0] = z;
+    T->f2[k][1] = shoup32(z, q);
+    uint32_t zi = (uint32_t)(inv_mod(z, q) * inv2 % q);
+    T->i2[k][0] = zi;
+    T->i2[k][1] = shoup32(zi, q);
+  }
+  for (int k = 0; k < 8; k++) T->f3[k] = tw(zeta(3, k)), T->i3[k] = itw(zeta(3, k));
+  for (int k = 0; k < 24; k++) T->f4[k] = tw(zeta(4, k)), T->i4[k] = itw(zeta(4, k));
+  for (int k = 0; k < 72; k++) T->f5[k] = tw(zeta(5, k)), T->i5[k] = itw(zeta(5, k));
+  for (int k = 0; k < 216; k++) T->f6[k] = tw(zeta(6, k)), T->i6[k] = itw(zeta(6, k));
+  T->inv2 = (uint32_t)inv2;
+  T->inv2s = shoup32(T->inv2, q);
+  T->inv3 = (uint32_t)inv3;
+  T->inv3s = shoup32(T->inv3, q);
+  T->det = (uint32_t)inv_mod((2ull * T->z6 + q - 1) % q, q);
+  T->dets = shoup32(T->det, q);
+  return T;
+}
+
+const Ntt648Tables* ntt648_tables(uint32_t q) {
+  static std::mutex mu;
+  static Ntt648Tables* cache[7] = {nullptr};
+  int pi = prime_index(q);
+  if (pi < 0 || quadratic_slots(q)) return nullptr;
+  std::lock_guard<std::mutex> g(mu);
+  if (!cache[pi]) cache[pi] = build_ntt648(q);
+  return cache[pi];
 }
 
 static RefTables build_ref() {

@@ -6,7 +6,7 @@
 // psi'^2 (quadratic-leaf primes). These are exactly the R_162 slots of the reference's commitment
 // components (crates/pcs/src/ring/mod.rs:22-55), so the 648-slot commitment of a ring element
 // w = sum_k X^k w_k(X^4) is the 4x4 "module" product of the key's components with these
-// transforms; see DESIGN.md for the algebra.
+// transforms: Y_k'(v) = sum_i [sum_{d+k=k'} a_d w_k + theta^v sum_{d+k=k'+4} a_d w_k] at leaf v.
 //
 // The 162-point tree (this project's own; the reference has only the 648-point trees of
 // crates/pcs/src/params.rs): level 0 splits Y^162 - Y^81 + 1 into Y^81 - theta^81 and
@@ -72,6 +72,11 @@ struct RefTables {
   uint32_t quad_class_slot[2][N162];
 };
 const RefTables& ref_tables();
+
+// Tables of the reference's 648-point transform for a splitting prime (nullptr for a
+// quadratic-leaf prime); the struct is defined with the device structs.
+struct Ntt648Tables;
+const Ntt648Tables* ntt648_tables(uint32_t q);
 
 // xorshift64* state transition as GF(2) columns: jump[k][c] = T^(2^k) applied to e_c.
 const std::vector<uint64_t>& xorshift_jumps();  // 64 * 64 words

@@ -229,7 +229,7 @@ class PublicParameters:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and nat._lib is not None:
+        if h and nat is not None and getattr(nat, "_lib", None) is not None:
             nat._lib.lbg_public_parameters_free(h)
             self._h = None
 
@@ -292,7 +292,7 @@ class Witness:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and nat._lib is not None:
+        if h and nat is not None and getattr(nat, "_lib", None) is not None:
             nat._lib.lbg_witness_free(h)
             self._h = None
 
@@ -359,7 +359,7 @@ class CommitmentOpening:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and nat._lib is not None:
+        if h and nat is not None and getattr(nat, "_lib", None) is not None:
             nat._lib.lbg_opening_free(h)
             self._h = None
 
@@ -395,6 +395,11 @@ class Prover:
             c = Commitment(pr.primes(), r, matrix=m)
         return c, CommitmentOpening(self, op)
 
+    def keep_transform(self, enable: bool = True):
+        """Keep the base limb's transform from commit for the fold, or transform the witness again
+        in the fold (the default); the results are the same."""
+        check(lib().lbg_prover_set_kept_transform(self._h, int(enable)))
+
     def recycle(self, opening: CommitmentOpening):
         lib().lbg_opening_free(opening._take())
 
@@ -406,7 +411,7 @@ class Prover:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and nat._lib is not None:
+        if h and nat is not None and getattr(nat, "_lib", None) is not None:
             nat._lib.lbg_prover_free(h)
             self._h = None
 
@@ -442,7 +447,7 @@ class Transcript:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and nat._lib is not None:
+        if h and nat is not None and getattr(nat, "_lib", None) is not None:
             nat._lib.lbg_transcript_free(h)
             self._h = None
 

@@ -111,7 +111,7 @@ class Server:
             try:
                 b.assign([r.column_log_len for r in reqs])
                 b.witness_random([r.seed for r in reqs], [r.kind for r in reqs])
-                rounds = b.round(self.domain, pool=self.pool, transcript=self.transcript)
+                rounds = b.round(self.domain, pool=self.pool, transcript=self.transcript, copy=self.keep_results)
                 self.batches += 1
                 err = None
             except Exception as e:  # noqa: BLE001 - reported on every request of the batch

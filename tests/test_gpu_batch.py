@@ -25,14 +25,18 @@ def make(row_log, primes, dropped, col_logs):
     return L, pp, b
 
 
-@pytest.mark.parametrize("graphs", [False, True], ids=["stream", "graph"])
-def test_batch_round_equals_single_rounds(graphs):
+@pytest.mark.parametrize("graphs,keep,transcript", [(False, False, "host"), (True, False, "host"),
+                                                    (False, True, "device"), (True, True, "device")],
+                         ids=["stream", "graph", "stream-kept", "graph-kept"])
+def test_batch_round_equals_single_rounds(graphs, keep, transcript):
     col_logs = [3, 1, 5, 2, 4, 1]
     row_log, primes = 7, [3889, 9721]
     L, pp, b = make(row_log, primes, 0, col_logs)
+    if keep:
+        b.keep_transform(True)
     if graphs:
         b.use_graphs(True)
-    rounds = b.round(DOMAIN)
+    rounds = b.round(DOMAIN, transcript=transcript)
     for i, cl in enumerate(col_logs):
         single = product_round((row_log + cl, cl, primes, 0), witness_seed=seeds(len(col_logs))[i])
         assert np.array_equal(rounds[i].matrix, single["commitment"].matrix), i

@@ -183,12 +183,14 @@ def test_fold_and_fold_commitment(oracle, shape):
     verifier = L.Verifier(pp)
     P = oracle_params(oracle, shape)
     elems = w.elements()
-    for ch in [sampled_challenges(oracle, params.columns(), 3), edge_challenges(params.columns())]:
-        c, op = prover.commit(w)
-        v = prover.fold(op, FoldingChallenges(ch))
-        assert np.array_equal(v.elements, oracle.fold(P, elems, ch, threads=8))
-        fc = verifier.fold_commitment(c, FoldingChallenges(ch))
-        assert np.array_equal(fc.rows, oracle.fold_commitment(P, c.matrix, ch))
+    for keep in [True, False]:  # the fold from the kept transform, and transforming the witness again
+        prover.keep_transform(keep)
+        for ch in [sampled_challenges(oracle, params.columns(), 3), edge_challenges(params.columns())]:
+            c, op = prover.commit(w)
+            v = prover.fold(op, FoldingChallenges(ch))
+            assert np.array_equal(v.elements, oracle.fold(P, elems, ch, threads=8)), keep
+            fc = verifier.fold_commitment(c, FoldingChallenges(ch))
+            assert np.array_equal(fc.rows, oracle.fold_commitment(P, c.matrix, ch))
 
 
 def test_verifier_identities_hold_for_gpu_outputs(oracle):
