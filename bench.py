@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-ntt", action="store_true")
+    ap.add_argument("--no-suites", action="store_true")
     ap.add_argument("--ntt-count", type=int, default=1 << 20, help="ring elements of the NTT microbenchmark")
     ap.add_argument("--served-requests", type=int, default=10000)
     ap.add_argument("--served-plain-sample", type=int, default=200)
@@ -341,6 +342,95 @@ def run_batched(instances, steps, flush_bytes=256 << 20):
                                   "transcripts, outputs read back) vs one plain API round per instance"}}
 
 
+def run_suites(steps, flush_bytes=256 << 20):
+    """Every size suite of Params::sized (crates/pcs/src/scheme/params.rs:91-128) in Opening::Clear
+    and bit-dropped mode, plain single-instance path: commit + fold on the device (L2 flushed
+    before each step, CUDA events on the prover's stream, the round's real folding challenges),
+    plus Params::basic() (suite s) as a whole round through the public API and as the device round."""
+    import ctypes
+
+    import torch
+
+    import labinius_b200 as L
+    from labinius_b200._native import check, lib, ptr
+    from labinius_b200.batch import Batch
+
+    N = lib()
+    flush = torch.empty(flush_bytes // 4, dtype=torch.int32, device="cuda")
+    out = []
+    for suite in L.SUITES:
+        for opening in (L.Opening.clear(), L.Opening.bit_dropped(suite.dropped_bits)):
+            params = L.Params.sized(suite, opening)
+            n = params.witness_len()
+            pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+            w = L.Witness.random(pp, WITNESS_SEED)
+            prover, verifier = L.Prover(pp), L.Verifier(pp)
+            c0, op0 = prover.commit(w)
+            t = L.Transcript(DOMAIN)
+            point = verifier.derive_evaluation_point(t, c0)
+            ch = verifier.derive_folding_challenges(t, w.row_evaluate(point))
+            prover.recycle(op0)
+            chal = np.ascontiguousarray(ch.challenges)
+            st = torch.cuda.ExternalStream(N.lbg_prover_stream(prover._h))
+
+            def step():
+                op = ctypes.c_void_p()
+                check(N.lbg_commit(prover._h, w._h, None, None, None, ctypes.byref(op)))
+                check(N.lbg_fold(prover._h, op, ptr(chal), len(chal), None))
+
+            for _ in range(2):
+                step()
+            check(N.lbg_prover_sync(prover._h))
+            ts = []
+            for _ in range(steps):
+                with torch.cuda.stream(st):
+                    flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(st)
+                step()
+                b.record(st)
+                b.synchronize()
+                ts.append(a.elapsed_time(b))
+            ms = float(np.median(ts))
+            out.append({"suite": suite.name[4:], "opening": opening.kind, "log2_n": params.witness_log_len,
+                        "columns": params.columns(), "moduli": params.primes(),
+                        "dropped_bits": params.dropped_bits(), "commit_fold_ms": ms, "elems_s": n / (ms / 1000)})
+            del prover, verifier, w, pp
+    # Params::basic(): the whole round, public API (host transcript) and device round
+    params = L.Params.basic()
+    pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+    w = L.Witness.random(pp, WITNESS_SEED)
+    prover, verifier = L.Prover(pp), L.Verifier(pp)
+
+    def api_round():
+        c, op = prover.commit(w)
+        t = L.Transcript(DOMAIN)
+        point = verifier.derive_evaluation_point(t, c)
+        w.mle_evaluate(point)
+        row = w.row_evaluate(point)
+        ch = verifier.derive_folding_challenges(t, row)
+        prover.fold(op, ch)
+
+    api_round()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        api_round()
+    api_ms = (time.perf_counter() - t0) * 1000 / steps
+    b = Batch(pp, [params.column_log_len])
+    b.witness_random([WITNESS_SEED])
+    b.round(DOMAIN, copy=False)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        b.round(DOMAIN, copy=False)
+    dev_ms = (time.perf_counter() - t0) * 1000 / steps
+    basic = {"suite": "basic", "log2_n": 18, "round_api_ms": api_ms, "round_device_ms": dev_ms,
+             "round_api_elems_s": params.witness_len() / (api_ms / 1000),
+             "round_device_elems_s": params.witness_len() / (dev_ms / 1000),
+             "workload": "Params::basic(): commit, evaluation point, mle and row evaluation, folding challenges, "
+                         "fold; host clock around the calls (results read back)"}
+    return {"plain": out, "basic_round": basic}
+
+
 def run_ntt_micro(steps, count=1 << 20, q=3889):
     """The 648-point forward transform and its inverse over all ring elements of a 2^22 witness
     (2^20 ring elements, q = 3889, coefficients uniform in [0, q) from a seeded generator), each
@@ -624,6 +714,9 @@ def run_ours(args):
     batched = None
     if not args.no_batched:
         batched = run_batched(args.batch_instances, max(3, min(args.steps, 5)))
+    suites = None
+    if not args.no_suites and rank == 0:
+        suites = run_suites(max(3, min(args.steps, 5)))
     ntt_micro = None
     if not args.no_ntt:
         ntt_micro = run_ntt_micro(max(3, min(args.steps, 10)), count=args.ntt_count)
@@ -662,6 +755,7 @@ def run_ours(args):
         "batched": batched,
         "served": served,
         "ntt_microbench": ntt_micro,
+        "suites": suites,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -604,7 +604,25 @@ __global__ void __launch_bounds__(RE_THREADS) k_row_eval(const uint64_t* __restr
   uint64_t S[8][3];
 #pragma unroll
   for (int r = 0; r < 8; r++) S[r][0] = S[r][1] = S[r][2] = 0;
+  // the next group's 8 witness words are loaded one group ahead, under the table build
+  uint64_t wn[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) wn[k] = 0;
+  if (active && g0 < g1) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) wn[k] = __ldg(col + (size_t)(8 * g0 + k) * 3);
+  }
   for (int g = g0; g < g1; g++) {
+    // this group's 8 bit rows of the thread's byte position, transposed: byte r = bit 8m + r of
+    // the 8 rows
+    uint64_t x = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) x |= ((wn[k] >> sh) & 0xFF) << (8 * k);
+    x = transpose8x8(x);
+    if (active && g + 1 < g1) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) wn[k] = __ldg(col + (size_t)(8 * (g + 1) + k) * 3);
+    }
     __syncthreads();  // the previous group's lookups are done with T
     if (t < 32) {
       // 16 combinations of rows 0..3 (t < 16) or 4..7 of the group
@@ -625,10 +643,6 @@ __global__ void __launch_bounds__(RE_THREADS) k_row_eval(const uint64_t* __restr
     for (int q = 0; q < 3; q++) T[t][q] = L4[0][t & 15][q] ^ L4[1][t >> 4][q];
     __syncthreads();
     if (active) {
-      uint64_t x = 0;
-#pragma unroll
-      for (int k = 0; k < 8; k++) x |= ((__ldg(col + (size_t)(8 * g + k) * 3) >> sh) & 0xFF) << (8 * k);
-      x = transpose8x8(x);
 #pragma unroll
       for (int r = 0; r < 8; r++) {
         const uint64_t* e = T[(x >> (8 * r)) & 0xFF];
@@ -1249,8 +1263,8 @@ cudaError_t launch_row_eval(const uint64_t* W, size_t wdim, int cols, const uint
   int sms = 148;
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // enough CTAs for about four per SM, each with at least 8 groups of rows
-  int splits = std::max(1, std::min(G / 8, (4 * sms + ntiles - 1) / ntiles));
+  // enough CTAs for about eight per SM, each with at least 8 groups of rows
+  int splits = std::max(1, std::min(G / 8, (8 * sms + ntiles - 1) / ntiles));
   int gps = (G + splits - 1) / splits;
   splits = (G + gps - 1) / gps;
   k_row_eval<<<dim3(ntiles, splits), RE_THREADS, 0, st>>>(W, (int)wdim, cols, eq, tiles, gps,
