@@ -587,8 +587,7 @@ __global__ void __launch_bounds__(RE_THREADS) k_row_eval(const uint64_t* __restr
                                                          const uint64_t* __restrict__ eq_all,
                                                          const int4* __restrict__ tiles, int groups_per_split,
                                                          unsigned long long* __restrict__ u) {
-  __shared__ uint64_t T[256][3];
-  __shared__ uint64_t L4[2][16][3];
+  __shared__ uint64_t T[2][256][3];  // this group's table and the next one's
   __shared__ uint64_t Q[RE_COLS][21][4];
   int4 tile;
   if (tiles) tile = tiles[blockIdx.x];
@@ -612,45 +611,49 @@ __global__ void __launch_bounds__(RE_THREADS) k_row_eval(const uint64_t* __restr
 #pragma unroll
     for (int k = 0; k < 8; k++) wn[k] = __ldg(col + (size_t)(8 * g0 + k) * 3);
   }
+  // entry t of group g's table: the XOR of eq over the rows 8g + k for the set bits k of t
+  auto build = [&](int g, uint64_t (*Td)[3]) {
+    const uint64_t* e = eq + (size_t)(8 * g) * 3;
+    uint64_t a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      uint64_t msk = 0 - (uint64_t)((t >> k) & 1);
+      a0 ^= __ldg(e + 3 * k) & msk;
+      a1 ^= __ldg(e + 3 * k + 1) & msk;
+      a2 ^= __ldg(e + 3 * k + 2) & msk;
+    }
+    Td[t][0] = a0;
+    Td[t][1] = a1;
+    Td[t][2] = a2;
+  };
+  if (g0 < g1) build(g0, T[0]);
+  __syncthreads();
   for (int g = g0; g < g1; g++) {
+    const int cur = (g - g0) & 1;
     // this group's 8 bit rows of the thread's byte position, transposed: byte r = bit 8m + r of
     // the 8 rows
     uint64_t x = 0;
 #pragma unroll
     for (int k = 0; k < 8; k++) x |= ((wn[k] >> sh) & 0xFF) << (8 * k);
     x = transpose8x8(x);
-    if (active && g + 1 < g1) {
+    if (g + 1 < g1) {
+      if (active) {
 #pragma unroll
-      for (int k = 0; k < 8; k++) wn[k] = __ldg(col + (size_t)(8 * (g + 1) + k) * 3);
+        for (int k = 0; k < 8; k++) wn[k] = __ldg(col + (size_t)(8 * (g + 1) + k) * 3);
+      }
+      build(g + 1, T[cur ^ 1]);
     }
-    __syncthreads();  // the previous group's lookups are done with T
-    if (t < 32) {
-      // 16 combinations of rows 0..3 (t < 16) or 4..7 of the group
-      const uint64_t* e = eq + (size_t)(8 * g + 4 * (t >> 4)) * 3;
-      uint64_t a0 = 0, a1 = 0, a2 = 0;
-      for (int k = 0; k < 4; k++)
-        if ((t >> k) & 1) {
-          a0 ^= __ldg(e + 3 * k);
-          a1 ^= __ldg(e + 3 * k + 1);
-          a2 ^= __ldg(e + 3 * k + 2);
-        }
-      L4[t >> 4][t & 15][0] = a0;
-      L4[t >> 4][t & 15][1] = a1;
-      L4[t >> 4][t & 15][2] = a2;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 3; q++) T[t][q] = L4[0][t & 15][q] ^ L4[1][t >> 4][q];
-    __syncthreads();
     if (active) {
 #pragma unroll
       for (int r = 0; r < 8; r++) {
-        const uint64_t* e = T[(x >> (8 * r)) & 0xFF];
+        const uint64_t* e = T[cur][(x >> (8 * r)) & 0xFF];
         S[r][0] ^= e[0];
         S[r][1] ^= e[1];
         S[r][2] ^= e[2];
       }
     }
+    // the next table is complete, and every lookup into this one is done before it is rebuilt
+    __syncthreads();
   }
   // this thread's share of sum_b x^b S_b: bits 8m + r, placed from word `limb` on
   if (active) {

@@ -250,74 +250,95 @@ __device__ __forceinline__ uint32_t below(dev::Reader& x, uint32_t n) {
   return 0;
 }
 
-// One thread per column: derive("short-challenge") with the column's counter, then the
-// sampler's attempts (crates/pcs/src/challenge.rs:517-533): a partial Fisher-Yates shuffle of
-// 0..161, the sorted positions, the sign hash, and the spectral bound in f64 in the host's
-// operation order (no contraction).
-__global__ void k_challenges(const RoundInst* __restrict__ inst, const int* __restrict__ col_inst, int total_cols,
-                             SamplerTables tab, lbg_challenge_d* __restrict__ out) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= total_cols) return;
+// One warp per column: lane 0 derives "short-challenge" with the column's counter and runs the
+// sampler's sequential part of each attempt (crates/pcs/src/challenge.rs:517-533: a partial
+// Fisher-Yates shuffle of 0..161, the sorted positions, the sign hash); the 32 lanes then test
+// the spectral bound for 81 evaluation points between them, each point's sum in f64 in the host's
+// operation order (no contraction). The first attempt every point passes is the challenge.
+constexpr int CHAL_WARPS = 4;
+
+__global__ void __launch_bounds__(32 * CHAL_WARPS)
+    k_challenges(const RoundInst* __restrict__ inst, const int* __restrict__ col_inst, int total_cols,
+                 SamplerTables tab, lbg_challenge_d* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * CHAL_WARPS + (threadIdx.x >> 5);
+  if (j >= total_cols) return;  // the whole warp
   const RoundInst& I = inst[col_inst[j]];
-  uint64_t jj = (uint64_t)(j - (int)I.col_off);
-  XofRoot root;
-  dev::derive_root(I.st, I.chal_counter + jj, c_chal_label, 15, root);
+  const uint32_t weight = tab.weight < 32 ? tab.weight : 32;
   dev::Reader x;
-  x.init(root);
-  uint32_t weight = tab.weight;
+  if (lane == 0) {
+    XofRoot root;
+    dev::derive_root(I.st, I.chal_counter + (uint64_t)(j - (int)I.col_off), c_chal_label, 15, root);
+    x.init(root);
+  }
   for (int attempt = 0; attempt < 4096; attempt++) {  // an attempt passes with probability ~2/3
-    uint8_t perm[162];
-    for (int i = 0; i < 162; i++) perm[i] = (uint8_t)i;
-    for (uint32_t i = 0; i < weight; i++) {
-      uint32_t k = i + below(x, 162 - i);
-      uint8_t t = perm[i];
-      perm[i] = perm[k];
-      perm[k] = t;
-    }
-    uint64_t seen[3] = {0, 0, 0};
-    for (uint32_t i = 0; i < weight; i++) seen[perm[i] >> 6] |= 1ull << (perm[i] & 63);
-    uint8_t pos[32];
-    for (int i = 0; i < 32; i++) pos[i] = 0;
-    int n = 0;
-    for (int w = 0; w < 3; w++)
-      for (uint64_t b = seen[w]; b; b &= b - 1) pos[n++] = (uint8_t)(64 * w + __ffsll((long long)b) - 1);
-    // signs: derive-key hash of le64(weight) || positions (one block, one chunk, root)
-    uint8_t blk[64];
-    for (int i = 0; i < 64; i++) blk[i] = 0;
-    for (int i = 0; i < 8; i++) blk[i] = (uint8_t)((uint64_t)weight >> (8 * i));
-    for (uint32_t i = 0; i < weight; i++) blk[8 + i] = pos[i];
-    uint32_t m[16], o[16];
-    dev::bytes_to_words(blk, m, 16);
-    dev::compress(tab.signs_key, m, 0, 8 + weight,
-                  b3::DERIVE_KEY_MATERIAL | b3::CHUNK_START | b3::CHUNK_END | b3::ROOT, o);
-    uint32_t signs = o[0] & (uint32_t)((1ull << weight) - 1);
-    bool ok = true;
-    for (int u = 0; u < 81 && ok; u++) {
-      double vr = 0.0, vi = 0.0;
+    uint32_t pw[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // the sorted positions, four per word
+    uint32_t signs = 0;
+    if (lane == 0) {
+      uint8_t perm[162];
+      for (int i = 0; i < 162; i++) perm[i] = (uint8_t)i;
       for (uint32_t i = 0; i < weight; i++) {
-        int p = pos[i];
-        double re = __ldg(tab.re + 81 * p + u), im = __ldg(tab.im + 81 * p + u);
-        bool neg = (signs >> i) & 1;
-        vr = __dadd_rn(vr, neg ? -re : re);
-        vi = __dadd_rn(vi, neg ? -im : im);
+        uint32_t k = i + below(x, 162 - i);
+        uint8_t t = perm[i];
+        perm[i] = perm[k];
+        perm[k] = t;
+      }
+      uint64_t seen[3] = {0, 0, 0};
+      for (uint32_t i = 0; i < weight; i++) seen[perm[i] >> 6] |= 1ull << (perm[i] & 63);
+      uint8_t pos[32];
+      for (int i = 0; i < 32; i++) pos[i] = 0;
+      int n = 0;
+      for (int w = 0; w < 3; w++)
+        for (uint64_t b = seen[w]; b; b &= b - 1) pos[n++] = (uint8_t)(64 * w + __ffsll((long long)b) - 1);
+      // signs: derive-key hash of le64(weight) || positions (one block, one chunk, root)
+      uint8_t blk[64];
+      for (int i = 0; i < 64; i++) blk[i] = 0;
+      for (int i = 0; i < 8; i++) blk[i] = (uint8_t)((uint64_t)weight >> (8 * i));
+      for (uint32_t i = 0; i < weight; i++) blk[8 + i] = pos[i];
+      uint32_t m[16], o[16];
+      dev::bytes_to_words(blk, m, 16);
+      dev::compress(tab.signs_key, m, 0, 8 + weight,
+                    b3::DERIVE_KEY_MATERIAL | b3::CHUNK_START | b3::CHUNK_END | b3::ROOT, o);
+      signs = o[0] & (uint32_t)((1ull << weight) - 1);
+      dev::bytes_to_words(pos, pw, 8);
+    }
+#pragma unroll
+    for (int w = 0; w < 8; w++) pw[w] = __shfl_sync(0xffffffffu, pw[w], 0);
+    signs = __shfl_sync(0xffffffffu, signs, 0);
+    bool bad = false;
+    for (int u = lane; u < 81; u += 32) {
+      double vr = 0.0, vi = 0.0;
+#pragma unroll
+      for (int i = 0; i < 32; i++) {
+        if (i < (int)weight) {
+          int p = (pw[i >> 2] >> (8 * (i & 3))) & 0xFF;
+          double re = __ldg(tab.re + 81 * p + u), im = __ldg(tab.im + 81 * p + u);
+          bool neg = (signs >> i) & 1;
+          vr = __dadd_rn(vr, neg ? -re : re);
+          vi = __dadd_rn(vi, neg ? -im : im);
+        }
       }
       double xx = __dadd_rn(__dmul_rn(vr, vr), __dmul_rn(vi, vi));
-      if (xx > tab.bound_sq) ok = false;
+      if (xx > tab.bound_sq) bad = true;
     }
-    if (ok) {
-      lbg_challenge_d c;
-      for (int i = 0; i < 32; i++) c.positions[i] = pos[i];
-      c.signs = signs;
-      c.weight = weight;
-      out[j] = c;
+    if (!__any_sync(0xffffffffu, bad)) {
+      if (lane == 0) {
+        lbg_challenge_d c;
+        for (int i = 0; i < 32; i++) c.positions[i] = (uint8_t)(pw[i >> 2] >> (8 * (i & 3)));
+        c.signs = signs;
+        c.weight = weight;
+        out[j] = c;
+      }
       return;
     }
   }
-  lbg_challenge_d none;  // weight 0: no challenge found (the host reports it)
-  for (int i = 0; i < 32; i++) none.positions[i] = 0;
-  none.signs = 0;
-  none.weight = 0;
-  out[j] = none;
+  if (lane == 0) {
+    lbg_challenge_d none;  // weight 0: no challenge found (the host reports it)
+    for (int i = 0; i < 32; i++) none.positions[i] = 0;
+    none.signs = 0;
+    none.weight = 0;
+    out[j] = none;
+  }
 }
 
 // One thread per output byte: bit g of the stream is bit r of field f of element g / bits_per.
@@ -455,7 +476,8 @@ cudaError_t sampler_tables(int device, SamplerTables& out) {
 
 cudaError_t launch_challenges(const RoundInst* d_inst, const int* col_inst, int total_cols, SamplerTables tab,
                               lbg_challenge_d* out, cudaStream_t st) {
-  k_challenges<<<(total_cols + 63) / 64, 64, 0, st>>>(d_inst, col_inst, total_cols, tab, out);
+  k_challenges<<<(total_cols + CHAL_WARPS - 1) / CHAL_WARPS, 32 * CHAL_WARPS, 0, st>>>(d_inst, col_inst, total_cols,
+                                                                                     tab, out);
   return cudaGetLastError();
 }
 
