@@ -711,6 +711,31 @@ def run_ours(args):
                "h2d_bytes_per_step": 24 * n + chal.nbytes, "d2h_bytes_per_step": mat.nbytes + vout.nbytes,
                "timing": "host wall clock around synchronous API calls, max over ranks"}
 
+    # the verifier's side of the round (crates/bench/src/bin/labinius.rs:151-176), on the device:
+    # fold_commitment, fold_row_evaluation, verify_evaluation, verify_opening (Clear)
+    verifier_times = None
+    if rank == 0:
+        c1, op1 = prover.commit(w)
+        t1 = L.Transcript(DOMAIN)
+        pt1 = verifier.derive_evaluation_point(t1, c1)
+        mle1, row1 = w.mle_evaluate(pt1), w.row_evaluate(pt1)
+        ch1 = verifier.derive_folding_challenges(t1, row1)
+        v1 = prover.fold(op1, ch1)
+
+        def vstep():
+            fc = verifier.fold_commitment(c1, ch1)
+            fr = verifier.fold_row_evaluation(row1, ch1)
+            verifier.verify_evaluation(pt1, mle1, row1)
+            verifier.verify_opening(c1, ch1, pt1, L.OpeningMessage.clear(fc, v1, fr))
+
+        vstep()
+        tv0 = time.perf_counter()
+        for _ in range(3):
+            vstep()
+        verifier_times = {"verify_ms": (time.perf_counter() - tv0) * 1000 / 3, "accepted": True,
+                          "workload": "fold_commitment + fold_row_evaluation + verify_evaluation + verify_opening "
+                                      "(Clear) at the bench's suite, host clock, inputs from host memory"}
+
     batched = None
     if not args.no_batched:
         batched = run_batched(args.batch_instances, max(3, min(args.steps, 5)))
@@ -756,6 +781,7 @@ def run_ours(args):
         "served": served,
         "ntt_microbench": ntt_micro,
         "suites": suites,
+        "verifier": verifier_times,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

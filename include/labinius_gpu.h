@@ -136,6 +136,23 @@ int lbg_prover_folded(const lbg_prover* pr, int16_t* v_out);
 int lbg_fold_commitment(const lbg_pp* pp, const int16_t* matrix, size_t columns,
                         const lbg_challenge* challenges, size_t r, int16_t* out);
 
+/* Verifier::fold_row_evaluation (crates/pcs/src/scheme/verifier.rs:148-154, eval::fold_binary
+ * crates/pcs/src/eval.rs:195-200): out = sum_j (c_j mod 2) u_j. */
+int lbg_fold_row_evaluation(const lbg_pp* pp, const uint64_t* u, const lbg_challenge* challenges, size_t r,
+                            uint64_t out[3]);
+/* Verifier::verify_evaluation (crates/pcs/src/scheme/verifier.rs:157-174): *accepted = 1 when
+ * u . eq(p1) equals the claimed value (and the lengths match), else 0. */
+int lbg_verify_evaluation(const lbg_pp* pp, const uint64_t* p1, size_t p1_len, const uint64_t claimed[3],
+                          const uint64_t* u, size_t r, int* accepted);
+/* Verifier::verify_folded_opening (crates/pcs/src/scheme/verifier.rs:178-231), Opening::Clear:
+ * *accepted = 1 when v (int16 [len_ring][648]) is centred within the base modulus with its squared
+ * norm within Params::fold_cap, A v equals the folded commitment (int16 [4][limbs][162]) on every
+ * limb, and eq(p0) . (v mod 2) equals the folded row value; else 0. Bit-dropped parameters return
+ * LBG_ERR_UNSUPPORTED. */
+int lbg_verify_folded_opening(const lbg_pp* pp, const int16_t* folded_commitment, const int16_t* v,
+                              const uint64_t* p0, size_t p0_len, const uint64_t folded_row_value[3],
+                              int* accepted);
+
 /* Transcript (crates/pcs/src/challenge.rs:66-161), host side. */
 lbg_transcript* lbg_transcript_new(const uint8_t* domain, size_t len);
 lbg_transcript* lbg_transcript_clone(const lbg_transcript* t);

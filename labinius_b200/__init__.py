@@ -14,6 +14,7 @@ from .scheme import (  # noqa: F401
     FoldingChallenges,
     Modulus,
     Opening,
+    OpeningMessage,
     ParamError,
     Params,
     Prover,

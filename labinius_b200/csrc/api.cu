@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -161,6 +162,7 @@ static int upload_prime(lbg_pp* pp, int k) {
       uint64_t zi = inv_mod(T.z_level[L][kk], q);
       D->zinv3[L][kk] = (uint32_t)(zi * T.inv3 % q);
       D->zinv3sq[L][kk] = (uint32_t)(zi * zi % q * T.inv3 % q);
+      D->zfwd[L][kk] = T.z_level[L][kk];
     }
   }
   D->omega = T.omega;
@@ -779,6 +781,105 @@ int lbg_fold_commitment(const lbg_pp* pp_c, const int16_t* matrix, size_t column
   }
   LBG_CU(cudaMemcpyAsync(out, pp->d_fc, 4 * L * N162 * 2, cudaMemcpyDeviceToHost, pp->stream));
   LBG_CU(cudaStreamSynchronize(pp->stream));
+  return LBG_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// verifier
+// ---------------------------------------------------------------------------------------------
+int lbg_fold_row_evaluation(const lbg_pp* pp_c, const uint64_t* u, const lbg_challenge* challenges, size_t r,
+                            uint64_t out[3]) {
+  if (!pp_c || !u || !challenges || !out) return fail(LBG_ERR_INVALID, "null argument");
+  lbg_pp* pp = const_cast<lbg_pp*>(pp_c);
+  if (r != pp->cols) return fail(LBG_ERR_INVALID, "one challenge per column");
+  std::lock_guard<std::mutex> g(pp->mu);
+  LBG_CU(cudaSetDevice(pp->device));
+  LBG_CU(cudaMemcpyAsync(pp->d_u, u, r * 24, cudaMemcpyHostToDevice, pp->stream));
+  LBG_CU(cudaMemcpyAsync(pp->d_ch, challenges, r * sizeof(lbg_challenge), cudaMemcpyHostToDevice, pp->stream));
+  LBG_CU(launch_fold_binary(pp->d_u, pp->d_ch, (int)r, pp->d_out, pp->stream));
+  LBG_CU(cudaMemcpyAsync(out, pp->d_out, 24, cudaMemcpyDeviceToHost, pp->stream));
+  LBG_CU(cudaStreamSynchronize(pp->stream));
+  return LBG_OK;
+}
+
+int lbg_verify_evaluation(const lbg_pp* pp_c, const uint64_t* p1, size_t p1_len, const uint64_t claimed[3],
+                          const uint64_t* u, size_t r, int* accepted) {
+  if (!pp_c || !p1 || !claimed || !u || !accepted) return fail(LBG_ERR_INVALID, "null argument");
+  lbg_pp* pp = const_cast<lbg_pp*>(pp_c);
+  *accepted = 0;
+  if (r != pp->cols || p1_len != (size_t)pp->params.column_log_len) return LBG_OK;  // Rejected
+  std::lock_guard<std::mutex> g(pp->mu);
+  LBG_CU(cudaSetDevice(pp->device));
+  LBG_CU(cudaMemcpyAsync(pp->d_u, u, r * 24, cudaMemcpyHostToDevice, pp->stream));
+  LBG_CU(cudaMemcpyAsync(pp->d_p + 3 * 32, p1, p1_len * 24, cudaMemcpyHostToDevice, pp->stream));
+  LBG_CU(launch_claim(pp->d_u, (int)r, pp->d_p + 3 * 32, (int)p1_len, pp->d_out, pp->stream));
+  uint64_t t[3];
+  LBG_CU(cudaMemcpyAsync(t, pp->d_out, 24, cudaMemcpyDeviceToHost, pp->stream));
+  LBG_CU(cudaStreamSynchronize(pp->stream));
+  *accepted = t[0] == claimed[0] && t[1] == claimed[1] && t[2] == claimed[2];
+  return LBG_OK;
+}
+
+// Verifier::verify_folded_opening (crates/pcs/src/scheme/verifier.rs:178-231), Opening::Clear: v
+// centred within the base modulus and its squared norm within fold_cap (params.rs:259-265), A v
+// equal to the folded commitment on every limb, and eq(p0) . (v mod 2) equal to the folded row
+// value. Device scratch is allocated per call (a verifier's call, not the prover's hot path).
+int lbg_verify_folded_opening(const lbg_pp* pp_c, const int16_t* folded_commitment, const int16_t* v,
+                              const uint64_t* p0, size_t p0_len, const uint64_t folded_row_value[3],
+                              int* accepted) {
+  if (!pp_c || !folded_commitment || !v || !p0 || !folded_row_value || !accepted)
+    return fail(LBG_ERR_INVALID, "null argument");
+  lbg_pp* pp = const_cast<lbg_pp*>(pp_c);
+  *accepted = 0;
+  if (pp->params.opening != LBG_OPENING_CLEAR) return fail(LBG_ERR_UNSUPPORTED, "the bit-dropped opening check is not on the device");
+  if (4 * pp->len_ring != ((size_t)1 << p0_len) || p0_len != (size_t)(pp->params.witness_log_len - pp->params.column_log_len))
+    return LBG_OK;  // Rejected, as binary_check's length test
+  std::lock_guard<std::mutex> g(pp->mu);
+  LBG_CU(cudaSetDevice(pp->device));
+  cudaStream_t st = pp->stream;
+  size_t L = pp->len_ring, nv = L * N648, fcn = 4 * (size_t)pp->limbs * N162;
+  int16_t* d_v = nullptr;
+  int16_t* d_fc = nullptr;
+  uint32_t* d_vhat = nullptr;
+  uint64_t* d_bits = nullptr;
+  VerifyFlags* d_f = nullptr;
+  auto release = [&]() {
+    cudaFree(d_v);
+    cudaFree(d_fc);
+    cudaFree(d_vhat);
+    cudaFree(d_bits);
+    cudaFree(d_f);
+  };
+  if (cudaMalloc((void**)&d_v, nv * 2) != cudaSuccess || cudaMalloc((void**)&d_fc, fcn * 2) != cudaSuccess ||
+      cudaMalloc((void**)&d_vhat, nv * 4) != cudaSuccess || cudaMalloc((void**)&d_bits, 4 * L * 24) != cudaSuccess ||
+      cudaMalloc((void**)&d_f, sizeof(VerifyFlags)) != cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return fail(LBG_ERR_OOM, "verifier: device allocation failed");
+  }
+  cudaError_t e = cudaMemcpyAsync(d_v, v, nv * 2, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_fc, folded_commitment, fcn * 2, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_f, 0, sizeof(VerifyFlags), st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(pp->d_p, p0, p0_len * 24, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_v_norm(d_v, L, d_f, st);
+  for (int k = 0; k < pp->limbs && e == cudaSuccess; k++)
+    e = launch_v_limb(pp->pidx[k], d_v, L, pp->d_prime[k], d_vhat, pp->d_Ahat + (size_t)k * L * N162 * 2, k,
+                      pp->limbs, d_fc, d_f, st);
+  if (e == cudaSuccess) e = launch_v_parity(d_v, L, d_bits, st);
+  if (e == cudaSuccess) e = launch_eq_table(pp->d_p, (int)p0_len, 4 * L, pp->d_eq, st);
+  if (e == cudaSuccess) e = launch_row_eval(d_bits, 4 * L, 1, pp->d_eq, pp->d_out, st);
+  VerifyFlags f;
+  uint64_t ub[3];
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&f, d_f, sizeof(f), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ub, pp->d_out, 24, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  release();
+  if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("verify: ") + cudaGetErrorString(e));
+  int half = (int)(pp->primes[0] - 1) / 2;
+  double cap = std::ceil(108.0 * (double)(pp->n / 4 * N648));  // recursion::FOLD_CAP * (witness_len / 4) * N
+  bool ok = !f.wrapped && f.worst <= half && (double)f.normsq <= cap && !f.mismatch && ub[0] == folded_row_value[0] &&
+            ub[1] == folded_row_value[1] && ub[2] == folded_row_value[2];
+  *accepted = ok ? 1 : 0;
   return LBG_OK;
 }
 

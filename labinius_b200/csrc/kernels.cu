@@ -978,6 +978,148 @@ __global__ void __launch_bounds__(81 * NTT_E) k_ntt648_inv(const uint16_t* __res
 }
 
 // =============================================================================================
+// The verifier (crates/pcs/src/scheme/verifier.rs:157-231): the norm of v, A v on every limb against
+// the folded commitment, the binary check, the claim and the folded row value
+// =============================================================================================
+// Per ring element, the reference's 16 lane sums of squares (crates/pcs/src/simd/norm.rs:9-50):
+// lane l adds x[32b + 2l]^2 + x[32b + 2l + 1]^2 over the 32-coefficient blocks b (the last block's
+// 8 coefficients fall in lanes 0..3). A lane sum that reaches 2^31 wraps the reference's i32 lanes,
+// which rejects. worst = the largest 16-bit absolute value (|-32768| stays negative and never wins).
+__global__ void k_v_norm(const int16_t* __restrict__ v, size_t len_ring, VerifyFlags* __restrict__ f) {
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= len_ring) return;
+  const int16_t* x = v + e * N648;
+  uint64_t lane[16];
+  for (int l = 0; l < 16; l++) lane[l] = 0;
+  int worst = 0;
+  for (int i = 0; i < N648; i++) {
+    int xi = x[i];
+    lane[(i & 31) >> 1] += (uint64_t)(xi * xi);
+    int a = xi == -32768 ? -32768 : (xi < 0 ? -xi : xi);
+    worst = a > worst ? a : worst;
+  }
+  uint64_t sq = 0;
+  int wrapped = 0;
+  for (int l = 0; l < 16; l++) {
+    sq += lane[l];
+    if (lane[l] >= (1ull << 31)) wrapped = 1;
+  }
+  if (wrapped) atomicOr(&f->wrapped, 1);
+  atomicMax(&f->worst, worst);
+  atomicAdd(&f->normsq, (unsigned long long)sq);
+}
+
+// The 162-point transform of every component of every ring element of v, modulo one limb:
+// vhat[leaf][i][k] (component k of ring element i holds coefficients 4m + k).
+template <int PI>
+__global__ void k_v_transform(const int16_t* __restrict__ v, size_t len_ring, const DevPrime* __restrict__ D,
+                              uint32_t* __restrict__ vhat) {
+  size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= len_ring * 4) return;
+  size_t i = g >> 2;
+  int k = (int)(g & 3);
+  constexpr int32_t q = Pr<PI>::q;
+  uint32_t x[N162];
+  for (int m = 0; m < N162; m++) {
+    int32_t c = v[i * N648 + 4 * m + k] % q;
+    x[m] = (uint32_t)(c < 0 ? c + q : c);
+  }
+  ntt162_serial<PI>(x, *D);
+  for (int leaf = 0; leaf < N162; leaf++) vhat[((size_t)leaf * len_ring + i) * 4 + k] = x[leaf];
+}
+
+// A v at one leaf (one CTA per leaf): Y_k'(leaf) = sum_i the module product of the key's
+// components with v's (the commit's algebra), compared with the folded commitment's slot.
+template <int PI>
+__global__ void __launch_bounds__(256) k_v_mac(const uint32_t* __restrict__ vhat, size_t len_ring,
+                                               const int4* __restrict__ Ahat, const DevPrime* __restrict__ D,
+                                               int limb, int limbs, const int16_t* __restrict__ fc,
+                                               VerifyFlags* __restrict__ f) {
+  const int leaf = blockIdx.x;
+  long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  for (size_t i = threadIdx.x; i < len_ring; i += blockDim.x) {
+    uint4 w = ((const uint4*)vhat)[(size_t)leaf * len_ring + i];
+    int4 lo = __ldg(Ahat + (i * N162 + leaf) * 2), hi = __ldg(Ahat + (i * N162 + leaf) * 2 + 1);
+    long long w0 = w.x, w1 = w.y, w2 = w.z, w3 = w.w;
+    a0 += lo.x * w0 + hi.x * w3 + hi.y * w2 + hi.z * w1;
+    a1 += lo.y * w0 + lo.x * w1 + hi.y * w3 + hi.z * w2;
+    a2 += lo.z * w0 + lo.y * w1 + lo.x * w2 + hi.z * w3;
+    a3 += lo.w * w0 + lo.z * w1 + lo.y * w2 + lo.x * w3;
+  }
+  __shared__ long long red[4][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    a3 += __shfl_xor_sync(0xffffffffu, a3, o);
+  }
+  if (lane == 0) {
+    red[0][warp] = a0;
+    red[1][warp] = a1;
+    red[2][warp] = a2;
+    red[3][warp] = a3;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    constexpr long long q = Pr<PI>::q;
+    int s = D->leaf_to_pow3[leaf];
+    for (int row = 0; row < 4; row++) {
+      long long y = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) y += red[row][w];
+      y %= q;
+      if (y < 0) y += q;
+      if (center<PI>((uint32_t)y) != fc[(row * limbs + limb) * N162 + s]) atomicOr(&f->mismatch, 1);
+    }
+  }
+}
+
+// components_mod_2 (crates/pcs/src/eval.rs:205-230): F162 4m + k holds the parities of
+// coefficients 4p + k of ring element m, bit p.
+__global__ void k_v_parity(const int16_t* __restrict__ v, size_t len_ring, uint64_t* __restrict__ W) {
+  size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= len_ring * 4) return;
+  size_t m = g >> 2;
+  int k = (int)(g & 3);
+  uint64_t w[3] = {0, 0, 0};
+  for (int p = 0; p < N162; p++)
+    if (v[m * N648 + 4 * p + k] & 1) w[p >> 6] |= 1ull << (p & 63);
+  W[3 * g] = w[0];
+  W[3 * g + 1] = w[1];
+  W[3 * g + 2] = w[2];
+}
+
+// fold_binary (crates/pcs/src/eval.rs:195-200): sum_j (c_j mod 2) u_j, c_j mod 2 the F162 with
+// bits at the challenge's positions (crates/pcs/src/challenge.rs:274-281); out zeroed first.
+__global__ void k_fold_binary(const uint64_t* __restrict__ u, const lbg_challenge_d* __restrict__ ch, int r,
+                              unsigned long long* __restrict__ out) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t a0 = 0, a1 = 0, a2 = 0;
+  if (j < r) {
+    F162d c{{0, 0, 0}};
+    uint32_t wgt = ch[j].weight > 32 ? 32 : ch[j].weight;
+    for (uint32_t t = 0; t < wgt; t++) {
+      uint32_t p = ch[j].positions[t];
+      if (p < N162) c.w[p >> 6] |= 1ull << (p & 63);
+    }
+    F162d y = f_mul(c, F162d{{u[3 * j], u[3 * j + 1], u[3 * j + 2]}});
+    a0 = y.w[0];
+    a1 = y.w[1];
+    a2 = y.w[2];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 ^= __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 ^= __shfl_xor_sync(0xffffffffu, a1, o);
+    a2 ^= __shfl_xor_sync(0xffffffffu, a2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicXor(out, (unsigned long long)a0);
+    atomicXor(out + 1, (unsigned long long)a1);
+    atomicXor(out + 2, (unsigned long long)a2);
+  }
+}
+
+// =============================================================================================
 // Witness generation: keyed BLAKE3 XOF of "labinius/witness" (crates/pcs/src/scheme/witness.rs:66-87)
 // =============================================================================================
 __device__ __forceinline__ uint32_t rotr32(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
@@ -1309,6 +1451,32 @@ cudaError_t launch_ntt648(int pi, bool inverse, const uint16_t* in, uint16_t* ou
     default:
       return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_v_norm(const int16_t* v, size_t len_ring, VerifyFlags* f, cudaStream_t st) {
+  k_v_norm<<<blocks_for(len_ring, 128), 128, 0, st>>>(v, len_ring, f);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_v_limb(int pi, const int16_t* v, size_t len_ring, const DevPrime* D, uint32_t* vhat,
+                          const int4* Ahat, int limb, int limbs, const int16_t* fc, VerifyFlags* f, cudaStream_t st) {
+  LBG_DISPATCH(pi, (k_v_transform<P><<<blocks_for(len_ring * 4, 64), 64, 0, st>>>(v, len_ring, D, vhat)));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  LBG_DISPATCH(pi, (k_v_mac<P><<<N162, 256, 0, st>>>(vhat, len_ring, Ahat, D, limb, limbs, fc, f)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_v_parity(const int16_t* v, size_t len_ring, uint64_t* W, cudaStream_t st) {
+  k_v_parity<<<blocks_for(len_ring * 4, 128), 128, 0, st>>>(v, len_ring, W);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fold_binary(const uint64_t* u, const lbg_challenge_d* ch, int r, uint64_t* out, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(out, 0, 24, st);
+  if (e != cudaSuccess) return e;
+  k_fold_binary<<<blocks_for(r, 128), 128, 0, st>>>(u, ch, r, (unsigned long long*)out);
   return cudaGetLastError();
 }
 

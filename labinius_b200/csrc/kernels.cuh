@@ -177,6 +177,40 @@ __device__ void intt162_serial(uint32_t* x, const DevPrime& D) {
   }
 }
 
+// The forward 162-point transform of general coefficients in [0, q), in place on x[0..161], one
+// thread; leaves come out in the tree order the commit uses (the exact inverse of
+// intt162_serial). Used by the verifier, a few thousand per call.
+template <int PI>
+__device__ void ntt162_serial(uint32_t* x, const DevPrime& D) {
+  constexpr uint32_t q = Pr<PI>::q;
+  const uint32_t w = D.omega, w2 = mulmod<PI>(D.omega, D.omega);
+  // level 0: y0 = a + zeta6 b, y1 = a + (1 - zeta6) b
+  for (int i = 0; i < 81; i++) {
+    uint32_t a = x[i], b = x[i + 81];
+    uint32_t t = mulmod<PI>(D.zeta6, b);
+    x[i] = (a + t) % q;
+    x[i + 81] = (a + b + q - t) % q;
+  }
+  // radix-3 levels 1..4: sub-ring k of level L spans n = 81 / 3^{L-1}
+  for (int L = 1; L <= 4; L++) {
+    int n = 81;
+    for (int l = 1; l < L; l++) n /= 3;
+    int m = n / 3;
+    int subrings = 162 / n;
+    for (int k = 0; k < subrings; k++) {
+      uint32_t z = D.zfwd[L][k], z2 = mulmod<PI>(z, z);
+      int base = k * n;
+      for (int i = 0; i < m; i++) {
+        uint32_t a0 = x[base + i];
+        uint32_t t1 = mulmod<PI>(x[base + m + i], z), t2 = mulmod<PI>(x[base + 2 * m + i], z2);
+        x[base + i] = (a0 + t1 + t2) % q;
+        x[base + m + i] = (a0 + mulmod<PI>(w, t1) + mulmod<PI>(w2, t2)) % q;
+        x[base + 2 * m + i] = (a0 + mulmod<PI>(w2, t1) + mulmod<PI>(w, t2)) % q;
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // F162 arithmetic: GF(2)[x]/(x^162 + x^81 + 1) (crates/pcs/src/fields/scalar.rs:65-116)
 // ---------------------------------------------------------------------------------------------

@@ -78,6 +78,22 @@ cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq
 cudaError_t launch_row_eval(const uint64_t* W, size_t wdim, int cols, const uint64_t* eq, uint64_t* u,
                             cudaStream_t st, const int4* tiles = nullptr, int ntiles = 0);
 int row_eval_tile_cols();
+
+// The verifier's checks (crates/pcs/src/scheme/verifier.rs:157-231). Flags zeroed by the caller.
+struct VerifyFlags {
+  unsigned long long normsq;
+  int worst;
+  int wrapped;
+  int mismatch;
+  int pad_;
+};
+cudaError_t launch_v_norm(const int16_t* v, size_t len_ring, VerifyFlags* f, cudaStream_t st);
+// A v modulo one limb against the folded commitment [4][limbs][162]; vhat: len_ring * 648 u32.
+cudaError_t launch_v_limb(int pi, const int16_t* v, size_t len_ring, const DevPrime* D, uint32_t* vhat,
+                          const int4* Ahat, int limb, int limbs, const int16_t* fc, VerifyFlags* f, cudaStream_t st);
+// components_mod_2 of v as 4 len_ring F162.
+cudaError_t launch_v_parity(const int16_t* v, size_t len_ring, uint64_t* W, cudaStream_t st);
+cudaError_t launch_fold_binary(const uint64_t* u, const lbg_challenge_d* ch, int r, uint64_t* out, cudaStream_t st);
 // The reference's 648-point forward transform or its inverse of `count` ring elements (u16 in
 // [0, q), [count][648]) for the splitting prime with index pi; T: device copy of its tables.
 cudaError_t launch_ntt648(int pi, bool inverse, const uint16_t* in, uint16_t* out, size_t count,

@@ -23,6 +23,7 @@ struct DevPrime {
   uint32_t key_D[N162][4][4];
   uint32_t zinv3[5][54];  // 3^-1 z_{L,k}^-1 (inverse transform)
   uint32_t zinv3sq[5][54];  // 3^-1 z_{L,k}^-2
+  uint32_t zfwd[5][54];     // z_{L,k} (forward transform of general coefficients)
   uint32_t omega, inv3, zeta6, det0;
   uint32_t chal[N162 * N162];  // (-1)^p theta^{E[j] p}
 };

@@ -322,6 +322,20 @@ class FoldedWitness:
 
 
 @dataclass
+class OpeningMessage:
+    """OpeningMessage (crates/pcs/src/scheme/verifier.rs): what the prover sends for the opening
+    check; only the Clear arm is checked here."""
+    kind: str
+    folded_commitment: "FoldedCommitment" = None
+    folded_witness: FoldedWitness = None
+    folded_row_value: np.ndarray = None
+
+    @staticmethod
+    def clear(folded_commitment, folded_witness, folded_row_value) -> "OpeningMessage":
+        return OpeningMessage("clear", folded_commitment, folded_witness, folded_row_value)
+
+
+@dataclass
 class FoldedCommitment:
     primes: List[int]
     rows: np.ndarray  # int16 [4][limbs][162]
@@ -507,10 +521,53 @@ class Verifier:
                                         commitment.columns, ptr(ch), len(ch), ptr(out)))
         return FoldedCommitment(self.params.primes(), out)
 
-    def verify_evaluation(self, point: EvaluationPoint, claimed_value, row_evaluation: RowEvaluation, claim_fn):
-        """The claim check u . eq(p1) == t (crates/pcs/src/scheme/verifier.rs:157-174); `claim_fn`
-        computes u . eq(p1) (the verifier side is not on the GPU path)."""
-        if len(row_evaluation.values) != self.params.columns() or len(point.p1) != self.params.column_log_len:
+    def fold_row_evaluation(self, row_evaluation: RowEvaluation, challenges: FoldingChallenges) -> np.ndarray:
+        """u' = sum_j (c_j mod 2) u_j (crates/pcs/src/scheme/verifier.rs:148-154), on the device."""
+        u = np.ascontiguousarray(row_evaluation.values, dtype=np.uint64)
+        ch = np.ascontiguousarray(challenges.challenges, dtype=CHALLENGE_DTYPE)
+        if len(u) != self.params.columns() or len(ch) != len(u):
+            raise ValueError("one challenge per column")
+        out = np.zeros(3, np.uint64)
+        check(lib().lbg_fold_row_evaluation(self.pp._h, ptr(u), ptr(ch), len(ch), ptr(out)))
+        return out
+
+    def verify_evaluation(self, point: EvaluationPoint, claimed_value, row_evaluation: RowEvaluation):
+        """The claim check u . eq(p1) == t (crates/pcs/src/scheme/verifier.rs:157-174), on the device;
+        raises VerificationError on rejection."""
+        u = np.ascontiguousarray(row_evaluation.values, dtype=np.uint64)
+        p1 = np.ascontiguousarray(point.p1, dtype=np.uint64)
+        t = np.ascontiguousarray(claimed_value, dtype=np.uint64)
+        ok = ctypes.c_int(0)
+        check(lib().lbg_verify_evaluation(self.pp._h, ptr(p1), len(p1), ptr(t), ptr(u), len(u), ctypes.byref(ok)))
+        if not ok.value:
             raise VerificationError("Rejected")
-        if not _f162_eq(claim_fn(row_evaluation.values, point.p1), claimed_value):
+
+    def verify_folded_opening(self, folded_commitment: FoldedCommitment, folded_witness: FoldedWitness,
+                              point: EvaluationPoint, folded_row_value):
+        """The Clear opening check (crates/pcs/src/scheme/verifier.rs:178-231) on the device: v in
+        range and within the norm cap, A v equal to the folded commitment on every modulus, and
+        eq(p0) . (v mod 2) equal to u'. Raises VerificationError on rejection."""
+        if list(folded_commitment.primes) != self.params.primes():
             raise VerificationError("Rejected")
+        v = np.ascontiguousarray(folded_witness.elements, dtype=np.int16)
+        if v.shape != (self.params.len_ring(), 648):
+            raise VerificationError("Rejected")
+        fc = np.ascontiguousarray(folded_commitment.rows, dtype=np.int16)
+        p0 = np.ascontiguousarray(point.p0, dtype=np.uint64)
+        fr = np.ascontiguousarray(folded_row_value, dtype=np.uint64)
+        ok = ctypes.c_int(0)
+        check(lib().lbg_verify_folded_opening(self.pp._h, ptr(fc), ptr(v), ptr(p0), len(p0), ptr(fr),
+                                              ctypes.byref(ok)))
+        if not ok.value:
+            raise VerificationError("Rejected")
+
+    def verify_opening(self, commitment: Commitment, challenges: FoldingChallenges, point: EvaluationPoint,
+                       message: "OpeningMessage"):
+        """crates/pcs/src/scheme/verifier.rs:280-337: the check the parameters' opening mode names.
+        Opening::Clear runs on the device; the bit-dropped and recursive arms are not rebuilt."""
+        if self.params.opening.kind != "clear" or message.kind != "clear":
+            if self.params.opening.kind != message.kind:
+                raise VerificationError("Rejected")
+            raise NotImplementedError(f"the {message.kind} opening check is not on the device")
+        self.verify_folded_opening(message.folded_commitment, message.folded_witness, point,
+                                   message.folded_row_value)

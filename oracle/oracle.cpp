@@ -1103,8 +1103,26 @@ int orc_verify_folded_opening(const uint32_t* params, const int16_t* A, const in
   Params pr = make_params(params);
   size_t len_ring = pr.len_ring();
   int half = (int)(pr.primes[0] - 1) / 2;
-  for (size_t i = 0; i < len_ring * N; i++)
-    if (v[i] > half || v[i] < -half) return 0;
+  // the norm (crates/pcs/src/simd/norm.rs:9-50 per element, verifier.rs:189-201): 16 i32 lanes of
+  // pairwise squares per element, rejected when a lane reaches 2^31; the largest 16-bit absolute
+  // value (|-32768| stays negative); the squared norm against fold_cap (params.rs:259-265)
+  uint64_t normsq = 0;
+  int worst = 0;
+  for (size_t e = 0; e < len_ring; e++) {
+    uint64_t lane[16] = {0};
+    for (int i = 0; i < N; i++) {
+      int x = v[e * N + i];
+      lane[(i & 31) >> 1] += (uint64_t)((int64_t)x * x);
+      int a = x == -32768 ? -32768 : (x < 0 ? -x : x);
+      if (a > worst) worst = a;
+    }
+    for (int l = 0; l < 16; l++) {
+      if (lane[l] >= (1ull << 31)) return 0;
+      normsq += lane[l];
+    }
+  }
+  uint64_t fold_cap = (uint64_t)std::ceil(108.0 * (double)(pr.witness_len() / 4 * N));
+  if (worst > half || normsq > fold_cap) return 0;
   for (int k = 0; k < pr.limbs; k++) {
     const Prime& P = prime(pr.primes[k]);
     i64 q = P.q;
