@@ -153,6 +153,16 @@ int lbg_verify_folded_opening(const lbg_pp* pp, const int16_t* folded_commitment
                               const uint64_t* p0, size_t p0_len, const uint64_t folded_row_value[3],
                               int* accepted);
 
+/* switch::prove / prove_bits (crates/pcs/src/switch.rs:64-98, 133-168), the cross-field switch
+ * prover: the trace is the B128 words of the witness w (limbs 0 and 1 of each F162, as
+ * Witness::lifted holds them), r_hi its l = witness_log_len coordinates, r_lo empty (nlo = 0,
+ * words) or the 7 bit coordinates (bits), claim the B128 claim; the transcript t is driven as the
+ * reference's. Out: partials [128][2], rounds [l][2][3] (F162 pairs), opened [3], and the point
+ * the commitment must open at (p0 [row_log][3], p1 [column_log][3]). */
+int lbg_switch_prove(const lbg_pp* pp, const lbg_witness* w, const uint64_t* r_lo, size_t nlo, const uint64_t* r_hi,
+                     size_t l, const uint64_t claim[2], lbg_transcript* t, uint64_t* partials, uint64_t* rounds,
+                     uint64_t opened[3], uint64_t* p0_out, uint64_t* p1_out);
+
 /* Transcript (crates/pcs/src/challenge.rs:66-161), host side. */
 lbg_transcript* lbg_transcript_new(const uint8_t* domain, size_t len);
 lbg_transcript* lbg_transcript_clone(const lbg_transcript* t);

@@ -100,6 +100,7 @@ SIGNATURES = {
     "lbg_fold_row_evaluation": (_int, [_vp, _vp, _vp, _sz, _vp]),
     "lbg_verify_evaluation": (_int, [_vp, _vp, _sz, _vp, _vp, _sz, _vp]),
     "lbg_verify_folded_opening": (_int, [_vp, _vp, _vp, _vp, _sz, _vp, _vp]),
+    "lbg_switch_prove": (_int, [_vp, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "lbg_ntt648_forward": (_int, [ctypes.c_uint32, _vp, _vp, _sz, _vp]),
     "lbg_ntt648_inverse": (_int, [ctypes.c_uint32, _vp, _vp, _sz, _vp]),
     "lbg_batch_stream": (_vp, [_vp]),

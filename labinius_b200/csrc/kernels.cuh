@@ -7,6 +7,7 @@
 #pragma once
 #include <cstdint>
 
+#include "gf2_dev.cuh"
 #include "prime_structs.h"
 #include "ring_tables.h"
 
@@ -209,36 +210,6 @@ __device__ void ntt162_serial(uint32_t* x, const DevPrime& D) {
       }
     }
   }
-}
-
-// ---------------------------------------------------------------------------------------------
-// F162 arithmetic: GF(2)[x]/(x^162 + x^81 + 1) (crates/pcs/src/fields/scalar.rs:65-116)
-// ---------------------------------------------------------------------------------------------
-struct F162d {
-  uint64_t w[3];
-};
-__device__ __forceinline__ F162d f_add(F162d a, F162d b) {
-  return F162d{{a.w[0] ^ b.w[0], a.w[1] ^ b.w[1], a.w[2] ^ b.w[2]}};
-}
-// Shift-and-add product with the reduction folded into the shift (x^162 = x^81 + 1).
-__device__ inline F162d f_mul(F162d a, F162d b) {
-  F162d r{{0, 0, 0}};
-  const uint64_t M34 = (1ull << 34) - 1;
-  for (int i = 161; i >= 0; i--) {
-    // r <- r * x
-    uint64_t top = (r.w[2] >> 33) & 1;
-    r.w[2] = ((r.w[2] << 1) | (r.w[1] >> 63)) & M34;
-    r.w[1] = (r.w[1] << 1) | (r.w[0] >> 63);
-    r.w[0] <<= 1;
-    uint64_t tm = 0 - top;
-    r.w[0] ^= tm & 1;
-    r.w[1] ^= tm & (1ull << 17);
-    uint64_t bm = 0 - ((b.w[i >> 6] >> (i & 63)) & 1);
-    r.w[0] ^= a.w[0] & bm;
-    r.w[1] ^= a.w[1] & bm;
-    r.w[2] ^= a.w[2] & bm;
-  }
-  return r;
 }
 
 }  // namespace lbg

@@ -49,6 +49,35 @@ void Transcript::fill(const char* label, uint8_t* out, size_t n) {
   h.finalize(0, out, n);
 }
 
+void Transcript::absorb_b128(const uint64_t* words, size_t n) {
+  uint8_t b[8];
+  le64(n, b);
+  state_.update(b, 8);
+  for (size_t i = 0; i < 2 * n; i++) {
+    le64(words[i], b);
+    state_.update(b, 8);
+  }
+}
+
+void Transcript::absorb_f162(const uint64_t* words, size_t n) {
+  uint8_t b[8];
+  le64(n, b);
+  state_.update(b, 8);
+  for (size_t i = 0; i < 3 * n; i++) {
+    le64(words[i], b);
+    state_.update(b, 8);
+  }
+}
+
+void Transcript::sample_f162(const char* label, uint64_t* out, size_t n) {
+  std::vector<uint8_t> bytes(24 * n);
+  fill(label, bytes.data(), bytes.size());
+  for (size_t i = 0; i < n; i++) {
+    std::memcpy(out + 3 * i, bytes.data() + 24 * i, 24);
+    out[3 * i + 2] &= (1ull << 34) - 1;
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // the sampler
 // ---------------------------------------------------------------------------------------------

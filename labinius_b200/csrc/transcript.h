@@ -25,6 +25,13 @@ class Transcript {
   void absorb_u64(uint64_t x);
   void absorb_raw(const uint8_t* b, size_t len) { state_.update(b, len); }
   void fill(const char* label, uint8_t* out, size_t n);
+  // absorb_b128 / absorb_f162 (crates/pcs/src/challenge.rs:113-127): the count, then each value's
+  // little-endian words (2 per B128, 3 per F162).
+  void absorb_b128(const uint64_t* words, size_t n);
+  void absorb_f162(const uint64_t* words, size_t n);
+  // sample_f162 (crates/pcs/src/challenge.rs:129-140): n F162, three LE words each, the top one
+  // cut to 34 bits.
+  void sample_f162(const char* label, uint64_t* out, size_t n);
   Blake3 derive(const char* label);
   // The absorbing state and the derivation counter, for moving the transcript to the device.
   const Blake3& state() const { return state_; }

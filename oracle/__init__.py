@@ -69,6 +69,11 @@ def _setup(L):
         "orc_transcript_absorb_bytes": (None, [vp, vp, sz]),
         "orc_transcript_absorb_u64": (None, [vp, u64]),
         "orc_transcript_fill": (None, [vp, ctypes.c_char_p, vp, sz]),
+        "orc_transcript_absorb_raw": (None, [vp, vp, sz]),
+        "orc_switch_prove": (None, [vp, sz, vp, sz, vp, vp, vp, vp, vp, vp, vp]),
+        "orc_switch_verify": (i32, [sz, vp, sz, vp, vp, vp, vp, vp, vp, vp]),
+        "orc_switch_mle": (None, [vp, sz, vp, sz, vp, vp]),
+        "orc_b128_mul": (None, [vp, vp, vp]),
         "orc_sample_short_challenge": (None, [vp, u32, ctypes.c_double, vp, vp]),
         "orc_within": (i32, [vp, ctypes.c_double]),
         "orc_derive_evaluation_point": (None, [vp, vp, vp, vp, vp, vp, vp]),
@@ -405,3 +410,55 @@ def round_trip(params: Params, matrix_seed: bytes, witness_seed: bytes = None, w
         out["folded_commitment"] = fold_commitment(params, C, ch)
     out["transcript_tail"] = t.fill(b"labinius/test-tail", 32)
     return out
+
+
+# ---------------------------------------------------------------------------------------------
+# the cross-field switch (crates/pcs/src/switch.rs)
+# ---------------------------------------------------------------------------------------------
+def _b128(a):
+    a = np.ascontiguousarray(a, dtype=np.uint64).reshape(-1, 2)
+    return a if len(a) else np.zeros((1, 2), np.uint64)
+
+
+def b128_mul(a, b):
+    out = np.zeros(2, np.uint64)
+    lib().orc_b128_mul(_p(np.ascontiguousarray(a, np.uint64)), _p(np.ascontiguousarray(b, np.uint64)), _p(out))
+    return out
+
+
+def switch_mle(trace, r_hi, r_lo=None):
+    """switch::mle (r_lo None) or switch::bit_mle: a B128 [2] claim."""
+    tr = _b128(trace)
+    hi = _b128(r_hi)
+    lo = _b128(r_lo if r_lo is not None else np.zeros((0, 2), np.uint64))
+    nlo = 0 if r_lo is None else len(r_lo)
+    out = np.zeros(2, np.uint64)
+    lib().orc_switch_mle(_p(tr), len(r_hi), _p(lo), nlo, _p(hi), _p(out))
+    return out
+
+
+def switch_prove(trace, r_hi, claim, t: Transcript, r_lo=None):
+    """switch::prove / prove_bits: (partials [128][2], rounds [l][2][3], opened [3], r_pp [l][3])."""
+    l = len(r_hi)
+    nlo = 0 if r_lo is None else len(r_lo)
+    lo = _b128(r_lo if r_lo is not None else np.zeros((0, 2), np.uint64))
+    partials = np.zeros((128, 2), np.uint64)
+    rounds = np.zeros((l, 2, 3), np.uint64)
+    opened = np.zeros(3, np.uint64)
+    r_pp = np.zeros((l, 3), np.uint64)
+    lib().orc_switch_prove(_p(_b128(trace)), l, _p(lo), nlo, _p(_b128(r_hi)), _p(np.ascontiguousarray(claim, np.uint64)),
+                           t.h, _p(partials), _p(rounds), _p(opened), _p(r_pp))
+    return partials, rounds, opened, r_pp
+
+
+def switch_verify(r_hi, claim, partials, rounds, opened, t: Transcript, r_lo=None):
+    """switch::verify / verify_bits: (accepted, r_pp [l][3])."""
+    l = len(r_hi)
+    nlo = 0 if r_lo is None else len(r_lo)
+    lo = _b128(r_lo if r_lo is not None else np.zeros((0, 2), np.uint64))
+    r_pp = np.zeros((max(l, 1), 3), np.uint64)
+    ok = lib().orc_switch_verify(l, _p(lo), nlo, _p(_b128(r_hi)), _p(np.ascontiguousarray(claim, np.uint64)),
+                                 _p(np.ascontiguousarray(partials, np.uint64)),
+                                 _p(np.ascontiguousarray(rounds, np.uint64)),
+                                 _p(np.ascontiguousarray(opened, np.uint64)), t.h, _p(r_pp))
+    return bool(ok), r_pp[:l]

@@ -918,6 +918,128 @@ static Params make_params(const uint32_t* p) {
   return pr;
 }
 
+// ---------------------------------------------------------------------------------------------
+// The cross-field switch (crates/pcs/src/switch.rs, crates/pcs/src/fields/crossfield.rs,
+// crates/pcs/src/fields/sumcheck.rs), restated plainly.
+// ---------------------------------------------------------------------------------------------
+struct B128 {
+  u64 lo, hi;
+};
+static B128 b_add(B128 a, B128 b) { return B128{a.lo ^ b.lo, a.hi ^ b.hi}; }
+static bool b_bit(B128 a, int k) { return ((k < 64 ? a.lo >> k : a.hi >> (k - 64)) & 1) != 0; }
+// GF(2)[x] / (x^128 + x^7 + x^2 + x + 1) (crates/pcs/src/fields/scalar.rs:4, 41-63): the full
+// 256-bit product, then x^128 = x^7 + x^2 + x + 1 applied from the top bit down.
+static B128 b_mul(B128 a, B128 b) {
+  u64 p[4] = {0, 0, 0, 0};
+  u64 aw[2] = {a.lo, a.hi}, bw[2] = {b.lo, b.hi};
+  for (int i = 0; i < 2; i++)
+    for (int j = 0; j < 2; j++) {
+      u64 lo, hi;
+      clmul64(aw[i], bw[j], &lo, &hi);
+      p[i + j] ^= lo;
+      p[i + j + 1] ^= hi;
+    }
+  for (int bit = 255; bit >= 128; bit--) {
+    if ((p[bit >> 6] >> (bit & 63)) & 1) {
+      p[bit >> 6] ^= 1ull << (bit & 63);
+      for (int t : {0, 1, 2, 7}) {
+        int d = bit - 128 + t;
+        p[d >> 6] ^= 1ull << (d & 63);
+      }
+    }
+  }
+  return B128{p[0], p[1]};
+}
+static F162 f_from_b128(B128 x) { return F162{{x.lo, x.hi, 0}}; }
+static const F162 F_ONE = F162{{1, 0, 0}};
+
+// crates/pcs/src/fields/crossfield.rs:78-98 (doubling from the front: the last coordinate is bit 0)
+static std::vector<B128> eq_expand_b128(const std::vector<B128>& r) {
+  std::vector<B128> t(1, B128{1, 0});
+  for (B128 ri : r) {
+    std::vector<B128> n;
+    n.reserve(2 * t.size());
+    for (B128 x : t) {
+      B128 h = b_mul(x, ri);
+      n.push_back(b_add(x, h));
+      n.push_back(h);
+    }
+    t.swap(n);
+  }
+  return t;
+}
+// crates/pcs/src/fields/crossfield.rs:65-76
+static std::vector<F162> eq_expand_f162(const std::vector<F162>& r) {
+  std::vector<F162> t(1, F_ONE);
+  for (F162 ri : r) {
+    std::vector<F162> n;
+    n.reserve(2 * t.size());
+    for (F162 x : t) {
+      F162 h = f_mul(x, ri);
+      n.push_back(f_add(x, h));
+      n.push_back(h);
+    }
+    t.swap(n);
+  }
+  return t;
+}
+
+static void absorb_b128(Transcript& t, const std::vector<B128>& xs) {
+  t.put_u64(xs.size());
+  for (B128 x : xs) {
+    t.put_u64(x.lo);
+    t.put_u64(x.hi);
+  }
+}
+static void absorb_f162(Transcript& t, const std::vector<F162>& xs) {
+  t.put_u64(xs.size());
+  for (F162 x : xs)
+    for (int k = 0; k < 3; k++) t.put_u64(x.w[k]);
+}
+// crates/pcs/src/challenge.rs:129-149
+static std::vector<F162> sample_f162(Transcript& t, const char* label, size_t n) {
+  std::vector<uint8_t> b(24 * n);
+  t.fill(label, b.data(), b.size());
+  std::vector<F162> out(n);
+  for (size_t i = 0; i < n; i++) {
+    std::memcpy(out[i].w, b.data() + 24 * i, 24);
+    out[i].w[2] &= M34;
+  }
+  return out;
+}
+
+// The crossfield Tensor (crates/pcs/src/fields/crossfield.rs:9-62): 128 F162 coefficients of the
+// B128 basis x^i, and transparent_coeff (:100-110).
+static F162 transparent_coeff(const std::vector<B128>& r_hi, const std::vector<F162>& r_pp,
+                              const std::vector<F162>& batch) {
+  std::vector<F162> c(128, f_zero());
+  c[0] = F_ONE;
+  for (size_t i = 0; i < r_hi.size(); i++) {
+    std::vector<F162> vs(128), hs(128, f_zero());
+    for (int k = 0; k < 128; k++) vs[k] = f_mul(c[k], r_pp[i]);
+    for (int k = 127; k >= 0; k--) {
+      // hs = hs * x (coefficients shift up, the top one folds into 0, 1, 2, 7)
+      F162 top = hs[127];
+      for (int m = 127; m > 0; m--) hs[m] = hs[m - 1];
+      hs[0] = f_zero();
+      for (int tap : {0, 1, 2, 7}) hs[tap] = f_add(hs[tap], top);
+      if (b_bit(r_hi[i], k))
+        for (int m = 0; m < 128; m++) hs[m] = f_add(hs[m], c[m]);
+    }
+    for (int k = 0; k < 128; k++) c[k] = f_add(f_add(c[k], vs[k]), hs[k]);
+  }
+  F162 acc = f_zero();
+  for (int k = 0; k < 128; k++) acc = f_add(acc, f_mul(c[k], batch[k]));
+  return acc;
+}
+
+static void absorb_statement(Transcript& t, const std::vector<B128>& r_lo, const std::vector<B128>& r_hi, B128 claim) {
+  t.absorb_bytes((const uint8_t*)"labinius/switch", 15);
+  absorb_b128(t, r_lo);
+  absorb_b128(t, r_hi);
+  absorb_b128(t, std::vector<B128>{claim});
+}
+
 extern "C" {
 
 void orc_blake3(int mode, const uint8_t* key, size_t key_len, const uint8_t* data, size_t len,
@@ -1170,6 +1292,144 @@ void orc_fold_binary(const uint64_t* u, const void* challenges, size_t r, uint64
   F162 acc = f_zero();
   for (size_t j = 0; j < r; j++) acc = f_add(acc, f_mul(challenge_f162(c[j]), ((const F162*)u)[j]));
   std::memcpy(out, acc.w, 24);
+}
+
+
+// switch::prove / prove_bits (crates/pcs/src/switch.rs:133-168): partials [128][2], rounds [l][2][3],
+// opened [3], r_pp [l][3] (the sumcheck's coordinates, in round order).
+void orc_switch_prove(const uint64_t* trace, size_t l, const uint64_t* r_lo, size_t nlo, const uint64_t* r_hi,
+                      const uint64_t* claim, void* t, uint64_t* partials, uint64_t* rounds, uint64_t* opened,
+                      uint64_t* r_pp) {
+  Transcript& tr = *(Transcript*)t;
+  size_t n = (size_t)1 << l;
+  std::vector<B128> lo(nlo), hi(l), tw(n);
+  for (size_t i = 0; i < nlo; i++) lo[i] = B128{r_lo[2 * i], r_lo[2 * i + 1]};
+  for (size_t i = 0; i < l; i++) hi[i] = B128{r_hi[2 * i], r_hi[2 * i + 1]};
+  for (size_t j = 0; j < n; j++) tw[j] = B128{trace[2 * j], trace[2 * j + 1]};
+  absorb_statement(tr, lo, hi, B128{claim[0], claim[1]});
+  std::vector<B128> eq = eq_expand_b128(hi);
+  std::vector<B128> v(128, B128{0, 0});
+  for (size_t j = 0; j < n; j++)
+    for (int k = 0; k < 128; k++)
+      if (b_bit(tw[j], k)) v[k] = b_add(v[k], eq[j]);
+  absorb_b128(tr, v);
+  std::vector<F162> batch = eq_expand_f162(sample_f162(tr, "labinius/switch-batch", 7));
+  std::vector<F162> a(n), pp(n);
+  for (size_t j = 0; j < n; j++) {
+    F162 x = f_zero();
+    for (int k = 0; k < 128; k++)
+      if (b_bit(eq[j], k)) x = f_add(x, batch[k]);
+    a[j] = x;
+    pp[j] = f_from_b128(tw[j]);
+  }
+  size_t half = n;
+  for (size_t round = 0; round < l; round++) {
+    half /= 2;
+    F162 e0 = f_zero(), einf = f_zero();
+    for (size_t j = 0; j < half; j++) {
+      e0 = f_add(e0, f_mul(a[j], pp[j]));
+      einf = f_add(einf, f_mul(f_add(a[j], a[j + half]), f_add(pp[j], pp[j + half])));
+    }
+    absorb_f162(tr, std::vector<F162>{e0, einf});
+    F162 r = sample_f162(tr, "labinius/switch-round", 1)[0];
+    for (size_t j = 0; j < half; j++) {
+      a[j] = f_add(a[j], f_mul(r, f_add(a[j], a[j + half])));
+      pp[j] = f_add(pp[j], f_mul(r, f_add(pp[j], pp[j + half])));
+    }
+    std::memcpy(rounds + 6 * round, e0.w, 24);
+    std::memcpy(rounds + 6 * round + 3, einf.w, 24);
+    std::memcpy(r_pp + 3 * round, r.w, 24);
+  }
+  for (int k = 0; k < 128; k++) {
+    partials[2 * k] = v[k].lo;
+    partials[2 * k + 1] = v[k].hi;
+  }
+  std::memcpy(opened, pp[0].w, 24);
+}
+
+// switch::verify / verify_bits (crates/pcs/src/switch.rs:171-209): 1 on acceptance, r_pp out.
+int orc_switch_verify(size_t l, const uint64_t* r_lo, size_t nlo, const uint64_t* r_hi, const uint64_t* claim,
+                      const uint64_t* partials, const uint64_t* rounds, const uint64_t* opened, void* t,
+                      uint64_t* r_pp) {
+  Transcript& tr = *(Transcript*)t;
+  std::vector<B128> lo(nlo), hi(l), v(128);
+  for (size_t i = 0; i < nlo; i++) lo[i] = B128{r_lo[2 * i], r_lo[2 * i + 1]};
+  for (size_t i = 0; i < l; i++) hi[i] = B128{r_hi[2 * i], r_hi[2 * i + 1]};
+  for (int k = 0; k < 128; k++) v[k] = B128{partials[2 * k], partials[2 * k + 1]};
+  B128 cl{claim[0], claim[1]};
+  absorb_statement(tr, lo, hi, cl);
+  // weights: eq(r_lo, k) for bits, the basis x^k for words
+  std::vector<B128> w;
+  if (nlo == 0)
+    for (int k = 0; k < 128; k++) w.push_back(k < 64 ? B128{1ull << k, 0} : B128{0, 1ull << (k - 64)});
+  else
+    w = eq_expand_b128(lo);
+  B128 rec{0, 0};
+  for (int k = 0; k < 128; k++) rec = b_add(rec, b_mul(v[k], w[k]));
+  if (rec.lo != cl.lo || rec.hi != cl.hi) return 0;
+  absorb_b128(tr, v);
+  std::vector<F162> batch = eq_expand_f162(sample_f162(tr, "labinius/switch-batch", 7));
+  // slice_sum: u[k] bit i = bit k of v[i]
+  F162 s = f_zero();
+  for (int k = 0; k < 128; k++) {
+    B128 u{0, 0};
+    for (int i = 0; i < 128; i++)
+      if (b_bit(v[i], k)) (i < 64 ? u.lo : u.hi) |= 1ull << (i & 63);
+    s = f_add(s, f_mul(f_from_b128(u), batch[k]));
+  }
+  std::vector<F162> rp;
+  for (size_t round = 0; round < l; round++) {
+    F162 e0, einf;
+    std::memcpy(e0.w, rounds + 6 * round, 24);
+    std::memcpy(einf.w, rounds + 6 * round + 3, 24);
+    absorb_f162(tr, std::vector<F162>{e0, einf});
+    F162 r = sample_f162(tr, "labinius/switch-round", 1)[0];
+    F162 e1 = f_add(s, e0);
+    s = f_add(f_add(e0, f_mul(r, f_add(f_add(e0, e1), einf))), f_mul(f_mul(r, r), einf));
+    rp.push_back(r);
+    std::memcpy(r_pp + 3 * round, r.w, 24);
+  }
+  F162 d = transparent_coeff(hi, rp, batch);
+  if (d.w[0] == 0 && d.w[1] == 0 && d.w[2] == 0) return 0;
+  F162 op;
+  std::memcpy(op.w, opened, 24);
+  F162 want = f_mul(d, op);
+  return s.w[0] == want.w[0] && s.w[1] == want.w[1] && s.w[2] == want.w[2];
+}
+
+// switch::mle and bit_mle (crates/pcs/src/switch.rs:38-58).
+void orc_switch_mle(const uint64_t* trace, size_t l, const uint64_t* r_lo, size_t nlo, const uint64_t* r_hi,
+                    uint64_t* out) {
+  size_t n = (size_t)1 << l;
+  std::vector<B128> hi(l), lo(nlo);
+  for (size_t i = 0; i < l; i++) hi[i] = B128{r_hi[2 * i], r_hi[2 * i + 1]};
+  for (size_t i = 0; i < nlo; i++) lo[i] = B128{r_lo[2 * i], r_lo[2 * i + 1]};
+  std::vector<B128> eq = eq_expand_b128(hi), eql;
+  if (nlo) eql = eq_expand_b128(lo);
+  B128 acc{0, 0};
+  for (size_t j = 0; j < n; j++) {
+    B128 word{trace[2 * j], trace[2 * j + 1]};
+    if (nlo) {
+      B128 bits{0, 0};
+      for (int k = 0; k < 128; k++)
+        if (b_bit(word, k)) bits = b_add(bits, eql[k]);
+      word = bits;
+    }
+    acc = b_add(acc, b_mul(word, eq[j]));
+  }
+  out[0] = acc.lo;
+  out[1] = acc.hi;
+}
+
+void orc_b128_mul(const uint64_t* a, const uint64_t* b, uint64_t* out) {
+  B128 r = b_mul(B128{a[0], a[1]}, B128{b[0], b[1]});
+  out[0] = r.lo;
+  out[1] = r.hi;
+}
+
+void orc_transcript_absorb_raw(void* t, const uint8_t* b, size_t len) {
+  Transcript& tr = *(Transcript*)t;
+  tr.state.insert(tr.state.end(), b, b + len);
 }
 
 }  // extern "C"
