@@ -269,6 +269,21 @@ typedef struct lbg_batch_outputs {
   int16_t* v;                 /* [count][len_ring][648] */
 } lbg_batch_outputs;
 int lbg_batch_round(lbg_batch* b, const uint8_t* domain, size_t domain_len, const lbg_batch_outputs* out);
+/* Instances of the assigned layout that are B128 traces (Witness::lifted, e.g. kind 1 of
+ * lbg_batch_witness_generate) opened through the cross-field switch. Their device round is that of
+ * crates/pcs/examples/two_fields.rs:176-194: Prover::commit, absorb_bytes(Commitment::to_bytes),
+ * switch::prove (crates/pcs/src/switch.rs:65-74), row_evaluate at the switch's point,
+ * FoldingChallenges::derive, Prover::fold; the mle output is the value at that point. flags[i] = 1
+ * marks instance i; r_hi holds, for each marked instance in order, its witness_log_len B128
+ * coordinates (2 words each); claims holds one B128 per marked instance, or is null, and then each
+ * marked instance states its trace's value at r_hi (word-level statements). Kept until the next
+ * lbg_batch_assign; flags null unmarks every instance. */
+int lbg_batch_set_switch(lbg_batch* b, const uint8_t* flags, const uint64_t* r_hi, const uint64_t* claims);
+/* After lbg_batch_round: each marked instance's switch proof in order (crates/pcs/src/switch.rs:19-27):
+ * partials [128][2], rounds [l][2][3] (one instance after another), opened [3], and its claim [2].
+ * Any pointer may be null. */
+int lbg_batch_switch_outputs(const lbg_batch* b, uint64_t* partials, uint64_t* rounds, uint64_t* opened,
+                             uint64_t* claims);
 void* lbg_batch_stream(const lbg_batch* b);
 uint64_t lbg_batch_launch_count(const lbg_batch* b);
 

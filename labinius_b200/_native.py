@@ -95,6 +95,8 @@ SIGNATURES = {
     "lbg_batch_mle_evaluate": (_int, [_vp, _vp, _vp, _vp]),
     "lbg_batch_fold": (_int, [_vp, _vp, _sz, _vp]),
     "lbg_batch_round": (_int, [_vp, _vp, _sz, _vp]),
+    "lbg_batch_set_switch": (_int, [_vp, _vp, _vp, _vp]),
+    "lbg_batch_switch_outputs": (_int, [_vp, _vp, _vp, _vp, _vp]),
     "lbg_prover_set_kept_transform": (_int, [_vp, _int]),
     "lbg_batch_set_kept_transform": (_int, [_vp, _int]),
     "lbg_fold_row_evaluation": (_int, [_vp, _vp, _vp, _sz, _vp]),

@@ -45,6 +45,8 @@ class InstanceRound:
     mle: np.ndarray = None
     challenges: np.ndarray = None
     v: np.ndarray = None
+    switch: object = None      # SwitchProof of a B128 instance opened through the switch
+    claim: np.ndarray = None   # its B128 claim (uint64 [2])
 
 
 class Batch:
@@ -78,11 +80,38 @@ class Batch:
         self.cols = [1 << c for c in self.column_log_lens]
         self.col_off = np.concatenate([[0], np.cumsum(self.cols)]).astype(np.int64)
         self.total_cols = int(self.col_off[-1])
+        self.switch_flags = []
 
     def assign(self, column_log_lens):
         arr = np.array([int(c) for c in column_log_lens], np.uint32)
         check(lib().lbg_batch_assign(self._h, ptr(arr), len(arr)))
         self._layout(column_log_lens)
+
+    def set_switch(self, flags=None, r_his=None, claims=None):
+        """Mark instances as B128 traces (Witness::lifted, kind 1 of witness_random) that the device
+        round opens through the cross-field switch, as crates/pcs/examples/two_fields.rs:176-194
+        does: commit, absorb Commitment::to_bytes, switch::prove, row_evaluate at the switch's
+        point, FoldingChallenges::derive, fold. r_his: one array of witness_log_len B128
+        coordinates ([l][2] uint64) per marked instance, in order; claims: one B128 per marked
+        instance, or None (each instance states its trace's value at its point). None unmarks."""
+        if flags is None:
+            check(lib().lbg_batch_set_switch(self._h, None, None, None))
+            self.switch_flags = [0] * self.count
+            return
+        f = np.ascontiguousarray([1 if x else 0 for x in flags], np.uint8)
+        if len(f) != self.count:
+            raise ValueError("one flag per instance")
+        marked = [i for i in range(self.count) if f[i]]
+        if len(r_his) != len(marked):
+            raise ValueError("one point per marked instance")
+        for k, i in enumerate(marked):
+            if np.asarray(r_his[k]).size != 2 * (self.row_log + self.column_log_lens[i]):
+                raise ValueError("the point does not match the instance")
+        r = np.ascontiguousarray(np.concatenate([np.asarray(x, np.uint64).reshape(-1) for x in r_his])
+                                 if marked else np.zeros(2, np.uint64))
+        c = None if claims is None else np.ascontiguousarray(np.asarray(claims, np.uint64).reshape(-1, 2))
+        check(lib().lbg_batch_set_switch(self._h, ptr(f), ptr(r), ptr(c)))
+        self.switch_flags = list(f)
 
     def params_of(self, i) -> Params:
         p = self.pp.params
@@ -193,6 +222,8 @@ class Batch:
         valid until its next round."""
         if transcript == "device":
             return self._round_device(domain, copy)
+        if any(getattr(self, "switch_flags", [])):
+            raise ValueError("switch instances run their transcript on the device")
         rounds = self.commit()
         run = (lambda f, xs: list(pool.map(f, xs))) if pool is not None else (lambda f, xs: [f(x) for x in xs])
         ts = run(lambda i: self._point(i, rounds[i], domain), range(self.count))
@@ -261,7 +292,26 @@ class Batch:
                     if val is not None:
                         setattr(r, k, np.array(val))
             rounds.append(r)
+        self._attach_switch(rounds)
         return rounds
+
+    def _attach_switch(self, rounds):
+        from .switch import SwitchProof
+
+        marked = [i for i, f in enumerate(getattr(self, "switch_flags", [])) if f]
+        if not marked:
+            return
+        ls = [self.row_log + self.column_log_lens[i] for i in marked]
+        partials = np.zeros((len(marked), 128, 2), np.uint64)
+        rs = np.zeros((sum(ls), 2, 3), np.uint64)
+        opened = np.zeros((len(marked), 3), np.uint64)
+        claims = np.zeros((len(marked), 2), np.uint64)
+        check(lib().lbg_batch_switch_outputs(self._h, ptr(partials), ptr(rs), ptr(opened), ptr(claims)))
+        o = 0
+        for k, i in enumerate(marked):
+            rounds[i].switch = SwitchProof(partials[k], rs[o:o + ls[k]], opened[k])
+            rounds[i].claim = claims[k]
+            o += ls[k]
 
     def launch_count(self) -> int:
         return int(lib().lbg_batch_launch_count(self._h))

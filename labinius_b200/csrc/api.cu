@@ -16,6 +16,7 @@
 #include "launch.h"
 #include "ring_tables.h"
 #include "transcript.h"
+#include "upload.h"
 
 using namespace lbg;
 
@@ -171,7 +172,7 @@ static int upload_prime(lbg_pp* pp, int k) {
   D->det0 = T.det0;
   std::memcpy(D->chal, T.chal_table.data(), sizeof(D->chal));
   cudaError_t e = cudaMalloc((void**)&pp->d_prime[k], sizeof(DevPrime));
-  if (e == cudaSuccess) e = cudaMemcpy(pp->d_prime[k], D, sizeof(DevPrime), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = upload_sync(pp->d_prime[k], D, sizeof(DevPrime));
   delete D;
   if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("prime tables: ") + cudaGetErrorString(e));
   return LBG_OK;
@@ -193,6 +194,7 @@ void lbg_public_parameters_free(lbg_pp* pp) {
   cudaFree(pp->d_ch);
   cudaFree(pp->d_chat);
   cudaFree(pp->d_fc);
+  lbg_switch_release(pp);
   if (pp->stream) cudaStreamDestroy(pp->stream);
   delete pp;
 }
@@ -303,7 +305,7 @@ int lbg_witness_from_host(const lbg_pp* pp, const uint64_t* f162, size_t n, lbg_
   lbg_witness* w;
   int rc = witness_alloc(pp, n, &w);
   if (rc) return rc;
-  if (cudaMemcpy(w->d, f162, n * 24, cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (upload_sync(w->d, f162, n * 24) != cudaSuccess) {
     witness_release(w);
     return fail(LBG_ERR_CUDA, "witness upload");
   }
@@ -321,7 +323,7 @@ int lbg_witness_lifted(const lbg_pp* pp, const uint64_t* b128, size_t n, lbg_wit
   if (rc) return rc;
   uint64_t* tmp = nullptr;
   cudaError_t e = cudaMalloc((void**)&tmp, n * 16);
-  if (e == cudaSuccess) e = cudaMemcpy(tmp, b128, n * 16, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tmp, b128, n * 16, cudaMemcpyHostToDevice, pp->stream);
   if (e == cudaSuccess) e = launch_lift_b128(tmp, n, w->d, pp->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(pp->stream);
   cudaFree(tmp);

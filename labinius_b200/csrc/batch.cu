@@ -19,6 +19,7 @@
 #include "handles.h"
 #include "launch.h"
 #include "ring_tables.h"
+#include "switch.h"
 #include "transcript.h"
 #include "transcript_dev.h"
 
@@ -90,6 +91,17 @@ struct lbg_batch {
   size_t packed_cap = 0;
   std::vector<uint64_t> packed_off, packed_len;
   PackDropped pack{};
+  // switch instances: lifted B128 traces opened through the cross-field switch
+  std::vector<uint8_t> sw_flag;     // [count]
+  std::vector<SwInst> sw_h;         // host copies of the device table, in instance order
+  SwInst* d_sw_inst = nullptr;
+  size_t sw_inst_cap = 0;
+  SwSmall* d_sw_small = nullptr;
+  size_t sw_small_cap = 0;
+  uint8_t* d_sw_scratch = nullptr;
+  size_t sw_scratch_cap = 0;
+  uint64_t* d_sw_r = nullptr;       // the statements' r_hi
+  size_t sw_r_cap = 0;
 };
 
 static void free_graphs(lbg_batch* b) {
@@ -148,7 +160,7 @@ static int upload_splits(lbg_batch* b, int per) {
   std::vector<int> inst(b->total_cols / per);
   for (int i = 0; i < b->count; i++)
     for (size_t c = b->col_off[i]; c < b->col_off[i + 1]; c += per) inst[c / per] = i;
-  LBG_BCU(cudaMemcpy(b->d_split_inst, inst.data(), inst.size() * sizeof(int), cudaMemcpyHostToDevice));
+  LBG_BCU(cudaMemcpyAsync(b->d_split_inst, inst.data(), inst.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   b->fold_per = per;
   return LBG_OK;
 }
@@ -201,11 +213,15 @@ static void le64(uint64_t x, uint8_t* b) {
   for (int i = 0; i < 8; i++) b[i] = (uint8_t)(x >> (8 * i));
 }
 
+static bool is_switch(const lbg_batch* b, int i) { return !b->sw_flag.empty() && b->sw_flag[i]; }
+
 // Each instance's transcript up to the commitment's own bytes (host, once per layout and domain),
 // the byte layout of the two device absorbs (the commitment; the row values with their framing)
 // and the derivation counters. The transcript steps are those of derive_evaluation_point and
 // FoldingChallenges::derive (crates/pcs/src/scheme/verifier.rs:41-100,
-// crates/pcs/src/scheme/commitment.rs:217-229).
+// crates/pcs/src/scheme/commitment.rs:217-229); a switch instance's are those of a B128 trace
+// opened through the switch (crates/pcs/examples/two_fields.rs:176-194): the tagged commitment
+// (Commitment::to_bytes), the switch's own steps, then FoldingChallenges::derive.
 static int plan_round(lbg_batch* b, const uint8_t* domain, size_t domain_len) {
   const lbg_pp* pp = b->pp;
   int L = pp->limbs;
@@ -245,24 +261,42 @@ static int plan_round(lbg_batch* b, const uint8_t* domain, size_t domain_len) {
     RoundShape s = base;
     s.column_log_len = b->col_log[i];
     s.witness_log_len = row_log + b->col_log[i];
+    bool sw = is_switch(b, i);
+    uint32_t l = row_log + b->col_log[i];
     Transcript t(domain, domain_len);
-    absorb_commitment_header(s, t);
+    if (!sw) absorb_commitment_header(s, t);
     t.state().save(pre[i]);
     uint64_t len0 = absorbed_len(pre[i]);
     uint64_t cols = b->col_off[i + 1] - b->col_off[i];
     AbsorbSource sc;
     std::memset(&sc, 0, sizeof(sc));
+    // Commitment::to_bytes (crates/pcs/src/wire/mod.rs:307-333) as absorb_bytes frames it: the
+    // length, the form's tag, the column count (u32), then the body
+    auto tagged = [&](uint8_t tag, uint64_t body) {
+      le64(5 + body, sc.prefix);
+      sc.prefix[8] = tag;
+      for (int k = 0; k < 4; k++) sc.prefix[9 + k] = (uint8_t)(cols >> (8 * k));
+      sc.prefix_len = 13;
+    };
     if (!dropped) {
-      // absorb_elements per column: le64(4), then the column's 4 x limbs x 162 i16, little-endian
-      le64(4, sc.hdr);
-      sc.hdr_len = 8;
+      if (sw) {
+        tagged(0, cols * 4 * L * N162 * 2);  // the matrix column by column, i16 little-endian
+      } else {
+        // absorb_elements per column: le64(4), then the column's 4 x limbs x 162 i16, little-endian
+        le64(4, sc.hdr);
+        sc.hdr_len = 8;
+      }
       sc.rows = (uint32_t)cols;
       sc.row_bytes = (uint32_t)(4 * L * N162 * 2);
       sc.row_stride = sc.row_bytes;
       sc.data = (const uint8_t*)(b->d_C + b->col_off[i] * 4 * L * N162);
     } else {
-      le64(b->packed_len[i], sc.prefix);
-      sc.prefix_len = 8;
+      if (sw) {
+        tagged(2, b->packed_len[i]);
+      } else {
+        le64(b->packed_len[i], sc.prefix);
+        sc.prefix_len = 8;
+      }
       sc.rows = 1;
       sc.row_bytes = (uint32_t)b->packed_len[i];
       sc.row_stride = 0;
@@ -279,17 +313,19 @@ static int plan_round(lbg_batch* b, const uint8_t* domain, size_t domain_len) {
     su.rows = 1;
     su.row_bytes = (uint32_t)(24 * cols);
     su.data = (const uint8_t*)(b->d_u + 3 * b->col_off[i]);
-    plan_absorb(b->ab_u, b->d_states + i, len0 + sc.length(), su);
+    uint64_t sw_bytes = sw ? sw_transcript_bytes(l, 0) : 0;
+    plan_absorb(b->ab_u, b->d_states + i, len0 + sc.length() + sw_bytes, su);
     ri[i].st = b->d_states + i;
     ri[i].point_counter = t.counter();
-    ri[i].chal_counter = t.counter() + 1;
+    // the switch derives the batch, then one challenge per round
+    ri[i].chal_counter = t.counter() + (sw ? 1 + l : 1);
     ri[i].row_log = row_log;
     ri[i].col_log = b->col_log[i];
     ri[i].col_off = (uint32_t)b->col_off[i];
     ri[i].pad_ = 0;
   }
-  LBG_BCU(cudaMemcpy(b->d_prefix, pre.data(), pre.size() * sizeof(HasherState), cudaMemcpyHostToDevice));
-  LBG_BCU(cudaMemcpy(b->d_inst, ri.data(), ri.size() * sizeof(RoundInst), cudaMemcpyHostToDevice));
+  LBG_BCU(cudaMemcpyAsync(b->d_prefix, pre.data(), pre.size() * sizeof(HasherState), cudaMemcpyHostToDevice, b->stream));
+  LBG_BCU(cudaMemcpyAsync(b->d_inst, ri.data(), ri.size() * sizeof(RoundInst), cudaMemcpyHostToDevice, b->stream));
   LBG_BCU(upload_absorb(b->ab_commit));
   LBG_BCU(upload_absorb(b->ab_u));
   LBG_BCU(grow((void**)&b->d_stage, &b->stage_cap, std::max(b->ab_commit.stage_bytes, b->ab_u.stage_bytes)));
@@ -322,6 +358,9 @@ static cudaError_t enqueue_round(lbg_batch* b) {
   }
   if (e == cudaSuccess) e = launch_absorb(b->ab_commit, b->d_stage, b->d_cvs, b->d_oldcv, b->stream);
   if (e == cudaSuccess) e = launch_point(b->d_inst, b->count, (uint32_t)row_log, b->d_p0, b->d_p1, b->stream);
+  // switch instances: their evaluation point is where the switch's sumcheck ends
+  if (e == cudaSuccess && !b->sw_h.empty())
+    e = enqueue_switch(b->d_sw_inst, b->sw_h.data(), (int)b->sw_h.size(), b->stream, &b->launches);
   if (e == cudaSuccess) e = launch_eq_table(b->d_p0, row_log, b->wdim, b->d_eq, b->stream, b->count);
   if (e == cudaSuccess) e = launch_row_eval(b->d_w, b->wdim, cols, b->d_eq, b->d_u, b->stream, b->d_row_tiles, b->n_row_tiles);
   if (e == cudaSuccess) e = launch_claims(b->d_inst, b->d_col_inst, b->d_u, cols, b->d_p1, b->count, b->d_claim, b->stream);
@@ -341,7 +380,8 @@ void lbg_batch_free(lbg_batch* b) {
   free_graphs(b);
   void* ptrs[] = {b->d_w, b->d_col_inst, b->d_row_tiles, b->d_split_inst, b->d_partial, b->d_C, b->d_res, b->d_top, b->d_digits,
                   b->d_p0, b->d_p1, b->d_eq, b->d_u, b->d_claim, b->d_ch, b->d_chat, b->d_vhat, b->d_v,
-                  b->d_prefix, b->d_states, b->d_inst, b->d_oldcv, b->d_stage, b->d_cvs, b->d_packed, b->d_keep};
+                  b->d_prefix, b->d_states, b->d_inst, b->d_oldcv, b->d_stage, b->d_cvs, b->d_packed, b->d_keep,
+                  b->d_sw_inst, b->d_sw_small, b->d_sw_scratch, b->d_sw_r};
   for (void* p : ptrs) cudaFree(p);
   b->ab_commit.release();
   b->ab_u.release();
@@ -430,6 +470,8 @@ int lbg_batch_assign(lbg_batch* b, const uint32_t* column_log_lens, size_t count
     b->graphs = false;
   }
   b->plan_ok = false;
+  b->sw_flag.clear();
+  b->sw_h.clear();
   b->count = (int)count;
   b->col_log = cl;
   b->col_off = off;
@@ -438,13 +480,14 @@ int lbg_batch_assign(lbg_batch* b, const uint32_t* column_log_lens, size_t count
   std::vector<int> ci(b->total_cols);
   for (int i = 0; i < b->count; i++)
     for (size_t c = off[i]; c < off[i + 1]; c++) ci[c] = i;
-  LBG_BCU(cudaMemcpy(b->d_col_inst, ci.data(), ci.size() * sizeof(int), cudaMemcpyHostToDevice));
+  LBG_BCU(cudaMemcpyAsync(b->d_col_inst, ci.data(), ci.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   std::vector<int4> rtiles;
   int tc = row_eval_tile_cols();
   for (int i = 0; i < b->count; i++)
     for (size_t c = off[i]; c < off[i + 1]; c += tc)
       rtiles.push_back(make_int4((int)c, (int)std::min<size_t>(tc, off[i + 1] - c), i, 0));
-  LBG_BCU(cudaMemcpy(b->d_row_tiles, rtiles.data(), rtiles.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  LBG_BCU(cudaMemcpyAsync(b->d_row_tiles, rtiles.data(), rtiles.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                          b->stream));
   b->n_row_tiles = (int)rtiles.size();
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pp->device);
@@ -740,6 +783,11 @@ int lbg_batch_round(lbg_batch* b, const uint8_t* domain, size_t domain_len, cons
   }
   uint64_t per_round = 11 + 2 * pp->limbs + 3 +
                        (pp->params.opening == LBG_OPENING_BIT_DROPPED ? pp->limbs + 1 + b->count : 0);
+  if (!b->sw_h.empty()) {
+    uint32_t lmax = 0;
+    for (const SwInst& h : b->sw_h) lmax = std::max(lmax, h.l);
+    per_round += 7 + 2 * (uint64_t)lmax;
+  }
   if (b->graphs) {
     if (!b->g_round) {
       cudaGraph_t g = nullptr;
@@ -788,6 +836,94 @@ int lbg_batch_round(lbg_batch* b, const uint8_t* domain, size_t domain_len, cons
       std::memcpy(out->p1 + o, p1.data() + (size_t)i * 32 * 3, b->col_log[i] * 24);
       o += 3 * b->col_log[i];
     }
+  }
+  return LBG_OK;
+}
+
+int lbg_batch_set_switch(lbg_batch* b, const uint8_t* flags, const uint64_t* r_hi, const uint64_t* claims) {
+  if (!b) return fail(LBG_ERR_INVALID, "null batch");
+  if (b->count == 0) return fail(LBG_ERR_INVALID, "no instances assigned");
+  const lbg_pp* pp = b->pp;
+  LBG_BCU(cudaSetDevice(pp->device));
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  b->sw_flag.clear();
+  b->sw_h.clear();
+  b->plan_ok = false;
+  if (b->g_round) {
+    cudaGraphExecDestroy(b->g_round);
+    b->g_round = nullptr;
+  }
+  if (!flags) return LBG_OK;
+  uint32_t row_log = pp->params.witness_log_len - pp->params.column_log_len;
+  std::vector<int> list;
+  size_t scratch = 0, rwords = 0;
+  for (int i = 0; i < b->count; i++) {
+    if (!flags[i]) continue;
+    uint32_t l = row_log + b->col_log[i];
+    if (l > 32) return fail(LBG_ERR_PARAMS, "instance " + std::to_string(i) + ": a switch over more than 2^32 words");
+    list.push_back(i);
+    scratch += sw_scratch_bytes(l);
+    rwords += 2 * (size_t)l;
+  }
+  if (list.empty()) return LBG_OK;
+  if (!r_hi) return fail(LBG_ERR_INVALID, "switch instances need their r_hi");
+  size_t n = list.size();
+  LBG_BCU(grow((void**)&b->d_sw_inst, &b->sw_inst_cap, n * sizeof(SwInst)));
+  LBG_BCU(grow((void**)&b->d_sw_small, &b->sw_small_cap, n * sizeof(SwSmall)));
+  LBG_BCU(grow((void**)&b->d_sw_scratch, &b->sw_scratch_cap, scratch));
+  LBG_BCU(grow((void**)&b->d_sw_r, &b->sw_r_cap, rwords * 8));
+  LBG_BCU(cudaMemcpyAsync(b->d_sw_r, r_hi, rwords * 8, cudaMemcpyHostToDevice, b->stream));
+  LBG_BCU(cudaMemsetAsync(b->d_sw_small, 0, n * sizeof(SwSmall), b->stream));
+  if (claims)
+    LBG_BCU(cudaMemcpy2DAsync(&b->d_sw_small[0].claim[0], sizeof(SwSmall), claims, 16, 16, n, cudaMemcpyHostToDevice,
+                              b->stream));
+  std::vector<SwInst> hs(n);
+  size_t roff = 0, soff = 0;
+  for (size_t k = 0; k < n; k++) {
+    int i = list[k];
+    SwInst& h = hs[k];
+    std::memset(&h, 0, sizeof(h));
+    h.l = row_log + b->col_log[i];
+    h.w = b->d_w + b->col_off[i] * b->wdim * 3;
+    h.r_hi = b->d_sw_r + roff;
+    h.s = b->d_sw_small + k;
+    h.st = b->d_states + i;
+    h.counter0 = 0;  // the instance's transcript derives nothing before the switch
+    h.p0 = b->d_p0 + 3 * (size_t)row_log * i;
+    h.p1 = b->d_p1 + 3 * 32 * (size_t)i;
+    h.row_log = row_log;
+    h.col_log = b->col_log[i];
+    h.claim_given = claims ? 1 : 0;
+    sw_layout(h, b->d_sw_scratch + soff);
+    roff += 2 * (size_t)h.l;
+    soff += sw_scratch_bytes(h.l);
+  }
+  LBG_BCU(cudaMemcpyAsync(b->d_sw_inst, hs.data(), n * sizeof(SwInst), cudaMemcpyHostToDevice, b->stream));
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  b->sw_flag.assign(flags, flags + b->count);
+  b->sw_h = hs;
+  return LBG_OK;
+}
+
+int lbg_batch_switch_outputs(const lbg_batch* b, uint64_t* partials, uint64_t* rounds, uint64_t* opened,
+                             uint64_t* claims) {
+  if (!b) return fail(LBG_ERR_INVALID, "null batch");
+  size_t n = b->sw_h.size();
+  if (n == 0) return LBG_OK;
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  LBG_BCU(cudaStreamSynchronize(b->stream));
+  std::vector<SwSmall> hs(n);
+  LBG_BCU(cudaMemcpy(hs.data(), b->d_sw_small, n * sizeof(SwSmall), cudaMemcpyDeviceToHost));
+  size_t ro = 0;
+  for (size_t k = 0; k < n; k++) {
+    const SwSmall& o = hs[k];
+    if (o.status != 1) return fail(LBG_ERR_INVALID, "no switch has run since the statements were set");
+    uint32_t l = b->sw_h[k].l;
+    if (partials) std::memcpy(partials + 256 * k, o.v, 128 * 16);
+    if (rounds) std::memcpy(rounds + ro, o.rounds, (size_t)l * 48);
+    if (opened) std::memcpy(opened + 3 * k, o.opened, 24);
+    if (claims) std::memcpy(claims + 2 * k, o.claim, 16);
+    ro += 6 * (size_t)l;
   }
   return LBG_OK;
 }

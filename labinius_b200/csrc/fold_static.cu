@@ -25,6 +25,7 @@
 #include "launch.h"
 #include "prime_structs.h"
 #include "ring_tables.h"
+#include "upload.h"
 
 using namespace lbg;
 
@@ -91,7 +92,7 @@ int setup(int dev, int pi, uint32_t q, DeviceState** out) {
     const PrimeTables& T = prime_tables(q);
     static DevPrime staging;  // host copy, filled under the lock
     fill_tables(T, &staging);
-    cudaError_t e = cudaMemcpy(S.tables + pi, &staging, sizeof(DevPrime), cudaMemcpyHostToDevice);
+    cudaError_t e = upload_sync(S.tables + pi, &staging, sizeof(DevPrime));
     if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("table upload: ") + cudaGetErrorString(e));
     HotPrime h;
     std::memcpy(h.tw, T.tw, sizeof(h.tw));

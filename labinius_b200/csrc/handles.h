@@ -39,7 +39,11 @@ struct lbg_pp {
   lbg_challenge_d* d_ch = nullptr;
   uint32_t* d_chat = nullptr;  // [cols][162]
   int16_t* d_fc = nullptr;     // [4][limbs][162]
+  uint8_t* d_sw = nullptr;     // the switch prover's workspace (lbg_switch_prove), allocated on first use
 };
+
+// Frees the switch prover's workspace of pp (switch.cu).
+void lbg_switch_release(lbg_pp* pp);
 
 struct lbg_witness {
   std::atomic<int> refs{1};

@@ -1229,7 +1229,9 @@ __global__ void k_lift_b128(const uint64_t* __restrict__ b, size_t n, uint64_t* 
 static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
 cudaError_t upload_hot(int pi, const HotPrime& h) {
-  return cudaMemcpyToSymbol(c_hot, &h, sizeof(HotPrime), sizeof(HotPrime) * pi, cudaMemcpyHostToDevice);
+  cudaError_t e = cudaMemcpyToSymbol(c_hot, &h, sizeof(HotPrime), sizeof(HotPrime) * pi, cudaMemcpyHostToDevice);
+  // landed before any stream's kernels read it (the copy runs on the legacy default stream)
+  return e == cudaSuccess ? cudaStreamSynchronize(cudaStreamLegacy) : e;
 }
 
 cudaError_t launch_key_expand(const uint64_t* jumps, uint64_t state0, uint32_t q, int nb, int16_t* A,

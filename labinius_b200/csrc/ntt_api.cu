@@ -11,6 +11,7 @@
 #include "launch.h"
 #include "prime_structs.h"
 #include "ring_tables.h"
+#include "upload.h"
 
 using namespace lbg;
 
@@ -38,7 +39,7 @@ int run(uint32_t q, bool inverse, const uint16_t* in, uint16_t* out, size_t coun
     if (!g_tables[dev][pi]) {
       Ntt648Tables* p = nullptr;
       if (cudaMalloc((void**)&p, sizeof(Ntt648Tables)) != cudaSuccess ||
-          cudaMemcpy(p, host, sizeof(Ntt648Tables), cudaMemcpyHostToDevice) != cudaSuccess) {
+          upload_sync(p, host, sizeof(Ntt648Tables)) != cudaSuccess) {
         cudaGetLastError();
         cudaFree(p);
         return fail(LBG_ERR_CUDA, "transform tables");

@@ -1,18 +1,22 @@
 // The cross-field switch prover on the device (crates/pcs/src/switch.rs:133-168,
 // crates/pcs/src/fields/crossfield.rs, crates/pcs/src/fields/sumcheck.rs).
 //
-// A B128 trace committed as Witness::lifted carries a claim in B128; the switch turns it into the
-// F162 claim the commitment opens at the point its sumcheck ends on. The prover's work is three
-// passes over the trace and a sumcheck of l rounds:
+// A B128 trace of 2^l words, committed as Witness::lifted, carries a claim in B128 at r_hi; the
+// switch turns it into the F162 claim the commitment opens, at the point its sumcheck ends on.
+// The prover's work is three passes over the trace and a sumcheck of l rounds:
 //  * eq_hi = the expansion of r_hi (one B128 product per entry, from two half-size tables);
 //  * the 128 partial evaluations v[k] = sum_j bit_k(trace_j) eq_hi[j];
-//  * a_j = psi(eq_hi[j]) = sum_k bit_k(eq_hi[j]) batch[k] (byte tables of the batch in shared
-//    memory), p_j = the trace word as an F162;
-//  * each round sends (sum a0 p0, sum (a0 + a1)(p0 + p1)) over the index pairs (j, j + half),
-//    then folds both tables with the round's challenge r: x0 + r (x0 + x1). The fold of round k
-//    and the message of round k + 1 are one kernel; products by r go through 4-bit tables of
-//    r x^i in shared memory.
-// The transcript stays on the host (the prover's lbg_transcript): one short exchange per round.
+//  * a_j = psi(eq_hi[j]) = sum_k bit_k(eq_hi[j]) batch[k] (nibble tables of the batch in shared
+//    memory; psi is linear, so a_j + a_j' = psi(eq_j + eq_j')), p_j = the trace word as an F162;
+//  * round k sends (sum a0 p0, sum (a0 + a1)(p0 + p1)) over the index pairs (j, j + half) and
+//    folds both tables with its challenge r: x0 + r (x0 + x1). The fold of round k and the
+//    message of round k + 1 are one kernel; products by r go through 4-bit tables of (t x^4i) r
+//    in shared memory; round 0's tables are never stored (a and p are read through eq and the
+//    trace), so the folded tables take n/2 entries.
+// The transcript runs on the device too: each instance's hasher state absorbs the statement,
+// the partials and every message, and the batch and round challenges are derived from it (one
+// thread per instance), so a whole switch is one pass on a stream with no host round trip. The
+// single-instance entry point moves the caller's transcript to the device and back.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,60 +25,132 @@
 #include <vector>
 
 #include "../../include/labinius_gpu.h"
+#include "blake3_dev.cuh"
 #include "error.h"
 #include "gf2_dev.cuh"
 #include "handles.h"
+#include "switch.h"
 #include "transcript.h"
 
-using namespace lbg;
-
+namespace lbg {
 namespace {
 
-int fail(int code, const std::string& m) {
-  set_last_error(m);
-  return code;
+constexpr int SW_THREADS = 256;
+constexpr uint32_t SW_CAP = 148 * 8;  // blocks per instance and launch, at most
+
+__constant__ char c_sw_label[16] = "labinius/switch";
+__constant__ char c_sw_batch[22] = "labinius/switch-batch";
+__constant__ char c_sw_round[22] = "labinius/switch-round";
+
+// Work units of an instance with l variables in a launch: stage 0 counts elements, stage 1 the
+// pairs of round 0's message, stage 2 the work of round k's fold (the pairs of round k + 1's
+// message, or the one pair of the last fold; none once the instance's rounds are done).
+__host__ __device__ inline uint64_t sw_units(uint32_t l, int stage, int k) {
+  uint64_t n = 1ull << l;
+  if (stage == 0) return n;
+  if (stage == 1) return n / 2;
+  if ((uint32_t)k >= l) return 0;
+  if ((uint32_t)k + 1 == l) return 1;
+  return n >> (k + 2);
+}
+__host__ __device__ inline uint32_t sw_blocks(uint64_t units, int per_block) {
+  uint64_t b = (units + per_block - 1) / per_block;
+  return (uint32_t)(b < SW_CAP ? b : SW_CAP);
+}
+
+// Blocks are dealt to the instances in order, each getting sw_blocks(its units); this block's
+// instance (or -1), its rank among the instance's blocks and their number.
+__device__ __forceinline__ int sw_find(const SwInst* __restrict__ I, int count, int stage, int k, int per_block,
+                                       uint32_t& local, uint32_t& nblk) {
+  uint32_t b = blockIdx.x;
+  for (int i = 0; i < count; i++) {
+    uint32_t nb = sw_blocks(sw_units(I[i].l, stage, k), per_block);
+    if (b < nb) {
+      local = b;
+      nblk = nb;
+      return i;
+    }
+    b -= nb;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ B128d ld_b(const uint64_t* p, size_t j) {
+  ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p + 2 * j);
+  return B128d{v.x, v.y};
+}
+__device__ __forceinline__ void st_b(uint64_t* p, size_t j, B128d x) {
+  *reinterpret_cast<ulonglong2*>(p + 2 * j) = make_ulonglong2(x.lo, x.hi);
+}
+__device__ __forceinline__ F162d ld_f(const uint64_t* p, size_t j) {
+  return F162d{{p[3 * j], p[3 * j + 1], p[3 * j + 2]}};
+}
+__device__ __forceinline__ void st_f(uint64_t* p, size_t j, F162d x) {
+  p[3 * j] = x.w[0];
+  p[3 * j + 1] = x.w[1];
+  p[3 * j + 2] = x.w[2];
+}
+// trace word j as an F162 (the low 128 bits of the lifted element)
+__device__ __forceinline__ F162d ld_word(const uint64_t* __restrict__ w, size_t j) {
+  return F162d{{__ldg(w + 3 * j), __ldg(w + 3 * j + 1), 0}};
 }
 
 // Entry idx of the expansion of r[0..m): the product over rounds of r_round or 1 + r_round, by
 // bit m-1-round of idx (crates/pcs/src/fields/crossfield.rs:78-98: the last coordinate is bit 0).
-__global__ void k_sw_eq_tables(const B128d* __restrict__ r, int lh, int ll, B128d* __restrict__ e_hi,
-                               B128d* __restrict__ e_lo) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  int nh = 1 << lh, nl = 1 << ll;
+// Block (0, i) also clears instance i's partial and message accumulators and its status.
+__global__ void k_sw_tables(const SwInst* __restrict__ I) {
+  const SwInst& s = I[blockIdx.y];
+  if (blockIdx.x == 0) {
+    uint64_t* v = &s.s->v[0][0];
+    for (int t = threadIdx.x; t < 256; t += blockDim.x) v[t] = 0;
+    if (threadIdx.x < 8) s.s->msg[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s.s->status = 0;
+  }
+  uint32_t nh = 1u << s.lh, nl = 1u << s.ll;
+  uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= nh + nl) return;
   bool high = g < nh;
-  int idx = high ? g : g - nh;
-  int m = high ? lh : ll;
-  const B128d* rr = high ? r : r + lh;
+  uint32_t idx = high ? g : g - nh;
+  uint32_t m = high ? s.lh : s.ll;
+  const uint64_t* rr = s.r_hi + 2 * (high ? 0 : s.lh);
   B128d acc{1, 0};
-  for (int round = 0; round < m; round++) {
-    B128d f = rr[round];
+  for (uint32_t round = 0; round < m; round++) {
+    B128d f = ld_b(rr, round);
     if (!((idx >> (m - 1 - round)) & 1)) f.lo ^= 1;
     acc = b_mul(acc, f);
   }
-  (high ? e_hi : e_lo)[idx] = acc;
+  st_b(high ? s.e_hi : s.e_lo, idx, acc);
 }
 
-__global__ void k_sw_eq(const B128d* __restrict__ e_hi, const B128d* __restrict__ e_lo, int ll, size_t n,
-                        B128d* __restrict__ eq) {
-  size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  eq[j] = b_mul(e_hi[j >> ll], e_lo[j & ((1ull << ll) - 1)]);
+__global__ void __launch_bounds__(SW_THREADS) k_sw_eq(const SwInst* __restrict__ I, int count) {
+  uint32_t local, nblk;
+  int i = sw_find(I, count, 0, 0, SW_THREADS, local, nblk);
+  if (i < 0) return;
+  const SwInst& s = I[i];
+  size_t n = 1ull << s.l;
+  uint64_t lm = (1ull << s.ll) - 1;
+  for (size_t j = (size_t)local * SW_THREADS + threadIdx.x; j < n; j += (size_t)nblk * SW_THREADS)
+    st_b(s.eq, j, b_mul(ld_b(s.e_hi, j >> s.ll), ld_b(s.e_lo, j & lm)));
 }
 
-// v[k] = sum_j bit_k(trace_j) eq[j]: thread (sub, m) of a CTA adds, for its rows j, eq[j] into
+// v[k] = sum_j bit_k(trace_j) eq[j]: thread (sub, m) of a block adds, for its rows j, eq[j] into
 // the 8 partial sums of bits 8m .. 8m+7; the 16 row groups are then XOR-reduced and added to v.
-__global__ void __launch_bounds__(256) k_sw_partials(const uint64_t* __restrict__ W, const B128d* __restrict__ eq,
-                                                     size_t n, unsigned long long* __restrict__ v) {
+constexpr int SW_PARTIAL_ROWS = 128;  // rows per block before the cap
+__global__ void __launch_bounds__(SW_THREADS) k_sw_partials(const SwInst* __restrict__ I, int count) {
   __shared__ uint64_t red[16][128][2];
+  uint32_t local, nblk;
+  int i = sw_find(I, count, 0, 0, SW_PARTIAL_ROWS, local, nblk);
+  if (i < 0) return;
+  const SwInst& s = I[i];
+  size_t n = 1ull << s.l;
   const int sub = threadIdx.x >> 4, m = threadIdx.x & 15;
   uint64_t S[8][2];
 #pragma unroll
   for (int r = 0; r < 8; r++) S[r][0] = S[r][1] = 0;
-  for (size_t j = (size_t)blockIdx.x * 16 + sub; j < n; j += (size_t)gridDim.x * 16) {
-    uint64_t word = __ldg(W + 3 * j + (m >> 3));
+  for (size_t j = (size_t)local * 16 + sub; j < n; j += (size_t)nblk * 16) {
+    uint64_t word = __ldg(s.w + 3 * j + (m >> 3));
     uint32_t byte = (uint32_t)(word >> (8 * (m & 7))) & 0xFF;
-    B128d e = eq[j];
+    B128d e = ld_b(s.eq, j);
 #pragma unroll
     for (int r = 0; r < 8; r++) {
       uint64_t msk = 0 - (uint64_t)((byte >> r) & 1);
@@ -90,18 +166,69 @@ __global__ void __launch_bounds__(256) k_sw_partials(const uint64_t* __restrict_
   __syncthreads();
   if (threadIdx.x < 128) {
     uint64_t a = 0, b = 0;
-    for (int s = 0; s < 16; s++) {
-      a ^= red[s][threadIdx.x][0];
-      b ^= red[s][threadIdx.x][1];
+    for (int q = 0; q < 16; q++) {
+      a ^= red[q][threadIdx.x][0];
+      b ^= red[q][threadIdx.x][1];
     }
+    unsigned long long* v = reinterpret_cast<unsigned long long*>(&s.s->v[0][0]);
     atomicXor(v + 2 * threadIdx.x, (unsigned long long)a);
     atomicXor(v + 2 * threadIdx.x + 1, (unsigned long long)b);
   }
 }
 
-// batch = the expansion of the 7 sampled F162 (crossfield.rs:65-76); psi[c][t] = the XOR of
-// batch[8c + b] over the set bits b of t (crossfield.rs:112-130). One CTA of 256 threads.
-__global__ void k_sw_batch(const F162d* __restrict__ rp, F162d* __restrict__ batch, F162d* __restrict__ psi) {
+__device__ __forceinline__ uint64_t read_u64(dev::Reader& rd) {
+  uint64_t x = 0;
+  for (int b = 0; b < 8; b++) x |= (uint64_t)rd.byte() << (8 * b);
+  return x;
+}
+
+// One thread per instance: the claim (if the statement leaves it to the prover: the trace's value
+// at r_hi, sum_k v[k] x^k, crates/pcs/src/switch.rs:116-122), absorb_statement and the partials
+// (crates/pcs/src/switch.rs:124-129, 147-148), then the batch coordinates,
+// sample_f162("labinius/switch-batch", 7) (crates/pcs/src/switch.rs:149,
+// crates/pcs/src/challenge.rs:129-140).
+__global__ void k_sw_statement(const SwInst* __restrict__ I, int count) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const SwInst& s = I[i];
+  SwSmall* sm = s.s;
+  if (!s.claim_given) {
+    B128d acc{0, 0};
+    for (int k = 127; k >= 0; k--) acc = b_add(b_times_x(acc), B128d{sm->v[k][0], sm->v[k][1]});
+    sm->claim[0] = acc.lo;
+    sm->claim[1] = acc.hi;
+  }
+  dev::Absorber h;
+  h.load(s.st);
+  h.update_u64(15);
+  h.update((const uint8_t*)c_sw_label, 15);
+  h.update_u64(s.nlo);
+  for (uint32_t k = 0; k < 2 * s.nlo; k++) h.update_u64(s.r_lo[k]);
+  h.update_u64(s.l);
+  for (uint32_t k = 0; k < 2 * s.l; k++) h.update_u64(s.r_hi[k]);
+  h.update_u64(1);
+  h.update_u64(sm->claim[0]);
+  h.update_u64(sm->claim[1]);
+  h.update_u64(128);
+  for (int k = 0; k < 128; k++) {
+    h.update_u64(sm->v[k][0]);
+    h.update_u64(sm->v[k][1]);
+  }
+  h.store();
+  XofRoot root;
+  dev::derive_root(s.st, s.counter0, c_sw_batch, 21, root);
+  dev::Reader rd;
+  rd.init(root);
+  for (int c = 0; c < 7; c++) {
+    for (int w = 0; w < 3; w++) sm->rp[c][w] = read_u64(rd);
+    sm->rp[c][2] &= (1ull << 34) - 1;
+  }
+}
+
+// batch = the expansion of the 7 sampled F162 (crossfield.rs:65-76); psi[16 c + t] = the XOR of
+// batch[4c + b] over the set bits b of t (crossfield.rs:112-130). One block per instance.
+__global__ void k_sw_batch(const SwInst* __restrict__ I) {
+  const SwInst& s = I[blockIdx.x];
   __shared__ F162d t[2][128];
   if (threadIdx.x == 0) t[0][0] = F162d{{1, 0, 0}};
   __syncthreads();
@@ -110,73 +237,37 @@ __global__ void k_sw_batch(const F162d* __restrict__ rp, F162d* __restrict__ bat
     int size = 1 << round;
     if ((int)threadIdx.x < size) {
       F162d x = t[cur][threadIdx.x];
-      F162d h = f_mul(x, rp[round]);
+      F162d h = f_mul(x, ld_f(&s.s->rp[0][0], round));
       t[cur ^ 1][2 * threadIdx.x] = f_add(x, h);
       t[cur ^ 1][2 * threadIdx.x + 1] = h;
     }
     __syncthreads();
     cur ^= 1;
   }
-  if (threadIdx.x < 128) batch[threadIdx.x] = t[cur][threadIdx.x];
-  for (int e = threadIdx.x; e < 16 * 256; e += blockDim.x) {
-    int c = e >> 8, v = e & 255;
+  for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) {
+    int c = e >> 4, v = e & 15;
     F162d acc{{0, 0, 0}};
-    for (int b = 0; b < 8; b++)
-      if ((v >> b) & 1) acc = f_add(acc, t[cur][8 * c + b]);
-    psi[e] = acc;
+    for (int b = 0; b < 4; b++)
+      if ((v >> b) & 1) acc = f_add(acc, t[cur][4 * c + b]);
+    st_f(&s.s->psi[0][0], e, acc);
   }
 }
 
-__device__ __forceinline__ void xor_reduce_store(F162d e0, F162d ei, unsigned long long* msg) {
-  for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      e0.w[k] ^= __shfl_xor_sync(0xffffffffu, e0.w[k], o);
-      ei.w[k] ^= __shfl_xor_sync(0xffffffffu, ei.w[k], o);
-    }
-  }
-  if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      atomicXor(msg + k, (unsigned long long)e0.w[k]);
-      atomicXor(msg + 3 + k, (unsigned long long)ei.w[k]);
-    }
-  }
+__device__ __forceinline__ void load_table(F162d* dst, const uint64_t* src, int entries) {
+  for (int e = threadIdx.x; e < entries; e += blockDim.x) dst[e] = ld_f(src, e);
 }
 
 __device__ __forceinline__ F162d psi_of(const F162d* __restrict__ tab, B128d e) {
   F162d acc{{0, 0, 0}};
 #pragma unroll
-  for (int c = 0; c < 16; c++) {
-    uint32_t byte = (uint32_t)((c < 8 ? e.lo >> (8 * c) : e.hi >> (8 * (c - 8))) & 0xFF);
-    acc = f_add(acc, tab[c * 256 + byte]);
+  for (int c = 0; c < 32; c++) {
+    uint32_t nib = (uint32_t)((c < 16 ? e.lo >> (4 * c) : e.hi >> (4 * (c - 16))) & 15);
+    acc = f_add(acc, tab[16 * c + nib]);
   }
   return acc;
 }
 
-// a and p of every index, and round 0's message over the pairs (j, j + n/2).
-__global__ void __launch_bounds__(256) k_sw_init(const uint64_t* __restrict__ W, const B128d* __restrict__ eq,
-                                                 const F162d* __restrict__ psi_g, size_t n, F162d* __restrict__ a,
-                                                 F162d* __restrict__ p, unsigned long long* __restrict__ msg) {
-  extern __shared__ F162d psi[];  // [16][256]
-  for (int e = threadIdx.x; e < 16 * 256; e += blockDim.x) psi[e] = psi_g[e];
-  __syncthreads();
-  const size_t h = n / 2;
-  F162d e0{{0, 0, 0}}, ei{{0, 0, 0}};
-  for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < h; j += (size_t)gridDim.x * blockDim.x) {
-    F162d a0 = psi_of(psi, eq[j]), a1 = psi_of(psi, eq[j + h]);
-    F162d p0{{W[3 * j], W[3 * j + 1], 0}}, p1{{W[3 * (j + h)], W[3 * (j + h) + 1], 0}};
-    a[j] = a0;
-    a[j + h] = a1;
-    p[j] = p0;
-    p[j + h] = p1;
-    e0 = f_add(e0, f_mul(a0, p0));
-    ei = f_add(ei, f_mul(f_add(a0, a1), f_add(p0, p1)));
-  }
-  xor_reduce_store(e0, ei, msg);
-}
-
-// x r through 4-bit tables: T[i][t] = (t x^{4i}) r, 41 nibble positions.
+// x r through the round's tables: T[16 i + t] = (t x^{4i}) r, 41 nibble positions.
 __device__ __forceinline__ F162d cmul(const F162d* __restrict__ T, F162d x) {
   F162d acc{{0, 0, 0}};
 #pragma unroll
@@ -187,58 +278,244 @@ __device__ __forceinline__ F162d cmul(const F162d* __restrict__ T, F162d x) {
   return acc;
 }
 
-// Fold both tables with r (x0 + r (x0 + x1) over the pairs (j, j + half)); when half >= 2, also
-// the next round's message over the pairs (j, j + half/2) of the folded tables.
-__global__ void __launch_bounds__(256) k_sw_round(F162d* __restrict__ a, F162d* __restrict__ p, size_t half,
-                                                  const F162d* __restrict__ rr, unsigned long long* __restrict__ msg) {
-  __shared__ F162d R[164];
-  __shared__ F162d T[41 * 16];
+__device__ __forceinline__ void xor_reduce_store(F162d e0, F162d ei, uint64_t* msg) {
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      e0.w[k] ^= __shfl_xor_sync(0xffffffffu, e0.w[k], o);
+      ei.w[k] ^= __shfl_xor_sync(0xffffffffu, ei.w[k], o);
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    unsigned long long* m = reinterpret_cast<unsigned long long*>(msg);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      atomicXor(m + k, (unsigned long long)e0.w[k]);
+      atomicXor(m + 3 + k, (unsigned long long)ei.w[k]);
+    }
+  }
+}
+
+// Round 0's message over the pairs (j, j + n/2): a0 = psi(eq_j), a0 + a1 = psi(eq_j + eq_j+n/2).
+__global__ void __launch_bounds__(SW_THREADS) k_sw_init(const SwInst* __restrict__ I, int count) {
+  __shared__ F162d psi[512];
+  uint32_t local, nblk;
+  int i = sw_find(I, count, 1, 0, SW_THREADS, local, nblk);
+  if (i < 0) return;
+  const SwInst& s = I[i];
+  load_table(psi, &s.s->psi[0][0], 512);
+  __syncthreads();
+  const size_t h = (1ull << s.l) / 2;
+  F162d e0{{0, 0, 0}}, ei{{0, 0, 0}};
+  for (size_t j = (size_t)local * SW_THREADS + threadIdx.x; j < h; j += (size_t)nblk * SW_THREADS) {
+    B128d q0 = ld_b(s.eq, j), q1 = ld_b(s.eq, j + h);
+    F162d a0 = psi_of(psi, q0), ad = psi_of(psi, b_add(q0, q1));
+    F162d p0 = ld_word(s.w, j), p1 = ld_word(s.w, j + h);
+    e0 = f_add(e0, f_mul(a0, p0));
+    ei = f_add(ei, f_mul(ad, f_add(p0, p1)));
+  }
+  xor_reduce_store(e0, ei, &s.s->msg[0]);
+}
+
+// One block per instance whose round k is due: the round's message into the transcript,
+// sample_f162("labinius/switch-round", 1) (crates/pcs/src/switch.rs:152-159), the message
+// accumulators cleared, and the tables of (t x^{4i}) r for the fold.
+__global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
+  const SwInst& s = I[blockIdx.x];
+  if ((uint32_t)k >= s.l) return;
+  SwSmall* sm = s.s;
+  __shared__ F162d R4[41];
   if (threadIdx.x == 0) {
-    F162d x = *rr;
-    for (int k = 0; k < 164; k++) {
-      R[k] = x;
-      x = f_times_x(x);
+    uint64_t msg[6];
+    for (int q = 0; q < 6; q++) {
+      msg[q] = sm->msg[q];
+      sm->rounds[k][q] = msg[q];
+      sm->msg[q] = 0;
+    }
+    dev::Absorber h;
+    h.load(s.st);
+    h.update_u64(2);
+    for (int q = 0; q < 6; q++) h.update_u64(msg[q]);
+    h.store();
+    XofRoot root;
+    dev::derive_root(s.st, s.counter0 + 1 + (uint64_t)k, c_sw_round, 21, root);
+    dev::Reader rd;
+    rd.init(root);
+    F162d r;
+    for (int w = 0; w < 3; w++) r.w[w] = read_u64(rd);
+    r.w[2] &= (1ull << 34) - 1;
+    st_f(&sm->rr[0][0], k, r);
+    for (int q = 0; q < 41; q++) {
+      R4[q] = r;
+      r = f_times_x4(r);
     }
   }
   __syncthreads();
   for (int e = threadIdx.x; e < 41 * 16; e += blockDim.x) {
-    int i = e >> 4, t = e & 15;
-    F162d acc{{0, 0, 0}};
-    for (int b = 0; b < 4; b++)
-      if ((t >> b) & 1) acc = f_add(acc, R[4 * i + b]);
-    T[e] = acc;
+    int q = e >> 4, t = e & 15;
+    F162d x = R4[q], acc{{0, 0, 0}};
+    for (int b = 0; b < 4; b++) {
+      if ((t >> b) & 1) acc = f_add(acc, x);
+      x = f_times_x(x);
+    }
+    st_f(&sm->rtab[0][0], e, acc);
   }
+}
+
+// Round k's fold with its challenge (x0 + r (x0 + x1) over the pairs (j, j + half) of tables of
+// 2 half entries) and, when half >= 2, round k + 1's message over the pairs (j, j + half/2) of
+// the folded tables. FIRST (k = 0) reads the tables through eq and the trace and writes the
+// folded ones; later rounds fold in place.
+template <bool FIRST>
+__global__ void __launch_bounds__(SW_THREADS) k_sw_fold(const SwInst* __restrict__ I, int count, int k) {
+  __shared__ F162d T[41 * 16];
+  __shared__ F162d psi[FIRST ? 512 : 1];
+  uint32_t local, nblk;
+  int i = sw_find(I, count, 2, k, SW_THREADS, local, nblk);
+  if (i < 0) return;
+  const SwInst& s = I[i];
+  load_table(T, &s.s->rtab[0][0], 41 * 16);
+  if (FIRST) load_table(psi, &s.s->psi[0][0], 512);
   __syncthreads();
+  const size_t half = (1ull << s.l) >> (k + 1);
+  // the folded entry x (x < half) of both tables
+  auto fold_at = [&](size_t x, F162d& na, F162d& np) {
+    if (FIRST) {
+      B128d q0 = ld_b(s.eq, x), q1 = ld_b(s.eq, x + half);
+      F162d a0 = psi_of(psi, q0);
+      na = f_add(a0, cmul(T, psi_of(psi, b_add(q0, q1))));
+      F162d p0 = ld_word(s.w, x), p1 = ld_word(s.w, x + half);
+      np = f_add(p0, cmul(T, f_add(p0, p1)));
+    } else {
+      F162d a0 = ld_f(s.a, x), a1 = ld_f(s.a, x + half);
+      na = f_add(a0, cmul(T, f_add(a0, a1)));
+      F162d p0 = ld_f(s.p, x), p1 = ld_f(s.p, x + half);
+      np = f_add(p0, cmul(T, f_add(p0, p1)));
+    }
+  };
   if (half < 2) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      a[0] = f_add(a[0], cmul(T, f_add(a[0], a[1])));
-      p[0] = f_add(p[0], cmul(T, f_add(p[0], p[1])));
+    if (local == 0 && threadIdx.x == 0) {
+      F162d na, np;
+      fold_at(0, na, np);
+      st_f(s.a, 0, na);
+      st_f(s.p, 0, np);
     }
     return;
   }
   const size_t h2 = half / 2;
   F162d e0{{0, 0, 0}}, ei{{0, 0, 0}};
-  for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < h2; j += (size_t)gridDim.x * blockDim.x) {
-    F162d x0 = a[j], x1 = a[j + half], y0 = a[j + h2], y1 = a[j + h2 + half];
-    F162d na = f_add(x0, cmul(T, f_add(x0, x1))), nb = f_add(y0, cmul(T, f_add(y0, y1)));
-    F162d u0 = p[j], u1 = p[j + half], v0 = p[j + h2], v1 = p[j + h2 + half];
-    F162d pa = f_add(u0, cmul(T, f_add(u0, u1))), pb = f_add(v0, cmul(T, f_add(v0, v1)));
-    a[j] = na;
-    a[j + h2] = nb;
-    p[j] = pa;
-    p[j + h2] = pb;
+  for (size_t j = (size_t)local * SW_THREADS + threadIdx.x; j < h2; j += (size_t)nblk * SW_THREADS) {
+    F162d na, pa, nb, pb;
+    fold_at(j, na, pa);
+    fold_at(j + h2, nb, pb);
+    st_f(s.a, j, na);
+    st_f(s.a, j + h2, nb);
+    st_f(s.p, j, pa);
+    st_f(s.p, j + h2, pb);
     e0 = f_add(e0, f_mul(na, pa));
     ei = f_add(ei, f_mul(f_add(na, nb), f_add(pa, pb)));
   }
-  xor_reduce_store(e0, ei, msg);
+  xor_reduce_store(e0, ei, &s.s->msg[0]);
 }
 
-unsigned grid_for(size_t threads, int block) {
-  size_t g = (threads + block - 1) / block;
-  return (unsigned)std::max<size_t>(1, std::min<size_t>(g, 148 * 16));
+// One thread per instance: the opened value p[0] and the evaluation point, msb_first
+// (crates/pcs/src/scheme/commitment.rs:163-174): p0[i] = r_(l-1-i), p1[i] = r_(col_log-1-i).
+__global__ void k_sw_finish(const SwInst* __restrict__ I, int count) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const SwInst& s = I[i];
+  SwSmall* sm = s.s;
+  for (int w = 0; w < 3; w++) sm->opened[w] = s.p[w];
+  if (s.p0)
+    for (uint32_t q = 0; q < s.row_log; q++)
+      for (int w = 0; w < 3; w++) s.p0[3 * q + w] = sm->rr[s.l - 1 - q][w];
+  if (s.p1)
+    for (uint32_t q = 0; q < s.col_log; q++)
+      for (int w = 0; w < 3; w++) s.p1[3 * q + w] = sm->rr[s.col_log - 1 - q][w];
+  sm->status = 1;
 }
+
+size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
 }  // namespace
+
+size_t sw_scratch_bytes(uint32_t l) {
+  uint32_t lh = l / 2, ll = l - lh;
+  size_t n = (size_t)1 << l, half = std::max<size_t>(n / 2, 1);
+  return align256((size_t)16 << lh) + align256((size_t)16 << ll) + align256(16 * n) + 2 * align256(24 * half);
+}
+
+void sw_layout(SwInst& I, uint8_t* base) {
+  I.lh = I.l / 2;
+  I.ll = I.l - I.lh;
+  size_t n = (size_t)1 << I.l, half = std::max<size_t>(n / 2, 1);
+  I.e_hi = (uint64_t*)base;
+  base += align256((size_t)16 << I.lh);
+  I.e_lo = (uint64_t*)base;
+  base += align256((size_t)16 << I.ll);
+  I.eq = (uint64_t*)base;
+  base += align256(16 * n);
+  I.a = (uint64_t*)base;
+  base += align256(24 * half);
+  I.p = (uint64_t*)base;
+}
+
+cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStream_t st, uint64_t* launches) {
+  if (count <= 0) return cudaSuccess;
+  uint32_t lmax = 0, tabmax = 0;
+  for (int i = 0; i < count; i++) {
+    lmax = std::max(lmax, h[i].l);
+    tabmax = std::max(tabmax, (1u << h[i].lh) + (1u << h[i].ll));
+  }
+  auto blocks = [&](int stage, int k, int per) {
+    uint64_t t = 0;
+    for (int i = 0; i < count; i++) t += sw_blocks(sw_units(h[i].l, stage, k), per);
+    return (unsigned)t;
+  };
+  k_sw_tables<<<dim3((tabmax + 127) / 128, count), 128, 0, st>>>(d);
+  k_sw_eq<<<blocks(0, 0, SW_THREADS), SW_THREADS, 0, st>>>(d, count);
+  k_sw_partials<<<blocks(0, 0, SW_PARTIAL_ROWS), SW_THREADS, 0, st>>>(d, count);
+  k_sw_statement<<<(count + 31) / 32, 32, 0, st>>>(d, count);
+  k_sw_batch<<<count, 256, 0, st>>>(d);
+  k_sw_init<<<blocks(1, 0, SW_THREADS), SW_THREADS, 0, st>>>(d, count);
+  for (uint32_t k = 0; k < lmax; k++) {
+    k_sw_step<<<count, 128, 0, st>>>(d, (int)k);
+    unsigned g = blocks(2, (int)k, SW_THREADS);
+    if (k == 0)
+      k_sw_fold<true><<<g, SW_THREADS, 0, st>>>(d, count, 0);
+    else
+      k_sw_fold<false><<<g, SW_THREADS, 0, st>>>(d, count, (int)k);
+  }
+  k_sw_finish<<<(count + 31) / 32, 32, 0, st>>>(d, count);
+  if (launches) *launches += 7 + 2 * (uint64_t)lmax;
+  return cudaGetLastError();
+}
+
+}  // namespace lbg
+
+using namespace lbg;
+
+namespace {
+int fail(int code, const std::string& m) {
+  set_last_error(m);
+  return code;
+}
+
+size_t al256(size_t b) { return (b + 255) / 256 * 256; }
+
+// Bytes in front of the scratch in the entry point's workspace: the instance's small values, its
+// table entry, its hasher state and its coordinates (32 slots of r_hi, then r_lo).
+size_t sw_head_bytes() {
+  return al256(sizeof(SwSmall)) + al256(sizeof(SwInst)) + al256(sizeof(HasherState)) + al256(39 * 16);
+}
+}  // namespace
+
+void lbg_switch_release(lbg_pp* pp) {
+  if (pp && pp->d_sw) {
+    cudaFree(pp->d_sw);
+    pp->d_sw = nullptr;
+  }
+}
 
 extern "C" {
 
@@ -251,92 +528,70 @@ int lbg_switch_prove(const lbg_pp* pp_c, const lbg_witness* w, const uint64_t* r
   lbg_pp* pp = const_cast<lbg_pp*>(pp_c);
   if (l != pp->params.witness_log_len || w->n != pp->n) return fail(LBG_ERR_INVALID, "the point does not match the parameters");
   if (nlo != 0 && nlo != 7) return fail(LBG_ERR_INVALID, "a bit-level point has 7 low coordinates");
-  if (l < 1) return fail(LBG_ERR_INVALID, "an empty trace");
+  if (l < 1 || l > 32) return fail(LBG_ERR_INVALID, "the trace has 2^1 .. 2^32 words");
   Transcript& tr = t->t;
-  // absorb_statement (crates/pcs/src/switch.rs:124-129)
-  tr.absorb_bytes((const uint8_t*)"labinius/switch", 15);
-  tr.absorb_b128(r_lo, nlo);
-  tr.absorb_b128(r_hi, l);
-  tr.absorb_b128(claim, 1);
-
   std::lock_guard<std::mutex> g(pp->mu);
   if (cudaSetDevice(pp->device) != cudaSuccess) return fail(LBG_ERR_CUDA, "cudaSetDevice");
   cudaStream_t st = pp->stream;
-  size_t n = pp->n;
-  int lh = (int)(l / 2), ll = (int)(l - lh);
-  B128d *d_r = nullptr, *d_ehi = nullptr, *d_elo = nullptr, *d_eq = nullptr;
-  F162d *d_rp = nullptr, *d_batch = nullptr, *d_psi = nullptr, *d_a = nullptr, *d_p = nullptr, *d_rr = nullptr;
-  unsigned long long *d_v = nullptr, *d_msg = nullptr;
-  auto release = [&]() {
-    void* ptrs[] = {d_r, d_ehi, d_elo, d_eq, d_rp, d_batch, d_psi, d_a, d_p, d_rr, d_v, d_msg};
-    for (void* q : ptrs) cudaFree(q);
-  };
-  if (cudaMalloc((void**)&d_r, l * 16) != cudaSuccess || cudaMalloc((void**)&d_ehi, ((size_t)1 << lh) * 16) != cudaSuccess ||
-      cudaMalloc((void**)&d_elo, ((size_t)1 << ll) * 16) != cudaSuccess || cudaMalloc((void**)&d_eq, n * 16) != cudaSuccess ||
-      cudaMalloc((void**)&d_rp, 7 * 24) != cudaSuccess || cudaMalloc((void**)&d_batch, 128 * 24) != cudaSuccess ||
-      cudaMalloc((void**)&d_psi, 4096 * 24) != cudaSuccess || cudaMalloc((void**)&d_a, n * 24) != cudaSuccess ||
-      cudaMalloc((void**)&d_p, n * 24) != cudaSuccess || cudaMalloc((void**)&d_rr, 24) != cudaSuccess ||
-      cudaMalloc((void**)&d_v, 128 * 16) != cudaSuccess || cudaMalloc((void**)&d_msg, 48) != cudaSuccess) {
-    cudaGetLastError();
-    release();
-    return fail(LBG_ERR_OOM, "switch: device allocation failed");
-  }
-  std::vector<uint64_t> r_pp(3 * l);
-  uint64_t msg[6];
-  cudaError_t e = cudaMemcpyAsync(d_r, r_hi, l * 16, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) {
-    k_sw_eq_tables<<<grid_for(((size_t)1 << lh) + ((size_t)1 << ll), 128), 128, 0, st>>>(d_r, lh, ll, d_ehi, d_elo);
-    k_sw_eq<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_ehi, d_elo, ll, n, d_eq);
-    e = cudaMemsetAsync(d_v, 0, 128 * 16, st);
-  }
-  if (e == cudaSuccess) {
-    k_sw_partials<<<grid_for(n, 16), 256, 0, st>>>(w->d, d_eq, n, d_v);
-    e = cudaMemcpyAsync(partials, d_v, 128 * 16, cudaMemcpyDeviceToHost, st);
-  }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e == cudaSuccess) {
-    // the batch (crates/pcs/src/switch.rs:149-150)
-    tr.absorb_b128(partials, 128);
-    uint64_t rp[21];
-    tr.sample_f162("labinius/switch-batch", rp, 7);
-    e = cudaMemcpyAsync(d_rp, rp, 7 * 24, cudaMemcpyHostToDevice, st);
-  }
-  if (e == cudaSuccess) {
-    k_sw_batch<<<1, 256, 0, st>>>(d_rp, d_batch, d_psi);
-    e = cudaMemsetAsync(d_msg, 0, 48, st);
-  }
-  if (e == cudaSuccess) {
-    size_t smem = 4096 * sizeof(F162d);
-    cudaFuncSetAttribute(k_sw_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_sw_init<<<grid_for(n / 2, 256), 256, smem, st>>>(w->d, d_eq, d_psi, n, d_a, d_p, d_msg);
-    e = cudaMemcpyAsync(msg, d_msg, 48, cudaMemcpyDeviceToHost, st);
-  }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  for (size_t round = 0; round < l && e == cudaSuccess; round++) {
-    // the round's message, its challenge (crates/pcs/src/switch.rs:152-159)
-    tr.absorb_f162(msg, 2);
-    uint64_t r[3];
-    tr.sample_f162("labinius/switch-round", r, 1);
-    std::memcpy(rounds + 6 * round, msg, 48);
-    std::memcpy(r_pp.data() + 3 * round, r, 24);
-    size_t half = n >> (round + 1);
-    e = cudaMemcpyAsync(d_rr, r, 24, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_msg, 0, 48, st);
-    if (e == cudaSuccess) {
-      k_sw_round<<<half >= 2 ? grid_for(half / 2, 256) : 1, 256, 0, st>>>(d_a, d_p, half, d_rr, d_msg);
-      e = cudaMemcpyAsync(msg, d_msg, 48, cudaMemcpyDeviceToHost, st);
+  if (!pp->d_sw) {
+    if (cudaMalloc((void**)&pp->d_sw, sw_head_bytes() + sw_scratch_bytes((uint32_t)l)) != cudaSuccess) {
+      cudaGetLastError();
+      pp->d_sw = nullptr;
+      return fail(LBG_ERR_OOM, "switch: device allocation failed");
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   }
-  if (e == cudaSuccess) e = cudaMemcpyAsync(opened, d_p, 24, cudaMemcpyDeviceToHost, st);
+  uint8_t* base = pp->d_sw;
+  SwSmall* d_small = (SwSmall*)base;
+  base += al256(sizeof(SwSmall));
+  SwInst* d_inst = (SwInst*)base;
+  base += al256(sizeof(SwInst));
+  HasherState* d_st = (HasherState*)base;
+  base += al256(sizeof(HasherState));
+  uint64_t* d_r = (uint64_t*)base;
+  base += al256(39 * 16);
+
+  SwInst h;
+  std::memset(&h, 0, sizeof(h));
+  h.w = w->d;
+  h.r_hi = d_r;
+  h.r_lo = nlo ? d_r + 2 * 32 : nullptr;
+  h.s = d_small;
+  h.st = d_st;
+  h.counter0 = tr.counter();
+  h.l = (uint32_t)l;
+  h.nlo = (uint32_t)nlo;
+  h.row_log = (uint32_t)(l - pp->params.column_log_len);
+  h.col_log = pp->params.column_log_len;
+  h.claim_given = 1;
+  sw_layout(h, base);
+  HasherState hs;
+  tr.state().save(hs);
+  std::vector<uint64_t> rbuf(2 * 39, 0);
+  std::memcpy(rbuf.data(), r_hi, l * 16);
+  if (nlo) std::memcpy(rbuf.data() + 2 * 32, r_lo, nlo * 16);
+  std::vector<SwSmall> out(1);
+  cudaError_t e = cudaMemsetAsync(d_small, 0, sizeof(SwSmall), st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_small->claim, claim, 16, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_st, &hs, sizeof(hs), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_r, rbuf.data(), rbuf.size() * 8, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_inst, &h, sizeof(h), cudaMemcpyHostToDevice, st);
+  uint64_t launches = 0;
+  if (e == cudaSuccess) e = enqueue_switch(d_inst, &h, 1, st, &launches);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), d_small, sizeof(SwSmall), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, d_st, sizeof(hs), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e == cudaSuccess) e = cudaGetLastError();
-  release();
   if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("switch: ") + cudaGetErrorString(e));
+  const SwSmall& o = out[0];
+  if (o.status != 1) return fail(LBG_ERR_CUDA, "switch: the device pass did not complete");
+  tr.state().load(hs);
+  tr.set_counter(h.counter0 + 1 + l);
+  std::memcpy(partials, o.v, 128 * 16);
+  std::memcpy(rounds, o.rounds, l * 48);
+  std::memcpy(opened, o.opened, 24);
   // EvaluationPoint::msb_first (crates/pcs/src/scheme/commitment.rs:163-174)
   size_t cl = pp->params.column_log_len, rows = l - cl;
-  for (size_t i = 0; i < rows; i++) std::memcpy(p0_out + 3 * i, r_pp.data() + 3 * (l - 1 - i), 24);
-  for (size_t i = 0; i < cl; i++) std::memcpy(p1_out + 3 * i, r_pp.data() + 3 * (cl - 1 - i), 24);
+  for (size_t i = 0; i < rows; i++) std::memcpy(p0_out + 3 * i, o.rr[l - 1 - i], 24);
+  for (size_t i = 0; i < cl; i++) std::memcpy(p1_out + 3 * i, o.rr[cl - 1 - i], 24);
   return LBG_OK;
 }
 

@@ -12,6 +12,7 @@
 #include "blake3_dev.cuh"
 #include "transcript.h"
 #include "transcript_dev.h"
+#include "upload.h"
 
 namespace lbg {
 
@@ -417,12 +418,11 @@ cudaError_t upload_absorb(AbsorbPlan& p) {
   if (e == cudaSuccess) e = cudaMalloc((void**)&p.d_entry_job, p.entry_job.size() * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void**)&p.d_stage_word_off, p.stage_word_off.size() * sizeof(uint64_t));
   if (e == cudaSuccess)
-    e = cudaMemcpy(p.d_jobs, p.jobs.data(), p.jobs.size() * sizeof(AbsorbJob), cudaMemcpyHostToDevice);
+    e = upload_sync(p.d_jobs, p.jobs.data(), p.jobs.size() * sizeof(AbsorbJob));
   if (e == cudaSuccess)
-    e = cudaMemcpy(p.d_entry_job, p.entry_job.data(), p.entry_job.size() * sizeof(int), cudaMemcpyHostToDevice);
+    e = upload_sync(p.d_entry_job, p.entry_job.data(), p.entry_job.size() * sizeof(int));
   if (e == cudaSuccess)
-    e = cudaMemcpy(p.d_stage_word_off, p.stage_word_off.data(), p.stage_word_off.size() * sizeof(uint64_t),
-                   cudaMemcpyHostToDevice);
+    e = upload_sync(p.d_stage_word_off, p.stage_word_off.data(), p.stage_word_off.size() * sizeof(uint64_t));
   return e;
 }
 
@@ -455,8 +455,8 @@ cudaError_t sampler_tables(int device, SamplerTables& out) {
     double *r = nullptr, *i = nullptr;
     cudaError_t e = cudaMalloc((void**)&r, bytes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&i, bytes);
-    if (e == cudaSuccess) e = cudaMemcpy(r, sampler_phase_re(), bytes, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(i, sampler_phase_im(), bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = upload_sync(r, sampler_phase_re(), bytes);
+    if (e == cudaSuccess) e = upload_sync(i, sampler_phase_im(), bytes);
     if (e != cudaSuccess) {
       cudaFree(r);
       cudaFree(i);

@@ -14,6 +14,7 @@ where the Rust code panics on misuse (assert!), ``VerificationError`` on rejecti
 """
 import ctypes
 import enum
+import struct
 from dataclasses import dataclass, field
 from typing import List, Optional
 
@@ -350,12 +351,30 @@ class Commitment:
     matrix: Optional[np.ndarray] = None
     top: Optional[np.ndarray] = None
     digits: Optional[np.ndarray] = None
+    params: Optional["Params"] = None
 
     def moduli(self):
         return self.primes
 
     def rows(self):
         return 4
+
+    def to_bytes(self) -> bytes:
+        """wire::pack_tagged_commitment (crates/pcs/src/wire/mod.rs:307-333): the form's tag, the
+        column count as a little-endian u32, then the matrix's i16 slots column by column, or the
+        packed bit-dropped commitment."""
+        head = struct.pack("<I", self.columns)
+        if self.matrix is not None:
+            return b"\x00" + head + np.ascontiguousarray(self.matrix, dtype="<i2").tobytes()
+        if self.params is None:
+            raise ValueError("a bit-dropped commitment packs against its parameters")
+        top = np.ascontiguousarray(self.top, dtype=np.uint16)
+        digits = np.ascontiguousarray(self.digits, dtype=np.uint16)
+        cp = self.params.native()
+        size = lib().lbg_params_pack_dropped(ctypes.byref(cp), ptr(top), ptr(digits), None, 0)
+        out = np.zeros(size, np.uint8)
+        lib().lbg_params_pack_dropped(ctypes.byref(cp), ptr(top), ptr(digits), ptr(out), size)
+        return b"\x02" + head + out.tobytes()
 
 
 class CommitmentOpening:
@@ -402,11 +421,11 @@ class Prover:
             top = np.zeros(r * N, np.uint16)
             digits = np.zeros((max(L - 1, 1), r * N), np.uint16)
             check(lib().lbg_commit(self._h, witness._h, None, ptr(top), ptr(digits), ctypes.byref(op)))
-            c = Commitment(pr.primes(), r, top=top, digits=digits[: L - 1])
+            c = Commitment(pr.primes(), r, top=top, digits=digits[: L - 1], params=pr)
         else:
             m = np.zeros((r, 4, L, N162), np.int16)
             check(lib().lbg_commit(self._h, witness._h, ptr(m), None, None, ctypes.byref(op)))
-            c = Commitment(pr.primes(), r, matrix=m)
+            c = Commitment(pr.primes(), r, matrix=m, params=pr)
         return c, CommitmentOpening(self, op)
 
     def keep_transform(self, enable: bool = True):

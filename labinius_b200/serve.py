@@ -1,9 +1,13 @@
 """Serving: a request loop with continuous batching over device arenas.
 
-A request is one commit + open round (commit, evaluation point, mle and row evaluation, folding
-challenges, fold) of its own witness under the server's key: any column count 2^c with the key's
-column length, a witness drawn from the request's seed (kind 0: Witness::random; kind 1: a B128
-trace lifted, crates/pcs/src/scheme/witness.rs:45-87).
+A request is one commit + open round of its own witness under the server's key: any column
+count 2^c with the key's column length, a witness drawn from the request's seed. Kind 0 is
+Witness::random (crates/pcs/src/scheme/witness.rs:66-87), opened as the plain round does (commit,
+evaluation point, mle and row evaluation, folding challenges, fold). Kind 1 is a B128 trace,
+committed lifted (crates/pcs/src/scheme/witness.rs:45-52) and opened through the cross-field
+switch at the request's point r (crates/pcs/examples/two_fields.rs:176-194: commit, the tagged
+commitment absorbed, switch::prove of the trace's value at r, row evaluation at the switch's
+point, folding challenges, fold); its result carries the switch proof and the claim.
 
 Continuous batching: the server owns `slots` device arenas (lbg_batch, sized once; admission is by
 arena room, i.e. by the HBM each slot reserved). Whenever a slot is free it admits, in arrival
@@ -14,14 +18,18 @@ slot's stream from witness generation to the folded witnesses. While one slot re
 back and lays out its next batch, the other slot's round runs on its own stream: requests that
 arrive while others are on the GPU are admitted as soon as a slot and its memory free up, and
 their work overlaps on the device. The parameters, the key and each slot's state stay resident.
-With transcript="host" the transcript steps run in the library's host code on a thread pool.
+With transcript="host" (kind 0 requests only) the transcript steps run in the library's host code
+on a thread pool.
 """
 import collections
 import concurrent.futures
+import hashlib
 import threading
 import time
 from dataclasses import dataclass, field
 from typing import List, Optional
+
+import numpy as np
 
 from .batch import Batch, InstanceRound
 from .scheme import PublicParameters
@@ -31,7 +39,8 @@ from .scheme import PublicParameters
 class Request:
     column_log_len: int
     seed: bytes
-    kind: int = 0               # 0: Witness::random(seed); 1: lifted B128 trace from seed
+    kind: int = 0               # 0: Witness::random(seed); 1: lifted B128 trace from seed, opened through the switch
+    point: Optional[np.ndarray] = None  # kind 1: r, [witness_log_len][2] uint64 (default: drawn from the seed)
     arrival: float = 0.0        # seconds on the server's clock
     admitted: float = 0.0
     done: float = 0.0
@@ -70,6 +79,14 @@ class Server:
 
     def clock(self):
         return time.perf_counter() - self.t0
+
+    def switch_point(self, req: Request) -> np.ndarray:
+        """The B128 point a kind-1 request is opened at: its own, or SHAKE256 of its seed."""
+        l = self.pp.params.row_log_len() + req.column_log_len
+        if req.point is not None:
+            return np.ascontiguousarray(req.point, dtype=np.uint64).reshape(l, 2)
+        raw = hashlib.shake_256(bytes(req.seed) + b"labinius/served-point").digest(16 * l)
+        return np.frombuffer(raw, dtype="<u8").reshape(l, 2).copy()
 
     def submit(self, req: Request) -> Request:
         if (1 << req.column_log_len) > self.capacity:
@@ -111,6 +128,8 @@ class Server:
             try:
                 b.assign([r.column_log_len for r in reqs])
                 b.witness_random([r.seed for r in reqs], [r.kind for r in reqs])
+                if any(r.kind == 1 for r in reqs):
+                    b.set_switch([r.kind == 1 for r in reqs], [self.switch_point(r) for r in reqs if r.kind == 1])
                 rounds = b.round(self.domain, pool=self.pool, transcript=self.transcript, copy=self.keep_results)
                 self.batches += 1
                 err = None

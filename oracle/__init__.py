@@ -462,3 +462,48 @@ def switch_verify(r_hi, claim, partials, rounds, opened, t: Transcript, r_lo=Non
                                  _p(np.ascontiguousarray(rounds, np.uint64)),
                                  _p(np.ascontiguousarray(opened, np.uint64)), t.h, _p(r_pp))
     return bool(ok), r_pp[:l]
+
+
+def tagged_commitment(params: Params, C=None, top=None, digits=None) -> bytes:
+    """Commitment::to_bytes, wire::pack_tagged_commitment (crates/pcs/src/wire/mod.rs:307-333)."""
+    head = int(params.columns).to_bytes(4, "little")
+    if params.dropped_bits:
+        return b"\x02" + head + pack_dropped(params, top, digits)
+    return b"\x00" + head + np.ascontiguousarray(C, dtype="<i2").tobytes()
+
+
+def switch_round(params: Params, matrix_seed: bytes, trace, r_hi, claim_value=None,
+                 domain: bytes = b"labinius/reference"):
+    """A B128 trace committed as Witness::lifted and opened through the switch, the prover of
+    crates/pcs/examples/two_fields.rs:176-194: commit, absorb the tagged commitment, switch::prove
+    (the claim defaults to the trace's value at r_hi), row_evaluate at the switch's point,
+    FoldingChallenges::derive, fold."""
+    tr = np.ascontiguousarray(trace, dtype=np.uint64).reshape(-1, 2)
+    witness = np.zeros((len(tr), 3), np.uint64)
+    witness[:, :2] = tr  # F162::from_b128 (crates/pcs/src/fields/scalar.rs:72-74)
+    A = key_expand(params, key_seed(matrix_seed))
+    C = commit(params, A, witness)
+    out = dict(A=A, witness=witness, C=C)
+    t = Transcript(domain)
+    if params.dropped_bits:
+        top, digits = drop_bits(params, C)
+        out.update(top=top, digits=digits)
+        t.absorb_bytes(tagged_commitment(params, top=top, digits=digits))
+    else:
+        t.absorb_bytes(tagged_commitment(params, C=C))
+    c = switch_mle(tr, r_hi) if claim_value is None else np.asarray(claim_value, np.uint64)
+    partials, rounds, opened, r_pp = switch_prove(tr, r_hi, c, t)
+    rows, cl = params.row_log_len, params.column_log_len
+    p0 = np.ascontiguousarray(r_pp[::-1][:rows])  # EvaluationPoint::msb_first
+    p1 = np.ascontiguousarray(r_pp[:cl][::-1])
+    u = row_evaluate(witness, p0)
+    mle = claim(u, p1)
+    ch = derive_folding_challenges(params, t, u)
+    v = fold(params, witness, ch)
+    out.update(claim=c, partials=partials, rounds=rounds, opened=opened, p0=p0, p1=p1, u=u, mle=mle,
+               challenges=ch, v=v)
+    if not params.dropped_bits:
+        out["folded_commitment"] = fold_commitment(params, C, ch)
+    out["transcript_tail"] = t.fill(b"labinius/test-tail", 32)
+    return out
+

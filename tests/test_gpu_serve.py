@@ -1,6 +1,7 @@
 """Serving with continuous batching: each request's result in the mix equals the same request run
-alone through the single-instance path (native witnesses and lifted B128 traces, mixed sizes,
-arrivals while other requests are on the GPU); admission respects the arena size."""
+alone through the single-instance path (native witnesses, and B128 traces opened through the
+cross-field switch; mixed sizes, arrivals while other requests are on the GPU); admission respects
+the arena size."""
 import time
 
 import numpy as np
@@ -11,27 +12,37 @@ from rounds import DOMAIN, MATRIX_SEED, product_params
 pytestmark = pytest.mark.gpu
 
 
-def alone(oracle, row_log, primes, req):
-    """The request's round on its own: Witness::random or Witness::lifted, then the plain path."""
+def alone(oracle, row_log, primes, req, r_hi):
+    """The request's round on its own: Witness::random through the plain path, or a B128 trace
+    through the switch (crates/pcs/examples/two_fields.rs:176-194)."""
     import labinius_b200 as L
+    from labinius_b200 import switch
 
     cl = req.column_log_len
     params = product_params((row_log + cl, cl, primes, 0))
     pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+    prover, verifier = L.Prover(pp), L.Verifier(pp)
+    t = L.Transcript(DOMAIN)
+    proof = claim = None
     if req.kind == 1:
         n = params.witness_len()
         raw = oracle.blake3(b"labinius/b128-trace", 16 * n, key=req.seed)
-        w = L.Witness.lifted(pp, np.frombuffer(raw, dtype=np.uint64).reshape(-1, 2))
+        trace = np.frombuffer(raw, dtype=np.uint64).reshape(-1, 2)
+        w = L.Witness.lifted(pp, trace)
+        c, op = prover.commit(w)
+        t.absorb_bytes(c.to_bytes())
+        claim = oracle.switch_mle(trace, r_hi)
+        proof, point = switch.prove(pp, w, r_hi, claim, t)
+        mle = proof.opened
     else:
         w = L.Witness.random(pp, req.seed)
-    prover, verifier = L.Prover(pp), L.Verifier(pp)
-    c, op = prover.commit(w)
-    t = L.Transcript(DOMAIN)
-    point = verifier.derive_evaluation_point(t, c)
-    mle, row = w.mle_evaluate(point), w.row_evaluate(point)
+        c, op = prover.commit(w)
+        point = verifier.derive_evaluation_point(t, c)
+        mle = w.mle_evaluate(point)
+    row = w.row_evaluate(point)
     ch = verifier.derive_folding_challenges(t, row)
     v = prover.fold(op, ch)
-    return c.matrix, point, mle, row.values, ch.challenges, v.elements
+    return c.matrix, point, mle, row.values, ch.challenges, v.elements, proof, claim
 
 
 @pytest.mark.parametrize("transcript", ["device", "host"])
@@ -46,7 +57,8 @@ def test_results_in_the_mix_equal_results_alone(oracle, transcript):
     reqs = []
     for i in range(14):
         cl = int(rng.integers(1, 6))
-        reqs.append(srv.submit(Request(cl, bytes([0x40 + i]) * 32, kind=int(i % 5 == 4))))
+        kind = int(i % 5 == 4) if transcript == "device" else 0  # the switch runs its transcript on the device
+        reqs.append(srv.submit(Request(cl, bytes([0x40 + i]) * 32, kind=kind)))
         if i % 4 == 3:
             time.sleep(0.01)  # later arrivals join while earlier batches run
     too_big = srv.submit(Request(6, bytes(32)))  # 64 columns > 48
@@ -57,8 +69,13 @@ def test_results_in_the_mix_equal_results_alone(oracle, transcript):
     assert srv.batches >= 2
     for r in reqs:
         assert r.error is None, r.error
-        m, point, mle, u, ch, v = alone(oracle, row_log, primes, r)
+        m, point, mle, u, ch, v, proof, claim = alone(oracle, row_log, primes, r, srv.switch_point(r))
         res = r.result
+        if r.kind == 1:
+            assert np.array_equal(res.claim, claim)
+            assert np.array_equal(res.switch.partials, proof.partials)
+            assert np.array_equal(res.switch.rounds, proof.rounds)
+            assert np.array_equal(res.switch.opened, proof.opened)
         assert np.array_equal(res.matrix, m)
         assert np.array_equal(res.p0, point.p0) and np.array_equal(res.p1, point.p1)
         assert np.array_equal(res.mle, mle) and np.array_equal(res.u, u)
