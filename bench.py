@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-switch", action="store_true")
     ap.add_argument("--no-ntt", action="store_true")
     ap.add_argument("--no-suites", action="store_true")
     ap.add_argument("--ntt-count", type=int, default=1 << 20, help="ring elements of the NTT microbenchmark")
@@ -466,16 +467,64 @@ def run_ntt_micro(steps, count=1 << 20, q=3889):
             "bytes_per_ring_element": 2592, "workload": "all ring elements of a 2^22 witness, d = 648, q = 3889"}
 
 
+def b128_claim(partials):
+    """The trace's value at the switch's point from its partial evaluations, sum_k v_k x^k in B128
+    (crates/pcs/src/switch.rs:116-122)."""
+    acc = 0
+    for k in range(127, -1, -1):
+        acc <<= 1
+        if acc >> 128:
+            acc ^= (1 << 128) | 0x87
+        acc ^= int(partials[k][0]) | (int(partials[k][1]) << 64)
+    return np.array([acc & ((1 << 64) - 1), acc >> 64], np.uint64)
+
+
+def run_switch(steps, sizes=(18, 20, 22)):
+    """The cross-field switch prover (crates/pcs/src/switch.rs:65-74) through the API: a lifted B128
+    trace of 2^l words (column length 2048), a point r and the trace's value there, switch::prove
+    with the caller's transcript (moved to the device and back); host clock around the synchronous
+    call, inputs resident."""
+    import labinius_b200 as L
+    from labinius_b200 import switch
+
+    out = {}
+    for wl in sizes:
+        params = L.Params.new(wl, wl - 11, [L.Modulus.Q9721_FS_S])
+        pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+        rng = np.random.default_rng(wl)
+        n = params.witness_len()
+        trace = np.frombuffer(rng.bytes(16 * n), dtype=np.uint64).reshape(n, 2)
+        r = np.frombuffer(rng.bytes(16 * wl), dtype=np.uint64).reshape(wl, 2)
+        w = L.Witness.lifted(pp, trace)
+        proof, _ = switch.prove(pp, w, r, np.zeros(2, np.uint64), L.Transcript(b"claim"))
+        claim = b128_claim(proof.partials)
+        switch.prove(pp, w, r, claim, L.Transcript(DOMAIN))
+        ts = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            switch.prove(pp, w, r, claim, L.Transcript(DOMAIN))
+            ts.append(time.perf_counter() - t0)
+        ms = 1000 * float(np.median(ts))
+        out[f"2^{wl}"] = {"ms": ms, "elems_s": n / (ms / 1000)}
+        del w, pp
+    out["workload"] = ("switch::prove of a lifted B128 trace at a random point, claim = the trace's value there; "
+                       "median host-clock time of the synchronous API call")
+    return out
+
+
 def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
     """Served: commit+open requests with log2 n ~ U{18..22} (column length 2048, moduli [3889, 9721]),
-    80% Witness::random and 20% lifted B128 traces, each from its own seed, through the serving loop
-    (continuous batching over two device arenas, host steps on every host core). First the saturated
-    throughput (every request queued at once, a sample of the stream); then the Poisson stream of
-    `requests` arrivals at `load` x that throughput, with p50/p99 latency from arrival to result.
-    The comparison is the plain per-request path, one request after another (commit, evaluation
-    point, row and mle evaluation, folding challenges, fold), on a sample of the same requests,
-    its witnesses made before the clock starts."""
+    80% Witness::random and 20% B128 traces opened through the cross-field switch, each from its
+    own seed, through the serving loop (continuous batching over two device arenas, transcripts on
+    the device). First the saturated throughput (every request queued at once, a sample of the
+    stream); then the Poisson stream of `requests` arrivals at `load` x that throughput, with
+    p50/p99 latency from arrival to result. The comparison is the plain per-request path, one
+    request after another, on a sample of the same requests, its witnesses (and the B128 claims)
+    made before the clock starts: commit, evaluation point, row and mle evaluation, folding
+    challenges, fold; for a B128 trace commit, the tagged commitment absorbed, switch::prove, row
+    evaluation at its point, folding challenges, fold (crates/pcs/examples/two_fields.rs:176-194)."""
     import labinius_b200 as L
+    from labinius_b200 import switch
     from labinius_b200.batch import Batch
     from labinius_b200.serve import Request, Server
 
@@ -526,7 +575,7 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
     # the plain per-request path on a sample of the same requests
     pps = {}
     sample = list(range(min(plain_sample, requests)))
-    wits = []
+    wits, points, claims = [], {}, {}
     for i in sample:
         c = col_logs[i]
         if c not in pps:
@@ -539,6 +588,9 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
             g.witness_random([seeds[i]], [1])
             wits.append(L.Witness.lifted(p, np.ascontiguousarray(g.elements(0)[:, :2])))
             del g
+            points[i] = srv.switch_point(Request(col_logs[i], seeds[i], 1))
+            proof, _ = switch.prove(p, wits[-1], points[i], np.zeros(2, np.uint64), L.Transcript(b"claim"))
+            claims[i] = b128_claim(proof.partials)
         else:
             wits.append(L.Witness.random(p, seeds[i]))
     lat_plain = []
@@ -549,8 +601,12 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
         w = wits[k]
         c, op = prover.commit(w)
         t = L.Transcript(DOMAIN)
-        point = verifier.derive_evaluation_point(t, c)
-        w.mle_evaluate(point)
+        if kinds[i]:
+            t.absorb_bytes(c.to_bytes())
+            _, point = switch.prove(p, w, points[i], claims[i], t)
+        else:
+            point = verifier.derive_evaluation_point(t, c)
+            w.mle_evaluate(point)
         row = w.row_evaluate(point)
         ch = verifier.derive_folding_challenges(t, row)
         prover.fold(op, ch)
@@ -565,9 +621,12 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
             "plain_elems_s": plain_elems, "plain_sample": len(sample),
             "plain_p50_ms": float(np.percentile(lat_plain, 50)), "plain_p99_ms": float(np.percentile(lat_plain, 99)),
             "speedup_saturated_vs_plain": sat_elems / plain_elems,
-            "workload": "commit+open (commit, evaluation point, mle and row evaluation, folding challenges, fold) "
-                        "per request; log2 n ~ U{18..22}, column length 2048, moduli [3889, 9721]; 80% "
-                        "Witness::random, 20% lifted B128 traces; Poisson arrivals at load x saturated rate",
+            "workload": "commit+open per request; log2 n ~ U{18..22}, column length 2048, moduli [3889, 9721]; "
+                        "80% Witness::random (commit, evaluation point, mle and row evaluation, folding "
+                        "challenges, fold), 20% B128 traces opened through the cross-field switch at a point "
+                        "drawn from the request's seed (commit, tagged commitment absorbed, switch::prove of "
+                        "the trace's value there, row evaluation, folding challenges, fold); Poisson "
+                        "arrivals at load x saturated rate",
             "slots": slots, "slot_columns": 8192, "host_threads": os.cpu_count() or 1}
 
 
@@ -747,6 +806,9 @@ def run_ours(args):
         ntt_micro = run_ntt_micro(max(3, min(args.steps, 10)), count=args.ntt_count)
         for k in ("forward", "inverse"):
             ntt_micro[k]["frac_of_hbm"] = ntt_micro[k]["gbs"] / hbm
+    switch_times = None
+    if not args.no_switch and rank == 0:
+        switch_times = run_switch(max(3, min(args.steps, 10)))
     served = None
     if not args.no_served and rank == 0 and world == 1:
         served = run_served(args.served_requests, args.served_plain_sample)
@@ -779,6 +841,7 @@ def run_ours(args):
         "e2e": e2e,
         "batched": batched,
         "served": served,
+        "switch": switch_times,
         "ntt_microbench": ntt_micro,
         "suites": suites,
         "verifier": verifier_times,

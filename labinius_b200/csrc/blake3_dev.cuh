@@ -216,96 +216,62 @@ struct Tail {
   }
 };
 
-// In-place absorbs into a hasher state in device memory, by one thread, keeping the canonical form
-// of hasher_state.h (so the host and the parallel absorb kernels can continue from it): the
-// state's scalar fields and open block are worked on in registers, its subtree stack in place;
-// store() writes the rest back.
-struct Absorber {
-  HasherState* g;
-  uint32_t key[8];
-  uint32_t flags;
-  uint32_t cv[8];
-  uint8_t buf[64];
-  uint32_t buf_len, blocks, stack_len;
-  uint64_t chunk_counter;
+// A hasher state that one thread owns while it absorbs (a copy in shared memory, so the
+// sequential hashing of a transcript step is not bound by device-memory latency): absorbs in
+// place, keeping the canonical form of hasher_state.h, so the host and the parallel absorb
+// kernels can continue from it. hs_copy moves a state between device and shared memory with the
+// whole block.
+__device__ inline void hs_copy(HasherState* dst, const HasherState* src) {
+  static_assert(sizeof(HasherState) % 4 == 0, "HasherState is copied as words");
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+  uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(HasherState) / 4); i += blockDim.x) d[i] = s[i];
+}
 
-  __device__ void load(HasherState* s) {
-    g = s;
-    for (int i = 0; i < 8; i++) {
-      key[i] = s->key[i];
-      cv[i] = s->cv[i];
-    }
-    flags = s->flags;
-    for (int i = 0; i < 64; i++) buf[i] = s->buf[i];
-    buf_len = s->buf_len;
-    blocks = s->blocks;
-    chunk_counter = s->chunk_counter;
-    stack_len = s->stack_len < 54 ? s->stack_len : 54;
-  }
-
-  __device__ void store() {
-    for (int i = 0; i < 8; i++) g->cv[i] = cv[i];
-    for (int i = 0; i < 64; i++) g->buf[i] = buf[i];
-    g->buf_len = buf_len;
-    g->blocks = blocks;
-    g->chunk_counter = chunk_counter;
-    g->stack_len = stack_len;
-  }
-
-  __device__ void compress_buf(uint32_t fl, uint32_t out[16]) {
-    uint32_t m[16];
-    bytes_to_words(buf, m, 16);
-    compress(cv, m, chunk_counter, 64, fl, out);
-  }
-
-  // merge while the chunk count has trailing zero bits, then push (the host hasher's rule)
-  __device__ void push_cv(const uint32_t in[8], uint64_t total_chunks) {
-    uint32_t cur[8];
-    for (int i = 0; i < 8; i++) cur[i] = in[i];
-    while ((total_chunks & 1) == 0 && stack_len > 0) {
-      stack_len--;
-      parent_cv(key, flags, g->stack[stack_len], cur, cur);
-      total_chunks >>= 1;
-    }
-    if (stack_len < 54) {
-      for (int i = 0; i < 8; i++) g->stack[stack_len][i] = cur[i];
-      stack_len++;
-    }
-  }
-
-  __device__ void update(const uint8_t* p, uint32_t len) {
-    while (len > 0) {
-      if (blocks == 15 && buf_len == 64) {
-        uint32_t o[16];
-        compress_buf(flags | b3::CHUNK_END, o);
-        chunk_counter++;
-        push_cv(o, chunk_counter);
-        for (int i = 0; i < 8; i++) cv[i] = key[i];
-        buf_len = 0;
-        blocks = 0;
+__device__ inline void hs_absorb(HasherState* s, const uint8_t* p, uint32_t len) {
+  while (len > 0) {
+    if (s->buf_len == 64) {  // the open block is full and more bytes follow: compress it
+      uint32_t m[16], o[16];
+      bytes_to_words(s->buf, m, 16);
+      if (s->blocks == 15) {
+        compress(s->cv, m, s->chunk_counter, 64, s->flags | b3::CHUNK_END, o);
+        s->chunk_counter++;
+        // merge while the chunk count has trailing zero bits, then push (the host hasher's rule)
+        uint64_t total = s->chunk_counter;
+        uint32_t cur[8];
+        for (int i = 0; i < 8; i++) cur[i] = o[i];
+        while ((total & 1) == 0 && s->stack_len > 0) {
+          s->stack_len--;
+          parent_cv(s->key, s->flags, s->stack[s->stack_len], cur, cur);
+          total >>= 1;
+        }
+        if (s->stack_len < 54) {
+          for (int i = 0; i < 8; i++) s->stack[s->stack_len][i] = cur[i];
+          s->stack_len++;
+        }
+        for (int i = 0; i < 8; i++) s->cv[i] = s->key[i];
+        s->blocks = 0;
+      } else {
+        compress(s->cv, m, s->chunk_counter, 64, s->flags | (s->blocks == 0 ? b3::CHUNK_START : 0), o);
+        for (int i = 0; i < 8; i++) s->cv[i] = o[i];
+        s->blocks++;
       }
-      if (buf_len == 64) {
-        uint32_t o[16];
-        compress_buf(flags | (blocks == 0 ? b3::CHUNK_START : 0), o);
-        for (int i = 0; i < 8; i++) cv[i] = o[i];
-        blocks++;
-        buf_len = 0;
-      }
-      uint32_t take = 64 - buf_len;
-      if (take > len) take = len;
-      for (uint32_t i = 0; i < take; i++) buf[buf_len + i] = p[i];
-      buf_len += take;
-      p += take;
-      len -= take;
+      s->buf_len = 0;
     }
+    uint32_t take = 64 - s->buf_len;
+    if (take > len) take = len;
+    for (uint32_t i = 0; i < take; i++) s->buf[s->buf_len + i] = p[i];
+    s->buf_len += take;
+    p += take;
+    len -= take;
   }
+}
 
-  __device__ void update_u64(uint64_t x) {
-    uint8_t b[8];
-    for (int i = 0; i < 8; i++) b[i] = (uint8_t)(x >> (8 * i));
-    update(b, 8);
-  }
-};
+__device__ inline void hs_absorb_u64(HasherState* s, uint64_t x) {
+  uint8_t b[8];
+  for (int i = 0; i < 8; i++) b[i] = (uint8_t)(x >> (8 * i));
+  hs_absorb(s, b, 8);
+}
 
 // The transcript's derive(label) on a base state with derivation counter `counter`.
 __device__ __forceinline__ void derive_root(const HasherState* st, uint64_t counter, const char* label, uint32_t len,

@@ -182,47 +182,79 @@ __device__ __forceinline__ uint64_t read_u64(dev::Reader& rd) {
   return x;
 }
 
-// One thread per instance: the claim (if the statement leaves it to the prover: the trace's value
+// One block per instance: the claim (if the statement leaves it to the prover: the trace's value
 // at r_hi, sum_k v[k] x^k, crates/pcs/src/switch.rs:116-122), absorb_statement and the partials
-// (crates/pcs/src/switch.rs:124-129, 147-148), then the batch coordinates,
+// (crates/pcs/src/switch.rs:124-129, 147-148) staged as one byte string in shared memory and
+// absorbed by thread 0 into the shared copy of the hasher, then the batch coordinates,
 // sample_f162("labinius/switch-batch", 7) (crates/pcs/src/switch.rs:149,
 // crates/pcs/src/challenge.rs:129-140).
-__global__ void k_sw_statement(const SwInst* __restrict__ I, int count) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  const SwInst& s = I[i];
+constexpr int SW_STMT_MAX = 23 + 8 + 16 * 7 + 8 + 16 * 32 + 24 + 8 + 16 * 128;
+__global__ void k_sw_statement(const SwInst* __restrict__ I) {
+  const SwInst& s = I[blockIdx.x];
   SwSmall* sm = s.s;
-  if (!s.claim_given) {
-    B128d acc{0, 0};
-    for (int k = 127; k >= 0; k--) acc = b_add(b_times_x(acc), B128d{sm->v[k][0], sm->v[k][1]});
-    sm->claim[0] = acc.lo;
-    sm->claim[1] = acc.hi;
+  __shared__ HasherState sh;
+  __shared__ uint64_t v[256], claim[2];
+  __shared__ uint8_t bytes[SW_STMT_MAX];
+  dev::hs_copy(&sh, s.st);
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) v[t] = (&sm->v[0][0])[t];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    B128d acc{sm->claim[0], sm->claim[1]};
+    if (!s.claim_given) {
+      acc = B128d{0, 0};
+      for (int k = 127; k >= 0; k--) acc = b_add(b_times_x(acc), B128d{v[2 * k], v[2 * k + 1]});
+      sm->claim[0] = acc.lo;
+      sm->claim[1] = acc.hi;
+    }
+    claim[0] = acc.lo;
+    claim[1] = acc.hi;
   }
-  dev::Absorber h;
-  h.load(s.st);
-  h.update_u64(15);
-  h.update((const uint8_t*)c_sw_label, 15);
-  h.update_u64(s.nlo);
-  for (uint32_t k = 0; k < 2 * s.nlo; k++) h.update_u64(s.r_lo[k]);
-  h.update_u64(s.l);
-  for (uint32_t k = 0; k < 2 * s.l; k++) h.update_u64(s.r_hi[k]);
-  h.update_u64(1);
-  h.update_u64(sm->claim[0]);
-  h.update_u64(sm->claim[1]);
-  h.update_u64(128);
-  for (int k = 0; k < 128; k++) {
-    h.update_u64(sm->v[k][0]);
-    h.update_u64(sm->v[k][1]);
+  __syncthreads();
+  // the byte string: le64(15) "labinius/switch", le64(nlo) r_lo, le64(l) r_hi, le64(1) claim,
+  // le64(128) partials
+  const uint32_t o_lo = 31, o_hi = o_lo + 16 * s.nlo + 8, o_claim = o_hi + 16 * s.l + 8, o_v = o_claim + 24,
+                 total = o_v + 16 * 128;
+  for (uint32_t b = threadIdx.x; b < total; b += blockDim.x) {
+    uint64_t word;
+    uint32_t at;
+    if (b < 8) {
+      word = 15, at = b;
+    } else if (b < 23) {
+      bytes[b] = (uint8_t)c_sw_label[b - 8];
+      continue;
+    } else if (b < o_lo) {
+      word = s.nlo, at = b - 23;
+    } else if (b < o_hi - 8) {
+      word = s.r_lo[(b - o_lo) / 8], at = (b - o_lo) % 8;
+    } else if (b < o_hi) {
+      word = s.l, at = b - (o_hi - 8);
+    } else if (b < o_claim - 8) {
+      word = s.r_hi[(b - o_hi) / 8], at = (b - o_hi) % 8;
+    } else if (b < o_claim) {
+      word = 1, at = b - (o_claim - 8);
+    } else if (b < o_claim + 16) {
+      word = claim[(b - o_claim) / 8], at = (b - o_claim) % 8;
+    } else if (b < o_v) {
+      word = 128, at = b - (o_v - 8);
+    } else {
+      word = v[(b - o_v) / 8], at = (b - o_v) % 8;
+    }
+    bytes[b] = (uint8_t)(word >> (8 * at));
   }
-  h.store();
-  XofRoot root;
-  dev::derive_root(s.st, s.counter0, c_sw_batch, 21, root);
-  dev::Reader rd;
-  rd.init(root);
-  for (int c = 0; c < 7; c++) {
-    for (int w = 0; w < 3; w++) sm->rp[c][w] = read_u64(rd);
-    sm->rp[c][2] &= (1ull << 34) - 1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    dev::hs_absorb(&sh, bytes, total);
+    XofRoot root;
+    dev::derive_root(&sh, s.counter0, c_sw_batch, 21, root);
+    dev::Reader rd;
+    rd.init(root);
+    for (int c = 0; c < 7; c++) {
+      for (int w = 0; w < 3; w++) sm->rp[c][w] = read_u64(rd);
+      sm->rp[c][2] &= (1ull << 34) - 1;
+    }
   }
+  __syncthreads();
+  dev::hs_copy(s.st, &sh);
 }
 
 // batch = the expansion of the 7 sampled F162 (crossfield.rs:65-76); psi[16 c + t] = the XOR of
@@ -317,14 +349,19 @@ __global__ void __launch_bounds__(SW_THREADS) k_sw_init(const SwInst* __restrict
   xor_reduce_store(e0, ei, &s.s->msg[0]);
 }
 
-// One block per instance whose round k is due: the round's message into the transcript,
-// sample_f162("labinius/switch-round", 1) (crates/pcs/src/switch.rs:152-159), the message
-// accumulators cleared, and the tables of (t x^{4i}) r for the fold.
+// One block per instance whose round k is due: the round's message into the transcript (thread 0
+// on the shared copy of the hasher), sample_f162("labinius/switch-round", 1)
+// (crates/pcs/src/switch.rs:152-159), the message accumulators cleared, and the tables of
+// (t x^{4i}) r for the fold.
 __global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
   const SwInst& s = I[blockIdx.x];
   if ((uint32_t)k >= s.l) return;
   SwSmall* sm = s.s;
+  __shared__ HasherState sh;
   __shared__ F162d R4[41];
+  __shared__ uint8_t mb[56];
+  dev::hs_copy(&sh, s.st);
+  __syncthreads();
   if (threadIdx.x == 0) {
     uint64_t msg[6];
     for (int q = 0; q < 6; q++) {
@@ -332,13 +369,11 @@ __global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
       sm->rounds[k][q] = msg[q];
       sm->msg[q] = 0;
     }
-    dev::Absorber h;
-    h.load(s.st);
-    h.update_u64(2);
-    for (int q = 0; q < 6; q++) h.update_u64(msg[q]);
-    h.store();
+    // absorb_f162(&msg): le64(2), then the six words
+    for (int b = 0; b < 56; b++) mb[b] = (uint8_t)((b < 8 ? 2ull : msg[(b - 8) / 8]) >> (8 * (b % 8)));
+    dev::hs_absorb(&sh, mb, 56);
     XofRoot root;
-    dev::derive_root(s.st, s.counter0 + 1 + (uint64_t)k, c_sw_round, 21, root);
+    dev::derive_root(&sh, s.counter0 + 1 + (uint64_t)k, c_sw_round, 21, root);
     dev::Reader rd;
     rd.init(root);
     F162d r;
@@ -351,6 +386,7 @@ __global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
     }
   }
   __syncthreads();
+  dev::hs_copy(s.st, &sh);
   for (int e = threadIdx.x; e < 41 * 16; e += blockDim.x) {
     int q = e >> 4, t = e & 15;
     F162d x = R4[q], acc{{0, 0, 0}};
@@ -475,7 +511,7 @@ cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStre
   k_sw_tables<<<dim3((tabmax + 127) / 128, count), 128, 0, st>>>(d);
   k_sw_eq<<<blocks(0, 0, SW_THREADS), SW_THREADS, 0, st>>>(d, count);
   k_sw_partials<<<blocks(0, 0, SW_PARTIAL_ROWS), SW_THREADS, 0, st>>>(d, count);
-  k_sw_statement<<<(count + 31) / 32, 32, 0, st>>>(d, count);
+  k_sw_statement<<<count, 128, 0, st>>>(d);
   k_sw_batch<<<count, 256, 0, st>>>(d);
   k_sw_init<<<blocks(1, 0, SW_THREADS), SW_THREADS, 0, st>>>(d, count);
   for (uint32_t k = 0; k < lmax; k++) {
