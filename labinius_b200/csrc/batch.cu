@@ -786,7 +786,7 @@ int lbg_batch_round(lbg_batch* b, const uint8_t* domain, size_t domain_len, cons
   if (!b->sw_h.empty()) {
     uint32_t lmax = 0;
     for (const SwInst& h : b->sw_h) lmax = std::max(lmax, h.l);
-    per_round += 7 + 2 * (uint64_t)lmax;
+    per_round += sw_launches(lmax);
   }
   if (b->graphs) {
     if (!b->g_round) {

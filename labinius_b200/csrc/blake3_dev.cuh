@@ -216,11 +216,8 @@ struct Tail {
   }
 };
 
-// A hasher state that one thread owns while it absorbs (a copy in shared memory, so the
-// sequential hashing of a transcript step is not bound by device-memory latency): absorbs in
-// place, keeping the canonical form of hasher_state.h, so the host and the parallel absorb
-// kernels can continue from it. hs_copy moves a state between device and shared memory with the
-// whole block.
+// hs_copy moves a hasher state between device and shared memory with the whole block (the
+// transcript steps of the switch work on a shared copy).
 __device__ inline void hs_copy(HasherState* dst, const HasherState* src) {
   static_assert(sizeof(HasherState) % 4 == 0, "HasherState is copied as words");
   const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
@@ -228,49 +225,103 @@ __device__ inline void hs_copy(HasherState* dst, const HasherState* src) {
   for (int i = threadIdx.x; i < (int)(sizeof(HasherState) / 4); i += blockDim.x) d[i] = s[i];
 }
 
-__device__ inline void hs_absorb(HasherState* s, const uint8_t* p, uint32_t len) {
-  while (len > 0) {
-    if (s->buf_len == 64) {  // the open block is full and more bytes follow: compress it
-      uint32_t m[16], o[16];
-      bytes_to_words(s->buf, m, 16);
-      if (s->blocks == 15) {
-        compress(s->cv, m, s->chunk_counter, 64, s->flags | b3::CHUNK_END, o);
-        s->chunk_counter++;
-        // merge while the chunk count has trailing zero bits, then push (the host hasher's rule)
-        uint64_t total = s->chunk_counter;
-        uint32_t cur[8];
-        for (int i = 0; i < 8; i++) cur[i] = o[i];
-        while ((total & 1) == 0 && s->stack_len > 0) {
-          s->stack_len--;
-          parent_cv(s->key, s->flags, s->stack[s->stack_len], cur, cur);
-          total >>= 1;
-        }
-        if (s->stack_len < 54) {
-          for (int i = 0; i < 8; i++) s->stack[s->stack_len][i] = cur[i];
-          s->stack_len++;
-        }
-        for (int i = 0; i < 8; i++) s->cv[i] = s->key[i];
-        s->blocks = 0;
-      } else {
-        compress(s->cv, m, s->chunk_counter, 64, s->flags | (s->blocks == 0 ? b3::CHUNK_START : 0), o);
-        for (int i = 0; i < 8; i++) s->cv[i] = o[i];
-        s->blocks++;
+// Staged absorbs and derivations: the bytes to hash are first laid out by the whole block in a
+// word-aligned shared buffer, `stage` = the state's open block (buf_len bytes) followed by the new
+// bytes (`total` in all, zero-filled to the next 64-byte boundary); one thread then compresses
+// whole 64-byte blocks read as words, so its sequential work is the compressions alone. The
+// state keeps the canonical form of hasher_state.h, so the host and the parallel absorb kernels
+// can continue from it.
+//
+// hs_absorb_staged: every block of the stage but the last (it stays open, 1..64 bytes) is
+// compressed into s (in place, shared memory), completed chunks merged into its stack. Returns
+// the offset of the last block; the caller copies it into s->buf and sets s->buf_len.
+__device__ inline uint32_t hs_absorb_staged(HasherState* s, const uint32_t* stage, uint32_t total) {
+  uint32_t off = 0;
+  while (total - off > 64) {
+    uint32_t m[16], o[16];
+    for (int q = 0; q < 16; q++) m[q] = stage[off / 4 + q];
+    if (s->blocks == 15) {
+      compress(s->cv, m, s->chunk_counter, 64, s->flags | b3::CHUNK_END, o);
+      s->chunk_counter++;
+      uint64_t chunks = s->chunk_counter;
+      uint32_t cur[8];
+      for (int i = 0; i < 8; i++) cur[i] = o[i];
+      while ((chunks & 1) == 0 && s->stack_len > 0) {
+        s->stack_len--;
+        parent_cv(s->key, s->flags, s->stack[s->stack_len], cur, cur);
+        chunks >>= 1;
       }
-      s->buf_len = 0;
+      if (s->stack_len < 54) {
+        for (int i = 0; i < 8; i++) s->stack[s->stack_len][i] = cur[i];
+        s->stack_len++;
+      }
+      for (int i = 0; i < 8; i++) s->cv[i] = s->key[i];
+      s->blocks = 0;
+    } else {
+      compress(s->cv, m, s->chunk_counter, 64, s->flags | (s->blocks == 0 ? b3::CHUNK_START : 0), o);
+      for (int i = 0; i < 8; i++) s->cv[i] = o[i];
+      s->blocks++;
     }
-    uint32_t take = 64 - s->buf_len;
-    if (take > len) take = len;
-    for (uint32_t i = 0; i < take; i++) s->buf[s->buf_len + i] = p[i];
-    s->buf_len += take;
-    p += take;
-    len -= take;
+    off += 64;
   }
+  return off;
 }
 
-__device__ inline void hs_absorb_u64(HasherState* s, uint64_t x) {
-  uint8_t b[8];
-  for (int i = 0; i < 8; i++) b[i] = (uint8_t)(x >> (8 * i));
-  hs_absorb(s, b, 8);
+// The root node of a derivation from s: stage = s's open block followed by the derivation's
+// bytes (at most 128 bytes in all, so at most one chunk completes on the way). s is not changed.
+__device__ inline void hs_derive_staged(const HasherState* s, const uint32_t* stage, uint32_t total, XofRoot& r) {
+  uint32_t cv[8], extra[8];
+  for (int i = 0; i < 8; i++) cv[i] = s->cv[i];
+  uint32_t blocks = s->blocks, base_len = s->stack_len < 54 ? s->stack_len : 54;
+  uint64_t chunks = s->chunk_counter;
+  bool has_extra = false;
+  uint32_t off = 0;
+  while (total - off > 64) {
+    uint32_t m[16], o[16];
+    for (int q = 0; q < 16; q++) m[q] = stage[off / 4 + q];
+    if (blocks == 15) {
+      compress(cv, m, chunks, 64, s->flags | b3::CHUNK_END, o);
+      chunks++;
+      uint64_t t = chunks;
+      for (int i = 0; i < 8; i++) extra[i] = o[i];
+      while ((t & 1) == 0 && base_len > 0) {
+        base_len--;
+        parent_cv(s->key, s->flags, s->stack[base_len], extra, extra);
+        t >>= 1;
+      }
+      has_extra = true;
+      for (int i = 0; i < 8; i++) cv[i] = s->key[i];
+      blocks = 0;
+    } else {
+      compress(cv, m, chunks, 64, s->flags | (blocks == 0 ? b3::CHUNK_START : 0), o);
+      for (int i = 0; i < 8; i++) cv[i] = o[i];
+      blocks++;
+    }
+    off += 64;
+  }
+  uint32_t m[16];
+  for (int q = 0; q < 16; q++) m[q] = stage[off / 4 + q];
+  uint32_t block_len = total - off;
+  uint64_t counter = chunks;
+  uint32_t fl = s->flags | b3::CHUNK_END | (blocks == 0 ? b3::CHUNK_START : 0);
+  int entries = (int)base_len + (has_extra ? 1 : 0);
+  for (int e = entries - 1; e >= 0; e--) {
+    uint32_t o[16];
+    compress(cv, m, counter, block_len, fl, o);
+    const uint32_t* left = e >= (int)base_len ? extra : s->stack[e];
+    for (int i = 0; i < 8; i++) {
+      m[i] = left[i];
+      m[8 + i] = o[i];
+      cv[i] = s->key[i];
+    }
+    block_len = 64;
+    counter = 0;
+    fl = s->flags | b3::PARENT;
+  }
+  for (int i = 0; i < 8; i++) r.cv[i] = cv[i];
+  for (int i = 0; i < 16; i++) r.m[i] = m[i];
+  r.block_len = block_len;
+  r.flags = fl;
 }
 
 // The transcript's derive(label) on a base state with derivation counter `counter`.

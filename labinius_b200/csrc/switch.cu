@@ -3,16 +3,21 @@
 //
 // A B128 trace of 2^l words, committed as Witness::lifted, carries a claim in B128 at r_hi; the
 // switch turns it into the F162 claim the commitment opens, at the point its sumcheck ends on.
-// The prover's work is three passes over the trace and a sumcheck of l rounds:
+// The prover's work is two passes over the trace and a sumcheck of l rounds:
 //  * eq_hi = the expansion of r_hi (one B128 product per entry, from two half-size tables);
-//  * the 128 partial evaluations v[k] = sum_j bit_k(trace_j) eq_hi[j];
-//  * a_j = psi(eq_hi[j]) = sum_k bit_k(eq_hi[j]) batch[k] (nibble tables of the batch in shared
-//    memory; psi is linear, so a_j + a_j' = psi(eq_j + eq_j')), p_j = the trace word as an F162;
+//  * a_j = psi(eq_hi[j]) = sum_k bit_k(eq_hi[j]) batch[k], p_j = the trace word t_j as an F162;
 //  * round k sends (sum a0 p0, sum (a0 + a1)(p0 + p1)) over the index pairs (j, j + half) and
-//    folds both tables with its challenge r: x0 + r (x0 + x1). The fold of round k and the
-//    message of round k + 1 are one kernel; products by r go through 4-bit tables of (t x^4i) r
-//    in shared memory; round 0's tables are never stored (a and p are read through eq and the
-//    trace), so the folded tables take n/2 entries.
+//    folds both tables with its challenge r: x0 + r (x0 + x1).
+// The first pass needs no field product per element. The 128 partial evaluations
+// v[k] = sum_j bit_k(t_j) eq_j and round 0's message (sum_k batch[k] P_k, sum_k batch[k] Q_k with
+// P_k = sum_{j < n/2} bit_k(eq_j) t_j and Q_k the same over the pairs' sums) are all read off
+// three 128 x 128 GF(2) matrices sum_j t_j (x) eq_j (bit k of one times bit m of the other), over
+// j >= n/2, over j < n/2, and over the pairs (v is the sum of the first two, P and Q are columns
+// of the last two). They are accumulated by four Russians over groups of 8 rows (k_sw_sums).
+// The second pass is round 0's fold with round 1's message; later rounds fold in place. Every fold and the next message are one kernel; products by r go through 4-bit tables
+// of (t x^4i) r in shared memory, a through nibble tables of the batch (psi is linear, so
+// a_j + a_j' = psi(eq_j + eq_j')); round 0's tables are read through eq and the trace and never
+// stored, so the folded tables take n/2 entries.
 // The transcript runs on the device too: each instance's hasher state absorbs the statement,
 // the partials and every message, and the batch and round challenges are derived from it (one
 // thread per instance), so a whole switch is one pass on a stream with no host round trip. The
@@ -97,12 +102,12 @@ __device__ __forceinline__ F162d ld_word(const uint64_t* __restrict__ w, size_t 
 
 // Entry idx of the expansion of r[0..m): the product over rounds of r_round or 1 + r_round, by
 // bit m-1-round of idx (crates/pcs/src/fields/crossfield.rs:78-98: the last coordinate is bit 0).
-// Block (0, i) also clears instance i's partial and message accumulators and its status.
+// Block (0, i) also clears instance i's matrix and message accumulators and its status.
 __global__ void k_sw_tables(const SwInst* __restrict__ I) {
   const SwInst& s = I[blockIdx.y];
   if (blockIdx.x == 0) {
-    uint64_t* v = &s.s->v[0][0];
-    for (int t = threadIdx.x; t < 256; t += blockDim.x) v[t] = 0;
+    uint32_t* m = &s.s->mat[0][0][0];
+    for (int t = threadIdx.x; t < 3 * 128 * 4; t += blockDim.x) m[t] = 0;
     if (threadIdx.x < 8) s.s->msg[threadIdx.x] = 0;
     if (threadIdx.x == 0) s.s->status = 0;
   }
@@ -133,59 +138,122 @@ __global__ void __launch_bounds__(SW_THREADS) k_sw_eq(const SwInst* __restrict__
     st_b(s.eq, j, b_mul(ld_b(s.e_hi, j >> s.ll), ld_b(s.e_lo, j & lm)));
 }
 
-// v[k] = sum_j bit_k(trace_j) eq[j]: thread (sub, m) of a block adds, for its rows j, eq[j] into
-// the 8 partial sums of bits 8m .. 8m+7; the 16 row groups are then XOR-reduced and added to v.
-constexpr int SW_PARTIAL_ROWS = 128;  // rows per block before the cap
-__global__ void __launch_bounds__(SW_THREADS) k_sw_partials(const SwInst* __restrict__ I, int count) {
-  __shared__ uint64_t red[16][128][2];
-  uint32_t local, nblk;
-  int i = sw_find(I, count, 0, 0, SW_PARTIAL_ROWS, local, nblk);
-  if (i < 0) return;
-  const SwInst& s = I[i];
-  size_t n = 1ull << s.l;
-  const int sub = threadIdx.x >> 4, m = threadIdx.x & 15;
-  uint64_t S[8][2];
-#pragma unroll
-  for (int r = 0; r < 8; r++) S[r][0] = S[r][1] = 0;
-  for (size_t j = (size_t)local * 16 + sub; j < n; j += (size_t)nblk * 16) {
-    uint64_t word = __ldg(s.w + 3 * j + (m >> 3));
-    uint32_t byte = (uint32_t)(word >> (8 * (m & 7))) & 0xFF;
-    B128d e = ld_b(s.eq, j);
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-      uint64_t msk = 0 - (uint64_t)((byte >> r) & 1);
-      S[r][0] ^= e.lo & msk;
-      S[r][1] ^= e.hi & msk;
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < 8; r++) {
-    red[sub][8 * m + r][0] = S[r][0];
-    red[sub][8 * m + r][1] = S[r][1];
-  }
-  __syncthreads();
-  if (threadIdx.x < 128) {
-    uint64_t a = 0, b = 0;
-    for (int q = 0; q < 16; q++) {
-      a ^= red[q][threadIdx.x][0];
-      b ^= red[q][threadIdx.x][1];
-    }
-    unsigned long long* v = reinterpret_cast<unsigned long long*>(&s.s->v[0][0]);
-    atomicXor(v + 2 * threadIdx.x, (unsigned long long)a);
-    atomicXor(v + 2 * threadIdx.x + 1, (unsigned long long)b);
-  }
+// 8 x 8 bit transpose: byte r of x is row r (bit b = column b); on exit byte b holds column b
+// (bit r = row r's bit b). Three delta swaps of 1-, 2- and 4-bit blocks.
+__device__ __forceinline__ uint64_t transpose8(uint64_t x) {
+  uint64_t t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+  x ^= t ^ (t << 7);
+  t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+  x ^= t ^ (t << 14);
+  t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+  x ^= t ^ (t << 28);
+  return x;
 }
 
-__device__ __forceinline__ uint64_t read_u64(dev::Reader& rd) {
-  uint64_t x = 0;
-  for (int b = 0; b < 8; b++) x |= (uint64_t)rd.byte() << (8 * b);
-  return x;
+// One of the three matrices per blockIdx.y, over the pairs (j, j + n/2), j < n/2: kind 0 rows
+// j + n/2 (selector t, value eq), kind 1 rows j, kind 2 the pairs' sums. Row k of a matrix is the
+// XOR of the values of the rows whose selector has bit k set. Four Russians over groups of 8
+// rows: the 128 rows of an iteration are staged in shared memory; thread (g, c) (16 groups of 16
+// threads) builds entry c of its group's two 16-entry tables (XOR combinations of rows 0-3 and
+// 4-7 of the group), gathers byte c of the group's 8 selectors, transposes it (8 x 8 bits) into
+// the 8-row patterns of selector bits 8c .. 8c + 7, and adds two table entries per bit. The block's
+// rows are XOR-reduced in shared memory, then into the instance's matrix.
+constexpr int SW_SUM_ROWS = 2048;  // pairs per block before the cap
+__global__ void __launch_bounds__(SW_THREADS) k_sw_sums(const SwInst* __restrict__ I, int count) {
+  __shared__ uint4 sSel[128], sVal[128];
+  __shared__ uint4 sL[16][16], sH[16][16];
+  __shared__ uint32_t sAcc[128][4];
+  const int kind = blockIdx.y;
+  uint32_t local, nblk;
+  int i = sw_find(I, count, 1, 0, SW_SUM_ROWS, local, nblk);
+  if (i < 0) return;
+  const SwInst& s = I[i];
+  const size_t h = (1ull << s.l) / 2;
+  for (int t = threadIdx.x; t < 128 * 4; t += blockDim.x) (&sAcc[0][0])[t] = 0;
+  const int g = threadIdx.x >> 4, c = threadIdx.x & 15;
+  uint32_t acc[8][4];
+#pragma unroll
+  for (int b = 0; b < 8; b++) acc[b][0] = acc[b][1] = acc[b][2] = acc[b][3] = 0;
+  // staging: thread 2 r + 0 fetches the selector of row r of an iteration, thread 2 r + 1 its
+  // value; the next iteration's are fetched while this one is processed
+  const int r = threadIdx.x >> 1;
+  auto fetch = [&](size_t base, uint64_t& x0, uint64_t& x1) {
+    const size_t j = base + r;
+    x0 = 0, x1 = 0;
+    if (j < h) {
+      const size_t row = kind == 0 ? j + h : j;
+      if (threadIdx.x & 1) {
+        B128d q = ld_b(s.eq, row);
+        if (kind == 2) q = b_add(q, ld_b(s.eq, j + h));
+        x0 = q.lo, x1 = q.hi;
+      } else {
+        x0 = __ldg(s.w + 3 * row), x1 = __ldg(s.w + 3 * row + 1);
+        if (kind == 2) x0 ^= __ldg(s.w + 3 * (j + h)), x1 ^= __ldg(s.w + 3 * (j + h) + 1);
+      }
+    }
+  };
+  const size_t stride = (size_t)nblk * 128;
+  uint64_t n0, n1;
+  fetch((size_t)local * 128, n0, n1);
+  for (size_t base = (size_t)local * 128; base < h; base += stride) {
+    {
+      uint4 v = make_uint4((uint32_t)n0, (uint32_t)(n0 >> 32), (uint32_t)n1, (uint32_t)(n1 >> 32));
+      if (threadIdx.x & 1)
+        sVal[r] = v;
+      else
+        sSel[r] = v;
+    }
+    __syncthreads();
+    if (base + stride < h) fetch(base + stride, n0, n1);
+    {  // entry c of the group's tables
+      uint4 lo = make_uint4(0, 0, 0, 0), hi = make_uint4(0, 0, 0, 0);
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        uint4 x = sVal[8 * g + b], y = sVal[8 * g + 4 + b];
+        uint32_t mk = 0u - (uint32_t)((c >> b) & 1);
+        lo.x ^= x.x & mk, lo.y ^= x.y & mk, lo.z ^= x.z & mk, lo.w ^= x.w & mk;
+        hi.x ^= y.x & mk, hi.y ^= y.y & mk, hi.z ^= y.z & mk, hi.w ^= y.w & mk;
+      }
+      sL[g][c] = lo;
+      sH[g][c] = hi;
+    }
+    __syncwarp();
+    uint64_t x = 0;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      uint4 sel = sSel[8 * g + r];
+      uint32_t w = (c >> 2) == 0 ? sel.x : (c >> 2) == 1 ? sel.y : (c >> 2) == 2 ? sel.z : sel.w;
+      x |= (uint64_t)((w >> (8 * (c & 3))) & 0xFF) << (8 * r);
+    }
+    x = transpose8(x);
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+      const uint32_t idx = (uint32_t)(x >> (8 * b)) & 0xFF;
+      uint4 u = sL[g][idx & 15], v = sH[g][idx >> 4];
+      acc[b][0] ^= u.x ^ v.x;
+      acc[b][1] ^= u.y ^ v.y;
+      acc[b][2] ^= u.z ^ v.z;
+      acc[b][3] ^= u.w ^ v.w;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int b = 0; b < 8; b++)
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (acc[b][q]) atomicXor(&sAcc[8 * c + b][q], acc[b][q]);
+  __syncthreads();
+  uint32_t* m = &s.s->mat[kind][0][0];
+  for (int t = threadIdx.x; t < 128 * 4; t += blockDim.x) {
+    uint32_t val = (&sAcc[0][0])[t];
+    if (val) atomicXor(m + t, val);
+  }
 }
 
 // One block per instance: the claim (if the statement leaves it to the prover: the trace's value
 // at r_hi, sum_k v[k] x^k, crates/pcs/src/switch.rs:116-122), absorb_statement and the partials
-// (crates/pcs/src/switch.rs:124-129, 147-148) staged as one byte string in shared memory and
-// absorbed by thread 0 into the shared copy of the hasher, then the batch coordinates,
+// (crates/pcs/src/switch.rs:124-129, 147-148) staged behind the hasher's open block as one byte
+// string and absorbed into the shared copy of the hasher, then the batch coordinates,
 // sample_f162("labinius/switch-batch", 7) (crates/pcs/src/switch.rs:149,
 // crates/pcs/src/challenge.rs:129-140).
 constexpr int SW_STMT_MAX = 23 + 8 + 16 * 7 + 8 + 16 * 32 + 24 + 8 + 16 * 128;
@@ -194,9 +262,19 @@ __global__ void k_sw_statement(const SwInst* __restrict__ I) {
   SwSmall* sm = s.s;
   __shared__ HasherState sh;
   __shared__ uint64_t v[256], claim[2];
-  __shared__ uint8_t bytes[SW_STMT_MAX];
+  __shared__ uint32_t stage[(64 + SW_STMT_MAX + 63) / 64 * 16];
+  __shared__ uint32_t last;
+  uint8_t* bytes = reinterpret_cast<uint8_t*>(stage);
   dev::hs_copy(&sh, s.st);
-  for (int t = threadIdx.x; t < 256; t += blockDim.x) v[t] = (&sm->v[0][0])[t];
+  // v[k] is row k of the matrices over the rows j + n/2 and j < n/2 (bit m of word m / 32)
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) {
+    const uint32_t* hi = sm->mat[0][t >> 1];
+    const uint32_t* lo = sm->mat[1][t >> 1];
+    const int o = 2 * (t & 1);
+    uint64_t x = (uint64_t)(hi[o] ^ lo[o]) | ((uint64_t)(hi[o + 1] ^ lo[o + 1]) << 32);
+    v[t] = x;
+    (&sm->v[0][0])[t] = x;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     B128d acc{sm->claim[0], sm->claim[1]};
@@ -210,20 +288,23 @@ __global__ void k_sw_statement(const SwInst* __restrict__ I) {
     claim[1] = acc.hi;
   }
   __syncthreads();
-  // the byte string: le64(15) "labinius/switch", le64(nlo) r_lo, le64(l) r_hi, le64(1) claim,
+  // the open block, then le64(15) "labinius/switch", le64(nlo) r_lo, le64(l) r_hi, le64(1) claim,
   // le64(128) partials
-  const uint32_t o_lo = 31, o_hi = o_lo + 16 * s.nlo + 8, o_claim = o_hi + 16 * s.l + 8, o_v = o_claim + 24,
-                 total = o_v + 16 * 128;
-  for (uint32_t b = threadIdx.x; b < total; b += blockDim.x) {
-    uint64_t word;
-    uint32_t at;
-    if (b < 8) {
-      word = 15, at = b;
-    } else if (b < 23) {
-      bytes[b] = (uint8_t)c_sw_label[b - 8];
+  const uint32_t bl = sh.buf_len, o_lo = bl + 31, o_hi = o_lo + 16 * s.nlo + 8, o_claim = o_hi + 16 * s.l + 8,
+                 o_v = o_claim + 24, total = o_v + 16 * 128, padded = (total + 63) / 64 * 64;
+  for (uint32_t b = threadIdx.x; b < padded; b += blockDim.x) {
+    uint64_t word = 0;
+    uint32_t at = 0;
+    if (b < bl) {
+      bytes[b] = sh.buf[b];
+      continue;
+    } else if (b < bl + 8) {
+      word = 15, at = b - bl;
+    } else if (b < bl + 23) {
+      bytes[b] = (uint8_t)c_sw_label[b - bl - 8];
       continue;
     } else if (b < o_lo) {
-      word = s.nlo, at = b - 23;
+      word = s.nlo, at = b - (bl + 23);
     } else if (b < o_hi - 8) {
       word = s.r_lo[(b - o_lo) / 8], at = (b - o_lo) % 8;
     } else if (b < o_hi) {
@@ -236,20 +317,36 @@ __global__ void k_sw_statement(const SwInst* __restrict__ I) {
       word = claim[(b - o_claim) / 8], at = (b - o_claim) % 8;
     } else if (b < o_v) {
       word = 128, at = b - (o_v - 8);
-    } else {
+    } else if (b < total) {
       word = v[(b - o_v) / 8], at = (b - o_v) % 8;
     }
     bytes[b] = (uint8_t)(word >> (8 * at));
   }
   __syncthreads();
+  if (threadIdx.x == 0) last = dev::hs_absorb_staged(&sh, stage, total);
+  __syncthreads();
+  const uint32_t nbl = total - last;
+  for (uint32_t b = threadIdx.x; b < nbl; b += blockDim.x) sh.buf[b] = bytes[last + b];
+  __syncthreads();
+  // derive("labinius/switch-batch"): the open block, le64(counter), le64(21), the label
+  const uint32_t dtotal = nbl + 37;
+  for (uint32_t b = threadIdx.x; b < 128; b += blockDim.x) {
+    uint32_t x = 0;
+    if (b < nbl) x = sh.buf[b];
+    else if (b < nbl + 8) x = (uint32_t)(s.counter0 >> (8 * (b - nbl))) & 0xFF;
+    else if (b < nbl + 16) x = b == nbl + 8 ? 21 : 0;
+    else if (b < dtotal) x = (uint8_t)c_sw_batch[b - nbl - 16];
+    bytes[b] = (uint8_t)x;
+  }
+  if (threadIdx.x == 0) sh.buf_len = nbl;
+  __syncthreads();
   if (threadIdx.x == 0) {
-    dev::hs_absorb(&sh, bytes, total);
     XofRoot root;
-    dev::derive_root(&sh, s.counter0, c_sw_batch, 21, root);
-    dev::Reader rd;
-    rd.init(root);
+    dev::hs_derive_staged(&sh, stage, dtotal, root);
+    uint32_t out[48];
+    for (int t = 0; t < 3; t++) dev::root_block(root, t, out + 16 * t);
     for (int c = 0; c < 7; c++) {
-      for (int w = 0; w < 3; w++) sm->rp[c][w] = read_u64(rd);
+      for (int w = 0; w < 3; w++) sm->rp[c][w] = (uint64_t)out[6 * c + 2 * w] | ((uint64_t)out[6 * c + 2 * w + 1] << 32);
       sm->rp[c][2] &= (1ull << 34) - 1;
     }
   }
@@ -258,10 +355,15 @@ __global__ void k_sw_statement(const SwInst* __restrict__ I) {
 }
 
 // batch = the expansion of the 7 sampled F162 (crossfield.rs:65-76); psi[16 c + t] = the XOR of
-// batch[4c + b] over the set bits b of t (crossfield.rs:112-130). One block per instance.
-__global__ void k_sw_batch(const SwInst* __restrict__ I) {
+// batch[4c + b] over the set bits b of t (crossfield.rs:112-130); and round 0's message,
+// e0 = sum_k batch[k] P_k and einf = sum_k batch[k] Q_k, where P_k (bit m) is entry (m, k) of the
+// matrix over j < n/2 and Q_k of the matrix over the pairs. One block of 256 threads per instance.
+__global__ void __launch_bounds__(256) k_sw_batch(const SwInst* __restrict__ I) {
   const SwInst& s = I[blockIdx.x];
   __shared__ F162d t[2][128];
+  __shared__ uint32_t mpq[2][128][4];
+  __shared__ uint64_t red[8][6];
+  for (int e = threadIdx.x; e < 2 * 128 * 4; e += blockDim.x) (&mpq[0][0][0])[e] = (&s.s->mat[1][0][0])[e];
   if (threadIdx.x == 0) t[0][0] = F162d{{1, 0, 0}};
   __syncthreads();
   int cur = 0;
@@ -282,6 +384,23 @@ __global__ void k_sw_batch(const SwInst* __restrict__ I) {
     for (int b = 0; b < 4; b++)
       if ((v >> b) & 1) acc = f_add(acc, t[cur][4 * c + b]);
     st_f(&s.s->psi[0][0], e, acc);
+  }
+  // thread k < 128: P_k, thread 128 + k: Q_k, times batch[k]
+  const int k = threadIdx.x & 127, which = threadIdx.x >> 7;
+  uint64_t col[2] = {0, 0};
+  for (int m = 0; m < 128; m++) col[m >> 6] |= (uint64_t)((mpq[which][m][k >> 5] >> (k & 31)) & 1u) << (m & 63);
+  F162d prod = f_mul(t[cur][k], F162d{{col[0], col[1], 0}});
+  for (int o = 16; o > 0; o >>= 1)
+    for (int q = 0; q < 3; q++) prod.w[q] ^= __shfl_xor_sync(0xffffffffu, prod.w[q], o);
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+    for (int q = 0; q < 3; q++) red[warp][q] = prod.w[q];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int half = threadIdx.x / 3, q = threadIdx.x % 3;
+    uint64_t x = 0;
+    for (int w = 0; w < 4; w++) x ^= red[4 * half + w][q];
+    s.s->msg[3 * half + q] = x;
   }
 }
 
@@ -328,56 +447,62 @@ __device__ __forceinline__ void xor_reduce_store(F162d e0, F162d ei, uint64_t* m
   }
 }
 
-// Round 0's message over the pairs (j, j + n/2): a0 = psi(eq_j), a0 + a1 = psi(eq_j + eq_j+n/2).
-__global__ void __launch_bounds__(SW_THREADS) k_sw_init(const SwInst* __restrict__ I, int count) {
-  __shared__ F162d psi[512];
-  uint32_t local, nblk;
-  int i = sw_find(I, count, 1, 0, SW_THREADS, local, nblk);
-  if (i < 0) return;
-  const SwInst& s = I[i];
-  load_table(psi, &s.s->psi[0][0], 512);
-  __syncthreads();
-  const size_t h = (1ull << s.l) / 2;
-  F162d e0{{0, 0, 0}}, ei{{0, 0, 0}};
-  for (size_t j = (size_t)local * SW_THREADS + threadIdx.x; j < h; j += (size_t)nblk * SW_THREADS) {
-    B128d q0 = ld_b(s.eq, j), q1 = ld_b(s.eq, j + h);
-    F162d a0 = psi_of(psi, q0), ad = psi_of(psi, b_add(q0, q1));
-    F162d p0 = ld_word(s.w, j), p1 = ld_word(s.w, j + h);
-    e0 = f_add(e0, f_mul(a0, p0));
-    ei = f_add(ei, f_mul(ad, f_add(p0, p1)));
-  }
-  xor_reduce_store(e0, ei, &s.s->msg[0]);
-}
-
-// One block per instance whose round k is due: the round's message into the transcript (thread 0
-// on the shared copy of the hasher), sample_f162("labinius/switch-round", 1)
-// (crates/pcs/src/switch.rs:152-159), the message accumulators cleared, and the tables of
-// (t x^{4i}) r for the fold.
+// One block per instance whose round k is due: the round's message into the transcript and
+// sample_f162("labinius/switch-round", 1) (crates/pcs/src/switch.rs:152-159), both staged behind
+// the shared hasher's open block; the message accumulators cleared; the tables of (t x^{4i}) r
+// for the fold.
 __global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
   const SwInst& s = I[blockIdx.x];
   if ((uint32_t)k >= s.l) return;
   SwSmall* sm = s.s;
   __shared__ HasherState sh;
   __shared__ F162d R4[41];
-  __shared__ uint8_t mb[56];
+  __shared__ uint64_t msg[6];
+  __shared__ uint32_t stage[32];
+  __shared__ uint32_t last;
+  uint8_t* bytes = reinterpret_cast<uint8_t*>(stage);
   dev::hs_copy(&sh, s.st);
+  if (threadIdx.x < 6) msg[threadIdx.x] = sm->msg[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    sm->rounds[k][threadIdx.x] = msg[threadIdx.x];
+    sm->msg[threadIdx.x] = 0;
+  }
+  // absorb_f162(&msg): the open block, le64(2), the six words
+  const uint32_t bl = sh.buf_len, total = bl + 56;
+  for (uint32_t b = threadIdx.x; b < 128; b += blockDim.x) {
+    uint32_t x = 0;
+    if (b < bl) x = sh.buf[b];
+    else if (b < bl + 8) x = b == bl ? 2 : 0;
+    else if (b < total) x = (uint32_t)(msg[(b - bl - 8) / 8] >> (8 * ((b - bl) % 8))) & 0xFF;
+    bytes[b] = (uint8_t)x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) last = dev::hs_absorb_staged(&sh, stage, total);
+  __syncthreads();
+  const uint32_t nbl = total - last;
+  for (uint32_t b = threadIdx.x; b < nbl; b += blockDim.x) sh.buf[b] = bytes[last + b];
+  __syncthreads();
+  // derive("labinius/switch-round"): the open block, le64(counter), le64(21), the label
+  const uint64_t counter = s.counter0 + 1 + (uint64_t)k;
+  const uint32_t dtotal = nbl + 37;
+  for (uint32_t b = threadIdx.x; b < 128; b += blockDim.x) {
+    uint32_t x = 0;
+    if (b < nbl) x = sh.buf[b];
+    else if (b < nbl + 8) x = (uint32_t)(counter >> (8 * (b - nbl))) & 0xFF;
+    else if (b < nbl + 16) x = b == nbl + 8 ? 21 : 0;
+    else if (b < dtotal) x = (uint8_t)c_sw_round[b - nbl - 16];
+    bytes[b] = (uint8_t)x;
+  }
+  if (threadIdx.x == 0) sh.buf_len = nbl;
   __syncthreads();
   if (threadIdx.x == 0) {
-    uint64_t msg[6];
-    for (int q = 0; q < 6; q++) {
-      msg[q] = sm->msg[q];
-      sm->rounds[k][q] = msg[q];
-      sm->msg[q] = 0;
-    }
-    // absorb_f162(&msg): le64(2), then the six words
-    for (int b = 0; b < 56; b++) mb[b] = (uint8_t)((b < 8 ? 2ull : msg[(b - 8) / 8]) >> (8 * (b % 8)));
-    dev::hs_absorb(&sh, mb, 56);
     XofRoot root;
-    dev::derive_root(&sh, s.counter0 + 1 + (uint64_t)k, c_sw_round, 21, root);
-    dev::Reader rd;
-    rd.init(root);
+    dev::hs_derive_staged(&sh, stage, dtotal, root);
+    uint32_t out[16];
+    dev::root_block(root, 0, out);
     F162d r;
-    for (int w = 0; w < 3; w++) r.w[w] = read_u64(rd);
+    for (int w = 0; w < 3; w++) r.w[w] = (uint64_t)out[2 * w] | ((uint64_t)out[2 * w + 1] << 32);
     r.w[2] &= (1ull << 34) - 1;
     st_f(&sm->rr[0][0], k, r);
     for (int q = 0; q < 41; q++) {
@@ -510,10 +635,9 @@ cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStre
   };
   k_sw_tables<<<dim3((tabmax + 127) / 128, count), 128, 0, st>>>(d);
   k_sw_eq<<<blocks(0, 0, SW_THREADS), SW_THREADS, 0, st>>>(d, count);
-  k_sw_partials<<<blocks(0, 0, SW_PARTIAL_ROWS), SW_THREADS, 0, st>>>(d, count);
+  k_sw_sums<<<dim3(blocks(1, 0, SW_SUM_ROWS), 3), SW_THREADS, 0, st>>>(d, count);
   k_sw_statement<<<count, 128, 0, st>>>(d);
   k_sw_batch<<<count, 256, 0, st>>>(d);
-  k_sw_init<<<blocks(1, 0, SW_THREADS), SW_THREADS, 0, st>>>(d, count);
   for (uint32_t k = 0; k < lmax; k++) {
     k_sw_step<<<count, 128, 0, st>>>(d, (int)k);
     unsigned g = blocks(2, (int)k, SW_THREADS);
@@ -523,7 +647,7 @@ cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStre
       k_sw_fold<false><<<g, SW_THREADS, 0, st>>>(d, count, (int)k);
   }
   k_sw_finish<<<(count + 31) / 32, 32, 0, st>>>(d, count);
-  if (launches) *launches += 7 + 2 * (uint64_t)lmax;
+  if (launches) *launches += sw_launches(lmax);
   return cudaGetLastError();
 }
 

@@ -12,7 +12,11 @@ namespace lbg {
 
 // The small per-instance values of a switch: one device block per instance.
 struct SwSmall {
-  uint64_t v[128][2];         // the partial evaluations (XOR accumulators of the partials pass)
+  // the pass over the trace: three 128 x 128 GF(2) matrices, row k as 4 words (bit m of word
+  // m / 32): sum_j bit_k(t_j) bit_m(eq_j) over j >= n/2, over j < n/2, and over the pairs
+  // (j, j + n/2) with t_j + t_j+n/2 and eq_j + eq_j+n/2
+  uint32_t mat[3][128][4];
+  uint64_t v[128][2];         // the partial evaluations
   uint64_t msg[8];            // the running round's message (e0, einf): XOR accumulators
   uint64_t claim[2];          // the B128 claim: given, or the trace's value at r_hi
   uint64_t rp[8][3];          // the 7 batch coordinates
@@ -58,6 +62,9 @@ void sw_layout(SwInst& inst, uint8_t* base);
 // fold; the opened value and the evaluation point. Launches are counted into *launches.
 cudaError_t enqueue_switch(const SwInst* d_inst, const SwInst* h_inst, int count, cudaStream_t st,
                            uint64_t* launches);
+
+// Launches of enqueue_switch when the longest instance has lmax variables.
+inline uint64_t sw_launches(uint32_t lmax) { return 6 + 2 * (uint64_t)lmax; }
 
 // Transcript bytes a word-level (nlo = 0) or bit-level (nlo = 7) switch over l variables absorbs.
 inline uint64_t sw_transcript_bytes(uint32_t l, uint32_t nlo) {
