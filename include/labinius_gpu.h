@@ -148,10 +148,20 @@ int lbg_verify_evaluation(const lbg_pp* pp, const uint64_t* p1, size_t p1_len, c
  * *accepted = 1 when v (int16 [len_ring][648]) is centred within the base modulus with its squared
  * norm within Params::fold_cap, A v equals the folded commitment (int16 [4][limbs][162]) on every
  * limb, and eq(p0) . (v mod 2) equals the folded row value; else 0. Bit-dropped parameters return
- * LBG_ERR_UNSUPPORTED. */
+ * LBG_ERR_INVALID (their check is lbg_verify_folded_opening_bd). */
 int lbg_verify_folded_opening(const lbg_pp* pp, const int16_t* folded_commitment, const int16_t* v,
                               const uint64_t* p0, size_t p0_len, const uint64_t folded_row_value[3],
                               int* accepted);
+/* Verifier::verify_opening, bit-dropped arm (crates/pcs/src/scheme/verifier.rs:232-276): the same
+ * norm and binary checks, and the residual of crates/pcs/src/bd/residual.rs:66-130 (the columns
+ * rebuilt from the dropped commitment's top (uint16 [columns*648]) and digits (uint16
+ * [limbs-1][columns*648]), folded with the r challenges, subtracted from A v, recombined across the
+ * limbs) within bd::cap (crates/pcs/src/bd/mod.rs:72-75). residual_out (may be null): its squared
+ * norm, 128 bits, low word first. */
+int lbg_verify_folded_opening_bd(const lbg_pp* pp, const uint16_t* top, const uint16_t* digits,
+                                 const lbg_challenge* challenges, size_t r, const int16_t* v, const uint64_t* p0,
+                                 size_t p0_len, const uint64_t folded_row_value[3], int* accepted,
+                                 uint64_t residual_out[2]);
 
 /* switch::prove / prove_bits (crates/pcs/src/switch.rs:64-98, 133-168), the cross-field switch
  * prover: the trace is the B128 words of the witness w (limbs 0 and 1 of each F162, as

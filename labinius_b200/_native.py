@@ -96,6 +96,7 @@ SIGNATURES = {
     "lbg_batch_fold": (_int, [_vp, _vp, _sz, _vp]),
     "lbg_batch_round": (_int, [_vp, _vp, _sz, _vp]),
     "lbg_batch_set_switch": (_int, [_vp, _vp, _vp, _vp]),
+    "lbg_verify_folded_opening_bd": (_int, [_vp, _vp, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _vp, _vp]),
     "lbg_batch_switch_outputs": (_int, [_vp, _vp, _vp, _vp, _vp]),
     "lbg_prover_set_kept_transform": (_int, [_vp, _int]),
     "lbg_batch_set_kept_transform": (_int, [_vp, _int]),

@@ -833,7 +833,8 @@ int lbg_verify_folded_opening(const lbg_pp* pp_c, const int16_t* folded_commitme
     return fail(LBG_ERR_INVALID, "null argument");
   lbg_pp* pp = const_cast<lbg_pp*>(pp_c);
   *accepted = 0;
-  if (pp->params.opening != LBG_OPENING_CLEAR) return fail(LBG_ERR_UNSUPPORTED, "the bit-dropped opening check is not on the device");
+  if (pp->params.opening != LBG_OPENING_CLEAR)
+    return fail(LBG_ERR_INVALID, "bit-dropped parameters: the check is lbg_verify_folded_opening_bd");
   if (4 * pp->len_ring != ((size_t)1 << p0_len) || p0_len != (size_t)(pp->params.witness_log_len - pp->params.column_log_len))
     return LBG_OK;  // Rejected, as binary_check's length test
   std::lock_guard<std::mutex> g(pp->mu);
@@ -881,6 +882,100 @@ int lbg_verify_folded_opening(const lbg_pp* pp_c, const int16_t* folded_commitme
   double cap = std::ceil(108.0 * (double)(pp->n / 4 * N648));  // recursion::FOLD_CAP * (witness_len / 4) * N
   bool ok = !f.wrapped && f.worst <= half && (double)f.normsq <= cap && !f.mismatch && ub[0] == folded_row_value[0] &&
             ub[1] == folded_row_value[1] && ub[2] == folded_row_value[2];
+  *accepted = ok ? 1 : 0;
+  return LBG_OK;
+}
+
+// Verifier::verify_opening, bit-dropped arm (crates/pcs/src/scheme/verifier.rs:232-276): the norm
+// checks of the Clear arm, the bit-dropped residual (crates/pcs/src/bd/residual.rs:66-130) against
+// bd_cap (crates/pcs/src/bd/mod.rs:72-75), and the binary check.
+int lbg_verify_folded_opening_bd(const lbg_pp* pp_c, const uint16_t* top, const uint16_t* digits,
+                                 const lbg_challenge* challenges, size_t r, const int16_t* v, const uint64_t* p0,
+                                 size_t p0_len, const uint64_t folded_row_value[3], int* accepted,
+                                 uint64_t residual_out[2]) {
+  if (!pp_c || !top || !challenges || !v || !p0 || !folded_row_value || !accepted)
+    return fail(LBG_ERR_INVALID, "null argument");
+  lbg_pp* pp = const_cast<lbg_pp*>(pp_c);
+  *accepted = 0;
+  if (pp->params.opening != LBG_OPENING_BIT_DROPPED) return fail(LBG_ERR_INVALID, "the parameters are not bit-dropped");
+  int L = pp->limbs;
+  if (L > 1 && !digits) return fail(LBG_ERR_INVALID, "null argument");
+  if (r != pp->cols) return LBG_OK;  // Rejected: the residual's shape test
+  if (4 * pp->len_ring != ((size_t)1 << p0_len) || p0_len != (size_t)(pp->params.witness_log_len - pp->params.column_log_len))
+    return LBG_OK;  // Rejected, as binary_check's length test
+  std::lock_guard<std::mutex> g(pp->mu);
+  LBG_CU(cudaSetDevice(pp->device));
+  cudaStream_t st = pp->stream;
+  size_t Lr = pp->len_ring, nv = Lr * N648, count = pp->cols * N648;
+  int16_t* d_v = nullptr;
+  uint16_t* d_top = nullptr;
+  uint16_t* d_digits = nullptr;
+  uint32_t *d_vhat = nullptr, *d_diff = nullptr, *d_res = nullptr;
+  uint64_t* d_bits = nullptr;
+  unsigned long long* d_ns = nullptr;
+  VerifyFlags* d_f = nullptr;
+  auto release = [&]() {
+    void* ptrs[] = {d_v, d_top, d_digits, d_vhat, d_diff, d_res, d_bits, d_ns, d_f};
+    for (void* q : ptrs) cudaFree(q);
+  };
+  if (cudaMalloc((void**)&d_v, nv * 2) != cudaSuccess || cudaMalloc((void**)&d_top, count * 2) != cudaSuccess ||
+      cudaMalloc((void**)&d_digits, (size_t)(L > 1 ? L - 1 : 1) * count * 2) != cudaSuccess ||
+      cudaMalloc((void**)&d_vhat, nv * 4) != cudaSuccess || cudaMalloc((void**)&d_diff, 4 * N162 * 4) != cudaSuccess ||
+      cudaMalloc((void**)&d_res, (size_t)L * N648 * 4) != cudaSuccess || cudaMalloc((void**)&d_bits, 4 * Lr * 24) != cudaSuccess ||
+      cudaMalloc((void**)&d_ns, 16) != cudaSuccess || cudaMalloc((void**)&d_f, sizeof(VerifyFlags)) != cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return fail(LBG_ERR_OOM, "verifier: device allocation failed");
+  }
+  GarnerConsts gc;
+  std::memset(&gc, 0, sizeof(gc));
+  for (int k = 0; k < L; k++) {
+    gc.q[k] = pp->primes[k];
+    for (int m = 0; m < k; m++) gc.inv[k][m] = (uint32_t)inv_mod(pp->primes[m], pp->primes[k]);
+  }
+  gc.dropped_bits = pp->params.dropped_bits;
+  cudaError_t e = cudaMemcpyAsync(d_v, v, nv * 2, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_top, top, count * 2, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && L > 1)
+    e = cudaMemcpyAsync(d_digits, digits, (size_t)(L - 1) * count * 2, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(pp->d_ch, challenges, r * sizeof(lbg_challenge), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_f, 0, sizeof(VerifyFlags), st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(pp->d_p, p0, p0_len * 24, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_v_norm(d_v, Lr, d_f, st);
+  for (int k = 0; k < L && e == cudaSuccess; k++)
+    e = launch_bd_columns(pp->pidx[k], d_top, d_digits, (int)pp->cols, k, gc, L, pp->d_prime[k], pp->d_C, st);
+  for (int k = 0; k < L && e == cudaSuccess; k++) {
+    e = launch_challenge_slots(pp->pidx[k], pp->d_ch, (int)r, pp->d_prime[k], pp->d_chat, st);
+    if (e == cudaSuccess)
+      e = launch_fold_commitment(pp->pidx[k], pp->d_C, (int)pp->cols, k, L, pp->d_chat, pp->d_prime[k], pp->d_fc, st);
+  }
+  for (int k = 0; k < L && e == cudaSuccess; k++) {
+    e = launch_v_limb(pp->pidx[k], d_v, Lr, pp->d_prime[k], d_vhat, pp->d_Ahat + (size_t)k * Lr * N162 * 2, k, L,
+                      pp->d_fc, d_f, st, d_diff);
+    if (e == cudaSuccess) e = launch_bd_inverse(pp->pidx[k], d_diff, pp->d_prime[k], d_res + (size_t)k * N648, st);
+  }
+  if (e == cudaSuccess) e = launch_bd_normsq(d_res, L, gc, d_ns, st);
+  if (e == cudaSuccess) e = launch_v_parity(d_v, Lr, d_bits, st);
+  if (e == cudaSuccess) e = launch_eq_table(pp->d_p, (int)p0_len, 4 * Lr, pp->d_eq, st);
+  if (e == cudaSuccess) e = launch_row_eval(d_bits, 4 * Lr, 1, pp->d_eq, pp->d_out, st);
+  VerifyFlags f;
+  uint64_t ub[3], ns[2];
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&f, d_f, sizeof(f), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ub, pp->d_out, 24, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ns, d_ns, 16, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  release();
+  if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("verify: ") + cudaGetErrorString(e));
+  if (residual_out) {
+    residual_out[0] = ns[0];
+    residual_out[1] = ns[1];
+  }
+  int half = (int)(pp->primes[0] - 1) / 2;
+  double cap = std::ceil(108.0 * (double)(pp->n / 4 * N648));  // recursion::FOLD_CAP * (witness_len / 4) * N
+  double spread = (double)((1ull << (2 * pp->params.dropped_bits)) - 1) / 12.0;
+  uint64_t bd_cap = (uint64_t)std::ceil(4.0 * (double)(N648 * pp->cols * 28) * spread);  // bd::cap
+  bool ok = !f.wrapped && f.worst <= half && (double)f.normsq <= cap && ns[1] == 0 && ns[0] <= bd_cap &&
+            ub[0] == folded_row_value[0] && ub[1] == folded_row_value[1] && ub[2] == folded_row_value[2];
   *accepted = ok ? 1 : 0;
   return LBG_OK;
 }

@@ -537,6 +537,79 @@ __global__ void k_garner(const uint16_t* __restrict__ res, size_t count, int lim
   }
 }
 
+// The bit-dropped residual (crates/pcs/src/bd/residual.rs:66-130) on the device.
+// k_bd_columns: the columns rebuilt from the top bits and the Garner digits modulo limb `limb`
+// ((top << dropped_bits) + q_0 (d_1 + q_1 (d_2 + ...)), crates/pcs/src/simd/bd.rs:5-36), in the
+// commitment's component form: component d of column j is the forward 162-point transform of
+// coefficients 4m + d, written at C[j][d][limb][slot] centred (the inverse of k_column_residues).
+template <int PI>
+__global__ void k_bd_columns(const uint16_t* __restrict__ top, const uint16_t* __restrict__ digits, int cols, int limb,
+                             GarnerConsts g, int limbs, const DevPrime* __restrict__ D, int16_t* __restrict__ C) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= cols * 4) return;
+  int j = gid / 4, d = gid % 4;
+  constexpr uint32_t q = Pr<PI>::q;
+  const size_t count = (size_t)cols * N648;
+  uint32_t x[N162];
+  for (int m = 0; m < N162; m++) {
+    const size_t at = (size_t)j * N648 + 4 * m + d;
+    uint32_t inner = 0;
+    if (limbs > 1) {
+      inner = digits[(size_t)(limbs - 2) * count + at] % q;
+      for (int k = limbs - 3; k >= 0; k--) inner = (digits[(size_t)k * count + at] + inner * g.q[k + 1]) % q;
+    }
+    x[m] = (uint32_t)((((uint64_t)top[at] << g.dropped_bits) + (uint64_t)inner * g.q[0]) % q);
+  }
+  ntt162_serial<PI>(x, *D);
+  for (int s = 0; s < N162; s++) C[(((size_t)j * 4 + d) * limbs + limb) * N162 + s] = center<PI>(x[D->pow3_to_leaf[s]]);
+}
+
+// k_bd_inverse: A v - the folded commitment for one limb, diff[row][leaf], back to the 648
+// coefficients (row d holds coefficients 4m + d), modulo the limb.
+template <int PI>
+__global__ void k_bd_inverse(const uint32_t* __restrict__ diff, const DevPrime* __restrict__ D, uint32_t* __restrict__ res) {
+  const int d = threadIdx.x;
+  if (d >= 4) return;
+  uint32_t x[N162];
+  for (int leaf = 0; leaf < N162; leaf++) x[leaf] = diff[d * N162 + leaf];
+  intt162_serial<PI>(x, *D);
+  for (int m = 0; m < N162; m++) res[4 * m + d] = x[m];
+}
+
+// k_bd_normsq: the Garner recombination of the limbs' residues res[limb][648] and the squared norm
+// of the centred integers (crates/pcs/src/bd/digits.rs:229-260), one CTA, out = the 128-bit sum
+// as two words, low first.
+__global__ void k_bd_normsq(const uint32_t* __restrict__ res, int limbs, GarnerConsts g, unsigned long long* out) {
+  __shared__ unsigned __int128 red[1024];
+  const int i = threadIdx.x;
+  unsigned __int128 sq = 0;
+  if (i < N648) {
+    uint64_t mixed[7];
+    unsigned __int128 modulus = 1;
+    for (int k = 0; k < limbs; k++) {
+      const uint64_t q = g.q[k];
+      uint64_t x = res[(size_t)k * N648 + i] % q;
+      for (int m = 0; m < k; m++) x = (x + q - mixed[m] % q) % q * g.inv[k][m] % q;
+      mixed[k] = x;
+      modulus *= q;
+    }
+    unsigned __int128 value = 0;
+    for (int k = limbs - 1; k >= 0; k--) value = value * g.q[k] + mixed[k];
+    unsigned __int128 mag = value > modulus / 2 ? modulus - value : value;
+    sq = mag * mag;
+  }
+  red[i] = sq;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (i < o) red[i] += red[i + o];
+    __syncthreads();
+  }
+  if (i == 0) {
+    out[0] = (unsigned long long)red[0];
+    out[1] = (unsigned long long)(red[0] >> 64);
+  }
+}
+
 // =============================================================================================
 // Row evaluation over F162 (crates/pcs/src/eval.rs:51-63, 171-193)
 // =============================================================================================
@@ -1029,12 +1102,13 @@ __global__ void k_v_transform(const int16_t* __restrict__ v, size_t len_ring, co
 }
 
 // A v at one leaf (one CTA per leaf): Y_k'(leaf) = sum_i the module product of the key's
-// components with v's (the commit's algebra), compared with the folded commitment's slot.
+// components with v's (the commit's algebra), compared with the folded commitment's slot; with
+// `diff`, Y - fc modulo q is written to diff[row][leaf] instead.
 template <int PI>
 __global__ void __launch_bounds__(256) k_v_mac(const uint32_t* __restrict__ vhat, size_t len_ring,
                                                const int4* __restrict__ Ahat, const DevPrime* __restrict__ D,
                                                int limb, int limbs, const int16_t* __restrict__ fc,
-                                               VerifyFlags* __restrict__ f) {
+                                               VerifyFlags* __restrict__ f, uint32_t* __restrict__ diff) {
   const int leaf = blockIdx.x;
   long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
   for (size_t i = threadIdx.x; i < len_ring; i += blockDim.x) {
@@ -1069,7 +1143,11 @@ __global__ void __launch_bounds__(256) k_v_mac(const uint32_t* __restrict__ vhat
       for (int w = 0; w < (int)(blockDim.x >> 5); w++) y += red[row][w];
       y %= q;
       if (y < 0) y += q;
-      if (center<PI>((uint32_t)y) != fc[(row * limbs + limb) * N162 + s]) atomicOr(&f->mismatch, 1);
+      const int16_t c = fc[(row * limbs + limb) * N162 + s];
+      if (diff)
+        diff[row * N162 + leaf] = (uint32_t)((y + q - (c < 0 ? c + q : c)) % q);
+      else if (center<PI>((uint32_t)y) != c)
+        atomicOr(&f->mismatch, 1);
     }
   }
 }
@@ -1462,11 +1540,30 @@ cudaError_t launch_v_norm(const int16_t* v, size_t len_ring, VerifyFlags* f, cud
 }
 
 cudaError_t launch_v_limb(int pi, const int16_t* v, size_t len_ring, const DevPrime* D, uint32_t* vhat,
-                          const int4* Ahat, int limb, int limbs, const int16_t* fc, VerifyFlags* f, cudaStream_t st) {
+                          const int4* Ahat, int limb, int limbs, const int16_t* fc, VerifyFlags* f, cudaStream_t st,
+                          uint32_t* diff) {
   LBG_DISPATCH(pi, (k_v_transform<P><<<blocks_for(len_ring * 4, 64), 64, 0, st>>>(v, len_ring, D, vhat)));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  LBG_DISPATCH(pi, (k_v_mac<P><<<N162, 256, 0, st>>>(vhat, len_ring, Ahat, D, limb, limbs, fc, f)));
+  LBG_DISPATCH(pi, (k_v_mac<P><<<N162, 256, 0, st>>>(vhat, len_ring, Ahat, D, limb, limbs, fc, f, diff)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bd_columns(int pi, const uint16_t* top, const uint16_t* digits, int cols, int limb,
+                              const GarnerConsts& g, int limbs, const DevPrime* D, int16_t* C, cudaStream_t st) {
+  LBG_DISPATCH(pi, (k_bd_columns<P><<<blocks_for((size_t)cols * 4, 64), 64, 0, st>>>(top, digits, cols, limb, g,
+                                                                                      limbs, D, C)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bd_inverse(int pi, const uint32_t* diff, const DevPrime* D, uint32_t* res, cudaStream_t st) {
+  LBG_DISPATCH(pi, (k_bd_inverse<P><<<1, 4, 0, st>>>(diff, D, res)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bd_normsq(const uint32_t* res, int limbs, const GarnerConsts& g, unsigned long long* out,
+                             cudaStream_t st) {
+  k_bd_normsq<<<1, 1024, 0, st>>>(res, limbs, g, out);
   return cudaGetLastError();
 }
 

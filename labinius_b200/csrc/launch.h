@@ -90,7 +90,17 @@ struct VerifyFlags {
 cudaError_t launch_v_norm(const int16_t* v, size_t len_ring, VerifyFlags* f, cudaStream_t st);
 // A v modulo one limb against the folded commitment [4][limbs][162]; vhat: len_ring * 648 u32.
 cudaError_t launch_v_limb(int pi, const int16_t* v, size_t len_ring, const DevPrime* D, uint32_t* vhat,
-                          const int4* Ahat, int limb, int limbs, const int16_t* fc, VerifyFlags* f, cudaStream_t st);
+                          const int4* Ahat, int limb, int limbs, const int16_t* fc, VerifyFlags* f, cudaStream_t st,
+                          uint32_t* diff = nullptr);
+// The bit-dropped residual (crates/pcs/src/bd/residual.rs:66-130): the columns rebuilt from top
+// and digits in the commitment's component form C [cols][4][limbs][162] (limb `limb`); A v minus
+// the folded commitment (launch_v_limb with diff [4][162]) back to coefficients res [648]; the
+// Garner recombination of res [limbs][648] and its squared norm (128 bits, low word first).
+cudaError_t launch_bd_columns(int pi, const uint16_t* top, const uint16_t* digits, int cols, int limb,
+                              const GarnerConsts& g, int limbs, const DevPrime* D, int16_t* C, cudaStream_t st);
+cudaError_t launch_bd_inverse(int pi, const uint32_t* diff, const DevPrime* D, uint32_t* res, cudaStream_t st);
+cudaError_t launch_bd_normsq(const uint32_t* res, int limbs, const GarnerConsts& g, unsigned long long* out,
+                             cudaStream_t st);
 // components_mod_2 of v as 4 len_ring F162.
 cudaError_t launch_v_parity(const int16_t* v, size_t len_ring, uint64_t* W, cudaStream_t st);
 cudaError_t launch_fold_binary(const uint64_t* u, const lbg_challenge_d* ch, int r, uint64_t* out, cudaStream_t st);

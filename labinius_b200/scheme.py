@@ -325,7 +325,7 @@ class FoldedWitness:
 @dataclass
 class OpeningMessage:
     """OpeningMessage (crates/pcs/src/scheme/verifier.rs): what the prover sends for the opening
-    check; only the Clear arm is checked here."""
+    check; the Clear and bit-dropped arms are checked here (the recursive arm is not rebuilt)."""
     kind: str
     folded_commitment: "FoldedCommitment" = None
     folded_witness: FoldedWitness = None
@@ -334,6 +334,10 @@ class OpeningMessage:
     @staticmethod
     def clear(folded_commitment, folded_witness, folded_row_value) -> "OpeningMessage":
         return OpeningMessage("clear", folded_commitment, folded_witness, folded_row_value)
+
+    @staticmethod
+    def bit_dropped(folded_witness, folded_row_value) -> "OpeningMessage":
+        return OpeningMessage("bit_dropped", None, folded_witness, folded_row_value)
 
 
 @dataclass
@@ -580,13 +584,41 @@ class Verifier:
         if not ok.value:
             raise VerificationError("Rejected")
 
+    def bd_residual(self, commitment: Commitment, challenges: FoldingChallenges, folded_witness: FoldedWitness,
+                    point: EvaluationPoint, folded_row_value):
+        """The bit-dropped opening check (crates/pcs/src/scheme/verifier.rs:232-276) on the device:
+        returns (accepted, the squared norm of the residual, crates/pcs/src/bd/residual.rs:66-130)."""
+        v = np.ascontiguousarray(folded_witness.elements, dtype=np.int16)
+        if v.shape != (self.params.len_ring(), 648) or commitment.top is None:
+            return False, None
+        if list(commitment.primes) != self.params.primes():
+            return False, None
+        top = np.ascontiguousarray(commitment.top, dtype=np.uint16)
+        digits = np.ascontiguousarray(commitment.digits, dtype=np.uint16)
+        ch = np.ascontiguousarray(challenges.challenges, dtype=CHALLENGE_DTYPE)
+        p0 = np.ascontiguousarray(point.p0, dtype=np.uint64)
+        fr = np.ascontiguousarray(folded_row_value, dtype=np.uint64)
+        ok = ctypes.c_int(0)
+        res = np.zeros(2, np.uint64)
+        check(lib().lbg_verify_folded_opening_bd(self.pp._h, ptr(top), ptr(digits) if digits.size else None, ptr(ch),
+                                                 len(ch), ptr(v), ptr(p0), len(p0), ptr(fr), ctypes.byref(ok),
+                                                 ptr(res)))
+        return bool(ok.value), int(res[0]) | (int(res[1]) << 64)
+
     def verify_opening(self, commitment: Commitment, challenges: FoldingChallenges, point: EvaluationPoint,
                        message: "OpeningMessage"):
         """crates/pcs/src/scheme/verifier.rs:280-337: the check the parameters' opening mode names.
-        Opening::Clear runs on the device; the bit-dropped and recursive arms are not rebuilt."""
-        if self.params.opening.kind != "clear" or message.kind != "clear":
-            if self.params.opening.kind != message.kind:
+        Opening::Clear and BitDropped run on the device; the recursive arm is not rebuilt."""
+        if self.params.opening.kind != message.kind:
+            raise VerificationError("Rejected")
+        if message.kind == "clear":
+            self.verify_folded_opening(message.folded_commitment, message.folded_witness, point,
+                                       message.folded_row_value)
+        elif message.kind == "bit_dropped":
+            if commitment.params is not None and commitment.params.dropped_bits() != self.params.dropped_bits():
                 raise VerificationError("Rejected")
+            ok, _ = self.bd_residual(commitment, challenges, message.folded_witness, point, message.folded_row_value)
+            if not ok:
+                raise VerificationError("Rejected")
+        else:
             raise NotImplementedError(f"the {message.kind} opening check is not on the device")
-        self.verify_folded_opening(message.folded_commitment, message.folded_witness, point,
-                                   message.folded_row_value)

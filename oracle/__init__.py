@@ -79,6 +79,8 @@ def _setup(L):
         "orc_derive_evaluation_point": (None, [vp, vp, vp, vp, vp, vp, vp]),
         "orc_derive_folding_challenges": (None, [vp, vp, vp, vp]),
         "orc_verify_folded_opening": (i32, [vp, vp, vp, vp, vp, vp]),
+        "orc_bd_residual": (None, [vp, vp, vp, vp, vp, vp, vp]),
+        "orc_verify_folded_opening_bd": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "orc_fold_binary": (None, [vp, vp, sz, vp]),
     }
     for name, (res, args) in sig.items():
@@ -375,6 +377,41 @@ def verify_folded_opening(params: Params, A, folded_commitment, v, p0, folded_ro
     p0 = np.ascontiguousarray(p0, dtype=np.uint64)
     fr = np.ascontiguousarray(folded_row_value, dtype=np.uint64)
     return bool(lib().orc_verify_folded_opening(_p(pa), _p(A), _p(fc), _p(v), _p(p0), _p(fr)))
+
+
+def _dropped_args(params: Params, top, digits):
+    top = np.ascontiguousarray(top, dtype=np.uint16)
+    digits = np.ascontiguousarray(digits, dtype=np.uint16)
+    if digits.size == 0:
+        digits = np.zeros(1, np.uint16)
+    return top, digits
+
+
+def bd_residual(params: Params, A, top, digits, challenges, v):
+    """crates/pcs/src/bd/residual.rs:66-130: the squared norm (an int) of the bit-dropped residual."""
+    top, digits = _dropped_args(params, top, digits)
+    out = np.zeros(2, np.uint64)
+    lib().orc_bd_residual(_p(params.arr()), _p(np.ascontiguousarray(A, dtype=np.int16)), _p(top), _p(digits),
+                          _p(np.ascontiguousarray(challenges, dtype=CHALLENGE_DTYPE)),
+                          _p(np.ascontiguousarray(v, dtype=np.int16)), _p(out))
+    return int(out[0]) | (int(out[1]) << 64)
+
+
+def bd_cap(params: Params):
+    """crates/pcs/src/bd/mod.rs:72-75"""
+    import math
+
+    d = params.dropped_bits
+    return math.ceil(4.0 * float(N * params.columns * 28) * (float((1 << (2 * d)) - 1) / 12.0))
+
+
+def verify_folded_opening_bd(params: Params, A, top, digits, challenges, v, p0, folded_row_value):
+    """crates/pcs/src/scheme/verifier.rs:232-276"""
+    top, digits = _dropped_args(params, top, digits)
+    return bool(lib().orc_verify_folded_opening_bd(
+        _p(params.arr()), _p(np.ascontiguousarray(A, dtype=np.int16)), _p(top), _p(digits),
+        _p(np.ascontiguousarray(challenges, dtype=CHALLENGE_DTYPE)), _p(np.ascontiguousarray(v, dtype=np.int16)),
+        _p(np.ascontiguousarray(p0, dtype=np.uint64)), _p(np.ascontiguousarray(folded_row_value, dtype=np.uint64))))
 
 
 def fold_binary(u, challenges):

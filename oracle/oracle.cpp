@@ -1217,17 +1217,13 @@ void orc_derive_folding_challenges(const uint32_t* params, void* t, const uint64
   for (size_t j = 0; j < pr.columns(); j++) c[j] = sample_short_challenge(tr, 28, 12.0, nullptr);
 }
 
-// The verifier's folded-opening check, crates/pcs/src/scheme/verifier.rs:178-231: v centered in
-// range, A v equal to the folded commitment on every limb, and the binary check
-// (crates/pcs/src/eval.rs:202-249). Returns 1 on acceptance.
-int orc_verify_folded_opening(const uint32_t* params, const int16_t* A, const int16_t* folded_commitment,
-                              const int16_t* v, const uint64_t* p0, uint64_t* folded_row_value) {
-  Params pr = make_params(params);
+// The norm part of the folded-opening checks (crates/pcs/src/simd/norm.rs:9-50 per element,
+// crates/pcs/src/scheme/verifier.rs:189-201 and 246-260): 16 i32 lanes of pairwise squares per
+// element, rejected when a lane reaches 2^31; the largest 16-bit absolute value (|-32768| stays
+// negative); the squared norm against fold_cap (crates/pcs/src/scheme/params.rs:259-265).
+static bool norm_ok(const Params& pr, const int16_t* v) {
   size_t len_ring = pr.len_ring();
   int half = (int)(pr.primes[0] - 1) / 2;
-  // the norm (crates/pcs/src/simd/norm.rs:9-50 per element, verifier.rs:189-201): 16 i32 lanes of
-  // pairwise squares per element, rejected when a lane reaches 2^31; the largest 16-bit absolute
-  // value (|-32768| stays negative); the squared norm against fold_cap (params.rs:259-265)
   uint64_t normsq = 0;
   int worst = 0;
   for (size_t e = 0; e < len_ring; e++) {
@@ -1239,40 +1235,42 @@ int orc_verify_folded_opening(const uint32_t* params, const int16_t* A, const in
       if (a > worst) worst = a;
     }
     for (int l = 0; l < 16; l++) {
-      if (lane[l] >= (1ull << 31)) return 0;
+      if (lane[l] >= (1ull << 31)) return false;
       normsq += lane[l];
     }
   }
   uint64_t fold_cap = (uint64_t)std::ceil(108.0 * (double)(pr.witness_len() / 4 * N));
-  if (worst > half || normsq > fold_cap) return 0;
-  for (int k = 0; k < pr.limbs; k++) {
-    const Prime& P = prime(pr.primes[k]);
-    i64 q = P.q;
-    std::vector<i64> y(N, 0);
-    for (size_t i = 0; i < len_ring; i++) {
-      u32 c[N], w[N];
-      for (int x = 0; x < N; x++) c[x] = (u32)((((i64)v[i * N + x]) % q + q) % q);
-      ntt(P, c, w);
-      const int16_t* a = A + ((size_t)k * len_ring + i) * N;
-      if (!P.quad) {
-        for (int j = 0; j < N; j++) y[j] = (y[j] + (i64)w[j] * a[j]) % q;
-      } else {
-        for (int j = 0; j < 324; j++) {
-          i64 w0 = w[2 * j], w1 = w[2 * j + 1], a0 = a[2 * j], a1 = a[2 * j + 1];
-          y[2 * j] = (y[2 * j] + w0 * a0 + (i64)P.leaf_c[j] * ((w1 * a1) % q)) % q;
-          y[2 * j + 1] = (y[2 * j + 1] + w0 * a1 + w1 * a0) % q;
-        }
+  return worst <= half && normsq <= fold_cap;
+}
+
+// A v modulo limb k as the reference's 648 NTT slots (crates/pcs/src/fold.rs:733-797).
+static void a_times_v(const Params& pr, const int16_t* A, const int16_t* v, int k, u32* yy) {
+  size_t len_ring = pr.len_ring();
+  const Prime& P = prime(pr.primes[k]);
+  i64 q = P.q;
+  std::vector<i64> y(N, 0);
+  for (size_t i = 0; i < len_ring; i++) {
+    u32 c[N], w[N];
+    for (int x = 0; x < N; x++) c[x] = (u32)((((i64)v[i * N + x]) % q + q) % q);
+    ntt(P, c, w);
+    const int16_t* a = A + ((size_t)k * len_ring + i) * N;
+    if (!P.quad) {
+      for (int j = 0; j < N; j++) y[j] = (y[j] + (i64)w[j] * a[j]) % q;
+    } else {
+      for (int j = 0; j < 324; j++) {
+        i64 w0 = w[2 * j], w1 = w[2 * j + 1], a0 = a[2 * j], a1 = a[2 * j + 1];
+        y[2 * j] = (y[2 * j] + w0 * a0 + (i64)P.leaf_c[j] * ((w1 * a1) % q)) % q;
+        y[2 * j + 1] = (y[2 * j + 1] + w0 * a1 + w1 * a0) % q;
       }
     }
-    u32 yy[N];
-    for (int j = 0; j < N; j++) yy[j] = (u32)(((y[j] % q) + q) % q);
-    int16_t comp[4][N162];
-    components(P, yy, comp);
-    for (int row = 0; row < 4; row++)
-      for (int s = 0; s < N162; s++)
-        if (comp[row][s] != folded_commitment[(row * pr.limbs + k) * N162 + s]) return 0;
   }
-  // binary check: sum_i eq(p0, i) (v mod 2)_i == folded_row_value
+  for (int j = 0; j < N; j++) yy[j] = (u32)(((y[j] % q) + q) % q);
+}
+
+// The binary check (crates/pcs/src/eval.rs:202-249): sum_i eq(p0, i) (v mod 2)_i == the folded
+// row value.
+static bool binary_ok(const Params& pr, const int16_t* v, const uint64_t* p0, const uint64_t* folded_row_value) {
+  size_t len_ring = pr.len_ring();
   std::vector<F162> eq = eq_table((const F162*)p0, (int)pr.row_log_len());
   F162 acc = f_zero();
   for (size_t m = 0; m < len_ring; m++)
@@ -1284,6 +1282,112 @@ int orc_verify_folded_opening(const uint32_t* params, const int16_t* A, const in
     }
   F162 want = {{folded_row_value[0], folded_row_value[1], folded_row_value[2]}};
   return acc.w[0] == want.w[0] && acc.w[1] == want.w[1] && acc.w[2] == want.w[2];
+}
+
+// The verifier's folded-opening check, crates/pcs/src/scheme/verifier.rs:178-231: v centered in
+// range, A v equal to the folded commitment on every limb, and the binary check. Returns 1 on
+// acceptance.
+int orc_verify_folded_opening(const uint32_t* params, const int16_t* A, const int16_t* folded_commitment,
+                              const int16_t* v, const uint64_t* p0, uint64_t* folded_row_value) {
+  Params pr = make_params(params);
+  if (!norm_ok(pr, v)) return 0;
+  for (int k = 0; k < pr.limbs; k++) {
+    const Prime& P = prime(pr.primes[k]);
+    u32 yy[N];
+    a_times_v(pr, A, v, k, yy);
+    int16_t comp[4][N162];
+    components(P, yy, comp);
+    for (int row = 0; row < 4; row++)
+      for (int s = 0; s < N162; s++)
+        if (comp[row][s] != folded_commitment[(row * pr.limbs + k) * N162 + s]) return 0;
+  }
+  return binary_ok(pr, v, p0, folded_row_value) ? 1 : 0;
+}
+
+// The bit-dropped residual, crates/pcs/src/bd/residual.rs:66-130: per limb, the columns'
+// coefficients rebuilt from the top bits and the Garner digits (crates/pcs/src/simd/bd.rs:5-36:
+// (top << dropped_bits) + q_0 (d_1 + q_1 (d_2 + ...)) modulo the limb), folded with the
+// challenges, subtracted from A v, back to coefficients; then the Garner recombination of the
+// limbs and the squared norm of the centred result (crates/pcs/src/bd/digits.rs:229-260).
+// normsq_out: the 128-bit sum as two words, low first.
+void orc_bd_residual(const uint32_t* params, const int16_t* A, const uint16_t* top, const uint16_t* digits,
+                     const void* challenges, const int16_t* v, uint64_t* normsq_out) {
+  Params pr = make_params(params);
+  size_t r = pr.columns(), count = r * N;
+  int L = pr.limbs;
+  std::vector<int16_t> C(r * 4 * L * N162);
+  for (int k = 0; k < L; k++) {
+    const Prime& P = prime(pr.primes[k]);
+    i64 q = P.q;
+    for (size_t j = 0; j < r; j++) {
+      u32 x[N], y[N];
+      for (int i = 0; i < N; i++) {
+        size_t at = j * N + i;
+        i64 inner = 0;
+        if (L > 1) {
+          inner = digits[(size_t)(L - 2) * count + at] % q;
+          for (int m = L - 3; m >= 0; m--) inner = (digits[(size_t)m * count + at] + inner * pr.primes[m + 1]) % q;
+        }
+        i64 t = ((i64)top[at] << pr.dropped_bits) + inner * pr.primes[0];
+        x[i] = (u32)(t % q);
+      }
+      ntt(P, x, y);
+      int16_t comp[4][N162];
+      components(P, y, comp);
+      for (int row = 0; row < 4; row++)
+        for (int s = 0; s < N162; s++) C[((j * 4 + row) * L + k) * N162 + s] = comp[row][s];
+    }
+  }
+  std::vector<int16_t> fc(4 * L * N162);
+  fold_commitment(pr, C.data(), (const Challenge*)challenges, fc.data());
+  std::vector<std::vector<u32>> z(L, std::vector<u32>(N));
+  for (int k = 0; k < L; k++) {
+    const Prime& P = prime(pr.primes[k]);
+    u32 yy[N], fy[N], d[N];
+    a_times_v(pr, A, v, k, yy);
+    int16_t comp[4][N162];
+    for (int row = 0; row < 4; row++)
+      for (int s = 0; s < N162; s++) comp[row][s] = fc[(row * L + k) * N162 + s];
+    recombine(P, comp, fy);
+    for (int u = 0; u < N; u++) d[u] = (yy[u] + P.q - fy[u]) % P.q;
+    intt(P, d, z[k].data());
+  }
+  unsigned __int128 modulus = 1, normsq = 0;
+  for (int k = 0; k < L; k++) modulus *= pr.primes[k];
+  for (int i = 0; i < N; i++) {
+    u64 mixed[8];
+    for (int k = 0; k < L; k++) {
+      u64 q = pr.primes[k];
+      u64 x = z[k][i] % q;
+      for (int m = 0; m < k; m++) x = (x + q - mixed[m] % q) % q * inv_mod(pr.primes[m], q) % q;
+      mixed[k] = x;
+    }
+    unsigned __int128 value = 0;
+    for (int k = L - 1; k >= 0; k--) value = value * pr.primes[k] + mixed[k];
+    unsigned __int128 mag = value > modulus / 2 ? modulus - value : value;
+    normsq += mag * mag;
+  }
+  normsq_out[0] = (uint64_t)normsq;
+  normsq_out[1] = (uint64_t)(normsq >> 64);
+}
+
+// crates/pcs/src/bd/mod.rs:72-75: ceil(BD_CAP * (N * columns * DEFAULT_WEIGHT) * (4^d - 1) / 12).
+static uint64_t bd_cap(size_t columns, u32 d) {
+  double spread = (double)((1ull << (2 * d)) - 1) / 12.0;
+  return (uint64_t)std::ceil(4.0 * (double)(N * columns * 28) * spread);
+}
+
+// The verifier's bit-dropped opening check, crates/pcs/src/scheme/verifier.rs:232-276: the norm
+// checks, the residual against bd_cap, and the binary check. Returns 1 on acceptance.
+int orc_verify_folded_opening_bd(const uint32_t* params, const int16_t* A, const uint16_t* top,
+                                 const uint16_t* digits, const void* challenges, const int16_t* v,
+                                 const uint64_t* p0, uint64_t* folded_row_value) {
+  Params pr = make_params(params);
+  if (!norm_ok(pr, v)) return 0;
+  uint64_t ns[2];
+  orc_bd_residual(params, A, top, digits, challenges, v, ns);
+  if (ns[1] != 0 || ns[0] > bd_cap(pr.columns(), pr.dropped_bits)) return 0;
+  return binary_ok(pr, v, p0, folded_row_value) ? 1 : 0;
 }
 
 // crates/pcs/src/eval.rs:195-200: u^T (c mod 2).

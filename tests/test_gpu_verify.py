@@ -64,3 +64,44 @@ def test_verifier_on_device_matches_oracle(oracle, shape):
         want = oracle.verify_folded_opening(P, key, f, vv, r["p0"], rr)
         assert not want, name
         assert gpu_accepts(verifier, f, vv, point, rr) == want, name
+
+
+@pytest.mark.parametrize("shape", [(12, 4, [9721, 3889], 9), (12, 3, [3889, 2917, 4861], 10), (11, 3, [9721], 8)],
+                         ids=["two-limbs", "three-limbs", "one-limb"])
+def test_bit_dropped_opening_on_device_matches_oracle(oracle, shape):
+    """The bit-dropped arm (crates/pcs/src/scheme/verifier.rs:232-276): on an honest round the
+    device's residual (crates/pcs/src/bd/residual.rs:66-130) equals the oracle's to the bit and the
+    check accepts; tampered rounds get the oracle's verdict."""
+    import labinius_b200 as L
+
+    r = product_round(shape)
+    pp = r["pp"]
+    verifier = L.Verifier(pp)
+    P = oracle_params(oracle, shape)
+    key = pp.key()
+    c = r["commitment"]
+    ch = L.FoldingChallenges(r["challenges"])
+    point = L.EvaluationPoint(r["p0"], r["p1"])
+    fr = verifier.fold_row_evaluation(L.RowEvaluation(r["u"]), ch)
+    v = r["v"]
+    ok, res = verifier.bd_residual(c, ch, L.FoldedWitness(v), point, fr)
+    want = oracle.bd_residual(P, key, c.top, c.digits, r["challenges"], v)
+    assert res == want and ok
+    assert 0 < res <= oracle.bd_cap(P)
+    verifier.verify_opening(c, ch, point, L.OpeningMessage.bit_dropped(L.FoldedWitness(v), fr))
+
+    half = (shape[2][0] - 1) // 2
+    cases = []
+    v1 = v.copy(); v1[3, 17] += 1; cases.append(("v+1", c.top, c.digits, v1, fr))
+    v2 = v.copy(); v2[0, 0] = half + 1; cases.append(("out of range", c.top, c.digits, v2, fr))
+    fr2 = fr.copy(); fr2[0] ^= np.uint64(1); cases.append(("row value", c.top, c.digits, v, fr2))
+    t2 = (c.top.astype(np.int64) + 5) % (1 << 6); cases.append(("top", t2.astype(np.uint16), c.digits, v, fr))
+    if len(shape[2]) > 1:
+        d2 = c.digits.copy(); d2[0, ::3] = (d2[0, ::3] + 1) % shape[2][1]; cases.append(("digits", c.top, d2, v, fr))
+    for name, top, digits, vv, rr in cases:
+        want = oracle.verify_folded_opening_bd(P, key, top, digits, r["challenges"], vv, r["p0"], rr)
+        c2 = L.Commitment(c.primes, c.columns, top=top, digits=digits, params=c.params)
+        got, res2 = verifier.bd_residual(c2, ch, L.FoldedWitness(vv), point, rr)
+        assert got == want, name
+        assert res2 == oracle.bd_residual(P, key, top, digits, r["challenges"], vv), name
+        assert not want, name
