@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-switch", action="store_true")
+    ap.add_argument("--no-wire", action="store_true")
     ap.add_argument("--no-ntt", action="store_true")
     ap.add_argument("--no-suites", action="store_true")
     ap.add_argument("--ntt-count", type=int, default=1 << 20, help="ring elements of the NTT microbenchmark")
@@ -512,6 +513,33 @@ def run_switch(steps, sizes=(18, 20, 22)):
     return out
 
 
+def run_wire(L, prover, params, steps):
+    """wire::encode of the prover's last folded witness (crates/pcs/src/wire/rans.rs:18-105): on the
+    device from where Prover::fold left it, and through the host-memory entry point; the host clock
+    around the synchronous calls; the size against the zeroth-order entropy."""
+    from labinius_b200 import wire
+    from labinius_b200._native import check, lib, ptr
+
+    vv = np.zeros((params.len_ring(), 648), np.int16)
+    check(lib().lbg_prover_folded(prover._h, ptr(vv)))
+    data = wire.encode_folded(prover)
+    dev, host = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        wire.encode_folded(prover)
+        dev.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        wire.encode(vv, params.primes()[0])
+        host.append(time.perf_counter() - t0)
+    _, counts = np.unique(vv, return_counts=True)
+    p = counts / counts.sum()
+    entropy = float(-(counts * np.log2(p)).sum() / 8.0)
+    return {"coefficients": int(vv.size), "bytes": len(data), "bits_per_coefficient": 8.0 * len(data) / vv.size,
+            "entropy_bytes": entropy, "device_ms": 1000 * float(np.median(dev)),
+            "host_input_ms": 1000 * float(np.median(host)),
+            "workload": "the folded witness of the bench's step (len_ring x 648 int16), interleaved rANS, 64 lanes"}
+
+
 def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
     """Served: commit+open requests with log2 n ~ U{18..22} (column length 2048, moduli [3889, 9721]),
     80% Witness::random and 20% B128 traces opened through the cross-field switch, each from its
@@ -770,6 +798,12 @@ def run_ours(args):
                "h2d_bytes_per_step": 24 * n + chal.nbytes, "d2h_bytes_per_step": mat.nbytes + vout.nbytes,
                "timing": "host wall clock around synchronous API calls, max over ranks"}
 
+    # wire::encode of the folded witness (crates/bench/src/bin/labinius.rs:142, "encode folded
+    # witness"): from where the fold left it, and from host memory
+    wire_times = None
+    if rank == 0 and not args.no_wire:
+        wire_times = run_wire(L, prover, params, max(3, min(args.steps, 10)))
+
     # the verifier's side of the round (crates/bench/src/bin/labinius.rs:151-176), on the device:
     # fold_commitment, fold_row_evaluation, verify_evaluation, verify_opening (Clear)
     verifier_times = None
@@ -842,6 +876,7 @@ def run_ours(args):
         "batched": batched,
         "served": served,
         "switch": switch_times,
+        "wire": wire_times,
         "ntt_microbench": ntt_micro,
         "suites": suites,
         "verifier": verifier_times,

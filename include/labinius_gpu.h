@@ -173,6 +173,17 @@ int lbg_switch_prove(const lbg_pp* pp, const lbg_witness* w, const uint64_t* r_l
                      size_t l, const uint64_t claim[2], lbg_transcript* t, uint64_t* partials, uint64_t* rounds,
                      uint64_t opened[3], uint64_t* p0_out, uint64_t* p1_out);
 
+/* wire::encode (crates/pcs/src/wire/rans.rs:18-105): the folded witness, `elements` ring elements
+ * of 648 int16 coefficients (host memory), entropy-coded by interleaved static rANS over 64 lanes
+ * against its own histogram, base_q recorded in the header. Writes the bytes when out has room
+ * (cap >= the returned count; lbg_wire_encode_bound(elements) always is) and returns their count,
+ * or a negative status. The lanes, the histogram and the word placement run on the device. */
+long long lbg_wire_encode(const int16_t* v, size_t elements, uint32_t base_q, uint8_t* out, size_t cap);
+size_t lbg_wire_encode_bound(size_t elements);
+/* The same for the prover's last folded witness, read where Prover::fold left it on the device
+ * (no upload), base_q = the base modulus. */
+long long lbg_prover_encode_folded(lbg_prover* pr, uint8_t* out, size_t cap);
+
 /* Transcript (crates/pcs/src/challenge.rs:66-161), host side. */
 lbg_transcript* lbg_transcript_new(const uint8_t* domain, size_t len);
 lbg_transcript* lbg_transcript_clone(const lbg_transcript* t);

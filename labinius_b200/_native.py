@@ -96,6 +96,9 @@ SIGNATURES = {
     "lbg_batch_fold": (_int, [_vp, _vp, _sz, _vp]),
     "lbg_batch_round": (_int, [_vp, _vp, _sz, _vp]),
     "lbg_batch_set_switch": (_int, [_vp, _vp, _vp, _vp]),
+    "lbg_wire_encode": (ctypes.c_longlong, [_vp, _sz, ctypes.c_uint32, _vp, _sz]),
+    "lbg_wire_encode_bound": (_sz, [_sz]),
+    "lbg_prover_encode_folded": (ctypes.c_longlong, [_vp, _vp, _sz]),
     "lbg_verify_folded_opening_bd": (_int, [_vp, _vp, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _vp, _vp]),
     "lbg_batch_switch_outputs": (_int, [_vp, _vp, _vp, _vp, _vp]),
     "lbg_prover_set_kept_transform": (_int, [_vp, _int]),

@@ -80,6 +80,8 @@ def _setup(L):
         "orc_derive_folding_challenges": (None, [vp, vp, vp, vp]),
         "orc_verify_folded_opening": (i32, [vp, vp, vp, vp, vp, vp]),
         "orc_bd_residual": (None, [vp, vp, vp, vp, vp, vp, vp]),
+        "orc_wire_encode": (sz, [vp, sz, u32, vp, sz]),
+        "orc_wire_decode": (i32, [vp, sz, vp, sz, vp]),
         "orc_verify_folded_opening_bd": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "orc_fold_binary": (None, [vp, vp, sz, vp]),
     }
@@ -543,4 +545,24 @@ def switch_round(params: Params, matrix_seed: bytes, trace, r_hi, claim_value=No
         out["folded_commitment"] = fold_commitment(params, C, ch)
     out["transcript_tail"] = t.fill(b"labinius/test-tail", 32)
     return out
+
+
+def wire_encode(v, base_q: int) -> bytes:
+    """wire::encode (crates/pcs/src/wire/rans.rs:18-105): v is int16 [elements][648]."""
+    v = np.ascontiguousarray(v, dtype=np.int16).reshape(-1, N)
+    n = lib().orc_wire_encode(_p(v), len(v), base_q, None, 0)
+    out = np.zeros(max(n, 1), np.uint8)
+    lib().orc_wire_encode(_p(v), len(v), base_q, _p(out), n)
+    return out[:n].tobytes()
+
+
+def wire_decode(data: bytes):
+    """wire::decode (crates/pcs/src/wire/rans.rs:107-226): (status, v) with status 0 (ok),
+    1 (truncated) or 2 (malformed)."""
+    b = np.frombuffer(bytes(data), dtype=np.uint8).copy() if len(data) else np.zeros(1, np.uint8)
+    count = ctypes.c_size_t(0)
+    lib().orc_wire_decode(_p(b), len(data), None, 0, ctypes.byref(count))
+    v = np.zeros((count.value, N), np.int16) if count.value <= (1 << 20) else np.zeros((0, N), np.int16)
+    st = lib().orc_wire_decode(_p(b), len(data), _p(v) if v.size else None, v.size, ctypes.byref(count))
+    return st, v
 

@@ -905,7 +905,312 @@ static void absorb_parameters(const Params& pr, const uint8_t seed[32], Transcri
 // =============================================================================================
 // C ABI for the Python test harness (ctypes). Arrays are caller-owned.
 // =============================================================================================
+
 using namespace orc;
+
+// ---------------------------------------------------------------------------------------------
+// wire: the folded witness by interleaved static rANS (crates/pcs/src/wire/rans.rs:8-340, and the
+// bit writer and reader of crates/pcs/src/wire/mod.rs:57-205)
+// ---------------------------------------------------------------------------------------------
+namespace wire {
+constexpr u32 SCALE_BITS = 12, SCALE = 1u << SCALE_BITS, RANS_LOW = 1u << 16;
+constexpr size_t HEADER = 16, LANES = 64, MAX_ELEMENTS = (size_t)1 << 24;
+
+struct BitWriter {
+  std::vector<uint8_t> bytes;
+  u64 acc = 0;
+  u32 n = 0;
+  void put(u64 value, u32 bits) {
+    acc |= (value & ((1ull << bits) - 1)) << n;
+    n += bits;
+    while (n >= 8) {
+      bytes.push_back((uint8_t)acc);
+      acc >>= 8;
+      n -= 8;
+    }
+  }
+  void put_wide(u64 value, u32 bits) {
+    if (bits <= 32) {
+      put(value, bits);
+    } else {
+      put(value, 32);
+      put(value >> 32, bits - 32);
+    }
+  }
+  // Elias gamma, least significant bit first inside each field
+  void put_gamma(u64 value) {
+    u32 k = 63 - __builtin_clzll(value);
+    put(0, k);
+    put(1, 1);
+    put_wide(value & ((1ull << k) - 1), k);
+  }
+  std::vector<uint8_t> finish() {
+    if (n > 0) bytes.push_back((uint8_t)acc);
+    return bytes;
+  }
+};
+
+struct BitReader {
+  const uint8_t* b;
+  size_t len, pos = 0;
+  u64 acc = 0;
+  u32 n = 0;
+  BitReader(const uint8_t* bytes, size_t l) : b(bytes), len(l) {}
+  void refill() {
+    size_t rest = len - pos;
+    u64 word = 0;
+    for (size_t i = 0; i < 8 && i < rest; i++) word |= (u64)b[pos + i] << (8 * i);
+    acc |= word << n;
+    size_t take = std::min<size_t>((63 - n) >> 3, rest);
+    pos += take;
+    n += 8 * (u32)take;
+  }
+  bool get(u32 bits, u64& out) {
+    if (n < bits) {
+      refill();
+      if (n < bits) return false;
+    }
+    out = acc & ((1ull << bits) - 1);
+    acc >>= bits;
+    n -= bits;
+    return true;
+  }
+  bool get_wide(u32 bits, u64& out) {
+    if (bits <= 32) return get(bits, out);
+    u64 lo, hi;
+    if (!get(32, lo) || !get(bits - 32, hi)) return false;
+    out = lo | (hi << 32);
+    return true;
+  }
+  // 0: ok, 1: truncated, 2: malformed
+  int get_gamma(u64& out) {
+    u32 k = 0;
+    for (;;) {
+      u64 bit;
+      if (!get(1, bit)) return 1;
+      if (bit) break;
+      if (++k > 32) return 2;
+    }
+    u64 low;
+    if (!get_wide(k, low)) return 1;
+    out = (1ull << k) | low;
+    return 0;
+  }
+  size_t consumed() const { return pos - n / 8; }
+};
+
+static u32 raw_bits(size_t length) { return length <= 1 ? 0 : 64 - __builtin_clzll((u64)(length - 1)); }
+
+static std::vector<u32> starts(const std::vector<u32>& f) {
+  std::vector<u32> s(f.size());
+  u32 acc = 0;
+  for (size_t i = 0; i < f.size(); i++) {
+    s[i] = acc;
+    acc += f[i];
+  }
+  return s;
+}
+
+// The counts scaled to a total of exactly SCALE (crates/pcs/src/wire/rans.rs:231-268).
+static std::vector<u32> quantize(const std::vector<u64>& counts) {
+  size_t escape = counts.size() - 1;
+  std::vector<u64> w = counts;
+  std::vector<size_t> occ;
+  for (size_t i = 0; i < escape; i++)
+    if (w[i] > 0) occ.push_back(i);
+  if (occ.size() > SCALE - 1) {
+    std::sort(occ.begin(), occ.end(), [&](size_t a, size_t b) { return w[a] != w[b] ? w[a] > w[b] : a < b; });
+    for (size_t k = SCALE - 1; k < occ.size(); k++) {
+      w[escape] += w[occ[k]];
+      w[occ[k]] = 0;
+    }
+  }
+  u64 total = 0;
+  for (u64 x : w) total += x;
+  std::vector<size_t> occupied;
+  for (size_t i = 0; i < w.size(); i++)
+    if (w[i] > 0) occupied.push_back(i);
+  std::vector<u32> freq(w.size(), 0);
+  if (occupied.empty()) return freq;
+  u64 spare = SCALE - occupied.size(), used = 0;
+  std::vector<std::pair<u64, size_t>> rem;
+  for (size_t i : occupied) {
+    u64 share = w[i] * spare / total;
+    freq[i] = 1 + (u32)share;
+    used += share;
+    rem.push_back({w[i] * spare - share * total, i});
+  }
+  std::sort(rem.begin(), rem.end(), [](const std::pair<u64, size_t>& a, const std::pair<u64, size_t>& b) {
+    return a.first != b.first ? a.first > b.first : a.second < b.second;
+  });
+  for (size_t k = 0; k < (size_t)(spare - used); k++) freq[rem[k].second] += 1;
+  return freq;
+}
+
+struct Sym {
+  u64 reciprocal;
+  u32 frequency, bias;
+};
+static Sym make_sym(u32 f, u32 start) {
+  if (f == 0) return {0, 0, 0};
+  if (f == 1) return {~0ull, 1, start + SCALE - 1};
+  return {~0ull / f + 1, f, start};
+}
+static void renormalise(u32& x, std::vector<uint16_t>& words, size_t& top, bool needed) {
+  words[top] = (uint16_t)x;
+  top += needed ? 1 : 0;
+  x = needed ? x >> 16 : x;
+}
+static void put_symbol(u32& x, std::vector<uint16_t>& words, size_t& top, const Sym& s) {
+  renormalise(x, words, top, (x >> (32 - SCALE_BITS)) >= s.frequency);
+  u32 q = (u32)(((unsigned __int128)x * s.reciprocal) >> 64);
+  x = (q << SCALE_BITS) + (x - q * s.frequency) + s.bias;
+}
+static void put_bits(u32& x, std::vector<uint16_t>& words, size_t& top, u32 value, u32 bits) {
+  if (bits == 0) return;
+  renormalise(x, words, top, (x >> (32 - bits)) != 0);
+  x = (x << bits) | value;
+}
+
+static void le(std::vector<uint8_t>& out, u64 v, int bytes) {
+  for (int i = 0; i < bytes; i++) out.push_back((uint8_t)(v >> (8 * i)));
+}
+
+// wire::encode (crates/pcs/src/wire/rans.rs:18-105): v is elements x 648 coefficients.
+static std::vector<uint8_t> encode(const int16_t* v, size_t elements, uint16_t base_q, bool ntt) {
+  size_t coefficients = elements * N;
+  std::vector<uint8_t> out;
+  out.push_back(1);
+  out.push_back(ntt ? 1 : 0);
+  le(out, base_q, 2);
+  le(out, (u32)elements, 4);
+  if (coefficients == 0) {
+    le(out, 0, 4);
+    le(out, 0, 4);
+    return out;
+  }
+  int low = 32767, high = -32768;
+  for (size_t i = 0; i < coefficients; i++) {
+    low = std::min<int>(low, v[i]);
+    high = std::max<int>(high, v[i]);
+  }
+  size_t length = (size_t)(high - low + 1);
+  le(out, (u32)low, 4);
+  le(out, (u32)length, 4);
+  std::vector<u64> counts(length + 1, 0);
+  for (size_t i = 0; i < coefficients; i++) counts[v[i] - low]++;
+  std::vector<u32> freq = quantize(counts);
+  BitWriter w;
+  for (u32 f : freq) w.put_gamma((u64)f + 1);
+  std::vector<uint8_t> hdr = w.finish();
+  out.insert(out.end(), hdr.begin(), hdr.end());
+  std::vector<u32> start = starts(freq);
+  std::vector<Sym> sym(freq.size());
+  for (size_t s = 0; s < freq.size(); s++) sym[s] = make_sym(freq[s], start[s]);
+  u64 escaped = 0;
+  for (size_t s = 0; s < length; s++)
+    if (freq[s] == 0) escaped += counts[s];
+  u32 raw = raw_bits(length);
+  std::vector<u32> x(LANES, RANS_LOW);
+  std::vector<uint16_t> words(coefficients + escaped + 1);
+  size_t top = 0;
+  size_t groups = (coefficients + LANES - 1) / LANES;
+  for (size_t g = groups; g-- > 0;) {
+    size_t lanes = std::min(LANES, coefficients - g * LANES);
+    for (size_t k = lanes; k-- > 0;) {
+      size_t s = (size_t)(v[g * LANES + k] - low);
+      if (sym[s].frequency == 0) {
+        put_bits(x[k], words, top, (u32)s, raw);
+        put_symbol(x[k], words, top, sym[length]);
+      } else {
+        put_symbol(x[k], words, top, sym[s]);
+      }
+    }
+  }
+  for (u32 st : x) le(out, st, 4);
+  for (size_t i = 0; i < top; i++) le(out, words[top - 1 - i], 2);
+  return out;
+}
+
+// wire::decode (crates/pcs/src/wire/rans.rs:107-226), the scalar group loop: 0 on success, 1
+// truncated, 2 malformed; v gets count x 648 coefficients.
+static int decode(const uint8_t* b, size_t len, std::vector<int16_t>& v, size_t& count) {
+  if (len < HEADER) return 1;
+  if (b[0] != 1 || b[1] > 1) return 2;
+  auto rd32 = [&](size_t o) { return (u32)b[o] | ((u32)b[o + 1] << 8) | ((u32)b[o + 2] << 16) | ((u32)b[o + 3] << 24); };
+  count = rd32(4);
+  int low = (int)rd32(8);
+  size_t length = rd32(12);
+  if (count == 0) return (len == HEADER && length == 0) ? 0 : 2;
+  if (length == 0 || length > (1u << 16) || count > MAX_ELEMENTS || low < -32768 || low + (i64)length - 1 > 32767)
+    return 2;
+  BitReader r(b + HEADER, len - HEADER);
+  std::vector<u32> freq;
+  u64 total = 0;
+  for (size_t i = 0; i < length + 1; i++) {
+    u64 f;
+    int e = r.get_gamma(f);
+    if (e) return e;
+    f -= 1;
+    total += f;
+    if (total > SCALE) return 2;
+    freq.push_back((u32)f);
+  }
+  if (total != SCALE) return 2;
+  std::vector<u32> start = starts(freq);
+  std::vector<u64> table(SCALE);
+  for (size_t s = 0; s < freq.size(); s++)
+    for (u32 slot = start[s]; slot < start[s] + freq[s]; slot++)
+      table[slot] = (u64)freq[s] | ((u64)(slot - start[s]) << 16) | ((u64)s << 32);
+  size_t rest_off = HEADER + r.consumed();
+  if (len - rest_off < 4 * LANES) return 1;
+  u32 x[LANES];
+  for (size_t k = 0; k < LANES; k++) {
+    x[k] = rd32(rest_off + 4 * k);
+    if (x[k] < RANS_LOW) return 2;
+  }
+  const uint8_t* stream = b + rest_off + 4 * LANES;
+  size_t slen = len - rest_off - 4 * LANES;
+  if (slen % 2) return 2;
+  size_t nwords = slen / 2, pos = 0;
+  auto word = [&](size_t p) -> u32 { return p < nwords ? ((u32)stream[2 * p] | ((u32)stream[2 * p + 1] << 8)) : 0; };
+  u32 raw = raw_bits(length);
+  size_t coefficients = count * N;
+  v.assign(coefficients, 0);
+  for (size_t g = 0; g * LANES < coefficients; g++) {
+    size_t lanes = std::min(LANES, coefficients - g * LANES);
+    for (size_t k = 0; k < lanes; k++) {
+      u64 e = table[x[k] & (SCALE - 1)];
+      u32 y = (u32)(e & 0xFFFF) * (x[k] >> SCALE_BITS) + (u32)((e >> 16) & 0xFFFF);
+      bool ren = y < RANS_LOW;
+      u32 w = word(pos);
+      x[k] = ren ? (y << 16) | w : y;
+      pos += ren ? 1 : 0;
+      u32 s = (u32)(e >> 32);
+      if (s == length) {
+        if (raw == 0) {
+          s = 0;
+        } else {
+          u32 value = x[k] & ((1u << raw) - 1);
+          u32 y2 = x[k] >> raw;
+          bool ren2 = y2 < RANS_LOW;
+          u32 w2 = word(pos);
+          x[k] = ren2 ? (y2 << 16) | w2 : y2;
+          pos += ren2 ? 1 : 0;
+          s = value;
+        }
+        if (s >= length) return 2;
+      }
+      v[g * LANES + k] = (int16_t)(low + (int)s);
+    }
+    if (pos > nwords) return 1;
+  }
+  if (pos != nwords) return 2;
+  for (size_t k = 0; k < LANES; k++)
+    if (x[k] != RANS_LOW) return 2;
+  return 0;
+}
+}  // namespace wire
 
 static Params make_params(const uint32_t* p) {
   // p = [witness_log_len, column_log_len, limbs, dropped_bits, prime0, prime1, ...]
@@ -1536,4 +1841,21 @@ void orc_transcript_absorb_raw(void* t, const uint8_t* b, size_t len) {
   tr.state.insert(tr.state.end(), b, b + len);
 }
 
+
+// wire::encode / wire::decode (crates/pcs/src/wire/rans.rs): encode returns the byte count and
+// writes when out has room; decode returns 0 (ok), 1 (truncated), 2 (malformed), writing up to
+// cap coefficients and the element count.
+size_t orc_wire_encode(const int16_t* v, size_t elements, uint32_t base_q, uint8_t* out, size_t cap) {
+  std::vector<uint8_t> b = wire::encode(v, elements, (uint16_t)base_q, false);
+  if (out && cap >= b.size()) std::memcpy(out, b.data(), b.size());
+  return b.size();
+}
+int orc_wire_decode(const uint8_t* bytes, size_t len, int16_t* v, size_t cap, size_t* count) {
+  std::vector<int16_t> out;
+  size_t c = 0;
+  int e = wire::decode(bytes, len, out, c);
+  *count = c;
+  if (e == 0 && v && cap >= out.size()) std::memcpy(v, out.data(), out.size() * 2);
+  return e;
+}
 }  // extern "C"
