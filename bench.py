@@ -778,10 +778,11 @@ def run_ours(args):
         vout = torch.empty((params.len_ring(), 648), dtype=torch.int16, pin_memory=True).numpy()
 
         def e2e_step():
+            # Witness::from_elements + Prover::commit (the upload pipelined against the commit by
+            # column groups), then Prover::fold, results read back
             wh = ctypes.c_void_p()
-            check(N.lbg_witness_from_host(pp._h, ptr(hw), n, ctypes.byref(wh)))
             op = ctypes.c_void_p()
-            check(N.lbg_commit(prover._h, wh, ptr(mat), None, None, ctypes.byref(op)))
+            check(N.lbg_commit_host(prover._h, ptr(hw), n, ptr(mat), None, None, ctypes.byref(wh), ctypes.byref(op)))
             check(N.lbg_fold(prover._h, op, ptr(chal), len(chal), ptr(vout)))
             N.lbg_witness_free(wh)
 

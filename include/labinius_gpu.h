@@ -107,6 +107,12 @@ void lbg_witness_free(lbg_witness* w);
  * from the opening). The opening keeps a reference to the witness. */
 int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16_t* top_out,
                uint16_t* digits_out, lbg_opening** opening_out);
+/* Witness::from_elements + Prover::commit in one call, the upload pipelined against the commit:
+ * the n F162 at f162 (host memory; page-locked for the copies to overlap the commit) are copied in
+ * column groups on a second stream, and each group's commit starts as soon as it has landed.
+ * Outputs as lbg_commit; *w_out gets the device witness (free it with lbg_witness_free). */
+int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* matrix_out, uint16_t* top_out,
+                    uint16_t* digits_out, lbg_witness** w_out, lbg_opening** opening_out);
 int lbg_opening_matrix(const lbg_opening* op, int16_t* matrix_out);
 int lbg_opening_dropped(const lbg_opening* op, uint16_t* top_out, uint16_t* digits_out);
 /* Prover::recycle (crates/pcs/src/scheme/prover.rs:116-118): drop an unfolded opening. */

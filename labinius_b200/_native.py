@@ -96,6 +96,7 @@ SIGNATURES = {
     "lbg_batch_fold": (_int, [_vp, _vp, _sz, _vp]),
     "lbg_batch_round": (_int, [_vp, _vp, _sz, _vp]),
     "lbg_batch_set_switch": (_int, [_vp, _vp, _vp, _vp]),
+    "lbg_commit_host": (_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp, _vp]),
     "lbg_wire_encode": (ctypes.c_longlong, [_vp, _sz, ctypes.c_uint32, _vp, _sz]),
     "lbg_wire_encode_bound": (_sz, [_sz]),
     "lbg_prover_encode_folded": (ctypes.c_longlong, [_vp, _vp, _sz]),

@@ -379,6 +379,34 @@ void lbg_witness_free(lbg_witness* w) { witness_release(w); }
 // ---------------------------------------------------------------------------------------------
 // prover
 // ---------------------------------------------------------------------------------------------
+// The commit's grid over `cols` columns: column tiles x ring-element chunks. A wave of the commit
+// kernel is (SMs x resident CTAs) CTAs and its length is proportional to the chunk, so pick the
+// chunk count that minimises waves x chunk (ties: fewer chunks, fewer partial sums), with at most
+// max_partial chunk partials (chunks x cols) where the buffer is shared.
+static void commit_chunking(const lbg_pp* pp, int cols, long max_partial, int* chunk_out, int* nchunks_out) {
+  int col_tiles = (cols + commit_cols_per_cta() - 1) / commit_cols_per_cta();
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pp->device);
+  int slots = sms * commit_blocks_per_sm(pp->pidx[0]);
+  int step = commit_ring_per_step();
+  long best_cost = -1;
+  int max_chunks = (int)((pp->len_ring + step - 1) / step);
+  for (int nch = 1; nch <= max_chunks; nch++) {
+    int chunk = (int)((pp->len_ring + nch - 1) / nch);
+    chunk = (chunk + step - 1) / step * step;
+    int nact = (int)((pp->len_ring + chunk - 1) / chunk);
+    if ((long)nact * cols > max_partial) break;
+    long total = (long)col_tiles * nact;
+    long waves = (total + slots - 1) / slots;
+    long cost = waves * chunk;
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      *chunk_out = chunk;
+      *nchunks_out = nact;
+    }
+  }
+}
+
 static void free_bufs(OpeningBufs* b) {
   if (!b) return;
   cudaFree(b->d_C);
@@ -392,6 +420,11 @@ void lbg_prover_free(lbg_prover* pr) {
   if (!pr) return;
   cudaSetDevice(pr->pp->device);
   if (pr->stream) cudaStreamSynchronize(pr->stream);
+  if (pr->copy_stream) {
+    cudaStreamSynchronize(pr->copy_stream);
+    cudaStreamDestroy(pr->copy_stream);
+  }
+  for (auto e : pr->group_events) cudaEventDestroy(e);
   cudaFree(pr->d_partial);
   cudaFree(pr->d_vhat);
   cudaFree(pr->d_ch);
@@ -470,26 +503,9 @@ int lbg_prover_new(const lbg_pp* pp, lbg_prover** out) {
   // Grid: column tiles x ring-element chunks. A wave of the commit kernel is (SMs x resident CTAs)
   // CTAs and its length is proportional to the chunk, so pick the chunk count that minimises
   // waves x chunk (ties: fewer chunks, fewer partial sums).
-  int col_tiles = (int)((pp->cols + commit_cols_per_cta() - 1) / commit_cols_per_cta());
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pp->device);
-  int slots = sms * commit_blocks_per_sm(pp->pidx[0]);
-  int step = commit_ring_per_step();
-  long best_cost = -1;
-  int max_chunks = (int)((pp->len_ring + step - 1) / step);
-  for (int nch = 1; nch <= max_chunks; nch++) {
-    int chunk = (int)((pp->len_ring + nch - 1) / nch);
-    chunk = (chunk + step - 1) / step * step;
-    int nact = (int)((pp->len_ring + chunk - 1) / chunk);
-    long total = (long)col_tiles * nact;
-    long waves = (total + slots - 1) / slots;
-    long cost = waves * chunk;
-    if (best_cost < 0 || cost < best_cost) {
-      best_cost = cost;
-      pr->chunk = chunk;
-      pr->nchunks = nact;
-    }
-  }
+  commit_chunking(pp, (int)pp->cols, 1 << 30, &pr->chunk, &pr->nchunks);
   // the fold: position tiles x column splits, chosen the same way
   {
     int tiles = (int)((pp->wdim + fold_positions_per_cta() - 1) / fold_positions_per_cta());
@@ -646,6 +662,111 @@ int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16
     *opening_out = op;
   else
     lbg_opening_free(op);
+  return LBG_OK;
+}
+
+// Witness::from_elements + Prover::commit with the upload pipelined against the commit: the
+// witness (host memory; page-locked for the copies to overlap) arrives in column groups on the
+// prover's copy stream, and every limb's commit of a group starts on the compute stream as soon
+// as that group has landed. The results are those of lbg_witness_from_host + lbg_commit.
+int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* matrix_out, uint16_t* top_out,
+                    uint16_t* digits_out, lbg_witness** w_out, lbg_opening** opening_out) {
+  if (!pr || !f162 || !w_out) return fail(LBG_ERR_INVALID, "null argument");
+  *w_out = nullptr;
+  if (opening_out) *opening_out = nullptr;
+  const lbg_pp* pp = pr->pp;
+  if (n != pp->n) return fail(LBG_ERR_WITNESS, "the witness is not witness_len() elements");
+  LBG_CU(cudaSetDevice(pp->device));
+  const int cols = (int)pp->cols, L = pp->limbs;
+  // column groups of at least 128 columns, at most 8
+  int groups = 1;
+  while (groups < 8 && cols / (2 * groups) >= 128) groups *= 2;
+  const int gc = cols / groups;
+  int chunk = pr->chunk, nch = pr->nchunks;
+  if (groups > 1) commit_chunking(pp, gc, (long)pr->nchunks * cols, &chunk, &nch);
+  if (!pr->copy_stream && cudaStreamCreateWithFlags(&pr->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(LBG_ERR_CUDA, "copy stream");
+  while ((int)pr->group_events.size() < groups) {
+    cudaEvent_t ev;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail(LBG_ERR_CUDA, "event");
+    pr->group_events.push_back(ev);
+  }
+  lbg_witness* w;
+  int rc = witness_alloc(pp, n, &w);
+  if (rc) return rc;
+  OpeningBufs* b = nullptr;
+  rc = get_bufs(pr, &b);
+  if (rc) {
+    witness_release(w);
+    return rc;
+  }
+  cudaStream_t st = pr->stream, cp = pr->copy_stream;
+  const size_t per_col = pp->wdim * 3;  // u64 words of a column
+  cudaError_t e = cudaSuccess;
+  for (int g = 0; g < groups && e == cudaSuccess; g++) {
+    const size_t c0 = (size_t)g * gc;
+    e = cudaMemcpyAsync(w->d + c0 * per_col, f162 + c0 * per_col, (size_t)gc * per_col * 8, cudaMemcpyHostToDevice, cp);
+    if (e == cudaSuccess) e = cudaEventRecord(pr->group_events[g], cp);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, pr->group_events[g], 0);
+    for (int k = 0; k < L && e == cudaSuccess; k++) {
+      {
+        KernelScope ks(pr, "commit");
+        e = launch_commit(pp->pidx[k], w->d + c0 * per_col, pp->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2,
+                          pp->d_prime[k], gc, (int)pp->len_ring, chunk, nch, pr->d_partial, st,
+                          k == 0 && b->d_keep ? b->d_keep + c0 * pp->wdim * N162 : nullptr);
+      }
+      if (e == cudaSuccess) {
+        KernelScope ks(pr, "commit_finish");
+        e = launch_commit_finish(pp->pidx[k], pr->d_partial, nch, gc, pp->d_prime[k], k, L,
+                                 b->d_C + c0 * 4 * L * N162, st);
+      }
+    }
+  }
+  bool bd = pp->params.opening == LBG_OPENING_BIT_DROPPED;
+  size_t count = pp->cols * N648;
+  if (bd && e == cudaSuccess) {
+    for (int k = 0; k < L && e == cudaSuccess; k++) {
+      KernelScope ks(pr, "column_residues");
+      e = launch_column_residues(pp->pidx[k], b->d_C, cols, k, L, pp->d_prime[k], pr->d_res + (size_t)k * count, st);
+    }
+    if (e == cudaSuccess) {
+      GarnerConsts gcs;
+      std::memset(&gcs, 0, sizeof(gcs));
+      for (int k = 0; k < L; k++) {
+        gcs.q[k] = pp->primes[k];
+        for (int m = 0; m < k; m++) gcs.inv[k][m] = (uint32_t)inv_mod(pp->primes[m], pp->primes[k]);
+      }
+      gcs.dropped_bits = pp->params.dropped_bits;
+      KernelScope ks(pr, "garner");
+      e = launch_garner(pr->d_res, count, L, gcs, b->d_top, b->d_digits, st);
+    }
+  }
+  if (e == cudaSuccess && matrix_out && !bd)
+    e = cudaMemcpyAsync(matrix_out, b->d_C, pp->cols * 4 * L * N162 * 2, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && bd && top_out) e = cudaMemcpyAsync(top_out, b->d_top, count * 2, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && bd && digits_out && L > 1)
+    e = cudaMemcpyAsync(digits_out, b->d_digits, (size_t)(L - 1) * count * 2, cudaMemcpyDeviceToHost, st);
+  // the witness is complete once the compute stream has passed every group's event
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(cp);
+    {
+      std::lock_guard<std::mutex> g(pr->mu);
+      pr->spare.push_back(b);
+    }
+    witness_release(w);
+    return fail(LBG_ERR_CUDA, std::string("commit: ") + cudaGetErrorString(e));
+  }
+  lbg_opening* op = new lbg_opening();
+  op->pr = pr;
+  op->w = w;
+  w->refs.fetch_add(1);
+  op->bufs = b;
+  if (opening_out)
+    *opening_out = op;
+  else
+    lbg_opening_free(op);
+  *w_out = w;
   return LBG_OK;
 }
 

@@ -57,6 +57,8 @@ struct OpeningBufs;
 struct lbg_prover {
   const lbg_pp* pp = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;        // lbg_commit_host's uploads (created on first use)
+  std::vector<cudaEvent_t> group_events;     // one per column group of lbg_commit_host
   int chunk = 0, nchunks = 0;
   int fold_cols_per_split = 0;
   int32_t* d_partial = nullptr;

@@ -432,6 +432,29 @@ class Prover:
             c = Commitment(pr.primes(), r, matrix=m, params=pr)
         return c, CommitmentOpening(self, op)
 
+    def commit_elements(self, elements):
+        """Witness::from_elements then Prover::commit in one call, the upload of the elements
+        (uint64 [n][3]; page-locked for the copies to overlap) pipelined against the commit.
+        Returns (witness, commitment, opening)."""
+        pr = self.params
+        e = np.ascontiguousarray(elements, dtype=np.uint64).reshape(-1, 3)
+        if len(e) != pr.witness_len():
+            raise WitnessError("WrongLength")
+        L, r = len(pr.primes()), pr.columns()
+        op, wh = ctypes.c_void_p(), ctypes.c_void_p()
+        if pr.dropped_bits():
+            top = np.zeros(r * N, np.uint16)
+            digits = np.zeros((max(L - 1, 1), r * N), np.uint16)
+            check(lib().lbg_commit_host(self._h, ptr(e), len(e), None, ptr(top), ptr(digits), ctypes.byref(wh),
+                                        ctypes.byref(op)))
+            c = Commitment(pr.primes(), r, top=top, digits=digits[: L - 1], params=pr)
+        else:
+            m = np.zeros((r, 4, L, N162), np.int16)
+            check(lib().lbg_commit_host(self._h, ptr(e), len(e), ptr(m), None, None, ctypes.byref(wh),
+                                        ctypes.byref(op)))
+            c = Commitment(pr.primes(), r, matrix=m, params=pr)
+        return Witness(self.pp, wh), c, CommitmentOpening(self, op)
+
     def keep_transform(self, enable: bool = True):
         """Keep the base limb's transform from commit for the fold, or transform the witness again
         in the fold (the default); the results are the same."""

@@ -225,3 +225,34 @@ def test_errors_do_not_cross_the_boundary():
     # the prover still works after the rejected calls
     c2, op2 = prover.commit(w)
     assert np.array_equal(c.matrix, c2.matrix)
+
+
+@pytest.mark.parametrize("shape", [(20, 9, [3889, 2917, 4861], 0), (19, 8, [9721, 3889], 9), (14, 3, [2917], 0)],
+                         ids=["512-columns", "256-columns-bd", "8-columns"])
+def test_commit_from_host_memory_equals_upload_then_commit(shape):
+    """lbg_commit_host (the upload pipelined against the commit by column groups) gives the
+    commitment, the witness and, after the fold, the folded witness of Witness::from_elements +
+    Prover::commit."""
+    import labinius_b200 as L
+    from rounds import MATRIX_SEED, product_params
+
+    params = product_params(shape)
+    pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+    rng = np.random.default_rng(shape[0])
+    e = rng.integers(0, 2 ** 63, (params.witness_len(), 3), dtype=np.uint64)
+    e[:, 2] &= np.uint64((1 << 34) - 1)
+    prover = L.Prover(pp)
+    w1 = L.Witness.from_elements(pp, e)
+    c1, op1 = prover.commit(w1)
+    w2, c2, op2 = prover.commit_elements(e)
+    assert np.array_equal(w2.elements(), e)
+    if params.dropped_bits():
+        assert np.array_equal(c1.top, c2.top) and np.array_equal(c1.digits, c2.digits)
+    else:
+        assert np.array_equal(c1.matrix, c2.matrix)
+    ch = L.FoldingChallenges(np.zeros(params.columns(), L.CHALLENGE_DTYPE))
+    ch.challenges["weight"] = 28
+    ch.challenges["positions"][:, :28] = np.arange(0, 28 * 5, 5, dtype=np.uint8)
+    v1 = prover.fold(op1, ch)
+    v2 = prover.fold(op2, ch)
+    assert np.array_equal(v1.elements, v2.elements)
