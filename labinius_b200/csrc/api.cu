@@ -678,9 +678,9 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
   if (n != pp->n) return fail(LBG_ERR_WITNESS, "the witness is not witness_len() elements");
   LBG_CU(cudaSetDevice(pp->device));
   const int cols = (int)pp->cols, L = pp->limbs;
-  // column groups of at least 128 columns, at most 8
+  // column groups of at least 64 columns, at most 8
   int groups = 1;
-  while (groups < 8 && cols / (2 * groups) >= 128) groups *= 2;
+  while (groups < 8 && cols / (2 * groups) >= 64) groups *= 2;
   const int gc = cols / groups;
   int chunk = pr->chunk, nch = pr->nchunks;
   if (groups > 1) commit_chunking(pp, gc, (long)pr->nchunks * cols, &chunk, &nch);
