@@ -87,68 +87,60 @@ __device__ __forceinline__ uint32_t quotient(uint32_t x, uint64_t r) {
   return (uint32_t)(((uint64_t)x * (uint32_t)(r >> 32) + (lo >> 32)) >> 32);
 }
 
-// One thread per lane. cnt[i]: the words coefficient i pushed (0, 1 or 2); w2[2i ..]: those words in
-// the output's order (the reverse of the push order); states: the lanes' final states. The symbol
-// table is copied to shared memory when it fits (sym_smem), and each step's symbol is fetched one
-// step ahead of the state update that needs it.
-__global__ void __launch_bounds__(LANES) k_wire_lanes(const int16_t* __restrict__ v, size_t coefficients, int low,
+// One thread per lane. cnt[i]: the words coefficient i pushed (0, 1 or 2); w2[i]: those words in
+// the output's order (the reverse of the push order), the first in the low half; states: the
+// lanes' final states. The symbol table is copied to shared memory when it fits (sym_smem); the
+// step loop is unrolled so the table reads of later steps overlap a step's state update.
+__global__ void __launch_bounds__(LANES) k_wire_lanes(const int16_t* __restrict__ v, uint32_t coefficients, int low,
                                                       uint32_t length, uint32_t raw, const WireSym* __restrict__ gsyms,
                                                       int sym_smem, uint8_t* __restrict__ cnt,
-                                                      uint16_t* __restrict__ w2, uint32_t* __restrict__ states) {
-  __shared__ int16_t tile[TILE_GROUPS * LANES];
+                                                      uint32_t* __restrict__ w2, uint32_t* __restrict__ states) {
+  __shared__ __align__(16) int16_t tile[TILE_GROUPS * LANES];
   extern __shared__ WireSym ssyms[];
-  const int k = threadIdx.x;
+  const uint32_t k = threadIdx.x;
   if (sym_smem)
     for (uint32_t e = k; e <= length; e += LANES) ssyms[e] = gsyms[e];
   const WireSym* syms = sym_smem ? ssyms : gsyms;
-  const size_t groups = (coefficients + LANES - 1) / LANES;
+  const uint32_t groups = (coefficients + (uint32_t)LANES - 1) / (uint32_t)LANES;
   __syncthreads();
   const WireSym esc = syms[length];
   uint32_t x = RANS_LOW;
-  for (size_t end = groups; end > 0;) {
-    const size_t first = end > (size_t)TILE_GROUPS ? end - TILE_GROUPS : 0;
-    const size_t base = first * LANES, span = (end - first) * LANES;
-    for (size_t t = k; t < span; t += LANES) tile[t] = base + t < coefficients ? v[base + t] : 0;
+  for (uint32_t end = groups; end > 0;) {
+    const uint32_t first = end > (uint32_t)TILE_GROUPS ? end - TILE_GROUPS : 0;
+    const uint32_t base = first * (uint32_t)LANES, span = (end - first) * (uint32_t)LANES;
+    if (base + span <= coefficients) {  // 8 coefficients a load (base is a multiple of 64)
+      const uint4* src = reinterpret_cast<const uint4*>(v + base);
+      uint4* dst = reinterpret_cast<uint4*>(tile);
+      for (uint32_t t = k; t < span / 8; t += LANES) dst[t] = src[t];
+    } else {
+      for (uint32_t t = k; t < span; t += LANES) tile[t] = base + t < coefficients ? v[base + t] : 0;
+    }
     __syncthreads();
-    uint32_t s_next = (uint32_t)(tile[(end - 1 - first) * LANES + k] - low);
-    WireSym sym_next = syms[s_next < length ? s_next : length];
-    for (size_t g = end; g-- > first;) {
-      const size_t i = g * LANES + k;
-      const uint32_t s = s_next;
-      const WireSym sym = sym_next;
-      if (g > first) {  // the next step's symbol, ahead of this step's state update
-        s_next = (uint32_t)(tile[(g - 1 - first) * LANES + k] - low);
-        sym_next = syms[s_next < length ? s_next : length];
-      }
-      if (i >= coefficients) continue;
-      uint16_t pushed[2];
-      int n = 0;
-      auto put_symbol = [&](const WireSym& y) {
-        if ((x >> (32 - SCALE_BITS)) >= y.frequency) {  // renormalise
-          pushed[n++] = (uint16_t)x;
-          x >>= 16;
-        }
-        const uint32_t q = quotient(x, y.reciprocal);
-        x = (q << SCALE_BITS) + (x - q * y.frequency) + y.bias;
-      };
-      if (sym.frequency == 0) {  // the escape symbol after the raw index
+    const bool full = end * (uint32_t)LANES <= coefficients;  // every lane of this tile's groups is coded
+#pragma unroll 4
+    for (uint32_t g = end; g-- > first;) {
+      const uint32_t i = g * (uint32_t)LANES + k;
+      const uint32_t s = (uint32_t)(tile[(g - first) * LANES + k] - low);
+      WireSym y = syms[s < length ? s : length];
+      if (!full && i >= coefficients) continue;
+      uint32_t bits_word = 0, sym_word = 0, n_bits = 0, n_sym = 0;
+      if (y.frequency == 0) {  // the escape symbol after the raw index
         if (raw) {
-          if ((x >> (32 - raw)) != 0) {
-            pushed[n++] = (uint16_t)x;
-            x >>= 16;
-          }
+          n_bits = (x >> (32 - raw)) != 0;
+          bits_word = x & 0xFFFF;
+          x = n_bits ? x >> 16 : x;
           x = (x << raw) | s;
         }
-        put_symbol(esc);
-      } else {
-        put_symbol(sym);
+        y = esc;
       }
-      cnt[i] = (uint8_t)n;
-      if (n == 1) w2[2 * i] = pushed[0];
-      if (n == 2) {
-        w2[2 * i] = pushed[1];
-        w2[2 * i + 1] = pushed[0];
-      }
+      n_sym = (x >> (32 - SCALE_BITS)) >= y.frequency;  // renormalise
+      sym_word = x & 0xFFFF;
+      x = n_sym ? x >> 16 : x;
+      const uint32_t q = quotient(x, y.reciprocal);
+      x = (q << SCALE_BITS) + (x - q * y.frequency) + y.bias;
+      cnt[i] = (uint8_t)(n_bits + n_sym);
+      // output order: the symbol's word, then the raw bits' word
+      w2[i] = n_sym ? (sym_word | (n_bits ? bits_word << 16 : 0)) : bits_word;
     }
     __syncthreads();
     end = first;
@@ -195,7 +187,7 @@ __global__ void k_wire_scan_sums(uint32_t* __restrict__ sums, size_t nb, uint32_
 
 // sums[b] is now the inclusive scan of the block sums; element i's position is the block's
 // exclusive offset plus its exclusive rank within the block
-__global__ void k_wire_scatter(const uint8_t* __restrict__ cnt, const uint16_t* __restrict__ w2, size_t n,
+__global__ void k_wire_scatter(const uint8_t* __restrict__ cnt, const uint32_t* __restrict__ w2, size_t n,
                                const uint32_t* __restrict__ sums, uint8_t* __restrict__ out_words) {
   __shared__ uint32_t wsum[SCAN_BLOCK / 32];
   const size_t i = (size_t)blockIdx.x * SCAN_BLOCK + threadIdx.x;
@@ -219,8 +211,9 @@ __global__ void k_wire_scatter(const uint8_t* __restrict__ cnt, const uint16_t* 
   __syncthreads();
   const uint32_t block_off = blockIdx.x ? sums[blockIdx.x - 1] : 0;
   const uint32_t pos = block_off + (warp ? wsum[warp - 1] : 0) + incl - c;
+  const uint32_t ws = c ? w2[i] : 0;
   for (uint32_t e = 0; e < c; e++) {
-    const uint16_t w = w2[2 * i + e];
+    const uint32_t w = ws >> (16 * e);
     out_words[2 * (pos + e)] = (uint8_t)w;
     out_words[2 * (pos + e) + 1] = (uint8_t)(w >> 8);
   }
@@ -347,7 +340,7 @@ long long wire_encode_device(const int16_t* d_v, size_t elements, uint16_t base_
   unsigned long long* d_counts = nullptr;
   WireSym* d_syms = nullptr;
   uint8_t *d_cnt = nullptr, *d_out = nullptr;
-  uint16_t* d_w2 = nullptr;
+  uint32_t* d_w2 = nullptr;
   uint32_t *d_states = nullptr, *d_sums = nullptr, *d_total = nullptr;
   auto cuda_fail = [&](cudaError_t e) {
     cudaGetLastError();
@@ -410,8 +403,8 @@ long long wire_encode_device(const int16_t* d_v, size_t elements, uint16_t base_
     const int sym_smem = sym_bytes <= 160 * 1024;
     if (sym_smem)
       cudaFuncSetAttribute(k_wire_lanes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sym_bytes);
-    k_wire_lanes<<<1, LANES, sym_smem ? sym_bytes : 0, st>>>(d_v, n, low, length, raw, d_syms, sym_smem, d_cnt, d_w2,
-                                                             d_states);
+    k_wire_lanes<<<1, LANES, sym_smem ? sym_bytes : 0, st>>>(d_v, (uint32_t)n, low, length, raw, d_syms, sym_smem,
+                                                             d_cnt, d_w2, d_states);
     k_wire_scan_blocks<<<(unsigned)nb, SCAN_BLOCK, 0, st>>>(d_cnt, n, d_sums);
     k_wire_scan_sums<<<1, SCAN_BLOCK, 0, st>>>(d_sums, nb, d_total);
     e = cudaGetLastError();
