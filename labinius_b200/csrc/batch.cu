@@ -783,11 +783,7 @@ int lbg_batch_round(lbg_batch* b, const uint8_t* domain, size_t domain_len, cons
   }
   uint64_t per_round = 11 + 2 * pp->limbs + 3 +
                        (pp->params.opening == LBG_OPENING_BIT_DROPPED ? pp->limbs + 1 + b->count : 0);
-  if (!b->sw_h.empty()) {
-    uint32_t lmax = 0;
-    for (const SwInst& h : b->sw_h) lmax = std::max(lmax, h.l);
-    per_round += sw_launches(lmax);
-  }
+  per_round += sw_launches(b->sw_h.data(), (int)b->sw_h.size());
   if (b->graphs) {
     if (!b->g_round) {
       cudaGraph_t g = nullptr;

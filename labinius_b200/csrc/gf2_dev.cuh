@@ -129,6 +129,11 @@ __device__ __forceinline__ B128d b_times_x(B128d a) {
   uint64_t top = a.hi >> 63;
   return B128d{(a.lo << 1) ^ ((0 - top) & 0x87ull), (a.hi << 1) | (a.lo >> 63)};
 }
+// a * x^4: the four bits shifted past x^127 come back times x^7 + x^2 + x + 1.
+__device__ __forceinline__ B128d b_times_x4(B128d a) {
+  const uint64_t t = a.hi >> 60;
+  return B128d{(a.lo << 4) ^ (t << 7) ^ (t << 2) ^ (t << 1) ^ t, (a.hi << 4) | (a.lo >> 60)};
+}
 __device__ __forceinline__ B128d b_mul(B128d a, B128d b) {
   uint32_t A[5], B[4], c[8];
   A[0] = (uint32_t)a.lo;

@@ -86,11 +86,28 @@ __global__ void k_key_components(const int16_t* __restrict__ A, const DevPrime* 
 //           the column's 16) into smem What[ii][v][jj][k] (u16, in [0, 2q));
 //  phase B: lane l of warp w serves column l % 16 and the leaves v = 2 (w + 8 u) + l / 16; it
 //           accumulates Y_0..Y_3 of those leaves: 16 multiply-adds per (ring element, leaf).
+// Both global inputs arrive by asynchronous copies into shared memory: the step's key tile (the
+// four ring elements' Ahat, 20.7 KB contiguous) while phase A transforms, the next step's witness
+// tile while phase B multiplies.
 constexpr int CT = 16;   // columns per CTA
 constexpr int RT = 4;    // ring elements per step
 constexpr int VPT = 11;  // leaves per thread (8 warps x 2 halves x 11 >= 162)
-constexpr int WROW = RT * 12 + 1;          // staged witness words per column, padded
+constexpr int WROW = RT * 12 + 2;          // staged witness words per column, padded to 16 bytes
 constexpr int LUT_BYTES = 6 * 64 * 2;      // the six u16 tables
+constexpr int AT_BYTES = RT * N162 * 32;   // the step's key tile
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// all but the newest `N` of this thread's committed groups have landed
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 template <int PI>
 __device__ __forceinline__ void commit_phase_a_store(uint16_t* __restrict__ wt, int ii, int k, int jj,
@@ -125,14 +142,30 @@ __global__ void __launch_bounds__(256, 2)
              uint16_t* __restrict__ keep /* null, or the kept transform [cols][162][wdim] */) {
   extern __shared__ __align__(16) uint8_t smem[];
   uint16_t* lut = (uint16_t*)smem;                        // 6 * 64 u16
-  uint64_t* wtile = (uint64_t*)(smem + LUT_BYTES);        // CT rows of WROW u64 (one pad word)
+  uint64_t* wtile = (uint64_t*)(smem + LUT_BYTES);        // CT rows of WROW u64 (two pad words)
   uint16_t* wt = (uint16_t*)(smem + LUT_BYTES + CT * WROW * 8);  // RT * 162 * CT * 4 u16
+  int4* atile = (int4*)(smem + LUT_BYTES + CT * WROW * 8 + RT * N162 * CT * 4 * 2);  // [RT][162][2]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int j0 = blockIdx.x * CT;
   const int i_begin = blockIdx.y * chunk;
   const int i_end = min(len_ring, i_begin + chunk);
   for (int x = tid; x < 6 * 64; x += 256) lut[x] = (uint16_t)D->lut[x / 64][x % 64];
   const int jj_b = lane & 15, half = lane >> 4;
+  // the witness tile of the step at i0: column jj's 12 * nsteps words in place, zeros past the
+  // columns and ring elements of this CTA (plain stores to words no copy targets)
+  auto stage_witness = [&](int i0) {
+    const int words = 12 * min(RT, i_end - i0);
+    for (int x = tid; x < CT * RT * 12; x += 256) {
+      int jj = x / (RT * 12), wd = x % (RT * 12);
+      int j = j0 + jj;
+      if (j < cols && wd < words)
+        cp_async8(wtile + jj * WROW + wd, W + ((size_t)j * wdim + (size_t)4 * i0) * 3 + wd);
+      else
+        wtile[jj * WROW + wd] = 0;
+    }
+  };
+  if (i_begin < i_end) stage_witness(i_begin);
+  cp_async_commit();
 
   int32_t acc[VPT][4];
 #pragma unroll
@@ -141,16 +174,14 @@ __global__ void __launch_bounds__(256, 2)
   int since = 0;
 
   for (int i0 = i_begin; i0 < i_end; i0 += RT) {
-    __syncthreads();
-    // stage the witness tile: column jj, ring elements i0 .. i0+3 -> 16 F162 = 48 u64, contiguous
-    for (int x = tid; x < CT * RT * 12; x += 256) {
-      int jj = x / (RT * 12), wd = x % (RT * 12);
-      int j = j0 + jj;
-      uint64_t val = 0;
-      size_t f = (size_t)4 * i0 + wd / 3;  // F162 index inside the column
-      if (j < cols && f < (size_t)4 * i_end) val = W[((size_t)j * wdim + f) * 3 + wd % 3];
-      wtile[jj * WROW + wd] = val;
+    const int nsteps = min(RT, i_end - i0);
+    __syncthreads();  // the previous step's phase B is done with the key tile
+    {
+      const int4* src = Ahat + (size_t)i0 * N162 * 2;
+      for (int x = tid; x < nsteps * N162 * 2; x += 256) cp_async16(atile + x, src + x);
     }
+    cp_async_commit();
+    cp_async_wait<1>();  // this step's witness tile
     __syncthreads();
     {
       // lanes run over columns, so a warp's What stores hit 16 distinct banks
@@ -161,7 +192,8 @@ __global__ void __launch_bounds__(256, 2)
       commit_phase_a_store<PI>(wt, g >> 2, g & 3, jj, idx, (const uint8_t*)lut);
     }
     __syncthreads();
-    const int nsteps = min(RT, i_end - i0);
+    if (i0 + RT < i_end) stage_witness(i0 + RT);
+    cp_async_commit();
     if constexpr (KEEP) {
       // the kept transform (the fold's input) in blocks of 16 positions: keep[j][p / 16][v][p % 16],
       // p = 4 i + k, so this tile of a column is one contiguous 5184-byte block; a lane pair writes
@@ -180,15 +212,17 @@ __global__ void __launch_bounds__(256, 2)
         }
       }
     }
+    cp_async_wait<1>();  // this step's key tile
+    __syncthreads();
     for (int ii = 0; ii < nsteps; ii++) {
-      const int4* ah = Ahat + (size_t)(i0 + ii) * N162 * 2;
+      const int4* ah = atile + ii * N162 * 2;
 #pragma unroll
       for (int u = 0; u < VPT; u++) {
         int v = 2 * (warp + 8 * u) + half;
         if (v < N162) {
           uint2 wv = *(const uint2*)(wt + (((ii * N162) + v) * CT + jj_b) * 4);
           int32_t w0 = wv.x & 0xFFFF, w1 = wv.x >> 16, w2 = wv.y & 0xFFFF, w3 = wv.y >> 16;
-          int4 lo = __ldg(ah + 2 * v), hi = __ldg(ah + 2 * v + 1);
+          int4 lo = ah[2 * v], hi = ah[2 * v + 1];
           acc[u][0] += lo.x * w0 + hi.x * w3 + hi.y * w2 + hi.z * w1;
           acc[u][1] += lo.y * w0 + lo.x * w1 + hi.y * w3 + hi.z * w2;
           acc[u][2] += lo.z * w0 + lo.y * w1 + lo.x * w2 + hi.z * w3;
@@ -1326,7 +1360,7 @@ cudaError_t launch_key_components(int pi, const int16_t* A, const DevPrime* D, i
   return cudaGetLastError();
 }
 
-size_t commit_smem_bytes() { return LUT_BYTES + CT * WROW * 8 + RT * N162 * CT * 4 * 2; }
+size_t commit_smem_bytes() { return LUT_BYTES + CT * WROW * 8 + RT * N162 * CT * 4 * 2 + AT_BYTES; }
 
 int commit_blocks_per_sm(int pi) {
   int n = 0;

@@ -49,11 +49,17 @@ __constant__ char c_sw_round[22] = "labinius/switch-round";
 
 // Work units of an instance with l variables in a launch: stage 0 counts elements, stage 1 the
 // pairs of round 0's message, stage 2 the work of round k's fold (the pairs of round k + 1's
-// message, or the one pair of the last fold; none once the instance's rounds are done).
+// message, or the one pair of the last fold; none once the instance's rounds are done); stages 3
+// and 4 split the eq expansion: elements of instances whose low half-table is short (stage 3),
+// segments of 2^ll entries that share their high factor otherwise (stage 4).
+constexpr uint32_t SW_SEG_LL = 10;
 __host__ __device__ inline uint64_t sw_units(uint32_t l, int stage, int k) {
   uint64_t n = 1ull << l;
+  const uint32_t ll = l - l / 2;
   if (stage == 0) return n;
   if (stage == 1) return n / 2;
+  if (stage == 3) return ll < SW_SEG_LL ? n : 0;
+  if (stage == 4) return ll < SW_SEG_LL ? 0 : 1ull << (l / 2);
   if ((uint32_t)k >= l) return 0;
   if ((uint32_t)k + 1 == l) return 1;
   return n >> (k + 2);
@@ -129,13 +135,57 @@ __global__ void k_sw_tables(const SwInst* __restrict__ I) {
 
 __global__ void __launch_bounds__(SW_THREADS) k_sw_eq(const SwInst* __restrict__ I, int count) {
   uint32_t local, nblk;
-  int i = sw_find(I, count, 0, 0, SW_THREADS, local, nblk);
+  int i = sw_find(I, count, 3, 0, SW_THREADS, local, nblk);
   if (i < 0) return;
   const SwInst& s = I[i];
   size_t n = 1ull << s.l;
   uint64_t lm = (1ull << s.ll) - 1;
   for (size_t j = (size_t)local * SW_THREADS + threadIdx.x; j < n; j += (size_t)nblk * SW_THREADS)
     st_b(s.eq, j, b_mul(ld_b(s.e_hi, j >> s.ll), ld_b(s.e_lo, j & lm)));
+}
+
+// eq over segments: the 2^ll entries j = (a << ll) | b share e_hi[a], so a block builds the tables
+// of (t x^{4c}) e_hi[a] (32 nibble positions, 16 values) once and multiplies every e_lo[b] by 32
+// lookups.
+__global__ void __launch_bounds__(SW_THREADS) k_sw_eq_seg(const SwInst* __restrict__ I, int count) {
+  __shared__ B128d T[32 * 16];
+  __shared__ B128d R4[32];
+  uint32_t local, nblk;
+  int i = sw_find(I, count, 4, 0, 1, local, nblk);
+  if (i < 0) return;
+  const SwInst& s = I[i];
+  const uint32_t nseg = 1u << s.lh, seglen = 1u << s.ll;
+  for (uint32_t a = local; a < nseg; a += nblk) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      B128d r = ld_b(s.e_hi, a);
+      for (int c = 0; c < 32; c++) {
+        R4[c] = r;
+        r = b_times_x4(r);
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) {
+      const int c = e >> 4, t = e & 15;
+      B128d x = R4[c], acc{0, 0};
+      for (int b = 0; b < 4; b++) {
+        if ((t >> b) & 1) acc = b_add(acc, x);
+        x = b_times_x(x);
+      }
+      T[e] = acc;
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < seglen; b += blockDim.x) {
+      const B128d lo = ld_b(s.e_lo, b);
+      B128d acc{0, 0};
+#pragma unroll
+      for (int c = 0; c < 32; c++) {
+        const uint32_t nib = (uint32_t)((c < 16 ? lo.lo >> (4 * c) : lo.hi >> (4 * (c - 16))) & 15);
+        acc = b_add(acc, T[16 * c + nib]);
+      }
+      st_b(s.eq, ((size_t)a << s.ll) + b, acc);
+    }
+  }
 }
 
 // 8 x 8 bit transpose: byte r of x is row r (bit b = column b); on exit byte b holds column b
@@ -418,11 +468,13 @@ __device__ __forceinline__ F162d psi_of(const F162d* __restrict__ tab, B128d e) 
   return acc;
 }
 
-// x r through the round's tables: T[16 i + t] = (t x^{4i}) r, 41 nibble positions.
+// x r through the round's tables: T[16 i + t] = (t x^{4i}) r, 41 nibble positions (32 when x
+// has at most 128 bits).
+template <int POS = 41>
 __device__ __forceinline__ F162d cmul(const F162d* __restrict__ T, F162d x) {
   F162d acc{{0, 0, 0}};
 #pragma unroll
-  for (int i = 0; i < 41; i++) {
+  for (int i = 0; i < POS; i++) {
     uint32_t nib = (uint32_t)(x.w[i >> 4] >> (4 * (i & 15))) & 15;
     acc = f_add(acc, T[16 * i + nib]);
   }
@@ -512,6 +564,10 @@ __global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
   }
   __syncthreads();
   dev::hs_copy(s.st, &sh);
+  if (k == 0) {
+    const F162d r = R4[0];
+    for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) st_f(&sm->rpsi[0][0], e, f_mul(ld_f(&sm->psi[0][0], e), r));
+  }
   for (int e = threadIdx.x; e < 41 * 16; e += blockDim.x) {
     int q = e >> 4, t = e & 15;
     F162d x = R4[q], acc{{0, 0, 0}};
@@ -529,24 +585,29 @@ __global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
 // folded ones; later rounds fold in place.
 template <bool FIRST>
 __global__ void __launch_bounds__(SW_THREADS) k_sw_fold(const SwInst* __restrict__ I, int count, int k) {
-  __shared__ F162d T[41 * 16];
+  // round 0 multiplies only 128-bit words (trace pairs) by r, so it needs 32 of the 41 positions
+  __shared__ F162d T[(FIRST ? 32 : 41) * 16];
   __shared__ F162d psi[FIRST ? 512 : 1];
+  __shared__ F162d rpsi[FIRST ? 512 : 1];
   uint32_t local, nblk;
   int i = sw_find(I, count, 2, k, SW_THREADS, local, nblk);
   if (i < 0) return;
   const SwInst& s = I[i];
-  load_table(T, &s.s->rtab[0][0], 41 * 16);
-  if (FIRST) load_table(psi, &s.s->psi[0][0], 512);
+  load_table(T, &s.s->rtab[0][0], (FIRST ? 32 : 41) * 16);
+  if (FIRST) {
+    load_table(psi, &s.s->psi[0][0], 512);
+    load_table(rpsi, &s.s->rpsi[0][0], 512);
+  }
   __syncthreads();
   const size_t half = (1ull << s.l) >> (k + 1);
   // the folded entry x (x < half) of both tables
   auto fold_at = [&](size_t x, F162d& na, F162d& np) {
     if (FIRST) {
+      // psi is GF(2)-linear, so r psi(q0 + q1) reads r psi's own tables
       B128d q0 = ld_b(s.eq, x), q1 = ld_b(s.eq, x + half);
-      F162d a0 = psi_of(psi, q0);
-      na = f_add(a0, cmul(T, psi_of(psi, b_add(q0, q1))));
+      na = f_add(psi_of(psi, q0), psi_of(rpsi, b_add(q0, q1)));
       F162d p0 = ld_word(s.w, x), p1 = ld_word(s.w, x + half);
-      np = f_add(p0, cmul(T, f_add(p0, p1)));
+      np = f_add(p0, cmul<32>(T, f_add(p0, p1)));
     } else {
       F162d a0 = ld_f(s.a, x), a1 = ld_f(s.a, x + half);
       na = f_add(a0, cmul(T, f_add(a0, a1)));
@@ -621,6 +682,18 @@ void sw_layout(SwInst& I, uint8_t* base) {
   I.p = (uint64_t*)base;
 }
 
+uint64_t sw_launches(const SwInst* h, int count) {
+  if (count <= 0) return 0;
+  uint32_t lmax = 0;
+  bool short_eq = false, seg_eq = false;
+  for (int i = 0; i < count; i++) {
+    lmax = std::max(lmax, h[i].l);
+    short_eq |= sw_units(h[i].l, 3, 0) > 0;
+    seg_eq |= sw_units(h[i].l, 4, 0) > 0;
+  }
+  return 5 + (short_eq ? 1 : 0) + (seg_eq ? 1 : 0) + 2 * (uint64_t)lmax;
+}
+
 cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStream_t st, uint64_t* launches) {
   if (count <= 0) return cudaSuccess;
   uint32_t lmax = 0, tabmax = 0;
@@ -634,7 +707,8 @@ cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStre
     return (unsigned)t;
   };
   k_sw_tables<<<dim3((tabmax + 127) / 128, count), 128, 0, st>>>(d);
-  k_sw_eq<<<blocks(0, 0, SW_THREADS), SW_THREADS, 0, st>>>(d, count);
+  if (unsigned g = blocks(3, 0, SW_THREADS)) k_sw_eq<<<g, SW_THREADS, 0, st>>>(d, count);
+  if (unsigned g = blocks(4, 0, 1)) k_sw_eq_seg<<<g, SW_THREADS, 0, st>>>(d, count);
   k_sw_sums<<<dim3(blocks(1, 0, SW_SUM_ROWS), 3), SW_THREADS, 0, st>>>(d, count);
   k_sw_statement<<<count, 128, 0, st>>>(d);
   k_sw_batch<<<count, 256, 0, st>>>(d);
@@ -647,7 +721,7 @@ cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStre
       k_sw_fold<false><<<g, SW_THREADS, 0, st>>>(d, count, (int)k);
   }
   k_sw_finish<<<(count + 31) / 32, 32, 0, st>>>(d, count);
-  if (launches) *launches += sw_launches(lmax);
+  if (launches) *launches += sw_launches(h, count);
   return cudaGetLastError();
 }
 

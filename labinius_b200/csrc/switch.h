@@ -24,6 +24,7 @@ struct SwSmall {
   uint64_t rounds[32][6];     // the round messages
   uint64_t rtab[41 * 16][3];  // the running round's products by its challenge r: (t x^(4i)) r at 16 i + t
   uint64_t psi[32 * 16][3];   // psi by nibble: the XOR of batch[4c + b] over the set bits b of t at 16 c + t
+  uint64_t rpsi[32 * 16][3];  // the same times round 0's challenge
   uint64_t opened[3];
   uint32_t status;            // 0 once the instance's switch has run
   uint32_t pad_;
@@ -63,8 +64,8 @@ void sw_layout(SwInst& inst, uint8_t* base);
 cudaError_t enqueue_switch(const SwInst* d_inst, const SwInst* h_inst, int count, cudaStream_t st,
                            uint64_t* launches);
 
-// Launches of enqueue_switch when the longest instance has lmax variables.
-inline uint64_t sw_launches(uint32_t lmax) { return 6 + 2 * (uint64_t)lmax; }
+// Launches of enqueue_switch for the instances h[0..count).
+uint64_t sw_launches(const SwInst* h, int count);
 
 // Transcript bytes a word-level (nlo = 0) or bit-level (nlo = 7) switch over l variables absorbs.
 inline uint64_t sw_transcript_bytes(uint32_t l, uint32_t nlo) {
