@@ -89,6 +89,27 @@ __device__ __forceinline__ void bytes_to_words(const uint8_t* b, uint32_t* w, in
            ((uint32_t)b[4 * i + 3] << 24);
 }
 
+// One out-of-line copy of the compression for the single-thread transcript steps below: their
+// kernels run it a handful of times per launch, and one shared copy of its code stays in the
+// instruction cache where a copy inlined at every call site would be fetched cold each time.
+static __device__ __noinline__ void compress_ool(const uint32_t cv[8], const uint32_t msg[16], uint64_t counter,
+                                                 uint32_t block_len, uint32_t flags, uint32_t out[16]) {
+  compress(cv, msg, counter, block_len, flags, out);
+}
+static __device__ __forceinline__ void parent_cv_ool(const uint32_t key[8], uint32_t flags, const uint32_t l[8],
+                                                     const uint32_t r[8], uint32_t out[8]) {
+  uint32_t m[16], o[16];
+  for (int i = 0; i < 8; i++) {
+    m[i] = l[i];
+    m[8 + i] = r[i];
+  }
+  compress_ool(key, m, 0, 64, flags | b3::PARENT, o);
+  for (int i = 0; i < 8; i++) out[i] = o[i];
+}
+static __device__ __forceinline__ void root_block_ool(const XofRoot& r, uint64_t t, uint32_t out[16]) {
+  compress_ool(r.cv, r.m, t, r.block_len, r.flags | b3::ROOT, out);
+}
+
 // Output block t of a finalized hasher (its root node): 64 bytes as 16 words.
 __device__ __forceinline__ void root_block(const XofRoot& r, uint64_t t, uint32_t out[16]) {
   compress(r.cv, r.m, t, r.block_len, r.flags | b3::ROOT, out);
@@ -241,14 +262,14 @@ __device__ inline uint32_t hs_absorb_staged(HasherState* s, const uint32_t* stag
     uint32_t m[16], o[16];
     for (int q = 0; q < 16; q++) m[q] = stage[off / 4 + q];
     if (s->blocks == 15) {
-      compress(s->cv, m, s->chunk_counter, 64, s->flags | b3::CHUNK_END, o);
+      compress_ool(s->cv, m, s->chunk_counter, 64, s->flags | b3::CHUNK_END, o);
       s->chunk_counter++;
       uint64_t chunks = s->chunk_counter;
       uint32_t cur[8];
       for (int i = 0; i < 8; i++) cur[i] = o[i];
       while ((chunks & 1) == 0 && s->stack_len > 0) {
         s->stack_len--;
-        parent_cv(s->key, s->flags, s->stack[s->stack_len], cur, cur);
+        parent_cv_ool(s->key, s->flags, s->stack[s->stack_len], cur, cur);
         chunks >>= 1;
       }
       if (s->stack_len < 54) {
@@ -258,7 +279,7 @@ __device__ inline uint32_t hs_absorb_staged(HasherState* s, const uint32_t* stag
       for (int i = 0; i < 8; i++) s->cv[i] = s->key[i];
       s->blocks = 0;
     } else {
-      compress(s->cv, m, s->chunk_counter, 64, s->flags | (s->blocks == 0 ? b3::CHUNK_START : 0), o);
+      compress_ool(s->cv, m, s->chunk_counter, 64, s->flags | (s->blocks == 0 ? b3::CHUNK_START : 0), o);
       for (int i = 0; i < 8; i++) s->cv[i] = o[i];
       s->blocks++;
     }
@@ -280,20 +301,20 @@ __device__ inline void hs_derive_staged(const HasherState* s, const uint32_t* st
     uint32_t m[16], o[16];
     for (int q = 0; q < 16; q++) m[q] = stage[off / 4 + q];
     if (blocks == 15) {
-      compress(cv, m, chunks, 64, s->flags | b3::CHUNK_END, o);
+      compress_ool(cv, m, chunks, 64, s->flags | b3::CHUNK_END, o);
       chunks++;
       uint64_t t = chunks;
       for (int i = 0; i < 8; i++) extra[i] = o[i];
       while ((t & 1) == 0 && base_len > 0) {
         base_len--;
-        parent_cv(s->key, s->flags, s->stack[base_len], extra, extra);
+        parent_cv_ool(s->key, s->flags, s->stack[base_len], extra, extra);
         t >>= 1;
       }
       has_extra = true;
       for (int i = 0; i < 8; i++) cv[i] = s->key[i];
       blocks = 0;
     } else {
-      compress(cv, m, chunks, 64, s->flags | (blocks == 0 ? b3::CHUNK_START : 0), o);
+      compress_ool(cv, m, chunks, 64, s->flags | (blocks == 0 ? b3::CHUNK_START : 0), o);
       for (int i = 0; i < 8; i++) cv[i] = o[i];
       blocks++;
     }
@@ -307,7 +328,7 @@ __device__ inline void hs_derive_staged(const HasherState* s, const uint32_t* st
   int entries = (int)base_len + (has_extra ? 1 : 0);
   for (int e = entries - 1; e >= 0; e--) {
     uint32_t o[16];
-    compress(cv, m, counter, block_len, fl, o);
+    compress_ool(cv, m, counter, block_len, fl, o);
     const uint32_t* left = e >= (int)base_len ? extra : s->stack[e];
     for (int i = 0; i < 8; i++) {
       m[i] = left[i];

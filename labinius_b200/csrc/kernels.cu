@@ -93,7 +93,7 @@ constexpr int CT = 16;   // columns per CTA
 constexpr int RT = 4;    // ring elements per step
 constexpr int VPT = 11;  // leaves per thread (8 warps x 2 halves x 11 >= 162)
 constexpr int WROW = RT * 12 + 2;          // staged witness words per column, padded to 16 bytes
-constexpr int LUT_BYTES = 6 * 64 * 2;      // the six u16 tables
+constexpr int LUT_BYTES = NTT_LUT_U16 * 2;  // the transform's window tables
 constexpr int AT_BYTES = RT * N162 * 32;   // the step's key tile
 
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(256, 2)
              int32_t* __restrict__ partial /* [nchunks][cols][162][4] */,
              uint16_t* __restrict__ keep /* null, or the kept transform [cols][162][wdim] */) {
   extern __shared__ __align__(16) uint8_t smem[];
-  uint16_t* lut = (uint16_t*)smem;                        // 6 * 64 u16
+  uint16_t* lut = (uint16_t*)smem;                        // NTT_LUT_U16 u16
   uint64_t* wtile = (uint64_t*)(smem + LUT_BYTES);        // CT rows of WROW u64 (two pad words)
   uint16_t* wt = (uint16_t*)(smem + LUT_BYTES + CT * WROW * 8);  // RT * 162 * CT * 4 u16
   int4* atile = (int4*)(smem + LUT_BYTES + CT * WROW * 8 + RT * N162 * CT * 4 * 2);  // [RT][162][2]
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(256, 2)
   const int j0 = blockIdx.x * CT;
   const int i_begin = blockIdx.y * chunk;
   const int i_end = min(len_ring, i_begin + chunk);
-  for (int x = tid; x < 6 * 64; x += 256) lut[x] = (uint16_t)D->lut[x / 64][x % 64];
+  load_ntt_lut<PI>(lut, D);
   const int jj_b = lane & 15, half = lane >> 4;
   // the witness tile of the step at i0: column jj's 12 * nsteps words in place, zeros past the
   // columns and ring elements of this CTA (plain stores to words no copy targets)
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(256, 2)
   const size_t p0 = (size_t)blockIdx.x * FP;
   const int c_begin = blockIdx.y * cols_per_split;
   const int c_end = min(cols, c_begin + cols_per_split);
-  for (int x = tid; x < 6 * 64; x += 256) lut[x] = (uint16_t)D->lut[x / 64][x % 64];
+  load_ntt_lut<PI>(lut, D);
   uint32_t acc[VPW];
 #pragma unroll
   for (int u = 0; u < VPW; u++) acc[u] = 0;

@@ -95,6 +95,19 @@ __device__ __forceinline__ void bfly3(uint32_t& a0, uint32_t& a1, uint32_t& a2, 
   a2 = b - t1 - m;
 }
 
+// The same butterfly when a1 and a2 arrive already multiplied by z and z^2 (t1 = z a1, t2 = z^2 a2,
+// both in [0, q)): only the omega product is left, and every output stays within bfly3's bound.
+template <int PI>
+__device__ __forceinline__ void bfly3_scaled(uint32_t& a0, uint32_t& t1, uint32_t& t2, uint32_t om, uint32_t oms) {
+  constexpr uint32_t q = Pr<PI>::q;
+  uint32_t m = mul_shoup(t1 - t2 + 2 * q, om, oms, q);
+  uint32_t b = a0 + 4 * q;
+  uint32_t y0 = a0 + t1 + t2, y1 = b - t2 + m, y2 = b - t1 - m;
+  a0 = y0;
+  t1 = y1;
+  t2 = y2;
+}
+
 // The 27 six-bit LUT indices of one F162, as byte offsets into a u16 table (2 x index, one per
 // byte, four per word): index m collects bits m + 27 t, t = 0..5, of the element, the
 // coefficients that levels 0 and 1 of the tree combine.
@@ -119,9 +132,23 @@ __device__ __forceinline__ void f162_windows(uint64_t w0, uint64_t w1, uint64_t 
   }
 }
 
+// The shared-memory window tables of the transform: per block tau three 64-entry u16 tables of
+// 128 bytes each (one row of the 32 banks, so the 32 lanes' lookups never conflict): the window
+// values (levels 0 and 1 at once), and the same times the block's level-2 twiddle z and z^2, so
+// that level 2 reads its products instead of computing them.
+constexpr int NTT_LUT_U16 = 6 * 3 * 64;
+template <int PI>
+__device__ __forceinline__ void load_ntt_lut(uint16_t* __restrict__ lut, const DevPrime* __restrict__ D) {
+  for (int x = threadIdx.x; x < NTT_LUT_U16; x += blockDim.x) {
+    const int tau = x / 192, g = (x / 64) % 3;
+    uint32_t v = D->lut[tau][x % 64];
+    if (g) v = red_full<PI>(v * (g == 1 ? c_hot[PI].tw[tau][0].z : c_hot[PI].tw[tau][0].z2));
+    lut[x] = (uint16_t)v;
+  }
+}
+
 // Forward transform of one level-2 block (27 leaves) of one F162: v[x] = w(theta^{E[27 tau + x]}),
-// reduced to [0, 2q). `lut` holds the six blocks' 64-entry u16 tables in shared memory: 128 bytes
-// a block, one row of the 32 banks, so the 32 lanes' lookups never conflict.
+// reduced to [0, 2q), from the tables load_ntt_lut wrote.
 template <int PI, int TAU>
 __device__ __forceinline__ void ntt_block(const uint32_t idx[7], const uint8_t* __restrict__ lut,
                                           uint32_t v[27]) {
@@ -129,9 +156,9 @@ __device__ __forceinline__ void ntt_block(const uint32_t idx[7], const uint8_t* 
   const uint32_t om = H.omega, oms = H.omega_s;
 #pragma unroll
   for (int m = 0; m < 27; m++)
-    v[m] = *(const uint16_t*)(lut + TAU * 128 + __byte_perm(idx[m >> 2], 0, 0x4440 | (m & 3)));
+    v[m] = *(const uint16_t*)(lut + TAU * 384 + (m / 9) * 128 + __byte_perm(idx[m >> 2], 0, 0x4440 | (m & 3)));
 #pragma unroll
-  for (int i = 0; i < 9; i++) bfly3<PI>(v[i], v[9 + i], v[18 + i], H.tw[TAU][0], om, oms);
+  for (int i = 0; i < 9; i++) bfly3_scaled<PI>(v[i], v[9 + i], v[18 + i], om, oms);
 #pragma unroll
   for (int s = 0; s < 3; s++)
 #pragma unroll

@@ -47,9 +47,16 @@ __constant__ char c_sw_label[16] = "labinius/switch";
 __constant__ char c_sw_batch[22] = "labinius/switch-batch";
 __constant__ char c_sw_round[22] = "labinius/switch-round";
 
+// Rounds from sw_tail_start(l) on run in k_sw_tail: their messages sum at most 2^(SW_TAIL_LOG - 2)
+// pairs, little enough for one block, so the rounds that are left cost no launches.
+constexpr uint32_t SW_TAIL_LOG = 10;
+__host__ __device__ inline uint32_t sw_tail_start(uint32_t l) {
+  return l > SW_TAIL_LOG ? l - SW_TAIL_LOG : (l > 0 ? 1u : 0u);
+}
+
 // Work units of an instance with l variables in a launch: stage 0 counts elements, stage 1 the
 // pairs of round 0's message, stage 2 the work of round k's fold (the pairs of round k + 1's
-// message, or the one pair of the last fold; none once the instance's rounds are done); stages 3
+// message, or the one pair of the last fold; none from the instance's tail on); stages 3
 // and 4 split the eq expansion: elements of instances whose low half-table is short (stage 3),
 // segments of 2^ll entries that share their high factor otherwise (stage 4).
 constexpr uint32_t SW_SEG_LL = 10;
@@ -60,7 +67,7 @@ __host__ __device__ inline uint64_t sw_units(uint32_t l, int stage, int k) {
   if (stage == 1) return n / 2;
   if (stage == 3) return ll < SW_SEG_LL ? n : 0;
   if (stage == 4) return ll < SW_SEG_LL ? 0 : 1ull << (l / 2);
-  if ((uint32_t)k >= l) return 0;
+  if ((uint32_t)k >= sw_tail_start(l)) return 0;
   if ((uint32_t)k + 1 == l) return 1;
   return n >> (k + 2);
 }
@@ -394,7 +401,7 @@ __global__ void k_sw_statement(const SwInst* __restrict__ I) {
     XofRoot root;
     dev::hs_derive_staged(&sh, stage, dtotal, root);
     uint32_t out[48];
-    for (int t = 0; t < 3; t++) dev::root_block(root, t, out + 16 * t);
+    for (int t = 0; t < 3; t++) dev::root_block_ool(root, t, out + 16 * t);
     for (int c = 0; c < 7; c++) {
       for (int w = 0; w < 3; w++) sm->rp[c][w] = (uint64_t)out[6 * c + 2 * w] | ((uint64_t)out[6 * c + 2 * w + 1] << 32);
       sm->rp[c][2] &= (1ull << 34) - 1;
@@ -499,27 +506,17 @@ __device__ __forceinline__ void xor_reduce_store(F162d e0, F162d ei, uint64_t* m
   }
 }
 
-// One block per instance whose round k is due: the round's message into the transcript and
+// The transcript step of round k of one instance, on the whole block (it ends with a barrier):
+// the round's message msg (six words in shared memory) recorded and absorbed, then
 // sample_f162("labinius/switch-round", 1) (crates/pcs/src/switch.rs:152-159), both staged behind
-// the shared hasher's open block; the message accumulators cleared; the tables of (t x^{4i}) r
-// for the fold.
-__global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
-  const SwInst& s = I[blockIdx.x];
-  if ((uint32_t)k >= s.l) return;
+// the open block of sh, the block's shared copy of the instance's transcript hasher; the challenge
+// recorded and R4[i] = r x^{4i}, i < 41.
+__device__ void sw_transcript_step(const SwInst& s, int k, HasherState& sh, const uint64_t* msg, F162d* R4) {
   SwSmall* sm = s.s;
-  __shared__ HasherState sh;
-  __shared__ F162d R4[41];
-  __shared__ uint64_t msg[6];
   __shared__ uint32_t stage[32];
   __shared__ uint32_t last;
   uint8_t* bytes = reinterpret_cast<uint8_t*>(stage);
-  dev::hs_copy(&sh, s.st);
-  if (threadIdx.x < 6) msg[threadIdx.x] = sm->msg[threadIdx.x];
-  __syncthreads();
-  if (threadIdx.x < 6) {
-    sm->rounds[k][threadIdx.x] = msg[threadIdx.x];
-    sm->msg[threadIdx.x] = 0;
-  }
+  if (threadIdx.x < 6) sm->rounds[k][threadIdx.x] = msg[threadIdx.x];
   // absorb_f162(&msg): the open block, le64(2), the six words
   const uint32_t bl = sh.buf_len, total = bl + 56;
   for (uint32_t b = threadIdx.x; b < 128; b += blockDim.x) {
@@ -552,7 +549,7 @@ __global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
     XofRoot root;
     dev::hs_derive_staged(&sh, stage, dtotal, root);
     uint32_t out[16];
-    dev::root_block(root, 0, out);
+    dev::root_block_ool(root, 0, out);
     F162d r;
     for (int w = 0; w < 3; w++) r.w[w] = (uint64_t)out[2 * w] | ((uint64_t)out[2 * w + 1] << 32);
     r.w[2] &= (1ull << 34) - 1;
@@ -563,20 +560,39 @@ __global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
     }
   }
   __syncthreads();
+}
+
+// Entry e of the round's product tables: (t x^{4i}) r at e = 16 i + t, from R4[i] = r x^{4i}.
+__device__ __forceinline__ F162d rtab_entry(const F162d* R4, int e) {
+  F162d x = R4[e >> 4], acc{{0, 0, 0}};
+  for (int b = 0; b < 4; b++) {
+    if ((e >> b) & 1) acc = f_add(acc, x);
+    x = f_times_x(x);
+  }
+  return acc;
+}
+
+// One block per instance whose round k is due (k below its tail): the round's transcript step;
+// the message accumulators cleared; the tables of (t x^{4i}) r for the fold, and for round 0 the
+// psi tables times r.
+__global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
+  const SwInst& s = I[blockIdx.x];
+  if ((uint32_t)k >= sw_tail_start(s.l)) return;
+  SwSmall* sm = s.s;
+  __shared__ HasherState sh;
+  __shared__ F162d R4[41];
+  __shared__ uint64_t msg[6];
+  dev::hs_copy(&sh, s.st);
+  if (threadIdx.x < 6) msg[threadIdx.x] = sm->msg[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x < 6) sm->msg[threadIdx.x] = 0;
+  sw_transcript_step(s, k, sh, msg, R4);
   dev::hs_copy(s.st, &sh);
   if (k == 0) {
     const F162d r = R4[0];
     for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) st_f(&sm->rpsi[0][0], e, f_mul(ld_f(&sm->psi[0][0], e), r));
   }
-  for (int e = threadIdx.x; e < 41 * 16; e += blockDim.x) {
-    int q = e >> 4, t = e & 15;
-    F162d x = R4[q], acc{{0, 0, 0}};
-    for (int b = 0; b < 4; b++) {
-      if ((t >> b) & 1) acc = f_add(acc, x);
-      x = f_times_x(x);
-    }
-    st_f(&sm->rtab[0][0], e, acc);
-  }
+  for (int e = threadIdx.x; e < 41 * 16; e += blockDim.x) st_f(&sm->rtab[0][0], e, rtab_entry(R4, e));
 }
 
 // Round k's fold with its challenge (x0 + r (x0 + x1) over the pairs (j, j + half) of tables of
@@ -640,12 +656,13 @@ __global__ void __launch_bounds__(SW_THREADS) k_sw_fold(const SwInst* __restrict
   xor_reduce_store(e0, ei, &s.s->msg[0]);
 }
 
-// One thread per instance: the opened value p[0] and the evaluation point, msb_first
+// Out-of-line products for k_sw_tail: one copy of each in its code, which it runs once per round.
+__device__ __noinline__ F162d f_mul_ool(F162d a, F162d b) { return f_mul(a, b); }
+__device__ __noinline__ F162d cmul_ool(const F162d* T, F162d x) { return cmul<41>(T, x); }
+
+// The opened value p[0] and the evaluation point, msb_first
 // (crates/pcs/src/scheme/commitment.rs:163-174): p0[i] = r_(l-1-i), p1[i] = r_(col_log-1-i).
-__global__ void k_sw_finish(const SwInst* __restrict__ I, int count) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  const SwInst& s = I[i];
+__device__ void sw_finish(const SwInst& s) {
   SwSmall* sm = s.s;
   for (int w = 0; w < 3; w++) sm->opened[w] = s.p[w];
   if (s.p0)
@@ -655,6 +672,81 @@ __global__ void k_sw_finish(const SwInst* __restrict__ I, int count) {
     for (uint32_t q = 0; q < s.col_log; q++)
       for (int w = 0; w < 3; w++) s.p1[3 * q + w] = sm->rr[s.col_log - 1 - q][w];
   sm->status = 1;
+}
+
+// One block per instance: the rounds from sw_tail_start(l) on (each its transcript step, then its
+// fold and the next round's message, XOR-reduced over the block), with the hasher, the message
+// and the product tables in shared memory; then the opened value and the point.
+constexpr int SW_TAIL_THREADS = 256;
+__global__ void __launch_bounds__(SW_TAIL_THREADS) k_sw_tail(const SwInst* __restrict__ I) {
+  const SwInst& s = I[blockIdx.x];
+  SwSmall* sm = s.s;
+  __shared__ HasherState sh;
+  __shared__ F162d R4[41];
+  __shared__ F162d T[41 * 16];
+  __shared__ uint64_t msg[6];
+  __shared__ uint64_t red[SW_TAIL_THREADS / 32][6];
+  const uint32_t kt = sw_tail_start(s.l);
+  if (kt < s.l) {
+    dev::hs_copy(&sh, s.st);
+    if (threadIdx.x < 6) msg[threadIdx.x] = sm->msg[threadIdx.x];
+    __syncthreads();
+    for (uint32_t k = kt; k < s.l; k++) {
+      sw_transcript_step(s, (int)k, sh, msg, R4);
+      for (int e = threadIdx.x; e < 41 * 16; e += blockDim.x) T[e] = rtab_entry(R4, e);
+      __syncthreads();
+      const uint32_t half = 1u << (s.l - k - 1);
+      if (half < 2) {
+        if (threadIdx.x == 0) {
+          F162d a0 = ld_f(s.a, 0), a1 = ld_f(s.a, 1), p0 = ld_f(s.p, 0), p1 = ld_f(s.p, 1);
+          st_f(s.a, 0, f_add(a0, cmul_ool(T, f_add(a0, a1))));
+          st_f(s.p, 0, f_add(p0, cmul_ool(T, f_add(p0, p1))));
+        }
+      } else {
+        const uint32_t h2 = half / 2;
+        F162d e0{{0, 0, 0}}, ei{{0, 0, 0}};
+        for (uint32_t j = threadIdx.x; j < h2; j += blockDim.x) {
+          F162d na[2], np[2];
+#pragma unroll 1
+          for (int h = 0; h < 2; h++) {
+            const uint32_t x = j + h * h2;
+            F162d a0 = ld_f(s.a, x), a1 = ld_f(s.a, x + half), p0 = ld_f(s.p, x), p1 = ld_f(s.p, x + half);
+            na[h] = f_add(a0, cmul_ool(T, f_add(a0, a1)));
+            np[h] = f_add(p0, cmul_ool(T, f_add(p0, p1)));
+          }
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            st_f(s.a, j + h * h2, na[h]);
+            st_f(s.p, j + h * h2, np[h]);
+          }
+          e0 = f_add(e0, f_mul_ool(na[0], np[0]));
+          ei = f_add(ei, f_mul_ool(f_add(na[0], na[1]), f_add(np[0], np[1])));
+        }
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+          for (int w = 0; w < 3; w++) {
+            e0.w[w] ^= __shfl_xor_sync(0xffffffffu, e0.w[w], o);
+            ei.w[w] ^= __shfl_xor_sync(0xffffffffu, ei.w[w], o);
+          }
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+          for (int w = 0; w < 3; w++) {
+            red[threadIdx.x >> 5][w] = e0.w[w];
+            red[threadIdx.x >> 5][3 + w] = ei.w[w];
+          }
+        __syncthreads();
+        if (threadIdx.x < 6) {
+          uint64_t x = 0;
+          for (int w = 0; w < SW_TAIL_THREADS / 32; w++) x ^= red[w][threadIdx.x];
+          msg[threadIdx.x] = x;
+        }
+      }
+      __syncthreads();
+    }
+    dev::hs_copy(s.st, &sh);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) sw_finish(s);
 }
 
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }
@@ -684,21 +776,21 @@ void sw_layout(SwInst& I, uint8_t* base) {
 
 uint64_t sw_launches(const SwInst* h, int count) {
   if (count <= 0) return 0;
-  uint32_t lmax = 0;
+  uint32_t ktmax = 0;
   bool short_eq = false, seg_eq = false;
   for (int i = 0; i < count; i++) {
-    lmax = std::max(lmax, h[i].l);
+    ktmax = std::max(ktmax, sw_tail_start(h[i].l));
     short_eq |= sw_units(h[i].l, 3, 0) > 0;
     seg_eq |= sw_units(h[i].l, 4, 0) > 0;
   }
-  return 5 + (short_eq ? 1 : 0) + (seg_eq ? 1 : 0) + 2 * (uint64_t)lmax;
+  return 5 + (short_eq ? 1 : 0) + (seg_eq ? 1 : 0) + 2 * (uint64_t)ktmax;
 }
 
 cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStream_t st, uint64_t* launches) {
   if (count <= 0) return cudaSuccess;
-  uint32_t lmax = 0, tabmax = 0;
+  uint32_t ktmax = 0, tabmax = 0;
   for (int i = 0; i < count; i++) {
-    lmax = std::max(lmax, h[i].l);
+    ktmax = std::max(ktmax, sw_tail_start(h[i].l));
     tabmax = std::max(tabmax, (1u << h[i].lh) + (1u << h[i].ll));
   }
   auto blocks = [&](int stage, int k, int per) {
@@ -712,7 +804,7 @@ cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStre
   k_sw_sums<<<dim3(blocks(1, 0, SW_SUM_ROWS), 3), SW_THREADS, 0, st>>>(d, count);
   k_sw_statement<<<count, 128, 0, st>>>(d);
   k_sw_batch<<<count, 256, 0, st>>>(d);
-  for (uint32_t k = 0; k < lmax; k++) {
+  for (uint32_t k = 0; k < ktmax; k++) {
     k_sw_step<<<count, 128, 0, st>>>(d, (int)k);
     unsigned g = blocks(2, (int)k, SW_THREADS);
     if (k == 0)
@@ -720,7 +812,7 @@ cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStre
     else
       k_sw_fold<false><<<g, SW_THREADS, 0, st>>>(d, count, (int)k);
   }
-  k_sw_finish<<<(count + 31) / 32, 32, 0, st>>>(d, count);
+  k_sw_tail<<<count, SW_TAIL_THREADS, 0, st>>>(d);
   if (launches) *launches += sw_launches(h, count);
   return cudaGetLastError();
 }
