@@ -96,6 +96,9 @@ constexpr int WROW = RT * 12 + 2;          // staged witness words per column, p
 constexpr int LUT_BYTES = NTT_LUT_U16 * 2;  // the transform's window tables
 constexpr int AT_BYTES = RT * N162 * 32;   // the step's key tile
 
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
 }
@@ -330,6 +333,8 @@ __device__ __forceinline__ void fold_phase_a_store(uint16_t* __restrict__ wt, in
 // One CTA: 32 F162 positions x the columns [c_begin, c_end), eight columns per step.
 //  phase A: warp w transforms the F162 of column c + w at its lane's position into smem;
 //  phase B: warp w owns the leaves v = w + 8 u; lane = position; one multiply-add per (column, leaf).
+// The next step's witness words are loaded into registers while this step runs, and the step's
+// challenge slot values arrive in shared memory by cp.async while phase A transforms.
 // Split mode: the CTA's sums, reduced to [0, q), are added into vhat[p][v] (u32, zeroed by the
 // caller; with at most 2^16 column splits the total stays below 2^32) and k_fold_finish inverts.
 // Direct mode (one split): the CTA inverts its 32 positions itself and writes v, no vhat.
@@ -341,6 +346,7 @@ __global__ void __launch_bounds__(256, 2)
   extern __shared__ __align__(16) uint8_t smem[];
   uint16_t* lut = (uint16_t*)smem;
   uint16_t* wt = (uint16_t*)(smem + LUT_BYTES);  // FJ * 162 * FP u16
+  uint32_t* ctile = (uint32_t*)(smem + LUT_BYTES + FJ * N162 * FP * 2);  // [FJ][162]: the step's chat
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const size_t p0 = (size_t)blockIdx.x * FP;
   const int c_begin = blockIdx.y * cols_per_split;
@@ -351,30 +357,39 @@ __global__ void __launch_bounds__(256, 2)
   for (int u = 0; u < VPW; u++) acc[u] = 0;
   constexpr int RED = FoldRed<PI>::value;
   int since = 0;
+  // warp w's F162 of the step at j0: column j0 + w at the lane's position (zero past the range)
+  auto load_w = [&](int j0, uint64_t& e0, uint64_t& e1, uint64_t& e2) {
+    const int j = j0 + warp;
+    const size_t p = p0 + lane;
+    e0 = e1 = e2 = 0;
+    if (j < c_end && p < wdim) {
+      const uint64_t* e = W + ((size_t)j * wdim + p) * 3;
+      e0 = e[0];
+      e1 = e[1];
+      e2 = e[2];
+    }
+  };
+  uint64_t e0, e1, e2;
+  load_w(c_begin, e0, e1, e2);
   for (int j0 = c_begin; j0 < c_end; j0 += FJ) {
-    __syncthreads();
+    const int nj = min(FJ, c_end - j0);
+    __syncthreads();  // the previous step's phase B is done with wt and ctile
+    for (int x = tid; x < nj * N162; x += 256) cp_async4(ctile + x, chat + (size_t)j0 * N162 + x);
+    cp_async_commit();
     {
-      int j = j0 + warp;
-      size_t p = p0 + lane;
-      uint64_t e0 = 0, e1 = 0, e2 = 0;
-      if (j < c_end && p < wdim) {
-        const uint64_t* e = W + ((size_t)j * wdim + p) * 3;
-        e0 = e[0];
-        e1 = e[1];
-        e2 = e[2];
-      }
       uint32_t idx[7];
       f162_windows(e0, e1, e2, idx);
+      load_w(j0 + FJ, e0, e1, e2);
       fold_phase_a_store<PI>(wt, warp, lane, idx, (const uint8_t*)lut);
     }
+    cp_async_wait<0>();
     __syncthreads();
-    const int nj = min(FJ, c_end - j0);
     for (int jj = 0; jj < nj; jj++) {
-      const uint32_t* ch = chat + (size_t)(j0 + jj) * N162;
+      const uint32_t* ch = ctile + jj * N162;
 #pragma unroll
       for (int u = 0; u < VPW; u++) {
         int v = warp + 8 * u;
-        if (v < N162) acc[u] += __ldg(ch + v) * (uint32_t)wt[((jj * N162) + v) * FP + lane];
+        if (v < N162) acc[u] += ch[v] * (uint32_t)wt[((jj * N162) + v) * FP + lane];
       }
       if (++since >= RED) {
         since = 0;
@@ -1413,7 +1428,7 @@ cudaError_t launch_challenge_slots(int pi, const lbg_challenge_d* ch, int r, con
   return cudaGetLastError();
 }
 
-size_t fold_smem_bytes() { return LUT_BYTES + (size_t)FJ * N162 * FP * 2; }
+size_t fold_smem_bytes() { return LUT_BYTES + (size_t)FJ * N162 * FP * 2 + FJ * N162 * 4; }
 int fold_positions_per_cta() { return FP; }
 int fold_cols_per_step() { return FJ; }
 

@@ -195,114 +195,86 @@ __global__ void __launch_bounds__(SW_THREADS) k_sw_eq_seg(const SwInst* __restri
   }
 }
 
-// 8 x 8 bit transpose: byte r of x is row r (bit b = column b); on exit byte b holds column b
-// (bit r = row r's bit b). Three delta swaps of 1-, 2- and 4-bit blocks.
-__device__ __forceinline__ uint64_t transpose8(uint64_t x) {
-  uint64_t t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
-  x ^= t ^ (t << 7);
-  t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
-  x ^= t ^ (t << 14);
-  t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
-  x ^= t ^ (t << 28);
-  return x;
-}
-
-// One of the three matrices per blockIdx.y, over the pairs (j, j + n/2), j < n/2: kind 0 rows
-// j + n/2 (selector t, value eq), kind 1 rows j, kind 2 the pairs' sums. Row k of a matrix is the
-// XOR of the values of the rows whose selector has bit k set. Four Russians over groups of 8
-// rows: the 128 rows of an iteration are staged in shared memory; thread (g, c) (16 groups of 16
-// threads) builds entry c of its group's two 16-entry tables (XOR combinations of rows 0-3 and
-// 4-7 of the group), gathers byte c of the group's 8 selectors, transposes it (8 x 8 bits) into
-// the 8-row patterns of selector bits 8c .. 8c + 7, and adds two table entries per bit. The block's
-// rows are XOR-reduced in shared memory, then into the instance's matrix.
+// The three matrices in one pass over the pairs (j, j + n/2), j < n/2: kind 0 the rows j + n/2
+// (selector t, value eq), kind 1 the rows j, kind 2 the pairs' sums. Row k of a matrix is the XOR
+// of the values of the rows whose selector has bit k set. A CTA stages 256 pairs' three rows in
+// shared memory (the next 256 are loaded into registers meanwhile); warp w then runs through 32
+// of them with lane l owning the bits k = 4 l + q (q < 4) of all three matrices: per row, one
+// selector word and one value read by broadcast, four sign-extended bit masks and sixteen masked
+// XORs (one LOP3 each). The warps' sums are XOR-reduced in shared memory, then into the
+// instance's matrices.
 constexpr int SW_SUM_ROWS = 2048;  // pairs per block before the cap
 __global__ void __launch_bounds__(SW_THREADS) k_sw_sums(const SwInst* __restrict__ I, int count) {
-  __shared__ uint4 sSel[128], sVal[128];
-  __shared__ uint4 sL[16][16], sH[16][16];
-  __shared__ uint32_t sAcc[128][4];
-  const int kind = blockIdx.y;
+  __shared__ uint4 sSel[3][SW_THREADS], sVal[3][SW_THREADS];
+  __shared__ uint32_t sAcc[3][128][4];
   uint32_t local, nblk;
   int i = sw_find(I, count, 1, 0, SW_SUM_ROWS, local, nblk);
   if (i < 0) return;
   const SwInst& s = I[i];
   const size_t h = (1ull << s.l) / 2;
-  for (int t = threadIdx.x; t < 128 * 4; t += blockDim.x) (&sAcc[0][0])[t] = 0;
-  const int g = threadIdx.x >> 4, c = threadIdx.x & 15;
-  uint32_t acc[8][4];
+  for (int t = threadIdx.x; t < 3 * 128 * 4; t += blockDim.x) (&sAcc[0][0][0])[t] = 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t acc[3][4][4];
 #pragma unroll
-  for (int b = 0; b < 8; b++) acc[b][0] = acc[b][1] = acc[b][2] = acc[b][3] = 0;
-  // staging: thread 2 r + 0 fetches the selector of row r of an iteration, thread 2 r + 1 its
-  // value; the next iteration's are fetched while this one is processed
-  const int r = threadIdx.x >> 1;
-  auto fetch = [&](size_t base, uint64_t& x0, uint64_t& x1) {
-    const size_t j = base + r;
-    x0 = 0, x1 = 0;
+  for (int kind = 0; kind < 3; kind++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[kind][q][0] = acc[kind][q][1] = acc[kind][q][2] = acc[kind][q][3] = 0;
+  // pair base + threadIdx.x: its two trace words and eq values (zeros past the pairs)
+  uint64_t tl0, tl1, th0, th1;
+  B128d el, eh;
+  auto fetch = [&](size_t base) {
+    const size_t j = base + threadIdx.x;
+    tl0 = tl1 = th0 = th1 = 0;
+    el = eh = B128d{0, 0};
     if (j < h) {
-      const size_t row = kind == 0 ? j + h : j;
-      if (threadIdx.x & 1) {
-        B128d q = ld_b(s.eq, row);
-        if (kind == 2) q = b_add(q, ld_b(s.eq, j + h));
-        x0 = q.lo, x1 = q.hi;
-      } else {
-        x0 = __ldg(s.w + 3 * row), x1 = __ldg(s.w + 3 * row + 1);
-        if (kind == 2) x0 ^= __ldg(s.w + 3 * (j + h)), x1 ^= __ldg(s.w + 3 * (j + h) + 1);
-      }
+      tl0 = __ldg(s.w + 3 * j), tl1 = __ldg(s.w + 3 * j + 1);
+      th0 = __ldg(s.w + 3 * (j + h)), th1 = __ldg(s.w + 3 * (j + h) + 1);
+      el = ld_b(s.eq, j), eh = ld_b(s.eq, j + h);
     }
   };
-  const size_t stride = (size_t)nblk * 128;
-  uint64_t n0, n1;
-  fetch((size_t)local * 128, n0, n1);
-  for (size_t base = (size_t)local * 128; base < h; base += stride) {
-    {
-      uint4 v = make_uint4((uint32_t)n0, (uint32_t)(n0 >> 32), (uint32_t)n1, (uint32_t)(n1 >> 32));
-      if (threadIdx.x & 1)
-        sVal[r] = v;
-      else
-        sSel[r] = v;
-    }
+  auto u4 = [](uint64_t lo, uint64_t hi) {
+    return make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+  };
+  const size_t stride = (size_t)nblk * SW_THREADS;
+  fetch((size_t)local * SW_THREADS);
+  for (size_t base = (size_t)local * SW_THREADS; base < h; base += stride) {
+    __syncthreads();  // the previous chunk's rows are consumed
+    sSel[0][threadIdx.x] = u4(th0, th1);
+    sVal[0][threadIdx.x] = u4(eh.lo, eh.hi);
+    sSel[1][threadIdx.x] = u4(tl0, tl1);
+    sVal[1][threadIdx.x] = u4(el.lo, el.hi);
+    sSel[2][threadIdx.x] = u4(tl0 ^ th0, tl1 ^ th1);
+    sVal[2][threadIdx.x] = u4(el.lo ^ eh.lo, el.hi ^ eh.hi);
     __syncthreads();
-    if (base + stride < h) fetch(base + stride, n0, n1);
-    {  // entry c of the group's tables
-      uint4 lo = make_uint4(0, 0, 0, 0), hi = make_uint4(0, 0, 0, 0);
+    if (base + stride < h) fetch(base + stride);
+    for (int r = 0; r < 32; r++) {
+      const int row = 32 * warp + r;
 #pragma unroll
-      for (int b = 0; b < 4; b++) {
-        uint4 x = sVal[8 * g + b], y = sVal[8 * g + 4 + b];
-        uint32_t mk = 0u - (uint32_t)((c >> b) & 1);
-        lo.x ^= x.x & mk, lo.y ^= x.y & mk, lo.z ^= x.z & mk, lo.w ^= x.w & mk;
-        hi.x ^= y.x & mk, hi.y ^= y.y & mk, hi.z ^= y.z & mk, hi.w ^= y.w & mk;
+      for (int kind = 0; kind < 3; kind++) {
+        const uint32_t t = reinterpret_cast<const uint32_t*>(&sSel[kind][row])[lane >> 3];
+        const uint4 e = sVal[kind][row];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const uint32_t m = bit_mask(t, 4 * (lane & 7) + q);
+          acc[kind][q][0] ^= e.x & m;
+          acc[kind][q][1] ^= e.y & m;
+          acc[kind][q][2] ^= e.z & m;
+          acc[kind][q][3] ^= e.w & m;
+        }
       }
-      sL[g][c] = lo;
-      sH[g][c] = hi;
     }
-    __syncwarp();
-    uint64_t x = 0;
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-      uint4 sel = sSel[8 * g + r];
-      uint32_t w = (c >> 2) == 0 ? sel.x : (c >> 2) == 1 ? sel.y : (c >> 2) == 2 ? sel.z : sel.w;
-      x |= (uint64_t)((w >> (8 * (c & 3))) & 0xFF) << (8 * r);
-    }
-    x = transpose8(x);
-#pragma unroll
-    for (int b = 0; b < 8; b++) {
-      const uint32_t idx = (uint32_t)(x >> (8 * b)) & 0xFF;
-      uint4 u = sL[g][idx & 15], v = sH[g][idx >> 4];
-      acc[b][0] ^= u.x ^ v.x;
-      acc[b][1] ^= u.y ^ v.y;
-      acc[b][2] ^= u.z ^ v.z;
-      acc[b][3] ^= u.w ^ v.w;
-    }
-    __syncthreads();
   }
 #pragma unroll
-  for (int b = 0; b < 8; b++)
+  for (int kind = 0; kind < 3; kind++)
 #pragma unroll
     for (int q = 0; q < 4; q++)
-      if (acc[b][q]) atomicXor(&sAcc[8 * c + b][q], acc[b][q]);
+#pragma unroll
+      for (int w = 0; w < 4; w++)
+        if (acc[kind][q][w]) atomicXor(&sAcc[kind][4 * lane + q][w], acc[kind][q][w]);
   __syncthreads();
-  uint32_t* m = &s.s->mat[kind][0][0];
-  for (int t = threadIdx.x; t < 128 * 4; t += blockDim.x) {
-    uint32_t val = (&sAcc[0][0])[t];
+  uint32_t* m = &s.s->mat[0][0][0];
+  for (int t = threadIdx.x; t < 3 * 128 * 4; t += blockDim.x) {
+    uint32_t val = (&sAcc[0][0][0])[t];
     if (val) atomicXor(m + t, val);
   }
 }
@@ -801,7 +773,7 @@ cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStre
   k_sw_tables<<<dim3((tabmax + 127) / 128, count), 128, 0, st>>>(d);
   if (unsigned g = blocks(3, 0, SW_THREADS)) k_sw_eq<<<g, SW_THREADS, 0, st>>>(d, count);
   if (unsigned g = blocks(4, 0, 1)) k_sw_eq_seg<<<g, SW_THREADS, 0, st>>>(d, count);
-  k_sw_sums<<<dim3(blocks(1, 0, SW_SUM_ROWS), 3), SW_THREADS, 0, st>>>(d, count);
+  k_sw_sums<<<blocks(1, 0, SW_SUM_ROWS), SW_THREADS, 0, st>>>(d, count);
   k_sw_statement<<<count, 128, 0, st>>>(d);
   k_sw_batch<<<count, 256, 0, st>>>(d);
   for (uint32_t k = 0; k < ktmax; k++) {
