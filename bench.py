@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-switch", action="store_true")
     ap.add_argument("--no-wire", action="store_true")
+    ap.add_argument("--switch-sizes", default="18,20,22", help="log2 trace lengths of the switch line")
     ap.add_argument("--no-ntt", action="store_true")
     ap.add_argument("--no-suites", action="store_true")
     ap.add_argument("--ntt-count", type=int, default=1 << 20, help="ring elements of the NTT microbenchmark")
@@ -846,7 +847,7 @@ def run_ours(args):
             ntt_micro[k]["frac_of_hbm"] = ntt_micro[k]["gbs"] / hbm
     switch_times = None
     if not args.no_switch and rank == 0:
-        switch_times = run_switch(max(3, min(args.steps, 10)))
+        switch_times = run_switch(max(3, min(args.steps, 10)), tuple(int(x) for x in args.switch_sizes.split(",")))
     served = None
     if not args.no_served and rank == 0 and world == 1:
         served = run_served(args.served_requests, args.served_plain_sample)
