@@ -41,11 +41,12 @@ __device__ __forceinline__ F162d f_times_x4(F162d r) {
   return r;
 }
 
-// All ones when bit `pos` of x is set, else zero (a sign-extending one-bit field extract).
+// All ones when bit `pos` of x is set, else zero: the bit moved to the sign position, then an
+// arithmetic shift. With `pos` known at compile time the first shift is a multiply by a power of
+// two, which the compiler may issue to the multiply-add pipe, leaving one integer-pipe instruction
+// per mask.
 __device__ __forceinline__ uint32_t bit_mask(uint32_t x, uint32_t pos) {
-  int32_t r;
-  asm("bfe.s32 %0, %1, %2, 1;" : "=r"(r) : "r"(x), "r"(pos));
-  return (uint32_t)r;
+  return (uint32_t)((int32_t)(x << (31 - pos)) >> 31);
 }
 
 // c = a * b as polynomials. a's multiples by x^s (s < 4) fit NAX limbs; b has NB limbs, of which

@@ -684,14 +684,19 @@ __global__ void k_eq_table(const uint64_t* __restrict__ p, int n, size_t count, 
 
 // Row evaluation by the method of four Russians over 8-row groups (crates/pcs/src/eval.rs:136-193
 // computes the same sums one row at a time): u_j = sum_b x^b S_{j,b} mod x^162 + x^81 + 1 with
-// S_{j,b} = XOR of eq[i] over the rows i whose W[i][j] has bit b set. For a group of 8 rows the
-// 256 XOR-combinations of their eq values form a table T (built once per CTA and group, shared by
-// the CTA's columns); bit b of the 8 rows of column j, read as an 8-bit index, selects T's entry
-// to add to S_{j,b}. A thread owns one byte position m of one column (bits 8m .. 8m+7): it loads
-// the 8 rows' words, transposes the 8x8 bit block, and makes 8 lookups. CTAs split the rows;
-// partial results are combined with atomic XORs into u (zeroed first).
+// S_{j,b} = XOR of eq[i] over the rows i whose W[i][j] has bit b set. Bit b of the 8 rows of a
+// group, read as an 8-bit index, selects the XOR of their eq values to add to S_{j,b}; the index
+// is split into two nibbles looked up in two 16-entry tables (rows 0-3 and 4-7 of the group), so
+// a table is 16 entries of 3 words stored as three 128-byte word planes: the lanes' lookups hit
+// distinct banks or the same address, never a conflict. A thread owns one byte position m of one
+// column (bits 8m .. 8m+7): it gathers the 8 rows' bytes, transposes the 8x8 bit block and makes
+// 16 lookups. The witness rows of the CTA's columns and their eq values arrive in stages of 32
+// rows by cp.async, one stage ahead, coalesced (a column's rows are contiguous). CTAs split the
+// rows; partial results are combined with atomic XORs into u (zeroed first).
 constexpr int RE_COLS = 12;      // columns per CTA (12 x 21 byte positions = 252 threads)
 constexpr int RE_THREADS = 256;
+constexpr int RE_ROWS = 32;      // rows per stage (4 groups)
+constexpr int RE_WS = RE_ROWS * 3 + 3;  // staged words per column, padded so that columns start 6 banks apart
 
 __device__ __forceinline__ uint64_t transpose8x8(uint64_t x) {
   // byte k bit r -> byte r bit k
@@ -709,7 +714,9 @@ __global__ void __launch_bounds__(RE_THREADS) k_row_eval(const uint64_t* __restr
                                                          const uint64_t* __restrict__ eq_all,
                                                          const int4* __restrict__ tiles, int groups_per_split,
                                                          unsigned long long* __restrict__ u) {
-  __shared__ uint64_t T[2][256][3];  // this group's table and the next one's
+  __shared__ uint64_t Ws[2][RE_COLS][RE_WS];         // the stage's witness rows, per column
+  __shared__ uint64_t Es[2][RE_ROWS][3];             // the stage's eq values
+  __shared__ uint64_t TL[RE_ROWS / 8][2][3][16];     // per group: two nibble tables, word planes
   __shared__ uint64_t Q[RE_COLS][21][4];
   int4 tile;
   if (tiles) tile = tiles[blockIdx.x];
@@ -719,63 +726,63 @@ __global__ void __launch_bounds__(RE_THREADS) k_row_eval(const uint64_t* __restr
   const int c = t / 21, m = t - 21 * (t / 21);
   const bool active = c < tile.y;
   const int limb = m >> 3, sh = 8 * (m & 7);
-  const uint64_t* col = W + ((size_t)(tile.x + (active ? c : 0)) * wdim) * 3 + limb;
   const int G = wdim >> 3;
   const int g0 = blockIdx.y * groups_per_split, g1 = min(G, g0 + groups_per_split);
+  const int r0 = 8 * g0, r1 = 8 * g1;
   uint64_t S[8][3];
 #pragma unroll
   for (int r = 0; r < 8; r++) S[r][0] = S[r][1] = S[r][2] = 0;
-  // the next group's 8 witness words are loaded one group ahead, under the table build
-  uint64_t wn[8];
-#pragma unroll
-  for (int k = 0; k < 8; k++) wn[k] = 0;
-  if (active && g0 < g1) {
-#pragma unroll
-    for (int k = 0; k < 8; k++) wn[k] = __ldg(col + (size_t)(8 * g0 + k) * 3);
-  }
-  // entry t of group g's table: the XOR of eq over the rows 8g + k for the set bits k of t
-  auto build = [&](int g, uint64_t (*Td)[3]) {
-    const uint64_t* e = eq + (size_t)(8 * g) * 3;
-    uint64_t a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      uint64_t msk = 0 - (uint64_t)((t >> k) & 1);
-      a0 ^= __ldg(e + 3 * k) & msk;
-      a1 ^= __ldg(e + 3 * k + 1) & msk;
-      a2 ^= __ldg(e + 3 * k + 2) & msk;
+  // stage at row i0 into buffer b: each column's 3 * rows words, and the rows' eq values
+  auto stage = [&](int i0, int b) {
+    const int words = 3 * min(RE_ROWS, r1 - i0);
+    for (int x = t; x < tile.y * words; x += RE_THREADS) {
+      const int cc = x / words, wd = x - cc * words;
+      cp_async8(&Ws[b][cc][wd], W + ((size_t)(tile.x + cc) * wdim + i0) * 3 + wd);
     }
-    Td[t][0] = a0;
-    Td[t][1] = a1;
-    Td[t][2] = a2;
+    for (int x = t; x < words; x += RE_THREADS) cp_async8(&Es[b][0][0] + x, eq + (size_t)i0 * 3 + x);
   };
-  if (g0 < g1) build(g0, T[0]);
-  __syncthreads();
-  for (int g = g0; g < g1; g++) {
-    const int cur = (g - g0) & 1;
-    // this group's 8 bit rows of the thread's byte position, transposed: byte r = bit 8m + r of
-    // the 8 rows
-    uint64_t x = 0;
+  if (r0 < r1) stage(r0, 0);
+  cp_async_commit();
+  for (int i0 = r0, cur = 0; i0 < r1; i0 += RE_ROWS, cur ^= 1) {
+    const int ngroups = min(RE_ROWS, r1 - i0) >> 3;
+    cp_async_wait<0>();
+    __syncthreads();  // the stage has landed, and the previous stage's lookups are done
+    if (t < 32 * ngroups) {
+      // entry e of the half-table h of group q: the XOR of eq over rows 8q + 4h + k, k the set bits of e
+      const int q = t >> 5, h = (t >> 4) & 1, e = t & 15;
+      uint64_t a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll
-    for (int k = 0; k < 8; k++) x |= ((wn[k] >> sh) & 0xFF) << (8 * k);
-    x = transpose8x8(x);
-    if (g + 1 < g1) {
-      if (active) {
-#pragma unroll
-        for (int k = 0; k < 8; k++) wn[k] = __ldg(col + (size_t)(8 * (g + 1) + k) * 3);
+      for (int k = 0; k < 4; k++) {
+        const uint64_t msk = 0 - (uint64_t)((e >> k) & 1);
+        const uint64_t* x = Es[cur][8 * q + 4 * h + k];
+        a0 ^= x[0] & msk;
+        a1 ^= x[1] & msk;
+        a2 ^= x[2] & msk;
       }
-      build(g + 1, T[cur ^ 1]);
+      TL[q][h][0][e] = a0;
+      TL[q][h][1][e] = a1;
+      TL[q][h][2][e] = a2;
     }
+    if (i0 + RE_ROWS < r1) stage(i0 + RE_ROWS, cur ^ 1);
+    cp_async_commit();
+    __syncthreads();  // the tables are complete
     if (active) {
+      for (int q = 0; q < ngroups; q++) {
+        // this group's 8 bit rows of the thread's byte position, transposed: byte r = bit 8m + r
+        // of the 8 rows
+        uint64_t x = 0;
 #pragma unroll
-      for (int r = 0; r < 8; r++) {
-        const uint64_t* e = T[cur][(x >> (8 * r)) & 0xFF];
-        S[r][0] ^= e[0];
-        S[r][1] ^= e[1];
-        S[r][2] ^= e[2];
+        for (int k = 0; k < 8; k++) x |= ((Ws[cur][c][(8 * q + k) * 3 + limb] >> sh) & 0xFF) << (8 * k);
+        x = transpose8x8(x);
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+          const uint32_t idx = (uint32_t)(x >> (8 * r));
+          const uint32_t lo = idx & 15, hi = (idx >> 4) & 15;
+#pragma unroll
+          for (int w = 0; w < 3; w++) S[r][w] ^= TL[q][0][w][lo] ^ TL[q][1][w][hi];
+        }
       }
     }
-    // the next table is complete, and every lookup into this one is done before it is rebuilt
-    __syncthreads();
   }
   // this thread's share of sum_b x^b S_b: bits 8m + r, placed from word `limb` on
   if (active) {

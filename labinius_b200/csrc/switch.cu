@@ -235,6 +235,7 @@ __global__ void __launch_bounds__(SW_THREADS) k_sw_sums(const SwInst* __restrict
   auto u4 = [](uint64_t lo, uint64_t hi) {
     return make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
   };
+  const int sel_shift = 28 - 4 * (lane & 7);
   const size_t stride = (size_t)nblk * SW_THREADS;
   fetch((size_t)local * SW_THREADS);
   for (size_t base = (size_t)local * SW_THREADS; base < h; base += stride) {
@@ -251,11 +252,12 @@ __global__ void __launch_bounds__(SW_THREADS) k_sw_sums(const SwInst* __restrict
       const int row = 32 * warp + r;
 #pragma unroll
       for (int kind = 0; kind < 3; kind++) {
-        const uint32_t t = reinterpret_cast<const uint32_t*>(&sSel[kind][row])[lane >> 3];
+        // the lane's four selector bits moved to bits 28..31, then one mask per bit
+        const uint32_t t = reinterpret_cast<const uint32_t*>(&sSel[kind][row])[lane >> 3] << sel_shift;
         const uint4 e = sVal[kind][row];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          const uint32_t m = bit_mask(t, 4 * (lane & 7) + q);
+          const uint32_t m = bit_mask(t, 28 + q);
           acc[kind][q][0] ^= e.x & m;
           acc[kind][q][1] ^= e.y & m;
           acc[kind][q][2] ^= e.z & m;
