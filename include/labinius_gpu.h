@@ -240,9 +240,10 @@ int lbg_fold_static(uint32_t base_prime, uint32_t witness_log_len, uint32_t colu
  * (crates/pcs/src/scalar.rs:35-84 forward, :123-177 inverse), the kernels of the NTT
  * microbenchmark: `count` ring elements, u16 coefficients (forward) or slots in the reference's
  * slot order (inverse), all in [0, q), [count][648], device pointers, asynchronous on `stream`
- * (the current device's). Splitting primes (3889, 9721, 17497, 19441); quadratic-leaf primes
- * return LBG_ERR_UNSUPPORTED. No Rust API entry point corresponds (the reference calls its
- * transforms internally). */
+ * (the current device's). Both buffers 4-byte aligned (else LBG_ERR_INVALID); 16-byte aligned
+ * buffers take the faster forward kernel. Splitting primes (3889, 9721, 17497, 19441);
+ * quadratic-leaf primes return LBG_ERR_UNSUPPORTED. No Rust API entry point corresponds (the
+ * reference calls its transforms internally). */
 int lbg_ntt648_forward(uint32_t q, const uint16_t* d_in, uint16_t* d_out, size_t count, void* stream);
 int lbg_ntt648_inverse(uint32_t q, const uint16_t* d_in, uint16_t* d_out, size_t count, void* stream);
 

@@ -31,6 +31,8 @@ int run(uint32_t q, bool inverse, const uint16_t* in, uint16_t* out, size_t coun
   const Ntt648Tables* host = ntt648_tables(q);
   if (!host) return fail(LBG_ERR_UNSUPPORTED, "the 648-point transform here covers splitting primes only");
   if (count && (!in || !out)) return fail(LBG_ERR_INVALID, "null argument");
+  // the kernels store whole 32-bit words (16-byte chunks where both buffers allow)
+  if ((((uintptr_t)in | (uintptr_t)out) & 3) != 0) return fail(LBG_ERR_INVALID, "buffers must be 4-byte aligned");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return fail(LBG_ERR_CUDA, "no current device");
   Ntt648Tables* d = nullptr;

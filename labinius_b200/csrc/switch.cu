@@ -573,6 +573,12 @@ __global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
 // 2 half entries) and, when half >= 2, round k + 1's message over the pairs (j, j + half/2) of
 // the folded tables. FIRST (k = 0) reads the tables through eq and the trace and writes the
 // folded ones; later rounds fold in place.
+// Out-of-line products for the rounds where a thread folds at most one pair (k_sw_fold_small,
+// k_sw_tail): one copy of each in the kernel's code, so the few instructions each thread runs are
+// fetched once per SM instead of once per inlined copy.
+__device__ __noinline__ F162d f_mul_ool(F162d a, F162d b) { return f_mul(a, b); }
+__device__ __noinline__ F162d cmul_ool(const F162d* T, F162d x) { return cmul<41>(T, x); }
+
 template <bool FIRST>
 __global__ void __launch_bounds__(SW_THREADS) k_sw_fold(const SwInst* __restrict__ I, int count, int k) {
   // round 0 multiplies only 128-bit words (trace pairs) by r, so it needs 32 of the 41 positions
@@ -630,9 +636,39 @@ __global__ void __launch_bounds__(SW_THREADS) k_sw_fold(const SwInst* __restrict
   xor_reduce_store(e0, ei, &s.s->msg[0]);
 }
 
-// Out-of-line products for k_sw_tail: one copy of each in its code, which it runs once per round.
-__device__ __noinline__ F162d f_mul_ool(F162d a, F162d b) { return f_mul(a, b); }
-__device__ __noinline__ F162d cmul_ool(const F162d* T, F162d x) { return cmul<41>(T, x); }
+// k_sw_fold for a round k >= 1 whose launch gives every thread at most one pair (half >= 2): the
+// same arithmetic through one out-of-line copy of each product. Such rounds are bound by the
+// latency of one thread's work, not by throughput.
+__global__ void __launch_bounds__(SW_THREADS) k_sw_fold_small(const SwInst* __restrict__ I, int count, int k) {
+  __shared__ F162d T[41 * 16];
+  uint32_t local, nblk;
+  int i = sw_find(I, count, 2, k, SW_THREADS, local, nblk);
+  if (i < 0) return;
+  const SwInst& s = I[i];
+  load_table(T, &s.s->rtab[0][0], 41 * 16);
+  __syncthreads();
+  const size_t half = (1ull << s.l) >> (k + 1);
+  const size_t h2 = half / 2;
+  F162d e0{{0, 0, 0}}, ei{{0, 0, 0}};
+  for (size_t j = (size_t)local * SW_THREADS + threadIdx.x; j < h2; j += (size_t)nblk * SW_THREADS) {
+    F162d na[2], np[2];
+#pragma unroll 1
+    for (int h = 0; h < 2; h++) {
+      const size_t x = j + h * h2;
+      F162d a0 = ld_f(s.a, x), a1 = ld_f(s.a, x + half), p0 = ld_f(s.p, x), p1 = ld_f(s.p, x + half);
+      na[h] = f_add(a0, cmul_ool(T, f_add(a0, a1)));
+      np[h] = f_add(p0, cmul_ool(T, f_add(p0, p1)));
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      st_f(s.a, j + h * h2, na[h]);
+      st_f(s.p, j + h * h2, np[h]);
+    }
+    e0 = f_add(e0, f_mul_ool(na[0], np[0]));
+    ei = f_add(ei, f_mul_ool(f_add(na[0], na[1]), f_add(np[0], np[1])));
+  }
+  xor_reduce_store(e0, ei, &s.s->msg[0]);
+}
 
 // The opened value p[0] and the evaluation point, msb_first
 // (crates/pcs/src/scheme/commitment.rs:163-174): p0[i] = r_(l-1-i), p1[i] = r_(col_log-1-i).
@@ -781,10 +817,21 @@ cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStre
   for (uint32_t k = 0; k < ktmax; k++) {
     k_sw_step<<<count, 128, 0, st>>>(d, (int)k);
     unsigned g = blocks(2, (int)k, SW_THREADS);
-    if (k == 0)
+    if (k == 0) {
       k_sw_fold<true><<<g, SW_THREADS, 0, st>>>(d, count, 0);
-    else
-      k_sw_fold<false><<<g, SW_THREADS, 0, st>>>(d, count, (int)k);
+    } else {
+      // a launch that gives every thread at most one pair of a round with a message to compute
+      uint64_t most = 0;
+      bool last = false;
+      for (int i = 0; i < count; i++) {
+        most = std::max(most, sw_units(h[i].l, 2, (int)k));
+        last |= (uint32_t)k + 1 == h[i].l;
+      }
+      if (!last && most <= (uint64_t)SW_CAP * SW_THREADS)
+        k_sw_fold_small<<<g, SW_THREADS, 0, st>>>(d, count, (int)k);
+      else
+        k_sw_fold<false><<<g, SW_THREADS, 0, st>>>(d, count, (int)k);
+    }
   }
   k_sw_tail<<<count, SW_TAIL_THREADS, 0, st>>>(d);
   if (launches) *launches += sw_launches(h, count);

@@ -53,3 +53,28 @@ def test_quadratic_primes_refused():
     for q in [2917, 4861, 12637]:
         with pytest.raises(NativeError):
             ntt.forward(q, a)
+
+
+def test_forward_of_unaligned_buffers_matches():
+    """Buffers 4-byte but not 16-byte aligned take the non-persistent forward kernel; it agrees with
+    the aligned path (37 ring elements, a partial group). Buffers not 4-byte aligned are refused."""
+    import torch
+
+    from labinius_b200 import ntt
+
+    q, count = 9721, 37
+    g = torch.Generator(device="cuda").manual_seed(11)
+    a = torch.randint(0, q, (count, 648), dtype=torch.int16, device="cuda", generator=g)
+    want = ntt.forward(q, a)
+    src = torch.zeros(count * 648 + 8, dtype=torch.int16, device="cuda")
+    dst = torch.zeros(count * 648 + 8, dtype=torch.int16, device="cuda")
+    x = src[2:2 + count * 648].view(count, 648)
+    x.copy_(a)
+    y = dst[6:6 + count * 648].view(count, 648)
+    assert x.data_ptr() % 16 != 0 and y.data_ptr() % 16 != 0 and (x.data_ptr() | y.data_ptr()) % 4 == 0
+    ntt.forward(q, x, out=y)
+    assert torch.equal(y, want)
+    from labinius_b200._native import NativeError
+
+    with pytest.raises(NativeError):
+        ntt.forward(q, src[1:1 + count * 648].view(count, 648), out=y)
