@@ -425,6 +425,12 @@ void lbg_prover_free(lbg_prover* pr) {
     cudaStreamDestroy(pr->copy_stream);
   }
   for (auto e : pr->group_events) cudaEventDestroy(e);
+  for (auto sl : pr->limb_streams) {
+    cudaStreamSynchronize(sl);
+    cudaStreamDestroy(sl);
+  }
+  for (auto e : pr->limb_done) cudaEventDestroy(e);
+  for (auto* d : pr->limb_partial) cudaFree(d);
   cudaFree(pr->d_partial);
   cudaFree(pr->d_vhat);
   cudaFree(pr->d_ch);
@@ -691,6 +697,18 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
     if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail(LBG_ERR_CUDA, "event");
     pr->group_events.push_back(ev);
   }
+  while ((int)pr->limb_streams.size() < L - 1) {
+    cudaStream_t sl;
+    cudaEvent_t ev;
+    int32_t* part = nullptr;
+    if (cudaStreamCreateWithFlags(&sl, cudaStreamNonBlocking) != cudaSuccess) return fail(LBG_ERR_CUDA, "limb stream");
+    pr->limb_streams.push_back(sl);
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail(LBG_ERR_CUDA, "event");
+    pr->limb_done.push_back(ev);
+    if (cudaMalloc((void**)&part, (size_t)pr->nchunks * pp->cols * N162 * 16) != cudaSuccess)
+      return fail(LBG_ERR_OOM, "limb partials");
+    pr->limb_partial.push_back(part);
+  }
   lbg_witness* w;
   int rc = witness_alloc(pp, n, &w);
   if (rc) return rc;
@@ -707,20 +725,36 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
     const size_t c0 = (size_t)g * gc;
     e = cudaMemcpyAsync(w->d + c0 * per_col, f162 + c0 * per_col, (size_t)gc * per_col * 8, cudaMemcpyHostToDevice, cp);
     if (e == cudaSuccess) e = cudaEventRecord(pr->group_events[g], cp);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, pr->group_events[g], 0);
     for (int k = 0; k < L && e == cudaSuccess; k++) {
-      {
+      // limb 0 on the prover's stream (bracketed for the profile), limb k >= 1 on its own
+      cudaStream_t sk = k == 0 ? st : pr->limb_streams[k - 1];
+      int32_t* part = k == 0 ? pr->d_partial : pr->limb_partial[k - 1];
+      e = cudaStreamWaitEvent(sk, pr->group_events[g], 0);
+      if (e != cudaSuccess) break;
+      if (k == 0) {
         KernelScope ks(pr, "commit");
         e = launch_commit(pp->pidx[k], w->d + c0 * per_col, pp->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2,
-                          pp->d_prime[k], gc, (int)pp->len_ring, chunk, nch, pr->d_partial, st,
-                          k == 0 && b->d_keep ? b->d_keep + c0 * pp->wdim * N162 : nullptr);
+                          pp->d_prime[k], gc, (int)pp->len_ring, chunk, nch, part, sk,
+                          b->d_keep ? b->d_keep + c0 * pp->wdim * N162 : nullptr);
+      } else {
+        pr->launches += 1;
+        e = launch_commit(pp->pidx[k], w->d + c0 * per_col, pp->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2,
+                          pp->d_prime[k], gc, (int)pp->len_ring, chunk, nch, part, sk, nullptr);
       }
-      if (e == cudaSuccess) {
+      if (e != cudaSuccess) break;
+      if (k == 0) {
         KernelScope ks(pr, "commit_finish");
-        e = launch_commit_finish(pp->pidx[k], pr->d_partial, nch, gc, pp->d_prime[k], k, L,
-                                 b->d_C + c0 * 4 * L * N162, st);
+        e = launch_commit_finish(pp->pidx[k], part, nch, gc, pp->d_prime[k], k, L, b->d_C + c0 * 4 * L * N162, sk);
+      } else {
+        pr->launches += 1;
+        e = launch_commit_finish(pp->pidx[k], part, nch, gc, pp->d_prime[k], k, L, b->d_C + c0 * 4 * L * N162, sk);
       }
     }
+  }
+  // the prover's stream goes on once every limb stream has finished its groups
+  for (int k = 1; k < L && e == cudaSuccess; k++) {
+    e = cudaEventRecord(pr->limb_done[k - 1], pr->limb_streams[k - 1]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, pr->limb_done[k - 1], 0);
   }
   bool bd = pp->params.opening == LBG_OPENING_BIT_DROPPED;
   size_t count = pp->cols * N648;
@@ -750,6 +784,7 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     cudaStreamSynchronize(cp);
+    for (auto sl : pr->limb_streams) cudaStreamSynchronize(sl);
     {
       std::lock_guard<std::mutex> g(pr->mu);
       pr->spare.push_back(b);

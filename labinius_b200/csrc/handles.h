@@ -59,6 +59,11 @@ struct lbg_prover {
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream = nullptr;        // lbg_commit_host's uploads (created on first use)
   std::vector<cudaEvent_t> group_events;     // one per column group of lbg_commit_host
+  // lbg_commit_host commits limb k >= 1 on its own stream with its own chunk partials, so the
+  // limbs' launches of a column group overlap (created on first use)
+  std::vector<cudaStream_t> limb_streams;
+  std::vector<cudaEvent_t> limb_done;
+  std::vector<int32_t*> limb_partial;
   int chunk = 0, nchunks = 0;
   int fold_cols_per_split = 0;
   int32_t* d_partial = nullptr;
