@@ -531,21 +531,31 @@ __global__ void k_fold_finish(const uint32_t* __restrict__ vhat, size_t wdim, co
 // Verifier::fold_commitment: out[row][limb][s] = sum_j chat_j(s) C_j[row][limb][s]
 // (crates/pcs/src/scheme/verifier.rs:114-146).
 template <int PI>
-__global__ void k_fold_commitment(const int16_t* __restrict__ C, int cols, int limb, int limbs,
-                                  const uint32_t* __restrict__ chat, const DevPrime* __restrict__ D,
-                                  int16_t* __restrict__ out) {
-  int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= 4 * N162) return;
-  int row = gid / N162, s = gid % N162;
-  int leaf = D->pow3_to_leaf[s];
+__global__ void __launch_bounds__(1024) k_fold_commitment(const int16_t* __restrict__ C, int cols, int limb, int limbs,
+                                                          const uint32_t* __restrict__ chat,
+                                                          const DevPrime* __restrict__ D, int16_t* __restrict__ out) {
+  // CTA (slot group, row): lane = slot (consecutive slots, coalesced loads of C), warp w sums the
+  // columns w, w + 32, ...; the 32 warps' sums are added in shared memory
+  __shared__ uint32_t part[32][33];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.y, s = blockIdx.x * 32 + lane;
   constexpr int32_t q = Pr<PI>::q;
   uint64_t acc = 0;
-  for (int j = 0; j < cols; j++) {
-    int32_t c = C[(((size_t)j * 4 + row) * limbs + limb) * N162 + s];
-    uint32_t cm = (uint32_t)(c < 0 ? c + q : c);
-    acc += (uint64_t)chat[(size_t)j * N162 + leaf] * cm;
+  if (s < N162) {
+    const int leaf = D->pow3_to_leaf[s];
+    for (int j = warp; j < cols; j += 32) {
+      int32_t c = C[(((size_t)j * 4 + row) * limbs + limb) * N162 + s];
+      uint32_t cm = (uint32_t)(c < 0 ? c + q : c);
+      acc += (uint64_t)chat[(size_t)j * N162 + leaf] * cm;
+    }
   }
-  out[(row * limbs + limb) * N162 + s] = center<PI>((uint32_t)(acc % q));
+  part[warp][lane] = (uint32_t)(acc % q);
+  __syncthreads();
+  if (warp == 0 && s < N162) {
+    uint32_t t = 0;
+    for (int w = 0; w < 32; w++) t += part[w][lane];
+    out[(row * limbs + limb) * N162 + s] = center<PI>(t % q);
+  }
 }
 
 // =============================================================================================
@@ -1626,7 +1636,7 @@ cudaError_t launch_fold_kept(int pi, const uint16_t* keep, size_t wdim, int cols
 
 cudaError_t launch_fold_commitment(int pi, const int16_t* C, int cols, int limb, int limbs, const uint32_t* chat,
                                    const DevPrime* D, int16_t* out, cudaStream_t st) {
-  LBG_DISPATCH(pi, (k_fold_commitment<P><<<blocks_for(4 * N162, 128), 128, 0, st>>>(C, cols, limb, limbs, chat, D, out)));
+  LBG_DISPATCH(pi, (k_fold_commitment<P><<<dim3((N162 + 31) / 32, 4), 1024, 0, st>>>(C, cols, limb, limbs, chat, D, out)));
   return cudaGetLastError();
 }
 

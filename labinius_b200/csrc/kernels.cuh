@@ -50,16 +50,19 @@ __device__ __forceinline__ uint32_t red_full(uint32_t x) {
   uint32_t r = x - __umulhi(x, Pr<PI>::qs) * q;
   return r >= q ? r - q : r;
 }
+template <int PI>
+__device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b) {
+  static_assert((uint64_t)(Pr<PI>::q - 1) * (Pr<PI>::q - 1) < (1ull << 32), "the product fits 32 bits");
+  return red_full<PI>(a * b);
+}
 // x mod q up to one extra q: [0, 2q), for x < 2^32.
 template <int PI>
 __device__ __forceinline__ uint32_t red_half(uint32_t x) {
   return x - __umulhi(x, Pr<PI>::qs) * Pr<PI>::q;
 }
-// a * b mod q for a, b < q (rare paths).
+// a * b mod q for a, b < q (the product is below 2^32 for every prime here).
 template <int PI>
-__device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b) {
-  return (uint32_t)(((uint64_t)a * b) % Pr<PI>::q);
-}
+__device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b);
 // a signed accumulator brought back to |r| < 2q (exact modulo q).
 template <int PI>
 __device__ __forceinline__ int32_t red_signed(int32_t x) {
