@@ -1124,28 +1124,33 @@ __global__ void __launch_bounds__(81 * NTT_E) k_ntt648_inv(const uint16_t* __res
 // lane l adds x[32b + 2l]^2 + x[32b + 2l + 1]^2 over the 32-coefficient blocks b (the last block's
 // 8 coefficients fall in lanes 0..3). A lane sum that reaches 2^31 wraps the reference's i32 lanes,
 // which rejects. worst = the largest 16-bit absolute value (|-32768| stays negative and never wins).
-__global__ void k_v_norm(const int16_t* __restrict__ v, size_t len_ring, VerifyFlags* __restrict__ f) {
-  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_v_norm(const int16_t* __restrict__ v, size_t len_ring,
+                                                VerifyFlags* __restrict__ f) {
+  // a warp per ring element: warp lane t sums the squares of coefficients t, t + 32, ...; the
+  // reference's lane L is warp lanes 2L and 2L + 1
+  const size_t e = (size_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int t = threadIdx.x & 31;
   if (e >= len_ring) return;
   const int16_t* x = v + e * N648;
-  uint64_t lane[16];
-  for (int l = 0; l < 16; l++) lane[l] = 0;
+  uint64_t sq = 0;
   int worst = 0;
-  for (int i = 0; i < N648; i++) {
-    int xi = x[i];
-    lane[(i & 31) >> 1] += (uint64_t)(xi * xi);
-    int a = xi == -32768 ? -32768 : (xi < 0 ? -xi : xi);
+  for (int i = t; i < N648; i += 32) {
+    const int xi = x[i];
+    sq += (uint64_t)(xi * xi);
+    const int a = xi == -32768 ? -32768 : (xi < 0 ? -xi : xi);
     worst = a > worst ? a : worst;
   }
-  uint64_t sq = 0;
-  int wrapped = 0;
-  for (int l = 0; l < 16; l++) {
-    sq += lane[l];
-    if (lane[l] >= (1ull << 31)) wrapped = 1;
+  int wrapped = sq + __shfl_xor_sync(0xffffffffu, sq, 1) >= (1ull << 31);
+  for (int o = 16; o > 0; o >>= 1) {
+    sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    worst = max(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+    wrapped |= __shfl_xor_sync(0xffffffffu, wrapped, o);
   }
-  if (wrapped) atomicOr(&f->wrapped, 1);
-  atomicMax(&f->worst, worst);
-  atomicAdd(&f->normsq, (unsigned long long)sq);
+  if (t == 0) {
+    if (wrapped) atomicOr(&f->wrapped, 1);
+    atomicMax(&f->worst, worst);
+    atomicAdd(&f->normsq, (unsigned long long)sq);
+  }
 }
 
 // The 162-point transform of every component of every ring element of v, modulo one limb:
@@ -1730,7 +1735,7 @@ cudaError_t launch_ntt648(int pi, bool inverse, const uint16_t* in, uint16_t* ou
 }
 
 cudaError_t launch_v_norm(const int16_t* v, size_t len_ring, VerifyFlags* f, cudaStream_t st) {
-  k_v_norm<<<blocks_for(len_ring, 128), 128, 0, st>>>(v, len_ring, f);
+  k_v_norm<<<blocks_for(len_ring, 8), 256, 0, st>>>(v, len_ring, f);
   return cudaGetLastError();
 }
 
