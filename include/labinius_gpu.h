@@ -109,8 +109,10 @@ int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16
                uint16_t* digits_out, lbg_opening** opening_out);
 /* Witness::from_elements + Prover::commit in one call, the upload pipelined against the commit:
  * the n F162 at f162 (host memory; page-locked for the copies to overlap the commit) are copied in
- * column groups on a second stream, and each group's commit starts as soon as it has landed.
- * Outputs as lbg_commit; *w_out gets the device witness (free it with lbg_witness_free). */
+ * column groups on a second stream, and each group's commit starts as soon as it has landed (limb
+ * 0 on the prover's stream, each further limb on a stream of its own, so the limbs' commits of a
+ * group overlap). Outputs as lbg_commit; *w_out gets the device witness (free it with
+ * lbg_witness_free). */
 int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* matrix_out, uint16_t* top_out,
                     uint16_t* digits_out, lbg_witness** w_out, lbg_opening** opening_out);
 int lbg_opening_matrix(const lbg_opening* op, int16_t* matrix_out);
