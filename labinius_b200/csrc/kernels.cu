@@ -516,16 +516,21 @@ __global__ void __launch_bounds__(256, 2)
 // The inverse transform of each position's sums, centred, into the folded witness: position
 // p = 4 i + k gives coefficients 4 m + k of ring element i (crates/pcs/src/fold.rs:620-677).
 template <int PI>
-__global__ void k_fold_finish(const uint32_t* __restrict__ vhat, size_t wdim, const DevPrime* __restrict__ D,
-                              int16_t* __restrict__ v_out /* [len_ring][648] */) {
-  size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= wdim) return;
-  uint32_t x[N162];
-  for (int v = 0; v < N162; v++) x[v] = vhat[p * N162 + v] % Pr<PI>::q;
-  intt162_serial<PI>(x, *D);
-  size_t i = p / 4;
-  int k = (int)(p % 4);
-  for (int m = 0; m < N162; m++) v_out[i * N648 + 4 * m + k] = center<PI>(x[m]);
+__global__ void __launch_bounds__(216) k_fold_finish(const uint32_t* __restrict__ vhat, size_t wdim,
+                                                     const DevPrime* __restrict__ D,
+                                                     int16_t* __restrict__ v_out /* [len_ring][648] */) {
+  // four positions per CTA, 54 threads each: the inverse 162-point transform in shared memory
+  __shared__ uint32_t xs[4][N162];
+  const int g = threadIdx.x / 54, j = threadIdx.x - 54 * g;
+  const size_t p = (size_t)blockIdx.x * 4 + g;
+  for (int v = j; v < N162; v += 54) xs[g][v] = p < wdim ? vhat[p * N162 + v] % Pr<PI>::q : 0;
+  __syncthreads();
+  intt162_group<PI>(xs[g], j, *D);
+  if (p < wdim) {
+    const size_t i = p / 4;
+    const int k = (int)(p % 4);
+    for (int m = j; m < N162; m += 54) v_out[i * N648 + 4 * m + k] = center<PI>(xs[g][m]);
+  }
 }
 
 // Verifier::fold_commitment: out[row][limb][s] = sum_j chat_j(s) C_j[row][limb][s]
@@ -563,19 +568,21 @@ __global__ void __launch_bounds__(1024) k_fold_commitment(const int16_t* __restr
 // commitment (component d's coefficients are coefficients 4m + d), then Garner digits.
 // =============================================================================================
 template <int PI>
-__global__ void k_column_residues(const int16_t* __restrict__ C, int cols, int limb, int limbs,
-                                  const DevPrime* __restrict__ D, uint16_t* __restrict__ res /* [cols*648] */) {
-  int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= cols * 4) return;
-  int j = gid / 4, d = gid % 4;
+__global__ void __launch_bounds__(216) k_column_residues(const int16_t* __restrict__ C, int cols, int limb, int limbs,
+                                                         const DevPrime* __restrict__ D,
+                                                         uint16_t* __restrict__ res /* [cols*648] */) {
+  // one column per CTA, 54 threads per component: the inverse 162-point transform in shared memory
+  __shared__ uint32_t xs[4][N162];
+  const int d = threadIdx.x / 54, t = threadIdx.x - 54 * d;
+  const int j = blockIdx.x;
   constexpr int32_t q = Pr<PI>::q;
-  uint32_t x[N162];
-  for (int s = 0; s < N162; s++) {
+  for (int s = t; s < N162; s += 54) {
     int32_t c = C[(((size_t)j * 4 + d) * limbs + limb) * N162 + s];
-    x[D->pow3_to_leaf[s]] = (uint32_t)(c < 0 ? c + q : c);
+    xs[d][D->pow3_to_leaf[s]] = (uint32_t)(c < 0 ? c + q : c);
   }
-  intt162_serial<PI>(x, *D);
-  for (int m = 0; m < N162; m++) res[(size_t)j * N648 + 4 * m + d] = (uint16_t)x[m];
+  __syncthreads();
+  intt162_group<PI>(xs[d], t, *D);
+  for (int m = t; m < N162; m += 54) res[(size_t)j * N648 + 4 * m + d] = (uint16_t)xs[d][m];
 }
 
 __global__ void k_garner(const uint16_t* __restrict__ res, size_t count, int limbs, GarnerConsts g,
@@ -1607,7 +1614,7 @@ cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int co
                  cudaFuncSetAttribute(k_fold<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                  k_fold<P, false><<<grid, 256, smem, st>>>(W, wdim, cols, cols_per_split, chat, D, vhat, nullptr,
                                                           split_inst);
-                 k_fold_finish<P><<<blocks_for(positions, 64), 64, 0, st>>>(vhat, positions, D, v);
+                 k_fold_finish<P><<<blocks_for(positions, 4), 216, 0, st>>>(vhat, positions, D, v);
                }));
   return cudaGetLastError();
 }
@@ -1635,7 +1642,7 @@ cudaError_t launch_fold_kept(int pi, const uint16_t* keep, size_t wdim, int cols
                                                                 nullptr, split_inst);
                }));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  LBG_DISPATCH(pi, (k_fold_finish<P><<<blocks_for(wdim * instances, 64), 64, 0, st>>>(vhat, wdim * instances, D, v)));
+  LBG_DISPATCH(pi, (k_fold_finish<P><<<blocks_for(wdim * instances, 4), 216, 0, st>>>(vhat, wdim * instances, D, v)));
   return cudaGetLastError();
 }
 
@@ -1647,8 +1654,8 @@ cudaError_t launch_fold_commitment(int pi, const int16_t* C, int cols, int limb,
 
 cudaError_t launch_column_residues(int pi, const int16_t* C, int cols, int limb, int limbs, const DevPrime* D,
                                    uint16_t* res, cudaStream_t st) {
-  size_t n = (size_t)cols * 4;
-  LBG_DISPATCH(pi, (k_column_residues<P><<<blocks_for(n, 64), 64, 0, st>>>(C, cols, limb, limbs, D, res)));
+  if (cols <= 0) return cudaSuccess;
+  LBG_DISPATCH(pi, (k_column_residues<P><<<cols, 216, 0, st>>>(C, cols, limb, limbs, D, res)));
   return cudaGetLastError();
 }
 

@@ -208,6 +208,37 @@ __device__ void intt162_serial(uint32_t* x, const DevPrime& D) {
   }
 }
 
+// intt162_serial by a group of threads: x[0..161] in shared memory, thread j < 54 of the group
+// makes one radix-3 butterfly per level (the 54 of a level touch disjoint entries) and the
+// radix-2 pairs j and j + 54 of level 0, with the same arithmetic. Every thread of the block calls
+// it: it synchronises the block after each level.
+template <int PI>
+__device__ __forceinline__ void intt162_group(uint32_t* x, int j, const DevPrime& D) {
+  const uint32_t w = D.omega, w2 = mulmod<PI>(D.omega, D.omega);
+  for (int L = 4; L >= 1; L--) {
+    const int n = L == 4 ? 3 : L == 3 ? 9 : L == 2 ? 27 : 81, m = n / 3;
+    if (j < 54) {
+      const int k = j / m, i = j - k * m, base = k * n;
+      const uint32_t y0 = x[base + i], y1 = x[base + m + i], y2 = x[base + 2 * m + i];
+      const uint32_t s0 = red_full<PI>(y0 + y1 + y2);
+      const uint32_t s1 = red_full<PI>(y0 + mulmod<PI>(w2, y1) + mulmod<PI>(w, y2));
+      const uint32_t s2 = red_full<PI>(y0 + mulmod<PI>(w, y1) + mulmod<PI>(w2, y2));
+      x[base + i] = mulmod<PI>(s0, D.inv3);
+      x[base + m + i] = mulmod<PI>(s1, D.zinv3[L][k]);
+      x[base + 2 * m + i] = mulmod<PI>(s2, D.zinv3sq[L][k]);
+    }
+    __syncthreads();
+  }
+  constexpr uint32_t q = Pr<PI>::q;
+  for (int i = j; i < 81 && j < 54; i += 54) {
+    const uint32_t y0 = x[i], y1 = x[i + 81];
+    const uint32_t b = mulmod<PI>(red_full<PI>(y0 + q - y1), D.det0);
+    x[i] = red_full<PI>(y0 + q - mulmod<PI>(D.zeta6, b));
+    x[i + 81] = b;
+  }
+  __syncthreads();
+}
+
 // The forward 162-point transform of general coefficients in [0, q), in place on x[0..161], one
 // thread; leaves come out in the tree order the commit uses (the exact inverse of
 // intt162_serial). Used by the verifier, a few thousand per call.
