@@ -306,6 +306,21 @@ constexpr int FP = 32;  // positions per CTA
 constexpr int FJ = 8;   // columns per step
 constexpr int VPW = 21; // leaves per warp (8 warps, 162 leaves)
 
+// The inverse transforms of a CTA's FP positions' sums vh[FP][162] (shared memory), four positions
+// at a time by 54 threads each, centred into the folded witness (position p is coefficient
+// 4m + p % 4 of ring element p / 4). Every thread of the CTA calls it.
+template <int PI>
+__device__ __forceinline__ void fold_positions_out(uint32_t* vh, size_t p0, size_t wdim, const DevPrime* D,
+                                                   int16_t* v_out) {
+  const int tid = threadIdx.x, g = tid / 54, jj = tid - 54 * g;
+  for (int r = 0; r < FP / 4; r++) intt162_group<PI>(vh + (g < 4 ? 4 * r + g : 0) * N162, g < 4 ? jj : 54, *D);
+  for (int e = tid; e < FP * N162; e += blockDim.x) {
+    const int pl = e / N162, m = e - pl * N162;
+    const size_t p = p0 + pl;
+    if (p < wdim) v_out[(p / 4) * N648 + 4 * m + (p % 4)] = center<PI>(vh[pl * N162 + m]);
+  }
+}
+
 // Columns between two fold-backs of the unsigned accumulators: a column adds one product
 // chat * What < q * 2q per lane, and a fold-back leaves acc < 2q.
 template <int PI>
@@ -419,16 +434,7 @@ __global__ void __launch_bounds__(256, 2)
     if (v < N162) vh[lane * N162 + v] = red_full<PI>(acc[u]);
   }
   __syncthreads();
-  if (tid < FP) {
-    size_t p = p0 + tid;
-    if (p < wdim) {
-      uint32_t* x = vh + tid * N162;
-      intt162_serial<PI>(x, *D);
-      size_t i = p / 4;
-      int k = (int)(p % 4);
-      for (int m = 0; m < N162; m++) v_out[i * N648 + 4 * m + k] = center<PI>(x[m]);
-    }
-  }
+  fold_positions_out<PI>(vh, p0, wdim, D, v_out);
 }
 
 // The fold from the kept transform (keep[j][p / 16][v][p % 16], written by the commit at the base
@@ -500,16 +506,7 @@ __global__ void __launch_bounds__(256, 2)
       if (v < N162) vh[lane * N162 + v] = red_full<PI>(acc[u]);
     }
     __syncthreads();
-    if (tid < FP) {
-      size_t pp = p0 + tid;
-      if (pp < wdim) {
-        uint32_t* x = vh + tid * N162;
-        intt162_serial<PI>(x, *D);
-        size_t i = pp / 4;
-        int k = (int)(pp % 4);
-        for (int m = 0; m < N162; m++) v_out[i * N648 + 4 * m + k] = center<PI>(x[m]);
-      }
-    }
+    fold_positions_out<PI>(vh, p0, wdim, D, v_out);
   }
 }
 
@@ -609,25 +606,27 @@ __global__ void k_garner(const uint16_t* __restrict__ res, size_t count, int lim
 // commitment's component form: component d of column j is the forward 162-point transform of
 // coefficients 4m + d, written at C[j][d][limb][slot] centred (the inverse of k_column_residues).
 template <int PI>
-__global__ void k_bd_columns(const uint16_t* __restrict__ top, const uint16_t* __restrict__ digits, int cols, int limb,
+__global__ void __launch_bounds__(216) k_bd_columns(const uint16_t* __restrict__ top, const uint16_t* __restrict__ digits, int cols, int limb,
                              GarnerConsts g, int limbs, const DevPrime* __restrict__ D, int16_t* __restrict__ C) {
-  int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= cols * 4) return;
-  int j = gid / 4, d = gid % 4;
+  // one column per CTA, 54 threads per component, the transform in shared memory
+  __shared__ uint32_t xs[4][N162];
+  const int d = threadIdx.x / 54, t = threadIdx.x - 54 * d;
+  const int j = blockIdx.x;
   constexpr uint32_t q = Pr<PI>::q;
   const size_t count = (size_t)cols * N648;
-  uint32_t x[N162];
-  for (int m = 0; m < N162; m++) {
+  for (int m = t; m < N162; m += 54) {
     const size_t at = (size_t)j * N648 + 4 * m + d;
     uint32_t inner = 0;
     if (limbs > 1) {
       inner = digits[(size_t)(limbs - 2) * count + at] % q;
       for (int k = limbs - 3; k >= 0; k--) inner = (digits[(size_t)k * count + at] + inner * g.q[k + 1]) % q;
     }
-    x[m] = (uint32_t)((((uint64_t)top[at] << g.dropped_bits) + (uint64_t)inner * g.q[0]) % q);
+    xs[d][m] = (uint32_t)((((uint64_t)top[at] << g.dropped_bits) + (uint64_t)inner * g.q[0]) % q);
   }
-  ntt162_serial<PI>(x, *D);
-  for (int s = 0; s < N162; s++) C[(((size_t)j * 4 + d) * limbs + limb) * N162 + s] = center<PI>(x[D->pow3_to_leaf[s]]);
+  __syncthreads();
+  ntt162_group<PI>(xs[d], t, *D);
+  for (int s = t; s < N162; s += 54)
+    C[(((size_t)j * 4 + d) * limbs + limb) * N162 + s] = center<PI>(xs[d][D->pow3_to_leaf[s]]);
 }
 
 // k_bd_inverse: A v - the folded commitment for one limb, diff[row][leaf], back to the 648
@@ -1163,20 +1162,20 @@ __global__ void __launch_bounds__(256) k_v_norm(const int16_t* __restrict__ v, s
 // The 162-point transform of every component of every ring element of v, modulo one limb:
 // vhat[leaf][i][k] (component k of ring element i holds coefficients 4m + k).
 template <int PI>
-__global__ void k_v_transform(const int16_t* __restrict__ v, size_t len_ring, const DevPrime* __restrict__ D,
-                              uint32_t* __restrict__ vhat) {
-  size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= len_ring * 4) return;
-  size_t i = g >> 2;
-  int k = (int)(g & 3);
+__global__ void __launch_bounds__(216) k_v_transform(const int16_t* __restrict__ v, size_t len_ring,
+                                                     const DevPrime* __restrict__ D, uint32_t* __restrict__ vhat) {
+  // one ring element per CTA, 54 threads per component, the transform in shared memory
+  __shared__ uint32_t xs[4][N162];
+  const int k = threadIdx.x / 54, t = threadIdx.x - 54 * k;
+  const size_t i = blockIdx.x;
   constexpr int32_t q = Pr<PI>::q;
-  uint32_t x[N162];
-  for (int m = 0; m < N162; m++) {
+  for (int m = t; m < N162; m += 54) {
     int32_t c = v[i * N648 + 4 * m + k] % q;
-    x[m] = (uint32_t)(c < 0 ? c + q : c);
+    xs[k][m] = (uint32_t)(c < 0 ? c + q : c);
   }
-  ntt162_serial<PI>(x, *D);
-  for (int leaf = 0; leaf < N162; leaf++) vhat[((size_t)leaf * len_ring + i) * 4 + k] = x[leaf];
+  __syncthreads();
+  ntt162_group<PI>(xs[k], t, *D);
+  for (int leaf = t; leaf < N162; leaf += 54) vhat[((size_t)leaf * len_ring + i) * 4 + k] = xs[k][leaf];
 }
 
 // A v at one leaf (one CTA per leaf): Y_k'(leaf) = sum_i the module product of the key's
@@ -1749,7 +1748,7 @@ cudaError_t launch_v_norm(const int16_t* v, size_t len_ring, VerifyFlags* f, cud
 cudaError_t launch_v_limb(int pi, const int16_t* v, size_t len_ring, const DevPrime* D, uint32_t* vhat,
                           const int4* Ahat, int limb, int limbs, const int16_t* fc, VerifyFlags* f, cudaStream_t st,
                           uint32_t* diff) {
-  LBG_DISPATCH(pi, (k_v_transform<P><<<blocks_for(len_ring * 4, 64), 64, 0, st>>>(v, len_ring, D, vhat)));
+  if (len_ring > 0) LBG_DISPATCH(pi, (k_v_transform<P><<<(unsigned)len_ring, 216, 0, st>>>(v, len_ring, D, vhat)));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   LBG_DISPATCH(pi, (k_v_mac<P><<<N162, 256, 0, st>>>(vhat, len_ring, Ahat, D, limb, limbs, fc, f, diff)));
@@ -1758,8 +1757,7 @@ cudaError_t launch_v_limb(int pi, const int16_t* v, size_t len_ring, const DevPr
 
 cudaError_t launch_bd_columns(int pi, const uint16_t* top, const uint16_t* digits, int cols, int limb,
                               const GarnerConsts& g, int limbs, const DevPrime* D, int16_t* C, cudaStream_t st) {
-  LBG_DISPATCH(pi, (k_bd_columns<P><<<blocks_for((size_t)cols * 4, 64), 64, 0, st>>>(top, digits, cols, limb, g,
-                                                                                      limbs, D, C)));
+  if (cols > 0) LBG_DISPATCH(pi, (k_bd_columns<P><<<cols, 216, 0, st>>>(top, digits, cols, limb, g, limbs, D, C)));
   return cudaGetLastError();
 }
 

@@ -239,6 +239,34 @@ __device__ __forceinline__ void intt162_group(uint32_t* x, int j, const DevPrime
   __syncthreads();
 }
 
+// ntt162_serial by a group of threads (as intt162_group): level 0's pairs j and j + 54, then one
+// radix-3 butterfly per thread j < 54 and level. Every thread of the block calls it.
+template <int PI>
+__device__ __forceinline__ void ntt162_group(uint32_t* x, int j, const DevPrime& D) {
+  constexpr uint32_t q = Pr<PI>::q;
+  const uint32_t w = D.omega, w2 = mulmod<PI>(D.omega, D.omega);
+  for (int i = j; i < 81 && j < 54; i += 54) {
+    const uint32_t a = x[i], b = x[i + 81];
+    const uint32_t t = mulmod<PI>(D.zeta6, b);
+    x[i] = red_full<PI>(a + t);
+    x[i + 81] = red_full<PI>(a + b + q - t);
+  }
+  __syncthreads();
+  for (int L = 1; L <= 4; L++) {
+    const int n = L == 1 ? 81 : L == 2 ? 27 : L == 3 ? 9 : 3, m = n / 3;
+    if (j < 54) {
+      const int k = j / m, i = j - k * m, base = k * n;
+      const uint32_t z = D.zfwd[L][k], z2 = mulmod<PI>(z, z);
+      const uint32_t a0 = x[base + i];
+      const uint32_t t1 = mulmod<PI>(x[base + m + i], z), t2 = mulmod<PI>(x[base + 2 * m + i], z2);
+      x[base + i] = red_full<PI>(a0 + t1 + t2);
+      x[base + m + i] = red_full<PI>(a0 + mulmod<PI>(w, t1) + mulmod<PI>(w2, t2));
+      x[base + 2 * m + i] = red_full<PI>(a0 + mulmod<PI>(w2, t1) + mulmod<PI>(w, t2));
+    }
+    __syncthreads();
+  }
+}
+
 // The forward 162-point transform of general coefficients in [0, q), in place on x[0..161], one
 // thread; leaves come out in the tree order the commit uses (the exact inverse of
 // intt162_serial). Used by the verifier, a few thousand per call.
