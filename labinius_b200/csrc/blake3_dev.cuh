@@ -287,6 +287,68 @@ __device__ inline uint32_t hs_absorb_staged(HasherState* s, const uint32_t* stag
   }
   return off;
 }
+// hs_absorb_staged by a whole block: the chunks the stage's compressed blocks fall in are
+// compressed by one thread each (a chunk's blocks depend on one another, different chunks do
+// not), then thread 0 folds the completed chunks into the stack in order, as hs_absorb_staged
+// does one block at a time. cvs: shared scratch of 8 chaining values (a stage of at most
+// 8 * 1024 - 64 bytes). Every thread calls it; it returns the offset of the last block to all.
+__device__ inline uint32_t hs_absorb_staged_par(HasherState* s, const uint32_t* stage, uint32_t total,
+                                                uint32_t (*cvs)[8]) {
+  const uint32_t nb = (total + 63) / 64 - 1;  // every block but the last is compressed
+  const uint32_t B = s->blocks;
+  const uint32_t nch = nb == 0 ? 0 : (B + nb - 1) / 16 + 1;
+  // chunk r of the absorb: stage blocks [q0, q1), chunk positions from p0
+  auto span = [&](uint32_t r, uint32_t& q0, uint32_t& q1, uint32_t& p0) {
+    p0 = r == 0 ? B : 0;
+    q0 = r == 0 ? 0 : 16 * r - B;
+    q1 = 16 * (r + 1) - B < nb ? 16 * (r + 1) - B : nb;
+  };
+  if (threadIdx.x < nch) {
+    const uint32_t r = threadIdx.x;
+    uint32_t q0, q1, p0, cv[8], m[16], o[16];
+    span(r, q0, q1, p0);
+    for (int i = 0; i < 8; i++) cv[i] = r == 0 ? s->cv[i] : s->key[i];
+    for (uint32_t q = q0; q < q1; q++) {
+      const uint32_t pos = p0 + (q - q0);
+      for (int w = 0; w < 16; w++) m[w] = stage[q * 16 + w];
+      const uint32_t fl = s->flags | (pos == 0 ? b3::CHUNK_START : 0) | (pos == 15 ? b3::CHUNK_END : 0);
+      compress_ool(cv, m, s->chunk_counter + r, 64, fl, o);
+      for (int i = 0; i < 8; i++) cv[i] = o[i];
+    }
+    for (int i = 0; i < 8; i++) cvs[r][i] = cv[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (uint32_t r = 0; r < nch; r++) {
+      uint32_t q0, q1, p0;
+      span(r, q0, q1, p0);
+      const uint32_t done = p0 + (q1 - q0);  // the chunk's compressed blocks
+      if (done == 16) {
+        s->chunk_counter++;
+        uint64_t chunks = s->chunk_counter;
+        uint32_t cur[8];
+        for (int i = 0; i < 8; i++) cur[i] = cvs[r][i];
+        while ((chunks & 1) == 0 && s->stack_len > 0) {
+          s->stack_len--;
+          parent_cv_ool(s->key, s->flags, s->stack[s->stack_len], cur, cur);
+          chunks >>= 1;
+        }
+        if (s->stack_len < 54) {
+          for (int i = 0; i < 8; i++) s->stack[s->stack_len][i] = cur[i];
+          s->stack_len++;
+        }
+        for (int i = 0; i < 8; i++) s->cv[i] = s->key[i];
+        s->blocks = 0;
+      } else {
+        for (int i = 0; i < 8; i++) s->cv[i] = cvs[r][i];
+        s->blocks = done;
+      }
+    }
+  }
+  __syncthreads();
+  return nb * 64;
+}
+
 
 // The root node of a derivation from s: stage = s's open block followed by the derivation's
 // bytes (at most 128 bytes in all, so at most one chunk completes on the way). s is not changed.

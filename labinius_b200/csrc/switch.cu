@@ -13,14 +13,16 @@
 // P_k = sum_{j < n/2} bit_k(eq_j) t_j and Q_k the same over the pairs' sums) are all read off
 // three 128 x 128 GF(2) matrices sum_j t_j (x) eq_j (bit k of one times bit m of the other), over
 // j >= n/2, over j < n/2, and over the pairs (v is the sum of the first two, P and Q are columns
-// of the last two). They are accumulated by four Russians over groups of 8 rows (k_sw_sums).
-// The second pass is round 0's fold with round 1's message; later rounds fold in place. Every fold and the next message are one kernel; products by r go through 4-bit tables
-// of (t x^4i) r in shared memory, a through nibble tables of the batch (psi is linear, so
-// a_j + a_j' = psi(eq_j + eq_j')); round 0's tables are read through eq and the trace and never
-// stored, so the folded tables take n/2 entries.
+// of the last two). One pass accumulates all three, a warp lane owning four selector bits and
+// masking the value words by them (k_sw_sums).
+// The second pass is round 0's fold with round 1's message; later rounds fold in place. Every
+// fold and the next message are one kernel; products by r go through 4-bit tables of (t x^4i) r in
+// shared memory, a through nibble tables of the batch (psi is linear, so a_j + a_j' =
+// psi(eq_j + eq_j')); round 0's tables are read through eq and the trace and never stored, so the
+// folded tables take n/2 entries. The last rounds run in one CTA per instance (k_sw_tail).
 // The transcript runs on the device too: each instance's hasher state absorbs the statement,
 // the partials and every message, and the batch and round challenges are derived from it (one
-// thread per instance), so a whole switch is one pass on a stream with no host round trip. The
+// CTA per instance), so a whole switch is one pass on a stream with no host round trip. The
 // single-instance entry point moves the caller's transcript to the device and back.
 #include <cuda_runtime.h>
 
@@ -294,7 +296,8 @@ __global__ void k_sw_statement(const SwInst* __restrict__ I) {
   __shared__ HasherState sh;
   __shared__ uint64_t v[256], claim[2];
   __shared__ uint32_t stage[(64 + SW_STMT_MAX + 63) / 64 * 16];
-  __shared__ uint32_t last;
+  __shared__ uint32_t cvs[8][8];
+  uint32_t last;
   uint8_t* bytes = reinterpret_cast<uint8_t*>(stage);
   dev::hs_copy(&sh, s.st);
   // v[k] is row k of the matrices over the rows j + n/2 and j < n/2 (bit m of word m / 32)
@@ -354,8 +357,8 @@ __global__ void k_sw_statement(const SwInst* __restrict__ I) {
     bytes[b] = (uint8_t)(word >> (8 * at));
   }
   __syncthreads();
-  if (threadIdx.x == 0) last = dev::hs_absorb_staged(&sh, stage, total);
-  __syncthreads();
+  static_assert(64 + SW_STMT_MAX <= 8 * 1024 - 64, "the chunk-parallel absorb takes 8 chunks");
+  last = dev::hs_absorb_staged_par(&sh, stage, total, cvs);
   const uint32_t nbl = total - last;
   for (uint32_t b = threadIdx.x; b < nbl; b += blockDim.x) sh.buf[b] = bytes[last + b];
   __syncthreads();
