@@ -1,8 +1,8 @@
 """TEST INFRASTRUCTURE: Python bindings of the CPU oracle (``oracle/oracle.cpp``).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg import this
-module, and only as the checker or the timed CPU baseline. The product (``labinius_b200``) never
-imports it.
+module, and only to check the device's results or as the timed CPU baseline. The product
+(``labinius_b200``) never imports it.
 
 Parity unpinned: the reference (osdnk/labinius) ships no golden vectors for this path and cannot be
 built here; the oracle is a restatement of its scalar definitions, cross-checked against the
