@@ -577,7 +577,7 @@ __global__ void k_sw_step(const SwInst* __restrict__ I, int k) {
 // the folded tables. FIRST (k = 0) reads the tables through eq and the trace and writes the
 // folded ones; later rounds fold in place.
 // Out-of-line products for the rounds where a thread folds at most one pair (k_sw_fold_small,
-// k_sw_tail): one copy of each in the kernel's code, so the few instructions each thread runs are
+// k_sw_fold_split, k_sw_tail): one copy of each in the kernel's code, so the few instructions each thread runs are
 // fetched once per SM instead of once per inlined copy.
 __device__ __noinline__ F162d f_mul_ool(F162d a, F162d b) { return f_mul(a, b); }
 __device__ __noinline__ F162d cmul_ool(const F162d* T, F162d x) { return cmul<41>(T, x); }
@@ -669,6 +669,53 @@ __global__ void __launch_bounds__(SW_THREADS) k_sw_fold_small(const SwInst* __re
     }
     e0 = f_add(e0, f_mul_ool(na[0], np[0]));
     ei = f_add(ei, f_mul_ool(f_add(na[0], na[1]), f_add(np[0], np[1])));
+  }
+  xor_reduce_store(e0, ei, &s.s->msg[0]);
+}
+
+// k_sw_fold_small for rounds whose pairs leave most of the GPU idle, with a pair's work spread over
+// four warps: warps 4g + r of a CTA take the pairs 32 g + lane of the CTA's 64; warp role r folds
+// one of the pair's four entries (entry j + (r >> 1) h2 of table a or p by r & 1) through the
+// round's product tables, then roles 0 and 1 make the message's two products and roles 2 and 3
+// store the folded entries (every read of them is done by then). A thread's sequential work is
+// one product by r and at most one general product instead of four and two.
+constexpr int SW_SPLIT_PAIRS = 64;
+__global__ void __launch_bounds__(SW_THREADS) k_sw_fold_split(const SwInst* __restrict__ I, int count, int k) {
+  __shared__ F162d T[41 * 16];
+  __shared__ F162d N[2][4][32];
+  uint32_t local, nblk;
+  int i = sw_find(I, count, 2, k, SW_SPLIT_PAIRS, local, nblk);
+  if (i < 0) return;
+  const SwInst& s = I[i];
+  load_table(T, &s.s->rtab[0][0], 41 * 16);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = warp >> 2, r = warp & 3;
+  const size_t half = (1ull << s.l) >> (k + 1), h2 = half / 2;
+  F162d e0{{0, 0, 0}}, ei{{0, 0, 0}};
+  for (size_t base = (size_t)local * SW_SPLIT_PAIRS; base < h2; base += (size_t)nblk * SW_SPLIT_PAIRS) {
+    __syncthreads();  // the tables are loaded, and the last pass is done with N
+    const size_t j = base + 32 * g + lane;
+    const bool on = j < h2;
+    if (on) {
+      const uint64_t* tab = (r & 1) ? s.p : s.a;
+      const size_t x = j + (size_t)(r >> 1) * h2;
+      const F162d v0 = ld_f(tab, x), v1 = ld_f(tab, x + half);
+      N[g][r][lane] = f_add(v0, cmul_ool(T, f_add(v0, v1)));
+    }
+    __syncthreads();
+    if (on) {
+      const F162d na0 = N[g][0][lane], np0 = N[g][1][lane], na1 = N[g][2][lane], np1 = N[g][3][lane];
+      if (r == 0) {
+        e0 = f_add(e0, f_mul_ool(na0, np0));
+      } else if (r == 1) {
+        ei = f_add(ei, f_mul_ool(f_add(na0, na1), f_add(np0, np1)));
+      } else if (r == 2) {
+        st_f(s.a, j, na0);
+        st_f(s.a, j + h2, na1);
+      } else {
+        st_f(s.p, j, np0);
+        st_f(s.p, j + h2, np1);
+      }
+    }
   }
   xor_reduce_store(e0, ei, &s.s->msg[0]);
 }
@@ -830,7 +877,9 @@ cudaError_t enqueue_switch(const SwInst* d, const SwInst* h, int count, cudaStre
         most = std::max(most, sw_units(h[i].l, 2, (int)k));
         last |= (uint32_t)k + 1 == h[i].l;
       }
-      if (!last && most <= (uint64_t)SW_CAP * SW_THREADS)
+      if (!last && most <= (uint64_t)SW_CAP * SW_SPLIT_PAIRS)
+        k_sw_fold_split<<<blocks(2, (int)k, SW_SPLIT_PAIRS), SW_THREADS, 0, st>>>(d, count, (int)k);
+      else if (!last && most <= (uint64_t)SW_CAP * SW_THREADS)
         k_sw_fold_small<<<g, SW_THREADS, 0, st>>>(d, count, (int)k);
       else
         k_sw_fold<false><<<g, SW_THREADS, 0, st>>>(d, count, (int)k);
