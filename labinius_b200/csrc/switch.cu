@@ -746,6 +746,7 @@ __global__ void __launch_bounds__(SW_TAIL_THREADS) k_sw_tail(const SwInst* __res
   __shared__ F162d T[41 * 16];
   __shared__ uint64_t msg[6];
   __shared__ uint64_t red[SW_TAIL_THREADS / 32][6];
+  __shared__ F162d N[2][4][32];
   const uint32_t kt = sw_tail_start(s.l);
   if (kt < s.l) {
     dev::hs_copy(&sh, s.st);
@@ -765,22 +766,51 @@ __global__ void __launch_bounds__(SW_TAIL_THREADS) k_sw_tail(const SwInst* __res
       } else {
         const uint32_t h2 = half / 2;
         F162d e0{{0, 0, 0}}, ei{{0, 0, 0}};
-        for (uint32_t j = threadIdx.x; j < h2; j += blockDim.x) {
-          F162d na[2], np[2];
+        if (h2 <= (uint32_t)SW_SPLIT_PAIRS) {
+          // at most 64 pairs: a pair's four entries and two products over four warps, as
+          // k_sw_fold_split does
+          const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = warp >> 2, r = warp & 3;
+          const uint32_t j = 32 * g + lane;
+          const bool on = j < h2;
+          if (on) {
+            const uint64_t* tab = (r & 1) ? s.p : s.a;
+            const uint32_t x = j + (uint32_t)(r >> 1) * h2;
+            const F162d v0 = ld_f(tab, x), v1 = ld_f(tab, x + half);
+            N[g][r][lane] = f_add(v0, cmul_ool(T, f_add(v0, v1)));
+          }
+          __syncthreads();
+          if (on) {
+            const F162d na0 = N[g][0][lane], np0 = N[g][1][lane], na1 = N[g][2][lane], np1 = N[g][3][lane];
+            if (r == 0) {
+              e0 = f_mul_ool(na0, np0);
+            } else if (r == 1) {
+              ei = f_mul_ool(f_add(na0, na1), f_add(np0, np1));
+            } else if (r == 2) {
+              st_f(s.a, j, na0);
+              st_f(s.a, j + h2, na1);
+            } else {
+              st_f(s.p, j, np0);
+              st_f(s.p, j + h2, np1);
+            }
+          }
+        } else {
+          for (uint32_t j = threadIdx.x; j < h2; j += blockDim.x) {
+            F162d na[2], np[2];
 #pragma unroll 1
-          for (int h = 0; h < 2; h++) {
-            const uint32_t x = j + h * h2;
-            F162d a0 = ld_f(s.a, x), a1 = ld_f(s.a, x + half), p0 = ld_f(s.p, x), p1 = ld_f(s.p, x + half);
-            na[h] = f_add(a0, cmul_ool(T, f_add(a0, a1)));
-            np[h] = f_add(p0, cmul_ool(T, f_add(p0, p1)));
-          }
+            for (int h = 0; h < 2; h++) {
+              const uint32_t x = j + h * h2;
+              F162d a0 = ld_f(s.a, x), a1 = ld_f(s.a, x + half), p0 = ld_f(s.p, x), p1 = ld_f(s.p, x + half);
+              na[h] = f_add(a0, cmul_ool(T, f_add(a0, a1)));
+              np[h] = f_add(p0, cmul_ool(T, f_add(p0, p1)));
+            }
 #pragma unroll
-          for (int h = 0; h < 2; h++) {
-            st_f(s.a, j + h * h2, na[h]);
-            st_f(s.p, j + h * h2, np[h]);
+            for (int h = 0; h < 2; h++) {
+              st_f(s.a, j + h * h2, na[h]);
+              st_f(s.p, j + h * h2, np[h]);
+            }
+            e0 = f_add(e0, f_mul_ool(na[0], np[0]));
+            ei = f_add(ei, f_mul_ool(f_add(na[0], na[1]), f_add(np[0], np[1])));
           }
-          e0 = f_add(e0, f_mul_ool(na[0], np[0]));
-          ei = f_add(ei, f_mul_ool(f_add(na[0], na[1]), f_add(np[0], np[1])));
         }
         for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
