@@ -256,3 +256,28 @@ def test_commit_from_host_memory_equals_upload_then_commit(shape):
     v1 = prover.fold(op1, ch)
     v2 = prover.fold(op2, ch)
     assert np.array_equal(v1.elements, v2.elements)
+
+
+def test_commits_from_host_memory_in_a_row_stay_apart():
+    """Three lbg_commit_host calls in a row on one prover (the limbs' streams and chunk partials
+    reused, openings still open) each equal Witness::from_elements + Prover::commit of their own
+    witness; the folds of the three openings equal the device-witness folds."""
+    import labinius_b200 as L
+    from rounds import MATRIX_SEED, product_params
+
+    params = product_params((20, 9, [3889, 2917, 4861], 0))
+    pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+    prover = L.Prover(pp)
+    rng = np.random.default_rng(77)
+    ch = L.FoldingChallenges(np.zeros(params.columns(), L.CHALLENGE_DTYPE))
+    ch.challenges["weight"] = 28
+    ch.challenges["positions"][:, :28] = np.arange(0, 28 * 3, 3, dtype=np.uint8)
+    runs = []
+    for _ in range(3):
+        e = rng.integers(0, 2 ** 63, (params.witness_len(), 3), dtype=np.uint64)
+        e[:, 2] &= np.uint64((1 << 34) - 1)
+        runs.append((e,) + prover.commit_elements(e))
+    for e, w, c, op in runs:
+        c1, op1 = prover.commit(L.Witness.from_elements(pp, e))
+        assert np.array_equal(c.matrix, c1.matrix)
+        assert np.array_equal(prover.fold(op, ch).elements, prover.fold(op1, ch).elements)
