@@ -37,7 +37,6 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="l", choices=list(CONFIGS))
-    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
@@ -152,44 +151,86 @@ class Clocks:
 
 
 # ------------------------------------------------------------------------------------------------
-# CPU baseline: the oracle (a scalar C++ restatement of the reference's algorithm) on a sample
+# CPU baseline: the oracle (a scalar C++ restatement of the reference's algorithm), whole steps
 # ------------------------------------------------------------------------------------------------
-def cpu_baseline(params_tuple, budget_s, threads):
-    """Time the oracle's commit on a sample of columns and its fold on a sample of ring elements,
-    and scale each to the full round: elems/s = n / (t_commit_full + t_fold_full)."""
-    import oracle as O
+class OracleStep:
+    """The bench's step on the oracle: commit of every column on every limb, then the fold of every
+    ring element with the round's folding challenges (crates/bench/src/bin/labinius.rs:104-130, the
+    `commit` and `fold` rows). The challenges come from the oracle's own round (evaluation point,
+    row evaluation, FoldingChallenges::derive) on its first commitment, outside any timed step."""
 
-    O.build.build()
-    wl, cl, primes = params_tuple
-    P = O.Params(wl, cl, primes, 0)
-    A = O.key_expand(P, O.key_seed(MATRIX_SEED))
-    w = O.witness_random(P.witness_len, WITNESS_SEED)
-    t = O.Transcript(DOMAIN)
-    ch = np.zeros(P.columns, O.CHALLENGE_DTYPE)
-    t.absorb_u64(1)
-    for j in range(P.columns):
-        ch[j] = O.sample_short_challenge(t)[0]
-    # calibrate on one column / a few ring elements, then size the sample to the budget
-    t0 = time.perf_counter()
-    O.commit(P, A, w, 0, 1, threads=1)
-    per_col = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    O.fold(P, w, ch, 0, 4, threads=1)
-    per_ring = (time.perf_counter() - t0) / 4
-    cols = max(threads, int(0.5 * budget_s * threads / max(per_col, 1e-9)) // threads * threads)
-    cols = min(cols, P.columns)
-    rings = max(threads, int(0.5 * budget_s * threads / max(per_ring, 1e-9)) // threads * threads)
-    rings = min(rings, P.len_ring)
-    t0 = time.perf_counter()
-    O.commit(P, A, w, 0, cols, threads=threads)
-    tc = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    O.fold(P, w, ch, 0, rings, threads=threads)
-    tf = time.perf_counter() - t0
-    full = tc * P.columns / cols + tf * P.len_ring / rings
-    return {"value": P.witness_len / full, "unit": "elems/s", "cores": threads, "kind": "port",
-            "sample": f"oracle commit of {cols}/{P.columns} columns ({tc:.2f} s) and fold of {rings}/{P.len_ring} "
-                      f"ring elements ({tf:.2f} s) at 2^{wl}, scaled to the full round; {threads} threads"}
+    def __init__(self, params_tuple, witness_seed=None):
+        import oracle as O
+
+        O.build.build()
+        self.O = O
+        wl, cl, primes = params_tuple
+        self.P = O.Params(wl, cl, primes, 0)
+        self.A = O.key_expand(self.P, O.key_seed(MATRIX_SEED))
+        self.w = O.witness_random(self.P.witness_len, witness_seed or WITNESS_SEED)
+        self.ch = None
+
+    def challenges(self, C):
+        O = self.O
+        t = O.Transcript(DOMAIN)
+        p0, _ = O.derive_evaluation_point(self.P, MATRIX_SEED, t, C=C)
+        u = O.row_evaluate(self.w, p0)
+        self.ch = O.derive_folding_challenges(self.P, t, u)
+        return self.ch
+
+    def step(self, threads, ch=None):
+        """One whole step; returns (C, v, commit seconds, fold seconds)."""
+        O = self.O
+        t0 = time.perf_counter()
+        C = O.commit(self.P, self.A, self.w, threads=threads)
+        tc = time.perf_counter() - t0
+        if ch is None:
+            ch = self.ch if self.ch is not None else self.challenges(C)
+        t0 = time.perf_counter()
+        v = O.fold(self.P, self.w, ch, threads=threads)
+        tf = time.perf_counter() - t0
+        return C, v, tc, tf
+
+    def single_thread(self):
+        """The oracle on one thread: one column's commit and four ring elements' fold, scaled to
+        the whole step (a sample: a full one-thread step takes minutes)."""
+        O = self.O
+        ch = self.ch if self.ch is not None else np.zeros(self.P.columns, O.CHALLENGE_DTYPE)
+        t0 = time.perf_counter()
+        O.commit(self.P, self.A, self.w, 0, 1, threads=1)
+        tc = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        O.fold(self.P, self.w, ch, 0, 4, threads=1)
+        tf = time.perf_counter() - t0
+        full = tc * self.P.columns + tf * self.P.len_ring / 4
+        return {"value": self.P.witness_len / full, "unit": "elems/s", "cores": 1, "kind": "port",
+                "sample": f"oracle commit of 1/{self.P.columns} columns ({tc:.3f} s) and fold of "
+                          f"4/{self.P.len_ring} ring elements ({tf:.3f} s) on one thread, scaled to the step"}
+
+
+def host_cpu():
+    """The host's CPU model, for the baseline's record."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(params_tuple, threads, ch):
+    """One whole oracle step on all host threads with the GPU round's challenges; returns the
+    baseline record and the oracle's commitment and folded witness (the bench's parity check)."""
+    s = OracleStep(params_tuple)
+    C, v, tc, tf = s.step(threads, ch)
+    s.ch = ch
+    rec = {"value": s.P.witness_len / (tc + tf), "unit": "elems/s", "cores": threads, "kind": "port",
+           "sample": f"one whole step: oracle commit of {s.P.columns}/{s.P.columns} columns ({tc:.2f} s) and "
+                     f"fold of {s.P.len_ring}/{s.P.len_ring} ring elements ({tf:.2f} s) at 2^{s.P.witness_log_len}; "
+                     f"{threads} threads, unpinned, on {host_cpu()}",
+           "single_thread": s.single_thread()}
+    return rec, C, v
 
 
 def suite_shape(config):
@@ -199,31 +240,44 @@ def suite_shape(config):
     return params
 
 
+def bench_config(config, params, world):
+    """The `config` of both arms' lines (the same dict, so the lines compare)."""
+    return {"workload": f"suite {config}: 2^{params.witness_log_len} F162 in {params.columns()} columns, moduli "
+                        f"{params.primes()}, Opening::Clear, Witness::random(seed)",
+            "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"}
+
+
 # ------------------------------------------------------------------------------------------------
 # the reference arm
 # ------------------------------------------------------------------------------------------------
 def run_reference(args):
+    """The reference's algorithm on the host cores: the oracle port (the reference is a Rust
+    workspace and no Rust toolchain exists here or on the GPU box), whole steps of the bench's
+    workload on every host thread, timed by the host clock; warm-up steps untimed."""
     rank, world, local = dist()
     if rank != 0:
         return 0
     params = suite_shape(args.config)
-    shape = (params.witness_log_len, params.column_log_len, params.primes())
     threads = os.cpu_count() or 1
-    vals = []
-    budget = max(2.0, min(args.cpu_seconds, 60.0 / max(1, args.steps + args.warmup)))
-    for i in range(args.warmup + args.steps):
-        r = cpu_baseline(shape, budget, threads)
-        if i >= args.warmup:
-            vals.append(r)
-    value = float(np.median([v["value"] for v in vals]))
+    s = OracleStep((params.witness_log_len, params.column_log_len, params.primes()))
+    for _ in range(args.warmup):
+        s.step(threads)
+    times = []
+    for _ in range(args.steps):
+        _, _, tc, tf = s.step(threads)
+        times.append(tc + tf)
+    ms = 1000.0 * sum(times) / len(times)
+    value = params.witness_len() / (ms / 1000.0)
     line = {"metric": METRIC, "value": value, "unit": "elems/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * params.witness_len() / value, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32 mod q / GF(2)", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"suite {args.config}: 2^{params.witness_log_len} F162, {params.columns()} columns, "
-                                   f"moduli {params.primes()}, Clear", "cpu_threads": threads},
+            "config": bench_config(args.config, params, world),
             "cpu_baseline": {"value": value, "unit": "elems/s", "cores": threads, "kind": "port",
-                             "sample": vals[-1]["sample"]},
+                             "sample": f"{args.steps} whole steps (commit of all {params.columns()} columns on "
+                                       f"{len(params.primes())} limbs + fold of all {params.len_ring()} ring "
+                                       f"elements), {threads} threads, unpinned, on {host_cpu()}",
+                             "single_thread": s.single_thread()},
             "e2e": {"value": value, "unit": "elems/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -864,9 +918,22 @@ def run_ours(args):
         served = run_served(args.served_requests, args.served_plain_sample)
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline((params.witness_log_len, params.column_log_len, params.primes()), args.cpu_seconds,
-                           os.cpu_count() or 1)
+        # the device's commitment and folded witness of the step, through the public API with host
+        # buffers (the e2e step's outputs, or one more step), against the oracle's whole step
+        if e2e is None:
+            c_dev, op_dev = prover.commit(w)
+            gpu_C, gpu_v = c_dev.matrix, prover.fold(op_dev, ch).elements
+        else:
+            gpu_C, gpu_v = mat, vout
+        cpu, oC, ov = cpu_baseline((params.witness_log_len, params.column_log_len, params.primes()),
+                                   os.cpu_count() or 1, chal)
+        parity = {"checked": True, "C": bool(np.array_equal(gpu_C, oC)), "v": bool(np.array_equal(gpu_v, ov)),
+                  "columns": r, "ring_elements": params.len_ring(),
+                  "what": "the step's commitment matrix (every column, every limb) and folded witness (every "
+                          "ring element) from the device through the C ABI, against the oracle's whole step "
+                          "with the same challenges"}
 
     props = torch.cuda.get_device_properties(local)
     int_peak = props.multi_processor_count * 128 * float(clk.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
@@ -874,9 +941,8 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "elems/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 mod q / GF(2)", "data": "synthetic",
-        "config": {"workload": f"suite {args.config}: 2^{params.witness_log_len} F162 in {r} columns, moduli "
-                               f"{params.primes()}, Opening::Clear, Witness::random(seed)",
-                   "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
+        "config": bench_config(args.config, params, world),
+        "parity": parity,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": peak_src, "traffic": traffic, "kernel": "k_commit (one launch per limb)",
                      "per_launch_ms": per_launch_ms, "algorithmic_bytes_per_launch": algo_bytes,

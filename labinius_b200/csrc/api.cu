@@ -697,18 +697,28 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
     if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail(LBG_ERR_CUDA, "event");
     pr->group_events.push_back(ev);
   }
+  // a limb's stream, event and partials are made together and kept only when all three exist, so
+  // the three lists always have the same length
   while ((int)pr->limb_streams.size() < L - 1) {
-    cudaStream_t sl;
-    cudaEvent_t ev;
+    cudaStream_t sl = nullptr;
+    cudaEvent_t ev = nullptr;
     int32_t* part = nullptr;
     if (cudaStreamCreateWithFlags(&sl, cudaStreamNonBlocking) != cudaSuccess) return fail(LBG_ERR_CUDA, "limb stream");
-    pr->limb_streams.push_back(sl);
-    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail(LBG_ERR_CUDA, "event");
-    pr->limb_done.push_back(ev);
-    if (cudaMalloc((void**)&part, (size_t)pr->nchunks * pp->cols * N162 * 16) != cudaSuccess)
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+      cudaStreamDestroy(sl);
+      return fail(LBG_ERR_CUDA, "event");
+    }
+    if (cudaMalloc((void**)&part, (size_t)pr->nchunks * pp->cols * N162 * 16) != cudaSuccess) {
+      cudaEventDestroy(ev);
+      cudaStreamDestroy(sl);
       return fail(LBG_ERR_OOM, "limb partials");
+    }
+    pr->limb_streams.push_back(sl);
+    pr->limb_done.push_back(ev);
     pr->limb_partial.push_back(part);
   }
+  if (pr->limb_done.size() != pr->limb_streams.size() || pr->limb_partial.size() != pr->limb_streams.size())
+    return fail(LBG_ERR_INVALID, "limb streams, events and partials out of step");
   lbg_witness* w;
   int rc = witness_alloc(pp, n, &w);
   if (rc) return rc;
