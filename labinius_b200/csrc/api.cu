@@ -141,6 +141,12 @@ int lbg_params_check(const lbg_params* p) {
   return LBG_OK;
 }
 
+// After a synchronisation: a tensor-core kernel whose bounded wait ran out reports a timeout.
+static cudaError_t tc_checked(cudaError_t e) {
+  if (e == cudaSuccess && tc_timeout_take() == 1) return cudaErrorLaunchTimeout;
+  return e;
+}
+
 static int upload_prime(lbg_pp* pp, int k) {
   const PrimeTables& T = prime_tables(pp->primes[k]);
   HotPrime h;
@@ -174,6 +180,12 @@ static int upload_prime(lbg_pp* pp, int k) {
   cudaError_t e = cudaMalloc((void**)&pp->d_prime[k], sizeof(DevPrime));
   if (e == cudaSuccess) e = upload_sync(pp->d_prime[k], D, sizeof(DevPrime));
   delete D;
+  if (e == cudaSuccess) {
+    std::vector<uint8_t> tcb(TC_B_BYTES);
+    tc_transform_operand(T, tcb.data());
+    e = cudaMalloc((void**)&pp->d_tcb[k], TC_B_BYTES);
+    if (e == cudaSuccess) e = upload_sync(pp->d_tcb[k], tcb.data(), TC_B_BYTES);
+  }
   if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("prime tables: ") + cudaGetErrorString(e));
   return LBG_OK;
 }
@@ -184,7 +196,10 @@ void lbg_public_parameters_free(lbg_pp* pp) {
   if (pp->stream) cudaStreamSynchronize(pp->stream);
   cudaFree(pp->d_A);
   cudaFree(pp->d_Ahat);
-  for (int k = 0; k < 7; k++) cudaFree(pp->d_prime[k]);
+  for (int k = 0; k < 7; k++) {
+    cudaFree(pp->d_prime[k]);
+    cudaFree(pp->d_tcb[k]);
+  }
   cudaFree(pp->d_jumps);
   cudaFree(pp->d_eq);
   cudaFree(pp->d_p);
@@ -398,7 +413,9 @@ static void commit_chunking(const lbg_pp* pp, int cols, long max_partial, int* c
     if ((long)nact * cols > max_partial) break;
     long total = (long)col_tiles * nact;
     long waves = (total + slots - 1) / slots;
-    long cost = waves * chunk;
+    // the tensor-core kernel is persistent (its items run back to back on one CTA per SM): an item
+    // costs its chunk plus about two ring elements, a chunk of partial sums about one
+    long cost = commit_tc_enabled() ? waves * (chunk + 2) + nact : waves * chunk;
     if (best_cost < 0 || cost < best_cost) {
       best_cost = cost;
       *chunk_out = chunk;
@@ -512,11 +529,14 @@ int lbg_prover_new(const lbg_pp* pp, lbg_prover** out) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pp->device);
   commit_chunking(pp, (int)pp->cols, 1 << 30, &pr->chunk, &pr->nchunks);
-  // the fold: position tiles x column splits, chosen the same way
+  // the fold: position tiles x column splits, chosen the same way (the tensor-core kernel: 128
+  // positions per work item, one CTA per SM, one column a step)
   {
-    int tiles = (int)((pp->wdim + fold_positions_per_cta() - 1) / fold_positions_per_cta());
-    int fslots = sms * fold_blocks_per_sm(pp->pidx[0]);
-    int fstep = fold_cols_per_step();
+    const bool ftc = fold_tc_enabled();
+    const int fpos = ftc ? fold_tc_positions_per_cta() : fold_positions_per_cta();
+    int tiles = (int)((pp->wdim + fpos - 1) / fpos);
+    int fslots = sms * (ftc ? 1 : fold_blocks_per_sm(pp->pidx[0]));
+    int fstep = ftc ? 1 : fold_cols_per_step();
     long best = -1;
     int max_splits = (int)((pp->cols + fstep - 1) / fstep);
     for (int ns = 1; ns <= max_splits; ns++) {
@@ -524,7 +544,9 @@ int lbg_prover_new(const lbg_pp* pp, lbg_prover** out) {
       per = (per + fstep - 1) / fstep * fstep;
       int nact = (int)((pp->cols + per - 1) / per);
       long total = (long)tiles * nact;
-      long cost = ((total + fslots - 1) / fslots) * per;
+      // the tensor-core kernel runs its items back to back: an item costs its columns plus about
+      // two more (its sums added into vhat)
+      long cost = ((total + fslots - 1) / fslots) * (per + (ftc ? 2 : 0));
       if (best < 0 || cost < best) {
         best = cost;
         pr->fold_cols_per_split = per;
@@ -622,7 +644,7 @@ int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16
       KernelScope ks(pr, "commit");
       e = launch_commit(pp->pidx[k], w->d, pp->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2,
                         pp->d_prime[k], cols, (int)pp->len_ring, pr->chunk, pr->nchunks, pr->d_partial, st,
-                        k == 0 ? b->d_keep : nullptr);
+                        k == 0 ? b->d_keep : nullptr, pp->d_tcb[k]);
     }
     if (e == cudaSuccess) {
       KernelScope ks(pr, "commit_finish");
@@ -653,7 +675,7 @@ int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16
   if (e == cudaSuccess && bd && top_out) e = cudaMemcpyAsync(top_out, b->d_top, count * 2, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess && bd && digits_out && L > 1)
     e = cudaMemcpyAsync(digits_out, b->d_digits, (size_t)(L - 1) * count * 2, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess && (matrix_out || top_out || digits_out)) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && (matrix_out || top_out || digits_out)) e = tc_checked(cudaStreamSynchronize(st));
   if (e != cudaSuccess) {
     std::lock_guard<std::mutex> g(pr->mu);
     pr->spare.push_back(b);
@@ -745,11 +767,11 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
         KernelScope ks(pr, "commit");
         e = launch_commit(pp->pidx[k], w->d + c0 * per_col, pp->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2,
                           pp->d_prime[k], gc, (int)pp->len_ring, chunk, nch, part, sk,
-                          b->d_keep ? b->d_keep + c0 * pp->wdim * N162 : nullptr);
+                          b->d_keep ? b->d_keep + c0 * pp->wdim * N162 : nullptr, pp->d_tcb[k]);
       } else {
         pr->launches += 1;
         e = launch_commit(pp->pidx[k], w->d + c0 * per_col, pp->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2,
-                          pp->d_prime[k], gc, (int)pp->len_ring, chunk, nch, part, sk, nullptr);
+                          pp->d_prime[k], gc, (int)pp->len_ring, chunk, nch, part, sk, nullptr, pp->d_tcb[k]);
       }
       if (e != cudaSuccess) break;
       if (k == 0) {
@@ -791,7 +813,7 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
   if (e == cudaSuccess && bd && digits_out && L > 1)
     e = cudaMemcpyAsync(digits_out, b->d_digits, (size_t)(L - 1) * count * 2, cudaMemcpyDeviceToHost, st);
   // the witness is complete once the compute stream has passed every group's event
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = tc_checked(cudaStreamSynchronize(st));
   if (e != cudaSuccess) {
     cudaStreamSynchronize(cp);
     for (auto sl : pr->limb_streams) cudaStreamSynchronize(sl);
@@ -915,7 +937,7 @@ int lbg_fold(lbg_prover* pr, lbg_opening* op, const lbg_challenge* challenges, s
                            pr->d_chat, pp->d_prime[0], pr->d_vhat, pr->d_v, st);
     else
       e = launch_fold(pp->pidx[0], op->w->d, pp->wdim, (int)pp->cols, pr->fold_cols_per_split, pr->d_chat,
-                      pp->d_prime[0], pr->d_vhat, pr->d_v, st);
+                      pp->d_prime[0], pr->d_vhat, pr->d_v, st, 1, nullptr, pp->d_tcb[0]);
   }
   if (e == cudaSuccess && v_out) e = cudaMemcpyAsync(v_out, pr->d_v, pp->len_ring * N648 * 2, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess && v_out) e = cudaStreamSynchronize(st);

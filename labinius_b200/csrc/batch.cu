@@ -119,7 +119,7 @@ static cudaError_t enqueue_commit(lbg_batch* b) {
   for (int k = 0; k < L && e == cudaSuccess; k++) {
     e = launch_commit(pp->pidx[k], b->d_w, b->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2, pp->d_prime[k],
                       cols, (int)b->len_ring, b->chunk, b->nchunks, b->d_partial, b->stream,
-                      k == 0 && b->keep ? b->d_keep : nullptr);
+                      k == 0 && b->keep ? b->d_keep : nullptr, pp->d_tcb[k]);
     if (e == cudaSuccess)
       e = launch_commit_finish(pp->pidx[k], b->d_partial, b->nchunks, cols, pp->d_prime[k], k, L, b->d_C, b->stream);
   }
@@ -150,7 +150,7 @@ static cudaError_t enqueue_fold(lbg_batch* b) {
                          pp->d_prime[0], b->d_vhat, b->d_v, b->stream, b->count, b->d_split_inst);
   else if (e == cudaSuccess)
     e = launch_fold(pp->pidx[0], b->d_w, b->wdim, (int)b->total_cols, b->fold_per, b->d_chat, pp->d_prime[0],
-                    b->d_vhat, b->d_v, b->stream, b->count, b->d_split_inst);
+                    b->d_vhat, b->d_v, b->stream, b->count, b->d_split_inst, pp->d_tcb[0]);
   b->launches += 3;
   return e;
 }

@@ -29,6 +29,7 @@ struct lbg_pp {
   int16_t* d_A = nullptr;     // [limbs][len_ring][648]
   int4* d_Ahat = nullptr;     // [limbs][len_ring][162][2]
   DevPrime* d_prime[7] = {nullptr};
+  uint8_t* d_tcb[7] = {nullptr};  // per limb: the transform as a tensor-core operand (TC_B_BYTES)
   uint64_t* d_jumps = nullptr;
   std::mutex mu;              // guards the scratch below (Witness::row_evaluate takes &self)
   uint64_t* d_eq = nullptr;   // [wdim][3]

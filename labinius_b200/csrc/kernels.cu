@@ -2,8 +2,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 
 #include "kernels.cuh"
+#include "tcgen05.cuh"
 #include "launch.h"
 #include "transcript_dev.h"
 
@@ -280,6 +283,315 @@ __global__ void k_commit_finish(const int32_t* __restrict__ partial, int nchunks
 }
 
 // =============================================================================================
+// Commit on the tensor cores: the 162-point binary transform as a kind::i8 multiply
+// =============================================================================================
+// The transform of an F162 is linear in its bits: What(v) = sum_m bit_m T[m][v] with
+// T[m][v] = theta^{E[v] m} mod q. A step's 128 F162 (8 columns x 4 ring elements x 4 positions)
+// are the rows of an M = 128, N = 176, K = 384 multiply whose A row holds bit m at K-byte m and
+// 128 bit_m at K-byte 192 + m, and whose B (shared memory for the whole kernel) holds T split as
+// lo + 128 hi (tc_transform_operand): the s32 accumulator is the exact transform, < 2^22.
+//
+// The kernel is persistent: CTA b takes the work items b, b + gridDim.x, ... (an item is a tile of
+// 8 columns x a chunk of ring elements, partial[chunk][column] its output), and the steps of all
+// its items form one pipeline of two warp roles:
+//   producer (warp 16)  loads by bulk copies (cp.async.bulk, completion counted on mbarrier
+//            full[(g + 1) % 2]) step g + 1's witness rows and step g's key tile while step g is
+//            being prepared, then issues step g's 12 K-steps into tensor-memory accumulator g % 2
+//            and commits them to mbarrier mma[g % 2];
+//   compute (warps 0-15) per step g: expand step g's witness words into the A operand and meet the
+//            producer (named barrier 1); read step g - 1's accumulator (warp w: lanes of quadrant
+//            w % 4, leaves [40 (w / 4), + 40), warps 0-3 also 160-161), reduce to [0, 2q) into the
+//            transposed u16 tile What[ii][v][jj][k]; the module product with step g - 1's key
+//            tile, 16 multiply-adds per (ring element, leaf, column) accumulated in registers;
+//            release the key buffer (mbarrier kempty). After an item's last step its sums are
+//            written and the registers cleared.
+// Row r of a step is ring element ii = r / 32, column jj = (r / 4) % 8, position k = r % 4, so
+// warp quadrant ii holds ring element ii and its 32 lanes store 32 consecutive u16. Rows past the
+// item's columns or ring elements are zero (their words are not loaded).
+constexpr int TCC_CTHREADS = 512;                      // compute warps 0-15
+constexpr int TCC_THREADS = TCC_CTHREADS + 32;         // and the producer warp
+constexpr int TCC_CT = 8;                              // columns per item
+constexpr int TCC_RT = 4;                              // ring elements per step
+constexpr int TCC_WROW = TCC_RT * 12 + 2;              // staged witness words per column (400 bytes)
+constexpr int TCC_A_BYTES = 16 * TC_GROUP_BYTES;       // 128 rows x 384 bytes
+constexpr int TCC_WT_BYTES = TCC_RT * N162 * TCC_CT * 4 * 2;
+constexpr int TCC_AT_BYTES = TCC_RT * N162 * 32;       // a step's key tile
+constexpr int TCC_WTILE_BYTES = TCC_CT * TCC_WROW * 8;
+constexpr int TCC_OFF_A = TC_B_BYTES;
+constexpr int TCC_OFF_WT = TCC_OFF_A + TCC_A_BYTES;
+constexpr int TCC_OFF_AT = TCC_OFF_WT + TCC_WT_BYTES;          // two key tiles
+constexpr int TCC_OFF_WTILE = TCC_OFF_AT + 2 * TCC_AT_BYTES;   // two witness tiles
+constexpr int TCC_OFF_BAR = TCC_OFF_WTILE + 2 * TCC_WTILE_BYTES;
+constexpr int TCC_SMEM = TCC_OFF_BAR + 96 + 128;       // + barriers, tensor-memory slot, flag, alignment
+constexpr int TCC_VPT = 3;                             // leaves per thread in the module product
+constexpr uint32_t TCC_TMEM_COLS = 512;                // two accumulators at columns 0 and 256
+constexpr long long TC_WAIT_BUDGET = 2000000000ll;     // cycles (about a second) before a timeout
+
+static_assert(TCC_OFF_A % 128 == 0 && TCC_OFF_AT % 16 == 0 && TCC_OFF_WTILE % 16 == 0 && TCC_OFF_BAR % 8 == 0,
+              "alignment");
+static_assert(TCC_SMEM <= 232448, "shared memory per CTA");
+
+// A device-wide flag set by a tensor-core kernel whose bounded wait ran out (never in practice:
+// what it waits for takes microseconds). The host reads and clears it.
+__device__ int g_tc_timeout = 0;
+
+// Expand F162 bits 16c .. 16c + 15 of a row into the A operand: 16 bytes of bit values at K-chunk
+// c, and the same times 128 at K-chunk c + 12.
+__device__ __forceinline__ void tc_expand_chunk(uint8_t* sA, int r, int c, uint32_t u) {
+  uint4 b;
+  b.x = ((u & 15u) * 0x00204081u) & 0x01010101u;
+  b.y = (((u >> 4) & 15u) * 0x00204081u) & 0x01010101u;
+  b.z = (((u >> 8) & 15u) * 0x00204081u) & 0x01010101u;
+  b.w = (((u >> 12) & 15u) * 0x00204081u) & 0x01010101u;
+  uint8_t* p = sA + (r >> 3) * TC_GROUP_BYTES + c * 128 + (r & 7) * 16;
+  *(uint4*)p = b;
+  *(uint4*)(p + 12 * 128) = make_uint4(b.x << 7, b.y << 7, b.z << 7, b.w << 7);
+}
+
+// Row tid % 128 of the A operand from its F162's words (zero when !valid; at most 34 bits in the
+// third word), by `threads` threads (a multiple of 128).
+__device__ __forceinline__ void tc_build_row(uint8_t* sA, int tid, int threads, const uint64_t* e, bool valid) {
+  const int r = tid & 127;
+  const uint64_t w0 = valid ? e[0] : 0, w1 = valid ? e[1] : 0, w2 = valid ? e[2] & ((1ull << 34) - 1) : 0;
+  for (int c = tid >> 7; c < 12; c += threads >> 7) {
+    const uint64_t word = c < 4 ? w0 : c < 8 ? w1 : w2;
+    tc_expand_chunk(sA, r, c, (uint32_t)(word >> (16 * (c & 3))) & 0xFFFFu);
+  }
+}
+
+// Issue the 12 K-steps of one 128 x 176 x 384 transform multiply and commit them to `bar`.
+__device__ __forceinline__ void tc_transform_mma(uint32_t d_tmem, uint32_t sA_u, uint32_t sB_u, uint64_t* bar) {
+  constexpr uint32_t IDESC = tc::idesc_u8(128, TC_LEAVES);
+#pragma unroll
+  for (int kk = 0; kk < TC_KBYTES / 32; kk++)
+    tc::mma_i8(d_tmem, tc::smem_desc(sA_u + kk * 256, 128, TC_GROUP_BYTES),
+               tc::smem_desc(sB_u + kk * 256, 128, TC_GROUP_BYTES), IDESC, kk > 0);
+  tc::commit_to(bar);
+}
+
+// A bounded mbarrier wait that records a timeout in the CTA's flag and is skipped once it is set.
+__device__ __forceinline__ void tc_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  if (*abort) return;
+  if (!tc::mbar_wait(bar, parity, TC_WAIT_BUDGET)) *abort = 1;
+}
+
+// The CTA's work items in order, each a run of steps.
+struct TcItems {
+  int first, stride, total, col_tiles, chunk, len_ring;
+  __device__ int steps(int it) const {
+    const int i0 = (it / col_tiles) * chunk;
+    const int i1 = min(len_ring, i0 + chunk);
+    return i1 > i0 ? (i1 - i0 + TCC_RT - 1) / TCC_RT : 0;
+  }
+  __device__ int i0(int it, int st) const { return (it / col_tiles) * chunk + st * TCC_RT; }
+  // ring elements present in step st of item it
+  __device__ int n(int it, int st) const {
+    return min(TCC_RT, min(len_ring, (it / col_tiles) * chunk + chunk) - i0(it, st));
+  }
+  // the step after (it, st); it >= total when there is none
+  __device__ void next(int& it, int& st) const {
+    if (++st < steps(it)) return;
+    st = 0;
+    do it += stride;
+    while (it < total && steps(it) == 0);
+  }
+};
+
+template <int PI>
+__global__ void __launch_bounds__(TCC_THREADS, 1)
+    k_commit_tc(const uint64_t* __restrict__ W, size_t wdim, const int4* __restrict__ Ahat,
+                const uint8_t* __restrict__ tcb, int cols, int len_ring, int chunk, int nchunks,
+                int32_t* __restrict__ partial /* [nchunks][cols][162][4] */) {
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint8_t* sB = smem;
+  uint8_t* sA = smem + TCC_OFF_A;
+  uint16_t* wt = (uint16_t*)(smem + TCC_OFF_WT);
+  int4* atile = (int4*)(smem + TCC_OFF_AT);           // [2][4][162][2]
+  uint64_t* wtile = (uint64_t*)(smem + TCC_OFF_WTILE);  // [2][8][50]
+  uint64_t* full = (uint64_t*)(smem + TCC_OFF_BAR);     // [2]: step g's words and step g - 1's key tile
+  uint64_t* mma = full + 2;                             // [2]: step g's multiply done
+  uint64_t* kempty = full + 4;                          // [2]: the key buffer of step g - 2 read
+  uint64_t* bfull = full + 6;                           // the transform operand loaded
+  uint32_t* tslot = (uint32_t*)(full + 7);
+  volatile int* abort = (volatile int*)(full + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int col_tiles = (cols + TCC_CT - 1) / TCC_CT;
+  const TcItems items{(int)blockIdx.x, (int)gridDim.x, col_tiles * nchunks, col_tiles, chunk, len_ring};
+  int first = items.first;
+  while (first < items.total && items.steps(first) == 0) first += items.stride;
+  int S = 0;  // the CTA's steps
+  for (int it = first; it < items.total; it += items.stride) S += items.steps(it);
+
+  if (tid == 0) {
+    for (int b = 0; b < 7; b++) tc::mbar_init(&full[b], 1);
+    *abort = 0;
+    tc::mbar_init_fence();
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, TCC_TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tslot;
+
+  if (warp == TCC_CTHREADS / 32) {
+    // ---------------- producer ----------------
+    // the witness rows of step (it, st) into tile buffer b, bytes counted on full[b]
+    auto load_words = [&](int it, int st, int b) {
+      const int j0 = (it % col_tiles) * TCC_CT, i0 = items.i0(it, st), n = items.n(it, st);
+      for (int jj = 0; jj < TCC_CT && j0 + jj < cols; jj++)
+        tc::bulk_g2s(wtile + (b * TCC_CT + jj) * TCC_WROW, W + ((size_t)(j0 + jj) * wdim + (size_t)4 * i0) * 3,
+                     96u * n, &full[b]);
+    };
+    auto word_bytes = [&](int it, int st) {
+      return 96u * items.n(it, st) * min(TCC_CT, cols - (it % col_tiles) * TCC_CT);
+    };
+    const uint32_t sA_u = tc::smem_u32(sA), sB_u = tc::smem_u32(sB);
+    if (lane == 0 && S > 0) {
+      tc::mbar_arrive_expect_tx(bfull, TC_B_BYTES);
+      for (int x = 0; x < 4; x++)
+        tc::bulk_g2s(sB + x * (TC_B_BYTES / 4), tcb + x * (TC_B_BYTES / 4), TC_B_BYTES / 4, bfull);
+      tc::mbar_arrive_expect_tx(&full[0], word_bytes(first, 0));
+      load_words(first, 0, 0);
+    }
+    int it = first, st = 0;
+    for (int g = 0; g < S; g++) {
+      int nit = it, nst = st;
+      items.next(nit, nst);
+      if (lane == 0) {
+        // compute iteration g + 1 reads step g + 1's words and step g's key tile (buffer g % 2,
+        // whose previous tile, step g - 2's, the compute warps have released)
+        if (g >= 2) tc_wait(&kempty[g & 1], ((g - 2) >> 1) & 1, abort);
+        const uint32_t kb = (uint32_t)items.n(it, st) * N162 * 32;
+        const uint32_t wb = nit < items.total ? word_bytes(nit, nst) : 0u;
+        tc::mbar_arrive_expect_tx(&full[(g + 1) & 1], kb + wb);
+        tc::bulk_g2s(atile + (g & 1) * (TCC_RT * N162 * 2), Ahat + (size_t)items.i0(it, st) * N162 * 2, kb,
+                     &full[(g + 1) & 1]);
+        if (nit < items.total) load_words(nit, nst, (g + 1) & 1);
+      }
+      __syncwarp();
+      tc::named_sync(1, TCC_THREADS);  // step g's A operand is built
+      if (lane == 0) {
+        tc::fence_after_sync();
+        if (g == 0) tc_wait(bfull, 0, abort);
+        if (!*abort)
+          tc_transform_mma(tmem + (uint32_t)(g & 1) * 256u, sA_u, sB_u, &mma[g & 1]);
+        else
+          tc::mbar_arrive(&mma[g & 1]);
+      }
+      __syncwarp();
+      it = nit;
+      st = nst;
+    }
+  } else if (S > 0) {
+    // ---------------- compute ----------------
+    const int jj_b = lane & 7, sub = lane >> 3;
+    int32_t acc[TCC_VPT][4];
+#pragma unroll
+    for (int u = 0; u < TCC_VPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
+    constexpr int RED = CommitRed<PI>::value;
+    int since = 0;
+    int it = first, st = 0, p_it = -1, p_st = 0;
+    const int r = tid & 127;
+    for (int g = 0; g <= S; g++) {
+      tc_wait(&full[g & 1], (g >> 1) & 1, abort);                          // step g's words, step g - 1's key tile
+      if (g >= 1) tc_wait(&mma[(g - 1) & 1], ((g - 1) >> 1) & 1, abort);  // A free, accumulator g - 1 ready
+      if (g < S) {
+        const int jj = (r >> 2) & 7, ii = r >> 5;
+        const bool valid = (it % col_tiles) * TCC_CT + jj < cols && ii < items.n(it, st);
+        tc_build_row(sA, tid, TCC_CTHREADS, wtile + ((g & 1) * TCC_CT + jj) * TCC_WROW + (ii * 4 + (r & 3)) * 3,
+                     valid);
+        tc::fence_async_shared();
+        tc::fence_before_sync();
+        tc::named_sync(1, TCC_THREADS);  // meets the producer: lockstep, even when a wait timed out
+      }
+      if (g >= 1) {
+        const int nst = items.n(p_it, p_st);
+        tc::fence_after_sync();
+        {
+          const int quad = warp & 3, part = warp >> 2;
+          const uint32_t taddr = tmem + (uint32_t)((g - 1) & 1) * 256u + ((uint32_t)(32 * quad) << 16);
+          uint16_t* dst = wt + quad * N162 * 32 + lane;
+#pragma unroll
+          for (int c = 0; c < 5; c++) {
+            uint32_t x[8];
+            tc::tmem_ld8(taddr + 40 * part + 8 * c, x);
+#pragma unroll
+            for (int i = 0; i < 8; i++) dst[(40 * part + 8 * c + i) * 32] = (uint16_t)red_half<PI>(x[i]);
+          }
+          if (part == 0) {
+            uint32_t y[2];
+            tc::tmem_ld2(taddr + 160, y);
+            dst[160 * 32] = (uint16_t)red_half<PI>(y[0]);
+            dst[161 * 32] = (uint16_t)red_half<PI>(y[1]);
+          }
+        }
+        tc::fence_before_sync();
+        tc::named_sync(2, TCC_CTHREADS);  // the transform tile is complete
+        const int4* kt = atile + ((g - 1) & 1) * (TCC_RT * N162 * 2);
+        for (int ii = 0; ii < nst; ii++) {
+          const int4* ah = kt + ii * N162 * 2;
+#pragma unroll
+          for (int u = 0; u < TCC_VPT; u++) {
+            const int v = 4 * (warp + 16 * u) + sub;
+            if (v < N162) {
+              const uint2 wv = *(const uint2*)(wt + (((ii * N162) + v) * TCC_CT + jj_b) * 4);
+              const int32_t w0 = wv.x & 0xFFFF, w1 = wv.x >> 16, w2 = wv.y & 0xFFFF, w3 = wv.y >> 16;
+              const int4 lo = ah[2 * v], hi = ah[2 * v + 1];
+              acc[u][0] += lo.x * w0 + hi.x * w3 + hi.y * w2 + hi.z * w1;
+              acc[u][1] += lo.y * w0 + lo.x * w1 + hi.y * w3 + hi.z * w2;
+              acc[u][2] += lo.z * w0 + lo.y * w1 + lo.x * w2 + hi.z * w3;
+              acc[u][3] += lo.w * w0 + lo.z * w1 + lo.y * w2 + lo.x * w3;
+            }
+          }
+          if (++since >= RED) {
+            since = 0;
+#pragma unroll
+            for (int u = 0; u < TCC_VPT; u++)
+#pragma unroll
+              for (int c = 0; c < 4; c++) acc[u][c] = red_signed<PI>(acc[u][c]);
+          }
+        }
+        if (p_st + 1 == items.steps(p_it)) {
+          // the item's last step: its sums out, the registers cleared
+          const int j = (p_it % col_tiles) * TCC_CT + jj_b;
+          if (j < cols) {
+#pragma unroll
+            for (int u = 0; u < TCC_VPT; u++) {
+              const int v = 4 * (warp + 16 * u) + sub;
+              if (v < N162) {
+                int4 o;
+                o.x = (int)red_signed_full<PI>(acc[u][0]);
+                o.y = (int)red_signed_full<PI>(acc[u][1]);
+                o.z = (int)red_signed_full<PI>(acc[u][2]);
+                o.w = (int)red_signed_full<PI>(acc[u][3]);
+                ((int4*)partial)[((size_t)(p_it / col_tiles) * cols + j) * N162 + v] = o;
+              }
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < TCC_VPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
+          since = 0;
+        }
+        tc::fence_async_shared();         // this thread's reads of the key tile precede the next bulk copy into it
+        tc::named_sync(2, TCC_CTHREADS);  // the transform tile and the key tile are free
+        if (tid == 0) tc::mbar_arrive(&kempty[(g - 1) & 1]);
+      }
+      p_it = g < S ? it : -1;
+      p_st = st;
+      if (g < S) items.next(it, st);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, TCC_TMEM_COLS);
+  if (tid == 0 && *abort) atomicExch(&g_tc_timeout, 1);
+}
+
+// =============================================================================================
 // Fold: v_p = sum_j c_j(-Y) w_{j,p}(Y) in Z_q[Y]/(Y^162 - Y^81 + 1), one F162 position p at a time
 // =============================================================================================
 // Challenge slot values: chat[j][leaf] = c_j(-theta^{E[leaf]}) (crates/pcs/src/fold.rs:287-335).
@@ -507,6 +819,228 @@ __global__ void __launch_bounds__(256, 2)
     }
     __syncthreads();
     fold_positions_out<PI>(vh, p0, wdim, D, v_out);
+  }
+}
+
+// =============================================================================================
+// Fold on the tensor cores: the base limb's transforms by the same kind::i8 multiply
+// =============================================================================================
+// A work item is 128 consecutive positions p of the witness x a split of columns [c0, c1); the
+// kernel is persistent (CTA b takes items b, b + gridDim.x, ...) and all its items' steps, one
+// column each, form one pipeline of two warp roles:
+//   producer (warp 12)  loads step g + 1's 128 F162 (3 KB, one bulk copy counted on mbarrier
+//            full[(g + 1) % 2]) and issues step g's multiply into tensor-memory accumulator g % 2
+//            (mbarrier mma[g % 2]) as soon as its A operand (buffer g % 2) is built;
+//   compute (warps 0-11) per step g: expand step g's words into A buffer g % 2 and meet the
+//            producer (named barrier 1); read step g - 1's accumulator (warp w: the lanes of
+//            quadrant w % 4 = positions, leaves [56 (w / 4), + 56) up to 162), reduce to [0, 2q)
+//            and add chat_j(v) What_{j,p}(v) into per-thread accumulators; load step g + 1's chat
+//            row into ctile[(g + 1) % 3].
+// After an item's last column its sums, reduced to [0, q), are added into the transposed scratch
+// vhat_t[v][p] (u32, zeroed by the caller; a warp's 32 positions are one coalesced atomic add; at
+// most 2^16 splits keep the total below 2^32) and k_fold_finish_t inverts.
+constexpr int TCF_CTHREADS = 384;  // 12 compute warps: with the producer, 128 registers a thread
+constexpr int TCF_THREADS = TCF_CTHREADS + 32;
+constexpr int TCF_ROWS = 128;
+constexpr int TCF_WT_BYTES = TCF_ROWS * 24;  // one step's witness words
+constexpr int TCF_OFF_A = TC_B_BYTES;        // two A buffers
+constexpr int TCF_OFF_WTILE = TCF_OFF_A + 2 * TCC_A_BYTES;
+constexpr int TCF_OFF_CT = TCF_OFF_WTILE + 2 * TCF_WT_BYTES;
+constexpr int TCF_OFF_BAR = TCF_OFF_CT + 3 * 176 * 4;
+constexpr int TCF_SMEM = TCF_OFF_BAR + 64 + 128;
+constexpr uint32_t TCF_TMEM_COLS = 512;
+static_assert(TCF_OFF_WTILE % 16 == 0 && TCF_OFF_CT % 16 == 0 && TCF_OFF_BAR % 8 == 0, "alignment");
+static_assert(TCF_SMEM <= 232448, "shared memory per CTA");
+
+template <int PI>
+__global__ void __launch_bounds__(TCF_THREADS, 1)
+    k_fold_tc(const uint64_t* __restrict__ W, size_t wdim, int cols, int cols_per_split,
+              const uint32_t* __restrict__ chat, const uint8_t* __restrict__ tcb, uint32_t* __restrict__ vhat_t,
+              const int* __restrict__ split_inst) {
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint8_t* sB = smem;
+  uint8_t* sA = smem + TCF_OFF_A;
+  uint64_t* wtile = (uint64_t*)(smem + TCF_OFF_WTILE);
+  uint32_t* ctile = (uint32_t*)(smem + TCF_OFF_CT);  // [3][176]
+  uint64_t* full = (uint64_t*)(smem + TCF_OFF_BAR);  // [2]: step g's words
+  uint64_t* mma = full + 2;                          // [2]: step g's multiply done
+  uint64_t* bfull = full + 4;
+  uint32_t* tslot = (uint32_t*)(full + 5);
+  volatile int* abort = (volatile int*)(full + 6);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles = (int)((wdim + TCF_ROWS - 1) / TCF_ROWS);
+  const int splits = (cols + cols_per_split - 1) / cols_per_split;
+  const int total = tiles * splits;
+  // item it: position tile it % tiles, split it / tiles; step st is its column col0 + st
+  auto col0 = [&](int it) { return (it / tiles) * cols_per_split; };
+  auto ncol = [&](int it) { return max(0, min(cols, col0(it) + cols_per_split) - col0(it)); };
+  auto next = [&](int& it, int& st) {
+    if (++st < ncol(it)) return;
+    st = 0;
+    do it += gridDim.x;
+    while (it < total && ncol(it) == 0);
+  };
+  int first = blockIdx.x;
+  while (first < total && ncol(first) == 0) first += gridDim.x;
+  int S = 0;
+  for (int it = first; it < total; it += gridDim.x) S += ncol(it);
+
+  if (tid == 0) {
+    for (int b = 0; b < 5; b++) tc::mbar_init(&full[b], 1);
+    *abort = 0;
+    tc::mbar_init_fence();
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, TCF_TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tslot;
+
+  if (warp == TCF_CTHREADS / 32) {
+    // ---------------- producer ----------------
+    auto load_words = [&](int it, int st, int b) {
+      const size_t p0 = (size_t)(it % tiles) * TCF_ROWS;
+      tc::mbar_arrive_expect_tx(&full[b], TCF_WT_BYTES);
+      tc::bulk_g2s(wtile + b * (TCF_ROWS * 3), W + ((size_t)(col0(it) + st) * wdim + p0) * 3, TCF_WT_BYTES, &full[b]);
+    };
+    const uint32_t sA_u = tc::smem_u32(sA), sB_u = tc::smem_u32(sB);
+    if (lane == 0 && S > 0) {
+      tc::mbar_arrive_expect_tx(bfull, TC_B_BYTES);
+      for (int x = 0; x < 4; x++)
+        tc::bulk_g2s(sB + x * (TC_B_BYTES / 4), tcb + x * (TC_B_BYTES / 4), TC_B_BYTES / 4, bfull);
+      load_words(first, 0, 0);
+    }
+    int it = first, st = 0;
+    for (int g = 0; g < S; g++) {
+      int nit = it, nst = st;
+      next(nit, nst);
+      // step g + 1's words into buffer (g + 1) % 2, whose step g - 1 the compute warps have expanded
+      if (lane == 0 && nit < total) load_words(nit, nst, (g + 1) & 1);
+      __syncwarp();
+      tc::named_sync(1, TCF_THREADS);  // step g's A operand is built
+      if (lane == 0) {
+        tc::fence_after_sync();
+        if (g == 0) tc_wait(bfull, 0, abort);
+        if (!*abort)
+          tc_transform_mma(tmem + (uint32_t)(g & 1) * 256u, sA_u + (uint32_t)(g & 1) * TCC_A_BYTES, sB_u, &mma[g & 1]);
+        else
+          tc::mbar_arrive(&mma[g & 1]);
+      }
+      __syncwarp();
+      it = nit;
+      st = nst;
+    }
+  } else if (S > 0) {
+    // ---------------- compute ----------------
+    const int quad = warp & 3, part = warp >> 2;
+    const int v0 = 56 * part;  // leaves v0 .. v0 + 55 (v0 + 49 for the last part)
+    const int row = 32 * quad + lane;
+    uint32_t acc[56];
+#pragma unroll
+    for (int i = 0; i < 56; i++) acc[i] = 0;
+    constexpr int RED = FoldRed<PI>::value;
+    int since = 0;
+    int it = first, st = 0, p_it = -1, p_st = 0;
+    // step 0's chat row
+    if (tid < N162) ctile[tid] = chat[(size_t)col0(first) * N162 + tid];
+    tc::named_sync(2, TCF_CTHREADS);
+    for (int g = 0; g <= S; g++) {
+      int nit = it, nst = st;
+      if (g < S) next(nit, nst);
+      // step g + 1's chat row, stored at the end of the iteration
+      uint32_t cnext = 0;
+      const bool has_next = g + 1 < S && tid < N162;
+      if (has_next) cnext = __ldg(chat + (size_t)(col0(nit) + nst) * N162 + tid);
+      if (g < S) {
+        tc_wait(&full[g & 1], (g >> 1) & 1, abort);                   // step g's words
+        if (g >= 2) tc_wait(&mma[g & 1], ((g - 2) >> 1) & 1, abort);  // A buffer g % 2 free
+        tc_build_row(sA + (g & 1) * TCC_A_BYTES, tid, TCF_CTHREADS, wtile + (g & 1) * (TCF_ROWS * 3) + (tid & 127) * 3,
+                     true);
+        tc::fence_async_shared();
+        tc::fence_before_sync();
+        tc::named_sync(1, TCF_THREADS);  // meets the producer: lockstep, even when a wait timed out
+      }
+      if (g >= 1) {
+        tc_wait(&mma[(g - 1) & 1], ((g - 1) >> 1) & 1, abort);  // step g - 1's accumulator
+        tc::fence_after_sync();
+        const uint32_t taddr = tmem + (uint32_t)((g - 1) & 1) * 256u + ((uint32_t)(32 * quad) << 16);
+        const uint32_t* ch = ctile + ((g - 1) % 3) * 176;
+#pragma unroll
+        for (int c = 0; c < 7; c++) {
+          if (part < 2 || c < 6) {
+            uint32_t x[8];
+            tc::tmem_ld8(taddr + v0 + 8 * c, x);
+#pragma unroll
+            for (int i = 0; i < 8; i += 4) {
+              const uint4 c4 = *(const uint4*)(ch + v0 + 8 * c + i);
+              acc[8 * c + i] += c4.x * red_half<PI>(x[i]);
+              acc[8 * c + i + 1] += c4.y * red_half<PI>(x[i + 1]);
+              acc[8 * c + i + 2] += c4.z * red_half<PI>(x[i + 2]);
+              acc[8 * c + i + 3] += c4.w * red_half<PI>(x[i + 3]);
+            }
+          } else {
+            uint32_t y[2];
+            tc::tmem_ld2(taddr + 160, y);  // the last part's leaves 160 and 161
+            acc[48] += ch[160] * red_half<PI>(y[0]);
+            acc[49] += ch[161] * red_half<PI>(y[1]);
+          }
+        }
+        tc::fence_before_sync();
+        if (++since >= RED) {
+          since = 0;
+#pragma unroll
+          for (int i = 0; i < 56; i++) acc[i] = red_half<PI>(acc[i]);
+        }
+        if (p_st + 1 == ncol(p_it)) {
+          // the item's last column: its sums into vhat_t, a warp's 32 positions per add
+          const size_t p0 = (size_t)(p_it % tiles) * TCF_ROWS;
+          uint32_t* dst = vhat_t + (split_inst ? (size_t)split_inst[p_it / tiles] * wdim * N162 : 0) + p0 + row;
+          if (p0 + row < wdim) {
+#pragma unroll
+            for (int i = 0; i < 56; i++)
+              if (part < 2 || i < 50) atomicAdd(dst + (size_t)(v0 + i) * wdim, red_full<PI>(acc[i]));
+          }
+#pragma unroll
+          for (int i = 0; i < 56; i++) acc[i] = 0;
+          since = 0;
+        }
+      }
+      if (has_next) ctile[((g + 1) % 3) * 176 + tid] = cnext;
+      tc::named_sync(2, TCF_CTHREADS);  // the chat row of step g + 1 is in place
+      p_it = g < S ? it : -1;
+      p_st = st;
+      it = nit;
+      st = nst;
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, TCF_TMEM_COLS);
+  if (tid == 0 && *abort) atomicExch(&g_tc_timeout, 1);
+}
+
+// The inverse transform of each position's sums from the transposed scratch vhat_t (per instance
+// [162][wdim]), centred into the folded witness, as k_fold_finish.
+template <int PI>
+__global__ void __launch_bounds__(216) k_fold_finish_t(const uint32_t* __restrict__ vhat_t, size_t wdim,
+                                                       size_t positions, const DevPrime* __restrict__ D,
+                                                       int16_t* __restrict__ v_out /* [len_ring][648] */) {
+  __shared__ uint32_t xs[4][N162];
+  const int g = threadIdx.x / 54, j = threadIdx.x - 54 * g;
+  const size_t p = (size_t)blockIdx.x * 4 + g;
+  const size_t inst = p / wdim, pl = p - inst * wdim;
+  const uint32_t* src = vhat_t + inst * wdim * N162 + pl;
+  for (int v = j; v < N162; v += 54) xs[g][v] = p < positions ? src[(size_t)v * wdim] % Pr<PI>::q : 0;
+  __syncthreads();
+  intt162_group<PI>(xs[g], j, *D);
+  if (p < positions) {
+    const size_t i = p / 4;
+    const int k = (int)(p % 4);
+    for (int m = j; m < N162; m += 54) v_out[i * N648 + 4 * m + k] = center<PI>(xs[g][m]);
   }
 }
 
@@ -1520,34 +2054,82 @@ cudaError_t launch_key_components(int pi, const int16_t* A, const DevPrime* D, i
 
 size_t commit_smem_bytes() { return LUT_BYTES + CT * WROW * 8 + RT * N162 * CT * 4 * 2 + AT_BYTES; }
 
+// The commit's transforms run on the tensor cores (k_commit_tc) when LBG_COMMIT_KERNEL=tc, else on
+// the CUDA cores (k_commit) (both are exact; the switch is for comparing them). The commit
+// that keeps the base limb's transform for the fold always runs the CUDA-core kernel.
+bool commit_tc_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("LBG_COMMIT_KERNEL");
+    return e && std::string(e) == "tc";
+  }();
+  return on;
+}
+
 int commit_blocks_per_sm(int pi) {
   int n = 0;
-  size_t smem = commit_smem_bytes();
+  const bool tcm = commit_tc_enabled();
+  size_t smem = tcm ? (size_t)TCC_SMEM : commit_smem_bytes();
   cudaError_t e = cudaErrorInvalidValue;
   switch (pi) {
-#define LBG_OCC(I)                                                                                      \
-  case I:                                                                                               \
-    cudaFuncSetAttribute(k_commit<I, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_commit<I, false>, 256, smem);               \
+#define LBG_OCC(I)                                                                                        \
+  case I:                                                                                                 \
+    if (tcm) {                                                                                            \
+      cudaFuncSetAttribute(k_commit_tc<I>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_commit_tc<I>, TCC_THREADS, smem);           \
+    } else {                                                                                              \
+      cudaFuncSetAttribute(k_commit<I, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_commit<I, false>, 256, smem);               \
+    }                                                                                                     \
     break;
     LBG_OCC(0) LBG_OCC(1) LBG_OCC(2) LBG_OCC(3) LBG_OCC(4) LBG_OCC(5) LBG_OCC(6)
 #undef LBG_OCC
   }
   return (e == cudaSuccess && n > 0) ? n : 1;
 }
-int commit_cols_per_cta() { return CT; }
-int commit_ring_per_step() { return RT; }
+int commit_cols_per_cta() { return commit_tc_enabled() ? TCC_CT : CT; }
+int commit_ring_per_step() {
+  static_assert(RT == TCC_RT, "both commit kernels step over the same ring elements");
+  return RT;
+}
+
+int tc_timeout_take() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_tc_timeout, sizeof(int)) != cudaSuccess) return -1;
+  if (v) {
+    int z = 0;
+    cudaMemcpyToSymbol(g_tc_timeout, &z, sizeof(int));
+  }
+  return v;
+}
+
+static int sm_count() {
+  int dev = 0, nsm = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  return nsm;
+}
 
 cudaError_t launch_commit(int pi, const uint64_t* W, size_t wdim, const int4* Ahat, const DevPrime* D, int cols,
-                          int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st, uint16_t* keep) {
-  dim3 grid((cols + CT - 1) / CT, nchunks);
-  size_t smem = commit_smem_bytes();
+                          int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st, uint16_t* keep,
+                          const uint8_t* tcb) {
   if (keep) {
+    dim3 grid((cols + CT - 1) / CT, nchunks);
+    size_t smem = commit_smem_bytes();
     LBG_DISPATCH(pi, ({
                    cudaFuncSetAttribute(k_commit<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                    k_commit<P, true><<<grid, 256, smem, st>>>(W, wdim, Ahat, D, cols, len_ring, chunk, partial, keep);
                  }));
+  } else if (tcb && commit_tc_enabled()) {
+    // persistent: one CTA per SM (at most one per work item) over the column tiles x chunks
+    const long items = (long)((cols + TCC_CT - 1) / TCC_CT) * nchunks;
+    dim3 grid((unsigned)std::max<long>(1, std::min<long>(items, sm_count())));
+    LBG_DISPATCH(pi, ({
+                   cudaFuncSetAttribute(k_commit_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, TCC_SMEM);
+                   k_commit_tc<P><<<grid, TCC_THREADS, TCC_SMEM, st>>>(W, wdim, Ahat, tcb, cols, len_ring, chunk,
+                                                                       nchunks, partial);
+                 }));
   } else {
+    dim3 grid((cols + CT - 1) / CT, nchunks);
+    size_t smem = commit_smem_bytes();
     LBG_DISPATCH(pi, ({
                    cudaFuncSetAttribute(k_commit<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                    k_commit<P, false><<<grid, 256, smem, st>>>(W, wdim, Ahat, D, cols, len_ring, chunk, partial,
@@ -1591,9 +2173,37 @@ int fold_blocks_per_sm(int pi) {
   return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
+// The fold's transforms run on the tensor cores (k_fold_tc) when LBG_FOLD_KERNEL=tc, else on the
+// CUDA cores (k_fold) (both exact). The one-pass mode without scratch (vhat null) and the fold
+// from the kept transform always run on the CUDA cores.
+bool fold_tc_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("LBG_FOLD_KERNEL");
+    return e && std::string(e) == "tc";
+  }();
+  return on;
+}
+int fold_tc_positions_per_cta() { return TCF_ROWS; }
+
 cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
                         const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st, int instances,
-                        const int* split_inst) {
+                        const int* split_inst, const uint8_t* tcb) {
+  if (vhat && tcb && fold_tc_enabled()) {
+    int splits = (cols + cols_per_split - 1) / cols_per_split;
+    if (splits < 1 || splits > 65535) return cudaErrorInvalidValue;
+    const long items = (long)((wdim + TCF_ROWS - 1) / TCF_ROWS) * splits;
+    dim3 grid((unsigned)std::max<long>(1, std::min<long>(items, sm_count())));  // persistent, one CTA per SM
+    size_t positions = wdim * (size_t)instances;
+    cudaError_t e = cudaMemsetAsync(vhat, 0, positions * N162 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    LBG_DISPATCH(pi, ({
+                   cudaFuncSetAttribute(k_fold_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, TCF_SMEM);
+                   k_fold_tc<P><<<grid, TCF_THREADS, TCF_SMEM, st>>>(W, wdim, cols, cols_per_split, chat, tcb, vhat,
+                                                                     split_inst);
+                   k_fold_finish_t<P><<<blocks_for(positions, 4), 216, 0, st>>>(vhat, wdim, positions, D, v);
+                 }));
+    return cudaGetLastError();
+  }
   size_t smem = fold_smem_bytes();
   if (!vhat) {  // direct mode: one split, no scratch beyond chat
     dim3 grid(blocks_for(wdim, FP), 1);

@@ -41,9 +41,15 @@ int commit_blocks_per_sm(int pi);
 int commit_cols_per_cta();
 int commit_ring_per_step();
 // keep (optional): the base limb's transform of every F162, u16 [cols][162][wdim], for the fold.
+// tcb (optional): the limb's transform operand (tc_transform_operand, device memory); with it and
+// without keep, the transforms run on the tensor cores (k_commit_tc, persistent, one CTA per SM).
 cudaError_t launch_commit(int pi, const uint64_t* W, size_t wdim, const int4* Ahat, const DevPrime* D, int cols,
                           int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st,
-                          uint16_t* keep = nullptr);
+                          uint16_t* keep = nullptr, const uint8_t* tcb = nullptr);
+bool commit_tc_enabled();
+// 1 (and cleared) when a tensor-core kernel's bounded wait ran out since the last call, else 0;
+// -1 when the flag could not be read.
+int tc_timeout_take();
 cudaError_t launch_commit_finish(int pi, const int32_t* partial, int nchunks, int cols, const DevPrime* D,
                                  int limb, int limbs, int16_t* C, cudaStream_t st);
 cudaError_t launch_challenge_slots(int pi, const lbg_challenge_d* ch, int r, const DevPrime* D, uint32_t* chat,
@@ -57,9 +63,14 @@ int fold_blocks_per_sm(int pi);
 // the fold runs in one pass over all columns, each CTA inverting its own positions.
 // Many instances of the same column length (instances > 1): their columns one after another, each
 // split within one instance (split_inst[s] its instance), vhat and v one instance after another.
+// tcb (optional): the base limb's transform operand; with it and vhat, the transforms run on the
+// tensor cores (k_fold_tc, 128 positions per work item, persistent, one CTA per SM); vhat is then
+// read transposed ([instance][162][wdim]).
 cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
                         const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st, int instances = 1,
-                        const int* split_inst = nullptr);
+                        const int* split_inst = nullptr, const uint8_t* tcb = nullptr);
+bool fold_tc_enabled();
+int fold_tc_positions_per_cta();
 // The fold from the commit's kept transform instead of the witness (same splits and outputs).
 cudaError_t launch_fold_kept(int pi, const uint16_t* keep, size_t wdim, int cols, int cols_per_split,
                              const uint32_t* chat, const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st,

@@ -298,4 +298,18 @@ const std::vector<uint64_t>& xorshift_jumps() {
   return J;
 }
 
+void tc_transform_operand(const PrimeTables& T, uint8_t* out) {
+  for (int i = 0; i < TC_B_BYTES; i++) out[i] = 0;
+  for (int v = 0; v < N162; v++) {
+    uint64_t x = 1;
+    for (int m = 0; m < N162; m++) {
+      const uint32_t t = (uint32_t)x;
+      const int lo_kb = m, hi_kb = 192 + m;
+      out[(v / 8) * TC_GROUP_BYTES + (lo_kb / 16) * 128 + (v % 8) * 16 + lo_kb % 16] = (uint8_t)(t & 127u);
+      out[(v / 8) * TC_GROUP_BYTES + (hi_kb / 16) * 128 + (v % 8) * 16 + hi_kb % 16] = (uint8_t)(t >> 7);
+      x = x * T.theta_leaf[v] % T.q;
+    }
+  }
+}
+
 }  // namespace lbg

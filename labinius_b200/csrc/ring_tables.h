@@ -78,6 +78,19 @@ const RefTables& ref_tables();
 struct Ntt648Tables;
 const Ntt648Tables* ntt648_tables(uint32_t q);
 
+// The 162-point binary transform as a tensor-core operand: the matrix T[m][v] = theta^{E[v] m}
+// (bit m of an F162 times the value of Y^m at leaf v), split into T = lo + 128 hi with lo < 128 and
+// hi < 256 and laid out as the B operand of a kind::i8 multiply (N = 176 leaf rows, the last 14
+// zero; K = 384 bytes: lo for m < 162 at K-byte m, hi at K-byte 192 + m, zeros elsewhere), K-major
+// without swizzle: byte (v, kb) at (v / 8) * 3072 + (kb / 16) * 128 + (v % 8) * 16 + kb % 16.
+// With the A operand of an F162 row holding bit m at K-byte m and 128 * bit m at K-byte 192 + m,
+// the s32 product is sum_m bit_m T[m][v] exactly (at most 162 (q - 1) < 2^22).
+constexpr int TC_LEAVES = 176;          // N of the transform multiply
+constexpr int TC_KBYTES = 384;          // K of the transform multiply, in bytes
+constexpr int TC_GROUP_BYTES = 3072;    // one 8-row group: 24 core matrices of 128 bytes
+constexpr int TC_B_BYTES = (TC_LEAVES / 8) * TC_GROUP_BYTES;  // 67584
+void tc_transform_operand(const PrimeTables& T, uint8_t* out /* TC_B_BYTES */);
+
 // xorshift64* state transition as GF(2) columns: jump[k][c] = T^(2^k) applied to e_c.
 const std::vector<uint64_t>& xorshift_jumps();  // 64 * 64 words
 
