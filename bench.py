@@ -633,8 +633,9 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
         return L.Params.new(11 + c, c, [L.Modulus.Q9721_FS_S])
 
     pp = L.PublicParameters.from_seed(params(7), MATRIX_SEED)
+    # small requests (at most 2^20 F162) on a slot of their own, so that none waits behind large ones
     srv = Server(pp, capacity_columns=8192, max_requests=64, slots=slots, host_threads=os.cpu_count() or 1,
-                 keep_results=False)
+                 keep_results=False, small_log_len=9)
 
     def run(idx, rate):
         reqs, t0 = [], time.perf_counter()
@@ -655,14 +656,14 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
         last = max(r.done for r in reqs)
         elems = sum(1 << int(logs[i]) for i in idx)
         lat = np.array([r.latency for r in reqs]) * 1000
-        return elems / (last - first), len(idx) / (last - first), lat
+        return elems / (last - first), len(idx) / (last - first), lat, np.array([int(logs[i]) for i in idx])
 
     run(range(min(64, requests)), None)  # warm-up: arenas, graphs of the host pool
     sat_n = min(requests, 2000)
-    sat_elems, sat_reqs, _ = run(range(sat_n), None)
+    sat_elems, sat_reqs, _, _ = run(range(sat_n), None)
     rate = load * sat_reqs
     b0 = srv.batches
-    st_elems, st_reqs, lat = run(range(requests), rate)
+    st_elems, st_reqs, lat, lat_logs = run(range(requests), rate)
     batches = srv.batches - b0
     srv.close()
 
@@ -687,9 +688,10 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
             claims[i] = b128_claim(proof.partials)
         else:
             wits.append(L.Witness.random(p, seeds[i]))
-    lat_plain = []
+    lat_plain, plain_logs = [], []
     t0 = time.perf_counter()
     for k, i in enumerate(sample):
+        plain_logs.append(int(logs[i]))
         s0 = time.perf_counter()
         p, prover, verifier = pps[col_logs[i]]
         w = wits[k]
@@ -707,7 +709,18 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
         lat_plain.append((time.perf_counter() - s0) * 1000)
     plain_s = time.perf_counter() - t0
     plain_elems = sum(1 << int(logs[i]) for i in sample) / plain_s
-    return {"requests": requests, "rate_req_s": rate, "load": load, "batches": batches,
+    lat_plain, plain_logs = np.array(lat_plain), np.array(plain_logs)
+    by_size = {}
+    for lg in range(18, 23):
+        sel, psel = lat[lat_logs == lg], lat_plain[plain_logs == lg]
+        by_size[str(lg)] = {"requests": int(len(sel)),
+                            "p50_ms": float(np.percentile(sel, 50)) if len(sel) else None,
+                            "p99_ms": float(np.percentile(sel, 99)) if len(sel) else None,
+                            "plain_p50_ms": float(np.percentile(psel, 50)) if len(psel) else None,
+                            "plain_p99_ms": float(np.percentile(psel, 99)) if len(psel) else None}
+    return {"requests": requests, "rate_req_s": rate, "load": load, "batches": batches, "by_log2_n": by_size,
+            "admission": "arenas within half the free HBM, at most 8192 columns a batch; requests of at most "
+                         "2^20 F162 on a slot of their own, the other slot large ones first",
             "throughput_elems_s": st_elems, "throughput_req_s": st_reqs,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()),

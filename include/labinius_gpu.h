@@ -119,12 +119,24 @@ int lbg_opening_matrix(const lbg_opening* op, int16_t* matrix_out);
 int lbg_opening_dropped(const lbg_opening* op, uint16_t* top_out, uint16_t* digits_out);
 /* Prover::recycle (crates/pcs/src/scheme/prover.rs:116-118): drop an unfolded opening. */
 void lbg_opening_free(lbg_opening* op);
+/* wire::pack_commitment (crates/pcs/src/wire/mod.rs:226-245): the opening's commitment packed on the
+ * device from where lbg_commit left it; ceil(log2 q) bits per slot per limb, LSB first, in the
+ * matrix's column-major order (Clear), or wire::pack_dropped of the top bits and digits
+ * (bit-dropped, :386-397). out null: returns the byte count only; else cap >= that count. Returns the
+ * byte count or a negative status. */
+long long lbg_opening_pack_commitment(const lbg_opening* op, uint8_t* out, size_t cap);
 
 /* Witness::row_evaluate (crates/pcs/src/scheme/witness.rs:100-106, crates/pcs/src/eval.rs:171-182):
  * u_out = columns F162. */
 int lbg_row_evaluate(const lbg_pp* pp, const lbg_witness* w, const uint64_t* p0, size_t p0_len,
                      uint64_t* u_out);
 /* Witness::mle_evaluate (crates/pcs/src/scheme/witness.rs:94-98, crates/pcs/src/eval.rs:185-193). */
+/* Witness::row_evaluate followed by wire::pack_row_evaluation (crates/pcs/src/wire/mod.rs:435-459),
+ * both on the device: the row values (u_out, optional, [columns][3]) and their 162-bit packing, LSB
+ * first (out; out null: returns the byte count only, ceil(162 columns / 8); else cap >= it). Returns
+ * the byte count or a negative status. */
+long long lbg_row_evaluate_packed(const lbg_pp* pp, const lbg_witness* w, const uint64_t* p0, size_t p0_len,
+                                  uint64_t* u_out, uint8_t* out, size_t cap);
 int lbg_mle_evaluate(const lbg_pp* pp, const lbg_witness* w, const uint64_t* p0, size_t p0_len,
                      const uint64_t* p1, size_t p1_len, uint64_t out[3]);
 
@@ -261,6 +273,12 @@ int lbg_batch_new(const lbg_pp* pp, const uint32_t* column_log_lens, size_t coun
 /* An arena sized once for max_cols columns and max_instances instances; lbg_batch_assign lays a
  * new set of instances out in it without allocating (what a serving loop reuses). */
 int lbg_batch_new_capacity(const lbg_pp* pp, size_t max_cols, size_t max_instances, lbg_batch** out);
+/* The device bytes lbg_batch_new_capacity allocates for that capacity (the kept transform and the
+ * switch workspace come on use, on top); with lbg_device_memory, what a server sizes its arenas by.
+ * No counterpart in the reference (it has no server). */
+size_t lbg_batch_arena_bytes(const lbg_pp* pp, size_t max_cols, size_t max_instances);
+/* cudaMemGetInfo on the parameters' device: free and total bytes of device memory. */
+int lbg_device_memory(const lbg_pp* pp, size_t* free_bytes, size_t* total_bytes);
 int lbg_batch_assign(lbg_batch* b, const uint32_t* column_log_lens, size_t count);
 void lbg_batch_free(lbg_batch* b);
 size_t lbg_batch_columns(const lbg_batch* b);

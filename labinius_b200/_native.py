@@ -51,6 +51,10 @@ SIGNATURES = {
     "lbg_opening_matrix": (_int, [_vp, _vp]),
     "lbg_opening_dropped": (_int, [_vp, _vp, _vp]),
     "lbg_opening_free": (None, [_vp]),
+    "lbg_opening_pack_commitment": (ctypes.c_longlong, [_vp, _vp, _sz]),
+    "lbg_row_evaluate_packed": (ctypes.c_longlong, [_vp, _vp, _vp, _sz, _vp, _vp, _sz]),
+    "lbg_batch_arena_bytes": (_sz, [_vp, _sz, _sz]),
+    "lbg_device_memory": (_int, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),
     "lbg_row_evaluate": (_int, [_vp, _vp, _vp, _sz, _vp]),
     "lbg_mle_evaluate": (_int, [_vp, _vp, _vp, _sz, _vp, _sz, _vp]),
     "lbg_fold": (_int, [_vp, _vp, _vp, _sz, _vp]),

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "liblabinius_gpu.so")
-SOURCES = ["api.cu", "kernels.cu", "fold_static.cu", "batch.cu", "transcript_dev.cu", "ntt_api.cu", "switch.cu", "wire.cu", "ring_tables.cpp", "blake3_host.cpp", "transcript.cpp"]
+SOURCES = ["api.cu", "kernels.cu", "fold_static.cu", "batch.cu", "transcript_dev.cu", "ntt_api.cu", "switch.cu", "wire.cu", "wire_pack.cu", "ring_tables.cpp", "blake3_host.cpp", "transcript.cpp"]
 HEADERS = ["kernels.cuh", "tcgen05.cuh", "gf2_dev.cuh", "prime_structs.h", "hasher_state.h", "blake3_dev.cuh", "transcript_dev.h", "switch.h", "upload.h", "error.h", "handles.h", "launch.h", "ring_tables.h", "blake3_host.h", "transcript.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -209,6 +209,7 @@ void lbg_public_parameters_free(lbg_pp* pp) {
   cudaFree(pp->d_ch);
   cudaFree(pp->d_chat);
   cudaFree(pp->d_fc);
+  cudaFree(pp->d_wire);
   lbg_switch_release(pp);
   if (pp->stream) cudaStreamDestroy(pp->stream);
   delete pp;
@@ -453,6 +454,7 @@ void lbg_prover_free(lbg_prover* pr) {
   cudaFree(pr->d_ch);
   cudaFree(pr->d_chat);
   cudaFree(pr->d_v);
+  cudaFree(pr->d_wire);
   cudaFree(pr->d_res);
   for (auto* b : pr->spare) free_bufs(b);
   for (auto& m : pr->marks) {
@@ -834,6 +836,13 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
   else
     lbg_opening_free(op);
   *w_out = w;
+  return LBG_OK;
+}
+
+int lbg_device_memory(const lbg_pp* pp, size_t* free_bytes, size_t* total_bytes) {
+  if (!pp || !free_bytes || !total_bytes) return fail(LBG_ERR_INVALID, "null argument");
+  LBG_CU(cudaSetDevice(pp->device));
+  LBG_CU(cudaMemGetInfo(free_bytes, total_bytes));
   return LBG_OK;
 }
 

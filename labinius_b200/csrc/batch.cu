@@ -389,6 +389,21 @@ void lbg_batch_free(lbg_batch* b) {
   delete b;
 }
 
+// The device bytes lbg_batch_new_capacity allocates for an arena of this size (the buffers below,
+// in the same order); the kept transform, the switch workspace and the packed bit-dropped bytes
+// are allocated later, on use.
+size_t lbg_batch_arena_bytes(const lbg_pp* pp, size_t max_cols, size_t max_instances) {
+  if (!pp) return 0;
+  const size_t L = (size_t)pp->limbs, C = max_cols, I = max_instances, wdim = pp->wdim;
+  const size_t count648 = C * N648;
+  size_t chunks = (pp->len_ring + commit_ring_per_step() - 1) / commit_ring_per_step();
+  if (chunks > 64) chunks = 64;
+  return C * wdim * 24 + C * sizeof(int) + C * sizeof(int4) + C * sizeof(int) + chunks * C * N162 * 16 +
+         C * 4 * L * N162 * 2 + L * count648 * 2 + count648 * 2 + (L > 1 ? L - 1 : 1) * count648 * 2 + I * 32 * 24 * 2 +
+         I * wdim * 24 + C * 24 + I * 24 + C * sizeof(lbg_challenge_d) + C * N162 * 4 + I * wdim * N162 * 4 +
+         I * pp->len_ring * N648 * 2 + 2 * I * sizeof(HasherState) + I * sizeof(RoundInst) + I * 32;
+}
+
 // An arena of `max_cols` columns and `max_instances` instances: the device buffers are sized once;
 // lbg_batch_assign lays out a set of instances inside it without allocating.
 int lbg_batch_new_capacity(const lbg_pp* pp, size_t max_cols, size_t max_instances, lbg_batch** out) {

@@ -41,6 +41,8 @@ struct lbg_pp {
   uint32_t* d_chat = nullptr;  // [cols][162]
   int16_t* d_fc = nullptr;     // [4][limbs][162]
   uint8_t* d_sw = nullptr;     // the switch prover's workspace (lbg_switch_prove), allocated on first use
+  uint8_t* d_wire = nullptr;   // lbg_row_evaluate_packed's bytes (grown on use)
+  size_t wire_cap = 0;
 };
 
 // Frees the switch prover's workspace of pp (switch.cu).
@@ -72,6 +74,8 @@ struct lbg_prover {
   lbg_challenge_d* d_ch = nullptr;
   uint32_t* d_chat = nullptr;
   int16_t* d_v = nullptr;     // [len_ring][648]
+  uint8_t* d_wire = nullptr;  // lbg_opening_pack_commitment's bytes (grown on use)
+  size_t wire_cap = 0;
   uint16_t* d_res = nullptr;  // [limbs][cols*648]
   std::mutex mu;
   std::vector<struct OpeningBufs*> spare;

@@ -9,9 +9,15 @@ switch at the request's point r (crates/pcs/examples/two_fields.rs:176-194: comm
 commitment absorbed, switch::prove of the trace's value at r, row evaluation at the switch's
 point, folding challenges, fold); its result carries the switch proof and the claim.
 
-Continuous batching: the server owns `slots` device arenas (lbg_batch, sized once; admission is by
-arena room, i.e. by the HBM each slot reserved). Whenever a slot is free it admits, in arrival
-order, every queued request that fits, lays them out in the arena and runs their rounds together:
+Continuous batching: the server owns `slots` device arenas (lbg_batch, sized once). Each slot's
+arena fits `hbm_fraction` of the device's free memory split over the slots (cudaMemGetInfo through
+lbg_device_memory, and lbg_batch_arena_bytes per arena); a given `capacity_columns` (the most
+columns one batch runs, a latency bound) caps it further. Admission is by arena room, i.e. by the
+HBM each slot reserved, and by size class: with `small_log_len` set, requests of at most
+2^small_log_len columns are small; slot 0 runs small requests only, the other slots run the large
+ones and take small ones when no large request waits, so a small request never queues behind a
+batch of large ones. Whenever a slot is free it admits, in arrival order within its class, every
+queued request that fits, lays them out in the arena and runs their rounds together:
 each device stage is one launch over all of them, and the transcripts (absorbs, evaluation point,
 challenge sampling) run on the device too (lbg_batch_round), so a batch is one pass on the
 slot's stream from witness generation to the folded witnesses. While one slot reads its results
@@ -56,24 +62,46 @@ class Request:
         return self.done - self.arrival
 
 
+def arena_columns(pp: PublicParameters, hbm_fraction: float, slots: int, max_requests: int,
+                  max_columns: int = 1 << 16) -> int:
+    """The columns each of `slots` arenas can hold in `hbm_fraction` of the device's free memory (a
+    power of two, at most max_columns): free bytes from lbg_device_memory, bytes per arena from
+    lbg_batch_arena_bytes."""
+    import ctypes
+
+    from ._native import check, lib
+
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    check(lib().lbg_device_memory(pp._h, ctypes.byref(free), ctypes.byref(total)))
+    budget = hbm_fraction * free.value / slots
+    cols = 1
+    while cols * 2 <= max_columns and lib().lbg_batch_arena_bytes(pp._h, cols * 2, max_requests) <= budget:
+        cols *= 2
+    return cols
+
+
 class Server:
-    def __init__(self, pp: PublicParameters, capacity_columns: int, max_requests: int = 256, slots: int = 2,
-                 host_threads: int = 16, domain: bytes = b"labinius/reference", keep_results: bool = True,
-                 transcript: str = "device"):
+    def __init__(self, pp: PublicParameters, capacity_columns: Optional[int] = None, max_requests: int = 256,
+                 slots: int = 2, host_threads: int = 16, domain: bytes = b"labinius/reference",
+                 keep_results: bool = True, transcript: str = "device", hbm_fraction: float = 0.5,
+                 small_log_len: Optional[int] = None):
         self.pp = pp
-        self.capacity = capacity_columns
+        self.memory_columns = arena_columns(pp, hbm_fraction, slots, max_requests)
+        self.capacity = self.memory_columns if capacity_columns is None else min(capacity_columns, self.memory_columns)
         self.max_requests = max_requests
         self.domain = domain
         self.keep_results = keep_results
         self.transcript = transcript
-        self.slots = [Batch(pp, capacity=(capacity_columns, max_requests)) for _ in range(slots)]
+        self.small_log_len = small_log_len if slots >= 2 else None
+        self.slots = [Batch(pp, capacity=(self.capacity, max_requests)) for _ in range(slots)]
         self.pool = concurrent.futures.ThreadPoolExecutor(host_threads)
-        self.queue = collections.deque()
+        self.small = collections.deque()  # every request when no size classes are set
+        self.large = collections.deque()
         self.cv = threading.Condition()
         self.stop = False
         self.t0 = time.perf_counter()
         self.batches = 0
-        self.workers = [threading.Thread(target=self._work, args=(b,), daemon=True) for b in self.slots]
+        self.workers = [threading.Thread(target=self._work, args=(b, i), daemon=True) for i, b in enumerate(self.slots)]
         for w in self.workers:
             w.start()
 
@@ -97,29 +125,39 @@ class Server:
         with self.cv:
             if not req.arrival:
                 req.arrival = self.clock()
-            self.queue.append(req)
-            self.cv.notify()
+            if self.small_log_len is None or req.column_log_len <= self.small_log_len:
+                self.small.append(req)
+            else:
+                self.large.append(req)
+            self.cv.notify_all()
         return req
 
-    def _admit(self) -> List[Request]:
+    def _queue_for(self, slot: int):
+        """The queue slot `slot` serves next: slot 0 the small requests only (with size classes),
+        the others the large ones first, then the small ones."""
+        if self.small_log_len is None or slot == 0:
+            return self.small
+        return self.large if self.large else self.small
+
+    def _admit(self, q) -> List[Request]:
         """Arrival order, as many as fit the arena (columns) and its request table."""
         taken, cols = [], 0
-        while self.queue and len(taken) < self.max_requests:
-            c = 1 << self.queue[0].column_log_len
+        while q and len(taken) < self.max_requests:
+            c = 1 << q[0].column_log_len
             if cols + c > self.capacity:
                 break
             cols += c
-            taken.append(self.queue.popleft())
+            taken.append(q.popleft())
         return taken
 
-    def _work(self, b: Batch):
+    def _work(self, b: Batch, slot: int):
         while True:
             with self.cv:
-                while not self.queue and not self.stop:
+                while not self._queue_for(slot) and not self.stop:
                     self.cv.wait()
-                if self.stop and not self.queue:
+                if self.stop and not self._queue_for(slot):
                     return
-                reqs = self._admit()
+                reqs = self._admit(self._queue_for(slot))
             if not reqs:
                 continue
             now = self.clock()

@@ -28,3 +28,29 @@ def encode_folded(prover) -> bytes:
     out = np.zeros(cap, np.uint8)
     n = lib().lbg_prover_encode_folded(prover._h, ptr(out), cap)
     return _result(n, out)
+
+
+def pack_commitment(opening) -> bytes:
+    """wire::pack_commitment (crates/pcs/src/wire/mod.rs:226-245) of the commitment an opening holds,
+    packed on the device where Prover::commit left it (the bit-dropped form is wire::pack_dropped)."""
+    n = int(lib().lbg_opening_pack_commitment(opening._h, None, 0))
+    if n < 0:
+        check(n)
+    out = np.zeros(max(n, 1), np.uint8)
+    return _result(lib().lbg_opening_pack_commitment(opening._h, ptr(out), n), out)
+
+
+def row_evaluate_packed(witness, point):
+    """Witness::row_evaluate and wire::pack_row_evaluation (crates/pcs/src/wire/mod.rs:435-459), both on
+    the device: (RowEvaluation, its bytes)."""
+    from .scheme import RowEvaluation
+
+    pp = witness.pp
+    p0 = np.ascontiguousarray(point.p0, dtype=np.uint64)
+    n = int(lib().lbg_row_evaluate_packed(pp._h, None, None, 0, None, None, 0))
+    if n < 0:
+        check(n)
+    u = np.zeros((pp.params.columns(), 3), np.uint64)
+    out = np.zeros(max(n, 1), np.uint8)
+    m = lib().lbg_row_evaluate_packed(pp._h, witness._h, ptr(p0), len(p0), ptr(u), ptr(out), n)
+    return RowEvaluation(u), _result(m, out)

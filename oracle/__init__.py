@@ -566,3 +566,72 @@ def wire_decode(data: bytes):
     st = lib().orc_wire_decode(_p(b), len(data), _p(v) if v.size else None, v.size, ctypes.byref(count))
     return st, v
 
+
+
+# ---------------------------------------------------------------------------------------------
+# wire: the bit-packed commitment and row evaluation (crates/pcs/src/wire/mod.rs)
+# ---------------------------------------------------------------------------------------------
+def residue_bits(q: int) -> int:
+    """crates/pcs/src/wire/mod.rs:77-79: bits of q - 1."""
+    return int(q - 1).bit_length()
+
+
+def pack_commitment(params: Params, C) -> bytes:
+    """wire::pack_commitment (crates/pcs/src/wire/mod.rs:226-245) of a Clear commitment matrix
+    C [columns][4][limbs][162]: element by element (column-major), limb by limb, slot by slot,
+    slot mod q in residue_bits(q) bits."""
+    C = np.asarray(C, dtype=np.int64).reshape(-1, params.limbs, N162)
+    # one row of bits per element: limb 0's 162 slots, then limb 1's, ...; each slot's residue in
+    # residue_bits(q) bits, least significant first (BitWriter::put, crates/pcs/src/wire/mod.rs:101-110)
+    cols = []
+    for k, q in enumerate(params.primes):
+        v = (C[:, k, :] % q).astype(np.uint64).reshape(len(C), N162, 1)
+        bits = residue_bits(q)
+        cols.append(((v >> np.arange(bits, dtype=np.uint64)) & np.uint64(1)).astype(np.uint8).reshape(len(C), -1))
+    stream = np.concatenate(cols, axis=1).reshape(-1)
+    return np.packbits(stream, bitorder="little").tobytes()
+
+
+def unpack_commitment(params: Params, data: bytes):
+    """wire::unpack_commitment (crates/pcs/src/wire/mod.rs:248-300), Clear: (status, C) with status
+    0 (ok) or 2 (malformed: wrong length or a value >= q)."""
+    bits = [residue_bits(q) for q in params.primes]
+    n = 4 * params.columns
+    if len(data) != (n * N162 * sum(bits) + 7) // 8:
+        return 2, None
+    stream = np.unpackbits(np.frombuffer(bytes(data), dtype=np.uint8), bitorder="little")
+    stream = stream[: n * N162 * sum(bits)].reshape(n, -1)
+    C = np.zeros((n, params.limbs, N162), np.int16)
+    off = 0
+    for k, (q, b) in enumerate(zip(params.primes, bits)):
+        blk = stream[:, off: off + N162 * b].reshape(n, N162, b).astype(np.uint64)
+        vals = (blk << np.arange(b, dtype=np.uint64)).sum(axis=2)
+        if (vals >= q).any():
+            return 2, None
+        half = (q - 1) // 2
+        C[:, k, :] = np.where(vals > half, vals.astype(np.int64) - q, vals.astype(np.int64))
+        off += N162 * b
+    return 0, C.reshape(params.columns, 4, params.limbs, N162)
+
+
+def pack_f162(u) -> bytes:
+    """wire::pack_f162 / pack_row_evaluation (crates/pcs/src/wire/mod.rs:435-453): 162 bits per
+    element (64 + 64 + 34), least significant first, back to back."""
+    u = np.ascontiguousarray(u, dtype=np.uint64).reshape(-1, 3)
+    parts = [((u[:, w:w + 1] >> np.arange(64 if w < 2 else 34, dtype=np.uint64)) & np.uint64(1)).astype(np.uint8)
+             for w in range(3)]
+    return np.packbits(np.concatenate(parts, axis=1).reshape(-1), bitorder="little").tobytes()
+
+
+def unpack_f162(data: bytes, count: int):
+    """wire::unpack_f162 (crates/pcs/src/wire/mod.rs:456-470): (status, u) with status 0 or 2 (the
+    length is not ceil(162 count / 8))."""
+    if len(data) != (count * 162 + 7) // 8:
+        return 2, None
+    stream = np.unpackbits(np.frombuffer(bytes(data), dtype=np.uint8), bitorder="little")[: count * 162]
+    b = stream.reshape(count, 162).astype(np.uint64)
+    u = np.zeros((count, 3), np.uint64)
+    u[:, 0] = (b[:, :64] << np.arange(64, dtype=np.uint64)).sum(axis=1, dtype=np.uint64)
+    u[:, 1] = (b[:, 64:128] << np.arange(64, dtype=np.uint64)).sum(axis=1, dtype=np.uint64)
+    u[:, 2] = (b[:, 128:] << np.arange(34, dtype=np.uint64)).sum(axis=1, dtype=np.uint64)
+    return 0, u

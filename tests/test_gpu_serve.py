@@ -45,14 +45,16 @@ def alone(oracle, row_log, primes, req, r_hi):
     return c.matrix, point, mle, row.values, ch.challenges, v.elements, proof, claim
 
 
-@pytest.mark.parametrize("transcript", ["device", "host"])
-def test_results_in_the_mix_equal_results_alone(oracle, transcript):
+@pytest.mark.parametrize("transcript,small", [("device", None), ("host", None), ("device", 2)],
+                         ids=["device", "host", "size-classes"])
+def test_results_in_the_mix_equal_results_alone(oracle, transcript, small):
     import labinius_b200 as L
     from labinius_b200.serve import Request, Server
 
     row_log, primes = 8, [3889, 9721]
     pp = L.PublicParameters.from_seed(product_params((row_log + 3, 3, primes, 0)), MATRIX_SEED)
-    srv = Server(pp, capacity_columns=48, max_requests=8, slots=2, host_threads=4, transcript=transcript)
+    srv = Server(pp, capacity_columns=48, max_requests=8, slots=2, host_threads=4, transcript=transcript,
+                 small_log_len=small)
     rng = np.random.default_rng(4)
     reqs = []
     for i in range(14):
@@ -81,3 +83,23 @@ def test_results_in_the_mix_equal_results_alone(oracle, transcript):
         assert np.array_equal(res.mle, mle) and np.array_equal(res.u, u)
         assert np.array_equal(res.challenges, ch)
         assert np.array_equal(res.v, v)
+
+
+def test_arenas_are_sized_from_free_device_memory():
+    """Without a capacity the arenas take hbm_fraction of the free device memory: the columns are
+    a power of two whose arena fits the share and whose double does not (or the cap)."""
+    import ctypes
+
+    import labinius_b200 as L
+    from labinius_b200._native import check, lib
+    from labinius_b200.serve import arena_columns
+
+    pp = L.PublicParameters.from_seed(product_params((11 + 3, 3, [3889, 9721], 0)), MATRIX_SEED)
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    check(lib().lbg_device_memory(pp._h, ctypes.byref(free), ctypes.byref(total)))
+    assert 0 < free.value <= total.value
+    cols = arena_columns(pp, 0.01, 2, 16)
+    share = 0.01 * free.value / 2
+    assert cols & (cols - 1) == 0
+    assert lib().lbg_batch_arena_bytes(pp._h, cols, 16) <= share or cols == 1
+    assert cols == 1 << 16 or lib().lbg_batch_arena_bytes(pp._h, 2 * cols, 16) > share

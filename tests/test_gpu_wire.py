@@ -74,3 +74,56 @@ def test_any_i16_and_every_tail_length_encode_as_the_oracle(oracle):
                 state = (state * 6364136223846793005 + 1442695040888963407) & M64
                 v[e, i] = sum((state >> (10 * k)) & 0x3F for k in range(6)) - 189
         same(oracle, v)
+
+
+# ---------------------------------------------------------------------------------------------
+# the bit-packed commitment and row evaluation, from device memory (crates/pcs/src/wire/mod.rs:
+# 226-245, 386-397, 435-459)
+# ---------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("shape", [(12, 3, [3889], 0), (12, 4, [3889, 2917, 4861], 0), (11, 2, [19441, 12637], 0),
+                                   (13, 5, [17497, 2917, 9721], 0), (12, 4, [3889, 2917, 4861], 9),
+                                   (11, 3, [2917], 8), (22, 9, [3889, 2917, 4861], 0)],
+                         ids=["1limb", "3limbs", "large", "mixed", "bd9", "bd-1limb", "suite-l"])
+def test_pack_commitment_from_the_device_equals_the_oracle(oracle, shape):
+    import labinius_b200 as L
+    from labinius_b200 import wire
+    from rounds import MATRIX_SEED, WITNESS_SEED, product_params
+
+    wl, cl, primes, dropped = shape
+    params = product_params(shape)
+    pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+    w = L.Witness.random(pp, WITNESS_SEED)
+    prover = L.Prover(pp)
+    c, op = prover.commit(w)
+    got = wire.pack_commitment(op)
+    P = oracle.Params(wl, cl, primes, dropped)
+    if dropped:
+        assert got == oracle.pack_dropped(P, c.top, c.digits)
+    else:
+        assert got == oracle.pack_commitment(P, c.matrix)
+        st, back = oracle.unpack_commitment(P, got)
+        assert st == 0 and np.array_equal(back, c.matrix)
+    prover.recycle(op)
+
+
+@pytest.mark.parametrize("shape", [(12, 3, [3889], 0), (13, 7, [9721], 0), (22, 9, [3889, 2917, 4861], 0)],
+                         ids=["8cols", "128cols", "suite-l"])
+def test_pack_row_evaluation_from_the_device_equals_the_oracle(oracle, shape):
+    import labinius_b200 as L
+    from labinius_b200 import EvaluationPoint, wire
+    from rounds import MATRIX_SEED, WITNESS_SEED, product_params
+
+    params = product_params(shape)
+    pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+    w = L.Witness.random(pp, WITNESS_SEED)
+    rng = np.random.default_rng(3)
+    p0 = rng.integers(0, 2 ** 63, (params.row_log_len(), 3), dtype=np.uint64)
+    p0[:, 2] &= np.uint64((1 << 34) - 1)
+    p1 = rng.integers(0, 2 ** 63, (params.column_log_len, 3), dtype=np.uint64)
+    p1[:, 2] &= np.uint64((1 << 34) - 1)
+    pt = EvaluationPoint(p0, p1)
+    row, got = wire.row_evaluate_packed(w, pt)
+    assert np.array_equal(row.values, w.row_evaluate(pt).values)
+    assert got == oracle.pack_f162(row.values)
+    st, back = oracle.unpack_f162(got, params.columns())
+    assert st == 0 and np.array_equal(back, row.values)

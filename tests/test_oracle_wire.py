@@ -114,3 +114,85 @@ def test_a_stream_short_or_long_by_one_word_on_any_lane_is_refused(oracle):
         data = round_trips(oracle, v)
         assert oracle.wire_decode(data[:-2])[0] != 0
         assert oracle.wire_decode(data + b"\x00\x00")[0] != 0
+
+
+# ---------------------------------------------------------------------------------------------
+# the bit-packed commitment and row evaluation (crates/pcs/src/wire/mod.rs:85-140, 226-300, 435-470)
+# ---------------------------------------------------------------------------------------------
+class _BitWriter:
+    """crates/pcs/src/wire/mod.rs:85-139, restated literally (accumulator, bit count, bytes)."""
+
+    def __init__(self):
+        self.bytes, self.acc, self.n = bytearray(), 0, 0
+
+    def put(self, value, bits):
+        self.acc |= (value & ((1 << bits) - 1)) << self.n
+        self.n += bits
+        while self.n >= 8:
+            self.bytes.append(self.acc & 0xFF)
+            self.acc >>= 8
+            self.n -= 8
+
+    def finish(self):
+        if self.n > 0:
+            self.bytes.append(self.acc & 0xFF)
+        return bytes(self.bytes)
+
+
+def _small_commitment(oracle, primes, cl=2, wl=10):
+    P = oracle.Params(wl, cl, primes, 0)
+    A = oracle.key_expand(P, oracle.key_seed(bytes([0x5A]) * 32))
+    w = oracle.witness_random(P.witness_len, bytes([0xC7]) * 32)
+    return P, oracle.commit(P, A, w), w
+
+
+@pytest.mark.parametrize("primes", [[3889], [3889, 2917, 4861], [19441, 2917], [12637, 9721, 17497]])
+def test_pack_commitment_is_the_reference_bit_writer(oracle, primes):
+    P, C, _ = _small_commitment(oracle, primes)
+    w = _BitWriter()
+    for elem in C.reshape(-1, P.limbs, 162):
+        for k, q in enumerate(primes):
+            for slot in elem[k]:
+                w.put(int(slot) % q, oracle.residue_bits(q))
+    want = w.finish()
+    got = oracle.pack_commitment(P, C)
+    assert got == want
+    # the size of crates/pcs/src/wire/mod.rs:381-384
+    assert len(got) == (4 * P.columns * 162 * sum(oracle.residue_bits(q) for q in primes) + 7) // 8
+    st, back = oracle.unpack_commitment(P, got)
+    assert st == 0 and np.array_equal(back, C)
+
+
+def test_unpack_commitment_refuses_what_the_reference_refuses(oracle):
+    P, C, _ = _small_commitment(oracle, [3889, 2917])
+    b = oracle.pack_commitment(P, C)
+    assert oracle.unpack_commitment(P, b[:-1])[0] == 2
+    assert oracle.unpack_commitment(P, b + b"\0")[0] == 2
+    # a residue equal to q is malformed (crates/pcs/src/wire/mod.rs:282-284): the first slot's 12 bits
+    bad = bytearray(b)
+    v = 3889
+    bad[0] = v & 0xFF
+    bad[1] = (bad[1] & 0xF0) | (v >> 8)
+    assert oracle.unpack_commitment(P, bytes(bad))[0] == 2
+
+
+def test_pack_f162_is_the_reference_bit_writer(oracle):
+    rng = np.random.default_rng(11)
+    for count in [1, 2, 3, 7, 8, 64, 129]:
+        u = rng.integers(0, 2 ** 63, (count, 3), dtype=np.uint64) * np.uint64(2) + rng.integers(0, 2, (count, 3),
+                                                                                              dtype=np.uint64)
+        u[:, 2] &= np.uint64((1 << 34) - 1)
+        w = _BitWriter()
+        for x in u:
+            w.put(int(x[0]) & 0xFFFFFFFF, 32)
+            w.put(int(x[0]) >> 32, 32)
+            w.put(int(x[1]) & 0xFFFFFFFF, 32)
+            w.put(int(x[1]) >> 32, 32)
+            w.put(int(x[2]) & 0xFFFFFFFF, 32)
+            w.put(int(x[2]) >> 32, 2)
+        got = oracle.pack_f162(u)
+        assert got == w.finish()
+        assert len(got) == (162 * count + 7) // 8
+        st, back = oracle.unpack_f162(got, count)
+        assert st == 0 and np.array_equal(back, u)
+        assert oracle.unpack_f162(got[:-1], count)[0] == 2
