@@ -313,7 +313,7 @@ constexpr int TCC_THREADS = TCC_CTHREADS + 32;         // and the producer warp
 constexpr int TCC_CT = 8;                              // columns per item
 constexpr int TCC_RT = 4;                              // ring elements per step
 constexpr int TCC_WROW = TCC_RT * 12 + 2;              // staged witness words per column (400 bytes)
-constexpr int TCC_A_BYTES = 16 * TC_GROUP_BYTES;       // 128 rows x 384 bytes
+constexpr int TCC_A_BYTES = 128 * TC_KBYTES;           // 128 rows x 384 bytes
 constexpr int TCC_WT_BYTES = TCC_RT * N162 * TCC_CT * 4 * 2;
 constexpr int TCC_AT_BYTES = TCC_RT * N162 * 32;       // a step's key tile
 constexpr int TCC_WTILE_BYTES = TCC_CT * TCC_WROW * 8;
@@ -322,12 +322,12 @@ constexpr int TCC_OFF_WT = TCC_OFF_A + TCC_A_BYTES;
 constexpr int TCC_OFF_AT = TCC_OFF_WT + TCC_WT_BYTES;          // two key tiles
 constexpr int TCC_OFF_WTILE = TCC_OFF_AT + 2 * TCC_AT_BYTES;   // two witness tiles
 constexpr int TCC_OFF_BAR = TCC_OFF_WTILE + 2 * TCC_WTILE_BYTES;
-constexpr int TCC_SMEM = TCC_OFF_BAR + 96 + 128;       // + barriers, tensor-memory slot, flag, alignment
+constexpr int TCC_SMEM = TCC_OFF_BAR + 96 + 1024;      // + barriers, tensor-memory slot, flag, alignment
 constexpr int TCC_VPT = 3;                             // leaves per thread in the module product
 constexpr uint32_t TCC_TMEM_COLS = 512;                // two accumulators at columns 0 and 256
 constexpr long long TC_WAIT_BUDGET = 2000000000ll;     // cycles (about a second) before a timeout
 
-static_assert(TCC_OFF_A % 128 == 0 && TCC_OFF_AT % 16 == 0 && TCC_OFF_WTILE % 16 == 0 && TCC_OFF_BAR % 8 == 0,
+static_assert(TCC_OFF_A % TC_ATOM == 0 && TCC_OFF_AT % 16 == 0 && TCC_OFF_WTILE % 16 == 0 && TCC_OFF_BAR % 8 == 0,
               "alignment");
 static_assert(TCC_SMEM <= 232448, "shared memory per CTA");
 
@@ -343,9 +343,8 @@ __device__ __forceinline__ void tc_expand_chunk(uint8_t* sA, int r, int c, uint3
   b.y = (((u >> 4) & 15u) * 0x00204081u) & 0x01010101u;
   b.z = (((u >> 8) & 15u) * 0x00204081u) & 0x01010101u;
   b.w = (((u >> 12) & 15u) * 0x00204081u) & 0x01010101u;
-  uint8_t* p = sA + (r >> 3) * TC_GROUP_BYTES + c * 128 + (r & 7) * 16;
-  *(uint4*)p = b;
-  *(uint4*)(p + 12 * 128) = make_uint4(b.x << 7, b.y << 7, b.z << 7, b.w << 7);
+  *(uint4*)(sA + tc_swizzled_offset(r, 16 * c, 128)) = b;
+  *(uint4*)(sA + tc_swizzled_offset(r, 16 * c + 192, 128)) = make_uint4(b.x << 7, b.y << 7, b.z << 7, b.w << 7);
 }
 
 // Row tid % 128 of the A operand from its F162's words (zero when !valid; at most 34 bits in the
@@ -363,9 +362,12 @@ __device__ __forceinline__ void tc_build_row(uint8_t* sA, int tid, int threads, 
 __device__ __forceinline__ void tc_transform_mma(uint32_t d_tmem, uint32_t sA_u, uint32_t sB_u, uint64_t* bar) {
   constexpr uint32_t IDESC = tc::idesc_u8(128, TC_LEAVES);
 #pragma unroll
-  for (int kk = 0; kk < TC_KBYTES / 32; kk++)
-    tc::mma_i8(d_tmem, tc::smem_desc(sA_u + kk * 256, 128, TC_GROUP_BYTES),
-               tc::smem_desc(sB_u + kk * 256, 128, TC_GROUP_BYTES), IDESC, kk > 0);
+  for (int kk = 0; kk < TC_KBYTES / 32; kk++) {
+    // K-step kk: atom kk / 4, 32-byte step kk % 4 inside it
+    const uint32_t a = sA_u + (kk >> 2) * (128 * 128) + (kk & 3) * 32;
+    const uint32_t b = sB_u + (kk >> 2) * (TC_LEAVES * 128) + (kk & 3) * 32;
+    tc::mma_i8(d_tmem, tc::smem_desc_sw128(a, TC_ATOM), tc::smem_desc_sw128(b, TC_ATOM), IDESC, kk > 0);
+  }
   tc::commit_to(bar);
 }
 
@@ -402,8 +404,8 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
     k_commit_tc(const uint64_t* __restrict__ W, size_t wdim, const int4* __restrict__ Ahat,
                 const uint8_t* __restrict__ tcb, int cols, int len_ring, int chunk, int nchunks,
                 int32_t* __restrict__ partial /* [nchunks][cols][162][4] */) {
-  extern __shared__ __align__(128) uint8_t smem_raw[];
-  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);  // swizzle atoms
   uint8_t* sB = smem;
   uint8_t* sA = smem + TCC_OFF_A;
   uint16_t* wt = (uint16_t*)(smem + TCC_OFF_WT);
@@ -847,9 +849,9 @@ constexpr int TCF_OFF_A = TC_B_BYTES;        // two A buffers
 constexpr int TCF_OFF_WTILE = TCF_OFF_A + 2 * TCC_A_BYTES;
 constexpr int TCF_OFF_CT = TCF_OFF_WTILE + 2 * TCF_WT_BYTES;
 constexpr int TCF_OFF_BAR = TCF_OFF_CT + 3 * 176 * 4;
-constexpr int TCF_SMEM = TCF_OFF_BAR + 64 + 128;
+constexpr int TCF_SMEM = TCF_OFF_BAR + 64 + 1024;
 constexpr uint32_t TCF_TMEM_COLS = 512;
-static_assert(TCF_OFF_WTILE % 16 == 0 && TCF_OFF_CT % 16 == 0 && TCF_OFF_BAR % 8 == 0, "alignment");
+static_assert(TCF_OFF_A % TC_ATOM == 0 && (TCF_OFF_A + TCC_A_BYTES) % TC_ATOM == 0 && TCF_OFF_WTILE % 16 == 0 && TCF_OFF_CT % 16 == 0 && TCF_OFF_BAR % 8 == 0, "alignment");
 static_assert(TCF_SMEM <= 232448, "shared memory per CTA");
 
 template <int PI>
@@ -857,8 +859,8 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
     k_fold_tc(const uint64_t* __restrict__ W, size_t wdim, int cols, int cols_per_split,
               const uint32_t* __restrict__ chat, const uint8_t* __restrict__ tcb, uint32_t* __restrict__ vhat_t,
               const int* __restrict__ split_inst) {
-  extern __shared__ __align__(128) uint8_t smem_raw[];
-  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);  // swizzle atoms
   uint8_t* sB = smem;
   uint8_t* sA = smem + TCF_OFF_A;
   uint64_t* wtile = (uint64_t*)(smem + TCF_OFF_WTILE);

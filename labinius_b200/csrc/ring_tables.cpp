@@ -305,8 +305,8 @@ void tc_transform_operand(const PrimeTables& T, uint8_t* out) {
     for (int m = 0; m < N162; m++) {
       const uint32_t t = (uint32_t)x;
       const int lo_kb = m, hi_kb = 192 + m;
-      out[(v / 8) * TC_GROUP_BYTES + (lo_kb / 16) * 128 + (v % 8) * 16 + lo_kb % 16] = (uint8_t)(t & 127u);
-      out[(v / 8) * TC_GROUP_BYTES + (hi_kb / 16) * 128 + (v % 8) * 16 + hi_kb % 16] = (uint8_t)(t >> 7);
+      out[tc_swizzled_offset(v, lo_kb, TC_LEAVES)] = (uint8_t)(t & 127u);
+      out[tc_swizzled_offset(v, hi_kb, TC_LEAVES)] = (uint8_t)(t >> 7);
       x = x * T.theta_leaf[v] % T.q;
     }
   }

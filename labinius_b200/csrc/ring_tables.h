@@ -82,13 +82,25 @@ const Ntt648Tables* ntt648_tables(uint32_t q);
 // (bit m of an F162 times the value of Y^m at leaf v), split into T = lo + 128 hi with lo < 128 and
 // hi < 256 and laid out as the B operand of a kind::i8 multiply (N = 176 leaf rows, the last 14
 // zero; K = 384 bytes: lo for m < 162 at K-byte m, hi at K-byte 192 + m, zeros elsewhere), K-major
-// without swizzle: byte (v, kb) at (v / 8) * 3072 + (kb / 16) * 128 + (v % 8) * 16 + kb % 16.
-// With the A operand of an F162 row holding bit m at K-byte m and 128 * bit m at K-byte 192 + m,
-// the s32 product is sum_m bit_m T[m][v] exactly (at most 162 (q - 1) < 2^22).
+// with the 128-byte swizzle: 8-row x 128-byte atoms of 1024 bytes, the 16-byte chunk c of a row
+// stored at chunk c ^ (row % 8) (tc_swizzled_offset). With the A operand of an F162 row holding
+// bit m at K-byte m and 128 * bit m at K-byte 192 + m, the s32 product is sum_m bit_m T[m][v]
+// exactly (at most 162 (q - 1) < 2^22).
 constexpr int TC_LEAVES = 176;          // N of the transform multiply
 constexpr int TC_KBYTES = 384;          // K of the transform multiply, in bytes
-constexpr int TC_GROUP_BYTES = 3072;    // one 8-row group: 24 core matrices of 128 bytes
-constexpr int TC_B_BYTES = (TC_LEAVES / 8) * TC_GROUP_BYTES;  // 67584
+constexpr int TC_ATOM = 1024;           // one swizzle atom: 8 rows x 128 bytes
+constexpr int TC_B_BYTES = TC_LEAVES * TC_KBYTES;  // 67584
+// Byte offset of (row, K-byte kb) in a K-major, 128-byte-swizzled operand of `rows` rows (a
+// multiple of 8): the K-atoms (128 bytes of K) one after another, each holding all row groups.
+#ifdef __CUDACC__
+#define LBG_HOST_DEVICE __host__ __device__
+#else
+#define LBG_HOST_DEVICE
+#endif
+LBG_HOST_DEVICE constexpr int tc_swizzled_offset(int row, int kb, int rows) {
+  return (kb >> 7) * (rows * 128) + (row >> 3) * TC_ATOM + (row & 7) * 128 + ((((kb >> 4) & 7) ^ (row & 7)) << 4) +
+         (kb & 15);
+}
 void tc_transform_operand(const PrimeTables& T, uint8_t* out /* TC_B_BYTES */);
 
 // xorshift64* state transition as GF(2) columns: jump[k][c] = T^(2^k) applied to e_c.

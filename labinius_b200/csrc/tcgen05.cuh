@@ -5,8 +5,8 @@
 //
 // Conventions used by the kernels here (one CTA, cta_group::1, M = 128):
 // * accumulator row r lives in tensor-memory lane r; warp w may read lanes 32 (w % 4) .. + 31;
-// * operands are K-major without swizzle: 8-row x 16-byte core matrices of 128 contiguous bytes,
-//   core matrices adjacent in K `lbo` bytes apart, adjacent 8-row groups `sbo` bytes apart;
+// * operands are K-major with the 128-byte swizzle: 8-row x 128-byte atoms (1024-byte aligned),
+//   the 16-byte chunk c of row r at chunk c ^ (r % 8); adjacent 8-row groups `sbo` bytes apart;
 // * every wait on an mbarrier is bounded by a cycle budget and reports a timeout instead of
 //   spinning for ever.
 #pragma once
@@ -83,10 +83,12 @@ __device__ __forceinline__ void named_sync(int id, int threads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
 
-// Shared-memory matrix descriptor: K-major, no swizzle (layout type 0), descriptor version 1.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+// Shared-memory matrix descriptor: K-major with the 128-byte swizzle (layout type 2), descriptor
+// version 1; the leading-byte offset is unused by this layout (16 bytes), `sbo` the stride between
+// 8-row groups. The start address may step through an atom's 128 bytes of K in 32-byte steps.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
+         (1ull << 46) | (2ull << 61);
 }
 
 // Instruction descriptor of kind::i8: unsigned 8-bit A and B, both K-major, s32 accumulator,
