@@ -106,7 +106,7 @@ def test_pack_commitment_from_the_device_equals_the_oracle(oracle, shape):
     prover.recycle(op)
 
 
-@pytest.mark.parametrize("shape", [(12, 3, [3889], 0), (13, 7, [9721], 0), (22, 9, [3889, 2917, 4861], 0)],
+@pytest.mark.parametrize("shape", [(12, 3, [3889], 0), (14, 7, [9721], 0), (22, 9, [3889, 2917, 4861], 0)],
                          ids=["8cols", "128cols", "suite-l"])
 def test_pack_row_evaluation_from_the_device_equals_the_oracle(oracle, shape):
     import labinius_b200 as L
