@@ -335,26 +335,61 @@ static_assert(TCC_SMEM <= 232448, "shared memory per CTA");
 // what it waits for takes microseconds). The host reads and clears it.
 __device__ int g_tc_timeout = 0;
 
-// Expand F162 bits 16c .. 16c + 15 of a row into the A operand: 16 bytes of bit values at K-chunk
-// c, and the same times 128 at K-chunk c + 12.
-__device__ __forceinline__ void tc_expand_chunk(uint8_t* sA, int r, int c, uint32_t u) {
-  uint4 b;
-  b.x = ((u & 15u) * 0x00204081u) & 0x01010101u;
-  b.y = (((u >> 4) & 15u) * 0x00204081u) & 0x01010101u;
-  b.z = (((u >> 8) & 15u) * 0x00204081u) & 0x01010101u;
-  b.w = (((u >> 12) & 15u) * 0x00204081u) & 0x01010101u;
-  *(uint4*)(sA + tc_swizzled_offset(r, 16 * c, 128)) = b;
-  *(uint4*)(sA + tc_swizzled_offset(r, 16 * c + 192, 128)) = make_uint4(b.x << 7, b.y << 7, b.z << 7, b.w << 7);
+// The same without a plan kept in registers: offsets computed at each call (NC chunks per thread).
+template <int NC>
+__device__ __forceinline__ void tc_build_row_inline(uint8_t* sA, int tid, int threads, const uint64_t* e) {
+  const int r = tid & 127, step = threads >> 7;
+  const uint64_t w0 = e[0], w1 = e[1], w2 = e[2] & ((1ull << 34) - 1);
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    const int c = (tid >> 7) + step * k;
+    const uint64_t word = (c >> 2) == 0 ? w0 : (c >> 2) == 1 ? w1 : w2;
+    const uint32_t u = (uint32_t)(word >> (16 * (c & 3))) & 0xFFFFu;
+    uint4 b;
+    b.x = ((u & 15u) * 0x00204081u) & 0x01010101u;
+    b.y = (((u >> 4) & 15u) * 0x00204081u) & 0x01010101u;
+    b.z = (((u >> 8) & 15u) * 0x00204081u) & 0x01010101u;
+    b.w = (((u >> 12) & 15u) * 0x00204081u) & 0x01010101u;
+    *(uint4*)(sA + tc_swizzled_offset(r, 16 * c, 128)) = b;
+    *(uint4*)(sA + tc_swizzled_offset(r, 16 * c + 192, 128)) = make_uint4(b.x << 7, b.y << 7, b.z << 7, b.w << 7);
+  }
 }
 
-// Row tid % 128 of the A operand from its F162's words (zero when !valid; at most 34 bits in the
-// third word), by `threads` threads (a multiple of 128).
-__device__ __forceinline__ void tc_build_row(uint8_t* sA, int tid, int threads, const uint64_t* e, bool valid) {
-  const int r = tid & 127;
+// What one thread writes of the A operand, planned once: row tid % 128, its NC chunks
+// c_k = tid / 128 + (threads / 128) k of 16 bits (bits 16 c_k ..) with their swizzled offsets in
+// the bit plane and in the times-128 plane.
+template <int NC>
+struct TcRowPlan {
+  int off_lo[NC], off_hi[NC], word[NC], shift[NC];
+  __device__ TcRowPlan(int tid, int threads) {
+    const int r = tid & 127, step = threads >> 7;
+#pragma unroll
+    for (int k = 0; k < NC; k++) {
+      const int c = (tid >> 7) + step * k;
+      off_lo[k] = tc_swizzled_offset(r, 16 * c, 128);
+      off_hi[k] = tc_swizzled_offset(r, 16 * c + 192, 128);
+      word[k] = c >> 2;
+      shift[k] = 16 * (c & 3);
+    }
+  }
+};
+
+// The thread's part of its row of the A operand from the row's F162 words (zero when !valid; at
+// most 34 bits in the third word).
+template <int NC>
+__device__ __forceinline__ void tc_build_row(uint8_t* sA, const TcRowPlan<NC>& pl, const uint64_t* e, bool valid) {
   const uint64_t w0 = valid ? e[0] : 0, w1 = valid ? e[1] : 0, w2 = valid ? e[2] & ((1ull << 34) - 1) : 0;
-  for (int c = tid >> 7; c < 12; c += threads >> 7) {
-    const uint64_t word = c < 4 ? w0 : c < 8 ? w1 : w2;
-    tc_expand_chunk(sA, r, c, (uint32_t)(word >> (16 * (c & 3))) & 0xFFFFu);
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    const uint64_t word = pl.word[k] == 0 ? w0 : pl.word[k] == 1 ? w1 : w2;
+    const uint32_t u = (uint32_t)(word >> pl.shift[k]) & 0xFFFFu;
+    uint4 b;
+    b.x = ((u & 15u) * 0x00204081u) & 0x01010101u;
+    b.y = (((u >> 4) & 15u) * 0x00204081u) & 0x01010101u;
+    b.z = (((u >> 8) & 15u) * 0x00204081u) & 0x01010101u;
+    b.w = (((u >> 12) & 15u) * 0x00204081u) & 0x01010101u;
+    *(uint4*)(sA + pl.off_lo[k]) = b;
+    *(uint4*)(sA + pl.off_hi[k]) = make_uint4(b.x << 7, b.y << 7, b.z << 7, b.w << 7);
   }
 }
 
@@ -498,14 +533,14 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
     int since = 0;
     int it = first, st = 0, p_it = -1, p_st = 0;
     const int r = tid & 127;
+    const TcRowPlan<12 * 128 / TCC_CTHREADS> plan(tid, TCC_CTHREADS);
     for (int g = 0; g <= S; g++) {
       tc_wait(&full[g & 1], (g >> 1) & 1, abort);                          // step g's words, step g - 1's key tile
       if (g >= 1) tc_wait(&mma[(g - 1) & 1], ((g - 1) >> 1) & 1, abort);  // A free, accumulator g - 1 ready
       if (g < S) {
         const int jj = (r >> 2) & 7, ii = r >> 5;
         const bool valid = (it % col_tiles) * TCC_CT + jj < cols && ii < items.n(it, st);
-        tc_build_row(sA, tid, TCC_CTHREADS, wtile + ((g & 1) * TCC_CT + jj) * TCC_WROW + (ii * 4 + (r & 3)) * 3,
-                     valid);
+        tc_build_row(sA, plan, wtile + ((g & 1) * TCC_CT + jj) * TCC_WROW + (ii * 4 + (r & 3)) * 3, valid);
         tc::fence_async_shared();
         tc::fence_before_sync();
         tc::named_sync(1, TCC_THREADS);  // meets the producer: lockstep, even when a wait timed out
@@ -517,13 +552,12 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
           const int quad = warp & 3, part = warp >> 2;
           const uint32_t taddr = tmem + (uint32_t)((g - 1) & 1) * 256u + ((uint32_t)(32 * quad) << 16);
           uint16_t* dst = wt + quad * N162 * 32 + lane;
+          uint32_t x[40];  // five loads, one wait
 #pragma unroll
-          for (int c = 0; c < 5; c++) {
-            uint32_t x[8];
-            tc::tmem_ld8(taddr + 40 * part + 8 * c, x);
+          for (int c = 0; c < 5; c++) tc::tmem_ld8_nowait(taddr + 40 * part + 8 * c, x + 8 * c);
+          tc::tmem_wait_ld(x);
 #pragma unroll
-            for (int i = 0; i < 8; i++) dst[(40 * part + 8 * c + i) * 32] = (uint16_t)red_half<PI>(x[i]);
-          }
+          for (int i = 0; i < 40; i++) dst[(40 * part + i) * 32] = (uint16_t)red_half<PI>(x[i]);
           if (part == 0) {
             uint32_t y[2];
             tc::tmem_ld2(taddr + 160, y);
@@ -960,8 +994,8 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
       if (g < S) {
         tc_wait(&full[g & 1], (g >> 1) & 1, abort);                   // step g's words
         if (g >= 2) tc_wait(&mma[g & 1], ((g - 2) >> 1) & 1, abort);  // A buffer g % 2 free
-        tc_build_row(sA + (g & 1) * TCC_A_BYTES, tid, TCF_CTHREADS, wtile + (g & 1) * (TCF_ROWS * 3) + (tid & 127) * 3,
-                     true);
+        tc_build_row_inline<12 * 128 / TCF_CTHREADS>(sA + (g & 1) * TCC_A_BYTES, tid, TCF_CTHREADS,
+                                                   wtile + (g & 1) * (TCF_ROWS * 3) + (tid & 127) * 3);
         tc::fence_async_shared();
         tc::fence_before_sync();
         tc::named_sync(1, TCF_THREADS);  // meets the producer: lockstep, even when a wait timed out
@@ -971,25 +1005,40 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
         tc::fence_after_sync();
         const uint32_t taddr = tmem + (uint32_t)((g - 1) & 1) * 256u + ((uint32_t)(32 * quad) << 16);
         const uint32_t* ch = ctile + ((g - 1) % 3) * 176;
+        // leaves v0 .. v0 + 47 in three batches of 16 (two loads, one wait), then v0 + 48 .. v0 + 55
+        // (the last part: its leaves 160-161)
 #pragma unroll
-        for (int c = 0; c < 7; c++) {
-          if (part < 2 || c < 6) {
-            uint32_t x[8];
-            tc::tmem_ld8(taddr + v0 + 8 * c, x);
+        for (int bt = 0; bt < 3; bt++) {
+          uint32_t x[16];
+          tc::tmem_ld8_nowait(taddr + v0 + 16 * bt, x);
+          tc::tmem_ld8_nowait(taddr + v0 + 16 * bt + 8, x + 8);
+          tc::tmem_wait_ld(x);
 #pragma unroll
-            for (int i = 0; i < 8; i += 4) {
-              const uint4 c4 = *(const uint4*)(ch + v0 + 8 * c + i);
-              acc[8 * c + i] += c4.x * red_half<PI>(x[i]);
-              acc[8 * c + i + 1] += c4.y * red_half<PI>(x[i + 1]);
-              acc[8 * c + i + 2] += c4.z * red_half<PI>(x[i + 2]);
-              acc[8 * c + i + 3] += c4.w * red_half<PI>(x[i + 3]);
-            }
-          } else {
-            uint32_t y[2];
-            tc::tmem_ld2(taddr + 160, y);  // the last part's leaves 160 and 161
-            acc[48] += ch[160] * red_half<PI>(y[0]);
-            acc[49] += ch[161] * red_half<PI>(y[1]);
+          for (int i = 0; i < 16; i += 4) {
+            const uint4 c4 = *(const uint4*)(ch + v0 + 16 * bt + i);
+            acc[16 * bt + i] += c4.x * red_half<PI>(x[i]);
+            acc[16 * bt + i + 1] += c4.y * red_half<PI>(x[i + 1]);
+            acc[16 * bt + i + 2] += c4.z * red_half<PI>(x[i + 2]);
+            acc[16 * bt + i + 3] += c4.w * red_half<PI>(x[i + 3]);
           }
+        }
+        if (part < 2) {
+          uint32_t x[8];
+          tc::tmem_ld8_nowait(taddr + v0 + 48, x);
+          tc::tmem_wait_ld(x);
+#pragma unroll
+          for (int i = 0; i < 8; i += 4) {
+            const uint4 c4 = *(const uint4*)(ch + v0 + 48 + i);
+            acc[48 + i] += c4.x * red_half<PI>(x[i]);
+            acc[49 + i] += c4.y * red_half<PI>(x[i + 1]);
+            acc[50 + i] += c4.z * red_half<PI>(x[i + 2]);
+            acc[51 + i] += c4.w * red_half<PI>(x[i + 3]);
+          }
+        } else {
+          uint32_t y[2];
+          tc::tmem_ld2(taddr + 160, y);  // the last part's leaves 160 and 161
+          acc[48] += ch[160] * red_half<PI>(y[0]);
+          acc[49] += ch[161] * red_half<PI>(y[1]);
         }
         tc::fence_before_sync();
         if (++since >= RED) {
