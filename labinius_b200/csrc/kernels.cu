@@ -2224,13 +2224,13 @@ int fold_blocks_per_sm(int pi) {
   return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
-// The fold's transforms run on the tensor cores (k_fold_tc) when LBG_FOLD_KERNEL=tc, else on the
-// CUDA cores (k_fold) (both exact). The one-pass mode without scratch (vhat null) and the fold
+// The fold's transforms run on the tensor cores (k_fold_tc) unless LBG_FOLD_KERNEL=scalar selects
+// the CUDA-core kernel (k_fold) (both exact). The one-pass mode without scratch (vhat null) and the fold
 // from the kept transform always run on the CUDA cores.
 bool fold_tc_enabled() {
   static const bool on = [] {
     const char* e = getenv("LBG_FOLD_KERNEL");
-    return e && std::string(e) == "tc";
+    return !(e && std::string(e) == "scalar");
   }();
   return on;
 }
