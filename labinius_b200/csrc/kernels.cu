@@ -322,7 +322,8 @@ constexpr int TCC_OFF_WT = TCC_OFF_A + TCC_A_BYTES;
 constexpr int TCC_OFF_AT = TCC_OFF_WT + TCC_WT_BYTES;          // two key tiles
 constexpr int TCC_OFF_WTILE = TCC_OFF_AT + 2 * TCC_AT_BYTES;   // two witness tiles
 constexpr int TCC_OFF_BAR = TCC_OFF_WTILE + 2 * TCC_WTILE_BYTES;
-constexpr int TCC_SMEM = TCC_OFF_BAR + 96 + 1024;      // + barriers, tensor-memory slot, flag, alignment
+constexpr int TCC_OFF_CUR = TCC_OFF_BAR + 96;          // four step cursors
+constexpr int TCC_SMEM = TCC_OFF_CUR + 4 * 32 + 1024;  // + barriers, tensor-memory slot, flag, cursors, alignment
 constexpr int TCC_VPT = 3;                             // leaves per thread in the module product
 constexpr uint32_t TCC_TMEM_COLS = 512;                // two accumulators at columns 0 and 256
 constexpr long long TC_WAIT_BUDGET = 2000000000ll;     // cycles (about a second) before a timeout
@@ -412,7 +413,8 @@ __device__ __forceinline__ void tc_wait(uint64_t* bar, uint32_t parity, volatile
   if (!tc::mbar_wait(bar, parity, TC_WAIT_BUDGET)) *abort = 1;
 }
 
-// The CTA's work items in order, each a run of steps.
+// The CTA's work items in order, each a run of steps: item `it` is column tile it % col_tiles
+// and ring-element chunk it / col_tiles.
 struct TcItems {
   int first, stride, total, col_tiles, chunk, len_ring;
   __device__ int steps(int it) const {
@@ -420,18 +422,40 @@ struct TcItems {
     const int i1 = min(len_ring, i0 + chunk);
     return i1 > i0 ? (i1 - i0 + TCC_RT - 1) / TCC_RT : 0;
   }
-  __device__ int i0(int it, int st) const { return (it / col_tiles) * chunk + st * TCC_RT; }
-  // ring elements present in step st of item it
-  __device__ int n(int it, int st) const {
-    return min(TCC_RT, min(len_ring, (it / col_tiles) * chunk + chunk) - i0(it, st));
-  }
-  // the step after (it, st); it >= total when there is none
-  __device__ void next(int& it, int& st) const {
-    if (++st < steps(it)) return;
+};
+
+// A position in that sequence, with the item's bounds computed once when the item starts (one
+// division per item rather than several per step): step st of item it covers ring elements
+// [i, min(i + TCC_RT, iend)) of columns [j0, j0 + TCC_CT).
+struct TcCursor {
+  int it, st, steps, j0, i, iend, ci;
+  __device__ void load(const TcItems& I, int item) {
+    it = item;
     st = 0;
-    do it += stride;
-    while (it < total && steps(it) == 0);
+    steps = 0;
+    while (it < I.total) {
+      ci = it / I.col_tiles;
+      const int i0 = ci * I.chunk, i1 = min(I.len_ring, i0 + I.chunk);
+      if (i1 > i0) {
+        j0 = (it - ci * I.col_tiles) * TCC_CT;
+        i = i0;
+        iend = i1;
+        steps = (i1 - i0 + TCC_RT - 1) / TCC_RT;
+        return;
+      }
+      it += I.stride;
+    }
   }
+  __device__ void advance(const TcItems& I) {
+    if (++st < steps) {
+      i += TCC_RT;
+      return;
+    }
+    load(I, it + I.stride);
+  }
+  __device__ int n() const { return min(TCC_RT, iend - i); }  // ring elements in this step
+  __device__ bool last() const { return st + 1 == steps; }
+  __device__ bool valid(const TcItems& I) const { return it < I.total; }
 };
 
 template <int PI>
@@ -452,17 +476,19 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
   uint64_t* bfull = full + 6;                           // the transform operand loaded
   uint32_t* tslot = (uint32_t*)(full + 7);
   volatile int* abort = (volatile int*)(full + 8);
+  // step g's cursor in slot g % 4: the producer writes step g + 1's before named barrier 1 of step
+  // g; the compute warps read step g's (build) and step g - 1's (module product) after it
+  TcCursor* curs = (TcCursor*)(smem + TCC_OFF_CUR);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int col_tiles = (cols + TCC_CT - 1) / TCC_CT;
   const TcItems items{(int)blockIdx.x, (int)gridDim.x, col_tiles * nchunks, col_tiles, chunk, len_ring};
-  int first = items.first;
-  while (first < items.total && items.steps(first) == 0) first += items.stride;
   int S = 0;  // the CTA's steps
-  for (int it = first; it < items.total; it += items.stride) S += items.steps(it);
+  for (int it = items.first; it < items.total; it += items.stride) S += items.steps(it);
 
   if (tid == 0) {
     for (int b = 0; b < 7; b++) tc::mbar_init(&full[b], 1);
     *abort = 0;
+    curs[0].load(items, items.first);
     tc::mbar_init_fence();
   }
   if (warp == 0) {
@@ -476,38 +502,37 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
 
   if (warp == TCC_CTHREADS / 32) {
     // ---------------- producer ----------------
-    // the witness rows of step (it, st) into tile buffer b, bytes counted on full[b]
-    auto load_words = [&](int it, int st, int b) {
-      const int j0 = (it % col_tiles) * TCC_CT, i0 = items.i0(it, st), n = items.n(it, st);
-      for (int jj = 0; jj < TCC_CT && j0 + jj < cols; jj++)
-        tc::bulk_g2s(wtile + (b * TCC_CT + jj) * TCC_WROW, W + ((size_t)(j0 + jj) * wdim + (size_t)4 * i0) * 3,
+    // the witness rows of step c into tile buffer b, bytes counted on full[b]
+    auto load_words = [&](const TcCursor& c, int b) {
+      const int n = c.n();
+      for (int jj = 0; jj < TCC_CT && c.j0 + jj < cols; jj++)
+        tc::bulk_g2s(wtile + (b * TCC_CT + jj) * TCC_WROW, W + ((size_t)(c.j0 + jj) * wdim + (size_t)4 * c.i) * 3,
                      96u * n, &full[b]);
     };
-    auto word_bytes = [&](int it, int st) {
-      return 96u * items.n(it, st) * min(TCC_CT, cols - (it % col_tiles) * TCC_CT);
-    };
+    auto word_bytes = [&](const TcCursor& c) { return 96u * c.n() * min(TCC_CT, cols - c.j0); };
     const uint32_t sA_u = tc::smem_u32(sA), sB_u = tc::smem_u32(sB);
+    TcCursor cur = curs[0];
     if (lane == 0 && S > 0) {
       tc::mbar_arrive_expect_tx(bfull, TC_B_BYTES);
       for (int x = 0; x < 4; x++)
         tc::bulk_g2s(sB + x * (TC_B_BYTES / 4), tcb + x * (TC_B_BYTES / 4), TC_B_BYTES / 4, bfull);
-      tc::mbar_arrive_expect_tx(&full[0], word_bytes(first, 0));
-      load_words(first, 0, 0);
+      tc::mbar_arrive_expect_tx(&full[0], word_bytes(cur));
+      load_words(cur, 0);
     }
-    int it = first, st = 0;
     for (int g = 0; g < S; g++) {
-      int nit = it, nst = st;
-      items.next(nit, nst);
+      TcCursor nxt = cur;
+      nxt.advance(items);
       if (lane == 0) {
         // compute iteration g + 1 reads step g + 1's words and step g's key tile (buffer g % 2,
         // whose previous tile, step g - 2's, the compute warps have released)
         if (g >= 2) tc_wait(&kempty[g & 1], ((g - 2) >> 1) & 1, abort);
-        const uint32_t kb = (uint32_t)items.n(it, st) * N162 * 32;
-        const uint32_t wb = nit < items.total ? word_bytes(nit, nst) : 0u;
+        const uint32_t kb = (uint32_t)cur.n() * N162 * 32;
+        const bool more = nxt.valid(items);
+        const uint32_t wb = more ? word_bytes(nxt) : 0u;
         tc::mbar_arrive_expect_tx(&full[(g + 1) & 1], kb + wb);
-        tc::bulk_g2s(atile + (g & 1) * (TCC_RT * N162 * 2), Ahat + (size_t)items.i0(it, st) * N162 * 2, kb,
-                     &full[(g + 1) & 1]);
-        if (nit < items.total) load_words(nit, nst, (g + 1) & 1);
+        tc::bulk_g2s(atile + (g & 1) * (TCC_RT * N162 * 2), Ahat + (size_t)cur.i * N162 * 2, kb, &full[(g + 1) & 1]);
+        if (more) load_words(nxt, (g + 1) & 1);
+        curs[(g + 1) & 3] = nxt;
       }
       __syncwarp();
       tc::named_sync(1, TCC_THREADS);  // step g's A operand is built
@@ -520,8 +545,7 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
           tc::mbar_arrive(&mma[g & 1]);
       }
       __syncwarp();
-      it = nit;
-      st = nst;
+      cur = nxt;
     }
   } else if (S > 0) {
     // ---------------- compute ----------------
@@ -531,22 +555,23 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
     for (int u = 0; u < TCC_VPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
     constexpr int RED = CommitRed<PI>::value;
     int since = 0;
-    int it = first, st = 0, p_it = -1, p_st = 0;
     const int r = tid & 127;
     const TcRowPlan<12 * 128 / TCC_CTHREADS> plan(tid, TCC_CTHREADS);
     for (int g = 0; g <= S; g++) {
       tc_wait(&full[g & 1], (g >> 1) & 1, abort);                          // step g's words, step g - 1's key tile
       if (g >= 1) tc_wait(&mma[(g - 1) & 1], ((g - 1) >> 1) & 1, abort);  // A free, accumulator g - 1 ready
       if (g < S) {
+        const TcCursor& cur = curs[g & 3];
         const int jj = (r >> 2) & 7, ii = r >> 5;
-        const bool valid = (it % col_tiles) * TCC_CT + jj < cols && ii < items.n(it, st);
+        const bool valid = cur.j0 + jj < cols && ii < cur.n();
         tc_build_row(sA, plan, wtile + ((g & 1) * TCC_CT + jj) * TCC_WROW + (ii * 4 + (r & 3)) * 3, valid);
         tc::fence_async_shared();
         tc::fence_before_sync();
         tc::named_sync(1, TCC_THREADS);  // meets the producer: lockstep, even when a wait timed out
       }
       if (g >= 1) {
-        const int nst = items.n(p_it, p_st);
+        const TcCursor& prev = curs[(g - 1) & 3];
+        const int nst = prev.n();
         tc::fence_after_sync();
         {
           const int quad = warp & 3, part = warp >> 2;
@@ -591,9 +616,9 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
               for (int c = 0; c < 4; c++) acc[u][c] = red_signed<PI>(acc[u][c]);
           }
         }
-        if (p_st + 1 == items.steps(p_it)) {
+        if (prev.last()) {
           // the item's last step: its sums out, the registers cleared
-          const int j = (p_it % col_tiles) * TCC_CT + jj_b;
+          const int j = prev.j0 + jj_b;
           if (j < cols) {
 #pragma unroll
             for (int u = 0; u < TCC_VPT; u++) {
@@ -604,7 +629,7 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
                 o.y = (int)red_signed_full<PI>(acc[u][1]);
                 o.z = (int)red_signed_full<PI>(acc[u][2]);
                 o.w = (int)red_signed_full<PI>(acc[u][3]);
-                ((int4*)partial)[((size_t)(p_it / col_tiles) * cols + j) * N162 + v] = o;
+                ((int4*)partial)[((size_t)prev.ci * cols + j) * N162 + v] = o;
               }
             }
           }
@@ -616,9 +641,6 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
         tc::named_sync(2, TCC_CTHREADS);  // the transform tile and the key tile are free
         if (tid == 0) tc::mbar_arrive(&kempty[(g - 1) & 1]);
       }
-      p_it = g < S ? it : -1;
-      p_st = st;
-      if (g < S) items.next(it, st);
     }
   }
   tc::fence_before_sync();
@@ -883,10 +905,33 @@ constexpr int TCF_OFF_A = TC_B_BYTES;        // two A buffers
 constexpr int TCF_OFF_WTILE = TCF_OFF_A + 2 * TCC_A_BYTES;
 constexpr int TCF_OFF_CT = TCF_OFF_WTILE + 2 * TCF_WT_BYTES;
 constexpr int TCF_OFF_BAR = TCF_OFF_CT + 3 * 176 * 4;
-constexpr int TCF_SMEM = TCF_OFF_BAR + 64 + 1024;
+constexpr int TCF_OFF_CUR = TCF_OFF_BAR + 64;  // four step cursors
+constexpr int TCF_SMEM = TCF_OFF_CUR + 4 * 32 + 1024;
 constexpr uint32_t TCF_TMEM_COLS = 512;
 static_assert(TCF_OFF_A % TC_ATOM == 0 && (TCF_OFF_A + TCC_A_BYTES) % TC_ATOM == 0 && TCF_OFF_WTILE % 16 == 0 && TCF_OFF_CT % 16 == 0 && TCF_OFF_BAR % 8 == 0, "alignment");
 static_assert(TCF_SMEM <= 232448, "shared memory per CTA");
+
+// A position in a CTA's fold items (item it: position tile it % tiles, column split it / tiles;
+// step st is column c0 + st), the item's bounds computed once when it starts.
+struct TcfCursor {
+  int it, st, n, c0, tile, split;
+  __device__ void load(int item, int stride, int total, int tiles, int cols, int cols_per_split) {
+    it = item;
+    st = 0;
+    n = 0;
+    while (it < total) {
+      split = it / tiles;
+      c0 = split * cols_per_split;
+      n = min(cols, c0 + cols_per_split) - c0;
+      if (n > 0) {
+        tile = it - split * tiles;
+        return;
+      }
+      n = 0;
+      it += stride;
+    }
+  }
+};
 
 template <int PI>
 __global__ void __launch_bounds__(TCF_THREADS, 1)
@@ -908,23 +953,23 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
   const int tiles = (int)((wdim + TCF_ROWS - 1) / TCF_ROWS);
   const int splits = (cols + cols_per_split - 1) / cols_per_split;
   const int total = tiles * splits;
-  // item it: position tile it % tiles, split it / tiles; step st is its column col0 + st
-  auto col0 = [&](int it) { return (it / tiles) * cols_per_split; };
-  auto ncol = [&](int it) { return max(0, min(cols, col0(it) + cols_per_split) - col0(it)); };
-  auto next = [&](int& it, int& st) {
-    if (++st < ncol(it)) return;
-    st = 0;
-    do it += gridDim.x;
-    while (it < total && ncol(it) == 0);
+  auto advance = [&](TcfCursor& c) {
+    if (++c.st < c.n) return;
+    c.load(c.it + (int)gridDim.x, (int)gridDim.x, total, tiles, cols, cols_per_split);
   };
-  int first = blockIdx.x;
-  while (first < total && ncol(first) == 0) first += gridDim.x;
+  // step g's cursor in slot g % 4: the producer writes step g + 1's before named barrier 1 of step
+  // g; the compute warps read step g + 1's (chat row) and step g - 1's (item end) after it
+  TcfCursor* curs = (TcfCursor*)(smem + TCF_OFF_CUR);
   int S = 0;
-  for (int it = first; it < total; it += gridDim.x) S += ncol(it);
+  for (int it = blockIdx.x; it < total; it += gridDim.x) {
+    const int c0 = (it / tiles) * cols_per_split;
+    S += max(0, min(cols, c0 + cols_per_split) - c0);
+  }
 
   if (tid == 0) {
     for (int b = 0; b < 5; b++) tc::mbar_init(&full[b], 1);
     *abort = 0;
+    curs[0].load(blockIdx.x, (int)gridDim.x, total, tiles, cols, cols_per_split);
     tc::mbar_init_fence();
   }
   if (warp == 0) {
@@ -938,24 +983,27 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
 
   if (warp == TCF_CTHREADS / 32) {
     // ---------------- producer ----------------
-    auto load_words = [&](int it, int st, int b) {
-      const size_t p0 = (size_t)(it % tiles) * TCF_ROWS;
+    auto load_words = [&](const TcfCursor& c, int b) {
+      const size_t p0 = (size_t)c.tile * TCF_ROWS;
       tc::mbar_arrive_expect_tx(&full[b], TCF_WT_BYTES);
-      tc::bulk_g2s(wtile + b * (TCF_ROWS * 3), W + ((size_t)(col0(it) + st) * wdim + p0) * 3, TCF_WT_BYTES, &full[b]);
+      tc::bulk_g2s(wtile + b * (TCF_ROWS * 3), W + ((size_t)(c.c0 + c.st) * wdim + p0) * 3, TCF_WT_BYTES, &full[b]);
     };
     const uint32_t sA_u = tc::smem_u32(sA), sB_u = tc::smem_u32(sB);
+    TcfCursor cur = curs[0];
     if (lane == 0 && S > 0) {
       tc::mbar_arrive_expect_tx(bfull, TC_B_BYTES);
       for (int x = 0; x < 4; x++)
         tc::bulk_g2s(sB + x * (TC_B_BYTES / 4), tcb + x * (TC_B_BYTES / 4), TC_B_BYTES / 4, bfull);
-      load_words(first, 0, 0);
+      load_words(cur, 0);
     }
-    int it = first, st = 0;
     for (int g = 0; g < S; g++) {
-      int nit = it, nst = st;
-      next(nit, nst);
+      TcfCursor nxt = cur;
+      advance(nxt);
       // step g + 1's words into buffer (g + 1) % 2, whose step g - 1 the compute warps have expanded
-      if (lane == 0 && nit < total) load_words(nit, nst, (g + 1) & 1);
+      if (lane == 0) {
+        if (nxt.it < total) load_words(nxt, (g + 1) & 1);
+        curs[(g + 1) & 3] = nxt;
+      }
       __syncwarp();
       tc::named_sync(1, TCF_THREADS);  // step g's A operand is built
       if (lane == 0) {
@@ -967,8 +1015,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
           tc::mbar_arrive(&mma[g & 1]);
       }
       __syncwarp();
-      it = nit;
-      st = nst;
+      cur = nxt;
     }
   } else if (S > 0) {
     // ---------------- compute ----------------
@@ -980,17 +1027,12 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
     for (int i = 0; i < 56; i++) acc[i] = 0;
     constexpr int RED = FoldRed<PI>::value;
     int since = 0;
-    int it = first, st = 0, p_it = -1, p_st = 0;
     // step 0's chat row
-    if (tid < N162) ctile[tid] = chat[(size_t)col0(first) * N162 + tid];
+    if (tid < N162) ctile[tid] = chat[(size_t)curs[0].c0 * N162 + tid];
     tc::named_sync(2, TCF_CTHREADS);
     for (int g = 0; g <= S; g++) {
-      int nit = it, nst = st;
-      if (g < S) next(nit, nst);
-      // step g + 1's chat row, stored at the end of the iteration
-      uint32_t cnext = 0;
+      uint32_t cnext = 0;  // step g + 1's chat row, stored at the end of the iteration
       const bool has_next = g + 1 < S && tid < N162;
-      if (has_next) cnext = __ldg(chat + (size_t)(col0(nit) + nst) * N162 + tid);
       if (g < S) {
         tc_wait(&full[g & 1], (g >> 1) & 1, abort);                   // step g's words
         if (g >= 2) tc_wait(&mma[g & 1], ((g - 2) >> 1) & 1, abort);  // A buffer g % 2 free
@@ -1000,7 +1042,12 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
         tc::fence_before_sync();
         tc::named_sync(1, TCF_THREADS);  // meets the producer: lockstep, even when a wait timed out
       }
+      if (has_next) {
+        const TcfCursor& nxt = curs[(g + 1) & 3];
+        cnext = __ldg(chat + (size_t)(nxt.c0 + nxt.st) * N162 + tid);
+      }
       if (g >= 1) {
+        const TcfCursor& prev = curs[(g - 1) & 3];
         tc_wait(&mma[(g - 1) & 1], ((g - 1) >> 1) & 1, abort);  // step g - 1's accumulator
         tc::fence_after_sync();
         const uint32_t taddr = tmem + (uint32_t)((g - 1) & 1) * 256u + ((uint32_t)(32 * quad) << 16);
@@ -1046,14 +1093,19 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
 #pragma unroll
           for (int i = 0; i < 56; i++) acc[i] = red_half<PI>(acc[i]);
         }
-        if (p_st + 1 == ncol(p_it)) {
+        if (prev.st + 1 == prev.n) {
           // the item's last column: its sums into vhat_t, a warp's 32 positions per add
-          const size_t p0 = (size_t)(p_it % tiles) * TCF_ROWS;
-          uint32_t* dst = vhat_t + (split_inst ? (size_t)split_inst[p_it / tiles] * wdim * N162 : 0) + p0 + row;
+          const size_t p0 = (size_t)prev.tile * TCF_ROWS;
+          uint32_t* dst = vhat_t + (split_inst ? (size_t)split_inst[prev.split] * wdim * N162 : 0) + p0 + row;
           if (p0 + row < wdim) {
 #pragma unroll
-            for (int i = 0; i < 56; i++)
-              if (part < 2 || i < 50) atomicAdd(dst + (size_t)(v0 + i) * wdim, red_full<PI>(acc[i]));
+            // one pointer walked by an opaque stride, so that the 56 addresses are not hoisted
+            // out of the step loop into registers
+            size_t stride = wdim;
+            asm volatile("" : "+l"(stride));
+            uint32_t* d = dst + (size_t)v0 * stride;
+            for (int i = 0; i < 56; i++, d += stride)
+              if (part < 2 || i < 50) atomicAdd(d, red_full<PI>(acc[i]));
           }
 #pragma unroll
           for (int i = 0; i < 56; i++) acc[i] = 0;
@@ -1062,10 +1114,6 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
       }
       if (has_next) ctile[((g + 1) % 3) * 176 + tid] = cnext;
       tc::named_sync(2, TCF_CTHREADS);  // the chat row of step g + 1 is in place
-      p_it = g < S ? it : -1;
-      p_st = st;
-      it = nit;
-      st = nst;
     }
   }
   tc::fence_before_sync();

@@ -52,15 +52,26 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// A potentially blocking test: the thread may be suspended (issuing nothing) for a hardware time
+// limit while the phase is incomplete.
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
 // Wait for the phase with the given parity to complete; false when `budget` clock cycles passed
 // first (the caller records the timeout and winds down).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long budget) {
-  if (mbar_test(bar, parity)) return true;
+  if (mbar_try(bar, parity)) return true;
   const long long t0 = clock64();
-  while (!mbar_test(bar, parity)) {
+  while (!mbar_try(bar, parity))
     if (clock64() - t0 > budget) return false;
-    __nanosleep(32);
-  }
   return true;
 }
 // One arrival on an mbarrier, and an arrival that also expects `bytes` of bulk copies.
