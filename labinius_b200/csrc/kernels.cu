@@ -286,61 +286,71 @@ __global__ void k_commit_finish(const int32_t* __restrict__ partial, int nchunks
 // Commit on the tensor cores: the 162-point binary transform as a kind::i8 multiply
 // =============================================================================================
 // The transform of an F162 is linear in its bits: What(v) = sum_m bit_m T[m][v] with
-// T[m][v] = theta^{E[v] m} mod q. A step's 128 F162 (8 columns x 4 ring elements x 4 positions)
-// are the rows of an M = 128, N = 176, K = 384 multiply whose A row holds bit m at K-byte m and
-// 128 bit_m at K-byte 192 + m, and whose B (shared memory for the whole kernel) holds T split as
-// lo + 128 hi (tc_transform_operand): the s32 accumulator is the exact transform, < 2^22.
+// T[m][v] = theta^{E[v] m} mod q. A step's 128 F162 (32 columns x the 4 positions of one ring
+// element) are the rows of an M = 128, N = 176, K = 384 multiply whose A row holds bit m at K-byte
+// m and 128 bit_m at K-byte 192 + m, and whose B (shared memory for the whole kernel) holds T split
+// as lo + 128 hi (tc_transform_operand): the s32 accumulator is the exact transform, < 2^22.
+//
+// Row r of a step is column jj = 8 (r / 32) + r % 8 of the tile and position k = (r / 8) % 4 of
+// the ring element, so that the 16x256b tensor-memory load hands each thread the four positions
+// of one column at two leaves: the module product's operands arrive in registers, with no pass
+// through shared memory.
 //
 // The kernel is persistent: CTA b takes the work items b, b + gridDim.x, ... (an item is a tile of
-// 8 columns x a chunk of ring elements, partial[chunk][column] its output), and the steps of all
-// its items form one pipeline of two warp roles:
-//   producer (warp 16)  loads by bulk copies (cp.async.bulk, completion counted on mbarrier
-//            full[(g + 1) % 2]) step g + 1's witness rows and step g's key tile while step g is
-//            being prepared, then issues step g's 12 K-steps into tensor-memory accumulator g % 2
-//            and commits them to mbarrier mma[g % 2];
-//   compute (warps 0-15) per step g: expand step g's witness words into the A operand and meet the
-//            producer (named barrier 1); read step g - 1's accumulator (warp w: lanes of quadrant
-//            w % 4, leaves [40 (w / 4), + 40), warps 0-3 also 160-161), reduce to [0, 2q) into the
-//            transposed u16 tile What[ii][v][jj][k]; the module product with step g - 1's key
-//            tile, 16 multiply-adds per (ring element, leaf, column) accumulated in registers;
-//            release the key buffer (mbarrier kempty). After an item's last step its sums are
-//            written and the registers cleared.
-// Row r of a step is ring element ii = r / 32, column jj = (r / 4) % 8, position k = r % 4, so
-// warp quadrant ii holds ring element ii and its 32 lanes store 32 consecutive u16. Rows past the
-// item's columns or ring elements are zero (their words are not loaded).
-constexpr int TCC_CTHREADS = 512;                      // compute warps 0-15
-constexpr int TCC_THREADS = TCC_CTHREADS + 32;         // and the producer warp
-constexpr int TCC_CT = 8;                              // columns per item
-constexpr int TCC_RT = 4;                              // ring elements per step
-constexpr int TCC_WROW = TCC_RT * 12 + 2;              // staged witness words per column (400 bytes)
+// 32 columns x a chunk of ring elements, partial[chunk][column] its output), and the steps of all
+// its items, one ring element each, form one pipeline of two warp roles (slot g % 2 of each
+// mbarrier pair serves step g; every wait is bounded):
+//   producer (warp 12, one lane) copies step g's key tile into buffer g % 2 once step g - 2's is
+//            released (kempty; completion counted on kfull) and writes step g + 1's cursor, then,
+//            at named barrier 1, issues step g's 12 K-steps into tensor-memory accumulator g % 2
+//            and commits them to mma;
+//   compute (warps 0-11) per step g: expand step g's witness words (wtile g % 2, landed on wfull)
+//            into A buffer g % 2 and meet the producer (named barrier 1); start the 8-byte copies
+//            of step g + 1's words (cp.async, one word a thread, counted on wfull); read step
+//            g - 1's accumulator, warp w the lanes of quadrant w % 4 (columns 8 (w % 4) .. + 7)
+//            and leaves [56 (w / 4), + 56): thread t column 8 (w % 4) + t / 4 at 14 leaves,
+//            reduced to [0, 2q), times the key, 16 multiply-adds per (leaf, column) into 56
+//            registers; release the key tile. After an item's last step each thread writes its
+//            column's sums and clears its registers.
+// A buffer g % 2 is free for step g once step g - 2's multiply is done, which every compute warp
+// saw before reading that step's accumulator; accumulator g % 2 is free once every compute warp
+// has passed named barrier 1 of step g. Rows of columns past the last are zero.
+constexpr int TCC_CTHREADS = 384;                      // compute warps 0-11
+constexpr int TCC_THREADS = TCC_CTHREADS + 32;         // and the producer warp (13 warps: 128 registers)
+constexpr int TCC_CT = 32;                             // columns per item
+constexpr int TCC_RT = 1;                              // ring elements per step
+constexpr int TCC_LPT = 14;                            // leaves per compute thread
 constexpr int TCC_A_BYTES = 128 * TC_KBYTES;           // 128 rows x 384 bytes
-constexpr int TCC_WT_BYTES = TCC_RT * N162 * TCC_CT * 4 * 2;
-constexpr int TCC_AT_BYTES = TCC_RT * N162 * 32;       // a step's key tile
-constexpr int TCC_WTILE_BYTES = TCC_CT * TCC_WROW * 8;
-constexpr int TCC_OFF_A = TC_B_BYTES;
-constexpr int TCC_OFF_WT = TCC_OFF_A + TCC_A_BYTES;
-constexpr int TCC_OFF_AT = TCC_OFF_WT + TCC_WT_BYTES;          // two key tiles
-constexpr int TCC_OFF_WTILE = TCC_OFF_AT + 2 * TCC_AT_BYTES;   // two witness tiles
-constexpr int TCC_OFF_BAR = TCC_OFF_WTILE + 2 * TCC_WTILE_BYTES;
-constexpr int TCC_OFF_CUR = TCC_OFF_BAR + 96;          // four step cursors
+constexpr int TCC_AT_BYTES = N162 * 32;                // a step's key tile
+constexpr int TCC_WT_BYTES = 128 * 24;                 // a step's witness words (three per row)
+constexpr int TCC_OFF_A = TC_B_BYTES;                  // two A buffers
+constexpr int TCC_OFF_AT = TCC_OFF_A + 2 * TCC_A_BYTES;        // two key tiles
+constexpr int TCC_OFF_WT = TCC_OFF_AT + 2 * TCC_AT_BYTES;      // two witness tiles
+constexpr int TCC_OFF_BAR = TCC_OFF_WT + 2 * TCC_WT_BYTES;
+constexpr int TCC_OFF_CUR = TCC_OFF_BAR + 128;         // four step cursors
 constexpr int TCC_SMEM = TCC_OFF_CUR + 4 * 32 + 1024;  // + barriers, tensor-memory slot, flag, cursors, alignment
-constexpr int TCC_VPT = 3;                             // leaves per thread in the module product
 constexpr uint32_t TCC_TMEM_COLS = 512;                // two accumulators at columns 0 and 256
 constexpr long long TC_WAIT_BUDGET = 2000000000ll;     // cycles (about a second) before a timeout
 
-static_assert(TCC_OFF_A % TC_ATOM == 0 && TCC_OFF_AT % 16 == 0 && TCC_OFF_WTILE % 16 == 0 && TCC_OFF_BAR % 8 == 0,
+static_assert(TCC_OFF_A % TC_ATOM == 0 && TCC_A_BYTES % TC_ATOM == 0 && TCC_OFF_AT % 16 == 0 &&
+                  TCC_OFF_WT % 16 == 0 && TCC_OFF_BAR % 8 == 0 && TCC_OFF_CUR % 16 == 0,
               "alignment");
 static_assert(TCC_SMEM <= 232448, "shared memory per CTA");
+static_assert(TCC_CTHREADS == 3 * 128 && 3 * 56 >= N162,
+              "twelve warps: four quadrants x three leaf ranges; three threads per row's words");
 
 // A device-wide flag set by a tensor-core kernel whose bounded wait ran out (never in practice:
 // what it waits for takes microseconds). The host reads and clears it.
 __device__ int g_tc_timeout = 0;
 
-// The same without a plan kept in registers: offsets computed at each call (NC chunks per thread).
+// The thread's part of the A operand: row tid % 128, its NC chunks c_k = tid / 128 + (threads / 128) k
+// of 16 bits (bits 16 c_k ..) expanded to bytes at their swizzled offsets in the bit plane and in the
+// times-128 plane, from the row's F162 words (zero when !valid; at most 34 bits in the third word).
 template <int NC>
-__device__ __forceinline__ void tc_build_row_inline(uint8_t* sA, int tid, int threads, const uint64_t* e) {
+__device__ __forceinline__ void tc_build_row_inline(uint8_t* sA, int tid, int threads, const uint64_t* e,
+                                                    bool valid = true) {
   const int r = tid & 127, step = threads >> 7;
-  const uint64_t w0 = e[0], w1 = e[1], w2 = e[2] & ((1ull << 34) - 1);
+  const uint64_t w0 = valid ? e[0] : 0, w1 = valid ? e[1] : 0, w2 = valid ? e[2] & ((1ull << 34) - 1) : 0;
 #pragma unroll
   for (int k = 0; k < NC; k++) {
     const int c = (tid >> 7) + step * k;
@@ -353,44 +363,6 @@ __device__ __forceinline__ void tc_build_row_inline(uint8_t* sA, int tid, int th
     b.w = (((u >> 12) & 15u) * 0x00204081u) & 0x01010101u;
     *(uint4*)(sA + tc_swizzled_offset(r, 16 * c, 128)) = b;
     *(uint4*)(sA + tc_swizzled_offset(r, 16 * c + 192, 128)) = make_uint4(b.x << 7, b.y << 7, b.z << 7, b.w << 7);
-  }
-}
-
-// What one thread writes of the A operand, planned once: row tid % 128, its NC chunks
-// c_k = tid / 128 + (threads / 128) k of 16 bits (bits 16 c_k ..) with their swizzled offsets in
-// the bit plane and in the times-128 plane.
-template <int NC>
-struct TcRowPlan {
-  int off_lo[NC], off_hi[NC], word[NC], shift[NC];
-  __device__ TcRowPlan(int tid, int threads) {
-    const int r = tid & 127, step = threads >> 7;
-#pragma unroll
-    for (int k = 0; k < NC; k++) {
-      const int c = (tid >> 7) + step * k;
-      off_lo[k] = tc_swizzled_offset(r, 16 * c, 128);
-      off_hi[k] = tc_swizzled_offset(r, 16 * c + 192, 128);
-      word[k] = c >> 2;
-      shift[k] = 16 * (c & 3);
-    }
-  }
-};
-
-// The thread's part of its row of the A operand from the row's F162 words (zero when !valid; at
-// most 34 bits in the third word).
-template <int NC>
-__device__ __forceinline__ void tc_build_row(uint8_t* sA, const TcRowPlan<NC>& pl, const uint64_t* e, bool valid) {
-  const uint64_t w0 = valid ? e[0] : 0, w1 = valid ? e[1] : 0, w2 = valid ? e[2] & ((1ull << 34) - 1) : 0;
-#pragma unroll
-  for (int k = 0; k < NC; k++) {
-    const uint64_t word = pl.word[k] == 0 ? w0 : pl.word[k] == 1 ? w1 : w2;
-    const uint32_t u = (uint32_t)(word >> pl.shift[k]) & 0xFFFFu;
-    uint4 b;
-    b.x = ((u & 15u) * 0x00204081u) & 0x01010101u;
-    b.y = (((u >> 4) & 15u) * 0x00204081u) & 0x01010101u;
-    b.z = (((u >> 8) & 15u) * 0x00204081u) & 0x01010101u;
-    b.w = (((u >> 12) & 15u) * 0x00204081u) & 0x01010101u;
-    *(uint4*)(sA + pl.off_lo[k]) = b;
-    *(uint4*)(sA + pl.off_hi[k]) = make_uint4(b.x << 7, b.y << 7, b.z << 7, b.w << 7);
   }
 }
 
@@ -466,18 +438,18 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);  // swizzle atoms
   uint8_t* sB = smem;
-  uint8_t* sA = smem + TCC_OFF_A;
-  uint16_t* wt = (uint16_t*)(smem + TCC_OFF_WT);
-  int4* atile = (int4*)(smem + TCC_OFF_AT);           // [2][4][162][2]
-  uint64_t* wtile = (uint64_t*)(smem + TCC_OFF_WTILE);  // [2][8][50]
-  uint64_t* full = (uint64_t*)(smem + TCC_OFF_BAR);     // [2]: step g's words and step g - 1's key tile
-  uint64_t* mma = full + 2;                             // [2]: step g's multiply done
-  uint64_t* kempty = full + 4;                          // [2]: the key buffer of step g - 2 read
-  uint64_t* bfull = full + 6;                           // the transform operand loaded
-  uint32_t* tslot = (uint32_t*)(full + 7);
-  volatile int* abort = (volatile int*)(full + 8);
+  uint8_t* sA = smem + TCC_OFF_A;                       // [2] A operands
+  int4* atile = (int4*)(smem + TCC_OFF_AT);             // [2][162][2] key tiles
+  uint64_t* wtile = (uint64_t*)(smem + TCC_OFF_WT);     // [2][128][3] witness words of the rows
+  uint64_t* wfull = (uint64_t*)(smem + TCC_OFF_BAR);    // [2] words landed (cp.async, every compute thread)
+  uint64_t* mma = wfull + 2;                            // [2] multiply done (tcgen05.commit)
+  uint64_t* kfull = wfull + 4;                          // [2] key tile landed (bulk copy)
+  uint64_t* kempty = wfull + 6;                         // [2] key tile read (compute warps)
+  uint64_t* bfull = wfull + 8;                          // the transform operand landed
+  uint32_t* tslot = (uint32_t*)(wfull + 9);
+  volatile int* abort = (volatile int*)(wfull + 10);
   // step g's cursor in slot g % 4: the producer writes step g + 1's before named barrier 1 of step
-  // g; the compute warps read step g's (build) and step g - 1's (module product) after it
+  // g; the compute warps read step g + 1's (word copies) and step g - 1's (item end) after it
   TcCursor* curs = (TcCursor*)(smem + TCC_OFF_CUR);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int col_tiles = (cols + TCC_CT - 1) / TCC_CT;
@@ -486,7 +458,13 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
   for (int it = items.first; it < items.total; it += items.stride) S += items.steps(it);
 
   if (tid == 0) {
-    for (int b = 0; b < 7; b++) tc::mbar_init(&full[b], 1);
+    for (int b = 0; b < 2; b++) {
+      tc::mbar_init(&wfull[b], TCC_CTHREADS);
+      tc::mbar_init(&mma[b], 1);
+      tc::mbar_init(&kfull[b], 1);
+      tc::mbar_init(&kempty[b], TCC_CTHREADS / 32);
+    }
+    tc::mbar_init(bfull, 1);
     *abort = 0;
     curs[0].load(items, items.first);
     tc::mbar_init_fence();
@@ -501,37 +479,23 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
   const uint32_t tmem = *tslot;
 
   if (warp == TCC_CTHREADS / 32) {
-    // ---------------- producer ----------------
-    // the witness rows of step c into tile buffer b, bytes counted on full[b]
-    auto load_words = [&](const TcCursor& c, int b) {
-      const int n = c.n();
-      for (int jj = 0; jj < TCC_CT && c.j0 + jj < cols; jj++)
-        tc::bulk_g2s(wtile + (b * TCC_CT + jj) * TCC_WROW, W + ((size_t)(c.j0 + jj) * wdim + (size_t)4 * c.i) * 3,
-                     96u * n, &full[b]);
-    };
-    auto word_bytes = [&](const TcCursor& c) { return 96u * c.n() * min(TCC_CT, cols - c.j0); };
+    // ---------------- producer (one lane) ----------------
     const uint32_t sA_u = tc::smem_u32(sA), sB_u = tc::smem_u32(sB);
     TcCursor cur = curs[0];
     if (lane == 0 && S > 0) {
       tc::mbar_arrive_expect_tx(bfull, TC_B_BYTES);
       for (int x = 0; x < 4; x++)
         tc::bulk_g2s(sB + x * (TC_B_BYTES / 4), tcb + x * (TC_B_BYTES / 4), TC_B_BYTES / 4, bfull);
-      tc::mbar_arrive_expect_tx(&full[0], word_bytes(cur));
-      load_words(cur, 0);
     }
     for (int g = 0; g < S; g++) {
+      const int b = g & 1;
       TcCursor nxt = cur;
       nxt.advance(items);
       if (lane == 0) {
-        // compute iteration g + 1 reads step g + 1's words and step g's key tile (buffer g % 2,
-        // whose previous tile, step g - 2's, the compute warps have released)
-        if (g >= 2) tc_wait(&kempty[g & 1], ((g - 2) >> 1) & 1, abort);
-        const uint32_t kb = (uint32_t)cur.n() * N162 * 32;
-        const bool more = nxt.valid(items);
-        const uint32_t wb = more ? word_bytes(nxt) : 0u;
-        tc::mbar_arrive_expect_tx(&full[(g + 1) & 1], kb + wb);
-        tc::bulk_g2s(atile + (g & 1) * (TCC_RT * N162 * 2), Ahat + (size_t)cur.i * N162 * 2, kb, &full[(g + 1) & 1]);
-        if (more) load_words(nxt, (g + 1) & 1);
+        // step g's key tile into buffer b, released by step g - 2's module product
+        if (g >= 2) tc_wait(&kempty[b], ((g - 2) >> 1) & 1, abort);
+        tc::mbar_arrive_expect_tx(&kfull[b], TCC_AT_BYTES);
+        tc::bulk_g2s(atile + b * (N162 * 2), Ahat + (size_t)cur.i * N162 * 2, TCC_AT_BYTES, &kfull[b]);
         curs[(g + 1) & 3] = nxt;
       }
       __syncwarp();
@@ -540,108 +504,134 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
         tc::fence_after_sync();
         if (g == 0) tc_wait(bfull, 0, abort);
         if (!*abort)
-          tc_transform_mma(tmem + (uint32_t)(g & 1) * 256u, sA_u, sB_u, &mma[g & 1]);
+          tc_transform_mma(tmem + (uint32_t)b * 256u, sA_u + (uint32_t)b * TCC_A_BYTES, sB_u, &mma[b]);
         else
-          tc::mbar_arrive(&mma[g & 1]);
+          tc::mbar_arrive(&mma[b]);
       }
       __syncwarp();
       cur = nxt;
     }
+    if (lane == 0) {
+      // the last key copies and multiplies have landed before the CTA winds down (bounded waits
+      // that ignore the abort flag: nothing of this CTA may still be in flight at its exit)
+      for (int g = S - 2 < 0 ? 0 : S - 2; g < S; g++) {
+        tc::mbar_wait(&kfull[g & 1], (g >> 1) & 1, TC_WAIT_BUDGET);
+        tc::mbar_wait(&mma[g & 1], (g >> 1) & 1, TC_WAIT_BUDGET);
+      }
+    }
   } else if (S > 0) {
     // ---------------- compute ----------------
-    const int jj_b = lane & 7, sub = lane >> 3;
-    int32_t acc[TCC_VPT][4];
+    const int quad = warp & 3, part = warp >> 2;
+    const int jq = 8 * quad + (lane >> 2);      // the thread's column in the tile
+    const int v0 = 56 * part + 2 * (lane & 3);  // its leaves: v0 + 8 c + l, c < 7, l < 2
+    // the word this thread copies for every step: word wx of row wr (column wj, position wk)
+    const int wr = tid / 3, wx = tid - 3 * (tid / 3);
+    const int wj = 8 * (wr >> 5) + (wr & 7), wk = (wr >> 3) & 3;
+    auto copy_words = [&](const TcCursor& c, int b) {
+      if (c.j0 + wj < cols)
+        tc::cp_async8(wtile + (b * 128 + wr) * 3 + wx, W + ((size_t)(c.j0 + wj) * wdim + (size_t)4 * c.i + wk) * 3 + wx);
+      tc::cp_async_arrive(&wfull[b]);
+    };
+    const int r = tid & 127;
+    const int rj = 8 * (r >> 5) + (r & 7);  // the built row's column
+    int32_t acc[TCC_LPT][4];
 #pragma unroll
-    for (int u = 0; u < TCC_VPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
+    for (int u = 0; u < TCC_LPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
     constexpr int RED = CommitRed<PI>::value;
     int since = 0;
-    const int r = tid & 127;
-    const TcRowPlan<12 * 128 / TCC_CTHREADS> plan(tid, TCC_CTHREADS);
+    // one leaf's module product: positions w0..w3 of the column's ring element, key (lo, hi)
+    auto product = [&](int32_t(&a)[4], uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3, const int4* ah) {
+      const int32_t w0 = (int32_t)red_half<PI>(x0), w1 = (int32_t)red_half<PI>(x1);
+      const int32_t w2 = (int32_t)red_half<PI>(x2), w3 = (int32_t)red_half<PI>(x3);
+      const int4 lo = ah[0], hi = ah[1];
+      a[0] += lo.x * w0 + hi.x * w3 + hi.y * w2 + hi.z * w1;
+      a[1] += lo.y * w0 + lo.x * w1 + hi.y * w3 + hi.z * w2;
+      a[2] += lo.z * w0 + lo.y * w1 + lo.x * w2 + hi.z * w3;
+      a[3] += lo.w * w0 + lo.z * w1 + lo.y * w2 + lo.x * w3;
+    };
+    copy_words(curs[0], 0);
     for (int g = 0; g <= S; g++) {
-      tc_wait(&full[g & 1], (g >> 1) & 1, abort);                          // step g's words, step g - 1's key tile
-      if (g >= 1) tc_wait(&mma[(g - 1) & 1], ((g - 1) >> 1) & 1, abort);  // A free, accumulator g - 1 ready
       if (g < S) {
-        const TcCursor& cur = curs[g & 3];
-        const int jj = (r >> 2) & 7, ii = r >> 5;
-        const bool valid = cur.j0 + jj < cols && ii < cur.n();
-        tc_build_row(sA, plan, wtile + ((g & 1) * TCC_CT + jj) * TCC_WROW + (ii * 4 + (r & 3)) * 3, valid);
+        const int b = g & 1;
+        tc_wait(&wfull[b], (g >> 1) & 1, abort);  // step g's words
+        tc_build_row_inline<12 * 128 / TCC_CTHREADS>(sA + b * TCC_A_BYTES, tid, TCC_CTHREADS,
+                                                   wtile + (b * 128 + r) * 3, curs[g & 3].j0 + rj < cols);
         tc::fence_async_shared();
         tc::fence_before_sync();
         tc::named_sync(1, TCC_THREADS);  // meets the producer: lockstep, even when a wait timed out
+        if (g + 1 < S) copy_words(curs[(g + 1) & 3], (g + 1) & 1);
       }
       if (g >= 1) {
+        const int b = (g - 1) & 1;
+        const uint32_t par = ((g - 1) >> 1) & 1;
         const TcCursor& prev = curs[(g - 1) & 3];
-        const int nst = prev.n();
+        tc_wait(&mma[b], par, abort);    // step g - 1's accumulator
+        tc_wait(&kfull[b], par, abort);  // step g - 1's key tile
         tc::fence_after_sync();
-        {
-          const int quad = warp & 3, part = warp >> 2;
-          const uint32_t taddr = tmem + (uint32_t)((g - 1) & 1) * 256u + ((uint32_t)(32 * quad) << 16);
-          uint16_t* dst = wt + quad * N162 * 32 + lane;
-          uint32_t x[40];  // five loads, one wait
+        // lanes 32 quad .. + 15 hold positions 0-1 of the quadrant's 8 columns, + 16 .. 31 positions 2-3
+        const uint32_t ta = tmem + (uint32_t)b * 256u + ((uint32_t)(32 * quad) << 16) + 56 * part;
+        const uint32_t tb = ta + (16u << 16);
+        const int4* kt = atile + b * (N162 * 2) + 2 * v0;  // the key at the thread's first leaf
 #pragma unroll
-          for (int c = 0; c < 5; c++) tc::tmem_ld8_nowait(taddr + 40 * part + 8 * c, x + 8 * c);
+        for (int cp = 0; cp < 3; cp++) {
+          // chunks 2 cp and 2 cp + 1 (16 columns): x[0..7] positions 0-1, x[8..15] positions 2-3
+          uint32_t x[16];
+          tc::tmem_ld16x256_x2_nowait(ta + 16 * cp, x);
+          tc::tmem_ld16x256_x2_nowait(tb + 16 * cp, x + 8);
           tc::tmem_wait_ld(x);
 #pragma unroll
-          for (int i = 0; i < 40; i++) dst[(40 * part + i) * 32] = (uint16_t)red_half<PI>(x[i]);
-          if (part == 0) {
-            uint32_t y[2];
-            tc::tmem_ld2(taddr + 160, y);
-            dst[160 * 32] = (uint16_t)red_half<PI>(y[0]);
-            dst[161 * 32] = (uint16_t)red_half<PI>(y[1]);
-          }
+          for (int h = 0; h < 2; h++)
+#pragma unroll
+            for (int l = 0; l < 2; l++)
+              product(acc[2 * (2 * cp + h) + l], x[4 * h + l], x[4 * h + 2 + l], x[8 + 4 * h + l],
+                      x[8 + 4 * h + 2 + l], kt + 2 * (8 * (2 * cp + h) + l));
+        }
+        {
+          // chunk 6; the last leaf range's pads (leaves 162 - 167) use leaf 161's key, unused
+          uint32_t x[8];
+          tc::tmem_ld16x256_x1_nowait(ta + 48, x);
+          tc::tmem_ld16x256_x1_nowait(tb + 48, x + 4);
+          tc::tmem_wait_ld(x);
+#pragma unroll
+          for (int l = 0; l < 2; l++)
+            product(acc[12 + l], x[l], x[2 + l], x[4 + l], x[6 + l], kt + 2 * (min(v0 + 48 + l, N162 - 1) - v0));
         }
         tc::fence_before_sync();
-        tc::named_sync(2, TCC_CTHREADS);  // the transform tile is complete
-        const int4* kt = atile + ((g - 1) & 1) * (TCC_RT * N162 * 2);
-        for (int ii = 0; ii < nst; ii++) {
-          const int4* ah = kt + ii * N162 * 2;
+        tc::fence_async_shared();  // this warp's reads of the key tile precede the next bulk copy into it
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&kempty[b]);
+        if (++since >= RED) {
+          since = 0;
 #pragma unroll
-          for (int u = 0; u < TCC_VPT; u++) {
-            const int v = 4 * (warp + 16 * u) + sub;
-            if (v < N162) {
-              const uint2 wv = *(const uint2*)(wt + (((ii * N162) + v) * TCC_CT + jj_b) * 4);
-              const int32_t w0 = wv.x & 0xFFFF, w1 = wv.x >> 16, w2 = wv.y & 0xFFFF, w3 = wv.y >> 16;
-              const int4 lo = ah[2 * v], hi = ah[2 * v + 1];
-              acc[u][0] += lo.x * w0 + hi.x * w3 + hi.y * w2 + hi.z * w1;
-              acc[u][1] += lo.y * w0 + lo.x * w1 + hi.y * w3 + hi.z * w2;
-              acc[u][2] += lo.z * w0 + lo.y * w1 + lo.x * w2 + hi.z * w3;
-              acc[u][3] += lo.w * w0 + lo.z * w1 + lo.y * w2 + lo.x * w3;
-            }
-          }
-          if (++since >= RED) {
-            since = 0;
+          for (int u = 0; u < TCC_LPT; u++)
 #pragma unroll
-            for (int u = 0; u < TCC_VPT; u++)
-#pragma unroll
-              for (int c = 0; c < 4; c++) acc[u][c] = red_signed<PI>(acc[u][c]);
-          }
+            for (int c = 0; c < 4; c++) acc[u][c] = red_signed<PI>(acc[u][c]);
         }
         if (prev.last()) {
-          // the item's last step: its sums out, the registers cleared
-          const int j = prev.j0 + jj_b;
+          // the item's last step: the column's sums out, the registers cleared
+          const int j = prev.j0 + jq;
           if (j < cols) {
+            int4* dst = (int4*)partial + ((size_t)prev.ci * cols + j) * N162;
 #pragma unroll
-            for (int u = 0; u < TCC_VPT; u++) {
-              const int v = 4 * (warp + 16 * u) + sub;
+            for (int u = 0; u < TCC_LPT; u++) {
+              const int v = v0 + 8 * (u >> 1) + (u & 1);
               if (v < N162) {
                 int4 o;
                 o.x = (int)red_signed_full<PI>(acc[u][0]);
                 o.y = (int)red_signed_full<PI>(acc[u][1]);
                 o.z = (int)red_signed_full<PI>(acc[u][2]);
                 o.w = (int)red_signed_full<PI>(acc[u][3]);
-                ((int4*)partial)[((size_t)prev.ci * cols + j) * N162 + v] = o;
+                dst[v] = o;
               }
             }
           }
 #pragma unroll
-          for (int u = 0; u < TCC_VPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
+          for (int u = 0; u < TCC_LPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
           since = 0;
         }
-        tc::fence_async_shared();         // this thread's reads of the key tile precede the next bulk copy into it
-        tc::named_sync(2, TCC_CTHREADS);  // the transform tile and the key tile are free
-        if (tid == 0) tc::mbar_arrive(&kempty[(g - 1) & 1]);
       }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy of this thread outlives the CTA
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -2153,13 +2143,13 @@ cudaError_t launch_key_components(int pi, const int16_t* A, const DevPrime* D, i
 
 size_t commit_smem_bytes() { return LUT_BYTES + CT * WROW * 8 + RT * N162 * CT * 4 * 2 + AT_BYTES; }
 
-// The commit's transforms run on the tensor cores (k_commit_tc) when LBG_COMMIT_KERNEL=tc, else on
-// the CUDA cores (k_commit) (both are exact; the switch is for comparing them). The commit
+// The commit's transforms run on the tensor cores (k_commit_tc) unless LBG_COMMIT_KERNEL=scalar
+// selects the CUDA cores (k_commit) (both are exact; the switch is for comparing them). The commit
 // that keeps the base limb's transform for the fold always runs the CUDA-core kernel.
 bool commit_tc_enabled() {
   static const bool on = [] {
     const char* e = getenv("LBG_COMMIT_KERNEL");
-    return e && std::string(e) == "tc";
+    return !(e && std::string(e) == "scalar");
   }();
   return on;
 }
@@ -2186,10 +2176,8 @@ int commit_blocks_per_sm(int pi) {
   return (e == cudaSuccess && n > 0) ? n : 1;
 }
 int commit_cols_per_cta() { return commit_tc_enabled() ? TCC_CT : CT; }
-int commit_ring_per_step() {
-  static_assert(RT == TCC_RT, "both commit kernels step over the same ring elements");
-  return RT;
-}
+// Chunks are whole steps of the scalar kernel (RT ring elements); the tensor-core kernel takes any.
+int commit_ring_per_step() { return RT; }
 
 int tc_timeout_take() {
   int v = 0;
