@@ -606,7 +606,7 @@ def run_wire(L, prover, params, steps):
             "workload": "the folded witness of the bench's step (len_ring x 648 int16), interleaved rANS, 64 lanes"}
 
 
-def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
+def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027, server_kw=None):
     """Served: commit+open requests with log2 n ~ U{18..22} (column length 2048, moduli [3889, 9721]),
     80% Witness::random and 20% B128 traces opened through the cross-field switch, each from its
     own seed, through the serving loop (continuous batching over two device arenas, transcripts on
@@ -634,8 +634,13 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
 
     pp = L.PublicParameters.from_seed(params(7), MATRIX_SEED)
     # small requests (at most 2^20 F162) on a slot of their own, so that none waits behind large ones
-    srv = Server(pp, capacity_columns=8192, max_requests=64, slots=slots, host_threads=os.cpu_count() or 1,
-                 keep_results=False, small_log_len=9)
+    # at most 4096 columns a batch (two 2^22 requests): a request that arrives while a batch runs waits
+    # for at most that much work (at 8192 columns the p99 at 0.7 load was 29 ms, at 4096 20 ms, for
+    # 2% less saturated throughput)
+    kw = dict(capacity_columns=4096, max_requests=64, slots=slots, host_threads=os.cpu_count() or 1,
+              keep_results=False, small_log_len=9)
+    kw.update(server_kw or {})
+    srv = Server(pp, **kw)
 
     def run(idx, rate):
         reqs, t0 = [], time.perf_counter()
@@ -666,6 +671,13 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
     st_elems, st_reqs, lat, lat_logs = run(range(requests), rate)
     batches = srv.batches - b0
     srv.close()
+    if plain_sample == 0:
+        return {"rate_req_s": rate, "batches": batches, "throughput_elems_s": st_elems,
+                "saturated_elems_s": sat_elems, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)),
+                "by_log2_n": {str(lg): [float(np.percentile(lat[lat_logs == lg], 50)),
+                                        float(np.percentile(lat[lat_logs == lg], 99))]
+                              for lg in range(18, 23) if (lat_logs == lg).any()}}
 
     # the plain per-request path on a sample of the same requests
     pps = {}
@@ -719,8 +731,9 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
                             "plain_p50_ms": float(np.percentile(psel, 50)) if len(psel) else None,
                             "plain_p99_ms": float(np.percentile(psel, 99)) if len(psel) else None}
     return {"requests": requests, "rate_req_s": rate, "load": load, "batches": batches, "by_log2_n": by_size,
-            "admission": "arenas within half the free HBM, at most 8192 columns a batch; requests of at most "
-                         "2^20 F162 on a slot of their own, the other slot large ones first",
+            "admission": "arenas within half the free HBM, at most %d columns a batch; requests of at most "
+                         "2^20 F162 on a slot of their own (greatest stream priority), the other slot large ones "
+                         "first" % kw["capacity_columns"],
             "throughput_elems_s": st_elems, "throughput_req_s": st_reqs,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()),
@@ -734,7 +747,7 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027):
                         "drawn from the request's seed (commit, tagged commitment absorbed, switch::prove of "
                         "the trace's value there, row evaluation, folding challenges, fold); Poisson "
                         "arrivals at load x saturated rate",
-            "slots": slots, "slot_columns": 8192, "host_threads": os.cpu_count() or 1}
+            "slots": slots, "slot_columns": kw["capacity_columns"], "host_threads": os.cpu_count() or 1}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -856,26 +869,40 @@ def run_ours(args):
         mat = torch.empty((r, 4, L_, 162), dtype=torch.int16, pin_memory=True).numpy()
         vout = torch.empty((params.len_ring(), 648), dtype=torch.int16, pin_memory=True).numpy()
 
-        def e2e_step():
+        # the same witness in ordinary pageable memory, as a Rust Vec<F162> or a numpy array is
+        hw_pageable = np.array(hw, copy=True)
+        mat_pageable = np.empty_like(mat)
+        vout_pageable = np.empty_like(vout)
+
+        def e2e_step(src=hw, m=mat, v=vout):
             # Witness::from_elements + Prover::commit (the upload pipelined against the commit by
             # column groups), then Prover::fold, results read back
             wh = ctypes.c_void_p()
             op = ctypes.c_void_p()
-            check(N.lbg_commit_host(prover._h, ptr(hw), n, ptr(mat), None, None, ctypes.byref(wh), ctypes.byref(op)))
-            check(N.lbg_fold(prover._h, op, ptr(chal), len(chal), ptr(vout)))
+            check(N.lbg_commit_host(prover._h, ptr(src), n, ptr(m), None, None, ctypes.byref(wh), ctypes.byref(op)))
+            check(N.lbg_fold(prover._h, op, ptr(chal), len(chal), ptr(v)))
             N.lbg_witness_free(wh)
 
-        for _ in range(2):
-            e2e_step()
-        torch.cuda.synchronize()
-        barrier(world)
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            e2e_step()
-        torch.cuda.synchronize()
-        e2e_ms = allreduce_max((time.perf_counter() - t0) * 1000.0 / args.steps, world, "cuda")
+        def timed_e2e(**kw):
+            for _ in range(2):
+                e2e_step(**kw)
+            torch.cuda.synchronize()
+            barrier(world)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                e2e_step(**kw)
+            torch.cuda.synchronize()
+            return allreduce_max((time.perf_counter() - t0) * 1000.0 / args.steps, world, "cuda")
+
+        e2e_ms = timed_e2e()
+        e2e_pageable_ms = timed_e2e(src=hw_pageable, m=mat_pageable, v=vout_pageable)
         e2e = {"value": whole_job_value(world, n, e2e_ms), "unit": "elems/s", "ms_per_step": e2e_ms,
                "h2d_bytes_per_step": 24 * n + chal.nbytes, "d2h_bytes_per_step": mat.nbytes + vout.nbytes,
+               "host_memory": "page-locked witness, commitment and folded-witness buffers",
+               "pageable": {"value": whole_job_value(world, n, e2e_pageable_ms), "unit": "elems/s",
+                            "ms_per_step": e2e_pageable_ms,
+                            "host_memory": "ordinary pageable buffers (the witness staged through the prover's "
+                                           "page-locked ring by host threads)"},
                "timing": "host wall clock around synchronous API calls, max over ranks"}
 
     # wire::encode of the folded witness (crates/bench/src/bin/labinius.rs:142, "encode folded

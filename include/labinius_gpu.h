@@ -44,7 +44,7 @@ extern "C" {
 #define LBG_ERR_PARAMS (-2)      /* ParamError (crates/pcs/src/scheme/params.rs:20-50) */
 #define LBG_ERR_CUDA (-3)        /* a CUDA call failed */
 #define LBG_ERR_OOM (-4)         /* device allocation failed */
-#define LBG_ERR_UNSUPPORTED (-5) /* e.g. Opening::Recursive: LaBRADOR stays on the host */
+#define LBG_ERR_UNSUPPORTED (-5) /* a step of the recursive round that LaBRADOR makes on the host */
 #define LBG_ERR_WITNESS (-6)     /* WitnessError::WrongLength (crates/pcs/src/scheme/witness.rs:10-23) */
 
 #define LBG_OPENING_CLEAR 0
@@ -108,11 +108,13 @@ void lbg_witness_free(lbg_witness* w);
 int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16_t* top_out,
                uint16_t* digits_out, lbg_opening** opening_out);
 /* Witness::from_elements + Prover::commit in one call, the upload pipelined against the commit:
- * the n F162 at f162 (host memory; page-locked for the copies to overlap the commit) are copied in
- * column groups on a second stream, and each group's commit starts as soon as it has landed (limb
- * 0 on the prover's stream, each further limb on a stream of its own, so the limbs' commits of a
- * group overlap). Outputs as lbg_commit; *w_out gets the device witness (free it with
- * lbg_witness_free). */
+ * the n F162 at f162 (host memory) are copied in column groups on a second stream, and each group's
+ * commit starts as soon as it has landed (limb 0 on the prover's stream, each further limb on a
+ * stream of its own, so the limbs' commits of a group overlap). Page-locked memory is copied
+ * directly; pageable memory (a Rust Vec<F162>) passes group by group through the prover's ring of
+ * three page-locked staging buffers (one column group each, allocated on first use), filled by a
+ * few host threads while the device copies and commits the groups before. Outputs as lbg_commit;
+ * *w_out gets the device witness (free it with lbg_witness_free). */
 int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* matrix_out, uint16_t* top_out,
                     uint16_t* digits_out, lbg_witness** w_out, lbg_opening** opening_out);
 int lbg_opening_matrix(const lbg_opening* op, int16_t* matrix_out);
@@ -125,6 +127,20 @@ void lbg_opening_free(lbg_opening* op);
  * (bit-dropped, :386-397). out null: returns the byte count only; else cap >= that count. Returns the
  * byte count or a negative status. */
 long long lbg_opening_pack_commitment(const lbg_opening* op, uint8_t* out, size_t cap);
+/* Opening::Recursive, the commitment's half that runs here (crates/pcs/src/scheme/prover.rs:55-91 with
+ * the recursion set up): recursion::limbs::residues (crates/pcs/src/recursion/limbs.rs:379-398) of the
+ * opening's commitment, computed on the device, for the host's LaBRADOR bridge to commit as
+ * T_y = key_y.commit_blocks(residues). out: int16 [limbs * 4][polys][64]; vector 4 k + l holds, for
+ * limb k and component l, each column's coefficients 4 m + l centred and times (-1)^m, in chunks of
+ * 54 (chunk b of column j is polynomial b * columns + j, positions 0..53), the rest zero. polys >=
+ * 3 * columns (the reference pads to a multiple of 32). Clear and recursive commitments. */
+int lbg_opening_residues(const lbg_opening* op, size_t polys, int16_t* out);
+/* Prover::commit_left_expansion (crates/pcs/src/scheme/prover.rs:95-115), the vector half: u of the
+ * row values (columns F162, [columns][3]) on the device, chunk b of lift(u_j) (its bits as 0/1
+ * coefficients, crates/pcs/src/recursion/binary.rs:49-51, chunk.rs:76-86) at polynomial b * columns
+ * + j of out (int16 [rank][64], rank >= 3 * columns, the recursion setup's ranks[U]), the rest
+ * zero. T_u = key_u.commit_blocks(u) is LaBRADOR's, on the host. */
+int lbg_left_expansion(const lbg_pp* pp, const uint64_t* row_values, size_t columns, size_t rank, int16_t* out);
 
 /* Witness::row_evaluate (crates/pcs/src/scheme/witness.rs:100-106, crates/pcs/src/eval.rs:171-182):
  * u_out = columns F162. */
@@ -333,6 +349,14 @@ int lbg_batch_set_switch(lbg_batch* b, const uint8_t* flags, const uint64_t* r_h
 int lbg_batch_switch_outputs(const lbg_batch* b, uint64_t* partials, uint64_t* rounds, uint64_t* opened,
                              uint64_t* claims);
 void* lbg_batch_stream(const lbg_batch* b);
+/* No reference counterpart (the reference has no server): the batch's stream at the device's
+ * greatest (high != 0) or default priority, so that a slot of small requests is scheduled ahead of
+ * a slot of large ones when both wait for SMs. Drains the old stream and drops captured graphs. */
+int lbg_batch_set_priority(lbg_batch* b, int high);
+/* No reference counterpart: at most `ctas` CTAs (one per SM; 0: every SM) for the batch's
+ * persistent commit and fold launches, so that a second batch's launches find SMs free while this
+ * one runs (a server's slot of large requests beside its slot of small ones). Drops captured graphs. */
+int lbg_batch_set_sm_limit(lbg_batch* b, int ctas);
 uint64_t lbg_batch_launch_count(const lbg_batch* b);
 
 /* Shape queries. */

@@ -115,6 +115,10 @@ SIGNATURES = {
     "lbg_ntt648_forward": (_int, [ctypes.c_uint32, _vp, _vp, _sz, _vp]),
     "lbg_ntt648_inverse": (_int, [ctypes.c_uint32, _vp, _vp, _sz, _vp]),
     "lbg_batch_stream": (_vp, [_vp]),
+    "lbg_batch_set_priority": (_int, [_vp, _int]),
+    "lbg_opening_residues": (_int, [_vp, _sz, _vp]),
+    "lbg_left_expansion": (_int, [_vp, _vp, _sz, _sz, _vp]),
+    "lbg_batch_set_sm_limit": (_int, [_vp, _int]),
     "lbg_batch_launch_count": (_u64, [_vp]),
 }
 

@@ -137,6 +137,14 @@ class Batch:
     def use_graphs(self, enable=True):
         check(lib().lbg_batch_use_graphs(self._h, int(enable)))
 
+    def set_sm_limit(self, ctas=0):
+        """At most `ctas` CTAs (one per SM; 0: every SM) for the persistent commit and fold launches."""
+        check(lib().lbg_batch_set_sm_limit(self._h, int(ctas)))
+
+    def set_priority(self, high=True):
+        """Run the batch's stream at the device's greatest priority (or the default)."""
+        check(lib().lbg_batch_set_priority(self._h, int(high)))
+
     def keep_transform(self, enable=True):
         """The fold reads the commit's kept transform (on) or transforms the witness again (off)."""
         check(lib().lbg_batch_set_kept_transform(self._h, int(enable)))

@@ -1,7 +1,7 @@
 """Build the CUDA extension in-tree: ``labinius_b200/liblabinius_gpu.so`` for sm_100a.
 
-One nvcc invocation over the C ABI (api.cu), the kernels (kernels.cu) and the host tables,
-BLAKE3 and transcript (.cpp). The library exports only the C ABI of include/labinius_gpu.h.
+One nvcc invocation per source (the C ABI, the kernels, the host tables, BLAKE3 and transcript),
+run in parallel, then one link. The library exports only the C ABI of include/labinius_gpu.h.
 """
 import os
 import subprocess
@@ -11,7 +11,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "liblabinius_gpu.so")
 SOURCES = ["api.cu", "kernels.cu", "fold_static.cu", "batch.cu", "transcript_dev.cu", "ntt_api.cu", "switch.cu", "wire.cu", "wire_pack.cu", "ring_tables.cpp", "blake3_host.cpp", "transcript.cpp"]
-HEADERS = ["kernels.cuh", "tcgen05.cuh", "gf2_dev.cuh", "prime_structs.h", "hasher_state.h", "blake3_dev.cuh", "transcript_dev.h", "switch.h", "upload.h", "error.h", "handles.h", "launch.h", "ring_tables.h", "blake3_host.h", "transcript.h"]
+HEADERS = ["kernels.cuh", "copy_pool.h", "tcgen05.cuh", "gf2_dev.cuh", "prime_structs.h", "hasher_state.h", "blake3_dev.cuh", "transcript_dev.h", "switch.h", "upload.h", "error.h", "handles.h", "launch.h", "ring_tables.h", "blake3_host.h", "transcript.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -37,14 +37,27 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object (in parallel, one nvcc per source) under _build/, then link
+    the shared library."""
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fvisibility=hidden",
-           "-I", INCLUDE, "-o", LIB + ".tmp", *sources()]
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+             "-Xcompiler", "-fvisibility=hidden", "-I", INCLUDE]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.check_call(cmd)
+        flags.insert(0, "-Xptxas=-v")
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        subprocess.check_call([nvcc(), *flags, "-c", "-o", obj, src])
+        return obj
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 4)) as ex:
+        objs = list(ex.map(compile_one, sources()))
+    subprocess.check_call([nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lpthread"])
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

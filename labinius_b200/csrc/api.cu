@@ -7,6 +7,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/labinius_gpu.h"
@@ -133,7 +134,6 @@ int lbg_params_check(const lbg_params* p) {
       if (p->moduli[j] == p->moduli[i])
         return fail(LBG_ERR_PARAMS, j == 0 ? "the base modulus is listed again as an extra one" : "a modulus is listed twice");
   }
-  if (p->opening == LBG_OPENING_RECURSIVE) return fail(LBG_ERR_UNSUPPORTED, "Opening::Recursive runs LaBRADOR on the host; not on this path");
   if (p->opening == LBG_OPENING_BIT_DROPPED && (p->dropped_bits < 1 || p->dropped_bits > 14))
     return fail(LBG_ERR_PARAMS, "dropped bits out of range");
   if (p->opening > LBG_OPENING_RECURSIVE) return fail(LBG_ERR_PARAMS, "unknown opening mode");
@@ -210,6 +210,7 @@ void lbg_public_parameters_free(lbg_pp* pp) {
   cudaFree(pp->d_chat);
   cudaFree(pp->d_fc);
   cudaFree(pp->d_wire);
+  cudaFree(pp->d_lift);
   lbg_switch_release(pp);
   if (pp->stream) cudaStreamDestroy(pp->stream);
   delete pp;
@@ -449,12 +450,18 @@ void lbg_prover_free(lbg_prover* pr) {
   }
   for (auto e : pr->limb_done) cudaEventDestroy(e);
   for (auto* d : pr->limb_partial) cudaFree(d);
+  for (int s = 0; s < lbg_prover::STAGES; s++) {
+    if (pr->stage_copied[s]) cudaEventDestroy(pr->stage_copied[s]);
+    if (pr->stage[s]) cudaFreeHost(pr->stage[s]);
+  }
+  delete pr->copy_pool;
   cudaFree(pr->d_partial);
   cudaFree(pr->d_vhat);
   cudaFree(pr->d_ch);
   cudaFree(pr->d_chat);
   cudaFree(pr->d_v);
   cudaFree(pr->d_wire);
+  cudaFree(pr->d_rec);
   cudaFree(pr->d_res);
   for (auto* b : pr->spare) free_bufs(b);
   for (auto& m : pr->marks) {
@@ -695,10 +702,57 @@ int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16
   return LBG_OK;
 }
 
+// Whether host memory `p` is pageable (not page-locked or registered with CUDA).
+static bool host_pageable(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return a.type == cudaMemoryTypeUnregistered;
+}
+
+// The staging ring of lbg_commit_host for pageable witnesses: STAGES page-locked buffers of at
+// least `bytes`, their copy events, and the host copy threads. Waits for any copy still reading
+// the buffers (a previous call's) before they are handed out again.
+static int stage_ready(lbg_prover* pr, size_t bytes) {
+  for (int s = 0; s < lbg_prover::STAGES; s++)
+    if (pr->stage_copied[s]) LBG_CU(cudaEventSynchronize(pr->stage_copied[s]));
+  if (pr->stage_bytes < bytes) {
+    for (int s = 0; s < lbg_prover::STAGES; s++) {
+      if (pr->stage[s]) cudaFreeHost(pr->stage[s]);
+      pr->stage[s] = nullptr;
+    }
+    pr->stage_bytes = 0;
+    for (int s = 0; s < lbg_prover::STAGES; s++)
+      if (cudaHostAlloc(&pr->stage[s], bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        for (int t = 0; t <= s; t++) {
+          if (pr->stage[t]) cudaFreeHost(pr->stage[t]);
+          pr->stage[t] = nullptr;
+        }
+        return fail(LBG_ERR_OOM, "page-locked staging buffers");
+      }
+    pr->stage_bytes = bytes;
+  }
+  for (int s = 0; s < lbg_prover::STAGES; s++)
+    if (!pr->stage_copied[s] && cudaEventCreateWithFlags(&pr->stage_copied[s], cudaEventDisableTiming) != cudaSuccess)
+      return fail(LBG_ERR_CUDA, "event");
+  if (!pr->copy_pool) {
+    unsigned hc = std::thread::hardware_concurrency();
+    int workers = hc >= 16 ? 7 : hc >= 4 ? (int)hc / 2 - 1 : 0;
+    pr->copy_pool = new lbg::CopyPool(workers);
+  }
+  return LBG_OK;
+}
+
 // Witness::from_elements + Prover::commit with the upload pipelined against the commit: the
-// witness (host memory; page-locked for the copies to overlap) arrives in column groups on the
-// prover's copy stream, and every limb's commit of a group starts on the compute stream as soon
-// as that group has landed. The results are those of lbg_witness_from_host + lbg_commit.
+// witness arrives in column groups on the prover's copy stream, and every limb's commit of a
+// group starts on the compute stream as soon as that group has landed. Page-locked host memory is
+// copied to the device directly; pageable memory (a Rust Vec, a numpy array) passes group by
+// group through a ring of page-locked staging buffers, each filled by several host threads while
+// the device copies the previous group out and commits the ones before. The results are those of
+// lbg_witness_from_host + lbg_commit.
 int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* matrix_out, uint16_t* top_out,
                     uint16_t* digits_out, lbg_witness** w_out, lbg_opening** opening_out) {
   if (!pr || !f162 || !w_out) return fail(LBG_ERR_INVALID, "null argument");
@@ -754,10 +808,31 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
   }
   cudaStream_t st = pr->stream, cp = pr->copy_stream;
   const size_t per_col = pp->wdim * 3;  // u64 words of a column
+  const size_t group_bytes = (size_t)gc * per_col * 8;
+  const bool pageable = host_pageable(f162);
+  if (pageable) {
+    rc = stage_ready(pr, group_bytes);
+    if (rc) {
+      std::lock_guard<std::mutex> g(pr->mu);
+      pr->spare.push_back(b);
+      witness_release(w);
+      return rc;
+    }
+  }
   cudaError_t e = cudaSuccess;
   for (int g = 0; g < groups && e == cudaSuccess; g++) {
     const size_t c0 = (size_t)g * gc;
-    e = cudaMemcpyAsync(w->d + c0 * per_col, f162 + c0 * per_col, (size_t)gc * per_col * 8, cudaMemcpyHostToDevice, cp);
+    if (pageable) {
+      // stage g % STAGES is free once the device copy of group g - STAGES out of it has finished
+      const int s = g % lbg_prover::STAGES;
+      e = cudaEventSynchronize(pr->stage_copied[s]);
+      if (e != cudaSuccess) break;
+      pr->copy_pool->copy(pr->stage[s], f162 + c0 * per_col, group_bytes);
+      e = cudaMemcpyAsync(w->d + c0 * per_col, pr->stage[s], group_bytes, cudaMemcpyHostToDevice, cp);
+      if (e == cudaSuccess) e = cudaEventRecord(pr->stage_copied[s], cp);
+    } else {
+      e = cudaMemcpyAsync(w->d + c0 * per_col, f162 + c0 * per_col, group_bytes, cudaMemcpyHostToDevice, cp);
+    }
     if (e == cudaSuccess) e = cudaEventRecord(pr->group_events[g], cp);
     for (int k = 0; k < L && e == cudaSuccess; k++) {
       // limb 0 on the prover's stream (bracketed for the profile), limb k >= 1 on its own
@@ -867,6 +942,67 @@ int lbg_opening_dropped(const lbg_opening* op, uint16_t* top_out, uint16_t* digi
     LBG_CU(cudaMemcpyAsync(digits_out, op->bufs->d_digits, (size_t)(pp->limbs - 1) * count * 2,
                            cudaMemcpyDeviceToHost, op->pr->stream));
   LBG_CU(cudaStreamSynchronize(op->pr->stream));
+  return LBG_OK;
+}
+
+// Grows a device buffer to at least `bytes` (contents not kept).
+static int grow(void** buf, size_t* cap, size_t bytes) {
+  if (*cap >= bytes) return LBG_OK;
+  cudaFree(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  if (cudaMalloc(buf, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(LBG_ERR_OOM, "device buffer");
+  }
+  *cap = bytes;
+  return LBG_OK;
+}
+
+// recursion::limbs::residues (crates/pcs/src/recursion/limbs.rs:379-398) of the opening's commitment,
+// computed on the device from where the commit left it: per limb, the columns' coefficients
+// (k_column_residues), then the four component vectors of chunked, signed, centred coefficients.
+int lbg_opening_residues(const lbg_opening* op, size_t polys, int16_t* out) {
+  if (!op || !out) return fail(LBG_ERR_INVALID, "null argument");
+  lbg_prover* pr = op->pr;
+  const lbg_pp* pp = pr->pp;
+  if (pp->params.opening == LBG_OPENING_BIT_DROPPED)
+    return fail(LBG_ERR_INVALID, "a bit-dropped commitment keeps no matrix to take residues of");
+  const int cols = (int)pp->cols, L = pp->limbs;
+  if (polys < (size_t)3 * cols) return fail(LBG_ERR_INVALID, "fewer polynomials than 3 x columns");
+  LBG_CU(cudaSetDevice(pp->device));
+  std::lock_guard<std::mutex> g(pr->mu);
+  const size_t per_limb = 4 * polys * 64;
+  int rc = grow((void**)&pr->d_rec, &pr->rec_cap, (size_t)L * per_limb * 2);
+  if (rc) return rc;
+  const size_t count = pp->cols * N648;
+  cudaStream_t st = pr->stream;
+  for (int k = 0; k < L; k++) {
+    LBG_CU(launch_column_residues(pp->pidx[k], op->bufs->d_C, cols, k, L, pp->d_prime[k], pr->d_res + (size_t)k * count,
+                                  st));
+    LBG_CU(launch_recursion_residues(pr->d_res + (size_t)k * count, cols, polys, pp->primes[k],
+                                     pr->d_rec + (size_t)k * per_limb, st));
+  }
+  pr->launches += 2 * L;
+  LBG_CU(cudaMemcpyAsync(out, pr->d_rec, (size_t)L * per_limb * 2, cudaMemcpyDeviceToHost, st));
+  LBG_CU(cudaStreamSynchronize(st));
+  return LBG_OK;
+}
+
+// Prover::commit_left_expansion's vector u (crates/pcs/src/scheme/prover.rs:95-115) on the device.
+int lbg_left_expansion(const lbg_pp* pp_c, const uint64_t* row_values, size_t cols, size_t rank, int16_t* out) {
+  if (!pp_c || !row_values || !out) return fail(LBG_ERR_INVALID, "null argument");
+  lbg_pp* pp = const_cast<lbg_pp*>(pp_c);
+  if (cols != pp->cols) return fail(LBG_ERR_INVALID, "the row evaluation does not match the parameters");
+  if (rank < 3 * cols) return fail(LBG_ERR_INVALID, "fewer polynomials than 3 x columns");
+  std::lock_guard<std::mutex> g(pp->mu);
+  LBG_CU(cudaSetDevice(pp->device));
+  int rc = grow((void**)&pp->d_lift, &pp->lift_cap, rank * 64 * 2);
+  if (rc) return rc;
+  LBG_CU(cudaMemcpyAsync(pp->d_u, row_values, cols * 24, cudaMemcpyHostToDevice, pp->stream));
+  LBG_CU(launch_left_expansion(pp->d_u, (int)cols, rank, pp->d_lift, pp->stream));
+  LBG_CU(cudaMemcpyAsync(out, pp->d_lift, rank * 64 * 2, cudaMemcpyDeviceToHost, pp->stream));
+  LBG_CU(cudaStreamSynchronize(pp->stream));
   return LBG_OK;
 }
 
@@ -1219,11 +1355,21 @@ static int derive_point(const RoundShape& s, lbg_transcript* t, const int16_t* m
   return LBG_OK;
 }
 
+// The recursive opening's transcript absorbs LaBRADOR commitments (T_y for the evaluation point,
+// T_u for the folding challenges: crates/pcs/src/scheme/verifier.rs), which the host's LaBRADOR
+// bridge makes; the library's transcript steps cover the Clear and bit-dropped rounds only.
+static int refuse_recursive(uint32_t opening) {
+  return opening == LBG_OPENING_RECURSIVE
+             ? fail(LBG_ERR_UNSUPPORTED, "the recursive round absorbs LaBRADOR commitments made on the host")
+             : LBG_OK;
+}
+
 int lbg_params_derive_evaluation_point(const lbg_params* p, const uint8_t matrix_seed[32], lbg_transcript* t,
                                        const int16_t* matrix, const uint16_t* top, const uint16_t* digits,
                                        uint64_t* p0_out, uint64_t* p1_out) {
   if (!p || !matrix_seed || !t || !p0_out || !p1_out) return fail(LBG_ERR_INVALID, "null argument");
   int rc = lbg_params_check(p);
+  if (!rc) rc = refuse_recursive(p->opening);
   if (rc) return rc;
   return derive_point(shape_of_params(p, matrix_seed), t, matrix, top, digits, p0_out, p1_out);
 }
@@ -1232,6 +1378,7 @@ int lbg_params_derive_folding_challenges(const lbg_params* p, lbg_transcript* t,
                                          lbg_challenge* out) {
   if (!p || !t || !u || !out) return fail(LBG_ERR_INVALID, "null argument");
   int rc = lbg_params_check(p);
+  if (!rc) rc = refuse_recursive(p->opening);
   if (rc) return rc;
   derive_folding_challenges(shape_of_params(p, nullptr), t->t, u, (Challenge*)out);
   return LBG_OK;
@@ -1248,11 +1395,13 @@ size_t lbg_params_pack_dropped(const lbg_params* p, const uint16_t* top, const u
 int lbg_derive_evaluation_point(const lbg_pp* pp, lbg_transcript* t, const int16_t* matrix, const uint16_t* top,
                                 const uint16_t* digits, uint64_t* p0_out, uint64_t* p1_out) {
   if (!pp || !t || !p0_out || !p1_out) return fail(LBG_ERR_INVALID, "null argument");
+  if (int rc = refuse_recursive(pp->params.opening)) return rc;
   return derive_point(shape_of(pp), t, matrix, top, digits, p0_out, p1_out);
 }
 
 int lbg_derive_folding_challenges(const lbg_pp* pp, lbg_transcript* t, const uint64_t* u, lbg_challenge* out) {
   if (!pp || !t || !u || !out) return fail(LBG_ERR_INVALID, "null argument");
+  if (int rc = refuse_recursive(pp->params.opening)) return rc;
   derive_folding_challenges(shape_of(pp), t->t, u, (Challenge*)out);
   return LBG_OK;
 }

@@ -72,6 +72,7 @@ struct lbg_batch {
   uint32_t* d_vhat = nullptr;     // [count][wdim][162]
   int16_t* d_v = nullptr;         // [count][len_ring][648]
   bool graphs = false;
+  int sm_cap = 0;                 // CTAs of the persistent commit and fold launches (0: one per SM)
   cudaGraphExec_t g_commit = nullptr, g_fold = nullptr, g_round = nullptr;
   uint64_t launches = 0;
   // the round on the device: per-instance transcripts, planned once per layout and domain
@@ -112,7 +113,14 @@ static void free_graphs(lbg_batch* b) {
 }
 
 // The device work of each stage, enqueued on the batch's stream (also what the graphs capture).
+// The batch's cap on the persistent kernels' CTAs, for the launches enqueued in its scope.
+struct CapScope {
+  explicit CapScope(int ctas) { set_persistent_cap(ctas); }
+  ~CapScope() { set_persistent_cap(0); }
+};
+
 static cudaError_t enqueue_commit(lbg_batch* b) {
+  CapScope cap(b->sm_cap);
   const lbg_pp* pp = b->pp;
   int L = pp->limbs, cols = (int)b->total_cols;
   cudaError_t e = cudaSuccess;
@@ -143,6 +151,7 @@ static cudaError_t enqueue_commit(lbg_batch* b) {
 }
 
 static cudaError_t enqueue_fold(lbg_batch* b) {
+  CapScope cap(b->sm_cap);
   const lbg_pp* pp = b->pp;
   cudaError_t e = launch_challenge_slots(pp->pidx[0], b->d_ch, (int)b->total_cols, pp->d_prime[0], b->d_chat, b->stream);
   if (e == cudaSuccess && b->keep)
@@ -404,11 +413,44 @@ size_t lbg_batch_arena_bytes(const lbg_pp* pp, size_t max_cols, size_t max_insta
          I * pp->len_ring * N648 * 2 + 2 * I * sizeof(HasherState) + I * sizeof(RoundInst) + I * 32;
 }
 
+// The batch's stream at the device's greatest (high != 0) or default priority: when both are
+// waiting for SMs, the CTAs of a high-priority stream's launches are scheduled first. The stream is
+// replaced (after the old one drains) and the graphs captured on it are dropped, so their next
+// capture takes the new priority.
+int lbg_batch_set_priority(lbg_batch* b, int high) {
+  if (!b) return fail(LBG_ERR_INVALID, "null argument");
+  LBG_BCU(cudaSetDevice(b->pp->device));
+  int least = 0, greatest = 0;
+  LBG_BCU(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  cudaStream_t st = nullptr;
+  LBG_BCU(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, high ? greatest : 0));
+  cudaStreamSynchronize(b->stream);
+  free_graphs(b);
+  cudaStreamDestroy(b->stream);
+  b->stream = st;
+  return LBG_OK;
+}
+
+// At most `ctas` CTAs (one per SM) for the batch's persistent commit and fold launches (0: every SM),
+// so that another slot's launches find SMs free while this batch runs. Drops captured graphs.
+int lbg_batch_set_sm_limit(lbg_batch* b, int ctas) {
+  if (!b || ctas < 0) return fail(LBG_ERR_INVALID, "null argument or negative limit");
+  if (b->sm_cap != ctas) {
+    LBG_BCU(cudaSetDevice(b->pp->device));
+    cudaStreamSynchronize(b->stream);
+    free_graphs(b);
+    b->sm_cap = ctas;
+  }
+  return LBG_OK;
+}
+
 // An arena of `max_cols` columns and `max_instances` instances: the device buffers are sized once;
 // lbg_batch_assign lays out a set of instances inside it without allocating.
 int lbg_batch_new_capacity(const lbg_pp* pp, size_t max_cols, size_t max_instances, lbg_batch** out) {
   if (!pp || !out || max_cols == 0 || max_instances == 0) return fail(LBG_ERR_INVALID, "null argument or empty batch");
   *out = nullptr;
+  if (pp->params.opening == LBG_OPENING_RECURSIVE)
+    return fail(LBG_ERR_UNSUPPORTED, "batched rounds cover the Clear and bit-dropped openings");
   if (max_instances > 65536) return fail(LBG_ERR_INVALID, "at most 65536 instances");
   if (max_cols > ((size_t)1 << 30) / pp->wdim) return fail(LBG_ERR_PARAMS, "batch too large");
   lbg_batch* b = new lbg_batch();

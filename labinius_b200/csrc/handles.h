@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/labinius_gpu.h"
+#include "copy_pool.h"
 #include "launch.h"
 #include "prime_structs.h"
 #include "transcript.h"
@@ -43,6 +44,8 @@ struct lbg_pp {
   uint8_t* d_sw = nullptr;     // the switch prover's workspace (lbg_switch_prove), allocated on first use
   uint8_t* d_wire = nullptr;   // lbg_row_evaluate_packed's bytes (grown on use)
   size_t wire_cap = 0;
+  int16_t* d_lift = nullptr;   // lbg_left_expansion's vector (grown on use)
+  size_t lift_cap = 0;
 };
 
 // Frees the switch prover's workspace of pp (switch.cu).
@@ -67,6 +70,13 @@ struct lbg_prover {
   std::vector<cudaStream_t> limb_streams;
   std::vector<cudaEvent_t> limb_done;
   std::vector<int32_t*> limb_partial;
+  // lbg_commit_host from pageable host memory: the column groups pass through a ring of
+  // page-locked staging buffers, filled by a few host threads (created on first use)
+  static constexpr int STAGES = 3;
+  void* stage[STAGES] = {nullptr, nullptr, nullptr};
+  size_t stage_bytes = 0;
+  cudaEvent_t stage_copied[STAGES] = {nullptr, nullptr, nullptr};  // the device copy out of stage s
+  lbg::CopyPool* copy_pool = nullptr;
   int chunk = 0, nchunks = 0;
   int fold_cols_per_split = 0;
   int32_t* d_partial = nullptr;
@@ -77,6 +87,8 @@ struct lbg_prover {
   uint8_t* d_wire = nullptr;  // lbg_opening_pack_commitment's bytes (grown on use)
   size_t wire_cap = 0;
   uint16_t* d_res = nullptr;  // [limbs][cols*648]
+  int16_t* d_rec = nullptr;   // lbg_opening_residues' vectors (grown on use)
+  size_t rec_cap = 0;
   std::mutex mu;
   std::vector<struct OpeningBufs*> spare;
   // the fold reads the commit's kept transform (the reference's AuxData, crates/pcs/src/key.rs:275-326)

@@ -315,7 +315,19 @@ __global__ void k_commit_finish(const int32_t* __restrict__ partial, int nchunks
 // A buffer g % 2 is free for step g once step g - 2's multiply is done, which every compute warp
 // saw before reading that step's accumulator; accumulator g % 2 is free once every compute warp
 // has passed named barrier 1 of step g. Rows of columns past the last are zero.
-constexpr int TCC_CTHREADS = 384;                      // compute warps 0-11
+// CW compute warps (12: three leaf ranges of 56 leaves, 14 a thread, 128 registers; 16: four ranges
+// of 48, 40, 40, 40 leaves, at most 12 a thread, 120 registers) and the producer warp.
+template <int CW>
+struct TccShape {
+  static constexpr int CTHREADS = CW * 32;
+  static constexpr int THREADS = CTHREADS + 32;
+  static constexpr int LPT = CW == 12 ? 14 : 12;  // leaves per compute thread (at most)
+  static_assert(CW == 12 || CW == 16, "twelve or sixteen compute warps");
+  // first leaf of leaf range `part`, and the number of eight-leaf chunks in it
+  __device__ static int base(int part) { return CW == 12 ? 56 * part : (part == 0 ? 0 : 8 + 40 * part); }
+  __device__ static int chunks(int part) { return CW == 12 ? 7 : (part == 0 ? 6 : 5); }
+};
+constexpr int TCC_CTHREADS = 384;                      // the default: compute warps 0-11
 constexpr int TCC_THREADS = TCC_CTHREADS + 32;         // and the producer warp (13 warps: 128 registers)
 constexpr int TCC_CT = 32;                             // columns per item
 constexpr int TCC_RT = 1;                              // ring elements per step
@@ -336,8 +348,8 @@ static_assert(TCC_OFF_A % TC_ATOM == 0 && TCC_A_BYTES % TC_ATOM == 0 && TCC_OFF_
                   TCC_OFF_WT % 16 == 0 && TCC_OFF_BAR % 8 == 0 && TCC_OFF_CUR % 16 == 0,
               "alignment");
 static_assert(TCC_SMEM <= 232448, "shared memory per CTA");
-static_assert(TCC_CTHREADS == 3 * 128 && 3 * 56 >= N162,
-              "twelve warps: four quadrants x three leaf ranges; three threads per row's words");
+static_assert(TCC_CTHREADS == 3 * 128 && 3 * 56 >= N162 && 48 + 3 * 40 >= N162,
+              "four quadrants x three or four leaf ranges; the first 384 compute threads copy the rows' words");
 
 // A device-wide flag set by a tensor-core kernel whose bounded wait ran out (never in practice:
 // what it waits for takes microseconds). The host reads and clears it.
@@ -430,8 +442,8 @@ struct TcCursor {
   __device__ bool valid(const TcItems& I) const { return it < I.total; }
 };
 
-template <int PI>
-__global__ void __launch_bounds__(TCC_THREADS, 1)
+template <int PI, int CW>
+__global__ void __maxnreg__(CW == 12 ? 128 : 112)
     k_commit_tc(const uint64_t* __restrict__ W, size_t wdim, const int4* __restrict__ Ahat,
                 const uint8_t* __restrict__ tcb, int cols, int len_ring, int chunk, int nchunks,
                 int32_t* __restrict__ partial /* [nchunks][cols][162][4] */) {
@@ -451,6 +463,8 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
   // step g's cursor in slot g % 4: the producer writes step g + 1's before named barrier 1 of step
   // g; the compute warps read step g + 1's (word copies) and step g - 1's (item end) after it
   TcCursor* curs = (TcCursor*)(smem + TCC_OFF_CUR);
+  using Sh = TccShape<CW>;
+  constexpr int CTHREADS = Sh::CTHREADS, THREADS = Sh::THREADS, LPT = Sh::LPT;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int col_tiles = (cols + TCC_CT - 1) / TCC_CT;
   const TcItems items{(int)blockIdx.x, (int)gridDim.x, col_tiles * nchunks, col_tiles, chunk, len_ring};
@@ -459,10 +473,10 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
 
   if (tid == 0) {
     for (int b = 0; b < 2; b++) {
-      tc::mbar_init(&wfull[b], TCC_CTHREADS);
+      tc::mbar_init(&wfull[b], CTHREADS);
       tc::mbar_init(&mma[b], 1);
       tc::mbar_init(&kfull[b], 1);
-      tc::mbar_init(&kempty[b], TCC_CTHREADS / 32);
+      tc::mbar_init(&kempty[b], CTHREADS / 32);
     }
     tc::mbar_init(bfull, 1);
     *abort = 0;
@@ -478,7 +492,7 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
   tc::fence_after_sync();
   const uint32_t tmem = *tslot;
 
-  if (warp == TCC_CTHREADS / 32) {
+  if (warp == CTHREADS / 32) {
     // ---------------- producer (one lane) ----------------
     const uint32_t sA_u = tc::smem_u32(sA), sB_u = tc::smem_u32(sB);
     TcCursor cur = curs[0];
@@ -499,7 +513,7 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
         curs[(g + 1) & 3] = nxt;
       }
       __syncwarp();
-      tc::named_sync(1, TCC_THREADS);  // step g's A operand is built
+      tc::named_sync(1, THREADS);  // step g's A operand is built
       if (lane == 0) {
         tc::fence_after_sync();
         if (g == 0) tc_wait(bfull, 0, abort);
@@ -522,21 +536,22 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
   } else if (S > 0) {
     // ---------------- compute ----------------
     const int quad = warp & 3, part = warp >> 2;
-    const int jq = 8 * quad + (lane >> 2);      // the thread's column in the tile
-    const int v0 = 56 * part + 2 * (lane & 3);  // its leaves: v0 + 8 c + l, c < 7, l < 2
+    const int jq = 8 * quad + (lane >> 2);               // the thread's column in the tile
+    const int v0 = Sh::base(part) + 2 * (lane & 3);      // its leaves: v0 + 8 c + l, c < chunks, l < 2
+    const int nlv = 2 * Sh::chunks(part);                // its leaf slots
     // the word this thread copies for every step: word wx of row wr (column wj, position wk)
     const int wr = tid / 3, wx = tid - 3 * (tid / 3);
     const int wj = 8 * (wr >> 5) + (wr & 7), wk = (wr >> 3) & 3;
     auto copy_words = [&](const TcCursor& c, int b) {
-      if (c.j0 + wj < cols)
+      if (tid < 384 && c.j0 + wj < cols)
         tc::cp_async8(wtile + (b * 128 + wr) * 3 + wx, W + ((size_t)(c.j0 + wj) * wdim + (size_t)4 * c.i + wk) * 3 + wx);
       tc::cp_async_arrive(&wfull[b]);
     };
     const int r = tid & 127;
     const int rj = 8 * (r >> 5) + (r & 7);  // the built row's column
-    int32_t acc[TCC_LPT][4];
+    int32_t acc[LPT][4];
 #pragma unroll
-    for (int u = 0; u < TCC_LPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
+    for (int u = 0; u < LPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
     constexpr int RED = CommitRed<PI>::value;
     int since = 0;
     // one leaf's module product: positions w0..w3 of the column's ring element, key (lo, hi)
@@ -554,11 +569,11 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
       if (g < S) {
         const int b = g & 1;
         tc_wait(&wfull[b], (g >> 1) & 1, abort);  // step g's words
-        tc_build_row_inline<12 * 128 / TCC_CTHREADS>(sA + b * TCC_A_BYTES, tid, TCC_CTHREADS,
+        tc_build_row_inline<12 * 128 / CTHREADS>(sA + b * TCC_A_BYTES, tid, CTHREADS,
                                                    wtile + (b * 128 + r) * 3, curs[g & 3].j0 + rj < cols);
         tc::fence_async_shared();
         tc::fence_before_sync();
-        tc::named_sync(1, TCC_THREADS);  // meets the producer: lockstep, even when a wait timed out
+        tc::named_sync(1, THREADS);  // meets the producer: lockstep, even when a wait timed out
         if (g + 1 < S) copy_words(curs[(g + 1) & 3], (g + 1) & 1);
       }
       if (g >= 1) {
@@ -569,12 +584,11 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
         tc_wait(&kfull[b], par, abort);  // step g - 1's key tile
         tc::fence_after_sync();
         // lanes 32 quad .. + 15 hold positions 0-1 of the quadrant's 8 columns, + 16 .. 31 positions 2-3
-        const uint32_t ta = tmem + (uint32_t)b * 256u + ((uint32_t)(32 * quad) << 16) + 56 * part;
+        const uint32_t ta = tmem + (uint32_t)b * 256u + ((uint32_t)(32 * quad) << 16) + Sh::base(part);
         const uint32_t tb = ta + (16u << 16);
         const int4* kt = atile + b * (N162 * 2) + 2 * v0;  // the key at the thread's first leaf
-#pragma unroll
-        for (int cp = 0; cp < 3; cp++) {
-          // chunks 2 cp and 2 cp + 1 (16 columns): x[0..7] positions 0-1, x[8..15] positions 2-3
+        // chunk pairs (16 leaves, all below 162) by x2 loads: x[0..7] positions 0-1, x[8..15] positions 2-3
+        auto pair = [&](int cp) {
           uint32_t x[16];
           tc::tmem_ld16x256_x2_nowait(ta + 16 * cp, x);
           tc::tmem_ld16x256_x2_nowait(tb + 16 * cp, x + 8);
@@ -585,16 +599,29 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
             for (int l = 0; l < 2; l++)
               product(acc[2 * (2 * cp + h) + l], x[4 * h + l], x[4 * h + 2 + l], x[8 + 4 * h + l],
                       x[8 + 4 * h + 2 + l], kt + 2 * (8 * (2 * cp + h) + l));
-        }
-        {
-          // chunk 6; the last leaf range's pads (leaves 162 - 167) use leaf 161's key, unused
+        };
+        // a last single chunk by x1 loads; the last leaf range's pads (leaves 162 - 167) use leaf
+        // 161's key, unused
+        auto single = [&](int c) {
           uint32_t x[8];
-          tc::tmem_ld16x256_x1_nowait(ta + 48, x);
-          tc::tmem_ld16x256_x1_nowait(tb + 48, x + 4);
+          tc::tmem_ld16x256_x1_nowait(ta + 8 * c, x);
+          tc::tmem_ld16x256_x1_nowait(tb + 8 * c, x + 4);
           tc::tmem_wait_ld(x);
 #pragma unroll
           for (int l = 0; l < 2; l++)
-            product(acc[12 + l], x[l], x[2 + l], x[4 + l], x[6 + l], kt + 2 * (min(v0 + 48 + l, N162 - 1) - v0));
+            product(acc[2 * c + l], x[l], x[2 + l], x[4 + l], x[6 + l], kt + 2 * (min(v0 + 8 * c + l, N162 - 1) - v0));
+        };
+        if (CW == 12) {
+#pragma unroll
+          for (int cp = 0; cp < 3; cp++) pair(cp);
+          single(6);
+        } else {
+          pair(0);
+          pair(1);
+          if (part == 0)
+            pair(2);
+          else
+            single(4);
         }
         tc::fence_before_sync();
         tc::fence_async_shared();  // this warp's reads of the key tile precede the next bulk copy into it
@@ -603,7 +630,7 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
         if (++since >= RED) {
           since = 0;
 #pragma unroll
-          for (int u = 0; u < TCC_LPT; u++)
+          for (int u = 0; u < LPT; u++)
 #pragma unroll
             for (int c = 0; c < 4; c++) acc[u][c] = red_signed<PI>(acc[u][c]);
         }
@@ -613,9 +640,9 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
           if (j < cols) {
             int4* dst = (int4*)partial + ((size_t)prev.ci * cols + j) * N162;
 #pragma unroll
-            for (int u = 0; u < TCC_LPT; u++) {
+            for (int u = 0; u < LPT; u++) {
               const int v = v0 + 8 * (u >> 1) + (u & 1);
-              if (v < N162) {
+              if (u < nlv && v < N162) {
                 int4 o;
                 o.x = (int)red_signed_full<PI>(acc[u][0]);
                 o.y = (int)red_signed_full<PI>(acc[u][1]);
@@ -626,7 +653,7 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
             }
           }
 #pragma unroll
-          for (int u = 0; u < TCC_LPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
+          for (int u = 0; u < LPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0;
           since = 0;
         }
       }
@@ -1203,6 +1230,48 @@ __global__ void __launch_bounds__(216) k_column_residues(const int16_t* __restri
   __syncthreads();
   intt162_group<PI>(xs[d], t, *D);
   for (int m = t; m < N162; m += 54) res[(size_t)j * N648 + 4 * m + d] = (uint16_t)xs[d][m];
+}
+
+// The recursive opening's residues (crates/pcs/src/recursion/limbs.rs:379-398, drain_batch :311-325):
+// for one limb, vector l (component l) holds each column's coefficients 4m + l, centred, times
+// (-1)^m, cut into three chunks of 54 (chunk b of column j is polynomial b * cols + j, positions
+// 0..53; the rest of the 64 positions and the padding polynomials are zero). One thread per output
+// coefficient; `res` is the limb's coefficients in [0, q) as k_column_residues leaves them.
+__global__ void k_recursion_residues(const uint16_t* __restrict__ res, int cols, size_t polys, int32_t q,
+                                     int16_t* __restrict__ out /* [4][polys][64] */) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 4 * polys * 64) return;
+  const int pos = (int)(i & 63);
+  const size_t poly = (i >> 6) % polys;
+  const int l = (int)((i >> 6) / polys);
+  int32_t v = 0;
+  if (pos < 54 && poly < (size_t)3 * cols) {
+    const int b = (int)(poly / cols), j = (int)(poly - (size_t)b * cols);
+    const int m = 54 * b + pos;
+    int32_t c = res[(size_t)j * N648 + 4 * m + l];
+    if (c > (q - 1) / 2) c -= q;
+    v = (m & 1) ? -c : c;
+  }
+  out[i] = (int16_t)v;
+}
+
+// Prover::commit_left_expansion's vector u (crates/pcs/src/scheme/prover.rs:95-115): chunk b of the
+// lift of row value j (its bits 54 b .. 54 b + 53 as 0/1 coefficients, crates/pcs/src/recursion/
+// binary.rs:49-51, chunk.rs:76-86) at polynomial b * cols + j; the rest zero. One thread per output
+// coefficient.
+__global__ void k_left_expansion(const uint64_t* __restrict__ u /* [cols][3] */, int cols, size_t rank,
+                                 int16_t* __restrict__ out /* [rank][64] */) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rank * 64) return;
+  const int pos = (int)(i & 63);
+  const size_t poly = i >> 6;
+  int16_t v = 0;
+  if (pos < 54 && poly < (size_t)3 * cols) {
+    const int b = (int)(poly / cols), j = (int)(poly - (size_t)b * cols);
+    const int bit = 54 * b + pos;
+    v = (int16_t)((u[(size_t)j * 3 + (bit >> 6)] >> (bit & 63)) & 1);
+  }
+  out[i] = v;
 }
 
 __global__ void k_garner(const uint16_t* __restrict__ res, size_t count, int limbs, GarnerConsts g,
@@ -2154,6 +2223,16 @@ bool commit_tc_enabled() {
   return on;
 }
 
+// Compute warps of the tensor-core commit: 12 unless LBG_COMMIT_WARPS=16 (both exact; the switch is
+// for timing them against each other).
+static int commit_tc_warps() {
+  static const int w = [] {
+    const char* e = getenv("LBG_COMMIT_WARPS");
+    return (e && std::string(e) == "16") ? 16 : 12;
+  }();
+  return w;
+}
+
 int commit_blocks_per_sm(int pi) {
   int n = 0;
   const bool tcm = commit_tc_enabled();
@@ -2163,8 +2242,8 @@ int commit_blocks_per_sm(int pi) {
 #define LBG_OCC(I)                                                                                        \
   case I:                                                                                                 \
     if (tcm) {                                                                                            \
-      cudaFuncSetAttribute(k_commit_tc<I>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_commit_tc<I>, TCC_THREADS, smem);           \
+      cudaFuncSetAttribute(k_commit_tc<I, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_commit_tc<I, 12>, TCC_THREADS, smem);       \
     } else {                                                                                              \
       cudaFuncSetAttribute(k_commit<I, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_commit<I, false>, 256, smem);               \
@@ -2195,6 +2274,16 @@ static int sm_count() {
   return nsm;
 }
 
+// The most CTAs (one per SM) the persistent tensor-core kernels launched from this host thread
+// take; 0: every SM. A server gives its large requests' slot fewer than all SMs so that a slot of
+// small requests finds SMs free instead of waiting for a whole persistent launch to end.
+static thread_local int t_persistent_cap = 0;
+void set_persistent_cap(int ctas) { t_persistent_cap = ctas > 0 ? ctas : 0; }
+static int persistent_ctas() {
+  const int n = sm_count();
+  return t_persistent_cap > 0 && t_persistent_cap < n ? t_persistent_cap : n;
+}
+
 cudaError_t launch_commit(int pi, const uint64_t* W, size_t wdim, const int4* Ahat, const DevPrime* D, int cols,
                           int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st, uint16_t* keep,
                           const uint8_t* tcb) {
@@ -2208,11 +2297,17 @@ cudaError_t launch_commit(int pi, const uint64_t* W, size_t wdim, const int4* Ah
   } else if (tcb && commit_tc_enabled()) {
     // persistent: one CTA per SM (at most one per work item) over the column tiles x chunks
     const long items = (long)((cols + TCC_CT - 1) / TCC_CT) * nchunks;
-    dim3 grid((unsigned)std::max<long>(1, std::min<long>(items, sm_count())));
+    dim3 grid((unsigned)std::max<long>(1, std::min<long>(items, persistent_ctas())));
     LBG_DISPATCH(pi, ({
-                   cudaFuncSetAttribute(k_commit_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, TCC_SMEM);
-                   k_commit_tc<P><<<grid, TCC_THREADS, TCC_SMEM, st>>>(W, wdim, Ahat, tcb, cols, len_ring, chunk,
-                                                                       nchunks, partial);
+                   if (commit_tc_warps() == 16) {
+                     cudaFuncSetAttribute(k_commit_tc<P, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, TCC_SMEM);
+                     k_commit_tc<P, 16><<<grid, TccShape<16>::THREADS, TCC_SMEM, st>>>(W, wdim, Ahat, tcb, cols,
+                                                                                      len_ring, chunk, nchunks, partial);
+                   } else {
+                     cudaFuncSetAttribute(k_commit_tc<P, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize, TCC_SMEM);
+                     k_commit_tc<P, 12><<<grid, TCC_THREADS, TCC_SMEM, st>>>(W, wdim, Ahat, tcb, cols, len_ring,
+                                                                             chunk, nchunks, partial);
+                   }
                  }));
   } else {
     dim3 grid((cols + CT - 1) / CT, nchunks);
@@ -2279,7 +2374,7 @@ cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int co
     int splits = (cols + cols_per_split - 1) / cols_per_split;
     if (splits < 1 || splits > 65535) return cudaErrorInvalidValue;
     const long items = (long)((wdim + TCF_ROWS - 1) / TCF_ROWS) * splits;
-    dim3 grid((unsigned)std::max<long>(1, std::min<long>(items, sm_count())));  // persistent, one CTA per SM
+    dim3 grid((unsigned)std::max<long>(1, std::min<long>(items, persistent_ctas())));  // persistent, one CTA per SM
     size_t positions = wdim * (size_t)instances;
     cudaError_t e = cudaMemsetAsync(vhat, 0, positions * N162 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
@@ -2352,6 +2447,21 @@ cudaError_t launch_column_residues(int pi, const int16_t* C, int cols, int limb,
                                    uint16_t* res, cudaStream_t st) {
   if (cols <= 0) return cudaSuccess;
   LBG_DISPATCH(pi, (k_column_residues<P><<<cols, 216, 0, st>>>(C, cols, limb, limbs, D, res)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_recursion_residues(const uint16_t* res, int cols, size_t polys, uint32_t q, int16_t* out,
+                                      cudaStream_t st) {
+  const size_t n = 4 * polys * 64;
+  if (n == 0) return cudaSuccess;
+  k_recursion_residues<<<blocks_for(n, 256), 256, 0, st>>>(res, cols, polys, (int32_t)q, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_left_expansion(const uint64_t* u, int cols, size_t rank, int16_t* out, cudaStream_t st) {
+  const size_t n = rank * 64;
+  if (n == 0) return cudaSuccess;
+  k_left_expansion<<<blocks_for(n, 256), 256, 0, st>>>(u, cols, rank, out);
   return cudaGetLastError();
 }
 

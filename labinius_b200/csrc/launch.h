@@ -47,6 +47,9 @@ cudaError_t launch_commit(int pi, const uint64_t* W, size_t wdim, const int4* Ah
                           int len_ring, int chunk, int nchunks, int32_t* partial, cudaStream_t st,
                           uint16_t* keep = nullptr, const uint8_t* tcb = nullptr);
 bool commit_tc_enabled();
+// At most `ctas` CTAs for the persistent tensor-core kernels launched from the calling host thread
+// (0: one per SM).
+void set_persistent_cap(int ctas);
 // 1 (and cleared) when a tensor-core kernel's bounded wait ran out since the last call, else 0;
 // -1 when the flag could not be read.
 int tc_timeout_take();
@@ -79,6 +82,11 @@ cudaError_t launch_fold_commitment(int pi, const int16_t* C, int cols, int limb,
                                    const DevPrime* D, int16_t* out, cudaStream_t st);
 cudaError_t launch_column_residues(int pi, const int16_t* C, int cols, int limb, int limbs, const DevPrime* D,
                                    uint16_t* res, cudaStream_t st);
+// The recursive opening's residue vectors of one limb from its coefficients (k_column_residues), and
+// the left expansion's vector from the row values.
+cudaError_t launch_recursion_residues(const uint16_t* res, int cols, size_t polys, uint32_t q, int16_t* out,
+                                      cudaStream_t st);
+cudaError_t launch_left_expansion(const uint64_t* u, int cols, size_t rank, int16_t* out, cudaStream_t st);
 cudaError_t launch_garner(const uint16_t* res, size_t count, int limbs, const GarnerConsts& g, uint16_t* top,
                           uint16_t* digits, cudaStream_t st);
 cudaError_t launch_eq_table(const uint64_t* p, int n, size_t count, uint64_t* eq, cudaStream_t st,

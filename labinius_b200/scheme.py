@@ -381,6 +381,12 @@ class Commitment:
         return b"\x02" + head + out.tobytes()
 
 
+def recursion_polys(columns: int) -> int:
+    """Polynomials of a residue or left-expansion vector: three chunks per column, padded to a
+    multiple of 32 (crates/pcs/src/recursion/limbs.rs:388, recursion/mod.rs PAD)."""
+    return -(-3 * columns // 32) * 32
+
+
 class CommitmentOpening:
     """The device handle a commitment leaves for the fold (crates/pcs/src/scheme/commitment.rs:120-139)."""
 
@@ -393,6 +399,19 @@ class CommitmentOpening:
         if h is None:
             raise ValueError("this opening was already consumed")
         return h
+
+    def residues(self, polys: Optional[int] = None) -> np.ndarray:
+        """recursion::limbs::residues of the commitment (crates/pcs/src/recursion/limbs.rs:379-398),
+        computed on the device: int16 [limbs * 4][polys][64], polys = 3 x columns rounded up to a
+        multiple of 32 by default. With the recursion on, the host's LaBRADOR bridge commits these
+        as T_y."""
+        if self._h is None:
+            raise ValueError("this opening was already consumed")
+        pr = self.prover.params
+        polys = recursion_polys(pr.columns()) if polys is None else int(polys)
+        out = np.zeros((len(pr.primes()) * 4, polys, 64), np.int16)
+        check(lib().lbg_opening_residues(self._h, polys, ptr(out)))
+        return out
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -432,10 +451,24 @@ class Prover:
             c = Commitment(pr.primes(), r, matrix=m, params=pr)
         return c, CommitmentOpening(self, op)
 
+    def commit_left_expansion_vector(self, row: "RowEvaluation", rank: Optional[int] = None) -> np.ndarray:
+        """Prover::commit_left_expansion's vector u (crates/pcs/src/scheme/prover.rs:95-115), made on the
+        device: int16 [rank][64], chunk b of lift(u_j) at polynomial b x columns + j. rank is the
+        recursion setup's ranks[U] (default: 3 x columns rounded up to a multiple of 32);
+        T_u = key_u.commit_blocks(u) is LaBRADOR's, on the host."""
+        pr = self.params
+        r = pr.columns()
+        rank = recursion_polys(r) if rank is None else int(rank)
+        vals = np.ascontiguousarray(row.values, dtype=np.uint64).reshape(-1, 3)
+        out = np.zeros((rank, 64), np.int16)
+        check(lib().lbg_left_expansion(self.pp._h, ptr(vals), len(vals), rank, ptr(out)))
+        return out
+
     def commit_elements(self, elements):
         """Witness::from_elements then Prover::commit in one call, the upload of the elements
-        (uint64 [n][3]; page-locked for the copies to overlap) pipelined against the commit.
-        Returns (witness, commitment, opening)."""
+        (uint64 [n][3]) pipelined against the commit: page-locked memory is copied directly,
+        pageable memory through the prover's page-locked staging ring. Returns (witness,
+        commitment, opening)."""
         pr = self.params
         e = np.ascontiguousarray(elements, dtype=np.uint64).reshape(-1, 3)
         if len(e) != pr.witness_len():

@@ -16,7 +16,10 @@ columns one batch runs, a latency bound) caps it further. Admission is by arena 
 HBM each slot reserved, and by size class: with `small_log_len` set, requests of at most
 2^small_log_len columns are small; slot 0 runs small requests only, the other slots run the large
 ones and take small ones when no large request waits, so a small request never queues behind a
-batch of large ones. Whenever a slot is free it admits, in arrival order within its class, every
+batch of large ones; the small slot's stream runs at the device's greatest priority, so its launches
+take SMs ahead of a large batch's once those free up, and with `large_sm_limit` the large slots'
+persistent commit and fold launches take at most that many SMs, so the small slot never waits for
+one of them to end. Whenever a slot is free it admits, in arrival order within its class, every
 queued request that fits, lays them out in the arena and runs their rounds together:
 each device stage is one launch over all of them, and the transcripts (absorbs, evaluation point,
 challenge sampling) run on the device too (lbg_batch_round), so a batch is one pass on the
@@ -84,7 +87,7 @@ class Server:
     def __init__(self, pp: PublicParameters, capacity_columns: Optional[int] = None, max_requests: int = 256,
                  slots: int = 2, host_threads: int = 16, domain: bytes = b"labinius/reference",
                  keep_results: bool = True, transcript: str = "device", hbm_fraction: float = 0.5,
-                 small_log_len: Optional[int] = None):
+                 small_log_len: Optional[int] = None, large_sm_limit: int = 0):
         self.pp = pp
         self.memory_columns = arena_columns(pp, hbm_fraction, slots, max_requests)
         self.capacity = self.memory_columns if capacity_columns is None else min(capacity_columns, self.memory_columns)
@@ -94,6 +97,12 @@ class Server:
         self.transcript = transcript
         self.small_log_len = small_log_len if slots >= 2 else None
         self.slots = [Batch(pp, capacity=(self.capacity, max_requests)) for _ in range(slots)]
+        if self.small_log_len is not None:
+            # the small requests' slot is scheduled ahead of the large ones' when both wait for SMs,
+            # and the large ones' persistent launches leave SMs free for it (large_sm_limit CTAs)
+            self.slots[0].set_priority(True)
+            for b in self.slots[1:]:
+                b.set_sm_limit(large_sm_limit)
         self.pool = concurrent.futures.ThreadPoolExecutor(host_threads)
         self.small = collections.deque()  # every request when no size classes are set
         self.large = collections.deque()

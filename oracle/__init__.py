@@ -62,6 +62,8 @@ def _setup(L):
         "orc_fold_commitment": (None, [vp, vp, vp, vp]),
         "orc_slot_table": (None, [u32, vp]),
         "orc_drop_bits": (None, [vp, vp, vp, vp]),
+        "orc_recursion_residues": (None, [vp, vp, sz, vp]),
+        "orc_left_expansion": (None, [vp, sz, sz, vp]),
         "orc_pack_dropped": (sz, [vp, vp, vp, vp, sz]),
         "orc_transcript_new": (vp, [vp, sz]),
         "orc_transcript_free": (None, [vp]),
@@ -299,6 +301,31 @@ def drop_bits(params: Params, C):
     pa = params.arr()
     lib().orc_drop_bits(_p(pa), _p(C), _p(top), _p(digits))
     return top, digits[: params.limbs - 1]
+
+
+def recursion_polys(columns: int) -> int:
+    """Three chunks per column, padded to a multiple of 32 (crates/pcs/src/recursion/limbs.rs:388)."""
+    return -(-3 * columns // 32) * 32
+
+
+def recursion_residues(params: Params, C, polys=None):
+    """recursion::limbs::residues (crates/pcs/src/recursion/limbs.rs:379-398): int16
+    [limbs * 4][polys][64]."""
+    C = np.ascontiguousarray(C, dtype=np.int16)
+    polys = recursion_polys(params.columns) if polys is None else int(polys)
+    out = np.zeros((params.limbs * 4, polys, 64), np.int16)
+    lib().orc_recursion_residues(_p(params.arr()), _p(C), polys, _p(out))
+    return out
+
+
+def left_expansion(u, rank=None):
+    """Prover::commit_left_expansion's vector u (crates/pcs/src/scheme/prover.rs:95-115): int16
+    [rank][64]."""
+    u = np.ascontiguousarray(u, dtype=np.uint64).reshape(-1, 3)
+    rank = recursion_polys(len(u)) if rank is None else int(rank)
+    out = np.zeros((rank, 64), np.int16)
+    lib().orc_left_expansion(_p(u), len(u), rank, _p(out))
+    return out
 
 
 def pack_dropped(params: Params, top, digits):

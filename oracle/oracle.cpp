@@ -856,6 +856,47 @@ static void drop_bits(const Params& pr, const int16_t* C, uint16_t* top, uint16_
   }
 }
 
+// crates/pcs/src/recursion/limbs.rs:379-398 (residues), :267-309 (columns_split: recombination, inverse
+// transform, fully reduced and centred) and :311-325 (drain_batch: vector l of a limb holds
+// coefficient 4m + l times (-1)^m, chunk b = coefficients 54b..54b+53 of column j at polynomial
+// b r + j); vectors padded with zero polynomials to `polys` (crates/pcs/src/recursion/mod.rs PAD).
+static void recursion_residues(const Params& pr, const int16_t* C, size_t polys, int16_t* out) {
+  size_t r = pr.columns();
+  int L = pr.limbs;
+  std::memset(out, 0, (size_t)L * 4 * polys * 64 * sizeof(int16_t));
+  for (int k = 0; k < L; k++) {
+    const Prime& P = prime(pr.primes[k]);
+    for (size_t j = 0; j < r; j++) {
+      int16_t comp[4][N162];
+      for (int row = 0; row < 4; row++)
+        for (int s = 0; s < N162; s++) comp[row][s] = C[((j * 4 + row) * L + k) * N162 + s];
+      u32 y[N], coef[N];
+      recombine(P, comp, y);
+      intt(P, y, coef);
+      for (int l = 0; l < 4; l++)
+        for (int b = 0; b < 3; b++)
+          for (int u = 0; u < 54; u++) {
+            int m = 54 * b + u;
+            i64 c = center((i64)coef[4 * m + l], (i64)P.q);
+            out[(((size_t)(4 * k + l)) * polys + (size_t)b * r + j) * 64 + u] = (int16_t)(m % 2 == 0 ? c : -c);
+          }
+    }
+  }
+}
+
+// crates/pcs/src/scheme/prover.rs:95-115 (commit_left_expansion's u), crates/pcs/src/recursion/
+// binary.rs:49-51 (lift: bit p of the F162 as coefficient p), chunk.rs:76-86 (chunk b: coefficients
+// 54b..54b+53 at positions 0..53).
+static void left_expansion(const uint64_t* u, size_t r, size_t rank, int16_t* out) {
+  std::memset(out, 0, rank * 64 * sizeof(int16_t));
+  for (int b = 0; b < 3; b++)
+    for (size_t j = 0; j < r; j++)
+      for (int t = 0; t < 54; t++) {
+        int p = 54 * b + t;
+        out[((size_t)b * r + j) * 64 + t] = (int16_t)((u[j * 3 + (p >> 6)] >> (p & 63)) & 1);
+      }
+}
+
 static u32 residue_bits(u32 q) { return 32 - __builtin_clz(q - 1); }
 static u32 top_bits(u32 q, u32 d) {
   u32 bound = ((q - 1) + (1u << (d - 1))) >> d;
@@ -1465,6 +1506,11 @@ size_t orc_pack_dropped(const uint32_t* params, const uint16_t* top, const uint1
   if (out && cap >= b.size()) std::memcpy(out, b.data(), b.size());
   return b.size();
 }
+
+void orc_recursion_residues(const uint32_t* params, const int16_t* C, size_t polys, int16_t* out) {
+  recursion_residues(make_params(params), C, polys, out);
+}
+void orc_left_expansion(const uint64_t* u, size_t r, size_t rank, int16_t* out) { left_expansion(u, r, rank, out); }
 
 // Transcript handles.
 void* orc_transcript_new(const uint8_t* domain, size_t len) { return new Transcript(domain, len); }

@@ -61,7 +61,10 @@ def test_params_check_mirrors_param_error(native):
     assert P(18, 7, [3889, 3889]) == native.LBG_ERR_PARAMS
     assert P(18, 7, [3889, 9721, 9721]) == native.LBG_ERR_PARAMS
     assert P(18, 7, [3889, 1234]) == native.LBG_ERR_PARAMS
-    assert P(18, 7, [3889], opening=2) == native.LBG_ERR_UNSUPPORTED
+    # Opening::Recursive validates like the other openings (crates/pcs/src/scheme/params.rs:171-203)
+    assert P(18, 8, [3889, 2917, 4861], opening=2) == 0
+    assert P(18, 19, [3889], opening=2) == native.LBG_ERR_PARAMS
+    assert P(18, 7, [3889], opening=3) == native.LBG_ERR_PARAMS
     assert P(18, 7, [3889, 2917, 4861], opening=1, bits=9) == 0
 
 

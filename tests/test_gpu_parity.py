@@ -281,3 +281,33 @@ def test_commits_from_host_memory_in_a_row_stay_apart():
         c1, op1 = prover.commit(L.Witness.from_elements(pp, e))
         assert np.array_equal(c.matrix, c1.matrix)
         assert np.array_equal(prover.fold(op, ch).elements, prover.fold(op1, ch).elements)
+
+
+def test_commit_from_pageable_and_page_locked_memory_agree():
+    """lbg_commit_host stages a pageable witness through its page-locked ring and copies a
+    page-locked one directly; both give Witness::from_elements + Prover::commit's commitment and
+    witness, three calls in a row alternating the two kinds of memory."""
+    import torch
+
+    import labinius_b200 as L
+    from rounds import MATRIX_SEED, product_params
+
+    params = product_params((20, 9, [3889, 2917, 4861], 0))
+    pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+    prover = L.Prover(pp)
+    rng = np.random.default_rng(5)
+    for locked in (True, False, True):
+        e = rng.integers(0, 2 ** 63, (params.witness_len(), 3), dtype=np.uint64)
+        e[:, 2] &= np.uint64((1 << 34) - 1)
+        if locked:
+            t = torch.empty((params.witness_len(), 3), dtype=torch.int64, pin_memory=True)
+            src = t.numpy().view(np.uint64)
+            src[:] = e
+        else:
+            src = e
+        w, c, op = prover.commit_elements(src)
+        c1, op1 = prover.commit(L.Witness.from_elements(pp, e))
+        assert np.array_equal(w.elements(), e)
+        assert np.array_equal(c.matrix, c1.matrix)
+        prover.recycle(op)
+        prover.recycle(op1)

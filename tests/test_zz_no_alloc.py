@@ -13,7 +13,8 @@ from rounds import MATRIX_SEED, WITNESS_SEED, product_params
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("shape", [(12, 4, [3889, 2917, 4861], 0), (13, 5, [2917, 9721], 0)], ids=["3889", "2917"])
+@pytest.mark.parametrize("shape", [(12, 4, [3889, 2917, 4861], 0), (13, 5, [2917, 9721], 0), (17, 10, [9721, 3889], 0)],
+                         ids=["3889", "2917", "1024-columns"])
 def test_fold_static_matches_fold(shape):
     import torch
 
@@ -36,13 +37,17 @@ def test_fold_static_matches_fold(shape):
     d_ch = torch.from_numpy(np.ascontiguousarray(ch.challenges).view(np.uint8).copy()).cuda()
     d_v = torch.empty((params.len_ring(), 648), dtype=torch.int16, device="cuda")
     base, wl, cl, r = params.primes()[0], params.witness_log_len, params.column_log_len, params.columns()
+    free_after = []
     for _ in range(2):
         d_v.fill_(0x5A5A)
         torch.cuda.synchronize()
         rc = lib().lbg_fold_static(base, wl, cl, d_w.data_ptr(), d_ch.data_ptr(), r, d_v.data_ptr(), None)
         assert rc == LBG_OK, lib().lbg_last_error()
         torch.cuda.synchronize()
+        free_after.append(torch.cuda.mem_get_info()[0])
         assert np.array_equal(d_v.cpu().numpy(), want)
+    # the second call took no device memory (the first may have loaded the module's static arrays)
+    assert free_after[1] == free_after[0]
 
     # beyond the static maximum: rejected with a clear message, nothing launched
     rc = lib().lbg_fold_static(base, 20, 11, d_w.data_ptr(), d_ch.data_ptr(), 2048, d_v.data_ptr(), None)
