@@ -353,6 +353,7 @@ def run_batched(instances, steps, flush_bytes=256 << 20):
         one(i)
     torch.cuda.synchronize()
     seq_dev, seq_wall = 0.0, 0.0
+    by_size = {}  # log2 n -> [instances, device ms summed over the steps]
     for _ in range(steps):
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -366,10 +367,20 @@ def run_batched(instances, steps, flush_bytes=256 << 20):
             one(i)
             e1.record(st)
             e1.synchronize()
-            seq_dev += e0.elapsed_time(e1)
+            dt = e0.elapsed_time(e1)
+            seq_dev += dt
+            bs = by_size.setdefault(int(logs[i]), [0, 0.0])
+            bs[0] += 1
+            bs[1] += dt
         seq_wall += (time.perf_counter() - t0) * 1000
     seq_dev /= steps
     seq_wall /= steps
+    # per size: the single-instance path's device rate. Batching runs the same per-element work, so
+    # its device time is at best the elements at the best single-instance rate: that bounds the ratio.
+    per_size = {str(lg): {"instances": v[0] // steps, "device_ms_each": v[1] / v[0],
+                          "elems_s": (1 << lg) / (v[1] / v[0] / 1000)} for lg, v in sorted(by_size.items())}
+    best_rate = max(v["elems_s"] for v in per_size.values())
+    ceiling = seq_dev / (total / best_rate * 1000)
 
     # the whole round (commit, evaluation point, mle and row evaluation, folding challenges, fold):
     # the batch's device round (one graph, transcripts on the device, results read back) against one
@@ -401,6 +412,7 @@ def run_batched(instances, steps, flush_bytes=256 << 20):
             "elements": total, "log2_sizes": [int(x) for x in logs],
             "sequential_device_ms": seq_dev, "sequential_wall_ms": seq_wall,
             "speedup_vs_sequential_device": seq_dev / ms, "speedup_vs_sequential_wall": seq_wall / ms,
+            "sequential_by_log2_n": per_size, "ceiling_vs_sequential_device": ceiling,
             "schedule": tuned, "gpu_launches_per_step": launches, "graphs": True,
             "workload": "commit (2 limbs: 3889, 9721) + fold of every instance, column length 2048",
             "round": {"batched_ms": round_ms, "sequential_plain_ms": plain_round_ms,

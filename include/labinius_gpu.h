@@ -308,6 +308,9 @@ int lbg_batch_use_graphs(lbg_batch* b, int enable);
 /* The autotuner times candidate commit chunkings and fold splits on the batch's own shape, and
  * whether the fold reads the commit's kept transform, and keeps the fastest. */
 int lbg_batch_autotune(lbg_batch* b, uint32_t* chunks_out, uint32_t* fold_cols_out);
+/* The schedule lbg_batch_autotune chose beyond its two outputs: the tensor-core commit's compute
+ * warps (12 with a producer warp, or 16) and whether the fold reads the kept transform. */
+int lbg_batch_schedule(const lbg_batch* b, uint32_t* commit_warps, int* kept_transform);
 /* The kept transform on or off by hand (off by default; see lbg_prover_set_kept_transform). */
 int lbg_batch_set_kept_transform(lbg_batch* b, int enable);
 int lbg_batch_commit(lbg_batch* b, int16_t* matrix_out, uint16_t* top_out, uint16_t* digits_out);

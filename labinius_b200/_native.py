@@ -116,6 +116,7 @@ SIGNATURES = {
     "lbg_ntt648_inverse": (_int, [ctypes.c_uint32, _vp, _vp, _sz, _vp]),
     "lbg_batch_stream": (_vp, [_vp]),
     "lbg_batch_set_priority": (_int, [_vp, _int]),
+    "lbg_batch_schedule": (_int, [_vp, _vp, _vp]),
     "lbg_opening_residues": (_int, [_vp, _sz, _vp]),
     "lbg_left_expansion": (_int, [_vp, _vp, _sz, _sz, _vp]),
     "lbg_batch_set_sm_limit": (_int, [_vp, _int]),

@@ -152,7 +152,10 @@ class Batch:
     def autotune(self):
         c, f = ctypes.c_uint32(), ctypes.c_uint32()
         check(lib().lbg_batch_autotune(self._h, ctypes.byref(c), ctypes.byref(f)))
-        return {"commit_chunks": c.value, "fold_columns_per_split": f.value}
+        w, k = ctypes.c_uint32(), ctypes.c_int()
+        check(lib().lbg_batch_schedule(self._h, ctypes.byref(w), ctypes.byref(k)))
+        return {"commit_chunks": c.value, "fold_columns_per_split": f.value, "commit_warps": w.value,
+                "kept_transform": bool(k.value)}
 
     def commit(self) -> List[InstanceRound]:
         C, L = self.total_cols, self.limbs

@@ -73,6 +73,7 @@ struct lbg_batch {
   int16_t* d_v = nullptr;         // [count][len_ring][648]
   bool graphs = false;
   int sm_cap = 0;                 // CTAs of the persistent commit and fold launches (0: one per SM)
+  int commit_warps = 0;           // the tensor-core commit's compute warps (0: the default; autotuned)
   cudaGraphExec_t g_commit = nullptr, g_fold = nullptr, g_round = nullptr;
   uint64_t launches = 0;
   // the round on the device: per-instance transcripts, planned once per layout and domain
@@ -115,12 +116,18 @@ static void free_graphs(lbg_batch* b) {
 // The device work of each stage, enqueued on the batch's stream (also what the graphs capture).
 // The batch's cap on the persistent kernels' CTAs, for the launches enqueued in its scope.
 struct CapScope {
-  explicit CapScope(int ctas) { set_persistent_cap(ctas); }
-  ~CapScope() { set_persistent_cap(0); }
+  explicit CapScope(int ctas, int warps = 0) {
+    set_persistent_cap(ctas);
+    set_commit_warps(warps);
+  }
+  ~CapScope() {
+    set_persistent_cap(0);
+    set_commit_warps(0);
+  }
 };
 
 static cudaError_t enqueue_commit(lbg_batch* b) {
-  CapScope cap(b->sm_cap);
+  CapScope cap(b->sm_cap, b->commit_warps);
   const lbg_pp* pp = b->pp;
   int L = pp->limbs, cols = (int)b->total_cols;
   cudaError_t e = cudaSuccess;
@@ -716,6 +723,18 @@ int lbg_batch_autotune(lbg_batch* b, uint32_t* chunks_out, uint32_t* fold_cols_o
     }
   }
   set_chunks(b, best_c);
+  // the commit's CTA shape: 12 compute warps and a producer warp, or 16 compute warps
+  best = -1;
+  int best_w = 12;
+  for (int w : {12, 16}) {
+    b->commit_warps = w;
+    float t = time_stage(b, enqueue_commit);
+    if (best < 0 || t < best) {
+      best = t;
+      best_w = w;
+    }
+  }
+  b->commit_warps = best_w;
   best = -1;
   int best_p = b->fold_per;
   for (int per = 8; per <= std::min(256, 1 << b->min_col_log); per *= 2) {
@@ -751,6 +770,13 @@ int lbg_batch_autotune(lbg_batch* b, uint32_t* chunks_out, uint32_t* fold_cols_o
   if (chunks_out) *chunks_out = (uint32_t)b->nchunks;
   if (fold_cols_out) *fold_cols_out = (uint32_t)b->fold_per;
   if (had) return lbg_batch_use_graphs(b, 1);
+  return LBG_OK;
+}
+
+int lbg_batch_schedule(const lbg_batch* b, uint32_t* commit_warps, int* kept_transform) {
+  if (!b) return fail(LBG_ERR_INVALID, "null batch");
+  if (commit_warps) *commit_warps = (uint32_t)(b->commit_warps ? b->commit_warps : 12);
+  if (kept_transform) *kept_transform = b->keep ? 1 : 0;
   return LBG_OK;
 }
 

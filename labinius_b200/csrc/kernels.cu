@@ -315,12 +315,15 @@ __global__ void k_commit_finish(const int32_t* __restrict__ partial, int nchunks
 // A buffer g % 2 is free for step g once step g - 2's multiply is done, which every compute warp
 // saw before reading that step's accumulator; accumulator g % 2 is free once every compute warp
 // has passed named barrier 1 of step g. Rows of columns past the last are zero.
-// CW compute warps (12: three leaf ranges of 56 leaves, 14 a thread, 128 registers; 16: four ranges
-// of 48, 40, 40, 40 leaves, at most 12 a thread, 120 registers) and the producer warp.
+// CW compute warps. 12: three leaf ranges of 56 leaves (14 a thread) and a producer warp (13 warps,
+// 128 registers). 16: four ranges of 48, 40, 40, 40 leaves (at most 12 a thread) and no producer
+// warp: thread 0 issues the key copies and the multiplies after each step's barrier (16 warps, 128
+// registers: a 17th warp would cost the registers of four, which allocate in groups of four warps).
 template <int CW>
 struct TccShape {
   static constexpr int CTHREADS = CW * 32;
-  static constexpr int THREADS = CTHREADS + 32;
+  static constexpr bool PRODUCER = CW == 12;  // a warp of its own issues the copies and multiplies
+  static constexpr int THREADS = CTHREADS + (PRODUCER ? 32 : 0);
   static constexpr int LPT = CW == 12 ? 14 : 12;  // leaves per compute thread (at most)
   static_assert(CW == 12 || CW == 16, "twelve or sixteen compute warps");
   // first leaf of leaf range `part`, and the number of eight-leaf chunks in it
@@ -443,7 +446,7 @@ struct TcCursor {
 };
 
 template <int PI, int CW>
-__global__ void __maxnreg__(CW == 12 ? 128 : 112)
+__global__ void __launch_bounds__(TccShape<CW>::THREADS, 1)
     k_commit_tc(const uint64_t* __restrict__ W, size_t wdim, const int4* __restrict__ Ahat,
                 const uint8_t* __restrict__ tcb, int cols, int len_ring, int chunk, int nchunks,
                 int32_t* __restrict__ partial /* [nchunks][cols][162][4] */) {
@@ -492,7 +495,7 @@ __global__ void __maxnreg__(CW == 12 ? 128 : 112)
   tc::fence_after_sync();
   const uint32_t tmem = *tslot;
 
-  if (warp == CTHREADS / 32) {
+  if (Sh::PRODUCER && warp == CTHREADS / 32) {
     // ---------------- producer (one lane) ----------------
     const uint32_t sA_u = tc::smem_u32(sA), sB_u = tc::smem_u32(sB);
     TcCursor cur = curs[0];
@@ -564,16 +567,45 @@ __global__ void __maxnreg__(CW == 12 ? 128 : 112)
       a[2] += lo.z * w0 + lo.y * w1 + lo.x * w2 + hi.z * w3;
       a[3] += lo.w * w0 + lo.z * w1 + lo.y * w2 + lo.x * w3;
     };
+    // without a producer warp, thread 0 keeps the cursor sequence and issues, after step g's
+    // barrier, step g's key copy into buffer g % 2 (its last reader, step g - 2's module product,
+    // finished before that barrier) and step g's multiply
+    TcCursor pcur;
+    if (!Sh::PRODUCER && tid == 0) {
+      pcur = curs[0];
+      tc::mbar_arrive_expect_tx(bfull, TC_B_BYTES);
+      for (int x = 0; x < 4; x++)
+        tc::bulk_g2s(sB + x * (TC_B_BYTES / 4), tcb + x * (TC_B_BYTES / 4), TC_B_BYTES / 4, bfull);
+    }
     copy_words(curs[0], 0);
     for (int g = 0; g <= S; g++) {
       if (g < S) {
         const int b = g & 1;
+        if (!Sh::PRODUCER && tid == 0) {
+          // step g + 1's cursor, read after this step's barrier (its slot's last reader was step
+          // g - 3's module product, before the previous barrier)
+          pcur.advance(items);
+          curs[(g + 1) & 3] = pcur;
+        }
         tc_wait(&wfull[b], (g >> 1) & 1, abort);  // step g's words
         tc_build_row_inline<12 * 128 / CTHREADS>(sA + b * TCC_A_BYTES, tid, CTHREADS,
                                                    wtile + (b * 128 + r) * 3, curs[g & 3].j0 + rj < cols);
         tc::fence_async_shared();
         tc::fence_before_sync();
         tc::named_sync(1, THREADS);  // meets the producer: lockstep, even when a wait timed out
+        if (!Sh::PRODUCER && tid == 0) {
+          tc::fence_after_sync();
+          if (g == 0) tc_wait(bfull, 0, abort);
+          if (!*abort) {
+            tc::mbar_arrive_expect_tx(&kfull[b], TCC_AT_BYTES);
+            tc::bulk_g2s(atile + b * (N162 * 2), Ahat + (size_t)curs[g & 3].i * N162 * 2, TCC_AT_BYTES, &kfull[b]);
+            tc_transform_mma(tmem + (uint32_t)b * 256u, tc::smem_u32(sA) + (uint32_t)b * TCC_A_BYTES,
+                             tc::smem_u32(sB), &mma[b]);
+          } else {
+            tc::mbar_arrive(&kfull[b]);
+            tc::mbar_arrive(&mma[b]);
+          }
+        }
         if (g + 1 < S) copy_words(curs[(g + 1) & 3], (g + 1) & 1);
       }
       if (g >= 1) {
@@ -625,8 +657,10 @@ __global__ void __maxnreg__(CW == 12 ? 128 : 112)
         }
         tc::fence_before_sync();
         tc::fence_async_shared();  // this warp's reads of the key tile precede the next bulk copy into it
-        __syncwarp();
-        if (lane == 0) tc::mbar_arrive(&kempty[b]);
+        if (Sh::PRODUCER) {
+          __syncwarp();
+          if (lane == 0) tc::mbar_arrive(&kempty[b]);
+        }
         if (++since >= RED) {
           since = 0;
 #pragma unroll
@@ -659,6 +693,14 @@ __global__ void __maxnreg__(CW == 12 ? 128 : 112)
       }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");  // no copy of this thread outlives the CTA
+    if (!Sh::PRODUCER && tid == 0) {
+      // as the producer warp does: the last key copies and multiplies have landed (bounded waits
+      // that ignore the abort flag)
+      for (int g = S - 2 < 0 ? 0 : S - 2; g < S; g++) {
+        tc::mbar_wait(&kfull[g & 1], (g >> 1) & 1, TC_WAIT_BUDGET);
+        tc::mbar_wait(&mma[g & 1], (g >> 1) & 1, TC_WAIT_BUDGET);
+      }
+    }
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -2223,14 +2265,16 @@ bool commit_tc_enabled() {
   return on;
 }
 
-// Compute warps of the tensor-core commit: 12 unless LBG_COMMIT_WARPS=16 (both exact; the switch is
-// for timing them against each other).
+// Compute warps of the tensor-core commit: the calling thread's choice (set_commit_warps, the batch
+// autotuner's), else 12 unless LBG_COMMIT_WARPS=16 (both exact).
+static thread_local int t_commit_warps = 0;
+void set_commit_warps(int warps) { t_commit_warps = (warps == 12 || warps == 16) ? warps : 0; }
 static int commit_tc_warps() {
   static const int w = [] {
     const char* e = getenv("LBG_COMMIT_WARPS");
     return (e && std::string(e) == "16") ? 16 : 12;
   }();
-  return w;
+  return t_commit_warps ? t_commit_warps : w;
 }
 
 int commit_blocks_per_sm(int pi) {

@@ -50,6 +50,9 @@ bool commit_tc_enabled();
 // At most `ctas` CTAs for the persistent tensor-core kernels launched from the calling host thread
 // (0: one per SM).
 void set_persistent_cap(int ctas);
+// The tensor-core commit's compute warps (12 or 16; 0: the default) for launches from the calling
+// host thread.
+void set_commit_warps(int warps);
 // 1 (and cleared) when a tensor-core kernel's bounded wait ran out since the last call, else 0;
 // -1 when the flag could not be read.
 int tc_timeout_take();

@@ -87,7 +87,7 @@ class Server:
     def __init__(self, pp: PublicParameters, capacity_columns: Optional[int] = None, max_requests: int = 256,
                  slots: int = 2, host_threads: int = 16, domain: bytes = b"labinius/reference",
                  keep_results: bool = True, transcript: str = "device", hbm_fraction: float = 0.5,
-                 small_log_len: Optional[int] = None, large_sm_limit: int = 0):
+                 small_log_len: Optional[int] = None, large_sm_limit: int = 0, small_slot_takes_large: bool = False):
         self.pp = pp
         self.memory_columns = arena_columns(pp, hbm_fraction, slots, max_requests)
         self.capacity = self.memory_columns if capacity_columns is None else min(capacity_columns, self.memory_columns)
@@ -96,6 +96,7 @@ class Server:
         self.keep_results = keep_results
         self.transcript = transcript
         self.small_log_len = small_log_len if slots >= 2 else None
+        self.small_slot_takes_large = small_slot_takes_large
         self.slots = [Batch(pp, capacity=(self.capacity, max_requests)) for _ in range(slots)]
         if self.small_log_len is not None:
             # the small requests' slot is scheduled ahead of the large ones' when both wait for SMs,
@@ -142,10 +143,14 @@ class Server:
         return req
 
     def _queue_for(self, slot: int):
-        """The queue slot `slot` serves next: slot 0 the small requests only (with size classes),
-        the others the large ones first, then the small ones."""
-        if self.small_log_len is None or slot == 0:
+        """The queue slot `slot` serves next: slot 0 the small requests (with size classes; also the
+        large ones when no small one waits and small_slot_takes_large is set), the others the large
+        ones first, then the small ones."""
+        if self.small_log_len is None:
             return self.small
+        if slot == 0:
+            # the small slot: small requests, and large ones too when it would idle otherwise
+            return self.large if (self.small_slot_takes_large and not self.small and self.large) else self.small
         return self.large if self.large else self.small
 
     def _admit(self, q) -> List[Request]:
