@@ -618,10 +618,10 @@ def run_wire(L, prover, params, steps):
             "workload": "the folded witness of the bench's step (len_ring x 648 int16), interleaved rANS, 64 lanes"}
 
 
-def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027, server_kw=None):
+def run_served(requests, plain_sample, load=0.7, slots=3, seed=2027, server_kw=None):
     """Served: commit+open requests with log2 n ~ U{18..22} (column length 2048, moduli [3889, 9721]),
     80% Witness::random and 20% B128 traces opened through the cross-field switch, each from its
-    own seed, through the serving loop (continuous batching over two device arenas, transcripts on
+    own seed, through the serving loop (continuous batching over three device arenas, transcripts on
     the device). First the saturated throughput (every request queued at once, a sample of the
     stream); then the Poisson stream of `requests` arrivals at `load` x that throughput, with
     p50/p99 latency from arrival to result. The comparison is the plain per-request path, one
@@ -646,10 +646,11 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027, server_kw=N
 
     pp = L.PublicParameters.from_seed(params(7), MATRIX_SEED)
     # small requests (at most 2^20 F162) on a slot of their own, so that none waits behind large ones
-    # at most 4096 columns a batch (two 2^22 requests): a request that arrives while a batch runs waits
-    # for at most that much work (at 8192 columns the p99 at 0.7 load was 29 ms, at 4096 20 ms, for
-    # 2% less saturated throughput)
-    kw = dict(capacity_columns=4096, max_requests=64, slots=slots, host_threads=os.cpu_count() or 1,
+    # three slots (one for small requests, two taking large ones first) of at most 2048 columns a batch
+    # (one 2^22 request): a large request waits for at most one batch of large work per slot. Measured
+    # at 0.7 load over 10,000 requests: two slots of 4096 columns p99 28 ms, three of 4096 25 ms, three
+    # of 2048 23 ms, for 6% less saturated throughput than two of 4096.
+    kw = dict(capacity_columns=2048, max_requests=64, slots=slots, host_threads=os.cpu_count() or 1,
               keep_results=False, small_log_len=9)
     kw.update(server_kw or {})
     srv = Server(pp, **kw)
@@ -744,8 +745,8 @@ def run_served(requests, plain_sample, load=0.7, slots=2, seed=2027, server_kw=N
                             "plain_p99_ms": float(np.percentile(psel, 99)) if len(psel) else None}
     return {"requests": requests, "rate_req_s": rate, "load": load, "batches": batches, "by_log2_n": by_size,
             "admission": "arenas within half the free HBM, at most %d columns a batch; requests of at most "
-                         "2^20 F162 on a slot of their own (greatest stream priority), the other slot large ones "
-                         "first" % kw["capacity_columns"],
+                         "2^20 F162 on a slot of their own (greatest stream priority), the other %d slots large "
+                         "ones first" % (kw["capacity_columns"], slots - 1),
             "throughput_elems_s": st_elems, "throughput_req_s": st_reqs,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()),

@@ -76,3 +76,33 @@ def test_residues_and_left_expansion_match_oracle(shape):
     # the transcript of the recursive round absorbs LaBRADOR's T_y and T_u: refused here
     with pytest.raises(NativeError):
         L.Verifier(pp).derive_evaluation_point(L.Transcript(b"labinius/reference"), c)
+
+
+def test_recursive_entry_points_refuse_misuse():
+    """Too few polynomials, a row evaluation of the wrong width and a bit-dropped commitment are
+    refused with a message; nothing is launched and the prover stays usable."""
+    import labinius_b200 as L
+    from labinius_b200._native import LBG_ERR_INVALID, NativeError
+
+    params = recursive_params(12, 4, [3889, 9721])
+    pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+    w = L.Witness.random(pp, WITNESS_SEED)
+    prover = L.Prover(pp)
+    c, op = prover.commit(w)
+    with pytest.raises(NativeError) as e:
+        op.residues(3 * params.columns() - 1)
+    assert e.value.code == LBG_ERR_INVALID
+    row = L.RowEvaluation(np.zeros((params.columns() + 1, 3), np.uint64))
+    with pytest.raises(NativeError):
+        prover.commit_left_expansion_vector(row)
+    with pytest.raises(NativeError):
+        prover.commit_left_expansion_vector(L.RowEvaluation(np.zeros((params.columns(), 3), np.uint64)),
+                                            3 * params.columns() - 1)
+    assert np.array_equal(op.residues(), O.recursion_residues(O.Params(12, 4, [3889, 9721]), c.matrix))
+
+    bd = L.Params.with_base(12, 4, L.Modulus(3889), [L.Modulus(2917), L.Modulus(4861)], L.Opening.bit_dropped(9))
+    ppb = L.PublicParameters.from_seed(bd, MATRIX_SEED)
+    pb = L.Prover(ppb)
+    _, opb = pb.commit(L.Witness.random(ppb, WITNESS_SEED))
+    with pytest.raises(NativeError):
+        opb.residues()
