@@ -762,12 +762,30 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
   if (n != pp->n) return fail(LBG_ERR_WITNESS, "the witness is not witness_len() elements");
   LBG_CU(cudaSetDevice(pp->device));
   const int cols = (int)pp->cols, L = pp->limbs;
-  // column groups of at least 64 columns, at most 8
-  int groups = 1;
-  while (groups < 8 && cols / (2 * groups) >= 64) groups *= 2;
-  const int gc = cols / groups;
-  int chunk = pr->chunk, nch = pr->nchunks;
-  if (groups > 1) commit_chunking(pp, gc, (long)pr->nchunks * cols, &chunk, &nch);
+  // column groups of at least 64 columns, at most 8; the first one split in two halves, so that the
+  // commit starts after half a group's copy
+  int ngroups = 1;
+  while (ngroups < 8 && cols / (2 * ngroups) >= 64) ngroups *= 2;
+  const int gc = cols / ngroups;
+  std::vector<int> gstart, gcols;  // the groups' first columns and widths
+  if (ngroups > 1) {
+    gstart = {0, gc / 2};
+    gcols = {gc / 2, gc / 2};
+  } else {
+    gstart = {0};
+    gcols = {gc};
+  }
+  for (int g = 1; g < ngroups; g++) {
+    gstart.push_back(g * gc);
+    gcols.push_back(gc);
+  }
+  const int groups = (int)gstart.size();
+  // the chunking of each group width
+  int chunk = pr->chunk, nch = pr->nchunks, chunk_h = pr->chunk, nch_h = pr->nchunks;
+  if (ngroups > 1) {
+    commit_chunking(pp, gc, (long)pr->nchunks * cols, &chunk, &nch);
+    commit_chunking(pp, gc / 2, (long)pr->nchunks * cols, &chunk_h, &nch_h);
+  }
   if (!pr->copy_stream && cudaStreamCreateWithFlags(&pr->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(LBG_ERR_CUDA, "copy stream");
   while ((int)pr->group_events.size() < groups) {
@@ -808,7 +826,7 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
   }
   cudaStream_t st = pr->stream, cp = pr->copy_stream;
   const size_t per_col = pp->wdim * 3;  // u64 words of a column
-  const size_t group_bytes = (size_t)gc * per_col * 8;
+  const size_t group_bytes = (size_t)gc * per_col * 8;  // the widest group's
   const bool pageable = host_pageable(f162);
   if (pageable) {
     rc = stage_ready(pr, group_bytes);
@@ -821,17 +839,20 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
   }
   cudaError_t e = cudaSuccess;
   for (int g = 0; g < groups && e == cudaSuccess; g++) {
-    const size_t c0 = (size_t)g * gc;
+    const size_t c0 = (size_t)gstart[g];
+    const int gw = gcols[g];
+    const int gch = gw == gc ? chunk : chunk_h, gnch = gw == gc ? nch : nch_h;
+    const size_t gbytes = (size_t)gw * per_col * 8;
     if (pageable) {
       // stage g % STAGES is free once the device copy of group g - STAGES out of it has finished
       const int s = g % lbg_prover::STAGES;
       e = cudaEventSynchronize(pr->stage_copied[s]);
       if (e != cudaSuccess) break;
-      pr->copy_pool->copy(pr->stage[s], f162 + c0 * per_col, group_bytes);
-      e = cudaMemcpyAsync(w->d + c0 * per_col, pr->stage[s], group_bytes, cudaMemcpyHostToDevice, cp);
+      pr->copy_pool->copy(pr->stage[s], f162 + c0 * per_col, gbytes);
+      e = cudaMemcpyAsync(w->d + c0 * per_col, pr->stage[s], gbytes, cudaMemcpyHostToDevice, cp);
       if (e == cudaSuccess) e = cudaEventRecord(pr->stage_copied[s], cp);
     } else {
-      e = cudaMemcpyAsync(w->d + c0 * per_col, f162 + c0 * per_col, group_bytes, cudaMemcpyHostToDevice, cp);
+      e = cudaMemcpyAsync(w->d + c0 * per_col, f162 + c0 * per_col, gbytes, cudaMemcpyHostToDevice, cp);
     }
     if (e == cudaSuccess) e = cudaEventRecord(pr->group_events[g], cp);
     for (int k = 0; k < L && e == cudaSuccess; k++) {
@@ -843,20 +864,20 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
       if (k == 0) {
         KernelScope ks(pr, "commit");
         e = launch_commit(pp->pidx[k], w->d + c0 * per_col, pp->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2,
-                          pp->d_prime[k], gc, (int)pp->len_ring, chunk, nch, part, sk,
+                          pp->d_prime[k], gw, (int)pp->len_ring, gch, gnch, part, sk,
                           b->d_keep ? b->d_keep + c0 * pp->wdim * N162 : nullptr, pp->d_tcb[k]);
       } else {
         pr->launches += 1;
         e = launch_commit(pp->pidx[k], w->d + c0 * per_col, pp->wdim, pp->d_Ahat + (size_t)k * pp->len_ring * N162 * 2,
-                          pp->d_prime[k], gc, (int)pp->len_ring, chunk, nch, part, sk, nullptr, pp->d_tcb[k]);
+                          pp->d_prime[k], gw, (int)pp->len_ring, gch, gnch, part, sk, nullptr, pp->d_tcb[k]);
       }
       if (e != cudaSuccess) break;
       if (k == 0) {
         KernelScope ks(pr, "commit_finish");
-        e = launch_commit_finish(pp->pidx[k], part, nch, gc, pp->d_prime[k], k, L, b->d_C + c0 * 4 * L * N162, sk);
+        e = launch_commit_finish(pp->pidx[k], part, gnch, gw, pp->d_prime[k], k, L, b->d_C + c0 * 4 * L * N162, sk);
       } else {
         pr->launches += 1;
-        e = launch_commit_finish(pp->pidx[k], part, nch, gc, pp->d_prime[k], k, L, b->d_C + c0 * 4 * L * N162, sk);
+        e = launch_commit_finish(pp->pidx[k], part, gnch, gw, pp->d_prime[k], k, L, b->d_C + c0 * 4 * L * N162, sk);
       }
     }
   }
