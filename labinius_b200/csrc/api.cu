@@ -462,6 +462,7 @@ void lbg_prover_free(lbg_prover* pr) {
   cudaFree(pr->d_v);
   cudaFree(pr->d_wire);
   cudaFree(pr->d_rec);
+  cudaFree(pr->d_gm);
   cudaFree(pr->d_res);
   for (auto* b : pr->spare) free_bufs(b);
   for (auto& m : pr->marks) {
@@ -568,7 +569,8 @@ int lbg_prover_new(const lbg_pp* pp, lbg_prover** out) {
       cudaMalloc((void**)&pr->d_ch, pp->cols * sizeof(lbg_challenge_d)) != cudaSuccess ||
       cudaMalloc((void**)&pr->d_chat, pp->cols * N162 * 4) != cudaSuccess ||
       cudaMalloc((void**)&pr->d_v, pp->len_ring * N648 * 2) != cudaSuccess ||
-      cudaMalloc((void**)&pr->d_res, (size_t)pp->limbs * count * 2) != cudaSuccess) {
+      cudaMalloc((void**)&pr->d_res, (size_t)pp->limbs * count * 2) != cudaSuccess ||
+      (fold_gm_enabled() && cudaMalloc((void**)&pr->d_gm, fold_gm_operand_bytes(pp->cols)) != cudaSuccess)) {
     cudaGetLastError();
     return bail(fail(LBG_ERR_OOM, "prover workspace: device allocation failed"));
   }
@@ -1101,6 +1103,9 @@ int lbg_fold(lbg_prover* pr, lbg_opening* op, const lbg_challenge* challenges, s
     if (op->bufs->d_keep)
       e = launch_fold_kept(pp->pidx[0], op->bufs->d_keep, pp->wdim, (int)pp->cols, pr->fold_cols_per_split,
                            pr->d_chat, pp->d_prime[0], pr->d_vhat, pr->d_v, st);
+    else if (pr->d_gm)
+      e = launch_fold_gm(pp->pidx[0], op->w->d, pp->wdim, (int)pp->cols, pr->fold_cols_per_split, pr->d_chat,
+                         pp->d_tcb[0], pr->d_gm, pp->d_prime[0], pr->d_vhat, pr->d_v, st);
     else
       e = launch_fold(pp->pidx[0], op->w->d, pp->wdim, (int)pp->cols, pr->fold_cols_per_split, pr->d_chat,
                       pp->d_prime[0], pr->d_vhat, pr->d_v, st, 1, nullptr, pp->d_tcb[0]);

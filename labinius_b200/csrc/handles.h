@@ -87,6 +87,7 @@ struct lbg_prover {
   uint8_t* d_wire = nullptr;  // lbg_opening_pack_commitment's bytes (grown on use)
   size_t wire_cap = 0;
   uint16_t* d_res = nullptr;  // [limbs][cols*648]
+  uint8_t* d_gm = nullptr;    // the fold's per-column tensor-core operands (LBG_FOLD_KERNEL=gm)
   int16_t* d_rec = nullptr;   // lbg_opening_residues' vectors (grown on use)
   size_t rec_cap = 0;
   std::mutex mu;

@@ -1183,6 +1183,232 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
 
 // The inverse transform of each position's sums from the transposed scratch vhat_t (per instance
 // [162][wdim]), centred into the folded witness, as k_fold_finish.
+// =============================================================================================
+// Fold as one tensor-core product per column: the challenge folded into the transform operand
+// =============================================================================================
+// v^_p(v) = sum_j c^_j(v) w^_{j,p}(v) = sum_j sum_m bit_m(W[j][p]) G_j[m][v] with
+// G_j[m][v] = c^_j(v) T[m][v] mod q: the challenge weight moves from the CUDA cores into the
+// multiply's B operand. k_fold_operand builds G_j for every column in the transform operand's layout
+// (lo + 128 hi, K-major, 128-byte swizzle); k_fold_gm then accumulates, for 128 positions, the
+// product of the bits (the commit's A operand, bits and 128 x bits) with G_j over all the columns
+// of a work item in one tensor-memory accumulator (below 2^31 for at most 512 columns: 512 x 162 x
+// (q - 1) < 2^31 for every prime here), and reads it back once per item. The CUDA cores only expand
+// the bits and reduce each item's sums.
+constexpr int GM_MAX_COLS_PER_SPLIT = 512;
+
+// One thread per (column j, row v of N, 16-byte chunk c of K): the chunk's 16 bytes of G_j.
+template <int PI>
+__global__ void k_fold_operand(const uint32_t* __restrict__ chat /* [cols][162] */, int cols,
+                               const uint8_t* __restrict__ tcb /* T, TC_B_BYTES */, uint8_t* __restrict__ G) {
+  constexpr uint32_t q = Pr<PI>::q;
+  const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr int CHUNKS = TC_KBYTES / 16;  // 24
+  if (gid >= (size_t)cols * TC_LEAVES * CHUNKS) return;
+  const int c = (int)(gid % CHUNKS);
+  const int v = (int)((gid / CHUNKS) % TC_LEAVES);
+  const int j = (int)(gid / ((size_t)CHUNKS * TC_LEAVES));
+  const int kb0 = 16 * c;
+  const bool hi = kb0 >= 192;
+  uint32_t bytes[4] = {0, 0, 0, 0};
+  if (v < N162) {
+    const uint32_t cv = chat[(size_t)j * N162 + v];
+#pragma unroll
+    for (int x = 0; x < 16; x++) {
+      const int m = (hi ? kb0 - 192 : kb0) + x;
+      if (m < N162) {
+        const uint32_t t = (uint32_t)tcb[tc_swizzled_offset(v, m, TC_LEAVES)] +
+                           128u * (uint32_t)tcb[tc_swizzled_offset(v, 192 + m, TC_LEAVES)];
+        const uint32_t g = red_full<PI>(cv * t);
+        bytes[x >> 2] |= (hi ? g >> 7 : g & 127u) << (8 * (x & 3));
+      }
+    }
+  }
+  *(uint4*)(G + (size_t)j * TC_B_BYTES + tc_swizzled_offset(v, kb0, TC_LEAVES)) =
+      make_uint4(bytes[0], bytes[1], bytes[2], bytes[3]);
+}
+
+// A position in a CTA's k_fold_gm items, as TcfCursor, with the accumulator the item uses (the
+// CTA's items alternate between two).
+struct GmCursor {
+  TcfCursor c;
+  int acc;
+};
+
+// Persistent over items (128 positions x a column split), one column a step, two warp roles:
+//   producer (warp 12, one lane): for step g, once step g - 2's multiply is done, copies G_j into B
+//            buffer g % 2 and step g + 1's witness words into wtile (g + 1) % 2 (bulk copies), writes
+//            step g + 1's cursor, meets the compute warps (named barrier 1), then issues step g's
+//            multiply into the item's accumulator (accumulating after the item's first K-step);
+//   compute (warps 0-11) for step g: once step g - 1's multiply is done (the A buffer is free), add
+//            the sums of an item that step g - 1 ended into vhat_t (warp w: the lanes of quadrant
+//            w % 4 = positions, leaves [56 (w / 4), + 56)), then expand step g's words into A and
+//            meet the producer.
+constexpr int GM_THREADS = TCF_THREADS;  // 12 compute warps and the producer warp
+constexpr int GM_OFF_A = 2 * TC_B_BYTES;  // two B buffers, then one A buffer
+constexpr int GM_OFF_WT = GM_OFF_A + TCC_A_BYTES;
+constexpr int GM_OFF_BAR = GM_OFF_WT + 2 * TCF_WT_BYTES;
+constexpr int GM_OFF_CUR = GM_OFF_BAR + 64;
+constexpr int GM_SMEM = GM_OFF_CUR + 4 * (int)sizeof(GmCursor) + 1024;
+static_assert(GM_OFF_A % TC_ATOM == 0 && TC_B_BYTES % TC_ATOM == 0 && GM_OFF_WT % 16 == 0 && GM_OFF_BAR % 8 == 0 &&
+                  GM_OFF_CUR % 8 == 0,
+              "alignment");
+static_assert(GM_SMEM <= 232448, "shared memory per CTA");
+
+// Issue the 12 K-steps of one column's 128 x 176 x 384 multiply (accumulating unless `first`) and
+// commit them to `bar`.
+__device__ __forceinline__ void gm_mma(uint32_t d_tmem, uint32_t sA_u, uint32_t sB_u, bool first, uint64_t* bar) {
+  constexpr uint32_t IDESC = tc::idesc_u8(128, TC_LEAVES);
+#pragma unroll
+  for (int kk = 0; kk < TC_KBYTES / 32; kk++) {
+    const uint32_t a = sA_u + (kk >> 2) * (128 * 128) + (kk & 3) * 32;
+    const uint32_t b = sB_u + (kk >> 2) * (TC_LEAVES * 128) + (kk & 3) * 32;
+    tc::mma_i8(d_tmem, tc::smem_desc_sw128(a, TC_ATOM), tc::smem_desc_sw128(b, TC_ATOM), IDESC,
+               (first && kk == 0) ? 0u : 1u);
+  }
+  tc::commit_to(bar);
+}
+
+template <int PI>
+__global__ void __launch_bounds__(GM_THREADS, 1)
+    k_fold_gm(const uint64_t* __restrict__ W, size_t wdim, int cols, int cols_per_split,
+              const uint8_t* __restrict__ G, uint32_t* __restrict__ vhat_t) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);  // swizzle atoms
+  uint8_t* sB = smem;                                                           // [2] G_j
+  uint8_t* sA = smem + GM_OFF_A;
+  uint64_t* wtile = (uint64_t*)(smem + GM_OFF_WT);  // [2][128][3]
+  uint64_t* wfull = (uint64_t*)(smem + GM_OFF_BAR);  // [2]: step g's words landed
+  uint64_t* bfull = wfull + 2;                       // [2]: step g's G_j landed
+  uint64_t* mma = wfull + 4;                         // [2]: step g's multiply done
+  uint32_t* tslot = (uint32_t*)(wfull + 6);
+  volatile int* abort = (volatile int*)(wfull + 7);
+  GmCursor* curs = (GmCursor*)(smem + GM_OFF_CUR);  // step g's cursor in slot g % 4
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles = (int)((wdim + TCF_ROWS - 1) / TCF_ROWS);
+  const int splits = (cols + cols_per_split - 1) / cols_per_split;
+  const int total = tiles * splits;
+  int S = 0;
+  for (int it = blockIdx.x; it < total; it += gridDim.x) {
+    const int c0 = (it / tiles) * cols_per_split;
+    S += max(0, min(cols, c0 + cols_per_split) - c0);
+  }
+  auto advance = [&](GmCursor& g) {
+    if (++g.c.st < g.c.n) return;
+    g.c.load(g.c.it + (int)gridDim.x, (int)gridDim.x, total, tiles, cols, cols_per_split);
+    g.acc ^= 1;
+  };
+
+  if (tid == 0) {
+    for (int b = 0; b < 6; b++) tc::mbar_init(&wfull[b], 1);
+    *abort = 0;
+    curs[0].c.load(blockIdx.x, (int)gridDim.x, total, tiles, cols, cols_per_split);
+    curs[0].acc = 0;
+    tc::mbar_init_fence();
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, TCF_TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tslot;
+
+  if (warp == TCF_CTHREADS / 32) {
+    // ---------------- producer (one lane) ----------------
+    auto load_words = [&](const GmCursor& g, int b) {
+      const size_t p0 = (size_t)g.c.tile * TCF_ROWS;
+      tc::mbar_arrive_expect_tx(&wfull[b], TCF_WT_BYTES);
+      tc::bulk_g2s(wtile + b * (TCF_ROWS * 3), W + ((size_t)(g.c.c0 + g.c.st) * wdim + p0) * 3, TCF_WT_BYTES,
+                   &wfull[b]);
+    };
+    const uint32_t sA_u = tc::smem_u32(sA), sB_u = tc::smem_u32(sB);
+    GmCursor cur = curs[0];
+    if (lane == 0 && S > 0) load_words(cur, 0);
+    for (int g = 0; g < S; g++) {
+      const int b = g & 1;
+      GmCursor nxt = cur;
+      advance(nxt);
+      if (lane == 0) {
+        // G_j of step g into B buffer b, whose last reader was step g - 2's multiply
+        if (g >= 2) tc_wait(&mma[b], ((g - 2) >> 1) & 1, abort);
+        const int j = cur.c.c0 + cur.c.st;
+        tc::mbar_arrive_expect_tx(&bfull[b], TC_B_BYTES);
+        for (int x = 0; x < 4; x++)
+          tc::bulk_g2s(sB + b * TC_B_BYTES + x * (TC_B_BYTES / 4), G + (size_t)j * TC_B_BYTES + x * (TC_B_BYTES / 4),
+                       TC_B_BYTES / 4, &bfull[b]);
+        // step g + 1's words into wtile (g + 1) % 2, whose step g - 1 the compute warps expanded
+        if (g + 1 < S) load_words(nxt, (g + 1) & 1);
+        curs[(g + 1) & 3] = nxt;
+      }
+      __syncwarp();
+      tc::named_sync(1, GM_THREADS);  // step g's A operand is built
+      if (lane == 0) {
+        tc::fence_after_sync();
+        tc_wait(&bfull[b], (g >> 1) & 1, abort);
+        if (!*abort)
+          gm_mma(tmem + (uint32_t)cur.acc * 256u, sA_u, sB_u + (uint32_t)b * TC_B_BYTES, cur.c.st == 0, &mma[b]);
+        else
+          tc::mbar_arrive(&mma[b]);
+      }
+      __syncwarp();
+      cur = nxt;
+    }
+    if (lane == 0) {
+      // the last copies and multiplies have landed before the CTA winds down (bounded waits that
+      // ignore the abort flag)
+      for (int g = S - 2 < 0 ? 0 : S - 2; g < S; g++) {
+        tc::mbar_wait(&bfull[g & 1], (g >> 1) & 1, TC_WAIT_BUDGET);
+        tc::mbar_wait(&mma[g & 1], (g >> 1) & 1, TC_WAIT_BUDGET);
+      }
+    }
+  } else if (S > 0) {
+    // ---------------- compute ----------------
+    const int quad = warp & 3, part = warp >> 2;
+    const int v0 = 56 * part;  // leaves v0 .. v0 + 55 (v0 + 49 for the last part)
+    const int row = 32 * quad + lane;
+    // the sums of the item that step s ended, from its accumulator into vhat_t
+    auto drain = [&](int s) {
+      const GmCursor& it = curs[s & 3];
+      const uint32_t taddr = tmem + (uint32_t)it.acc * 256u + ((uint32_t)(32 * quad) << 16) + v0;
+      const size_t p0 = (size_t)it.c.tile * TCF_ROWS;
+      uint32_t* d = vhat_t + p0 + row + (size_t)v0 * wdim;
+      const bool inside = p0 + row < wdim;
+#pragma unroll
+      for (int bt = 0; bt < 7; bt++) {
+        uint32_t x[8];
+        tc::tmem_ld8(taddr + 8 * bt, x);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const int v = v0 + 8 * bt + i;
+          if (inside && v < N162) atomicAdd(d + (size_t)(8 * bt + i) * wdim, red_full<PI>(x[i]));
+        }
+      }
+    };
+    for (int g = 0; g < S; g++) {
+      if (g >= 1) {
+        tc_wait(&mma[(g - 1) & 1], ((g - 1) >> 1) & 1, abort);  // step g - 1's multiply: A is free
+        tc::fence_after_sync();
+        const GmCursor& prev = curs[(g - 1) & 3];
+        if (prev.c.st + 1 == prev.c.n) drain(g - 1);
+      }
+      tc_wait(&wfull[g & 1], (g >> 1) & 1, abort);  // step g's words
+      tc_build_row_inline<12 * 128 / TCF_CTHREADS>(sA, tid, TCF_CTHREADS, wtile + (g & 1) * (TCF_ROWS * 3) + (tid & 127) * 3);
+      tc::fence_async_shared();
+      tc::fence_before_sync();
+      tc::named_sync(1, GM_THREADS);  // meets the producer: lockstep, even when a wait timed out
+    }
+    // the last item's sums
+    tc_wait(&mma[(S - 1) & 1], ((S - 1) >> 1) & 1, abort);
+    tc::fence_after_sync();
+    drain(S - 1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, TCF_TMEM_COLS);
+  if (tid == 0 && *abort) atomicExch(&g_tc_timeout, 1);
+}
+
 template <int PI>
 __global__ void __launch_bounds__(216) k_fold_finish_t(const uint32_t* __restrict__ vhat_t, size_t wdim,
                                                        size_t positions, const DevPrime* __restrict__ D,
@@ -2410,6 +2636,37 @@ bool fold_tc_enabled() {
   return on;
 }
 int fold_tc_positions_per_cta() { return TCF_ROWS; }
+
+// The single prover's fold takes k_fold_gm (the challenge in the multiply's operand) when
+// LBG_FOLD_KERNEL=gm.
+bool fold_gm_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("LBG_FOLD_KERNEL");
+    return e && std::string(e) == "gm";
+  }();
+  return on;
+}
+size_t fold_gm_operand_bytes(size_t cols) { return cols * (size_t)TC_B_BYTES; }
+
+cudaError_t launch_fold_gm(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
+                           const uint8_t* tcb, uint8_t* G, const DevPrime* D, uint32_t* vhat, int16_t* v,
+                           cudaStream_t st) {
+  if (cols <= 0 || cols_per_split <= 0) return cudaErrorInvalidValue;
+  cols_per_split = std::min(cols_per_split, GM_MAX_COLS_PER_SPLIT);
+  const int splits = (cols + cols_per_split - 1) / cols_per_split;
+  const long items = (long)((wdim + TCF_ROWS - 1) / TCF_ROWS) * splits;
+  dim3 grid((unsigned)std::max<long>(1, std::min<long>(items, persistent_ctas())));
+  cudaError_t e = cudaMemsetAsync(vhat, 0, wdim * N162 * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
+  const size_t nop = (size_t)cols * TC_LEAVES * (TC_KBYTES / 16);
+  LBG_DISPATCH(pi, ({
+                 k_fold_operand<P><<<blocks_for(nop, 256), 256, 0, st>>>(chat, cols, tcb, G);
+                 cudaFuncSetAttribute(k_fold_gm<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, GM_SMEM);
+                 k_fold_gm<P><<<grid, GM_THREADS, GM_SMEM, st>>>(W, wdim, cols, cols_per_split, G, vhat);
+                 k_fold_finish_t<P><<<blocks_for(wdim, 4), 216, 0, st>>>(vhat, wdim, wdim, D, v);
+               }));
+  return cudaGetLastError();
+}
 
 cudaError_t launch_fold(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
                         const DevPrime* D, uint32_t* vhat, int16_t* v, cudaStream_t st, int instances,
