@@ -84,12 +84,15 @@ int lbg_params_check(const lbg_params* p);
  * the host, A expanded on the device (xorshift64*, crates/pcs/src/key.rs:48-88) and kept
  * resident with its R_162 component form. */
 int lbg_public_parameters_from_seed(const lbg_params* p, const uint8_t matrix_seed[32], lbg_pp** out);
+/* Drops the caller's reference: the parameters are freed once the provers and batches made from them
+ * are freed too, so handles may be freed in any order. */
 void lbg_public_parameters_free(lbg_pp* pp);
 /* CommitmentKey::row (crates/pcs/src/key.rs:135-141) for every limb, into int16 [limbs][len_ring][648]. */
 int lbg_key_download(const lbg_pp* pp, int16_t* out);
 
 /* Prover::new (crates/pcs/src/scheme/prover.rs:31-53): device workspace + warm-up round. */
 int lbg_prover_new(const lbg_pp* pp, lbg_prover** out);
+/* Drops the caller's reference: the prover is freed once its openings are freed or folded. */
 void lbg_prover_free(lbg_prover* pr);
 
 /* Witness::from_elements (crates/pcs/src/scheme/witness.rs:54-62): upload n F162. */

@@ -21,6 +21,10 @@
 
 using namespace lbg;
 
+// The fold's per-column tensor-core operands take 67.5 KB a column (276 MB at 4096 columns); wider
+// witnesses fold with k_fold_tc instead.
+constexpr size_t LBG_FOLD_GM_MAX_COLUMNS = 4096;
+
 namespace {
 thread_local std::string g_err;
 
@@ -190,8 +194,18 @@ static int upload_prime(lbg_pp* pp, int k) {
   return LBG_OK;
 }
 
-void lbg_public_parameters_free(lbg_pp* pp) {
-  if (!pp) return;
+void lbg_pp_retain(const lbg_pp* pp) { const_cast<lbg_pp*>(pp)->refs.fetch_add(1); }
+
+static void pp_destroy(lbg_pp* pp);
+void lbg_pp_release(const lbg_pp* pp) {
+  lbg_pp* p = const_cast<lbg_pp*>(pp);
+  if (p && p->refs.fetch_sub(1) == 1) pp_destroy(p);
+}
+
+// The caller's reference; the parameters go once the provers and batches made from them are freed.
+void lbg_public_parameters_free(lbg_pp* pp) { lbg_pp_release(pp); }
+
+static void pp_destroy(lbg_pp* pp) {
   cudaSetDevice(pp->device);
   if (pp->stream) cudaStreamSynchronize(pp->stream);
   cudaFree(pp->d_A);
@@ -435,8 +449,16 @@ static void free_bufs(OpeningBufs* b) {
   delete b;
 }
 
-void lbg_prover_free(lbg_prover* pr) {
-  if (!pr) return;
+static void prover_destroy(lbg_prover* pr);
+static void prover_release(lbg_prover* pr) {
+  if (pr && pr->refs.fetch_sub(1) == 1) prover_destroy(pr);
+}
+
+// The caller's reference; the prover goes once its openings are freed or folded.
+void lbg_prover_free(lbg_prover* pr) { prover_release(pr); }
+
+static void prover_destroy(lbg_prover* pr) {
+  const lbg_pp* pp = pr->pp;
   cudaSetDevice(pr->pp->device);
   if (pr->stream) cudaStreamSynchronize(pr->stream);
   if (pr->copy_stream) {
@@ -472,6 +494,7 @@ void lbg_prover_free(lbg_prover* pr) {
   for (auto e : pr->event_pool) cudaEventDestroy(e);
   if (pr->stream) cudaStreamDestroy(pr->stream);
   delete pr;
+  lbg_pp_release(pp);
 }
 
 // The kept transform of an opening, when the prover keeps it and the device has the room
@@ -527,6 +550,7 @@ int lbg_prover_new(const lbg_pp* pp, lbg_prover** out) {
   LBG_CU(cudaSetDevice(pp->device));
   lbg_prover* pr = new lbg_prover();
   pr->pp = pp;
+  lbg_pp_retain(pp);  // released when the prover goes
   auto bail = [&](int code) {
     lbg_prover_free(pr);
     return code;
@@ -570,7 +594,8 @@ int lbg_prover_new(const lbg_pp* pp, lbg_prover** out) {
       cudaMalloc((void**)&pr->d_chat, pp->cols * N162 * 4) != cudaSuccess ||
       cudaMalloc((void**)&pr->d_v, pp->len_ring * N648 * 2) != cudaSuccess ||
       cudaMalloc((void**)&pr->d_res, (size_t)pp->limbs * count * 2) != cudaSuccess ||
-      (fold_gm_enabled() && cudaMalloc((void**)&pr->d_gm, fold_gm_operand_bytes(pp->cols)) != cudaSuccess)) {
+      (fold_gm_enabled() && pp->cols <= LBG_FOLD_GM_MAX_COLUMNS &&
+       cudaMalloc((void**)&pr->d_gm, fold_gm_operand_bytes(pp->cols)) != cudaSuccess)) {
     cudaGetLastError();
     return bail(fail(LBG_ERR_OOM, "prover workspace: device allocation failed"));
   }
@@ -694,6 +719,7 @@ int lbg_commit(lbg_prover* pr, const lbg_witness* w, int16_t* matrix_out, uint16
   }
   lbg_opening* op = new lbg_opening();
   op->pr = pr;
+  pr->refs.fetch_add(1);
   op->w = const_cast<lbg_witness*>(w);
   op->w->refs.fetch_add(1);
   op->bufs = b;
@@ -926,6 +952,7 @@ int lbg_commit_host(lbg_prover* pr, const uint64_t* f162, size_t n, int16_t* mat
   }
   lbg_opening* op = new lbg_opening();
   op->pr = pr;
+  pr->refs.fetch_add(1);
   op->w = w;
   w->refs.fetch_add(1);
   op->bufs = b;
@@ -1031,14 +1058,16 @@ int lbg_left_expansion(const lbg_pp* pp_c, const uint64_t* row_values, size_t co
 
 void lbg_opening_free(lbg_opening* op) {
   if (!op) return;
+  lbg_prover* pr = op->pr;
   {
-    std::lock_guard<std::mutex> g(op->pr->mu);
-    op->pr->spare.push_back(op->bufs);
+    std::lock_guard<std::mutex> g(pr->mu);
+    pr->spare.push_back(op->bufs);
   }
   // the last reference frees the witness with cudaFree, which waits for the device first
-  cudaSetDevice(op->pr->pp->device);
+  cudaSetDevice(pr->pp->device);
   witness_release(op->w);
   delete op;
+  prover_release(pr);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1099,7 +1128,8 @@ int lbg_fold(lbg_prover* pr, lbg_opening* op, const lbg_challenge* challenges, s
     e = launch_challenge_slots(pp->pidx[0], pr->d_ch, (int)r, pp->d_prime[0], pr->d_chat, st);
   }
   if (e == cudaSuccess) {
-    KernelScope ks(pr, "fold", 2);  // k_fold (or k_fold_kept) + k_fold_finish
+    // k_fold_operand + k_fold_gm + k_fold_finish_t, or k_fold_tc (k_fold, k_fold_kept) + the finish
+    KernelScope ks(pr, "fold", (pr->d_gm && !op->bufs->d_keep) ? 3 : 2);
     if (op->bufs->d_keep)
       e = launch_fold_kept(pp->pidx[0], op->bufs->d_keep, pp->wdim, (int)pp->cols, pr->fold_cols_per_split,
                            pr->d_chat, pp->d_prime[0], pr->d_vhat, pr->d_v, st);

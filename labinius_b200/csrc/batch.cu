@@ -402,7 +402,9 @@ void lbg_batch_free(lbg_batch* b) {
   b->ab_commit.release();
   b->ab_u.release();
   if (b->stream) cudaStreamDestroy(b->stream);
+  const lbg_pp* pp = b->pp;
   delete b;
+  lbg_pp_release(pp);
 }
 
 // The device bytes lbg_batch_new_capacity allocates for an arena of this size (the buffers below,
@@ -462,6 +464,7 @@ int lbg_batch_new_capacity(const lbg_pp* pp, size_t max_cols, size_t max_instanc
   if (max_cols > ((size_t)1 << 30) / pp->wdim) return fail(LBG_ERR_PARAMS, "batch too large");
   lbg_batch* b = new lbg_batch();
   b->pp = pp;
+  lbg_pp_retain(pp);  // released when the batch goes
   b->wdim = pp->wdim;
   b->len_ring = pp->len_ring;
   b->cap_cols = max_cols;

@@ -18,6 +18,9 @@ using lbg::lbg_challenge_d;
 using lbg::Transcript;
 
 struct lbg_pp {
+  // references: the caller's, and one per prover and batch made from it, so that the handles may be
+  // freed in any order (a garbage collector finalizes a cycle in no fixed order)
+  std::atomic<int> refs{1};
   lbg_params params;
   int limbs = 0;
   uint32_t primes[7];
@@ -50,6 +53,9 @@ struct lbg_pp {
 
 // Frees the switch prover's workspace of pp (switch.cu).
 void lbg_switch_release(lbg_pp* pp);
+// A reference to pp taken by a prover or batch, and its release (the last one frees pp).
+extern "C" void lbg_pp_retain(const lbg_pp* pp);
+extern "C" void lbg_pp_release(const lbg_pp* pp);
 
 struct lbg_witness {
   std::atomic<int> refs{1};
@@ -61,6 +67,7 @@ struct lbg_witness {
 struct OpeningBufs;
 
 struct lbg_prover {
+  std::atomic<int> refs{1};  // the caller's, and one per live opening
   const lbg_pp* pp = nullptr;
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream = nullptr;        // lbg_commit_host's uploads (created on first use)

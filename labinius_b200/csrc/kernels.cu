@@ -2637,12 +2637,12 @@ bool fold_tc_enabled() {
 }
 int fold_tc_positions_per_cta() { return TCF_ROWS; }
 
-// The single prover's fold takes k_fold_gm (the challenge in the multiply's operand) when
-// LBG_FOLD_KERNEL=gm.
+// The single prover's fold takes k_fold_gm (the challenge in the multiply's operand) unless
+// LBG_FOLD_KERNEL=tc (k_fold_tc) or scalar (k_fold) selects another (all exact).
 bool fold_gm_enabled() {
   static const bool on = [] {
     const char* e = getenv("LBG_FOLD_KERNEL");
-    return e && std::string(e) == "gm";
+    return !(e && (std::string(e) == "tc" || std::string(e) == "scalar"));
   }();
   return on;
 }

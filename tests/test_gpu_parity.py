@@ -311,3 +311,36 @@ def test_commit_from_pageable_and_page_locked_memory_agree():
         assert np.array_equal(c.matrix, c1.matrix)
         prover.recycle(op)
         prover.recycle(op1)
+
+
+def test_handles_free_in_any_order():
+    """Parameters freed before their prover, and a prover freed before its opening, stay valid until
+    the last handle that uses them goes (a garbage collector finalizes a cycle in no fixed order):
+    the opening still folds to the oracle's folded witness afterwards."""
+    import ctypes
+
+    import labinius_b200 as L
+    import oracle as O
+    from labinius_b200._native import LBG_OK, lib, ptr
+    from rounds import MATRIX_SEED, WITNESS_SEED, product_params
+
+    shape = (12, 4, [3889, 9721], 0)
+    params = product_params(shape)
+    N = lib()
+    pp, pr, w, op = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    p = params.native()
+    assert N.lbg_public_parameters_from_seed(ctypes.byref(p), ptr(np.frombuffer(MATRIX_SEED, np.uint8).copy()),
+                                             ctypes.byref(pp)) == LBG_OK
+    assert N.lbg_prover_new(pp, ctypes.byref(pr)) == LBG_OK
+    assert N.lbg_witness_random(pp, ptr(np.frombuffer(WITNESS_SEED, np.uint8).copy()), ctypes.byref(w)) == LBG_OK
+    assert N.lbg_commit(pr, w, None, None, None, ctypes.byref(op)) == LBG_OK
+    N.lbg_public_parameters_free(pp)  # the prover still holds the parameters
+    N.lbg_witness_free(w)             # the opening still holds the witness
+    N.lbg_prover_free(pr)             # the opening still holds the prover
+    ch = np.zeros(params.columns(), L.CHALLENGE_DTYPE)
+    ch["weight"] = 28
+    ch["positions"][:, :28] = (np.arange(28) * 5 + 2).astype(np.uint8)
+    v = np.zeros((params.len_ring(), 648), np.int16)
+    assert N.lbg_fold(pr, op, ptr(ch), len(ch), ptr(v)) == LBG_OK  # frees the opening, then the prover
+    P = O.Params(*shape[:3])
+    assert np.array_equal(v, O.fold(P, O.witness_random(P.witness_len, WITNESS_SEED), ch))
