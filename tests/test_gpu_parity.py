@@ -344,3 +344,28 @@ def test_handles_free_in_any_order():
     assert N.lbg_fold(pr, op, ptr(ch), len(ch), ptr(v)) == LBG_OK  # frees the opening, then the prover
     P = O.Params(*shape[:3])
     assert np.array_equal(v, O.fold(P, O.witness_random(P.witness_len, WITNESS_SEED), ch))
+
+
+def test_fold_of_a_wide_prover_matches_oracle():
+    """A prover of 8192 columns (more than the fold's per-column operands are kept for) folds through
+    the kernel that weights each column's transform on the CUDA cores; a 512-column prover through
+    the operand-folded kernel, with column splits capped at 512. Both equal the oracle's fold."""
+    import labinius_b200 as L
+    import oracle as O
+    from rounds import MATRIX_SEED, WITNESS_SEED, product_params
+
+    for shape in [(20, 13, [3889], 0), (16, 9, [9721, 3889], 0)]:
+        params = product_params(shape)
+        pp = L.PublicParameters.from_seed(params, MATRIX_SEED)
+        prover = L.Prover(pp)
+        _, op = prover.commit(L.Witness.random(pp, WITNESS_SEED))
+        rng = np.random.default_rng(shape[1])
+        ch = L.FoldingChallenges(np.zeros(params.columns(), L.CHALLENGE_DTYPE))
+        ch.challenges["weight"] = 28
+        for j in range(params.columns()):
+            ch.challenges["positions"][j, :28] = np.sort(rng.choice(162, 28, replace=False)).astype(np.uint8)
+        ch.challenges["signs"] = rng.integers(0, 2 ** 32, params.columns(), dtype=np.uint64).astype(np.uint32)
+        v = prover.fold(op, ch).elements
+        P = O.Params(*shape[:3])
+        want = O.fold(P, O.witness_random(P.witness_len, WITNESS_SEED), ch.challenges, threads=8)
+        assert np.array_equal(v, want), shape
