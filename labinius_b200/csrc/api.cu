@@ -225,6 +225,7 @@ static void pp_destroy(lbg_pp* pp) {
   cudaFree(pp->d_fc);
   cudaFree(pp->d_wire);
   cudaFree(pp->d_lift);
+  cudaFree(pp->d_vws);
   lbg_switch_release(pp);
   if (pp->stream) cudaStreamDestroy(pp->stream);
   delete pp;
@@ -1216,6 +1217,26 @@ int lbg_verify_evaluation(const lbg_pp* pp_c, const uint64_t* p1, size_t p1_len,
 // centred within the base modulus and its squared norm within fold_cap (params.rs:259-265), A v
 // equal to the folded commitment on every limb, and eq(p0) . (v mod 2) equal to the folded row
 // value. Device scratch is allocated per call (a verifier's call, not the prover's hot path).
+// The verifier's device scratch: one buffer kept in the parameters (grown on use, under pp->mu) and
+// carved per call, so that a verification allocates and frees nothing once it has run.
+extern "C++" {
+struct Carve {
+  uint8_t* base;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t bytes) {
+    T* p = reinterpret_cast<T*>(base + off);
+    off += (bytes + 255) & ~(size_t)255;
+    return p;
+  }
+};
+static size_t carve_size(std::initializer_list<size_t> parts) {
+  size_t n = 0;
+  for (size_t b : parts) n += (b + 255) & ~(size_t)255;
+  return n;
+}
+}  // extern "C++"
+
 int lbg_verify_folded_opening(const lbg_pp* pp_c, const int16_t* folded_commitment, const int16_t* v,
                               const uint64_t* p0, size_t p0_len, const uint64_t folded_row_value[3],
                               int* accepted) {
@@ -1231,25 +1252,16 @@ int lbg_verify_folded_opening(const lbg_pp* pp_c, const int16_t* folded_commitme
   LBG_CU(cudaSetDevice(pp->device));
   cudaStream_t st = pp->stream;
   size_t L = pp->len_ring, nv = L * N648, fcn = 4 * (size_t)pp->limbs * N162;
-  int16_t* d_v = nullptr;
-  int16_t* d_fc = nullptr;
-  uint32_t* d_vhat = nullptr;
-  uint64_t* d_bits = nullptr;
-  VerifyFlags* d_f = nullptr;
-  auto release = [&]() {
-    cudaFree(d_v);
-    cudaFree(d_fc);
-    cudaFree(d_vhat);
-    cudaFree(d_bits);
-    cudaFree(d_f);
-  };
-  if (cudaMalloc((void**)&d_v, nv * 2) != cudaSuccess || cudaMalloc((void**)&d_fc, fcn * 2) != cudaSuccess ||
-      cudaMalloc((void**)&d_vhat, nv * 4) != cudaSuccess || cudaMalloc((void**)&d_bits, 4 * L * 24) != cudaSuccess ||
-      cudaMalloc((void**)&d_f, sizeof(VerifyFlags)) != cudaSuccess) {
-    cudaGetLastError();
-    release();
-    return fail(LBG_ERR_OOM, "verifier: device allocation failed");
-  }
+  int rc = grow((void**)&pp->d_vws, &pp->vws_cap,
+                carve_size({nv * 2, fcn * 2, nv * 4, 4 * L * 24, sizeof(VerifyFlags)}));
+  if (rc) return rc;
+  Carve cv{pp->d_vws};
+  int16_t* d_v = cv.take<int16_t>(nv * 2);
+  int16_t* d_fc = cv.take<int16_t>(fcn * 2);
+  uint32_t* d_vhat = cv.take<uint32_t>(nv * 4);
+  uint64_t* d_bits = cv.take<uint64_t>(4 * L * 24);
+  VerifyFlags* d_f = cv.take<VerifyFlags>(sizeof(VerifyFlags));
+  auto release = [] {};
   cudaError_t e = cudaMemcpyAsync(d_v, v, nv * 2, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_fc, folded_commitment, fcn * 2, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_f, 0, sizeof(VerifyFlags), st);
@@ -1297,26 +1309,22 @@ int lbg_verify_folded_opening_bd(const lbg_pp* pp_c, const uint16_t* top, const 
   LBG_CU(cudaSetDevice(pp->device));
   cudaStream_t st = pp->stream;
   size_t Lr = pp->len_ring, nv = Lr * N648, count = pp->cols * N648;
-  int16_t* d_v = nullptr;
-  uint16_t* d_top = nullptr;
-  uint16_t* d_digits = nullptr;
-  uint32_t *d_vhat = nullptr, *d_diff = nullptr, *d_res = nullptr;
-  uint64_t* d_bits = nullptr;
-  unsigned long long* d_ns = nullptr;
-  VerifyFlags* d_f = nullptr;
-  auto release = [&]() {
-    void* ptrs[] = {d_v, d_top, d_digits, d_vhat, d_diff, d_res, d_bits, d_ns, d_f};
-    for (void* q : ptrs) cudaFree(q);
-  };
-  if (cudaMalloc((void**)&d_v, nv * 2) != cudaSuccess || cudaMalloc((void**)&d_top, count * 2) != cudaSuccess ||
-      cudaMalloc((void**)&d_digits, (size_t)(L > 1 ? L - 1 : 1) * count * 2) != cudaSuccess ||
-      cudaMalloc((void**)&d_vhat, nv * 4) != cudaSuccess || cudaMalloc((void**)&d_diff, 4 * N162 * 4) != cudaSuccess ||
-      cudaMalloc((void**)&d_res, (size_t)L * N648 * 4) != cudaSuccess || cudaMalloc((void**)&d_bits, 4 * Lr * 24) != cudaSuccess ||
-      cudaMalloc((void**)&d_ns, 16) != cudaSuccess || cudaMalloc((void**)&d_f, sizeof(VerifyFlags)) != cudaSuccess) {
-    cudaGetLastError();
-    release();
-    return fail(LBG_ERR_OOM, "verifier: device allocation failed");
-  }
+  const size_t ndig = (size_t)(L > 1 ? L - 1 : 1) * count * 2;
+  int rc = grow((void**)&pp->d_vws, &pp->vws_cap,
+                carve_size({nv * 2, count * 2, ndig, nv * 4, 4 * N162 * 4, (size_t)L * N648 * 4, 4 * Lr * 24, 16,
+                            sizeof(VerifyFlags)}));
+  if (rc) return rc;
+  Carve cv{pp->d_vws};
+  int16_t* d_v = cv.take<int16_t>(nv * 2);
+  uint16_t* d_top = cv.take<uint16_t>(count * 2);
+  uint16_t* d_digits = cv.take<uint16_t>(ndig);
+  uint32_t* d_vhat = cv.take<uint32_t>(nv * 4);
+  uint32_t* d_diff = cv.take<uint32_t>(4 * N162 * 4);
+  uint32_t* d_res = cv.take<uint32_t>((size_t)L * N648 * 4);
+  uint64_t* d_bits = cv.take<uint64_t>(4 * Lr * 24);
+  unsigned long long* d_ns = cv.take<unsigned long long>(16);
+  VerifyFlags* d_f = cv.take<VerifyFlags>(sizeof(VerifyFlags));
+  auto release = [] {};
   GarnerConsts gc;
   std::memset(&gc, 0, sizeof(gc));
   for (int k = 0; k < L; k++) {

@@ -49,6 +49,8 @@ struct lbg_pp {
   size_t wire_cap = 0;
   int16_t* d_lift = nullptr;   // lbg_left_expansion's vector (grown on use)
   size_t lift_cap = 0;
+  uint8_t* d_vws = nullptr;    // the verifier's scratch (grown on use, carved per call)
+  size_t vws_cap = 0;
 };
 
 // Frees the switch prover's workspace of pp (switch.cu).
