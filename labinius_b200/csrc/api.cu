@@ -185,10 +185,20 @@ static int upload_prime(lbg_pp* pp, int k) {
   if (e == cudaSuccess) e = upload_sync(pp->d_prime[k], D, sizeof(DevPrime));
   delete D;
   if (e == cudaSuccess) {
-    std::vector<uint8_t> tcb(TC_B_BYTES);
+    // the transform as the tensor-core operand, followed by the same T[m][v] as plain u16 rows
+    // (TC_T16_BYTES: row v, m = 0..175, zero past 161) for the fold's operand builder
+    std::vector<uint8_t> tcb(TC_B_BYTES + TC_T16_BYTES, 0);
     tc_transform_operand(T, tcb.data());
-    e = cudaMalloc((void**)&pp->d_tcb[k], TC_B_BYTES);
-    if (e == cudaSuccess) e = upload_sync(pp->d_tcb[k], tcb.data(), TC_B_BYTES);
+    uint16_t* t16 = reinterpret_cast<uint16_t*>(tcb.data() + TC_B_BYTES);
+    for (int v = 0; v < N162; v++) {
+      uint64_t x = 1;
+      for (int m = 0; m < N162; m++) {
+        t16[v * TC_LEAVES + m] = (uint16_t)x;
+        x = x * T.theta_leaf[v] % T.q;
+      }
+    }
+    e = cudaMalloc((void**)&pp->d_tcb[k], tcb.size());
+    if (e == cudaSuccess) e = upload_sync(pp->d_tcb[k], tcb.data(), tcb.size());
   }
   if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("prime tables: ") + cudaGetErrorString(e));
   return LBG_OK;

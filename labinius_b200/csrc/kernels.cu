@@ -1199,7 +1199,8 @@ constexpr int GM_MAX_COLS_PER_SPLIT = 512;
 // One thread per (column j, row v of N, 16-byte chunk c of K): the chunk's 16 bytes of G_j.
 template <int PI>
 __global__ void k_fold_operand(const uint32_t* __restrict__ chat /* [cols][162] */, int cols,
-                               const uint8_t* __restrict__ tcb /* T, TC_B_BYTES */, uint8_t* __restrict__ G) {
+                               const uint8_t* __restrict__ tcb /* T: the operand, then u16 rows */,
+                               uint8_t* __restrict__ G) {
   constexpr uint32_t q = Pr<PI>::q;
   const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   constexpr int CHUNKS = TC_KBYTES / 16;  // 24
@@ -1210,17 +1211,18 @@ __global__ void k_fold_operand(const uint32_t* __restrict__ chat /* [cols][162] 
   const int kb0 = 16 * c;
   const bool hi = kb0 >= 192;
   uint32_t bytes[4] = {0, 0, 0, 0};
-  if (v < N162) {
+  const int m0 = hi ? kb0 - 192 : kb0;
+  if (v < N162 && m0 < N162) {
     const uint32_t cv = chat[(size_t)j * N162 + v];
+    // T[m0 .. m0 + 15][v]: 32 bytes of the plain table after the operand (zero past m = 161)
+    const uint4* trow = reinterpret_cast<const uint4*>(tcb + TC_B_BYTES) + ((size_t)v * TC_LEAVES + m0) / 8;
+    const uint4 ta = trow[0], tb = trow[1];
+    const uint32_t tw[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
 #pragma unroll
     for (int x = 0; x < 16; x++) {
-      const int m = (hi ? kb0 - 192 : kb0) + x;
-      if (m < N162) {
-        const uint32_t t = (uint32_t)tcb[tc_swizzled_offset(v, m, TC_LEAVES)] +
-                           128u * (uint32_t)tcb[tc_swizzled_offset(v, 192 + m, TC_LEAVES)];
-        const uint32_t g = red_full<PI>(cv * t);
-        bytes[x >> 2] |= (hi ? g >> 7 : g & 127u) << (8 * (x & 3));
-      }
+      const uint32_t t = (tw[x >> 1] >> (16 * (x & 1))) & 0xFFFFu;
+      const uint32_t g = red_full<PI>(cv * t);
+      bytes[x >> 2] |= (hi ? g >> 7 : g & 127u) << (8 * (x & 3));
     }
   }
   *(uint4*)(G + (size_t)j * TC_B_BYTES + tc_swizzled_offset(v, kb0, TC_LEAVES)) =

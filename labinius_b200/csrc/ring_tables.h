@@ -90,6 +90,7 @@ constexpr int TC_LEAVES = 176;          // N of the transform multiply
 constexpr int TC_KBYTES = 384;          // K of the transform multiply, in bytes
 constexpr int TC_ATOM = 1024;           // one swizzle atom: 8 rows x 128 bytes
 constexpr int TC_B_BYTES = TC_LEAVES * TC_KBYTES;  // 67584
+constexpr int TC_T16_BYTES = TC_LEAVES * TC_LEAVES * 2;  // T[m][v] as u16 rows of 176 (v) x 176 (m)
 // Byte offset of (row, K-byte kb) in a K-major, 128-byte-swizzled operand of `rows` rows (a
 // multiple of 8): the K-atoms (128 bytes of K) one after another, each holding all row groups.
 #ifdef __CUDACC__
