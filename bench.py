@@ -677,12 +677,6 @@ def run_served(requests, plain_sample, load=0.7, slots=3, seed=2027, server_kw=N
         return elems / (last - first), len(idx) / (last - first), lat, np.array([int(logs[i]) for i in idx])
 
     run(range(min(64, requests)), None)  # warm-up: arenas, graphs of the host pool
-    # the objects the bench made so far move to the collector's permanent generation, so that its
-    # collections during the stream walk only the requests' own objects
-    import gc
-
-    gc.collect()
-    gc.freeze()
     sat_n = min(requests, 2000)
     sat_elems, sat_reqs, _, _ = run(range(sat_n), None)
     rate = load * sat_reqs
@@ -690,7 +684,6 @@ def run_served(requests, plain_sample, load=0.7, slots=3, seed=2027, server_kw=N
     st_elems, st_reqs, lat, lat_logs = run(range(requests), rate)
     batches = srv.batches - b0
     srv.close()
-    gc.unfreeze()
     if plain_sample == 0:
         return {"rate_req_s": rate, "batches": batches, "throughput_elems_s": st_elems,
                 "saturated_elems_s": sat_elems, "p50_ms": float(np.percentile(lat, 50)),
