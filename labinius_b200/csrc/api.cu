@@ -397,8 +397,7 @@ int lbg_witness_random(const lbg_pp* pp, const uint8_t seed[32], lbg_witness** o
                 ((uint32_t)msg[4 * i + 3] << 24);
   root.block_len = 16;
   root.flags = 16 | 1 | 2 | 8;  // keyed hash, chunk start, chunk end, root
-  cudaError_t e = launch_xof(root, pp->n * 24, (uint8_t*)w->d, pp->stream);
-  if (e == cudaSuccess) e = launch_mask_f162(w->d, pp->n, pp->stream);
+  cudaError_t e = launch_xof_f162(root, pp->n, w->d, pp->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(pp->stream);
   if (e != cudaSuccess) {
     witness_release(w);

@@ -618,8 +618,7 @@ int lbg_batch_witness_generate(lbg_batch* b, const uint8_t* seeds, const uint8_t
     if (kinds && kinds[i] == 1) {
       LBG_BCU(launch_xof_lifted(keyed_root(seeds + 32 * i, "labinius/b128-trace"), n, dst, b->stream));
     } else {
-      LBG_BCU(launch_xof(keyed_root(seeds + 32 * i, "labinius/witness"), n * 24, (uint8_t*)dst, b->stream));
-      LBG_BCU(launch_mask_f162(dst, n, b->stream));
+      LBG_BCU(launch_xof_f162(keyed_root(seeds + 32 * i, "labinius/witness"), n, dst, b->stream));
     }
   }
   LBG_BCU(cudaStreamSynchronize(b->stream));

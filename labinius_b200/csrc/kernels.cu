@@ -2299,11 +2299,48 @@ __global__ void k_xof_blocks(XofRoot root, size_t nbytes, uint8_t* __restrict__ 
 
 // A B128 trace from the XOF (16 bytes per element, little-endian), lifted as it is produced:
 // block t holds elements 4t .. 4t+3, written as F162 [lo, hi, 0] (crates/pcs/src/fields/scalar.rs:72-74).
+// Witness::random's words (crates/pcs/src/scheme/witness.rs:66-87): XOF block t is bytes 64 t .. 64 t +
+// 63 of the F162 array, the third limb of every element masked to 34 bits on the way (the word at
+// byte 20 of an element keeps its low two bits, the one at byte 16 is bits 0-31 of the limb), and
+// the block written as four 16-byte stores (16-byte aligned: W from cudaMalloc, instances at whole
+// columns).
+__global__ void k_xof_f162(XofRoot root, size_t n, uint64_t* __restrict__ W) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t nbytes = 24 * n;
+  if (t * 64 >= nbytes) return;
+  uint32_t o[16];
+  xof_block(root, t, o);
+  const int r0 = (int)(t % 3) * 16;  // 64 t mod 24
+#pragma unroll
+  for (int w = 0; w < 16; w++)
+    if ((r0 + 4 * w) % 24 == 20) o[w] &= 3u;
+  uint8_t* out = reinterpret_cast<uint8_t*>(W) + t * 64;
+  if (t * 64 + 64 <= nbytes) {
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      reinterpret_cast<uint4*>(out)[q] = make_uint4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+  } else {
+    // the last, partial block: whole words (24 n is a multiple of 8)
+    for (int w = 0; w < 16 && t * 64 + 4 * w < nbytes; w++) reinterpret_cast<uint32_t*>(out)[w] = o[w];
+  }
+}
+
 __global__ void k_xof_lifted(XofRoot root, size_t n, uint64_t* __restrict__ W) {
   size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t * 4 >= n) return;
   uint32_t o[16];
   xof_block(root, t, o);
+  if (4 * t + 4 <= n) {
+    // four whole elements, 96 bytes from byte 96 t: six 16-byte stores
+    uint4* d = reinterpret_cast<uint4*>(W + 12 * t);
+    d[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    d[1] = make_uint4(0, 0, o[4], o[5]);
+    d[2] = make_uint4(o[6], o[7], 0, 0);
+    d[3] = make_uint4(o[8], o[9], o[10], o[11]);
+    d[4] = make_uint4(0, 0, o[12], o[13]);
+    d[5] = make_uint4(o[14], o[15], 0, 0);
+    return;
+  }
   for (int k = 0; k < 4; k++) {
     size_t e = 4 * t + k;
     if (e >= n) break;
@@ -2897,6 +2934,12 @@ cudaError_t launch_fold_binary(const uint64_t* u, const lbg_challenge_d* ch, int
 cudaError_t launch_xof(const XofRoot& root, size_t nbytes, uint8_t* out, cudaStream_t st) {
   size_t blocks = (nbytes + 63) / 64;
   k_xof_blocks<<<blocks_for(blocks, 128), 128, 0, st>>>(root, nbytes, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_xof_f162(const XofRoot& root, size_t n, uint64_t* W, cudaStream_t st) {
+  size_t blocks = (24 * n + 63) / 64;
+  k_xof_f162<<<blocks_for(blocks, 128), 128, 0, st>>>(root, n, W);
   return cudaGetLastError();
 }
 

@@ -139,6 +139,8 @@ cudaError_t launch_ntt648(int pi, bool inverse, const uint16_t* in, uint16_t* ou
                           const Ntt648Tables* T, cudaStream_t st);
 cudaError_t launch_claim(const uint64_t* u, int cols, const uint64_t* p1, int n, uint64_t* out, cudaStream_t st);
 cudaError_t launch_xof(const XofRoot& root, size_t nbytes, uint8_t* out, cudaStream_t st);
+// Witness::random: the XOF bytes as F162 words, the third limb masked to 34 bits, in one pass.
+cudaError_t launch_xof_f162(const XofRoot& root, size_t n, uint64_t* W, cudaStream_t st);
 cudaError_t launch_mask_f162(uint64_t* W, size_t n, cudaStream_t st);
 // n B128 elements of a keyed XOF written lifted into F162 [lo, hi, 0].
 cudaError_t launch_xof_lifted(const XofRoot& root, size_t n, uint64_t* W, cudaStream_t st);
