@@ -70,6 +70,7 @@ struct lbg_batch {
   lbg_challenge_d* d_ch = nullptr;
   uint32_t* d_chat = nullptr;     // [total_cols][162]
   uint32_t* d_vhat = nullptr;     // [count][wdim][162]
+  uint8_t* d_gm = nullptr;        // the fold's per-column tensor-core operands (k_fold_gm)
   int16_t* d_v = nullptr;         // [count][len_ring][648]
   bool graphs = false;
   int sm_cap = 0;                 // CTAs of the persistent commit and fold launches (0: one per SM)
@@ -114,6 +115,11 @@ static void free_graphs(lbg_batch* b) {
 }
 
 // The device work of each stage, enqueued on the batch's stream (also what the graphs capture).
+// Batches of at most 32768 columns fold with the challenges in the tensor-core operand (k_fold_gm:
+// 67.5 KB of operand a column, 2.2 GB at the limit); wider ones weight the transforms on the CUDA
+// cores (k_fold_tc).
+static bool batch_fold_gm(size_t max_cols) { return fold_gm_enabled() && max_cols <= 32768; }
+
 // The batch's cap on the persistent kernels' CTAs, for the launches enqueued in its scope.
 struct CapScope {
   explicit CapScope(int ctas, int warps = 0) {
@@ -164,10 +170,13 @@ static cudaError_t enqueue_fold(lbg_batch* b) {
   if (e == cudaSuccess && b->keep)
     e = launch_fold_kept(pp->pidx[0], b->d_keep, b->wdim, (int)b->total_cols, b->fold_per, b->d_chat,
                          pp->d_prime[0], b->d_vhat, b->d_v, b->stream, b->count, b->d_split_inst);
+  else if (e == cudaSuccess && b->d_gm)
+    e = launch_fold_gm(pp->pidx[0], b->d_w, b->wdim, (int)b->total_cols, b->fold_per, b->d_chat, pp->d_tcb[0],
+                       b->d_gm, pp->d_prime[0], b->d_vhat, b->d_v, b->stream, b->count, b->d_split_inst);
   else if (e == cudaSuccess)
     e = launch_fold(pp->pidx[0], b->d_w, b->wdim, (int)b->total_cols, b->fold_per, b->d_chat, pp->d_prime[0],
                     b->d_vhat, b->d_v, b->stream, b->count, b->d_split_inst, pp->d_tcb[0]);
-  b->launches += 3;
+  b->launches += (b->d_gm && !b->keep) ? 4 : 3;
   return e;
 }
 
@@ -397,7 +406,7 @@ void lbg_batch_free(lbg_batch* b) {
   void* ptrs[] = {b->d_w, b->d_col_inst, b->d_row_tiles, b->d_split_inst, b->d_partial, b->d_C, b->d_res, b->d_top, b->d_digits,
                   b->d_p0, b->d_p1, b->d_eq, b->d_u, b->d_claim, b->d_ch, b->d_chat, b->d_vhat, b->d_v,
                   b->d_prefix, b->d_states, b->d_inst, b->d_oldcv, b->d_stage, b->d_cvs, b->d_packed, b->d_keep,
-                  b->d_sw_inst, b->d_sw_small, b->d_sw_scratch, b->d_sw_r};
+                  b->d_sw_inst, b->d_sw_small, b->d_sw_scratch, b->d_sw_r, b->d_gm};
   for (void* p : ptrs) cudaFree(p);
   b->ab_commit.release();
   b->ab_u.release();
@@ -419,7 +428,8 @@ size_t lbg_batch_arena_bytes(const lbg_pp* pp, size_t max_cols, size_t max_insta
   return C * wdim * 24 + C * sizeof(int) + C * sizeof(int4) + C * sizeof(int) + chunks * C * N162 * 16 +
          C * 4 * L * N162 * 2 + L * count648 * 2 + count648 * 2 + (L > 1 ? L - 1 : 1) * count648 * 2 + I * 32 * 24 * 2 +
          I * wdim * 24 + C * 24 + I * 24 + C * sizeof(lbg_challenge_d) + C * N162 * 4 + I * wdim * N162 * 4 +
-         I * pp->len_ring * N648 * 2 + 2 * I * sizeof(HasherState) + I * sizeof(RoundInst) + I * 32;
+         I * pp->len_ring * N648 * 2 + 2 * I * sizeof(HasherState) + I * sizeof(RoundInst) + I * 32 +
+         (batch_fold_gm(C) ? fold_gm_operand_bytes(C) : 0);
 }
 
 // The batch's stream at the device's greatest (high != 0) or default priority: when both are
@@ -500,7 +510,8 @@ int lbg_batch_new_capacity(const lbg_pp* pp, size_t max_cols, size_t max_instanc
             cudaMalloc((void**)&b->d_prefix, I * sizeof(HasherState)) == cudaSuccess &&
             cudaMalloc((void**)&b->d_states, I * sizeof(HasherState)) == cudaSuccess &&
             cudaMalloc((void**)&b->d_inst, I * sizeof(RoundInst)) == cudaSuccess &&
-            cudaMalloc((void**)&b->d_oldcv, I * 32) == cudaSuccess;
+            cudaMalloc((void**)&b->d_oldcv, I * 32) == cudaSuccess &&
+            (!batch_fold_gm(C) || cudaMalloc((void**)&b->d_gm, fold_gm_operand_bytes(C)) == cudaSuccess);
   if (!ok) {
     cudaGetLastError();
     return bail(fail(LBG_ERR_OOM, "batch: device allocation failed"));
@@ -843,7 +854,7 @@ int lbg_batch_fold(lbg_batch* b, const lbg_challenge* challenges, size_t r, int1
   LBG_BCU(cudaMemcpyAsync(b->d_ch, challenges, r * sizeof(lbg_challenge), cudaMemcpyHostToDevice, b->stream));
   if (b->graphs) {
     LBG_BCU(cudaGraphLaunch(b->g_fold, b->stream));
-    b->launches += 3;
+    b->launches += (b->d_gm && !b->keep) ? 4 : 3;
   } else {
     LBG_BCU(enqueue_fold(b));
   }
@@ -866,7 +877,7 @@ int lbg_batch_round(lbg_batch* b, const uint8_t* domain, size_t domain_len, cons
     int rc = plan_round(b, domain, domain_len);
     if (rc) return rc;
   }
-  uint64_t per_round = 11 + 2 * pp->limbs + 3 +
+  uint64_t per_round = 11 + 2 * pp->limbs + ((b->d_gm && !b->keep) ? 4 : 3) +
                        (pp->params.opening == LBG_OPENING_BIT_DROPPED ? pp->limbs + 1 + b->count : 0);
   per_round += sw_launches(b->sw_h.data(), (int)b->sw_h.size());
   if (b->graphs) {

@@ -1273,7 +1273,8 @@ __device__ __forceinline__ void gm_mma(uint32_t d_tmem, uint32_t sA_u, uint32_t 
 template <int PI>
 __global__ void __launch_bounds__(GM_THREADS, 1)
     k_fold_gm(const uint64_t* __restrict__ W, size_t wdim, int cols, int cols_per_split,
-              const uint8_t* __restrict__ G, uint32_t* __restrict__ vhat_t) {
+              const uint8_t* __restrict__ G, uint32_t* __restrict__ vhat_t,
+              const int* __restrict__ split_inst /* null: one instance */) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);  // swizzle atoms
   uint8_t* sB = smem;                                                           // [2] G_j
@@ -1374,7 +1375,8 @@ __global__ void __launch_bounds__(GM_THREADS, 1)
       const GmCursor& it = curs[s & 3];
       const uint32_t taddr = tmem + (uint32_t)it.acc * 256u + ((uint32_t)(32 * quad) << 16) + v0;
       const size_t p0 = (size_t)it.c.tile * TCF_ROWS;
-      uint32_t* d = vhat_t + p0 + row + (size_t)v0 * wdim;
+      uint32_t* d = vhat_t + (split_inst ? (size_t)split_inst[it.c.split] * wdim * N162 : 0) + p0 + row +
+                    (size_t)v0 * wdim;
       const bool inside = p0 + row < wdim;
 #pragma unroll
       for (int bt = 0; bt < 7; bt++) {
@@ -2689,20 +2691,24 @@ size_t fold_gm_operand_bytes(size_t cols) { return cols * (size_t)TC_B_BYTES; }
 
 cudaError_t launch_fold_gm(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
                            const uint8_t* tcb, uint8_t* G, const DevPrime* D, uint32_t* vhat, int16_t* v,
-                           cudaStream_t st) {
+                           cudaStream_t st, int instances, const int* split_inst) {
   if (cols <= 0 || cols_per_split <= 0) return cudaErrorInvalidValue;
-  cols_per_split = std::min(cols_per_split, GM_MAX_COLS_PER_SPLIT);
+  // one instance: splits of at most 512 columns; instances laid out one after another: the caller's
+  // splits (split_inst maps each to its instance; each at most 512 columns)
+  if (!split_inst) cols_per_split = std::min(cols_per_split, GM_MAX_COLS_PER_SPLIT);
+  if (cols_per_split > GM_MAX_COLS_PER_SPLIT) return cudaErrorInvalidValue;
   const int splits = (cols + cols_per_split - 1) / cols_per_split;
   const long items = (long)((wdim + TCF_ROWS - 1) / TCF_ROWS) * splits;
   dim3 grid((unsigned)std::max<long>(1, std::min<long>(items, persistent_ctas())));
-  cudaError_t e = cudaMemsetAsync(vhat, 0, wdim * N162 * sizeof(uint32_t), st);
+  const size_t positions = wdim * (size_t)instances;
+  cudaError_t e = cudaMemsetAsync(vhat, 0, positions * N162 * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   const size_t nop = (size_t)cols * TC_LEAVES * (TC_KBYTES / 16);
   LBG_DISPATCH(pi, ({
                  k_fold_operand<P><<<blocks_for(nop, 256), 256, 0, st>>>(chat, cols, tcb, G);
                  cudaFuncSetAttribute(k_fold_gm<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, GM_SMEM);
-                 k_fold_gm<P><<<grid, GM_THREADS, GM_SMEM, st>>>(W, wdim, cols, cols_per_split, G, vhat);
-                 k_fold_finish_t<P><<<blocks_for(wdim, 4), 216, 0, st>>>(vhat, wdim, wdim, D, v);
+                 k_fold_gm<P><<<grid, GM_THREADS, GM_SMEM, st>>>(W, wdim, cols, cols_per_split, G, vhat, split_inst);
+                 k_fold_finish_t<P><<<blocks_for(positions, 4), 216, 0, st>>>(vhat, wdim, positions, D, v);
                }));
   return cudaGetLastError();
 }

@@ -81,7 +81,7 @@ bool fold_gm_enabled();
 size_t fold_gm_operand_bytes(size_t cols);
 cudaError_t launch_fold_gm(int pi, const uint64_t* W, size_t wdim, int cols, int cols_per_split, const uint32_t* chat,
                            const uint8_t* tcb, uint8_t* G, const DevPrime* D, uint32_t* vhat, int16_t* v,
-                           cudaStream_t st);
+                           cudaStream_t st, int instances = 1, const int* split_inst = nullptr);
 bool fold_tc_enabled();
 int fold_tc_positions_per_cta();
 // The fold from the commit's kept transform instead of the witness (same splits and outputs).
