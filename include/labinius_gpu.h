@@ -260,8 +260,9 @@ size_t lbg_params_pack_dropped(const lbg_params* p, const uint16_t* top, const u
  * an embedding runtime that owns all device memory, or replays its steps where allocator calls
  * are not allowed, folds through this entry point, which allocates nothing. Witness (F162,
  * column-major as lbg_witness holds it), challenges and output v (int16 [len_ring][648]) are device
- * pointers the caller owns; the scratch and tables live in static device arrays (about 1.4 MB per
- * GPU, held until exit). At most LBG_FOLD_STATIC_MAX_COLUMNS columns; larger shapes are rejected.
+ * pointers the caller owns; the scratch and tables live in static device arrays (about 4 MB per
+ * GPU, held until exit). Columns of at most 4096 ring elements are split over several CTAs whose
+ * sums meet in that scratch, so short columns still fill the SMs. At most LBG_FOLD_STATIC_MAX_COLUMNS columns; larger shapes are rejected.
  * The first call on a device sets it up and synchronises (make it before any stream capture);
  * calls share the scratch, so calls that overlap on the GPU race. Asynchronous on `stream`. */
 #define LBG_FOLD_STATIC_MAX_COLUMNS 1024

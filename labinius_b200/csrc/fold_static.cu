@@ -3,8 +3,9 @@
 // Some callers of this library may not call cudaMalloc at the moment they fold: a prover embedded
 // in a runtime that owns all device memory through its own arena, or one that replays its steps
 // inside a stream it must not disturb with allocator calls. For them this file provides one entry
-// point that allocates no device memory: the fold's scratch (the challenges' slot values) lives in
-// a file-scope static device array of fixed size, and so do the per-prime tables the fold reads.
+// point that allocates no device memory: the fold's scratch (the challenges' slot values, and for
+// short columns the per-position sums) lives in file-scope static device arrays of fixed size, and
+// so do the per-prime tables the fold reads.
 // The caller passes the witness, the challenges and the output in device memory it owns.
 //
 // Limits and behaviour, for the caller:
@@ -16,6 +17,7 @@
 //  * all calls share the one scratch array: two calls whose work overlaps on the GPU race.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -33,17 +35,27 @@ namespace {
 
 constexpr size_t MAX_COLUMNS = LBG_FOLD_STATIC_MAX_COLUMNS;
 constexpr size_t SCRATCH_BYTES = MAX_COLUMNS * N162 * sizeof(uint32_t);  // 648 KiB of slot values
+// Positions (ring elements of one column) up to which the columns may be split over several CTAs,
+// each adding its columns' share into the per-position sums below. Longer columns already give
+// every SM a CTA of their own and fold in one pass; the split pays only below this length.
+constexpr size_t SPLIT_MAX_POSITIONS = 4096;
+constexpr size_t SUMS_BYTES = SPLIT_MAX_POSITIONS * N162 * sizeof(uint32_t);  // 2.53 MiB
 
 // The scratch: the challenges' slot values c_j(-theta^v), shared by every call on the device.
 static __device__ __align__(256) uint8_t g_fold_scratch[SCRATCH_BYTES];
+// The per-position sums of a split fold, shared by every call on the device like the slot values.
+static __device__ __align__(256) uint32_t g_fold_sums[SUMS_BYTES / sizeof(uint32_t)];
 // The fold's read-only per-prime tables, one slot per supported prime.
 static __device__ __align__(256) DevPrime g_fold_tables[7];
 
 struct DeviceState {
   bool ready = false;
   uint8_t* scratch = nullptr;
+  uint32_t* sums = nullptr;
   DevPrime* tables = nullptr;
+  int sms = 0;
   bool uploaded[7] = {false, false, false, false, false, false, false};
+  int blocks_per_sm[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 constexpr int MAX_DEVICES = 64;
 DeviceState g_state[MAX_DEVICES];
@@ -84,8 +96,12 @@ int setup(int dev, int pi, uint32_t q, DeviceState** out) {
   if (!S.ready) {
     cudaError_t e = cudaGetSymbolAddress((void**)&S.scratch, g_fold_scratch);
     if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    e = cudaGetSymbolAddress((void**)&S.sums, g_fold_sums);
+    if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("cudaGetSymbolAddress(sums): ") + cudaGetErrorString(e));
     e = cudaGetSymbolAddress((void**)&S.tables, g_fold_tables);
     if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("cudaGetSymbolAddress(tables): ") + cudaGetErrorString(e));
+    e = cudaDeviceGetAttribute(&S.sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("SM count: ") + cudaGetErrorString(e));
     S.ready = true;
   }
   if (!S.uploaded[pi]) {
@@ -102,10 +118,33 @@ int setup(int dev, int pi, uint32_t q, DeviceState** out) {
     if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("twiddle upload: ") + cudaGetErrorString(e));
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("set-up: ") + cudaGetErrorString(e));
+    S.blocks_per_sm[pi] = std::max(1, fold_blocks_per_sm(pi));
     S.uploaded[pi] = true;
   }
   *out = &S;
   return LBG_OK;
+}
+
+// Columns per split for a fold of `wdim` positions: the split count whose waves of CTAs (position
+// tiles x splits over the SMs' resident slots) cost the fewest column steps. 0 keeps one pass.
+int static_cols_per_split(const DeviceState& S, int pi, size_t wdim, int cols) {
+  if (wdim > SPLIT_MAX_POSITIONS) return 0;
+  const long tiles = (long)((wdim + fold_positions_per_cta() - 1) / fold_positions_per_cta());
+  const long slots = (long)S.sms * S.blocks_per_sm[pi];
+  const int step = fold_cols_per_step();
+  long best = -1;
+  int best_per = cols;
+  for (int ns = 1; ns <= (cols + step - 1) / step; ns++) {
+    int per = (cols + ns - 1) / ns;
+    per = (per + step - 1) / step * step;
+    long items = tiles * ((cols + per - 1) / per);
+    long cost = (items + slots - 1) / slots * per;
+    if (best < 0 || cost < best) {
+      best = cost;
+      best_per = per;
+    }
+  }
+  return best_per < cols ? best_per : 0;
 }
 
 }  // namespace
@@ -138,8 +177,11 @@ int lbg_fold_static(uint32_t base_prime, uint32_t witness_log_len, uint32_t colu
   uint32_t* d_chat = (uint32_t*)S->scratch;
   // every slot value of the r challenges is rewritten by the first launch, so nothing needs clearing
   e = launch_challenge_slots(pi, (const lbg_challenge_d*)d_challenges, (int)r, S->tables + pi, d_chat, st);
+  // short columns leave SMs idle in one pass: split the columns, each split adding into the static sums
+  const int per = static_cols_per_split(*S, pi, wdim, (int)cols);
   if (e == cudaSuccess)
-    e = launch_fold(pi, d_witness, wdim, (int)cols, (int)cols, d_chat, S->tables + pi, nullptr, d_v_out, st);
+    e = launch_fold(pi, d_witness, wdim, (int)cols, per ? per : (int)cols, d_chat, S->tables + pi,
+                    per ? S->sums : nullptr, d_v_out, st);
   if (e != cudaSuccess) return fail(LBG_ERR_CUDA, std::string("lbg_fold_static: ") + cudaGetErrorString(e));
   return LBG_OK;
 }

@@ -1,6 +1,6 @@
 """lbg_fold_static: the fold for callers that may not allocate device memory when they fold (an
 embedding runtime that owns all device memory through its own arena, or one that replays its
-steps where allocator calls are not allowed). Its scratch is a static device array, so it is
+steps where allocator calls are not allowed). Its scratch is in static device arrays, so it is
 checked here against the allocating entry point lbg_fold, twice in a row on the same scratch.
 
 This file is collected last (test_zz_*) and passes both alone in a fresh process and after the
@@ -13,8 +13,11 @@ from rounds import MATRIX_SEED, WITNESS_SEED, product_params
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("shape", [(12, 4, [3889, 2917, 4861], 0), (13, 5, [2917, 9721], 0), (17, 10, [9721, 3889], 0)],
-                         ids=["3889", "2917", "1024-columns"])
+# the first three and the 4096-position shape split their columns over CTAs that add into the static
+# sums; the 8192-position shape folds in one pass
+@pytest.mark.parametrize("shape", [(12, 4, [3889, 2917, 4861], 0), (13, 5, [2917, 9721], 0), (17, 10, [9721, 3889], 0),
+                                   (19, 7, [3889, 9721], 0), (20, 7, [2917, 9721], 0)],
+                         ids=["3889", "2917", "1024-columns", "split-4096-positions", "one-pass-8192-positions"])
 def test_fold_static_matches_fold(shape):
     import torch
 
