@@ -14,10 +14,11 @@ pytestmark = pytest.mark.gpu
 
 
 # the first three and the 4096-position shape split their columns over CTAs that add into the static
-# sums; the 8192-position shape folds in one pass
+# sums; the 8192-position shapes fold in one pass, the last at the 1024-column limit
 @pytest.mark.parametrize("shape", [(12, 4, [3889, 2917, 4861], 0), (13, 5, [2917, 9721], 0), (17, 10, [9721, 3889], 0),
-                                   (19, 7, [3889, 9721], 0), (20, 7, [2917, 9721], 0)],
-                         ids=["3889", "2917", "1024-columns", "split-4096-positions", "one-pass-8192-positions"])
+                                   (19, 7, [3889, 9721], 0), (20, 7, [2917, 9721], 0), (23, 10, [3889, 9721], 0)],
+                         ids=["3889", "2917", "1024-columns", "split-4096-positions", "one-pass-8192-positions",
+                              "one-pass-1024-columns"])
 def test_fold_static_matches_fold(shape):
     import torch
 
