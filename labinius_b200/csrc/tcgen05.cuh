@@ -81,7 +81,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-// Bulk copy (no multicast) of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
+// Bulk copy, to this CTA only, of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
 // this GPU's global memory into this CTA's shared memory; completion is counted on `bar`.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
